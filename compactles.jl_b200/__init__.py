@@ -1,0 +1,13 @@
+"""B200 implementation of CompactLES.jl's RHS-and-step hot path.
+
+Host-side mirror of the reference's operator interface (plan_direction /
+apply_along!, Solver / compute_rhs! / step! / max_rate / filter_state! /
+run!) over the C ABI of libcles.so (include/cles.h).  The CUDA library is
+required: every compute call goes through it and raises if it is missing.
+"""
+from . import abi
+from .problem import (ArtParams, DirichletBC, IdealMixture, IdealSpecies, Numerics, PER3,
+                      PeriodicBC, Prim, Problem, SlipWallBC, StepControl, Transport,
+                      conserved_from_prim, coords, grid_spacing, initialize, interior_slices,
+                      problem_desc, single_species, solver_desc, state_shape, tanh_blend,
+                      taylor_green_problem)

@@ -1,0 +1,312 @@
+"""Host-side frontend: the reference's Problem / Numerics / Prim vocabulary.
+
+Mirrors src/problem.jl (Prim :41-57, conserved_from_prim :76-90, initialize!
+:146-163, tanh_blend :172, Problem :243-252, Numerics :295-306, setup
+:321-345), the IdealMixture EOS (src/physics.jl:104-126), Transport
+(:589-593), ArtParams (src/artificial.jl:50-57) and StepControl
+(src/stepcontrol.jl:116-136).  Pure Python/numpy: it builds the flat
+cles_solver_desc descriptor and evaluates initial conditions on the host.
+Initial-condition callables are evaluated vectorised: ic(x, y, z) receives
+broadcastable numpy coordinate arrays and returns a Prim whose fields may be
+arrays.
+"""
+from dataclasses import dataclass, field
+from typing import Callable, Optional, Sequence, Tuple
+
+import numpy as np
+
+from . import abi
+
+
+# ------------------------------------------------------------------- EOS ----
+@dataclass
+class IdealSpecies:
+    name: str
+    R: float
+    gamma: float
+
+
+@dataclass
+class IdealMixture:
+    sp: Sequence[IdealSpecies]
+
+    @property
+    def Rk(self):
+        return [s.R for s in self.sp]
+
+    @property
+    def cvk(self):
+        return [s.R / (s.gamma - 1) for s in self.sp]
+
+    @property
+    def nspecies(self):
+        return len(self.sp)
+
+
+def single_species(gamma=1.4, R=1.0, name="gas"):
+    """single_species(; gamma, R, name) (src/physics.jl:125-126)."""
+    return IdealMixture([IdealSpecies(name, float(R), float(gamma))])
+
+
+@dataclass
+class Transport:
+    mu0: float = 0.0
+    Pr: float = 0.7
+    Sc: float = 0.7
+
+
+@dataclass
+class ArtParams:
+    enabled: bool = True
+    C_mu: float = 0.002
+    C_beta: float = 1.0
+    C_kappa: float = 0.01
+    C_D: float = 0.01
+    beta_sensor: str = "strain"
+
+
+@dataclass
+class StepControl:
+    predict: float = 0.0
+    max_growth: float = 0.0
+    landing_steps: int = 2
+    dt_min: float = 0.0
+    dt_min_ratio: float = 1e-8
+    retries: int = 0
+    cfl_backoff: float = 0.5
+    savepoint_interval: int = 25
+
+    def __post_init__(self):
+        if self.landing_steps < 1:
+            raise ValueError("StepControl: landing_steps must be >= 1 (1 is a hard clip onto the scheduled time)")
+
+    def to_c(self):
+        c = abi.cles_step_control()
+        for k in ("predict", "max_growth", "landing_steps", "dt_min", "dt_min_ratio",
+                  "retries", "cfl_backoff", "savepoint_interval"):
+            setattr(c, k, getattr(self, k))
+        return c
+
+
+# -------------------------------------------------------------- boundaries --
+class BoundaryCondition:
+    code = None
+
+
+class PeriodicBC(BoundaryCondition):
+    code = abi.CLES_BC_PERIODIC
+
+
+class SlipWallBC(BoundaryCondition):
+    code = abi.CLES_BC_SLIPWALL
+
+
+class DirichletBC(BoundaryCondition):
+    """DirichletBC with a state constant in time: `state` is a Prim (scalar
+    fields) imposed on every node of the face after each stage."""
+    code = abi.CLES_BC_DIRICHLET
+
+    def __init__(self, state):
+        self.state = state
+
+
+PER3 = tuple((PeriodicBC(), PeriodicBC()) for _ in range(3))
+
+
+# ------------------------------------------------------------------- Prim ----
+class Prim:
+    """Prim(; u, p, T_ion, rho, Y): exactly two of p, rho, T_ion."""
+
+    def __init__(self, u=(0.0, 0.0, 0.0), p=None, T_ion=None, rho=None, Y=(1.0,)):
+        given = [v is not None for v in (p, T_ion, rho)]
+        if sum(given) != 2:
+            raise ValueError("Prim: specify exactly two of p, rho, and T_ion; the EOS derives the third")
+        self.u = tuple(u)
+        self.p, self.T_ion, self.rho = p, T_ion, rho
+        self.Y = tuple(Y)
+        tot = sum(np.asarray(y, dtype=np.float64) for y in self.Y)
+        if np.any(np.abs(tot - 1) >= 1e-10):
+            raise ValueError("Prim: mass fractions must sum to 1")
+
+
+def conserved_from_prim(eos, pr):
+    """conserved_from_prim(::NavierStokes1T, ::IdealMixture, pr) (src/problem.jl:76-90),
+    vectorised over array-valued Prim fields; returns a list of n_cons arrays."""
+    N = len(pr.Y)
+    if N != eos.nspecies:
+        raise ValueError(f"Prim carries {N} mass fractions; EOS has {eos.nspecies} species")
+    Rk, cvk = eos.Rk, eos.cvk
+    Rm = 0.0
+    cvm = 0.0
+    for k in range(N):
+        Rm = Rm + pr.Y[k] * Rk[k]
+        cvm = cvm + pr.Y[k] * cvk[k]
+    rho = pr.p / (Rm * pr.T_ion) if pr.rho is None else pr.rho
+    T = pr.p / (rho * Rm) if pr.T_ion is None else pr.T_ion
+    u = pr.u
+    ke = 0.5 * (u[0] ** 2 + u[1] ** 2 + u[2] ** 2)
+    out = [rho * pr.Y[k] for k in range(N)]
+    out += [rho * u[0], rho * u[1], rho * u[2], rho * (cvm * T + ke)]
+    return out
+
+
+def tanh_blend(x, x0, delta):
+    """tanh_blend(x, x0, delta) (src/problem.jl:172)."""
+    return 0.5 * (1 + np.tanh((x - x0) / delta))
+
+
+# ---------------------------------------------------------- Problem/Numerics --
+@dataclass
+class Problem:
+    domain: Tuple[Tuple[float, float], Tuple[float, float], Tuple[float, float]]
+    bcs: tuple
+    ic: Callable
+    name: str = "problem"
+    eos: IdealMixture = field(default_factory=single_species)
+    transport: Transport = field(default_factory=Transport)
+
+
+@dataclass
+class Numerics:
+    n_global: Tuple[int, int, int]
+    deriv: Optional[object] = None       # cles_scheme; None = lele_d1_6()
+    filt: Optional[object] = None        # cles_scheme; None = compact_filter(0.45)
+    art: ArtParams = field(default_factory=ArtParams)
+    cfl: float = 0.5
+    control: StepControl = field(default_factory=StepControl)
+    filter_interval: int = 1
+    n_halo: int = 4
+    precision: str = "fp64"              # "fp64" (drop-in) or "mixed"
+
+
+_BETA = {"strain": abi.CLES_BETA_STRAIN, "gated_strain": abi.CLES_BETA_GATED_STRAIN,
+         "dilatation": abi.CLES_BETA_DILATATION}
+
+
+def solver_desc(n_global, L_domain, bcs, deriv, filt, eos=None, transport=None, art=None,
+                origin=(0.0, 0.0, 0.0), cfl=0.5, filter_interval=1, control=None,
+                n_halo=4, precision="fp64"):
+    """The flat descriptor for Solver(; n_global, L_domain, bcs, ...) (src/rhs.jl:122-135)."""
+    eos = eos or single_species()
+    transport = transport or Transport()
+    art = art or ArtParams()
+    control = control or StepControl()
+    if art.beta_sensor not in _BETA:
+        raise ValueError(f"art.beta_sensor must be :strain, :gated_strain or :dilatation, got :{art.beta_sensor}")
+    d = abi.cles_solver_desc()
+    ncons = eos.nspecies + 4
+    for k in range(3):
+        d.n_global[k] = int(n_global[k])
+        d.L[k] = float(L_domain[k])
+        d.origin[k] = float(origin[k])
+        lo, hi = bcs[k]
+        if (lo.code == abi.CLES_BC_PERIODIC) != (hi.code == abi.CLES_BC_PERIODIC):
+            raise ValueError(f"dimension {k + 1} mixes periodic and non-periodic conditions")
+        if n_global[k] == 1 and lo.code != abi.CLES_BC_PERIODIC:
+            raise ValueError(f"collapsed dimension {k + 1} must use (PeriodicBC(), PeriodicBC())")
+        for s, bc in enumerate((lo, hi)):
+            d.bc[k][s] = bc.code
+            if bc.code == abi.CLES_BC_DIRICHLET:
+                q = conserved_from_prim(eos, bc.state)
+                for c in range(ncons):
+                    d.bc_state[k][s][c] = float(np.asarray(q[c]))
+    if eos.nspecies > abi.CLES_MAX_SPECIES:
+        raise ValueError("too many species")
+    d.n_species = eos.nspecies
+    for k, s in enumerate(eos.sp):
+        d.R[k] = s.R
+        d.gamma[k] = s.gamma
+    d.mu0, d.Pr, d.Sc = transport.mu0, transport.Pr, transport.Sc
+    d.art_enabled = int(art.enabled)
+    d.C_mu, d.C_beta, d.C_kappa, d.C_D = art.C_mu, art.C_beta, art.C_kappa, art.C_D
+    d.beta_sensor = _BETA[art.beta_sensor]
+    d.deriv = deriv
+    d.filt = filt
+    d.cfl = float(cfl)
+    d.filter_interval = int(filter_interval)
+    d.control = control.to_c()
+    d.n_halo = int(n_halo)
+    d.precision = abi.CLES_PREC_MIXED if precision == "mixed" else abi.CLES_PREC_FP64
+    return d
+
+
+def grid_spacing(desc):
+    """h per dimension (src/rhs.jl:198-204): L/N periodic, L/(N-1) closed, 1 collapsed."""
+    h = []
+    for k in range(3):
+        n = desc.n_global[k]
+        if n == 1:
+            h.append(1.0)
+        elif desc.bc[k][0] == abi.CLES_BC_PERIODIC:
+            h.append(desc.L[k] / n)
+        else:
+            h.append(desc.L[k] / (n - 1))
+    return tuple(h)
+
+
+def coords(desc):
+    """Interior node coordinates per dimension (global_xcoord, src/rhs.jl:331-335)."""
+    h = grid_spacing(desc)
+    return tuple(desc.origin[k] + np.arange(desc.n_global[k]) * h[k] for k in range(3))
+
+
+def state_shape(desc, layout=abi.CLES_LAYOUT_PADDED):
+    ncons = desc.n_species + 4
+    sh = []
+    for k in (2, 1, 0):
+        n = desc.n_global[k]
+        pad = desc.n_halo if (n > 1 and layout == abi.CLES_LAYOUT_PADDED) else 0
+        sh.append(n + 2 * pad)
+    return (ncons,) + tuple(sh)
+
+
+def interior_slices(desc):
+    sl = []
+    for k in (2, 1, 0):
+        n = desc.n_global[k]
+        pad = desc.n_halo if n > 1 else 0
+        sl.append(slice(pad, pad + n))
+    return tuple(sl)
+
+
+def initialize(desc, ic, eos=None, layout=abi.CLES_LAYOUT_PADDED, Q=None):
+    """initialize!(solver, Q, ic) (src/problem.jl:146-163): evaluate ic at the
+    interior nodes and write the conserved state; halos are left as they are
+    (zero for a fresh array)."""
+    eos = eos or IdealMixture([IdealSpecies(f"species_{k}", desc.R[k], desc.gamma[k])
+                               for k in range(desc.n_species)])
+    if Q is None:
+        Q = np.zeros(state_shape(desc, layout))
+    x, y, z = coords(desc)
+    X = x[None, None, :]
+    Y = y[None, :, None]
+    Z = z[:, None, None]
+    pr = ic(X, Y, Z)
+    q = conserved_from_prim(eos, pr)
+    shape = (desc.n_global[2], desc.n_global[1], desc.n_global[0])
+    sl = interior_slices(desc) if layout == abi.CLES_LAYOUT_PADDED else (slice(None),) * 3
+    for c, qc in enumerate(q):
+        Q[(c,) + sl] = np.broadcast_to(np.asarray(qc, dtype=np.float64), shape)
+    return Q
+
+
+def problem_desc(prob, num, deriv, filt):
+    """Split setup(prob, num) (src/problem.jl:321-345) into the descriptor."""
+    origin = tuple(prob.domain[k][0] for k in range(3))
+    L = tuple(prob.domain[k][1] - prob.domain[k][0] for k in range(3))
+    if not all(v > 0 for v in L):
+        raise ValueError("domain extents must be positive")
+    return solver_desc(num.n_global, L, prob.bcs, deriv, filt, eos=prob.eos,
+                       transport=prob.transport, art=num.art, origin=origin, cfl=num.cfl,
+                       filter_interval=num.filter_interval, control=num.control,
+                       n_halo=num.n_halo, precision=num.precision)
+
+
+# ------------------------------------------------------------- test cases ----
+def taylor_green_problem(p0=71.43):
+    """The README quick-start Taylor-Green vortex on [0, 2pi]^3 (README.md:31-39)."""
+    two_pi = 2 * np.pi
+    return Problem(domain=((0.0, two_pi), (0.0, two_pi), (0.0, two_pi)), bcs=PER3,
+                   ic=lambda x, y, z: Prim(u=(np.sin(x) * np.cos(y), -np.cos(x) * np.sin(y), 0.0 * z),
+                                           p=p0 + 0.0 * x, rho=1.0 + 0.0 * x),
+                   name="taylor_green")

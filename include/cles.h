@@ -1,0 +1,301 @@
+/*
+ * cles.h — C ABI of the B200 implementation of CompactLES.jl's RHS-and-step
+ * hot path (compact derivatives/filters as batched line solves, Cook
+ * artificial properties, flux/RHS assembly, LSRK(5,4) with the CFL rate
+ * reduction).
+ *
+ * Every entry point is `extern "C"`, takes plain pointers and sizes, returns an
+ * int status (CLES_OK on success) and never lets an exception cross the ABI.
+ * The text of the last failure on the calling thread is cles_last_error().
+ *
+ * Citations name the reference function each entry point replaces, as
+ * path:line inside the CompactLES.jl source tree.
+ *
+ * Layouts.  A "padded" field is the reference's own storage
+ * (src/decomposition.jl:129-134): Float64, x fastest, extent n_local[d] +
+ * 2*n_halo on every active dimension and 1 on a collapsed one; a conserved
+ * state appends the component index as the slowest dimension.  An
+ * "interior" field drops the halos (extent n_local[d]).  Halos are never read
+ * by this library: periodic lines wrap by index, closed lines use closure
+ * rows, exactly the values the reference would read from current halos.
+ *
+ * Ownership.  The library allocates and frees its own device memory (plans,
+ * solver state, scratch).  Caller buffers (host or device) are never freed or
+ * retained past the call.  Calls on one solver/plan must be serialised by the
+ * caller (the reference's operators are likewise called from serial sections
+ * only, src/tridiag.jl:133-135); work is ordered on the stream given at
+ * creation.
+ */
+#ifndef CLES_H
+#define CLES_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ----------------------------------------------------- */
+#define CLES_OK        0
+#define CLES_EINVAL    1   /* bad descriptor; same checks as plan_direction (src/operators.jl:50-53) */
+#define CLES_ENOMEM    2   /* device allocation failed or HBM budget exceeded */
+#define CLES_ENUMERIC  3   /* non-finite / non-positive density seen by a kernel */
+#define CLES_ETIMEOUT  4   /* a bounded device wait expired */
+#define CLES_ECUDA     5   /* a CUDA runtime call failed */
+#define CLES_EFAILURE  6   /* run! raised SolverFailure (src/stepcontrol.jl:145-152) */
+
+/* ---- fixed maxima of the descriptors ----------------------------------- */
+#define CLES_MAX_Q        2   /* LHS half-bandwidth (1 tridiagonal, 2 pentadiagonal) */
+#define CLES_MAX_M        4   /* interior RHS half-width (<= n_halo of the reference) */
+#define CLES_MAX_NC       4   /* closure rows per edge */
+#define CLES_MAX_CLO_LEN  8   /* closure RHS stencil length */
+#define CLES_MAX_SPECIES  8
+
+/* element types */
+#define CLES_F64  0
+#define CLES_F32  1
+
+/* field layouts */
+#define CLES_LAYOUT_PADDED    0
+#define CLES_LAYOUT_INTERIOR  1
+
+/* boundary conditions (src/boundary.jl) */
+#define CLES_BC_PERIODIC   0   /* PeriodicBC */
+#define CLES_BC_SLIPWALL   1   /* SlipWallBC, enforce! at src/boundary.jl:232-243 */
+#define CLES_BC_DIRICHLET  2   /* DirichletBC with a state constant in time (src/problem.jl:192-207) */
+
+/* beta sensors (src/artificial.jl:50-57) */
+#define CLES_BETA_STRAIN        0
+#define CLES_BETA_GATED_STRAIN  1
+#define CLES_BETA_DILATATION    2
+
+/* precision modes */
+#define CLES_PREC_FP64   0   /* plain drop-in: everything FP64 */
+#define CLES_PREC_MIXED  1   /* FP32 fields and line solves, FP64 RK state and reductions */
+
+/* SolverFailure reasons (src/stepcontrol.jl:145-204) */
+#define CLES_FAIL_NONE              0
+#define CLES_FAIL_NONFINITE         1
+#define CLES_FAIL_NEGATIVE_DENSITY  2
+#define CLES_FAIL_PLANCK            3
+#define CLES_FAIL_DT_MIN            4
+#define CLES_FAIL_DT_COLLAPSE       5
+
+/* ---- scheme descriptor ------------------------------------------------
+ * One struct covers both CompactScheme (src/kernels.jl:28-50, q = 1) and
+ * BandedCompactScheme (src/kernels_banded.jl:19-39, q >= 1):
+ *   sum_s lhs[s-1] (g_{i-s} + g_{i+s}) + g_i = a0 f_i + sum_m coeffs[m-1] (f_{i+m} ± f_{i-m})
+ * with '+' and a0 for symmetric (filter) schemes, '-' for derivatives.
+ * Closure row j (0-based from the low edge) carries its full centred LHS band
+ * clo_lhs[j][0..2q] (diagonal at index q) and an RHS stencil on f[0..clo_len-1]
+ * counted inward from the edge; high-edge rows are mirrored by the planner
+ * exactly as plan_direction does (src/operators.jl:77-83,
+ * src/operators_banded.jl:91-98). */
+typedef struct cles_scheme {
+    char   name[48];
+    int    q;
+    double lhs[CLES_MAX_Q];
+    double a0;
+    int    M;
+    double coeffs[CLES_MAX_M];
+    int    symmetric;
+    int    nc;
+    double clo_lhs[CLES_MAX_NC][2 * CLES_MAX_Q + 1];
+    int    clo_len[CLES_MAX_NC];
+    double clo_rhs[CLES_MAX_NC][CLES_MAX_CLO_LEN];
+} cles_scheme;
+
+/* Scheme presets; replace lele_d1_6 / pade_d1_4 / compact_filter
+ * (src/kernels.jl:61-111) and lele_d1_10 (src/kernels_banded.jl:54-64). */
+int cles_scheme_lele_d1_6(cles_scheme* out);
+int cles_scheme_pade_d1_4(cles_scheme* out);
+int cles_scheme_compact_filter(double alphaf, cles_scheme* out);
+int cles_scheme_lele_d1_10(cles_scheme* out);
+
+/* ---- grid (the single-rank Decomp, src/decomposition.jl:80-122) -------- */
+typedef struct cles_grid {
+    int n_global[3];
+    int periodic[3];   /* per dimension; a collapsed dimension (n == 1) is inactive */
+    int n_halo;        /* halo width of padded fields on active dimensions (reference default 4) */
+} cles_grid;
+
+/* ---- library context ---------------------------------------------------- */
+typedef struct cles_ctx    cles_ctx;
+typedef struct cles_plan   cles_plan;
+typedef struct cles_solver cles_solver;
+
+/* Device selection and the stream every call of this context is ordered on
+ * (NULL = the legacy default stream).  hbm_budget_bytes = 0 means no budget. */
+int  cles_ctx_create(int device, void* stream, size_t hbm_budget_bytes, cles_ctx** out);
+void cles_ctx_destroy(cles_ctx* ctx);
+int  cles_ctx_set_stream(cles_ctx* ctx, void* stream);
+/* Text of the last failure on this thread ("" if none). */
+const char* cles_last_error(void);
+/* Number of kernels this library has launched so far in this process. */
+int64_t cles_kernel_launches(void);
+
+/* ---- directional plans ---------------------------------------------------
+ * cles_plan_create replaces plan_direction(decomp, scheme, dim, h)
+ * (src/operators.jl:44-101, src/operators_banded.jl:29-125): LHS assembly
+ * with closures, coupling blocks, 1/h prescale, factorisation.  dim is
+ * 1-based like the reference.  dtype CLES_F64 / CLES_F32, layout
+ * CLES_LAYOUT_PADDED / CLES_LAYOUT_INTERIOR.  Returns CLES_EINVAL for the
+ * reference's plan-time errors (extent below max(2nc+1, 2M+1, 2q+1), M > n_halo). */
+int  cles_plan_create(cles_ctx* ctx, const cles_grid* grid, const cles_scheme* scheme,
+                      int dim, double h, int dtype, int layout, cles_plan** out);
+void cles_plan_destroy(cles_plan* plan);
+
+/* cles_apply_along replaces apply_along!(out, plan, f, decomp)
+ * (src/operators.jl:199-215): fill -> batched line solve (+ reduced interface
+ * solve for periodic lines) -> scatter into the interior of out.  f and out
+ * are DEVICE pointers in the plan's layout/dtype; out may equal f. */
+int  cles_apply_along(cles_plan* plan, const void* f_dev, void* out_dev);
+/* Same, over `count` fields spaced `field_stride` elements apart (one launch). */
+int  cles_apply_along_batch(cles_plan* plan, const void* f_dev, void* out_dev,
+                            int count, int64_t field_stride);
+/* Same as cles_apply_along with HOST buffers (copies in and out through
+ * plan-owned device memory).  Float64 padded or interior per the plan. */
+int  cles_apply_along_host(cles_plan* plan, const void* f_host, void* out_host);
+
+/* ---- solver -------------------------------------------------------------- */
+
+/* StepControl (src/stepcontrol.jl:116-136). */
+typedef struct cles_step_control {
+    double predict;
+    double max_growth;
+    int    landing_steps;
+    double dt_min;
+    double dt_min_ratio;
+    int    retries;
+    double cfl_backoff;
+    int    savepoint_interval;
+} cles_step_control;
+void cles_step_control_default(cles_step_control* out);
+
+/* The Solver's scalar configuration (src/rhs.jl:122-135, src/problem.jl:243-306).
+ * Cartesian metric, no stretching, no folds, no sources. */
+typedef struct cles_solver_desc {
+    int    n_global[3];
+    double L[3];                 /* domain extents */
+    double origin[3];            /* low corner */
+    int    bc[3][2];             /* CLES_BC_* per (dim, side) */
+    /* conserved state imposed on a CLES_BC_DIRICHLET face (constant in time) */
+    double bc_state[3][2][CLES_MAX_SPECIES + 4];
+    int    n_species;            /* IdealMixture species count */
+    double R[CLES_MAX_SPECIES];  /* specific gas constants */
+    double gamma[CLES_MAX_SPECIES];
+    double mu0, Pr, Sc;          /* Transport (src/physics.jl:589-593) */
+    int    art_enabled;          /* ArtParams (src/artificial.jl:50-57) */
+    double C_mu, C_beta, C_kappa, C_D;
+    int    beta_sensor;
+    cles_scheme deriv;
+    cles_scheme filt;
+    double cfl;
+    int    filter_interval;
+    cles_step_control control;
+    int    n_halo;               /* halo width of padded host arrays (layout only) */
+    int    precision;            /* CLES_PREC_FP64 / CLES_PREC_MIXED */
+} cles_solver_desc;
+
+/* Defaults of Problem()/Numerics() for a grid: single_species(1.4, R=1),
+ * Transport(), ArtParams(), lele_d1_6, compact_filter(0.45), cfl 0.5,
+ * filter_interval 1, periodic everywhere, domain [0, L). */
+void cles_solver_desc_default(cles_solver_desc* out);
+
+typedef struct cles_solver_info {
+    int     n_local[3];
+    int     active[3];
+    double  h[3];
+    int     n_cons;
+    int     n_species;
+    int64_t cells;
+    int64_t padded_cells;
+    size_t  device_bytes;
+} cles_solver_info;
+
+/* Replaces Solver(...) + plan_direction per active dim (src/rhs.jl:122-311). */
+int  cles_solver_create(cles_ctx* ctx, const cles_solver_desc* desc, cles_solver** out);
+void cles_solver_destroy(cles_solver* s);
+int  cles_solver_info_get(const cles_solver* s, cles_solver_info* out);
+
+/* Conserved state in and out (host arrays, layout CLES_LAYOUT_PADDED or
+ * _INTERIOR, Float64, component slowest).  Output writes the interior only. */
+int  cles_set_state(cles_solver* s, const double* Q_host, int layout);
+int  cles_get_state(cles_solver* s, double* Q_host, int layout);
+/* Device pointer of the resident conserved state (interior layout, Float64,
+ * component stride = cells). */
+int  cles_state_device(cles_solver* s, double** Q_dev);
+
+/* Replaces apply_bcs!(solver, Q) (src/boundary.jl:280-286). */
+int  cles_apply_bcs(cles_solver* s);
+/* Replaces max_rate(solver, Q) (src/timestep.jl:125-175): refreshes the
+ * primitives from the resident state and returns (rate, min density). */
+int  cles_max_rate(cles_solver* s, double* rate, double* rho_min);
+/* Replaces compute_rhs!(solver, Q, dQ, primitives_current) (src/rhs.jl:624-694);
+ * dQ stays on the device (read it with cles_get_rhs). */
+int  cles_compute_rhs(cles_solver* s, int primitives_current);
+int  cles_get_rhs(cles_solver* s, double* dQ_host, int layout);
+/* Replaces step!(solver, Q, dQ, du, dt, prepared) (src/timestep.jl:72-99). */
+int  cles_step(cles_solver* s, double dt, int prepared);
+/* Replaces filter_state!(solver, Q) (src/timestep.jl:414-426). */
+int  cles_filter_state(cles_solver* s);
+
+/* Named solver fields for diagnostics and parity checks (interior, Float64). */
+#define CLES_FIELD_RHO        0
+#define CLES_FIELD_U          1
+#define CLES_FIELD_V          2
+#define CLES_FIELD_W          3
+#define CLES_FIELD_P          4
+#define CLES_FIELD_T          5
+#define CLES_FIELD_C          6
+#define CLES_FIELD_CP         7
+#define CLES_FIELD_MU_ART     8
+#define CLES_FIELD_BETA_ART   9
+#define CLES_FIELD_KAPPA_ART 10
+#define CLES_FIELD_SENSOR    11
+#define CLES_FIELD_Y0        16   /* + species index */
+#define CLES_FIELD_D_ART0    32   /* + species index */
+#define CLES_FIELD_GRAD_U0   48   /* + 3*(d-1) + (j-1): d/dx_d of u_j */
+int  cles_get_field(cles_solver* s, int which, double* host, int layout);
+
+/* Clock of the solver (solver.t, solver.step, solver.cfl). */
+int  cles_get_clock(const cles_solver* s, double* t, int64_t* step, double* cfl);
+int  cles_set_clock(cles_solver* s, double t, int64_t step, double cfl);
+
+/* check_step(control, dt, rho_min, dt_seen, step, t, cfl)
+ * (src/stepcontrol.jl:184-204); *reason = CLES_FAIL_* (CLES_FAIL_NONE = accepted). */
+int  cles_check_step(const cles_step_control* control, double dt, double rho_min,
+                     double dt_seen, int64_t step, double t, double cfl, int* reason);
+
+typedef struct cles_run_result {
+    int64_t steps;        /* steps completed by this call */
+    double  t;            /* solver.t after the call */
+    double  last_dt;
+    double  cfl;          /* solver.cfl after any retries */
+    int     failure;      /* CLES_FAIL_* that ended the run, or CLES_FAIL_NONE */
+    int     retries_used;
+} cles_run_result;
+
+/* Replaces run!(solver, Q; tfinal, nmax, control) without callbacks
+ * (src/timestep.jl:277-405): bcs -> max_rate -> dt/check_step (+ rollback and
+ * CFL backoff) -> step!(prepared) -> filter_state! every filter_interval steps.
+ * Returns CLES_EFAILURE when a SolverFailure is raised. */
+int  cles_run(cles_solver* s, double tfinal, int64_t nmax, cles_run_result* out);
+
+/* Host-buffer drop-in of one run! iteration, the unit the end-to-end
+ * benchmark times: copy Q_host (padded or interior, pinned or pageable) to
+ * the device, do one step of cles_run, copy the state back to Q_host. */
+int  cles_step_host(cles_solver* s, double* Q_host, int layout, double tfinal,
+                    cles_run_result* out);
+
+/* Volume-averaged kinetic energy ∫½ρ|u|²dV / V and dissipation rate
+ * (src/diagnostics.jl:354-378, bench/tgv_energy.jl:175-184) of the resident
+ * state. */
+int  cles_kinetic_energy(cles_solver* s, double* ke);
+int  cles_dissipation_rate(cles_solver* s, double* eps);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CLES_H */

@@ -1,0 +1,1317 @@
+// CPU FP64 oracle for the RHS-and-step hot path of CompactLES.jl.
+//
+// TEST INFRASTRUCTURE ONLY.  This file restates the reference's Julia
+// algorithm in C++ so that the CUDA library can be checked against it and so
+// that the CPU baseline can be timed.  Only tests/, __graft_entry__.smoke()
+// and bench.py's CPU-baseline / reference arm may load it.  Nothing in the
+// product links or calls it.
+//
+// Parity status: the reference is Julia and Julia is not available where
+// this runs, so bit-level agreement with the Julia runtime is unpinned.  The
+// restatement is pinned by the reference's own known-answer tests (spectral
+// accuracy, polynomial exactness, freestream, conservation, filter constants,
+// convergence orders, Sod/Lax/Shu-Osher/Woodward-Colella measured numbers and
+// stored profiles), which tests/test_oracle_*.py reproduce.
+//
+// Storage follows the reference (src/decomposition.jl:129-134): each field is
+// a padded array, x fastest, n_local + 2*n_halo per active dimension, and the
+// conserved state appends the component as the slowest index.  Loop order and
+// floating-point association follow the cited Julia lines; the file is
+// compiled with -ffp-contract=off so a*b+c is never fused, matching Julia
+// without @fastmath/muladd.
+//
+// The distributed spike solve (LineSolver / BandLineSolver with P > 1 ranks
+// along a dimension, src/tridiag.jl:85-170, src/banded.jl:108-214) is
+// restated too: a plan may emulate P ranks along its dimension in one
+// process, with the Allgather replaced by direct reads of every rank's ends.
+
+#include "../include/cles.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <limits>
+#include <memory>
+#include <string>
+#include <vector>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+namespace {
+
+// ---------------------------------------------------------------- helpers --
+
+// Julia's max/min on Float64: NaN wins, -0.0 < 0.0 (Base.max/min semantics).
+inline double jl_max(double x, double y) {
+    if (std::isnan(x)) return x;
+    if (std::isnan(y)) return y;
+    if (y > x) return y;
+    if (x > y) return x;
+    return std::signbit(x) ? y : x;
+}
+inline double jl_min(double x, double y) {
+    if (std::isnan(x)) return x;
+    if (std::isnan(y)) return y;
+    if (y < x) return y;
+    if (x < y) return x;
+    return std::signbit(x) ? x : y;
+}
+inline int jl_mod(int a, int n) { int r = a % n; return r < 0 ? r + n : r; }
+
+thread_local std::string g_err;
+
+// Minimum work (grid points) for a threaded region, as THREAD_MIN_WORK = 2^15
+// in src/threading.jl:47; below it loops run inline.
+const long kThreadMinWork = 1L << 15;
+void set_err(const std::string& s) { g_err = s; }
+
+// ----------------------------------------------------------- decomposition --
+// Single-process Decomp (src/decomposition.jl:80-122): n_local = n_global,
+// one rank in every sub-communicator.
+struct Decomp {
+    int ng[3];
+    bool periodic[3];
+    int nh;
+    bool active[3];
+    int nhd[3];
+    int nl[3];
+    int full[3];
+    size_t size() const { return (size_t)full[0] * full[1] * full[2]; }
+    // 0-based padded index
+    size_t at(int i, int j, int k) const { return (size_t)i + (size_t)full[0] * ((size_t)j + (size_t)full[1] * k); }
+    // at_lo_edge / at_hi_edge (src/decomposition.jl:137-140), one rank per dim.
+    bool closed(int d) const { return active[d] && !periodic[d]; }
+};
+
+Decomp make_decomp(const int ng[3], const int per[3], int nh) {
+    Decomp D;
+    D.nh = nh;
+    for (int d = 0; d < 3; ++d) {
+        D.ng[d] = ng[d];
+        D.active[d] = ng[d] > 1;
+        D.periodic[d] = D.active[d] ? (per[d] != 0) : true;
+        D.nhd[d] = D.active[d] ? nh : 0;
+        D.nl[d] = ng[d];
+        D.full[d] = ng[d] + 2 * D.nhd[d];
+    }
+    return D;
+}
+
+// local_range (src/decomposition.jl:73-78)
+void local_range(int N, int P, int r, int* n, int* off) {
+    int base = N / P, rem = N % P;
+    *n = base + (r < rem ? 1 : 0);
+    *off = r * base + std::min(r, rem);
+}
+
+// ------------------------------------------------------------------- halos --
+// wrap_dim! (src/halo.jl:27-36) for one field: periodic self-copy of n_halo
+// planes.  Used under selfwrap (periodic, one rank) only; closed dims are
+// left stale exactly like a PROC_NULL Sendrecv.
+void wrap_dim(const Decomp& D, double* f, int d) {
+    if (!D.active[d] || !D.periodic[d]) return;
+    const int nh = D.nh, n = D.nl[d];
+    const int F0 = D.full[0], F1 = D.full[1], F2 = D.full[2];
+    auto copy_plane = [&](int dst, int src) {
+        if (d == 0) {
+            for (int k = 0; k < F2; ++k)
+                for (int j = 0; j < F1; ++j) f[D.at(dst, j, k)] = f[D.at(src, j, k)];
+        } else if (d == 1) {
+            for (int k = 0; k < F2; ++k)
+                std::memcpy(&f[D.at(0, dst, k)], &f[D.at(0, src, k)], sizeof(double) * F0);
+        } else {
+            std::memcpy(&f[D.at(0, 0, dst)], &f[D.at(0, 0, src)], sizeof(double) * (size_t)F0 * F1);
+        }
+    };
+    // low halos 1:nh <- n+1:n+nh ; high halos n+nh+1:n+2nh <- nh+1:2nh (1-based)
+    for (int t = 0; t < nh; ++t) copy_plane(t, n + t);
+    for (int t = 0; t < nh; ++t) copy_plane(n + nh + t, nh + t);
+}
+// exchange_halos! (src/halo.jl:84-89): dims in order x, y, z.
+void exchange_halos(const Decomp& D, double* f) {
+    for (int d = 0; d < 3; ++d) wrap_dim(D, f, d);
+}
+// copy_interior! (src/halo.jl:102-112)
+void copy_interior(const Decomp& D, double* dst, const double* src) {
+    const int o1 = D.nhd[0], o2 = D.nhd[1], o3 = D.nhd[2];
+    const long work = (long)D.nl[0] * D.nl[1] * D.nl[2];
+#pragma omp parallel for collapse(2) schedule(static) if (work >= kThreadMinWork)
+    for (int k = 0; k < D.nl[2]; ++k)
+        for (int j = 0; j < D.nl[1]; ++j)
+            for (int i = 0; i < D.nl[0]; ++i) dst[D.at(i + o1, j + o2, k + o3)] = src[D.at(i + o1, j + o2, k + o3)];
+}
+
+// ------------------------------------------------------------------ schemes --
+// Presets restated from src/kernels.jl:61-111 and src/kernels_banded.jl:54-64.
+void scheme_clear(cles_scheme* s) { std::memset(s, 0, sizeof(*s)); }
+
+void set_tri_closure(cles_scheme* s, int j, double sub, double dia, double sup, std::initializer_list<double> rhs) {
+    s->clo_lhs[j][0] = sub; s->clo_lhs[j][1] = dia; s->clo_lhs[j][2] = sup;
+    int n = 0;
+    for (double v : rhs) s->clo_rhs[j][n++] = v;
+    s->clo_len[j] = n;
+}
+
+void preset_lele_d1_6(cles_scheme* s) {
+    scheme_clear(s);
+    std::snprintf(s->name, sizeof(s->name), "Lele C6 first derivative");
+    s->q = 1; s->lhs[0] = 1.0 / 3.0; s->a0 = 0.0;
+    s->M = 2; s->coeffs[0] = 7.0 / 9.0; s->coeffs[1] = 1.0 / 36.0;
+    s->symmetric = 0; s->nc = 2;
+    set_tri_closure(s, 0, 0.0, 1.0, 2.0, {-5.0 / 2.0, 2.0, 1.0 / 2.0});
+    set_tri_closure(s, 1, 1.0 / 4.0, 1.0, 1.0 / 4.0, {-3.0 / 4.0, 0.0, 3.0 / 4.0});
+}
+void preset_pade_d1_4(cles_scheme* s) {
+    scheme_clear(s);
+    std::snprintf(s->name, sizeof(s->name), "Pade C4 first derivative");
+    s->q = 1; s->lhs[0] = 1.0 / 4.0; s->a0 = 0.0;
+    s->M = 1; s->coeffs[0] = 3.0 / 4.0;
+    s->symmetric = 0; s->nc = 1;
+    set_tri_closure(s, 0, 0.0, 1.0, 2.0, {-5.0 / 2.0, 2.0, 1.0 / 2.0});
+}
+void preset_compact_filter(double alphaf, cles_scheme* s) {
+    scheme_clear(s);
+    std::snprintf(s->name, sizeof(s->name), "Gaitonde-Visbal C8 filter");
+    const double af = alphaf;
+    const double a0 = (93 + 70 * af) / 128;
+    const double a1 = (7 + 18 * af) / 16;
+    const double a2 = (-7 + 14 * af) / 32;
+    const double a3 = (1 - 2 * af) / 16;
+    const double a4 = (-1 + 2 * af) / 128;
+    s->q = 1; s->lhs[0] = af; s->a0 = a0;
+    s->M = 4; s->coeffs[0] = a1 / 2; s->coeffs[1] = a2 / 2; s->coeffs[2] = a3 / 2; s->coeffs[3] = a4 / 2;
+    s->symmetric = 1; s->nc = 4;
+    // boundary cascade: row 1 identity; rows 2-4 centred filters of order 2,4,6
+    const double b2[2] = {(1 + 2 * af) / 2, (1 + 2 * af) / 2};
+    const double b4[3] = {(5 + 6 * af) / 8, (1 + 2 * af) / 2, (-1 + 2 * af) / 8};
+    const double b6[4] = {(11 + 10 * af) / 16, (15 + 34 * af) / 32, (-3 + 6 * af) / 16, (1 - 2 * af) / 32};
+    auto ctr = [&](int j, const double* c, int len) {
+        // [c[m+1]/2 for m = len-1..1] ; c[1] ; [c[m+1]/2 for m = 1..len-1]
+        int n = 0;
+        for (int m = len - 1; m >= 1; --m) s->clo_rhs[j][n++] = c[m] / 2;
+        s->clo_rhs[j][n++] = c[0];
+        for (int m = 1; m <= len - 1; ++m) s->clo_rhs[j][n++] = c[m] / 2;
+        s->clo_len[j] = n;
+    };
+    s->clo_lhs[0][0] = 0.0; s->clo_lhs[0][1] = 1.0; s->clo_lhs[0][2] = 0.0;
+    s->clo_rhs[0][0] = 1.0; s->clo_len[0] = 1;
+    for (int j = 1; j < 4; ++j) { s->clo_lhs[j][0] = af; s->clo_lhs[j][1] = 1.0; s->clo_lhs[j][2] = af; }
+    ctr(1, b2, 2);
+    ctr(2, b4, 3);
+    ctr(3, b6, 4);
+}
+void preset_lele_d1_10(cles_scheme* s) {
+    scheme_clear(s);
+    std::snprintf(s->name, sizeof(s->name), "Lele C10 first derivative");
+    s->q = 2; s->lhs[0] = 1.0 / 2.0; s->lhs[1] = 1.0 / 20.0; s->a0 = 0.0;
+    s->M = 3; s->coeffs[0] = 17.0 / 24.0; s->coeffs[1] = 101.0 / 600.0; s->coeffs[2] = 1.0 / 600.0;
+    s->symmetric = 0; s->nc = 3;
+    const double l0[5] = {0, 0, 1, 2, 0}, l1[5] = {0, 1.0 / 4.0, 1, 1.0 / 4.0, 0}, l2[5] = {0, 1.0 / 3.0, 1, 1.0 / 3.0, 0};
+    const double r0[3] = {-5.0 / 2.0, 2.0, 1.0 / 2.0}, r1[3] = {-3.0 / 4.0, 0.0, 3.0 / 4.0};
+    const double r2[5] = {-1.0 / 36.0, -7.0 / 9.0, 0.0, 7.0 / 9.0, 1.0 / 36.0};
+    for (int t = 0; t < 5; ++t) { s->clo_lhs[0][t] = l0[t]; s->clo_lhs[1][t] = l1[t]; s->clo_lhs[2][t] = l2[t]; }
+    for (int t = 0; t < 3; ++t) { s->clo_rhs[0][t] = r0[t]; s->clo_rhs[1][t] = r1[t]; }
+    for (int t = 0; t < 5; ++t) s->clo_rhs[2][t] = r2[t];
+    s->clo_len[0] = 3; s->clo_len[1] = 3; s->clo_len[2] = 5;
+}
+
+// ------------------------------------------------------------- dense LU ------
+// The reduced interface system is LU-factorised by LinearAlgebra.lu! (LAPACK
+// getrf, partial pivoting) and solved by ldiv! (getrs) at src/tridiag.jl:123,157
+// and src/banded.jl:169,199.  Restated as the unblocked right-looking getf2
+// (pivot = first max |a|, column scaled by the reciprocal of the pivot) and
+// getrs (row swaps, unit-lower forward, upper backward with division).
+struct DenseLU {
+    int n = 0;
+    std::vector<double> a;  // column-major n x n, L\U
+    std::vector<int> piv;
+    void factor(std::vector<double> A, int nn) {
+        n = nn; a = std::move(A); piv.assign(n, 0);
+        for (int j = 0; j < n; ++j) {
+            int jp = j; double best = std::fabs(a[j + (size_t)n * j]);
+            for (int i = j + 1; i < n; ++i) {
+                double v = std::fabs(a[i + (size_t)n * j]);
+                if (v > best) { best = v; jp = i; }
+            }
+            piv[j] = jp;
+            if (a[jp + (size_t)n * j] != 0.0) {
+                if (jp != j)
+                    for (int c = 0; c < n; ++c) std::swap(a[j + (size_t)n * c], a[jp + (size_t)n * c]);
+                const double r = 1.0 / a[j + (size_t)n * j];
+                for (int i = j + 1; i < n; ++i) a[i + (size_t)n * j] *= r;
+            }
+            for (int c = j + 1; c < n; ++c) {
+                const double t = -a[j + (size_t)n * c];
+                if (t != 0.0)
+                    for (int i = j + 1; i < n; ++i) a[i + (size_t)n * c] += a[i + (size_t)n * j] * t;
+            }
+        }
+    }
+    void solve(double* b) const {  // one right-hand side, in place
+        for (int j = 0; j < n; ++j) if (piv[j] != j) std::swap(b[j], b[piv[j]]);
+        for (int k = 0; k < n; ++k)
+            if (b[k] != 0.0)
+                for (int i = k + 1; i < n; ++i) b[i] -= b[k] * a[i + (size_t)n * k];
+        for (int k = n - 1; k >= 0; --k)
+            if (b[k] != 0.0) {
+                b[k] /= a[k + (size_t)n * k];
+                for (int i = 0; i < k; ++i) b[i] -= b[k] * a[i + (size_t)n * k];
+            }
+    }
+};
+
+// ------------------------------------------------------------ line solvers ---
+// TriFactor + solve_col! (src/tridiag.jl:24-57)
+struct TriFactor {
+    int n = 0;
+    std::vector<double> l, dinv, c;
+    void build(const std::vector<double>& a, const std::vector<double>& b, const std::vector<double>& cc) {
+        n = (int)b.size();
+        l.assign(n, 0.0); dinv.assign(n, 0.0); c = cc;
+        double d = b[0];
+        dinv[0] = 1.0 / d;
+        for (int i = 1; i < n; ++i) {
+            l[i] = a[i] * dinv[i - 1];
+            d = b[i] - l[i] * c[i - 1];
+            dinv[i] = 1.0 / d;
+        }
+    }
+    // x: n values with stride st
+    void solve(double* x, ptrdiff_t st) const {
+        for (int i = 1; i < n; ++i) x[i * st] -= l[i] * x[(i - 1) * st];
+        x[(n - 1) * st] *= dinv[n - 1];
+        for (int i = n - 2; i >= 0; --i) x[i * st] = (x[i * st] - c[i] * x[(i + 1) * st]) * dinv[i];
+    }
+};
+
+// BandFactor + solve_col! (src/banded.jl:31-80).  Ab[(q+s) + (2q+1)*i] = A[i,i+s].
+struct BandFactor {
+    int n = 0, q = 0;
+    std::vector<double> L;  // q x n, L[(m-1) + q*k]
+    std::vector<double> U;  // (q+1) x n, U[s + (q+1)*i]
+    void build(const std::vector<double>& Ab, int nn, int qq) {
+        n = nn; q = qq;
+        const int W = 2 * q + 1;
+        std::vector<double> Wk = Ab;
+        L.assign((size_t)q * n, 0.0);
+        for (int k = 0; k < n - 1; ++k) {
+            const double piv = Wk[q + (size_t)W * k];
+            const int mmax = std::min(q, n - 1 - k);
+            for (int m = 1; m <= mmax; ++m) {
+                const int i = k + m;
+                const double lv = Wk[(q - m) + (size_t)W * i] / piv;
+                L[(m - 1) + (size_t)q * k] = lv;
+                for (int t = 1; t <= mmax; ++t)
+                    Wk[(q + t - m) + (size_t)W * i] -= lv * Wk[(q + t) + (size_t)W * k];
+            }
+        }
+        U.assign((size_t)(q + 1) * n, 0.0);
+        for (int i = 0; i < n; ++i)
+            for (int s = 0; s <= std::min(q, n - 1 - i); ++s) U[s + (size_t)(q + 1) * i] = Wk[(q + s) + (size_t)W * i];
+    }
+    // x path (solve_col!, division by the pivot)
+    void solve(double* x, ptrdiff_t st) const {
+        for (int k = 0; k < n - 1; ++k) {
+            const double xk = x[k * st];
+            for (int m = 1; m <= std::min(q, n - 1 - k); ++m) x[(k + m) * st] -= L[(m - 1) + (size_t)q * k] * xk;
+        }
+        for (int i = n - 1; i >= 0; --i) {
+            double acc = x[i * st];
+            for (int t = 1; t <= std::min(q, n - 1 - i); ++t) acc -= U[t + (size_t)(q + 1) * i] * x[(i + t) * st];
+            x[i * st] = acc / U[(size_t)(q + 1) * i];
+        }
+    }
+    // transposed path (solve_lines_t!, src/lines_transposed.jl:86-120):
+    // sequential in-place updates and multiplication by inv(U[1,i]).
+    void solve_t(double* x, ptrdiff_t st) const {
+        for (int k = 0; k < n - 1; ++k)
+            for (int m = 1; m <= std::min(q, n - 1 - k); ++m) {
+                const double lm = L[(m - 1) + (size_t)q * k];
+                if (lm == 0.0) continue;
+                x[(k + m) * st] -= lm * x[k * st];
+            }
+        for (int i = n - 1; i >= 0; --i) {
+            for (int t = 1; t <= std::min(q, n - 1 - i); ++t) x[i * st] -= U[t + (size_t)(q + 1) * i] * x[(i + t) * st];
+            const double u0 = 1.0 / U[(size_t)(q + 1) * i];
+            x[i * st] *= u0;
+        }
+    }
+};
+
+// One emulated rank's share of a line.
+struct RankPart {
+    int n = 0, off = 0;
+    bool lo_closed = false, hi_closed = false;
+    TriFactor tf;             // q == 1 path
+    BandFactor bf;            // q >= 2 path
+    std::vector<double> V, W; // n x q each (column-major: V[i + n*t])
+};
+
+// LineSolver / BandLineSolver with P emulated ranks (src/tridiag.jl:59-170,
+// src/banded.jl:82-214, src/lines_transposed.jl:22-151).
+struct DistSolver {
+    int n_global = 0, q = 1, P = 1;
+    bool periodic = false, banded = false, hasred = false;
+    std::vector<RankPart> parts;
+    DenseLU red;
+
+    void solve_local(const RankPart& rp, double* x, ptrdiff_t st, bool transposed) const {
+        if (!banded) rp.tf.solve(x, st);
+        else if (transposed) rp.bf.solve_t(x, st);
+        else rp.bf.solve(x, st);
+    }
+};
+
+// ------------------------------------------------------------------- plans ---
+struct Plan {
+    Decomp D;
+    int dim = 0;           // 0-based
+    int n = 0;
+    int lines = 0;
+    cles_scheme scheme;
+    bool lo_closed = false, hi_closed = false;
+    double a0 = 0.0;
+    std::vector<double> ci;
+    std::vector<std::vector<double>> clo, chi;
+    DistSolver ls;
+};
+
+// Build one rank's local tridiagonal LHS (src/operators.jl:66-84) and its
+// LineSolver pieces (src/tridiag.jl:85-100).
+void build_tri_part(const cles_scheme& s, RankPart& rp) {
+    const int n = rp.n, nc = s.nc;
+    const double al = s.lhs[0];
+    std::vector<double> a(n, al), b(n, 1.0), c(n, al);
+    if (rp.lo_closed)
+        for (int j = 0; j < nc; ++j) { a[j] = s.clo_lhs[j][0]; b[j] = s.clo_lhs[j][1]; c[j] = s.clo_lhs[j][2]; }
+    if (rp.hi_closed)
+        for (int j = 0; j < nc; ++j) {
+            const int r = n - 1 - j;
+            a[r] = s.clo_lhs[j][2]; b[r] = s.clo_lhs[j][1]; c[r] = s.clo_lhs[j][0];
+        }
+    const double aL = rp.lo_closed ? 0.0 : al;
+    const double cR = rp.hi_closed ? 0.0 : al;
+    rp.tf.build(a, b, c);
+    rp.V.assign(n, 0.0); rp.W.assign(n, 0.0);
+    if (aL != 0.0) { rp.V[0] = aL; rp.tf.solve(rp.V.data(), 1); }
+    if (cR != 0.0) { rp.W[n - 1] = cR; rp.tf.solve(rp.W.data(), 1); }
+}
+
+// One rank's banded LHS (src/operators_banded.jl:48-112) and BandLineSolver
+// spikes (src/banded.jl:108-135).
+bool build_band_part(const cles_scheme& s, RankPart& rp) {
+    const int n = rp.n, q = s.q, nc = s.nc, W = 2 * q + 1;
+    std::vector<double> Ab((size_t)W * n, 0.0);
+    for (int i = 0; i < n; ++i) {
+        Ab[q + (size_t)W * i] = 1.0;
+        for (int t = 1; t <= q; ++t) { Ab[(q + t) + (size_t)W * i] = s.lhs[t - 1]; Ab[(q - t) + (size_t)W * i] = s.lhs[t - 1]; }
+    }
+    if (rp.lo_closed)
+        for (int j = 0; j < nc; ++j)
+            for (int t = -q; t <= q; ++t) {
+                if (j + t < 0 && s.clo_lhs[j][q + t] != 0.0) { set_err("closure row references a column before the edge"); return false; }
+                Ab[(q + t) + (size_t)W * j] = s.clo_lhs[j][q + t];
+            }
+    if (rp.hi_closed)
+        for (int j = 0; j < nc; ++j) {
+            const int r = n - 1 - j;
+            for (int t = -q; t <= q; ++t) Ab[(q + t) + (size_t)W * r] = s.clo_lhs[j][q - t];
+        }
+    // Coupling blocks AL[r,t] = lhs[q+r-t] (t >= r), CR[r,t] = lhs[t+q-r] (t <= r), 1-based.
+    std::vector<double> AL((size_t)q * q, 0.0), CR((size_t)q * q, 0.0);
+    if (!rp.lo_closed)
+        for (int r = 1; r <= q; ++r) for (int t = r; t <= q; ++t) AL[(r - 1) + (size_t)q * (t - 1)] = s.lhs[q + r - t - 1];
+    if (!rp.hi_closed)
+        for (int r = 1; r <= q; ++r) for (int t = 1; t <= r; ++t) CR[(r - 1) + (size_t)q * (t - 1)] = s.lhs[t + q - r - 1];
+    rp.bf.build(Ab, n, q);
+    rp.V.assign((size_t)n * q, 0.0); rp.W.assign((size_t)n * q, 0.0);
+    bool alz = true, crz = true;
+    for (double v : AL) alz = alz && v == 0.0;
+    for (double v : CR) crz = crz && v == 0.0;
+    if (!alz)
+        for (int t = 0; t < q; ++t) {
+            for (int r = 0; r < q; ++r) rp.V[r + (size_t)n * t] = AL[r + (size_t)q * t];
+            rp.bf.solve(&rp.V[(size_t)n * t], 1);
+        }
+    if (!crz)
+        for (int t = 0; t < q; ++t) {
+            for (int r = 0; r < q; ++r) rp.W[(n - q + r) + (size_t)n * t] = CR[r + (size_t)q * t];
+            rp.bf.solve(&rp.W[(size_t)n * t], 1);
+        }
+    return true;
+}
+
+// Reduced matrix (src/tridiag.jl:100-123, src/banded.jl:136-169).
+void build_reduced(DistSolver& ls) {
+    const int q = ls.q, P = ls.P, m2 = 2 * q, N = m2 * P;
+    std::vector<double> R((size_t)N * N, 0.0);
+    auto Rat = [&](int r, int c) -> double& { return R[r + (size_t)N * c]; };
+    for (int rk = 0; rk < P; ++rk) {
+        const RankPart& rp = ls.parts[rk];
+        const int n = rp.n;
+        if (!ls.banded) {
+            const double v1 = rp.V[0], vn = rp.V[n - 1], w1 = rp.W[0], wn = rp.W[n - 1];
+            const int rlo = 2 * rk, rhi = 2 * rk + 1;
+            Rat(rlo, rlo) += 1; Rat(rhi, rhi) += 1;
+            const int cprev = 2 * jl_mod(rk - 1, P) + 1;
+            const int cnext = 2 * jl_mod(rk + 1, P);
+            Rat(rlo, cprev) += v1; Rat(rlo, cnext) += w1;
+            Rat(rhi, cprev) += vn; Rat(rhi, cnext) += wn;
+        } else {
+            const int rh = m2 * rk, rt = m2 * rk + q;
+            for (int r = 0; r < q; ++r) { Rat(rh + r, rh + r) += 1; Rat(rt + r, rt + r) += 1; }
+            const int cprev = m2 * jl_mod(rk - 1, P) + q;
+            const int cnext = m2 * jl_mod(rk + 1, P);
+            for (int t = 0; t < q; ++t)
+                for (int r = 0; r < q; ++r) {
+                    Rat(rh + r, cprev + t) += rp.V[r + (size_t)n * t];
+                    Rat(rt + r, cprev + t) += rp.V[(n - q + r) + (size_t)n * t];
+                    Rat(rh + r, cnext + t) += rp.W[r + (size_t)n * t];
+                    Rat(rt + r, cnext + t) += rp.W[(n - q + r) + (size_t)n * t];
+                }
+        }
+    }
+    ls.red.factor(R, N);
+}
+
+Plan* plan_create(const Decomp& D, const cles_scheme& s, int dim0, double h, int P) {
+    const int n = D.nl[dim0];
+    const int nc = s.nc, M = s.M, q = s.q;
+    if (!D.active[dim0]) { set_err("dimension is collapsed"); return nullptr; }
+    if (P < 1) P = 1;
+    const int nmin = (q >= 2) ? std::max({2 * nc + 1, 2 * M + 1, 2 * q + 1}) : std::max(2 * nc + 1, 2 * M + 1);
+    int nloc_min = n / P;
+    if (nloc_min < nmin) {
+        set_err("local extent " + std::to_string(nloc_min) + " along dim " + std::to_string(dim0 + 1) +
+                " too small for scheme '" + s.name + "' (need >= " + std::to_string(nmin) + ")");
+        return nullptr;
+    }
+    if (M > D.nh) { set_err("stencil half-width exceeds halo width"); return nullptr; }
+    auto* p = new Plan();
+    p->D = D; p->dim = dim0; p->n = n; p->scheme = s;
+    p->lo_closed = D.closed(dim0);
+    p->hi_closed = D.closed(dim0);
+    p->lines = 1;
+    for (int k = 0; k < 3; ++k) if (k != dim0) p->lines *= D.nl[k];
+    const double hinv = 1.0 / h;
+    const double sgn = s.symmetric ? 1.0 : -1.0;
+    const double scale = s.symmetric ? 1.0 : hinv;
+    p->a0 = s.a0;
+    for (int m = 0; m < M; ++m) p->ci.push_back(s.coeffs[m] * scale);
+    for (int j = 0; j < nc; ++j) {
+        std::vector<double> lo, hi;
+        for (int t = 0; t < s.clo_len[j]; ++t) { lo.push_back(s.clo_rhs[j][t] * scale); hi.push_back(s.clo_rhs[j][t] * (scale * sgn)); }
+        p->clo.push_back(lo); p->chi.push_back(hi);
+    }
+    DistSolver& ls = p->ls;
+    ls.n_global = n; ls.q = q; ls.P = P; ls.periodic = D.periodic[dim0]; ls.banded = (q >= 2);
+    ls.hasred = (P > 1) || ls.periodic;
+    ls.parts.resize(P);
+    for (int r = 0; r < P; ++r) {
+        RankPart& rp = ls.parts[r];
+        local_range(n, P, r, &rp.n, &rp.off);
+        rp.lo_closed = p->lo_closed && r == 0;
+        rp.hi_closed = p->hi_closed && r == P - 1;
+        if (!ls.banded) build_tri_part(s, rp);
+        else if (!build_band_part(s, rp)) { delete p; return nullptr; }
+    }
+    if (ls.hasred) build_reduced(ls);
+    return p;
+}
+
+// _fill_lines! / _fill_t! (src/operators.jl:113-174, :245-309) for one line;
+// reads f through a strided pointer whose index 0 is local interior row 1.
+inline void fill_line(const Plan& p, const double* fl, ptrdiff_t st, double* B, ptrdiff_t bst) {
+    const int n = p.n, M = (int)p.ci.size(), nc = (int)p.clo.size();
+    int i1 = 0, i2 = n - 1;
+    if (p.lo_closed) {
+        for (int jr = 0; jr < nc; ++jr) {
+            const auto& rhs = p.clo[jr];
+            double acc = 0.0;
+            for (size_t k = 0; k < rhs.size(); ++k) acc += rhs[k] * fl[(ptrdiff_t)k * st];
+            B[jr * bst] = acc;
+        }
+        i1 = nc;
+    }
+    if (p.hi_closed) {
+        for (int jr = 0; jr < nc; ++jr) {
+            const auto& rhs = p.chi[jr];
+            double acc = 0.0;
+            for (size_t k = 0; k < rhs.size(); ++k) acc += rhs[k] * fl[(ptrdiff_t)(n - 1 - (int)k) * st];
+            B[(n - 1 - jr) * bst] = acc;
+        }
+        i2 = n - 1 - nc;
+    }
+    if (p.scheme.symmetric) {
+        for (int i = i1; i <= i2; ++i) {
+            double acc = p.a0 * fl[(ptrdiff_t)i * st];
+            for (int m = 1; m <= M; ++m) acc += p.ci[m - 1] * (fl[(ptrdiff_t)(i + m) * st] + fl[(ptrdiff_t)(i - m) * st]);
+            B[i * bst] = acc;
+        }
+    } else {
+        for (int i = i1; i <= i2; ++i) {
+            double acc = 0.0;
+            for (int m = 1; m <= M; ++m) acc += p.ci[m - 1] * (fl[(ptrdiff_t)(i + m) * st] - fl[(ptrdiff_t)(i - m) * st]);
+            B[i * bst] = acc;
+        }
+    }
+}
+
+// solve_lines! / solve_lines_t! for one full line B (n values, stride bst),
+// emulating P ranks along it.
+void solve_line(const Plan& p, double* B, ptrdiff_t bst, bool transposed) {
+    const DistSolver& ls = p.ls;
+    for (const RankPart& rp : ls.parts) ls.solve_local(rp, B + (ptrdiff_t)rp.off * bst, bst, transposed);
+    if (!ls.hasred) return;
+    const int q = ls.q, P = ls.P, m2 = 2 * q;
+    std::vector<double> z((size_t)m2 * P);
+    for (int rk = 0; rk < P; ++rk) {
+        const RankPart& rp = ls.parts[rk];
+        const double* Bl = B + (ptrdiff_t)rp.off * bst;
+        for (int r = 0; r < q; ++r) {
+            z[m2 * rk + r] = Bl[(ptrdiff_t)r * bst];
+            z[m2 * rk + q + r] = Bl[(ptrdiff_t)(rp.n - q + r) * bst];
+        }
+    }
+    ls.red.solve(z.data());
+    for (int rk = 0; rk < P; ++rk) {
+        const RankPart& rp = ls.parts[rk];
+        double* Bl = B + (ptrdiff_t)rp.off * bst;
+        const int n = rp.n;
+        if (!ls.banded) {
+            const int cprev = 2 * jl_mod(rk - 1, P) + 1;
+            const int cnext = 2 * jl_mod(rk + 1, P);
+            const double xl = z[cprev], xr = z[cnext];
+            for (int i = 0; i < n; ++i) Bl[(ptrdiff_t)i * bst] -= rp.V[i] * xl + rp.W[i] * xr;
+        } else {
+            const int cprev = m2 * jl_mod(rk - 1, P) + q;
+            const int cnext = m2 * jl_mod(rk + 1, P);
+            if (!transposed) {
+                for (int i = 0; i < n; ++i) {
+                    double acc = 0.0;
+                    for (int t = 0; t < q; ++t) acc += rp.V[i + (size_t)n * t] * z[cprev + t] + rp.W[i + (size_t)n * t] * z[cnext + t];
+                    Bl[(ptrdiff_t)i * bst] -= acc;
+                }
+            } else {
+                for (int i = 0; i < n; ++i)
+                    for (int t = 0; t < q; ++t)
+                        Bl[(ptrdiff_t)i * bst] -= rp.V[i + (size_t)n * t] * z[cprev + t] + rp.W[i + (size_t)n * t] * z[cnext + t];
+            }
+        }
+    }
+}
+
+// apply_along! (src/operators.jl:199-215).  f must have current halos.
+void apply_along(const Plan& p, double* out, const double* f) {
+    const Decomp& D = p.D;
+    const int d = p.dim, n = p.n;
+    const int o1 = D.nhd[0], o2 = D.nhd[1], o3 = D.nhd[2];
+    int od1, od2;
+    if (d == 0) { od1 = 1; od2 = 2; } else if (d == 1) { od1 = 0; od2 = 2; } else { od1 = 0; od2 = 1; }
+    const int n1 = D.nl[od1];
+    const ptrdiff_t strides[3] = {1, (ptrdiff_t)D.full[0], (ptrdiff_t)D.full[0] * D.full[1]};
+    const ptrdiff_t st = strides[d];
+    const bool transposed = d > 0;
+    const long work = (long)p.lines * n;
+#pragma omp parallel if (work >= kThreadMinWork)
+    {
+        std::vector<double> B(n);
+#pragma omp for schedule(static)
+        for (int l = 0; l < p.lines; ++l) {
+            const int jj = l % n1, kk = l / n1;
+            int idx[3];
+            idx[d] = 0; idx[od1] = jj; idx[od2] = kk;
+            const size_t base = D.at(idx[0] + o1, idx[1] + o2, idx[2] + o3);
+            fill_line(p, f + base, st, B.data(), 1);
+            solve_line(p, B.data(), 1, transposed);
+            for (int i = 0; i < n; ++i) out[base + (size_t)i * st] = B[i];
+        }
+    }
+}
+
+// -------------------------------------------------------------- the solver ---
+struct Savepoint { std::vector<double> Q; double t; int64_t step; };
+
+struct Solver {
+    cles_solver_desc desc;
+    Decomp D;
+    int Ns = 1, ncons = 5, i_mom[3], i_energy;
+    double Rk[CLES_MAX_SPECIES], cvk[CLES_MAX_SPECIES], cpk[CLES_MAX_SPECIES];
+    double h[3];
+    std::unique_ptr<Plan> dplan[3], fplan[3];
+    size_t fs;  // padded field size
+    std::vector<double> Q, dQ, du;
+    std::vector<double> rho, u, v, w, p, T, c, cp;
+    std::vector<std::vector<double>> Y, D_art;
+    std::vector<double> grad_u[3][3], grad_T[3];
+    std::vector<std::vector<double>> grad_Y[3];
+    std::vector<double> mu_art, beta_art, kappa_art, strain, sensor, sensor_sp, tmp_a, tmp_b;
+    std::vector<double> flux[3][CLES_MAX_SPECIES + 4];
+    double t = 0.0, tstage = 0.0, dt_prev = 0.0, rate_prev = 0.0, cfl = 0.5;
+    int64_t step = 0;
+
+    double* comp(std::vector<double>& A, int cidx) { return A.data() + fs * cidx; }
+    double* vel(int j) { return j == 0 ? u.data() : j == 1 ? v.data() : w.data(); }
+};
+
+// _primitives!(::IdealMixture) over the full padded arrays (src/physics.jl:604-653).
+void primitives(Solver& S) {
+    const size_t fs = S.fs;
+    const int Ns = S.Ns;
+    const double* Q = S.Q.data();
+#pragma omp parallel for schedule(static) if ((long)fs >= kThreadMinWork)
+    for (size_t idx = 0; idx < fs; ++idx) {
+        double rho = 0.0;
+        for (int sp = 0; sp < Ns; ++sp) rho += Q[idx + fs * sp];
+        if (rho > 0) {
+            const double ri = 1 / rho;
+            double Rm = 0.0, cvm = 0.0;
+            for (int sp = 0; sp < Ns; ++sp) {
+                Rm += Q[idx + fs * sp] * S.Rk[sp];
+                cvm += Q[idx + fs * sp] * S.cvk[sp];
+                S.Y[sp][idx] = Q[idx + fs * sp] * ri;
+            }
+            Rm *= ri; cvm *= ri;
+            const double uu = Q[idx + fs * S.i_mom[0]] * ri;
+            const double vv = Q[idx + fs * S.i_mom[1]] * ri;
+            const double ww = Q[idx + fs * S.i_mom[2]] * ri;
+            const double e = Q[idx + fs * S.i_energy] * ri - 0.5 * (uu * uu + vv * vv + ww * ww);
+            const double Ti = jl_max(e / cvm, 1e-300);
+            const double pp = rho * Rm * Ti;
+            const double gm = 1 + Rm / cvm;
+            S.rho[idx] = rho; S.u[idx] = uu; S.v[idx] = vv; S.w[idx] = ww;
+            S.p[idx] = pp; S.T[idx] = Ti;
+            S.c[idx] = std::sqrt(gm * Rm * Ti);
+            S.cp[idx] = cvm + Rm;
+        } else {
+            S.rho[idx] = 1; S.u[idx] = 0; S.v[idx] = 0; S.w[idx] = 0;
+            S.p[idx] = 1; S.T[idx] = 1; S.c[idx] = 1; S.cp[idx] = 1;
+            for (int sp = 0; sp < Ns; ++sp) S.Y[sp][idx] = sp == 0 ? 1.0 : 0.0;
+        }
+    }
+}
+
+void exchange_state(Solver& S) {
+    // exchange_state! (src/halo.jl:93-99): per dim, every component.
+    for (int d = 0; d < 3; ++d)
+        for (int cc = 0; cc < S.ncons; ++cc) wrap_dim(S.D, S.comp(S.Q, cc), d);
+}
+
+template <class F>
+void for_interior(const Decomp& D, F&& fn) {
+    const int o1 = D.nhd[0], o2 = D.nhd[1], o3 = D.nhd[2];
+    const long work = (long)D.nl[0] * D.nl[1] * D.nl[2];
+#pragma omp parallel for collapse(2) schedule(static) if (work >= kThreadMinWork)
+    for (int k = 0; k < D.nl[2]; ++k)
+        for (int j = 0; j < D.nl[1]; ++j)
+            for (int i = 0; i < D.nl[0]; ++i) fn(D.at(i + o1, j + o2, k + o3), i, j, k);
+}
+
+void deriv_along(Solver& S, double* out, const double* f, int d) { apply_along(*S.dplan[d], out, f); }
+void filt_along(Solver& S, double* out, const double* f, int d) { apply_along(*S.fplan[d], out, f); }
+
+// compute_primitives_and_gradients! (src/rhs.jl:591-606), Cartesian: the
+// 1/h_d rescale multiplies by exactly 1 and is omitted.
+void primitives_and_gradients(Solver& S, bool primitives_current) {
+    if (!primitives_current) { exchange_state(S); primitives(S); }
+    for (int jj = 0; jj < 3; ++jj)
+        for (int d = 0; d < 3; ++d) {
+            if (S.D.active[d]) deriv_along(S, S.grad_u[d][jj].data(), S.vel(jj), d);
+            else std::fill(S.grad_u[d][jj].begin(), S.grad_u[d][jj].end(), 0.0);
+        }
+}
+
+// delta4_sum! (src/artificial.jl:67-94)
+void delta4_sum(Solver& S, std::vector<double>& out, const double* f, int wpow) {
+    const Decomp& D = S.D;
+    std::fill(out.begin(), out.end(), 0.0);
+    static const double D4[5] = {1.0, -4.0, 6.0, -4.0, 1.0};
+    for (int d = 0; d < 3; ++d) {
+        if (!D.active[d]) continue;
+        const double wd = wpow == 2 ? S.h[d] * S.h[d] : S.h[d];
+        const int nd = D.nl[d];
+        const int lomin = D.closed(d) ? 1 : -1;
+        const int himax = D.closed(d) ? nd : nd + 2;
+        const ptrdiff_t st = d == 0 ? 1 : d == 1 ? (ptrdiff_t)D.full[0] : (ptrdiff_t)D.full[0] * D.full[1];
+        double* o = out.data();
+        for_interior(D, [&](size_t I, int i, int j, int k) {
+            const int il = (d == 0 ? i : d == 1 ? j : k) + 1;
+            double acc = 0.0;
+            for (int m = -2; m <= 2; ++m) {
+                const int ilm = std::min(std::max(il + m, lomin), himax);
+                acc += D4[m + 2] * f[(ptrdiff_t)I + (ptrdiff_t)(ilm - il) * st];
+            }
+            o[I] += wd * std::fabs(acc);
+        });
+    }
+}
+
+// smooth! (src/artificial.jl:98-111)
+void smooth(Solver& S, double* f) {
+    for (int d = 0; d < 3; ++d) {
+        if (!S.D.active[d]) continue;
+        wrap_dim(S.D, f, d);
+        filt_along(S, S.tmp_a.data(), f, d);
+        copy_interior(S.D, f, S.tmp_a.data());
+    }
+}
+
+const double DUCROS_EPS = 1e-32;
+inline double compression_switch(Solver& S, size_t I) {
+    auto g = [&](int d, int j) { return S.grad_u[d][j][I]; };
+    const double div = g(0, 0) + g(1, 1) + g(2, 2);
+    if (!(div < 0)) return 0.0;
+    const double w1 = g(1, 2) - g(2, 1);
+    const double w2 = g(2, 0) - g(0, 2);
+    const double w3 = g(0, 1) - g(1, 0);
+    return div * div / (div * div + w1 * w1 + w2 * w2 + w3 * w3 + DUCROS_EPS);
+}
+
+// compute_artificial! (src/artificial.jl:261-359)
+void compute_artificial(Solver& S) {
+    const cles_solver_desc& A = S.desc;
+    if (!A.art_enabled) return;
+    const Decomp& D = S.D;
+    const double C_mu = A.C_mu, C_beta = A.C_beta, C_kappa = A.C_kappa, C_D = A.C_D;
+    for_interior(D, [&](size_t I, int, int, int) {
+        double ss = 0.0;
+        for (int b = 0; b < 3; ++b)
+            for (int a = 0; a < 3; ++a) {
+                const double Sab = 0.5 * (S.grad_u[a][b][I] + S.grad_u[b][a][I]);
+                ss += Sab * Sab;
+            }
+        S.strain[I] = std::sqrt(ss);
+    });
+    exchange_halos(D, S.strain.data());
+    delta4_sum(S, S.sensor, S.strain.data(), 2);
+    smooth(S, S.sensor.data());
+    for_interior(D, [&](size_t I, int, int, int) {
+        const double rs = S.rho[I] * jl_max(S.sensor[I], 0.0);
+        S.mu_art[I] = C_mu * rs;
+        S.beta_art[I] = C_beta * rs;
+    });
+    if (A.beta_sensor == CLES_BETA_GATED_STRAIN) {
+        for_interior(D, [&](size_t I, int, int, int) { S.beta_art[I] *= compression_switch(S, I); });
+    } else if (A.beta_sensor == CLES_BETA_DILATATION) {
+        for_interior(D, [&](size_t I, int, int, int) {
+            S.tmp_a[I] = S.grad_u[0][0][I] + S.grad_u[1][1][I] + S.grad_u[2][2][I];
+            S.tmp_b[I] = compression_switch(S, I);
+        });
+        exchange_halos(D, S.tmp_a.data());
+        delta4_sum(S, S.sensor, S.tmp_a.data(), 2);
+        smooth(S, S.sensor.data());
+        for_interior(D, [&](size_t I, int, int, int) {
+            S.beta_art[I] = C_beta * S.rho[I] * jl_max(S.sensor[I], 0.0) * S.tmp_b[I];
+        });
+    }
+    // internal energy over the full padded array
+    {
+        const size_t fs = S.fs;
+        const double* Q = S.Q.data();
+        const int m1 = S.i_mom[0], m2 = S.i_mom[1], m3 = S.i_mom[2], ie = S.i_energy;
+#pragma omp parallel for schedule(static) if ((long)fs >= kThreadMinWork)
+        for (size_t I = 0; I < fs; ++I) {
+            const double r = jl_max(S.rho[I], 1e-300);
+            const double q1 = Q[I + fs * m1], q2 = Q[I + fs * m2], q3 = Q[I + fs * m3];
+            const double ke = 0.5 * (q1 * q1 + q2 * q2 + q3 * q3) / r;
+            S.tmp_a[I] = (Q[I + fs * ie] - ke) / r;
+        }
+    }
+    exchange_halos(D, S.tmp_a.data());
+    delta4_sum(S, S.sensor, S.tmp_a.data(), 1);
+    smooth(S, S.sensor.data());
+    const double eps = std::numeric_limits<double>::epsilon();
+    for_interior(D, [&](size_t I, int, int, int) {
+        const double scale = S.rho[I] * S.c[I] / jl_max(S.T[I], eps);
+        S.kappa_art[I] = C_kappa * scale * jl_max(S.sensor[I], 0.0);
+    });
+    if (S.Ns > 1) {
+        for (int sp = 0; sp < S.Ns; ++sp) {
+            delta4_sum(S, S.sensor_sp, S.Y[sp].data(), 1);
+            smooth(S, S.sensor_sp.data());
+            for_interior(D, [&](size_t I, int, int, int) {
+                S.D_art[sp][I] = C_D * S.c[I] * jl_max(S.sensor_sp[I], 0.0);
+            });
+        }
+    }
+}
+
+// _assemble_fluxes! (src/rhs.jl:495-556)
+void assemble_fluxes(Solver& S) {
+    const cles_solver_desc& A = S.desc;
+    const double mu0 = A.mu0, Pr = A.Pr, Sc = A.Sc;
+    const int Ns = S.Ns, m1 = S.i_mom[0], m2 = S.i_mom[1], m3 = S.i_mom[2], ie = S.i_energy;
+    const size_t fs = S.fs;
+    for_interior(S.D, [&](size_t I, int, int, int) {
+        auto g = [&](int d, int j) { return S.grad_u[d][j][I]; };
+        const double r = S.rho[I];
+        const double uv[3] = {S.u[I], S.v[I], S.w[I]};
+        const double pp = S.p[I], Tp = S.T[I], E = S.Q[I + fs * ie];
+        const double mu = mu0 + S.mu_art[I];
+        const double be = S.beta_art[I];
+        const double ka = mu0 * S.cp[I] / Pr + S.kappa_art[I];
+        const double D0 = mu0 / (Sc * r);
+        const double divu = g(0, 0) + g(1, 1) + g(2, 2);
+        const double t11 = mu * (2 * g(0, 0) - (2.0 / 3.0) * divu) + be * divu;
+        const double t22 = mu * (2 * g(1, 1) - (2.0 / 3.0) * divu) + be * divu;
+        const double t33 = mu * (2 * g(2, 2) - (2.0 / 3.0) * divu) + be * divu;
+        const double t12 = mu * (g(0, 1) + g(1, 0));
+        const double t13 = mu * (g(0, 2) + g(2, 0));
+        const double t23 = mu * (g(1, 2) + g(2, 1));
+        const double tau[3][3] = {{t11, t12, t13}, {t12, t22, t23}, {t13, t23, t33}};
+        for (int d = 0; d < 3; ++d) {
+            const double ud = uv[d];
+            const double* td = tau[d];
+            double Vc = 0.0;
+            for (int sp = 0; sp < Ns; ++sp) Vc += (D0 + S.D_art[sp][I]) * S.grad_Y[d][sp][I];
+            double hdiff = 0.0;
+            for (int sp = 0; sp < Ns; ++sp) {
+                const double Dk = D0 + S.D_art[sp][I];
+                const double Jkd = r * (-Dk * S.grad_Y[d][sp][I] + S.Y[sp][I] * Vc);
+                S.flux[d][sp][I] = r * S.Y[sp][I] * ud + Jkd;
+                hdiff += S.cpk[sp] * Tp * Jkd;
+            }
+            S.flux[d][m1][I] = r * ud * uv[0] + (d == 0 ? pp : 0.0) - td[0];
+            S.flux[d][m2][I] = r * ud * uv[1] + (d == 1 ? pp : 0.0) - td[1];
+            S.flux[d][m3][I] = r * ud * uv[2] + (d == 2 ? pp : 0.0) - td[2];
+            S.flux[d][ie][I] = (E + pp) * ud - (uv[0] * td[0] + uv[1] * td[1] + uv[2] * td[2]) - ka * S.grad_T[d][I] + hdiff;
+        }
+    });
+}
+
+// compute_rhs! (src/rhs.jl:624-694), unitgeom branch.
+void compute_rhs(Solver& S, bool primitives_current) {
+    const Decomp& D = S.D;
+    primitives_and_gradients(S, primitives_current);
+    compute_artificial(S);
+    for (int d = 0; d < 3; ++d) {
+        if (!D.active[d]) continue;
+        deriv_along(S, S.grad_T[d].data(), S.T.data(), d);
+        for (int sp = 0; sp < S.Ns; ++sp) deriv_along(S, S.grad_Y[d][sp].data(), S.Y[sp].data(), d);
+    }
+    assemble_fluxes(S);
+    for (int d = 0; d < 3; ++d)
+        for (int cc = 0; cc < S.ncons; ++cc) wrap_dim(D, S.flux[d][cc].data(), d);
+    for (int cc = 0; cc < S.ncons; ++cc) {
+        double* dq = S.comp(S.dQ, cc);
+        for_interior(D, [&](size_t I, int, int, int) { dq[I] = 0; });
+        for (int d = 0; d < 3; ++d) {
+            if (!D.active[d]) continue;
+            deriv_along(S, S.tmp_a.data(), S.flux[d][cc].data(), d);
+            for_interior(D, [&](size_t I, int, int, int) { dq[I] -= S.tmp_a[I]; });
+        }
+    }
+}
+
+// enforce! for SlipWallBC (src/boundary.jl:232-243) and a time-constant
+// DirichletBC (src/problem.jl:209-221).
+void apply_bcs(Solver& S) {
+    const Decomp& D = S.D;
+    const size_t fs = S.fs;
+    for (int d = 0; d < 3; ++d)
+        for (int side = 0; side < 2; ++side) {
+            if (!D.active[d]) continue;
+            const int bc = S.desc.bc[d][side];
+            if (bc == CLES_BC_PERIODIC) continue;
+            const int wall = side == 0 ? 0 : D.nl[d] - 1;
+            int lo[3], hi[3];
+            for (int k = 0; k < 3; ++k) { lo[k] = 0; hi[k] = D.nl[k]; }
+            lo[d] = wall; hi[d] = wall + 1;
+            for (int k = lo[2]; k < hi[2]; ++k)
+                for (int j = lo[1]; j < hi[1]; ++j)
+                    for (int i = lo[0]; i < hi[0]; ++i) {
+                        const size_t I = D.at(i + D.nhd[0], j + D.nhd[1], k + D.nhd[2]);
+                        if (bc == CLES_BC_SLIPWALL) {
+                            double r = 0.0;
+                            for (int sp = 0; sp < S.Ns; ++sp) r += S.Q[I + fs * sp];
+                            const int mc = S.i_mom[d];
+                            const double mn = S.Q[I + fs * mc];
+                            S.Q[I + fs * S.i_energy] -= 0.5 * mn * mn / r;
+                            S.Q[I + fs * mc] = 0;
+                        } else if (bc == CLES_BC_DIRICHLET) {
+                            for (int cc = 0; cc < S.ncons; ++cc) S.Q[I + fs * cc] = S.desc.bc_state[d][side][cc];
+                        }
+                    }
+        }
+}
+
+const double RKA[5] = {0.0, -567301805773.0 / 1357537059087.0, -2404267990393.0 / 2016746695238.0,
+                       -3550918686646.0 / 2091501179385.0, -1275806237668.0 / 842570457699.0};
+const double RKB[5] = {1432997174477.0 / 9575080441755.0, 5161836677717.0 / 13612068292357.0,
+                       1720146321549.0 / 2090206949498.0, 3134564353537.0 / 4481467310338.0,
+                       2277821191437.0 / 14882151754819.0};
+const double RKC[5] = {0.0, 1432997174477.0 / 9575080441755.0, 2526269341429.0 / 6820363962896.0,
+                       2006345519317.0 / 3224310063776.0, 2802321613138.0 / 2924317926251.0};
+
+// step! (src/timestep.jl:72-99)
+void step(Solver& S, double dt, bool prepared) {
+    for (int stage = 0; stage < 5; ++stage) {
+        S.tstage = S.t + RKC[stage] * dt;
+        const bool first_prepared = prepared && stage == 0;
+        if (!first_prepared) apply_bcs(S);
+        compute_rhs(S, first_prepared);
+        const double A = RKA[stage], B = RKB[stage];
+        for (int cc = 0; cc < S.ncons; ++cc) {
+            double* du = S.comp(S.du, cc);
+            double* dq = S.comp(S.dQ, cc);
+            double* q = S.comp(S.Q, cc);
+            for_interior(S.D, [&](size_t I, int, int, int) {
+                const double vv = A * du[I] + dt * dq[I];
+                du[I] = vv;
+                q[I] += B * vv;
+            });
+        }
+    }
+    S.tstage = S.t + dt;
+    apply_bcs(S);
+}
+
+// max_rate (src/timestep.jl:125-175), Cartesian (inv_h = 1).
+void max_rate(Solver& S, double* rate_out, double* rho_min_out) {
+    exchange_state(S);
+    primitives(S);
+    const Decomp& D = S.D;
+    const cles_solver_desc& A = S.desc;
+    const double mu0 = A.mu0, Pr = A.Pr, Sc = A.Sc;
+    const size_t fs = S.fs;
+    double rate = 0.0, rmin = std::numeric_limits<double>::infinity();
+    const int o1 = D.nhd[0], o2 = D.nhd[1], o3 = D.nhd[2];
+    for (int k = 0; k < D.nl[2]; ++k)
+        for (int j = 0; j < D.nl[1]; ++j)
+            for (int i = 0; i < D.nl[0]; ++i) {
+                const size_t I = D.at(i + o1, j + o2, k + o3);
+                double rq = 0.0;
+                for (int sp = 0; sp < S.Ns; ++sp) rq += S.Q[I + fs * sp];
+                rmin = jl_min(rmin, rq);
+                const double r = S.rho[I];
+                const double ri = 1 / r;
+                const double cc = S.c[I], cpp = S.cp[I];
+                const double uv[3] = {S.u[I], S.v[I], S.w[I]};
+                double acc = 0.0, dsum = 0.0;
+                for (int d = 0; d < 3; ++d) {
+                    if (!D.active[d]) continue;
+                    const double idx = 1.0 / S.h[d];
+                    acc += (std::fabs(uv[d]) + cc) * idx;
+                    dsum += idx * idx;
+                }
+                acc += 0.0;  // curvature_rate, Cartesian
+                double Dmax = mu0 / (Sc * r);
+                for (int sp = 0; sp < S.Ns; ++sp) Dmax = jl_max(Dmax, mu0 / (Sc * r) + S.D_art[sp][I]);
+                const double nu = (mu0 + S.mu_art[I] + S.beta_art[I]) * ri +
+                                  (mu0 * cpp / Pr + S.kappa_art[I]) * ri / cpp + Dmax;
+                acc += 2 * nu * dsum;
+                rate = jl_max(rate, acc);
+            }
+    *rate_out = rate;
+    *rho_min_out = rmin;
+}
+
+// filter_state! (src/timestep.jl:414-426)
+void filter_state(Solver& S) {
+    for (int d = 0; d < 3; ++d) {
+        if (!S.D.active[d]) continue;
+        for (int cc = 0; cc < S.ncons; ++cc) wrap_dim(S.D, S.comp(S.Q, cc), d);
+        for (int cc = 0; cc < S.ncons; ++cc) {
+            filt_along(S, S.tmp_a.data(), S.comp(S.Q, cc), d);
+            copy_interior(S.D, S.comp(S.Q, cc), S.tmp_a.data());
+        }
+    }
+}
+
+const double PLANCK_TIME = 5.391247e-44;
+
+// check_step (src/stepcontrol.jl:184-204)
+int check_step(const cles_step_control& c, double dt, double rho_min, double dt_seen) {
+    if (!std::isfinite(dt)) return CLES_FAIL_NONFINITE;
+    if (!(rho_min > 0)) return CLES_FAIL_NEGATIVE_DENSITY;
+    if (!(dt > PLANCK_TIME)) return CLES_FAIL_PLANCK;
+    if (!(dt >= c.dt_min)) return CLES_FAIL_DT_MIN;
+    if (c.dt_min_ratio > 0 && dt_seen > 0)
+        if (!(dt >= c.dt_min_ratio * dt_seen)) return CLES_FAIL_DT_COLLAPSE;
+    return CLES_FAIL_NONE;
+}
+
+// predicted_dt (src/timestep.jl:29-42)
+double predicted_dt(Solver& S, const cles_step_control& c, double rate) {
+    double r = rate;
+    if (c.predict > 0 && S.rate_prev > 0) r = jl_max(r, r + c.predict * (r - S.rate_prev));
+    double dt = S.cfl / r;
+    if (c.max_growth > 0 && S.dt_prev > 0) dt = jl_min(dt, c.max_growth * S.dt_prev);
+    return dt;
+}
+
+// run! without callbacks (src/timestep.jl:277-405)
+int run(Solver& S, double tfinal, int64_t nmax, cles_run_result* res) {
+    const cles_step_control& ctl = S.desc.control;
+    std::unique_ptr<Savepoint> save;
+    if (ctl.retries > 0) save.reset(new Savepoint{S.Q, S.t, S.step});
+    int attempts = 0;
+    double dt_seen = 0.0;
+    int64_t guard_step = -1, done = 0;
+    double last_dt = 0.0;
+    int failure = CLES_FAIL_NONE;
+    while (S.t < tfinal && S.step < nmax) {
+        S.tstage = S.t;
+        apply_bcs(S);
+        double rate, rmin;
+        max_rate(S, &rate, &rmin);
+        double dt = predicted_dt(S, ctl, rate);
+        const int f = check_step(ctl, dt, rmin, dt_seen);
+        if (f != CLES_FAIL_NONE) {
+            if (!save || attempts >= ctl.retries) { failure = f; break; }
+            attempts += 1;
+            const int64_t fail_step = S.step;
+            S.Q = save->Q;
+            S.t = save->t;
+            S.step = save->step;
+            S.cfl *= ctl.cfl_backoff;
+            guard_step = fail_step;
+            S.dt_prev = 0.0; S.rate_prev = 0.0;
+            dt_seen = 0.0;
+            continue;
+        }
+        if (save && ctl.savepoint_interval > 0 && S.step > guard_step && S.step % ctl.savepoint_interval == 0) {
+            save->Q = S.Q; save->t = S.t; save->step = S.step;
+        }
+        dt_seen = jl_max(dt_seen, dt);
+        dt = jl_min(dt, tfinal - S.t);
+        step(S, dt, true);
+        S.t += dt;
+        S.step += 1;
+        S.dt_prev = dt;
+        S.rate_prev = rate;
+        last_dt = dt;
+        ++done;
+        if (S.desc.filter_interval > 0 && S.step % S.desc.filter_interval == 0) filter_state(S);
+    }
+    if (res) {
+        res->steps = done; res->t = S.t; res->last_dt = last_dt; res->cfl = S.cfl;
+        res->failure = failure; res->retries_used = attempts;
+    }
+    return failure == CLES_FAIL_NONE ? CLES_OK : CLES_EFAILURE;
+}
+
+// quad_weight / volume_integral (src/diagnostics.jl:41-80), no folds.
+double quad_weight(const Solver& S, int d, int i) {
+    const Decomp& D = S.D;
+    if (!(D.active[d] && !D.periodic[d])) return 1.0;
+    if (i == 0 || i == D.ng[d] - 1) return 0.5;
+    return 1.0;
+}
+double volume_integral(Solver& S, const double* f) {
+    const Decomp& D = S.D;
+    double dV = 1.0;
+    for (int d = 0; d < 3; ++d) dV *= D.active[d] ? S.h[d] : 1.0;
+    double acc = 0.0;
+    for (int k = 0; k < D.nl[2]; ++k) {
+        const double wk = quad_weight(S, 2, k);
+        for (int j = 0; j < D.nl[1]; ++j) {
+            const double wj = wk * quad_weight(S, 1, j);
+            for (int i = 0; i < D.nl[0]; ++i) {
+                const size_t I = D.at(i + D.nhd[0], j + D.nhd[1], k + D.nhd[2]);
+                acc += wj * quad_weight(S, 0, i) * f[I] / 1.0;
+            }
+        }
+    }
+    return acc * dV;
+}
+
+// dissipation_rate (src/diagnostics.jl:354-378)
+double dissipation_rate(Solver& S) {
+    primitives_and_gradients(S, false);
+    compute_artificial(S);
+    const double mu0 = S.desc.mu0;
+    std::fill(S.tmp_b.begin(), S.tmp_b.end(), 0.0);
+    for_interior(S.D, [&](size_t I, int, int, int) {
+        const double mu = mu0 + S.mu_art[I];
+        const double be = S.beta_art[I];
+        const double divu = S.grad_u[0][0][I] + S.grad_u[1][1][I] + S.grad_u[2][2][I];
+        double acc = 0.0;
+        for (int b = 0; b < 3; ++b)
+            for (int a = 0; a < 3; ++a) {
+                const double tau = mu * (S.grad_u[a][b][I] + S.grad_u[b][a][I]) + (a == b ? (be - 2 * mu / 3) * divu : 0.0);
+                acc += tau * S.grad_u[a][b][I];
+            }
+        S.tmp_b[I] = acc;
+    });
+    return volume_integral(S, S.tmp_b.data()) / volume_integral(S, S.rho.data());
+}
+
+// kinetic energy per unit volume (bench/tgv_energy.jl:175-184 uses rho = Q[1];
+// here the mixture density), divided by the domain volume.
+double kinetic_energy(Solver& S) {
+    const Decomp& D = S.D;
+    const size_t fs = S.fs;
+    double ke = 0.0;
+    for (int k = 0; k < D.nl[2]; ++k)
+        for (int j = 0; j < D.nl[1]; ++j)
+            for (int i = 0; i < D.nl[0]; ++i) {
+                const size_t I = D.at(i + D.nhd[0], j + D.nhd[1], k + D.nhd[2]);
+                double r = 0.0;
+                for (int sp = 0; sp < S.Ns; ++sp) r += S.Q[I + fs * sp];
+                const double q1 = S.Q[I + fs * S.i_mom[0]], q2 = S.Q[I + fs * S.i_mom[1]], q3 = S.Q[I + fs * S.i_mom[2]];
+                ke += 0.5 * (q1 * q1 + q2 * q2 + q3 * q3) / r;
+            }
+    double cellvol = 1.0, vol = 1.0;
+    for (int d = 0; d < 3; ++d) {
+        cellvol *= D.active[d] ? S.h[d] : 1.0;
+        vol *= D.active[d] ? S.desc.L[d] : 1.0;
+    }
+    return ke * cellvol / vol;
+}
+
+Solver* solver_create(const cles_solver_desc& A) {
+    for (int d = 0; d < 3; ++d) {
+        const bool p0 = A.bc[d][0] == CLES_BC_PERIODIC, p1 = A.bc[d][1] == CLES_BC_PERIODIC;
+        if (p0 != p1) { set_err("dimension " + std::to_string(d + 1) + " mixes periodic and non-periodic conditions"); return nullptr; }
+        if (A.n_global[d] < 1) { set_err("n_global must be >= 1"); return nullptr; }
+        if (A.n_global[d] == 1 && !p0) { set_err("collapsed dimension must use (PeriodicBC(), PeriodicBC())"); return nullptr; }
+    }
+    if (A.n_species < 1 || A.n_species > CLES_MAX_SPECIES) { set_err("bad species count"); return nullptr; }
+    auto S = std::make_unique<Solver>();
+    S->desc = A;
+    int per[3];
+    for (int d = 0; d < 3; ++d) per[d] = A.n_global[d] > 1 ? (A.bc[d][0] == CLES_BC_PERIODIC) : 1;
+    S->D = make_decomp(A.n_global, per, A.n_halo);
+    S->Ns = A.n_species; S->ncons = A.n_species + 4;
+    S->i_mom[0] = S->Ns; S->i_mom[1] = S->Ns + 1; S->i_mom[2] = S->Ns + 2; S->i_energy = S->Ns + 3;
+    for (int k = 0; k < S->Ns; ++k) {
+        S->Rk[k] = A.R[k];
+        S->cvk[k] = A.R[k] / (A.gamma[k] - 1);
+        S->cpk[k] = S->Rk[k] + S->cvk[k];
+    }
+    for (int d = 0; d < 3; ++d) {
+        if (!S->D.active[d]) S->h[d] = 1.0;
+        else S->h[d] = S->D.periodic[d] ? A.L[d] / A.n_global[d] : A.L[d] / (A.n_global[d] - 1);
+    }
+    for (int d = 0; d < 3; ++d) {
+        if (!S->D.active[d]) continue;
+        Plan* dp = plan_create(S->D, A.deriv, d, S->h[d], 1);
+        if (!dp) return nullptr;
+        S->dplan[d].reset(dp);
+        Plan* fp = plan_create(S->D, A.filt, d, S->h[d], 1);
+        if (!fp) return nullptr;
+        S->fplan[d].reset(fp);
+    }
+    const size_t fs = S->D.size();
+    S->fs = fs;
+    auto F = [&]() { return std::vector<double>(fs, 0.0); };
+    S->Q.assign(fs * S->ncons, 0.0); S->dQ.assign(fs * S->ncons, 0.0); S->du.assign(fs * S->ncons, 0.0);
+    S->rho = F(); S->u = F(); S->v = F(); S->w = F(); S->p = F(); S->T = F(); S->c = F(); S->cp = F();
+    for (int sp = 0; sp < S->Ns; ++sp) { S->Y.push_back(F()); S->D_art.push_back(F()); }
+    for (int d = 0; d < 3; ++d) {
+        for (int j = 0; j < 3; ++j) S->grad_u[d][j] = F();
+        S->grad_T[d] = F();
+        for (int sp = 0; sp < S->Ns; ++sp) S->grad_Y[d].push_back(F());
+        for (int cc = 0; cc < S->ncons; ++cc) S->flux[d][cc] = F();
+    }
+    S->mu_art = F(); S->beta_art = F(); S->kappa_art = F(); S->strain = F();
+    S->sensor = F(); S->sensor_sp = F(); S->tmp_a = F(); S->tmp_b = F();
+    S->cfl = A.cfl;
+    return S.release();
+}
+
+}  // namespace
+
+// ======================================================================
+// C interface (consumed by tests/ and bench.py through ctypes)
+// ======================================================================
+struct orc_plan { Plan* p; };
+struct orc_solver { Solver* s; };
+
+extern "C" {
+
+const char* orc_last_error(void) { return g_err.c_str(); }
+
+int orc_set_threads(int n) {
+#ifdef _OPENMP
+    if (n > 0) omp_set_num_threads(n);
+    return omp_get_max_threads();
+#else
+    (void)n;
+    return 1;
+#endif
+}
+
+int orc_scheme_lele_d1_6(cles_scheme* s) { preset_lele_d1_6(s); return 0; }
+int orc_scheme_pade_d1_4(cles_scheme* s) { preset_pade_d1_4(s); return 0; }
+int orc_scheme_compact_filter(double af, cles_scheme* s) { preset_compact_filter(af, s); return 0; }
+int orc_scheme_lele_d1_10(cles_scheme* s) { preset_lele_d1_10(s); return 0; }
+
+orc_plan* orc_plan_create(const cles_grid* g, const cles_scheme* s, int dim, double h, int P) {
+    Decomp D = make_decomp(g->n_global, g->periodic, g->n_halo);
+    if (dim < 1 || dim > 3) { set_err("dim must be 1..3"); return nullptr; }
+    Plan* p = plan_create(D, *s, dim - 1, h, P);
+    if (!p) return nullptr;
+    return new orc_plan{p};
+}
+void orc_plan_destroy(orc_plan* p) { if (p) { delete p->p; delete p; } }
+int orc_apply_along(orc_plan* p, const double* f, double* out) { apply_along(*p->p, out, f); return 0; }
+
+void orc_exchange_halos(const cles_grid* g, double* f) {
+    Decomp D = make_decomp(g->n_global, g->periodic, g->n_halo);
+    exchange_halos(D, f);
+}
+void orc_exchange_dim(const cles_grid* g, double* f, int dim) {
+    Decomp D = make_decomp(g->n_global, g->periodic, g->n_halo);
+    wrap_dim(D, f, dim - 1);
+}
+
+orc_solver* orc_solver_create(const cles_solver_desc* d) {
+    Solver* s = solver_create(*d);
+    if (!s) return nullptr;
+    return new orc_solver{s};
+}
+void orc_solver_destroy(orc_solver* s) { if (s) { delete s->s; delete s; } }
+int64_t orc_field_size(orc_solver* s) { return (int64_t)s->s->fs; }
+int orc_set_state(orc_solver* s, const double* Q) { std::memcpy(s->s->Q.data(), Q, sizeof(double) * s->s->Q.size()); return 0; }
+int orc_get_state(orc_solver* s, double* Q) { std::memcpy(Q, s->s->Q.data(), sizeof(double) * s->s->Q.size()); return 0; }
+int orc_get_rhs(orc_solver* s, double* dQ) { std::memcpy(dQ, s->s->dQ.data(), sizeof(double) * s->s->dQ.size()); return 0; }
+int orc_apply_bcs(orc_solver* s) { apply_bcs(*s->s); return 0; }
+int orc_compute_rhs(orc_solver* s, int primitives_current) { compute_rhs(*s->s, primitives_current != 0); return 0; }
+int orc_max_rate(orc_solver* s, double* rate, double* rmin) { max_rate(*s->s, rate, rmin); return 0; }
+int orc_step(orc_solver* s, double dt, int prepared) { step(*s->s, dt, prepared != 0); return 0; }
+int orc_filter_state(orc_solver* s) { filter_state(*s->s); return 0; }
+int orc_run(orc_solver* s, double tfinal, int64_t nmax, cles_run_result* r) { return run(*s->s, tfinal, nmax, r); }
+double orc_kinetic_energy(orc_solver* s) { return kinetic_energy(*s->s); }
+double orc_dissipation_rate(orc_solver* s) { return dissipation_rate(*s->s); }
+int orc_get_clock(orc_solver* s, double* t, int64_t* step_, double* cfl) { *t = s->s->t; *step_ = s->s->step; *cfl = s->s->cfl; return 0; }
+int orc_set_clock(orc_solver* s, double t, int64_t step_, double cfl) { s->s->t = t; s->s->step = step_; s->s->cfl = cfl; return 0; }
+
+// Padded full-array copies of named fields (same codes as CLES_FIELD_*).
+int orc_get_field(orc_solver* so, int which, double* out) {
+    Solver& S = *so->s;
+    const std::vector<double>* src = nullptr;
+    switch (which) {
+        case CLES_FIELD_RHO: src = &S.rho; break;
+        case CLES_FIELD_U: src = &S.u; break;
+        case CLES_FIELD_V: src = &S.v; break;
+        case CLES_FIELD_W: src = &S.w; break;
+        case CLES_FIELD_P: src = &S.p; break;
+        case CLES_FIELD_T: src = &S.T; break;
+        case CLES_FIELD_C: src = &S.c; break;
+        case CLES_FIELD_CP: src = &S.cp; break;
+        case CLES_FIELD_MU_ART: src = &S.mu_art; break;
+        case CLES_FIELD_BETA_ART: src = &S.beta_art; break;
+        case CLES_FIELD_KAPPA_ART: src = &S.kappa_art; break;
+        case CLES_FIELD_SENSOR: src = &S.sensor; break;
+        default:
+            if (which >= CLES_FIELD_Y0 && which < CLES_FIELD_Y0 + S.Ns) src = &S.Y[which - CLES_FIELD_Y0];
+            else if (which >= CLES_FIELD_D_ART0 && which < CLES_FIELD_D_ART0 + S.Ns) src = &S.D_art[which - CLES_FIELD_D_ART0];
+            else if (which >= CLES_FIELD_GRAD_U0 && which < CLES_FIELD_GRAD_U0 + 9) {
+                const int k = which - CLES_FIELD_GRAD_U0;
+                src = &S.grad_u[k / 3][k % 3];
+            }
+    }
+    if (!src) { set_err("unknown field"); return CLES_EINVAL; }
+    std::memcpy(out, src->data(), sizeof(double) * src->size());
+    return 0;
+}
+
+int orc_check_step(const cles_step_control* c, double dt, double rho_min, double dt_seen) {
+    return check_step(*c, dt, rho_min, dt_seen);
+}
+
+}  // extern "C"

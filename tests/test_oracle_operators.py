@@ -1,0 +1,215 @@
+"""Pins the CPU oracle's compact operators against the reference's own
+known-answer tests (test/runtests.jl and test/convergence.jl of CompactLES.jl).
+Each test names the reference lines it restates; tolerances are the
+reference's."""
+import numpy as np
+import pytest
+
+TWO_PI = 2 * np.pi
+
+
+def field_fill(orc, g, fn, h, origin=(0.0, 0.0, 0.0)):
+    f = np.zeros(orc.padded_shape(g))
+    x = origin[0] + np.arange(g.n_global[0]) * h[0]
+    y = origin[1] + np.arange(g.n_global[1]) * h[1]
+    z = origin[2] + np.arange(g.n_global[2]) * h[2]
+    orc.interior(g, f)[...] = np.broadcast_to(fn(x[None, None, :], y[None, :, None], z[:, None, None]),
+                                              orc.interior(g, f).shape)
+    return f, (x, y, z)
+
+
+def ferr(orc, g, f, fn, xyz):
+    x, y, z = xyz
+    ref = np.broadcast_to(fn(x[None, None, :], y[None, :, None], z[:, None, None]), orc.interior(g, f).shape)
+    return float(np.abs(orc.interior(g, f) - ref).max())
+
+
+def periodic_solver_grid(orc, n):
+    g = orc.grid(n, (1, 1, 1))
+    h = [TWO_PI / n[d] for d in range(3)]
+    return g, h
+
+
+def test_c6_periodic_spectral_accuracy(orc):
+    # test/runtests.jl:86-97
+    g, h = periodic_solver_grid(orc, (32, 32, 32))
+    f, xyz = field_fill(orc, g, lambda x, y, z: np.sin(3 * x) * np.cos(2 * y), h)
+    orc.exchange_halos(g, f)
+    s = orc.lele_d1_6()
+    d1 = orc.Plan(g, s, 1, h[0]).apply(f)
+    assert ferr(orc, g, d1, lambda x, y, z: 3 * np.cos(3 * x) * np.cos(2 * y), xyz) < 1e-4
+    d2 = orc.Plan(g, s, 2, h[1]).apply(f)
+    assert ferr(orc, g, d2, lambda x, y, z: -2 * np.sin(3 * x) * np.sin(2 * y), xyz) < 2e-5
+    d3 = orc.Plan(g, s, 3, h[2]).apply(f)
+    assert ferr(orc, g, d3, lambda x, y, z: 0.0 * x, xyz) < 1e-10
+
+
+def test_c10_accuracy_and_closed_polynomial(orc):
+    # test/runtests.jl:99-132
+    g, h = periodic_solver_grid(orc, (32, 32, 32))
+    f, xyz = field_fill(orc, g, lambda x, y, z: np.sin(3 * x) * np.cos(2 * y), h)
+    orc.exchange_halos(g, f)
+    s10 = orc.lele_d1_10()
+    e10 = ferr(orc, g, orc.Plan(g, s10, 1, h[0]).apply(f), lambda x, y, z: 3 * np.cos(3 * x) * np.cos(2 * y), xyz)
+    assert e10 < 1e-7
+    # the reference measures ~2.8e-8 here
+    assert 2.5e-8 < e10 < 3.1e-8
+    assert ferr(orc, g, orc.Plan(g, s10, 2, h[1]).apply(f), lambda x, y, z: -2 * np.sin(3 * x) * np.sin(2 * y), xyz) < 1e-8
+    assert ferr(orc, g, orc.Plan(g, s10, 3, h[2]).apply(f), lambda x, y, z: 0.0 * x, xyz) < 1e-12
+    e6 = ferr(orc, g, orc.Plan(g, orc.lele_d1_6(), 1, h[0]).apply(f), lambda x, y, z: 3 * np.cos(3 * x) * np.cos(2 * y), xyz)
+    assert e10 < e6 / 100
+    # closed domain, C10 closures: deg-3 polynomial exact
+    gc = orc.grid((32, 12, 12), (0, 1, 1))
+    hc = (1.0 / 31, 1.0 / 12, 1.0 / 12)
+    fc, xyzc = field_fill(orc, gc, lambda x, y, z: 1 + 2 * x + 3 * x ** 2 - x ** 3 + 0 * y, hc)
+    orc.exchange_halos(gc, fc)
+    dfc = orc.Plan(gc, s10, 1, hc[0]).apply(fc)
+    assert ferr(orc, gc, dfc, lambda x, y, z: 2 + 6 * x - 3 * x ** 2 + 0 * y, xyzc) < 1e-10
+
+
+def test_pade_c4_order(orc):
+    # test/runtests.jl:134-149
+    errs = []
+    for N in (16, 32, 64):
+        g = orc.grid((N, 12, 12), (1, 1, 1))
+        h = (TWO_PI / N, TWO_PI / 12, TWO_PI / 12)
+        f, xyz = field_fill(orc, g, lambda x, y, z: np.sin(x) + 0 * y, h)
+        orc.exchange_halos(g, f)
+        df = orc.Plan(g, orc.pade_d1_4(), 1, h[0]).apply(f)
+        errs.append(ferr(orc, g, df, lambda x, y, z: np.cos(x) + 0 * y, xyz))
+    p = np.log(errs[0] / errs[2]) / np.log(4)
+    assert 3.5 < p < 4.5
+    assert errs[2] < errs[1] < errs[0]
+
+
+@pytest.mark.parametrize("d", [1, 2, 3])
+def test_closures_polynomial_exactness_every_dim(orc, d):
+    # test/runtests.jl:151-169 (y/z walls, transposed path) and :205-214 (x)
+    ng = tuple(32 if k == d - 1 else 12 for k in range(3))
+    per = tuple(0 if k == d - 1 else 1 for k in range(3))
+    g = orc.grid(ng, per)
+    h = tuple(1.0 / 31 if k == d - 1 else 1.0 / 12 for k in range(3))
+    poly = lambda t: 1 + 2 * t + 3 * t ** 2 - t ** 3
+    dpoly = lambda t: 2 + 6 * t - 3 * t ** 2
+    sel = lambda x, y, z: (x, y, z)[d - 1] + 0 * x + 0 * y + 0 * z
+    f, xyz = field_fill(orc, g, lambda x, y, z: poly(sel(x, y, z)), h)
+    orc.exchange_halos(g, f)
+    for s in (orc.lele_d1_6(), orc.lele_d1_10()):
+        df = orc.Plan(g, s, d, h[d - 1]).apply(f)
+        assert ferr(orc, g, df, lambda x, y, z: dpoly(sel(x, y, z)), xyz) < 1e-10
+
+
+def test_transposed_path_equals_x_path(orc):
+    # test/runtests.jl:190-203
+    n = 24
+    g, h = periodic_solver_grid(orc, (n, n, n))
+    fn = lambda x, y, z: np.sin(2 * x + 0.3) * np.cos(y) + 0.1 + 0 * z
+    f, xyz = field_fill(orc, g, fn, h)
+    gg, _ = field_fill(orc, g, lambda x, y, z: fn(y, x, z), h)
+    orc.exchange_halos(g, f)
+    orc.exchange_halos(g, gg)
+    s = orc.lele_d1_6()
+    d1 = orc.interior(g, orc.Plan(g, s, 1, h[0]).apply(f))
+    d2 = orc.interior(g, orc.Plan(g, s, 2, h[1]).apply(gg))
+    assert np.abs(d1 - np.swapaxes(d2, 1, 2)).max() < 1e-11
+
+
+def filter_field(orc, g, f, s):
+    # filter_field! (src/operators.jl:223-231)
+    h = 1.0
+    for d in (1, 2, 3):
+        if g.n_global[d - 1] <= 1:
+            continue
+        orc.exchange_halos(g, f)
+        tmp = orc.Plan(g, s, d, h).apply(f)
+        orc.interior(g, f)[...] = orc.interior(g, tmp)
+    return f
+
+
+def test_filter_constants_and_nyquist(orc):
+    # test/runtests.jl:216-229
+    g = orc.grid((32, 12, 12), (1, 1, 1))
+    s = orc.compact_filter(0.45)
+    f = np.zeros(orc.padded_shape(g))
+    orc.interior(g, f)[...] = 1.0
+    filter_field(orc, g, f, s)
+    assert np.abs(orc.interior(g, f) - 1.0).max() < 1e-12
+    i = np.arange(1, 33)
+    orc.interior(g, f)[...] = (1.0 + 0.5 * (-1.0) ** i)[None, None, :]
+    filter_field(orc, g, f, s)
+    assert np.abs(orc.interior(g, f)[0, 0, :] - 1.0).max() < 0.35
+
+
+def test_filter_closed_edges_constant(orc):
+    # closure cascade rows sum to 1 + 2 alpha_f: constants pass unchanged
+    g = orc.grid((32, 16, 12), (0, 0, 1))
+    s = orc.compact_filter(0.45)
+    f = np.zeros(orc.padded_shape(g))
+    orc.interior(g, f)[...] = 2.5
+    filter_field(orc, g, f, s)
+    assert np.abs(orc.interior(g, f) - 2.5).max() < 1e-12
+
+
+def _order(Ns, errs):
+    x = np.log(np.array(Ns, float))
+    y = np.log(np.maximum(np.array(errs), 1e-16))
+    n = len(x)
+    return -(n * np.sum(x * y) - x.sum() * y.sum()) / (n * np.sum(x ** 2) - x.sum() ** 2)
+
+
+def _study(orc, scheme, Ns, periodic, L, fld, ref):
+    errs = []
+    for N in Ns:
+        g = orc.grid((N, 12, 12), (1 if periodic else 0, 1, 1))
+        hx = L / N if periodic else L / (N - 1)
+        h = (hx, L / 12, L / 12)
+        f, xyz = field_fill(orc, g, lambda x, y, z: fld(x) + 0 * y, h)
+        orc.exchange_halos(g, f)
+        df = orc.Plan(g, scheme, 1, hx).apply(f)
+        errs.append(ferr(orc, g, df, lambda x, y, z: ref(x) + 0 * y, xyz))
+    return _order(Ns, errs)
+
+
+def test_convergence_orders_match_reference(orc):
+    # test/convergence.jl:103-122 with the measured values printed there:
+    # C6 interior 6.01 | C10 interior 10.04 | C6 wall closures 3.17
+    p6 = _study(orc, orc.lele_d1_6(), (16, 32, 64), True, TWO_PI, np.sin, np.cos)
+    p10 = _study(orc, orc.lele_d1_10(), (16, 24, 32), True, TWO_PI, np.sin, np.cos)
+    pw = _study(orc, orc.lele_d1_6(), (24, 48, 96), False, 1.0,
+                lambda x: np.exp(np.sin(3 * x)), lambda x: 3 * np.cos(3 * x) * np.exp(np.sin(3 * x)))
+    # the reference's own guards (expect, tol) ...
+    assert abs(p6 - 6.0) < 1.2 and abs(p10 - 10.0) < 2.5 and abs(pw - 3.2) < 0.8
+    # ... and its measured values.  C10's finest error is 1.5e-13, where the
+    # rounding of the line solve moves the second decimal of the slope, so it
+    # is held to 0.02 rather than to the printed digits.
+    assert round(p6, 2) == 6.01
+    assert abs(p10 - 10.04) < 0.02
+    assert round(pw, 2) == 3.17
+
+
+@pytest.mark.parametrize("scheme", ["c6", "c10", "filt"])
+@pytest.mark.parametrize("periodic", [True, False])
+@pytest.mark.parametrize("d", [1, 2, 3])
+def test_distributed_spike_reproduces_single_domain(orc, scheme, periodic, d):
+    # The reduced-interface method with P ranks along a dimension reproduces
+    # the single-domain answer (test/mpi_tests.jl:31-37, :117-175).
+    mk = {"c6": orc.lele_d1_6, "c10": orc.lele_d1_10, "filt": lambda: orc.compact_filter(0.45)}[scheme]
+    ng = tuple(48 if k == d - 1 else 8 for k in range(3))
+    g = orc.grid(ng, tuple(1 if (k != d - 1 or periodic) else 0 for k in range(3)))
+    rng = np.random.default_rng(5)
+    f = np.zeros(orc.padded_shape(g))
+    orc.interior(g, f)[...] = rng.standard_normal(orc.interior(g, f).shape)
+    orc.exchange_halos(g, f)
+    h = 0.1
+    ref = orc.interior(g, orc.Plan(g, mk(), d, h, P=1).apply(f))
+    for P in (2, 3, 4):
+        out = orc.interior(g, orc.Plan(g, mk(), d, h, P=P).apply(f))
+        assert np.abs(out - ref).max() <= 1e-12 * np.abs(ref).max()
+
+
+def test_plan_errors_like_plan_direction(orc):
+    # src/operators.jl:50-53: extent below max(2nc+1, 2M+1) is an error
+    g = orc.grid((8, 12, 12), (1, 1, 1))
+    with pytest.raises(ValueError, match="too small"):
+        orc.Plan(g, orc.compact_filter(0.45), 1, 0.1)
+    orc.Plan(g, orc.lele_d1_6(), 1, 0.1)  # 2nc+1 = 5, 2M+1 = 5: fine
