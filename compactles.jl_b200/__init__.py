@@ -11,3 +11,6 @@ from .problem import (ArtParams, DirichletBC, IdealMixture, IdealSpecies, Numeri
                       conserved_from_prim, coords, grid_spacing, initialize, interior_slices,
                       problem_desc, single_species, solver_desc, state_shape, tanh_blend,
                       taylor_green_problem)
+from .api import (ClesError, Context, DirPlan, Solver, SolverFailure, apply_along, build, check_step,
+                  compact_filter, default_context, grid, kernel_launches, lele_d1_10, lele_d1_6, lib,
+                  pade_d1_4, plan_direction, profile_enable, profile_read, setup)

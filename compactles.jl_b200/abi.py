@@ -169,3 +169,12 @@ def step_control_default():
     c.cfl_backoff = 0.5
     c.savepoint_interval = 25
     return c
+
+
+class cles_profile_entry(C.Structure):
+    _fields_ = [
+        ("name", C.c_char * 32),
+        ("launches", C.c_int64),
+        ("total_ms", C.c_double),
+        ("bytes", C.c_double),
+    ]

@@ -1,0 +1,370 @@
+"""ctypes host mirror of the reference's operator interface over libcles.so.
+
+Names follow CompactLES.jl: plan_direction / apply_along (src/operators.jl),
+Solver / compute_rhs / step / max_rate / filter_state / run
+(src/rhs.jl, src/timestep.jl), check_step / SolverFailure
+(src/stepcontrol.jl).  Every compute call goes through the CUDA library; if
+libcles.so is missing or no B200 is visible these raise, there is no CPU
+fallback.
+"""
+import ctypes as C
+import os
+import pathlib
+import subprocess
+
+import numpy as np
+
+from . import abi
+from .problem import grid_spacing, state_shape
+
+_HERE = pathlib.Path(__file__).resolve().parent
+LIB_PATH = _HERE / "libcles.so"
+
+_lib = None
+
+
+class ClesError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"[cles status {code}] {msg}")
+        self.code = code
+
+
+class SolverFailure(RuntimeError):
+    """Raised by run when step control rejects a step (src/stepcontrol.jl:145-152)."""
+
+    def __init__(self, reason, result):
+        super().__init__(f"SolverFailure(:{reason}) at t = {result.t}, cfl = {result.cfl}")
+        self.reason = reason
+        self.result = result
+
+
+def build(jobs=8):
+    """Compile libcles.so in place (nvcc, sm_100a)."""
+    subprocess.run(["make", "-s", "-j", str(jobs), "-C", str(_HERE / "csrc")], check=True)
+
+
+def lib():
+    """The loaded libcles.so (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise ClesError(abi.CLES_ECUDA, f"{LIB_PATH} is missing: build it with compactles_b200.api.build()")
+        L = C.CDLL(str(LIB_PATH))
+        vp = C.c_void_p
+        dp = C.POINTER(C.c_double)
+        L.cles_last_error.restype = C.c_char_p
+        L.cles_kernel_launches.restype = C.c_int64
+        for nm in ("cles_scheme_lele_d1_6", "cles_scheme_pade_d1_4", "cles_scheme_lele_d1_10"):
+            getattr(L, nm).argtypes = [C.POINTER(abi.cles_scheme)]
+        L.cles_scheme_compact_filter.argtypes = [C.c_double, C.POINTER(abi.cles_scheme)]
+        L.cles_ctx_create.argtypes = [C.c_int, vp, C.c_size_t, C.POINTER(vp)]
+        L.cles_ctx_destroy.argtypes = [vp]
+        L.cles_ctx_set_stream.argtypes = [vp, vp]
+        L.cles_plan_create.argtypes = [vp, C.POINTER(abi.cles_grid), C.POINTER(abi.cles_scheme), C.c_int, C.c_double,
+                                       C.c_int, C.c_int, C.POINTER(vp)]
+        L.cles_plan_destroy.argtypes = [vp]
+        L.cles_apply_along.argtypes = [vp, vp, vp]
+        L.cles_apply_along_batch.argtypes = [vp, vp, vp, C.c_int, C.c_int64]
+        L.cles_apply_along_host.argtypes = [vp, vp, vp]
+        L.cles_step_control_default.argtypes = [C.POINTER(abi.cles_step_control)]
+        L.cles_step_control_default.restype = None
+        L.cles_solver_desc_default.argtypes = [C.POINTER(abi.cles_solver_desc)]
+        L.cles_solver_desc_default.restype = None
+        L.cles_solver_create.argtypes = [vp, C.POINTER(abi.cles_solver_desc), C.POINTER(vp)]
+        L.cles_solver_destroy.argtypes = [vp]
+        L.cles_solver_info_get.argtypes = [vp, C.POINTER(abi.cles_solver_info)]
+        L.cles_set_state.argtypes = [vp, vp, C.c_int]
+        L.cles_get_state.argtypes = [vp, vp, C.c_int]
+        L.cles_state_device.argtypes = [vp, C.POINTER(dp)]
+        L.cles_apply_bcs.argtypes = [vp]
+        L.cles_max_rate.argtypes = [vp, dp, dp]
+        L.cles_compute_rhs.argtypes = [vp, C.c_int]
+        L.cles_get_rhs.argtypes = [vp, vp, C.c_int]
+        L.cles_step.argtypes = [vp, C.c_double, C.c_int]
+        L.cles_filter_state.argtypes = [vp]
+        L.cles_get_field.argtypes = [vp, C.c_int, vp, C.c_int]
+        L.cles_get_clock.argtypes = [vp, dp, C.POINTER(C.c_int64), dp]
+        L.cles_set_clock.argtypes = [vp, C.c_double, C.c_int64, C.c_double]
+        L.cles_check_step.argtypes = [C.POINTER(abi.cles_step_control), C.c_double, C.c_double, C.c_double, C.c_int64,
+                                      C.c_double, C.c_double, C.POINTER(C.c_int)]
+        L.cles_run.argtypes = [vp, C.c_double, C.c_int64, C.POINTER(abi.cles_run_result)]
+        L.cles_step_host.argtypes = [vp, vp, C.c_int, C.c_double, C.POINTER(abi.cles_run_result)]
+        L.cles_profile_enable.argtypes = [C.c_int]
+        L.cles_profile_read.argtypes = [C.POINTER(abi.cles_profile_entry), C.c_int, C.POINTER(C.c_int)]
+        L.cles_kinetic_energy.argtypes = [vp, dp]
+        L.cles_dissipation_rate.argtypes = [vp, dp]
+        _lib = L
+    return _lib
+
+
+def _check(rc):
+    if rc != abi.CLES_OK:
+        raise ClesError(rc, lib().cles_last_error().decode())
+
+
+def kernel_launches():
+    return int(lib().cles_kernel_launches())
+
+
+def profile_enable(on=True):
+    """Bracket every compact-operator launch with CUDA events from now on (clears records)."""
+    _check(lib().cles_profile_enable(int(on)))
+
+
+def profile_read():
+    """{name: (launches, total_ms, algorithmic_bytes)} per direction since profile_enable."""
+    arr = (abi.cles_profile_entry * 8)()
+    n = C.c_int()
+    _check(lib().cles_profile_read(arr, 8, C.byref(n)))
+    return {arr[i].name.decode(): (arr[i].launches, arr[i].total_ms, arr[i].bytes) for i in range(n.value)}
+
+
+# ---------------------------------------------------------------- schemes ----
+def lele_d1_6():
+    s = abi.cles_scheme()
+    _check(lib().cles_scheme_lele_d1_6(C.byref(s)))
+    return s
+
+
+def pade_d1_4():
+    s = abi.cles_scheme()
+    _check(lib().cles_scheme_pade_d1_4(C.byref(s)))
+    return s
+
+
+def compact_filter(alphaf=0.45):
+    s = abi.cles_scheme()
+    _check(lib().cles_scheme_compact_filter(float(alphaf), C.byref(s)))
+    return s
+
+
+def lele_d1_10():
+    s = abi.cles_scheme()
+    _check(lib().cles_scheme_lele_d1_10(C.byref(s)))
+    return s
+
+
+def check_step(control, dt, rho_min, dt_seen, step=0, t=0.0, cfl=0.5):
+    """check_step (src/stepcontrol.jl:184-204) -> None or the failure reason."""
+    r = C.c_int()
+    _check(lib().cles_check_step(C.byref(control), float(dt), float(rho_min), float(dt_seen), int(step), float(t),
+                                 float(cfl), C.byref(r)))
+    return abi.FAIL_NAMES[r.value]
+
+
+# ---------------------------------------------------------------- context ----
+class Context:
+    """Device + stream every call is ordered on (cles_ctx)."""
+
+    def __init__(self, device=0, stream=None, hbm_budget=0):
+        self.ptr = C.c_void_p()
+        _check(lib().cles_ctx_create(int(device), C.c_void_p(stream or 0), int(hbm_budget), C.byref(self.ptr)))
+        self.device = device
+
+    def set_stream(self, stream):
+        _check(lib().cles_ctx_set_stream(self.ptr, C.c_void_p(stream or 0)))
+
+    def __del__(self):
+        try:
+            if self.ptr:
+                lib().cles_ctx_destroy(self.ptr)
+                self.ptr = None
+        except Exception:
+            pass
+
+
+_default_ctx = None
+
+
+def default_context():
+    global _default_ctx
+    if _default_ctx is None:
+        _default_ctx = Context(int(os.environ.get("CLES_DEVICE", "0")))
+    return _default_ctx
+
+
+def grid(n_global, periodic, n_halo=4):
+    g = abi.cles_grid()
+    for d in range(3):
+        g.n_global[d] = int(n_global[d])
+        g.periodic[d] = int(bool(periodic[d]))
+    g.n_halo = int(n_halo)
+    return g
+
+
+class DirPlan:
+    """plan_direction(decomp, scheme, dim, h) (src/operators.jl:44-101, src/operators_banded.jl:29-125)."""
+
+    def __init__(self, g, scheme, dim, h, dtype="f64", layout="padded", ctx=None):
+        self.ctx = ctx or default_context()
+        self.g = g
+        self.dim = dim
+        self.dtype = abi.CLES_F64 if dtype in ("f64", np.float64) else abi.CLES_F32
+        self.layout = abi.CLES_LAYOUT_PADDED if layout == "padded" else abi.CLES_LAYOUT_INTERIOR
+        self.ptr = C.c_void_p()
+        _check(lib().cles_plan_create(self.ctx.ptr, C.byref(g), C.byref(scheme), int(dim), float(h), self.dtype,
+                                      self.layout, C.byref(self.ptr)))
+
+    def shape(self):
+        sh = []
+        for k in (2, 1, 0):
+            n = self.g.n_global[k]
+            pad = self.g.n_halo if (n > 1 and self.layout == abi.CLES_LAYOUT_PADDED) else 0
+            sh.append(n + 2 * pad)
+        return tuple(sh)
+
+    def __del__(self):
+        try:
+            if self.ptr:
+                lib().cles_plan_destroy(self.ptr)
+                self.ptr = None
+        except Exception:
+            pass
+
+
+plan_direction = DirPlan
+
+
+def apply_along(out, plan, f):
+    """apply_along!(out, plan, f) (src/operators.jl:199-215).
+
+    numpy arrays: host path (copies through the plan's device buffers);
+    torch CUDA tensors: device path on the context's stream.  Writes the
+    interior of `out`."""
+    if hasattr(f, "data_ptr") and getattr(f, "is_cuda", False):
+        _check(lib().cles_apply_along(plan.ptr, C.c_void_p(f.data_ptr()), C.c_void_p(out.data_ptr())))
+        return out
+    want = np.float64 if plan.dtype == abi.CLES_F64 else np.float32
+    if f.dtype != want or out.dtype != want or not f.flags.c_contiguous or not out.flags.c_contiguous:
+        raise TypeError("apply_along host path needs C-contiguous arrays of the plan's dtype")
+    if f.shape != plan.shape() or out.shape != plan.shape():
+        raise ValueError(f"field shape {f.shape} does not match the plan's {plan.shape()}")
+    _check(lib().cles_apply_along_host(plan.ptr, f.ctypes.data_as(C.c_void_p), out.ctypes.data_as(C.c_void_p)))
+    return out
+
+
+# ----------------------------------------------------------------- solver ----
+class Solver:
+    """Device-resident Solver (src/rhs.jl:17-72) built from a cles_solver_desc."""
+
+    def __init__(self, desc, ctx=None):
+        self.ctx = ctx or default_context()
+        self.desc = desc
+        self.ptr = C.c_void_p()
+        _check(lib().cles_solver_create(self.ctx.ptr, C.byref(desc), C.byref(self.ptr)))
+        self.n_cons = desc.n_species + 4
+        self.h = grid_spacing(desc)
+
+    def __del__(self):
+        try:
+            if self.ptr:
+                lib().cles_solver_destroy(self.ptr)
+                self.ptr = None
+        except Exception:
+            pass
+
+    def info(self):
+        i = abi.cles_solver_info()
+        _check(lib().cles_solver_info_get(self.ptr, C.byref(i)))
+        return i
+
+    def _arr(self, layout, ncomp=None):
+        sh = state_shape(self.desc, layout)
+        if ncomp is not None:
+            sh = (ncomp,) + sh[1:]
+        return np.zeros(sh)
+
+    @staticmethod
+    def _layout(layout):
+        return abi.CLES_LAYOUT_PADDED if layout == "padded" else abi.CLES_LAYOUT_INTERIOR
+
+    def set_state(self, Q, layout="padded"):
+        Q = np.ascontiguousarray(Q, dtype=np.float64)
+        lay = self._layout(layout)
+        if Q.shape != state_shape(self.desc, lay):
+            raise ValueError(f"state shape {Q.shape} != {state_shape(self.desc, lay)}")
+        _check(lib().cles_set_state(self.ptr, Q.ctypes.data_as(C.c_void_p), lay))
+
+    def get_state(self, layout="padded"):
+        lay = self._layout(layout)
+        Q = self._arr(lay)
+        _check(lib().cles_get_state(self.ptr, Q.ctypes.data_as(C.c_void_p), lay))
+        return Q
+
+    def apply_bcs(self):
+        _check(lib().cles_apply_bcs(self.ptr))
+
+    def max_rate(self):
+        r, m = C.c_double(), C.c_double()
+        _check(lib().cles_max_rate(self.ptr, C.byref(r), C.byref(m)))
+        return r.value, m.value
+
+    def compute_rhs(self, primitives_current=False, layout="padded"):
+        _check(lib().cles_compute_rhs(self.ptr, int(primitives_current)))
+        lay = self._layout(layout)
+        dQ = self._arr(lay)
+        _check(lib().cles_get_rhs(self.ptr, dQ.ctypes.data_as(C.c_void_p), lay))
+        return dQ
+
+    def step(self, dt, prepared=False):
+        _check(lib().cles_step(self.ptr, float(dt), int(prepared)))
+
+    def filter_state(self):
+        _check(lib().cles_filter_state(self.ptr))
+
+    def field(self, which, layout="padded"):
+        lay = self._layout(layout)
+        out = self._arr(lay, ncomp=1)[0]
+        _check(lib().cles_get_field(self.ptr, int(which), out.ctypes.data_as(C.c_void_p), lay))
+        return out
+
+    def clock(self):
+        t, s, c = C.c_double(), C.c_int64(), C.c_double()
+        _check(lib().cles_get_clock(self.ptr, C.byref(t), C.byref(s), C.byref(c)))
+        return t.value, s.value, c.value
+
+    def set_clock(self, t, step, cfl):
+        _check(lib().cles_set_clock(self.ptr, float(t), int(step), float(cfl)))
+
+    def run(self, tfinal, nmax=2 ** 62, raise_on_failure=True):
+        """run!(solver, Q; tfinal, nmax) without callbacks (src/timestep.jl:277-405)."""
+        res = abi.cles_run_result()
+        rc = lib().cles_run(self.ptr, float(tfinal), int(nmax), C.byref(res))
+        if rc == abi.CLES_EFAILURE:
+            if raise_on_failure:
+                raise SolverFailure(abi.FAIL_NAMES[res.failure], res)
+            return res
+        _check(rc)
+        return res
+
+    def step_host(self, Q, tfinal, layout="padded"):
+        """One run! iteration on a host state array, updated in place."""
+        res = abi.cles_run_result()
+        rc = lib().cles_step_host(self.ptr, Q.ctypes.data_as(C.c_void_p), self._layout(layout), float(tfinal),
+                                  C.byref(res))
+        if rc not in (abi.CLES_OK, abi.CLES_EFAILURE):
+            _check(rc)
+        return res
+
+    def kinetic_energy(self):
+        v = C.c_double()
+        _check(lib().cles_kinetic_energy(self.ptr, C.byref(v)))
+        return v.value
+
+    def dissipation_rate(self):
+        v = C.c_double()
+        _check(lib().cles_dissipation_rate(self.ptr, C.byref(v)))
+        return v.value
+
+
+def setup(prob, num, ctx=None):
+    """setup(prob, num) -> (solver, Q) (src/problem.jl:321-345); Q is the padded host state,
+    already uploaded to the device solver."""
+    from .problem import initialize, problem_desc
+    deriv = num.deriv if num.deriv is not None else lele_d1_6()
+    filt = num.filt if num.filt is not None else compact_filter(0.45)
+    desc = problem_desc(prob, num, deriv, filt)
+    s = Solver(desc, ctx=ctx)
+    Q = initialize(desc, prob.ic, eos=prob.eos)
+    s.set_state(Q)
+    return s, Q

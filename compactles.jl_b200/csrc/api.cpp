@@ -1,0 +1,494 @@
+// C ABI of libcles.so (include/cles.h).  Every entry point catches every
+// exception, records its text for cles_last_error() and returns a status.
+
+#include <atomic>
+#include <cstdio>
+#include <cstring>
+#include <string>
+
+#include "solver.h"
+
+namespace cles {
+
+namespace {
+thread_local std::string g_last_error;
+std::atomic<int64_t> g_launches{0};
+}  // namespace
+
+namespace {
+struct ProfRec {
+    int family;
+    double bytes;
+    cudaEvent_t a, b;
+};
+bool g_prof_on = false;
+std::vector<ProfRec> g_prof;
+std::vector<cudaEvent_t> g_event_pool;
+size_t g_event_next = 0;
+cudaEvent_t next_event() {
+    if (g_event_next == g_event_pool.size()) {
+        cudaEvent_t e;
+        CLES_CUDA(cudaEventCreate(&e));
+        g_event_pool.push_back(e);
+    }
+    return g_event_pool[g_event_next++];
+}
+}  // namespace
+
+bool profiling() { return g_prof_on; }
+int prof_begin(cudaStream_t st, int family, double bytes) {
+    ProfRec r{family, bytes, next_event(), next_event()};
+    CLES_CUDA(cudaEventRecord(r.a, st));
+    g_prof.push_back(r);
+    return (int)g_prof.size() - 1;
+}
+void prof_end(int rec, cudaStream_t st) { CLES_CUDA(cudaEventRecord(g_prof[rec].b, st)); }
+
+void set_last_error(const std::string& s) { g_last_error = s; }
+void count_launch(int n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+void check_launch(const char* what) {
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) throw Error(CLES_ECUDA, std::string(what) + " launch: " + cudaGetErrorString(e));
+}
+
+// ---------------------------------------------------------------- presets ----
+// lele_d1_6 / pade_d1_4 / compact_filter (src/kernels.jl:61-111) and
+// lele_d1_10 (src/kernels_banded.jl:54-64).
+namespace {
+void clear(cles_scheme* s, const char* name) {
+    std::memset(s, 0, sizeof(*s));
+    std::snprintf(s->name, sizeof(s->name), "%s", name);
+}
+void tri_row(cles_scheme* s, int j, double sub, double dia, double sup, std::initializer_list<double> rhs) {
+    s->clo_lhs[j][0] = sub;
+    s->clo_lhs[j][1] = dia;
+    s->clo_lhs[j][2] = sup;
+    int k = 0;
+    for (double v : rhs) s->clo_rhs[j][k++] = v;
+    s->clo_len[j] = k;
+}
+}  // namespace
+
+}  // namespace cles
+
+using namespace cles;
+
+struct cles_plan {
+    cles_ctx* ctx = nullptr;
+    CompactPlan plan;
+    int layout = CLES_LAYOUT_PADDED;
+    int n[3]{}, pad[3]{};
+    int64_t elem_off = 0, sy = 0, sz = 0, field_elems = 0;
+    DevBuf fbuf, obuf;
+};
+
+struct cles_solver {
+    cles_ctx* ctx = nullptr;
+    std::unique_ptr<SolverBase> s;
+};
+
+#define API_BEGIN try {
+#define API_END                                         \
+    }                                                   \
+    catch (const cles::Error& e) {                      \
+        set_last_error(e.what());                       \
+        return e.code;                                  \
+    }                                                   \
+    catch (const std::exception& e) {                   \
+        set_last_error(e.what());                       \
+        return CLES_EINVAL;                             \
+    }                                                   \
+    catch (...) {                                       \
+        set_last_error("unknown error");                \
+        return CLES_EINVAL;                             \
+    }                                                   \
+    set_last_error("");                                 \
+    return CLES_OK;
+
+extern "C" {
+
+const char* cles_last_error(void) { return g_last_error.c_str(); }
+
+int cles_profile_enable(int on) {
+    API_BEGIN
+    g_prof.clear();
+    g_event_next = 0;
+    g_prof_on = on != 0;
+    API_END
+}
+
+int cles_profile_read(cles_profile_entry* out, int max_entries, int* n_entries) {
+    API_BEGIN
+    if (!out || !n_entries) throw Error(CLES_EINVAL, "null argument");
+    static const char* names[3] = {"compact_x", "compact_y", "compact_z"};
+    cles_profile_entry acc[3];
+    std::memset(acc, 0, sizeof(acc));
+    for (int k = 0; k < 3; ++k) std::snprintf(acc[k].name, sizeof(acc[k].name), "%s", names[k]);
+    for (const ProfRec& r : g_prof) {
+        CLES_CUDA(cudaEventSynchronize(r.b));
+        float ms = 0.f;
+        CLES_CUDA(cudaEventElapsedTime(&ms, r.a, r.b));
+        acc[r.family].launches += 1;
+        acc[r.family].total_ms += ms;
+        acc[r.family].bytes += r.bytes;
+    }
+    int n = 0;
+    for (int k = 0; k < 3 && n < max_entries; ++k)
+        if (acc[k].launches) out[n++] = acc[k];
+    *n_entries = n;
+    API_END
+}
+int64_t cles_kernel_launches(void) { return g_launches.load(); }
+
+int cles_scheme_lele_d1_6(cles_scheme* s) {
+    if (!s) return CLES_EINVAL;
+    clear(s, "Lele C6 first derivative");
+    s->q = 1;
+    s->lhs[0] = 1.0 / 3.0;
+    s->M = 2;
+    s->coeffs[0] = 7.0 / 9.0;
+    s->coeffs[1] = 1.0 / 36.0;
+    s->symmetric = 0;
+    s->nc = 2;
+    tri_row(s, 0, 0.0, 1.0, 2.0, {-5.0 / 2.0, 2.0, 1.0 / 2.0});
+    tri_row(s, 1, 1.0 / 4.0, 1.0, 1.0 / 4.0, {-3.0 / 4.0, 0.0, 3.0 / 4.0});
+    return CLES_OK;
+}
+
+int cles_scheme_pade_d1_4(cles_scheme* s) {
+    if (!s) return CLES_EINVAL;
+    clear(s, "Pade C4 first derivative");
+    s->q = 1;
+    s->lhs[0] = 1.0 / 4.0;
+    s->M = 1;
+    s->coeffs[0] = 3.0 / 4.0;
+    s->nc = 1;
+    tri_row(s, 0, 0.0, 1.0, 2.0, {-5.0 / 2.0, 2.0, 1.0 / 2.0});
+    return CLES_OK;
+}
+
+int cles_scheme_compact_filter(double af, cles_scheme* s) {
+    if (!s) return CLES_EINVAL;
+    clear(s, "Gaitonde-Visbal C8 filter");
+    s->q = 1;
+    s->lhs[0] = af;
+    s->a0 = (93 + 70 * af) / 128;
+    s->M = 4;
+    s->coeffs[0] = (7 + 18 * af) / 16 / 2;
+    s->coeffs[1] = (-7 + 14 * af) / 32 / 2;
+    s->coeffs[2] = (1 - 2 * af) / 16 / 2;
+    s->coeffs[3] = (-1 + 2 * af) / 128 / 2;
+    s->symmetric = 1;
+    s->nc = 4;
+    // row 1 unfiltered; rows 2-4 centred filters of order 2, 4, 6 with the same alpha_f
+    const double f2[2] = {(1 + 2 * af) / 2, (1 + 2 * af) / 2};
+    const double f4[3] = {(5 + 6 * af) / 8, (1 + 2 * af) / 2, (-1 + 2 * af) / 8};
+    const double f6[4] = {(11 + 10 * af) / 16, (15 + 34 * af) / 32, (-3 + 6 * af) / 16, (1 - 2 * af) / 32};
+    auto centred = [&](int j, const double* c, int len) {
+        int k = 0;
+        for (int m = len - 1; m >= 1; --m) s->clo_rhs[j][k++] = c[m] / 2;
+        s->clo_rhs[j][k++] = c[0];
+        for (int m = 1; m < len; ++m) s->clo_rhs[j][k++] = c[m] / 2;
+        s->clo_len[j] = k;
+    };
+    s->clo_lhs[0][1] = 1.0;
+    s->clo_rhs[0][0] = 1.0;
+    s->clo_len[0] = 1;
+    for (int j = 1; j < 4; ++j) {
+        s->clo_lhs[j][0] = af;
+        s->clo_lhs[j][1] = 1.0;
+        s->clo_lhs[j][2] = af;
+    }
+    centred(1, f2, 2);
+    centred(2, f4, 3);
+    centred(3, f6, 4);
+    return CLES_OK;
+}
+
+int cles_scheme_lele_d1_10(cles_scheme* s) {
+    if (!s) return CLES_EINVAL;
+    clear(s, "Lele C10 first derivative");
+    s->q = 2;
+    s->lhs[0] = 1.0 / 2.0;
+    s->lhs[1] = 1.0 / 20.0;
+    s->M = 3;
+    s->coeffs[0] = 17.0 / 24.0;
+    s->coeffs[1] = 101.0 / 600.0;
+    s->coeffs[2] = 1.0 / 600.0;
+    s->nc = 3;
+    // rows 1-2: the C6 one-sided closures; row 3: the C6 interior row
+    const double lhs[3][5] = {{0, 0, 1, 2, 0}, {0, 1.0 / 4.0, 1, 1.0 / 4.0, 0}, {0, 1.0 / 3.0, 1, 1.0 / 3.0, 0}};
+    for (int j = 0; j < 3; ++j)
+        for (int t = 0; t < 5; ++t) s->clo_lhs[j][t] = lhs[j][t];
+    const double r0[3] = {-5.0 / 2.0, 2.0, 1.0 / 2.0}, r1[3] = {-3.0 / 4.0, 0.0, 3.0 / 4.0};
+    const double r2[5] = {-1.0 / 36.0, -7.0 / 9.0, 0.0, 7.0 / 9.0, 1.0 / 36.0};
+    for (int t = 0; t < 3; ++t) { s->clo_rhs[0][t] = r0[t]; s->clo_rhs[1][t] = r1[t]; }
+    for (int t = 0; t < 5; ++t) s->clo_rhs[2][t] = r2[t];
+    s->clo_len[0] = 3;
+    s->clo_len[1] = 3;
+    s->clo_len[2] = 5;
+    return CLES_OK;
+}
+
+// ---------------------------------------------------------------- context ----
+int cles_ctx_create(int device, void* stream, size_t budget, cles_ctx** out) {
+    API_BEGIN
+    if (!out) throw Error(CLES_EINVAL, "null output pointer");
+    int count = 0;
+    CLES_CUDA(cudaGetDeviceCount(&count));
+    if (device < 0 || device >= count) throw Error(CLES_EINVAL, "no such CUDA device");
+    CLES_CUDA(cudaSetDevice(device));
+    cudaDeviceProp prop;
+    CLES_CUDA(cudaGetDeviceProperties(&prop, device));
+    if (prop.major < 10) throw Error(CLES_ECUDA, "this library is built for sm_100a (B200); device is sm_" +
+                                                      std::to_string(prop.major) + std::to_string(prop.minor));
+    auto* c = new cles_ctx();
+    c->device = device;
+    c->stream = reinterpret_cast<cudaStream_t>(stream);
+    c->budget = budget;
+    *out = c;
+    API_END
+}
+
+void cles_ctx_destroy(cles_ctx* ctx) { delete ctx; }
+
+int cles_ctx_set_stream(cles_ctx* ctx, void* stream) {
+    API_BEGIN
+    if (!ctx) throw Error(CLES_EINVAL, "null context");
+    ctx->stream = reinterpret_cast<cudaStream_t>(stream);
+    API_END
+}
+
+// ------------------------------------------------------------------ plans ----
+int cles_plan_create(cles_ctx* ctx, const cles_grid* grid, const cles_scheme* scheme, int dim, double h, int dtype,
+                     int layout, cles_plan** out) {
+    API_BEGIN
+    if (!ctx || !grid || !scheme || !out) throw Error(CLES_EINVAL, "null argument");
+    if (dim < 1 || dim > 3) throw Error(CLES_EINVAL, "dim must be 1, 2 or 3");
+    if (dtype != CLES_F64 && dtype != CLES_F32) throw Error(CLES_EINVAL, "dtype must be CLES_F64 or CLES_F32");
+    if (layout != CLES_LAYOUT_PADDED && layout != CLES_LAYOUT_INTERIOR) throw Error(CLES_EINVAL, "unknown layout");
+    if (!(h > 0)) throw Error(CLES_EINVAL, "grid spacing must be positive");
+    for (int k = 0; k < 3; ++k)
+        if (grid->n_global[k] < 1) throw Error(CLES_EINVAL, "n_global must be >= 1");
+    if (grid->n_global[dim - 1] <= 1) throw Error(CLES_EINVAL, "dimension is collapsed");
+    if (scheme->M > grid->n_halo && layout == CLES_LAYOUT_PADDED)
+        throw Error(CLES_EINVAL, "stencil half-width " + std::to_string(scheme->M) + " exceeds halo width " +
+                                     std::to_string(grid->n_halo));
+    CLES_CUDA(cudaSetDevice(ctx->device));
+    auto* p = new cles_plan();
+    try {
+        p->ctx = ctx;
+        p->layout = layout;
+        for (int k = 0; k < 3; ++k) {
+            p->n[k] = grid->n_global[k];
+            p->pad[k] = (layout == CLES_LAYOUT_PADDED && grid->n_global[k] > 1) ? grid->n_halo : 0;
+        }
+        const int d = dim - 1;
+        const bool periodic = grid->periodic[d] != 0;
+        build_compact_plan(p->plan, *scheme, p->n, d, periodic, h, dtype);
+        const int64_t F0 = p->n[0] + 2 * p->pad[0], F1 = p->n[1] + 2 * p->pad[1], F2 = p->n[2] + 2 * p->pad[2];
+        p->sy = F0;
+        p->sz = F0 * F1;
+        p->elem_off = p->pad[0] + p->pad[1] * F0 + p->pad[2] * F0 * F1;
+        p->field_elems = F0 * F1 * F2;
+    } catch (...) {
+        delete p;
+        throw;
+    }
+    *out = p;
+    API_END
+}
+
+void cles_plan_destroy(cles_plan* plan) {
+    if (!plan) return;
+    cudaSetDevice(plan->ctx->device);
+    delete plan;
+}
+
+static int apply_impl(cles_plan* plan, const void* f, void* out, int count, int64_t stride) {
+    API_BEGIN
+    if (!plan || !f || !out) throw Error(CLES_EINVAL, "null argument");
+    if (count < 1) throw Error(CLES_EINVAL, "count must be >= 1");
+    const size_t el = plan->plan.dtype == CLES_F64 ? sizeof(double) : sizeof(float);
+    FieldView vin{const_cast<char*>(reinterpret_cast<const char*>(f)) + el * plan->elem_off, stride, plan->sy, plan->sz};
+    FieldView vout{reinterpret_cast<char*>(out) + el * plan->elem_off, stride, plan->sy, plan->sz};
+    launch_compact(plan->plan, vin, vout, count, OUT_STORE, plan->ctx->stream);
+    API_END
+}
+
+int cles_apply_along(cles_plan* plan, const void* f_dev, void* out_dev) {
+    if (!plan) return CLES_EINVAL;
+    return apply_impl(plan, f_dev, out_dev, 1, plan->field_elems);
+}
+
+int cles_apply_along_batch(cles_plan* plan, const void* f_dev, void* out_dev, int count, int64_t field_stride) {
+    return apply_impl(plan, f_dev, out_dev, count, field_stride);
+}
+
+int cles_apply_along_host(cles_plan* plan, const void* f_host, void* out_host) {
+    API_BEGIN
+    if (!plan || !f_host || !out_host) throw Error(CLES_EINVAL, "null argument");
+    CLES_CUDA(cudaSetDevice(plan->ctx->device));
+    const size_t el = plan->plan.dtype == CLES_F64 ? sizeof(double) : sizeof(float);
+    const size_t bytes = el * (size_t)plan->field_elems;
+    if (!plan->fbuf.p) {
+        plan->fbuf.alloc(plan->ctx, bytes);
+        plan->obuf.alloc(plan->ctx, bytes);
+    }
+    cudaStream_t st = plan->ctx->stream;
+    CLES_CUDA(cudaMemcpyAsync(plan->fbuf.p, f_host, bytes, cudaMemcpyHostToDevice, st));
+    CLES_CUDA(cudaMemcpyAsync(plan->obuf.p, out_host, bytes, cudaMemcpyHostToDevice, st));
+    int rc = apply_impl(plan, plan->fbuf.p, plan->obuf.p, 1, plan->field_elems);
+    if (rc != CLES_OK) return rc;
+    CLES_CUDA(cudaMemcpyAsync(out_host, plan->obuf.p, bytes, cudaMemcpyDeviceToHost, st));
+    CLES_CUDA(cudaStreamSynchronize(st));
+    API_END
+}
+
+// ----------------------------------------------------------------- solver ----
+void cles_step_control_default(cles_step_control* c) {
+    if (!c) return;
+    c->predict = 0.0;
+    c->max_growth = 0.0;
+    c->landing_steps = 2;
+    c->dt_min = 0.0;
+    c->dt_min_ratio = 1e-8;
+    c->retries = 0;
+    c->cfl_backoff = 0.5;
+    c->savepoint_interval = 25;
+}
+
+void cles_solver_desc_default(cles_solver_desc* d) {
+    if (!d) return;
+    std::memset(d, 0, sizeof(*d));
+    for (int k = 0; k < 3; ++k) {
+        d->n_global[k] = 1;
+        d->L[k] = 1.0;
+        d->bc[k][0] = d->bc[k][1] = CLES_BC_PERIODIC;
+    }
+    d->n_species = 1;
+    d->R[0] = 1.0;
+    d->gamma[0] = 1.4;
+    d->mu0 = 0.0;
+    d->Pr = 0.7;
+    d->Sc = 0.7;
+    d->art_enabled = 1;
+    d->C_mu = 0.002;
+    d->C_beta = 1.0;
+    d->C_kappa = 0.01;
+    d->C_D = 0.01;
+    d->beta_sensor = CLES_BETA_STRAIN;
+    cles_scheme_lele_d1_6(&d->deriv);
+    cles_scheme_compact_filter(0.45, &d->filt);
+    d->cfl = 0.5;
+    d->filter_interval = 1;
+    cles_step_control_default(&d->control);
+    d->n_halo = 4;
+    d->precision = CLES_PREC_FP64;
+}
+
+int cles_solver_create(cles_ctx* ctx, const cles_solver_desc* desc, cles_solver** out) {
+    API_BEGIN
+    if (!ctx || !desc || !out) throw Error(CLES_EINVAL, "null argument");
+    CLES_CUDA(cudaSetDevice(ctx->device));
+    auto* s = new cles_solver();
+    s->ctx = ctx;
+    try {
+        s->s = make_solver(ctx, *desc);
+    } catch (...) {
+        delete s;
+        throw;
+    }
+    *out = s;
+    API_END
+}
+
+void cles_solver_destroy(cles_solver* s) {
+    if (!s) return;
+    cudaSetDevice(s->ctx->device);
+    delete s;
+}
+
+#define SOLVER_CALL(body)                                        \
+    API_BEGIN                                                    \
+    if (!s) throw Error(CLES_EINVAL, "null solver");             \
+    CLES_CUDA(cudaSetDevice(s->ctx->device));                    \
+    body;                                                        \
+    API_END
+
+int cles_solver_info_get(const cles_solver* s, cles_solver_info* out) {
+    API_BEGIN
+    if (!s || !out) throw Error(CLES_EINVAL, "null argument");
+    *out = s->s->info();
+    API_END
+}
+
+int cles_set_state(cles_solver* s, const double* Q, int layout) { SOLVER_CALL(s->s->set_state(Q, layout)) }
+int cles_get_state(cles_solver* s, double* Q, int layout) { SOLVER_CALL(s->s->get_state(Q, layout)) }
+int cles_state_device(cles_solver* s, double** Q) { SOLVER_CALL(*Q = s->s->state_device()) }
+int cles_apply_bcs(cles_solver* s) { SOLVER_CALL(s->s->apply_bcs()) }
+int cles_max_rate(cles_solver* s, double* rate, double* rho_min) { SOLVER_CALL(s->s->max_rate(rate, rho_min)) }
+int cles_compute_rhs(cles_solver* s, int primitives_current) { SOLVER_CALL(s->s->compute_rhs(primitives_current != 0)) }
+int cles_get_rhs(cles_solver* s, double* dQ, int layout) { SOLVER_CALL(s->s->get_rhs(dQ, layout)) }
+int cles_step(cles_solver* s, double dt, int prepared) { SOLVER_CALL(s->s->step(dt, prepared != 0)) }
+int cles_filter_state(cles_solver* s) { SOLVER_CALL(s->s->filter_state()) }
+int cles_get_field(cles_solver* s, int which, double* host, int layout) { SOLVER_CALL(s->s->get_field(which, host, layout)) }
+int cles_kinetic_energy(cles_solver* s, double* ke) { SOLVER_CALL(*ke = s->s->kinetic_energy()) }
+int cles_dissipation_rate(cles_solver* s, double* eps) { SOLVER_CALL(*eps = s->s->dissipation_rate()) }
+
+int cles_get_clock(const cles_solver* s, double* t, int64_t* step, double* cfl) {
+    API_BEGIN
+    if (!s) throw Error(CLES_EINVAL, "null solver");
+    if (t) *t = s->s->t;
+    if (step) *step = s->s->step_count;
+    if (cfl) *cfl = s->s->cfl;
+    API_END
+}
+
+int cles_set_clock(cles_solver* s, double t, int64_t step, double cfl) {
+    API_BEGIN
+    if (!s) throw Error(CLES_EINVAL, "null solver");
+    s->s->t = t;
+    s->s->step_count = step;
+    s->s->cfl = cfl;
+    API_END
+}
+
+int cles_check_step(const cles_step_control* c, double dt, double rho_min, double dt_seen, int64_t step, double t,
+                    double cfl, int* reason) {
+    API_BEGIN
+    (void)step; (void)t; (void)cfl;
+    if (!c || !reason) throw Error(CLES_EINVAL, "null argument");
+    *reason = check_step(*c, dt, rho_min, dt_seen);
+    API_END
+}
+
+int cles_run(cles_solver* s, double tfinal, int64_t nmax, cles_run_result* out) {
+    int rc = CLES_OK;
+    API_BEGIN
+    if (!s) throw Error(CLES_EINVAL, "null solver");
+    CLES_CUDA(cudaSetDevice(s->ctx->device));
+    rc = s->s->run(tfinal, nmax, out);
+    if (rc == CLES_EFAILURE) {
+        set_last_error("SolverFailure: step control rejected the step (see cles_run_result.failure)");
+        return rc;
+    }
+    API_END
+}
+
+int cles_step_host(cles_solver* s, double* Q_host, int layout, double tfinal, cles_run_result* out) {
+    int rc = CLES_OK;
+    API_BEGIN
+    if (!s || !Q_host) throw Error(CLES_EINVAL, "null argument");
+    CLES_CUDA(cudaSetDevice(s->ctx->device));
+    s->s->set_state(Q_host, layout);
+    rc = s->s->run(tfinal, s->s->step_count + 1, out);
+    s->s->get_state(Q_host, layout);
+    if (rc == CLES_EFAILURE) {
+        set_last_error("SolverFailure: step control rejected the step (see cles_run_result.failure)");
+        return rc;
+    }
+    API_END
+}
+
+}  // extern "C"

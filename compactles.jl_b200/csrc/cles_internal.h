@@ -1,0 +1,97 @@
+// Internal declarations shared by the host runtime and the CUDA kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/cles.h"
+
+namespace cles {
+
+// ---------------------------------------------------------------- errors ----
+struct Error : std::runtime_error {
+    int code;
+    Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+void set_last_error(const std::string& s);
+#define CLES_CUDA(call)                                                                         \
+    do {                                                                                        \
+        cudaError_t e_ = (call);                                                                \
+        if (e_ != cudaSuccess)                                                                  \
+            throw ::cles::Error(CLES_ECUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+void count_launch(int n = 1);
+// CUDA-event bracketing of compact launches (cles_profile_enable)
+bool profiling();
+int prof_begin(cudaStream_t st, int family, double bytes);
+void prof_end(int rec, cudaStream_t st);
+void check_launch(const char* what);
+
+// ------------------------------------------------------------ field views ----
+// A batch of scalar fields of one grid: element (i, j, k) of field b sits at
+// base + b*comp_stride + i + j*sy + k*sz (elements).  `base` points at
+// interior element (0, 0, 0).
+struct FieldView {
+    void* base;
+    int64_t comp_stride;
+    int64_t sy, sz;
+};
+
+// ------------------------------------------------------------ compact plans ---
+constexpr int kMaxSeg = 32;        // points per thread (register tile)
+constexpr int kMaxClo = CLES_MAX_NC;
+constexpr int kMaxCloLen = CLES_MAX_CLO_LEN;
+
+// Kernel parameters of one directional compact operator (passed by value).
+struct CompactParams {
+    int n;               // line length
+    int dim;             // 0, 1, 2
+    int nx, ny, nz;      // interior extents of the grid
+    int S;               // segments per line
+    int seg_base, seg_rem;  // segment s: length seg_base + (s < seg_rem), local_range split
+    int LB;              // lines per CTA
+    int q, M;
+    int symmetric;
+    int periodic;
+    int lo_closed, hi_closed;
+    int nc;
+    int hasred;
+    double a0;
+    double ci[CLES_MAX_M];
+    int clo_len[kMaxClo];
+    double clo[kMaxClo][kMaxCloLen];
+    double chi[kMaxClo][kMaxCloLen];
+    // offsets (elements) into the coefficient table
+    int64_t off_f0, off_f1, off_f2, off_f3, off_f4;  // q=1: l, dinv, c ; q=2: L1, L2, U1, U2, Uinv0
+    int64_t off_V, off_W;                              // V[s][t][i], W[s][t][i]
+    int64_t off_G;                                     // reduced inverse, (2qS) x (2qS) row-major
+    int64_t lines;
+};
+
+// Host-side plan: parameters plus the coefficient tables on the device.
+struct CompactPlan {
+    CompactParams P;
+    int dtype = CLES_F64;
+    double* tab64 = nullptr;
+    float* tab32 = nullptr;
+    size_t tab_elems = 0;
+    ~CompactPlan();
+};
+
+// Builds the plan of `scheme` along `dim` (0-based) of a grid with interior
+// extents n3[3]; periodic says whether the line wraps.
+void build_compact_plan(CompactPlan& plan, const cles_scheme& scheme, const int n3[3], int dim,
+                        bool periodic, double h, int dtype);
+
+// Output modes of the compact operator.
+enum { OUT_STORE = 0, OUT_NEGATE = 1, OUT_SUBTRACT = 2 };
+
+// Launch the operator over `count` fields of `in` into `out` (may alias).
+void launch_compact(const CompactPlan& plan, const FieldView& in, const FieldView& out, int count, int mode,
+                    cudaStream_t st);
+
+}  // namespace cles

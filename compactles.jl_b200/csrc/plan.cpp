@@ -1,0 +1,328 @@
+// Host-side construction of directional compact plans.
+//
+// A line of n points is the global banded system of plan_direction
+// (src/operators.jl:44-101, src/operators_banded.jl:29-125): interior rows
+// carry the scheme's LHS band, closed edges carry the closure rows (mirrored at
+// the high edge), periodic lines wrap.  The device solves it with the
+// reduced-interface ("spike") method of src/tridiag.jl:1-22 and
+// src/banded.jl:1-27, applied inside one line: the line is cut into S
+// segments of at most kMaxSeg points (one per thread), each segment is solved
+// locally with its own factorisation, the 2q head/tail values of all segments
+// form a (2qS)^2 reduced system whose inverse is precomputed here, and every
+// segment is corrected with its spike vectors.  With S = 1 and a periodic line
+// this is exactly the reference's single-rank self-coupled solve; with S > 1
+// it is the reference's P-rank distributed solve with ranks mapped to threads.
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+#include "cles_internal.h"
+
+namespace cles {
+
+namespace {
+
+struct Band {
+    int n, q;
+    bool periodic;
+    std::vector<double> a;  // n x (2q+1), a[i*(2q+1) + q + s] = A[i, i+s]
+    double at(int r, int c) const {
+        int s = c - r;
+        if (periodic) {
+            if (s > n / 2) s -= n;
+            if (s < -n / 2) s += n;
+        }
+        if (s < -q || s > q) return 0.0;
+        return a[(size_t)r * (2 * q + 1) + q + s];
+    }
+};
+
+// LU with partial pivoting of a dense N x N row-major matrix; returns inverse.
+std::vector<double> dense_inverse(std::vector<double> A, int N) {
+    std::vector<int> piv(N);
+    for (int k = 0; k < N; ++k) {
+        int p = k;
+        double best = std::fabs(A[(size_t)k * N + k]);
+        for (int i = k + 1; i < N; ++i)
+            if (std::fabs(A[(size_t)i * N + k]) > best) { best = std::fabs(A[(size_t)i * N + k]); p = i; }
+        if (best == 0.0) throw Error(CLES_EINVAL, "singular reduced interface system");
+        piv[k] = p;
+        if (p != k)
+            for (int j = 0; j < N; ++j) std::swap(A[(size_t)k * N + j], A[(size_t)p * N + j]);
+        const double inv = 1.0 / A[(size_t)k * N + k];
+        for (int i = k + 1; i < N; ++i) {
+            const double l = A[(size_t)i * N + k] * inv;
+            A[(size_t)i * N + k] = l;
+            if (l != 0.0)
+                for (int j = k + 1; j < N; ++j) A[(size_t)i * N + j] -= l * A[(size_t)k * N + j];
+        }
+    }
+    std::vector<double> X((size_t)N * N, 0.0), b(N);
+    for (int c = 0; c < N; ++c) {
+        std::fill(b.begin(), b.end(), 0.0);
+        b[c] = 1.0;
+        for (int k = 0; k < N; ++k) std::swap(b[k], b[piv[k]]);
+        for (int i = 0; i < N; ++i)
+            for (int k = 0; k < i; ++k) b[i] -= A[(size_t)i * N + k] * b[k];
+        for (int i = N - 1; i >= 0; --i) {
+            double acc = b[i];
+            for (int k = i + 1; k < N; ++k) acc -= A[(size_t)i * N + k] * b[k];
+            b[i] = acc / A[(size_t)i * N + i];
+        }
+        for (int r = 0; r < N; ++r) X[(size_t)r * N + c] = b[r];
+    }
+    return X;
+}
+
+// Local banded factorisation of rows/cols [off, off+m) of the band.
+struct LocalFactor {
+    int m, q;
+    std::vector<double> L;   // L[(t-1)*m + k]: multiplier eliminating row k+t with pivot row k
+    std::vector<double> U;   // U[t*m + i] = U[i, i+t], t = 0..q
+    void build(const Band& B, int off, int mm) {
+        m = mm; q = B.q;
+        const int W = 2 * q + 1;
+        std::vector<double> w((size_t)m * W, 0.0);
+        for (int i = 0; i < m; ++i)
+            for (int s = -q; s <= q; ++s) {
+                const int c = i + s;
+                if (c < 0 || c >= m) continue;
+                w[(size_t)i * W + q + s] = B.at(off + i, off + c);
+            }
+        L.assign((size_t)q * m, 0.0);
+        for (int k = 0; k < m - 1; ++k) {
+            const double piv = w[(size_t)k * W + q];
+            if (piv == 0.0) throw Error(CLES_EINVAL, "zero pivot in a segment factorisation");
+            const int tmax = std::min(q, m - 1 - k);
+            for (int t = 1; t <= tmax; ++t) {
+                const int i = k + t;
+                const double l = w[(size_t)i * W + q - t] / piv;
+                L[(size_t)(t - 1) * m + k] = l;
+                for (int u = 1; u <= tmax; ++u) w[(size_t)i * W + q + u - t] -= l * w[(size_t)k * W + q + u];
+            }
+        }
+        U.assign((size_t)(q + 1) * m, 0.0);
+        for (int i = 0; i < m; ++i)
+            for (int t = 0; t <= std::min(q, m - 1 - i); ++t) U[(size_t)t * m + i] = w[(size_t)i * W + q + t];
+    }
+    void solve(double* x) const {
+        for (int k = 0; k < m - 1; ++k)
+            for (int t = 1; t <= std::min(q, m - 1 - k); ++t) x[k + t] -= L[(size_t)(t - 1) * m + k] * x[k];
+        for (int i = m - 1; i >= 0; --i) {
+            double acc = x[i];
+            for (int t = 1; t <= std::min(q, m - 1 - i); ++t) acc -= U[(size_t)t * m + i] * x[i + t];
+            x[i] = acc / U[i];
+        }
+    }
+};
+
+}  // namespace
+
+CompactPlan::~CompactPlan() {
+    if (tab64) cudaFree(tab64);
+    if (tab32) cudaFree(tab32);
+}
+
+void build_compact_plan(CompactPlan& plan, const cles_scheme& s, const int n3[3], int dim, bool periodic,
+                        double h, int dtype) {
+    const int n = n3[dim];
+    const int q = s.q, M = s.M, nc = s.nc;
+    if (q < 1 || q > CLES_MAX_Q) throw Error(CLES_EINVAL, "scheme LHS half-bandwidth q must be 1 or 2");
+    if (M < 1 || M > CLES_MAX_M) throw Error(CLES_EINVAL, "scheme RHS half-width M must be 1..4");
+    if (nc < 0 || nc > CLES_MAX_NC) throw Error(CLES_EINVAL, "too many closure rows");
+    const int nmin = q >= 2 ? std::max({2 * nc + 1, 2 * M + 1, 2 * q + 1}) : std::max(2 * nc + 1, 2 * M + 1);
+    if (n < nmin)
+        throw Error(CLES_EINVAL, "local extent " + std::to_string(n) + " along dim " + std::to_string(dim + 1) +
+                                     " too small for scheme '" + std::string(s.name) + "' (need >= " +
+                                     std::to_string(nmin) + ")");
+    if (!periodic && M > nc)
+        throw Error(CLES_EINVAL, "closed lines need the RHS half-width M <= closure rows nc (halos are never read)");
+    for (int j = 0; j < nc; ++j)
+        if (s.clo_len[j] < 0 || s.clo_len[j] > CLES_MAX_CLO_LEN || s.clo_len[j] > n)
+            throw Error(CLES_EINVAL, "bad closure stencil length");
+
+    CompactParams& P = plan.P;
+    std::memset(&P, 0, sizeof(P));
+    P.n = n; P.dim = dim; P.nx = n3[0]; P.ny = n3[1]; P.nz = n3[2];
+    P.q = q; P.M = M; P.symmetric = s.symmetric; P.periodic = periodic ? 1 : 0;
+    P.lo_closed = periodic ? 0 : 1;
+    P.hi_closed = periodic ? 0 : 1;
+    P.nc = nc;
+    P.lines = 1;
+    for (int k = 0; k < 3; ++k) if (k != dim) P.lines *= n3[k];
+
+    // RHS coefficients prescaled by 1/h (derivatives) and the high-edge sign
+    // (src/operators.jl:87-92).
+    const double hinv = 1.0 / h;
+    const double sgn = s.symmetric ? 1.0 : -1.0;
+    const double scale = s.symmetric ? 1.0 : hinv;
+    P.a0 = s.a0;
+    for (int m = 0; m < M; ++m) P.ci[m] = s.coeffs[m] * scale;
+    for (int j = 0; j < nc; ++j) {
+        P.clo_len[j] = s.clo_len[j];
+        for (int t = 0; t < s.clo_len[j]; ++t) {
+            P.clo[j][t] = s.clo_rhs[j][t] * scale;
+            P.chi[j][t] = s.clo_rhs[j][t] * (scale * sgn);
+        }
+    }
+
+    // Global band with closures (src/operators.jl:66-84, src/operators_banded.jl:48-112).
+    Band B;
+    B.n = n; B.q = q; B.periodic = periodic;
+    const int W = 2 * q + 1;
+    B.a.assign((size_t)n * W, 0.0);
+    for (int i = 0; i < n; ++i) {
+        B.a[(size_t)i * W + q] = 1.0;
+        for (int t = 1; t <= q; ++t) {
+            B.a[(size_t)i * W + q + t] = s.lhs[t - 1];
+            B.a[(size_t)i * W + q - t] = s.lhs[t - 1];
+        }
+    }
+    if (!periodic) {
+        for (int j = 0; j < nc; ++j) {
+            for (int t = -q; t <= q; ++t) {
+                double v = s.clo_lhs[j][q + t];
+                if (j + t < 0) {
+                    if (q >= 2 && v != 0.0) throw Error(CLES_EINVAL, "closure row references a column before the edge");
+                    v = 0.0;  // tridiagonal row 1 ignores its sub-diagonal
+                }
+                B.a[(size_t)j * W + q + t] = v;
+            }
+            const int r = n - 1 - j;
+            for (int t = -q; t <= q; ++t) {
+                double v = s.clo_lhs[j][q - t];
+                if (r + t >= n) v = 0.0;
+                B.a[(size_t)r * W + q + t] = v;
+            }
+        }
+        // the first/last rows have no couplings beyond the edge
+        for (int i = 0; i < n; ++i)
+            for (int t = -q; t <= q; ++t)
+                if (i + t < 0 || i + t >= n) B.a[(size_t)i * W + q + t] = 0.0;
+    }
+
+    // Segmentation: S segments of at most kMaxSeg points, local_range split.
+    int S = (n + kMaxSeg - 1) / kMaxSeg;
+    if (S < 1) S = 1;
+    const int base = n / S, rem = n % S;
+    if (base < std::max(2 * q + 1, q + 1)) S = 1;  // tiny lines: one segment
+    P.S = S;
+    P.seg_base = n / S;
+    P.seg_rem = n % S;
+    if (P.seg_base + (P.seg_rem ? 1 : 0) > kMaxSeg) throw Error(CLES_EINVAL, "segment longer than the register tile");
+    (void)base; (void)rem;
+    int LB = 32;
+    while (LB > 1 && LB * S > 512) LB /= 2;
+    if (dim == 0) {
+        // x lines are staged in a transposed shared-memory tile of n x (LB+1)
+        const size_t el = dtype == CLES_F64 ? sizeof(double) : sizeof(float);
+        while (LB > 1 && (size_t)n * (LB + 1) * el > 110 * 1024) LB /= 2;
+        if ((size_t)n * (LB + 1) * el > 200 * 1024) throw Error(CLES_EINVAL, "x line too long for the shared-memory tile");
+    }
+    if (LB * S > 512) throw Error(CLES_EINVAL, "line too long for one CTA");
+    if (P.lines < LB) {
+        int l = 1;
+        while (l < P.lines) l *= 2;
+        LB = std::max(1, std::min(LB, l));
+    }
+    P.LB = LB;
+    P.hasred = (periodic || S > 1) ? 1 : 0;
+
+    auto seg_off = [&](int sg) { return sg * P.seg_base + std::min(sg, P.seg_rem); };
+    auto seg_len = [&](int sg) { return P.seg_base + (sg < P.seg_rem ? 1 : 0); };
+
+    // Table layout (elements): 5 coefficient arrays [S][kMaxSeg], V/W [S][q][kMaxSeg], G [N][N].
+    const int N = 2 * q * S;
+    const int64_t arr = (int64_t)S * kMaxSeg;
+    P.off_f0 = 0; P.off_f1 = arr; P.off_f2 = 2 * arr; P.off_f3 = 3 * arr; P.off_f4 = 4 * arr;
+    P.off_V = 5 * arr;
+    P.off_W = P.off_V + (int64_t)S * q * kMaxSeg;
+    P.off_G = P.off_W + (int64_t)S * q * kMaxSeg;
+    const int64_t total = P.off_G + (P.hasred ? (int64_t)N * N : 0);
+    std::vector<double> tab((size_t)total, 0.0);
+
+    std::vector<LocalFactor> fac(S);
+    std::vector<std::vector<double>> Vs(S), Ws(S);
+    for (int sg = 0; sg < S; ++sg) {
+        const int off = seg_off(sg), m = seg_len(sg);
+        LocalFactor& F = fac[sg];
+        F.build(B, off, m);
+        // coefficients
+        for (int i = 0; i < m; ++i) {
+            if (q == 1) {
+                // Thomas form of the same factorisation: l, 1/pivot, super-diagonal
+                tab[P.off_f0 + (size_t)sg * kMaxSeg + i] = i > 0 ? F.L[(size_t)i - 1] : 0.0;
+                tab[P.off_f1 + (size_t)sg * kMaxSeg + i] = 1.0 / F.U[i];
+                tab[P.off_f2 + (size_t)sg * kMaxSeg + i] = i < m - 1 ? F.U[(size_t)m + i] : 0.0;
+            } else {
+                tab[P.off_f0 + (size_t)sg * kMaxSeg + i] = F.L[i];                       // eliminates row i+1
+                tab[P.off_f1 + (size_t)sg * kMaxSeg + i] = F.L[(size_t)m + i];           // eliminates row i+2
+                tab[P.off_f2 + (size_t)sg * kMaxSeg + i] = F.U[(size_t)m + i];           // U[i, i+1]
+                tab[P.off_f3 + (size_t)sg * kMaxSeg + i] = F.U[(size_t)2 * m + i];       // U[i, i+2]
+                tab[P.off_f4 + (size_t)sg * kMaxSeg + i] = 1.0 / F.U[i];
+            }
+        }
+        // spikes: V[:, t] = T^-1 (coupling of rows 0..q-1 to the previous
+        // segment's tail unknown t), W[:, t] likewise for the next head.
+        Vs[sg].assign((size_t)q * m, 0.0);
+        Ws[sg].assign((size_t)q * m, 0.0);
+        const bool has_prev = periodic || sg > 0;
+        const bool has_next = periodic || sg < S - 1;
+        const int prev = (sg - 1 + S) % S, next = (sg + 1) % S;
+        for (int t = 0; t < q; ++t) {
+            std::vector<double> v(m, 0.0), w(m, 0.0);
+            bool nzv = false, nzw = false;
+            if (has_prev) {
+                const int col = seg_off(prev) + seg_len(prev) - q + t;  // tail unknown t of prev
+                for (int r = 0; r < std::min(q, m); ++r) { v[r] = B.at(off + r, col); nzv = nzv || v[r] != 0.0; }
+            }
+            if (has_next) {
+                const int col = seg_off(next) + t;  // head unknown t of next
+                for (int r = std::max(0, m - q); r < m; ++r) { w[r] = B.at(off + r, col); nzw = nzw || w[r] != 0.0; }
+            }
+            if (nzv) F.solve(v.data());
+            if (nzw) F.solve(w.data());
+            for (int i = 0; i < m; ++i) {
+                Vs[sg][(size_t)t * m + i] = v[i];
+                Ws[sg][(size_t)t * m + i] = w[i];
+                tab[P.off_V + ((size_t)sg * q + t) * kMaxSeg + i] = v[i];
+                tab[P.off_W + ((size_t)sg * q + t) * kMaxSeg + i] = w[i];
+            }
+        }
+    }
+    if (P.hasred) {
+        // Reduced system in z = (head_0, tail_0, head_1, tail_1, ...), 2q per segment.
+        std::vector<double> R((size_t)N * N, 0.0);
+        for (int sg = 0; sg < S; ++sg) {
+            const int m = seg_len(sg);
+            const int prev = (sg - 1 + S) % S, next = (sg + 1) % S;
+            for (int r = 0; r < q; ++r) {
+                const int rh = 2 * q * sg + r, rt = 2 * q * sg + q + r;
+                R[(size_t)rh * N + rh] += 1.0;
+                R[(size_t)rt * N + rt] += 1.0;
+                for (int t = 0; t < q; ++t) {
+                    const int cprev = 2 * q * prev + q + t, cnext = 2 * q * next + t;
+                    R[(size_t)rh * N + cprev] += Vs[sg][(size_t)t * m + r];
+                    R[(size_t)rt * N + cprev] += Vs[sg][(size_t)t * m + (m - q + r)];
+                    R[(size_t)rh * N + cnext] += Ws[sg][(size_t)t * m + r];
+                    R[(size_t)rt * N + cnext] += Ws[sg][(size_t)t * m + (m - q + r)];
+                }
+            }
+        }
+        std::vector<double> G = dense_inverse(R, N);
+        std::copy(G.begin(), G.end(), tab.begin() + P.off_G);
+    }
+
+    plan.dtype = dtype;
+    plan.tab_elems = (size_t)total;
+    CLES_CUDA(cudaMalloc(&plan.tab64, sizeof(double) * total));
+    CLES_CUDA(cudaMemcpy(plan.tab64, tab.data(), sizeof(double) * total, cudaMemcpyHostToDevice));
+    if (dtype == CLES_F32) {
+        std::vector<float> t32(tab.begin(), tab.end());
+        CLES_CUDA(cudaMalloc(&plan.tab32, sizeof(float) * total));
+        CLES_CUDA(cudaMemcpy(plan.tab32, t32.data(), sizeof(float) * total, cudaMemcpyHostToDevice));
+    }
+}
+
+}  // namespace cles

@@ -1,0 +1,571 @@
+// Pointwise kernels of the RHS and the integrator (interior layout, x fastest).
+//
+// F is the storage type of the derived fields (double in the plain form,
+// float in the mixed form); the conserved state Q and the RK register du are
+// always double.  Arithmetic follows the association order of the cited
+// reference lines.
+
+#include "pointwise.h"
+
+namespace cles {
+
+namespace {
+
+constexpr int kThreads = 256;
+
+// Julia's Base.max/min on floats: a NaN operand wins.
+__device__ __forceinline__ double jl_max(double x, double y) {
+    if (x != x) return x;
+    if (y != y) return y;
+    return y > x ? y : x;
+}
+__device__ __forceinline__ double jl_min(double x, double y) {
+    if (x != x) return x;
+    if (y != y) return y;
+    return y < x ? y : x;
+}
+
+inline unsigned grid_for(int64_t n) {
+    int64_t b = (n + kThreads - 1) / kThreads;
+    if (b > 148 * 64) b = 148 * 64;
+    return (unsigned)(b < 1 ? 1 : b);
+}
+
+#define GRID_STRIDE(idx, n) for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < (n); idx += (int64_t)gridDim.x * blockDim.x)
+
+// _primitives!(::IdealMixture) (src/physics.jl:604-653) at the interior.
+template <typename F>
+__global__ void k_primitives(const double* __restrict__ Q, F* __restrict__ prim, int64_t cells, int Ns, PhysConst pc) {
+    GRID_STRIDE(I, cells) {
+        double rho = 0.0;
+        for (int sp = 0; sp < Ns; ++sp) rho += Q[I + cells * sp];
+        F* out = prim + I;
+        if (rho > 0) {
+            const double ri = 1 / rho;
+            double Rm = 0.0, cvm = 0.0;
+            for (int sp = 0; sp < Ns; ++sp) {
+                const double q = Q[I + cells * sp];
+                Rm += q * pc.Rk[sp];
+                cvm += q * pc.cvk[sp];
+                out[cells * (P_Y0 + sp)] = F(q * ri);
+            }
+            Rm *= ri;
+            cvm *= ri;
+            const double u = Q[I + cells * (Ns + 0)] * ri;
+            const double v = Q[I + cells * (Ns + 1)] * ri;
+            const double w = Q[I + cells * (Ns + 2)] * ri;
+            const double e = Q[I + cells * (Ns + 3)] * ri - 0.5 * (u * u + v * v + w * w);
+            const double T = jl_max(e / cvm, 1e-300);
+            const double p = rho * Rm * T;
+            const double gm = 1 + Rm / cvm;
+            out[cells * P_RHO] = F(rho);
+            out[cells * P_U] = F(u);
+            out[cells * P_V] = F(v);
+            out[cells * P_W] = F(w);
+            out[cells * P_P] = F(p);
+            out[cells * P_T] = F(T);
+            out[cells * P_C] = F(sqrt(gm * Rm * T));
+            out[cells * P_CP] = F(cvm + Rm);
+        } else {
+            out[cells * P_RHO] = F(1);
+            out[cells * P_U] = F(0);
+            out[cells * P_V] = F(0);
+            out[cells * P_W] = F(0);
+            out[cells * P_P] = F(1);
+            out[cells * P_T] = F(1);
+            out[cells * P_C] = F(1);
+            out[cells * P_CP] = F(1);
+            for (int sp = 0; sp < Ns; ++sp) out[cells * (P_Y0 + sp)] = F(sp == 0 ? 1.0 : 0.0);
+        }
+    }
+}
+
+// |S| = sqrt(S_ij S_ij) (src/artificial.jl:287-300); g[3d+j] = d u_j / d x_d.
+template <typename F>
+__global__ void k_strain(const F* __restrict__ g, F* __restrict__ out, int64_t cells) {
+    GRID_STRIDE(I, cells) {
+        double gv[9];
+#pragma unroll
+        for (int k = 0; k < 9; ++k) gv[k] = double(g[I + cells * k]);
+        double ss = 0.0;
+#pragma unroll
+        for (int b = 0; b < 3; ++b)
+#pragma unroll
+            for (int a = 0; a < 3; ++a) {
+                const double Sab = 0.5 * (gv[3 * a + b] + gv[3 * b + a]);
+                ss += Sab * Sab;
+            }
+        out[I] = F(sqrt(ss));
+    }
+}
+
+// delta4_sum! (src/artificial.jl:67-94): sum_d h_d^p |(1,-4,6,-4,1) f| along d,
+// periodic wrap or clamping at closed edges.
+template <typename F>
+__global__ void k_delta4(const F* __restrict__ f, F* __restrict__ out, Grid3 g, double w0, double w1, double w2) {
+    const int64_t cells = (int64_t)g.n[0] * g.n[1] * g.n[2];
+    const double wd[3] = {w0, w1, w2};
+    const double D4[5] = {1.0, -4.0, 6.0, -4.0, 1.0};
+    const int64_t st[3] = {1, (int64_t)g.n[0], (int64_t)g.n[0] * g.n[1]};
+    GRID_STRIDE(I, cells) {
+        const int i = (int)(I % g.n[0]);
+        const int j = (int)((I / g.n[0]) % g.n[1]);
+        const int k = (int)(I / ((int64_t)g.n[0] * g.n[1]));
+        const int ijk[3] = {i, j, k};
+        double o = 0.0;
+        for (int d = 0; d < 3; ++d) {
+            if (!g.active[d]) continue;
+            const int nd = g.n[d];
+            const int il = ijk[d];
+            double acc = 0.0;
+#pragma unroll
+            for (int m = -2; m <= 2; ++m) {
+                int ilm = il + m;
+                if (g.periodic[d]) ilm = ilm < 0 ? ilm + nd : (ilm >= nd ? ilm - nd : ilm);
+                else ilm = ilm < 0 ? 0 : (ilm >= nd ? nd - 1 : ilm);
+                acc += D4[m + 2] * double(f[I + (int64_t)(ilm - il) * st[d]]);
+            }
+            o += wd[d] * fabs(acc);
+        }
+        out[I] = F(o);
+    }
+}
+
+// Ducros switch (src/artificial.jl:134-147)
+__device__ __forceinline__ double compression_switch(const double* gv) {
+    const double div = gv[0] + gv[4] + gv[8];
+    if (!(div < 0)) return 0.0;
+    const double w1 = gv[3 * 1 + 2] - gv[3 * 2 + 1];
+    const double w2 = gv[3 * 2 + 0] - gv[3 * 0 + 2];
+    const double w3 = gv[3 * 0 + 1] - gv[3 * 1 + 0];
+    return div * div / (div * div + w1 * w1 + w2 * w2 + w3 * w3 + 1e-32);
+}
+
+// mu*, beta* from the smoothed strain sensor (src/artificial.jl:306-313),
+// optional gating (gate_beta!, :164-175).
+template <typename F>
+__global__ void k_mu_beta(const F* __restrict__ sensor, const F* __restrict__ prim, const F* __restrict__ g,
+                          F* __restrict__ art, int64_t cells, double C_mu, double C_beta, int gate) {
+    GRID_STRIDE(I, cells) {
+        const double rs = double(prim[I + cells * P_RHO]) * jl_max(double(sensor[I]), 0.0);
+        double beta = C_beta * rs;
+        if (gate) {
+            double gv[9];
+            for (int k = 0; k < 9; ++k) gv[k] = double(g[I + cells * k]);
+            beta *= compression_switch(gv);
+        }
+        art[I + cells * A_MU] = F(C_mu * rs);
+        art[I + cells * A_BETA] = F(beta);
+    }
+}
+
+// dilatation and switch for the :dilatation beta sensor (src/artificial.jl:208-218)
+template <typename F>
+__global__ void k_dilatation(const F* __restrict__ g, F* __restrict__ div, F* __restrict__ sw, int64_t cells) {
+    GRID_STRIDE(I, cells) {
+        double gv[9];
+        for (int k = 0; k < 9; ++k) gv[k] = double(g[I + cells * k]);
+        div[I] = F(gv[0] + gv[4] + gv[8]);
+        sw[I] = F(compression_switch(gv));
+    }
+}
+
+template <typename F>
+__global__ void k_beta_dilatation(const F* __restrict__ sensor, const F* __restrict__ prim, const F* __restrict__ sw,
+                                  F* __restrict__ art, int64_t cells, double C_beta) {
+    GRID_STRIDE(I, cells) {
+        art[I + cells * A_BETA] =
+            F(C_beta * double(prim[I + cells * P_RHO]) * jl_max(double(sensor[I]), 0.0) * double(sw[I]));
+    }
+}
+
+// internal energy e = (E - |m|^2/2rho)/rho with rho floored (src/artificial.jl:322-330)
+template <typename F>
+__global__ void k_energy(const double* __restrict__ Q, const F* __restrict__ prim, F* __restrict__ out, int64_t cells,
+                         int Ns) {
+    GRID_STRIDE(I, cells) {
+        const double r = jl_max(double(prim[I + cells * P_RHO]), 1e-300);
+        const double q1 = Q[I + cells * (Ns + 0)], q2 = Q[I + cells * (Ns + 1)], q3 = Q[I + cells * (Ns + 2)];
+        const double ke = 0.5 * (q1 * q1 + q2 * q2 + q3 * q3) / r;
+        out[I] = F((Q[I + cells * (Ns + 3)] - ke) / r);
+    }
+}
+
+// kappa* = C_kappa (rho c / max(T, eps)) max(sensor, 0) (src/artificial.jl:334-341, src/physics.jl:155-156)
+template <typename F>
+__global__ void k_kappa(const F* __restrict__ sensor, const F* __restrict__ prim, F* __restrict__ art, int64_t cells,
+                        double C_kappa) {
+    GRID_STRIDE(I, cells) {
+        const double scale = double(prim[I + cells * P_RHO]) * double(prim[I + cells * P_C]) /
+                             jl_max(double(prim[I + cells * P_T]), 2.220446049250313e-16);
+        art[I + cells * A_KAPPA] = F(C_kappa * scale * jl_max(double(sensor[I]), 0.0));
+    }
+}
+
+// D*_k = C_D c max(sensor_k, 0) (src/artificial.jl:348-356)
+template <typename F>
+__global__ void k_dart(const F* __restrict__ sensor, const F* __restrict__ prim, F* __restrict__ art, int64_t cells,
+                       double C_D, int sp) {
+    GRID_STRIDE(I, cells) {
+        art[I + cells * (A_D0 + sp)] = F(C_D * double(prim[I + cells * P_C]) * jl_max(double(sensor[I]), 0.0));
+    }
+}
+
+// _assemble_fluxes! (src/rhs.jl:495-556).  gty[d*(1+Ns) + 0] = dT/dx_d,
+// gty[d*(1+Ns) + 1 + k] = dY_k/dx_d; flux[d*ncons + c].
+template <typename F>
+__global__ void k_fluxes(const double* __restrict__ Q, const F* __restrict__ prim, const F* __restrict__ g,
+                         const F* __restrict__ gty, const F* __restrict__ art, F* __restrict__ flux, int64_t cells,
+                         int Ns, PhysConst pc, double mu0, double Pr, double Sc) {
+    const int ncons = Ns + 4;
+    GRID_STRIDE(I, cells) {
+        double gv[9];
+#pragma unroll
+        for (int k = 0; k < 9; ++k) gv[k] = double(g[I + cells * k]);
+        const double r = double(prim[I + cells * P_RHO]);
+        const double uv[3] = {double(prim[I + cells * P_U]), double(prim[I + cells * P_V]), double(prim[I + cells * P_W])};
+        const double p = double(prim[I + cells * P_P]);
+        const double Tp = double(prim[I + cells * P_T]);
+        const double E = Q[I + cells * (Ns + 3)];
+        const double mu = mu0 + double(art[I + cells * A_MU]);
+        const double be = double(art[I + cells * A_BETA]);
+        const double ka = mu0 * double(prim[I + cells * P_CP]) / Pr + double(art[I + cells * A_KAPPA]);
+        const double D0 = mu0 / (Sc * r);
+        const double divu = gv[0] + gv[4] + gv[8];
+        const double t11 = mu * (2 * gv[0] - (2.0 / 3.0) * divu) + be * divu;
+        const double t22 = mu * (2 * gv[4] - (2.0 / 3.0) * divu) + be * divu;
+        const double t33 = mu * (2 * gv[8] - (2.0 / 3.0) * divu) + be * divu;
+        const double t12 = mu * (gv[1] + gv[3]);
+        const double t13 = mu * (gv[2] + gv[6]);
+        const double t23 = mu * (gv[5] + gv[7]);
+        const double tau[3][3] = {{t11, t12, t13}, {t12, t22, t23}, {t13, t23, t33}};
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            const double ud = uv[d];
+            const double* td = tau[d];
+            const F* gd = gty + cells * (int64_t)(d * (1 + Ns));
+            F* fd = flux + cells * (int64_t)(d * ncons);
+            double Vc = 0.0;
+            for (int sp = 0; sp < Ns; ++sp)
+                Vc += (D0 + double(art[I + cells * (A_D0 + sp)])) * double(gd[I + cells * (1 + sp)]);
+            double hdiff = 0.0;
+            for (int sp = 0; sp < Ns; ++sp) {
+                const double Dk = D0 + double(art[I + cells * (A_D0 + sp)]);
+                const double Yk = double(prim[I + cells * (P_Y0 + sp)]);
+                const double Jkd = r * (-Dk * double(gd[I + cells * (1 + sp)]) + Yk * Vc);
+                fd[I + cells * sp] = F(r * Yk * ud + Jkd);
+                hdiff += pc.cpk[sp] * Tp * Jkd;
+            }
+            fd[I + cells * (Ns + 0)] = F(r * ud * uv[0] + (d == 0 ? p : 0.0) - td[0]);
+            fd[I + cells * (Ns + 1)] = F(r * ud * uv[1] + (d == 1 ? p : 0.0) - td[1]);
+            fd[I + cells * (Ns + 2)] = F(r * ud * uv[2] + (d == 2 ? p : 0.0) - td[2]);
+            fd[I + cells * (Ns + 3)] =
+                F((E + p) * ud - (uv[0] * td[0] + uv[1] * td[1] + uv[2] * td[2]) - ka * double(gd[I]) + hdiff);
+        }
+    }
+}
+
+// Low-storage RK update (src/timestep.jl:86-95): v = A du + dt dQ; du = v; Q += B v.
+template <typename F>
+__global__ void k_lsrk(double* __restrict__ Q, double* __restrict__ du, const F* __restrict__ dQ, int64_t n, double A,
+                       double B, double dt) {
+    GRID_STRIDE(I, n) {
+        const double v = A * du[I] + dt * double(dQ[I]);
+        du[I] = v;
+        Q[I] += B * v;
+    }
+}
+
+// max_rate per-block partials (src/timestep.jl:125-175), Cartesian.
+template <typename F>
+__global__ void k_rate_partial(const double* __restrict__ Q, const F* __restrict__ prim, const F* __restrict__ art,
+                               double* __restrict__ part, int64_t cells, int Ns, double idx0, double idx1, double idx2,
+                               int a0, int a1, int a2, double mu0, double Pr, double Sc) {
+    double rate = 0.0, rmin = __longlong_as_double(0x7ff0000000000000LL);
+    const double idx[3] = {idx0, idx1, idx2};
+    const int act[3] = {a0, a1, a2};
+    GRID_STRIDE(I, cells) {
+        double rq = 0.0;
+        for (int sp = 0; sp < Ns; ++sp) rq += Q[I + cells * sp];
+        rmin = jl_min(rmin, rq);
+        const double r = double(prim[I + cells * P_RHO]);
+        const double ri = 1 / r;
+        const double c = double(prim[I + cells * P_C]);
+        const double cp = double(prim[I + cells * P_CP]);
+        const double uv[3] = {double(prim[I + cells * P_U]), double(prim[I + cells * P_V]), double(prim[I + cells * P_W])};
+        double acc = 0.0, dsum = 0.0;
+        for (int d = 0; d < 3; ++d) {
+            if (!act[d]) continue;
+            acc += (fabs(uv[d]) + c) * idx[d];
+            dsum += idx[d] * idx[d];
+        }
+        double Dmax = mu0 / (Sc * r);
+        for (int sp = 0; sp < Ns; ++sp) Dmax = jl_max(Dmax, mu0 / (Sc * r) + double(art[I + cells * (A_D0 + sp)]));
+        const double nu = (mu0 + double(art[I + cells * A_MU]) + double(art[I + cells * A_BETA])) * ri +
+                          (mu0 * cp / Pr + double(art[I + cells * A_KAPPA])) * ri / cp + Dmax;
+        acc += 2 * nu * dsum;
+        rate = jl_max(rate, acc);
+    }
+    // block reduction (max / min are exact, so the order does not matter)
+    __shared__ double sr[kThreads], sm[kThreads];
+    sr[threadIdx.x] = rate;
+    sm[threadIdx.x] = rmin;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if ((int)threadIdx.x < s) {
+            sr[threadIdx.x] = jl_max(sr[threadIdx.x], sr[threadIdx.x + s]);
+            sm[threadIdx.x] = jl_min(sm[threadIdx.x], sm[threadIdx.x + s]);
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        part[2 * blockIdx.x] = sr[0];
+        part[2 * blockIdx.x + 1] = sm[0];
+    }
+}
+
+__global__ void k_rate_final(const double* __restrict__ part, int nb, double* __restrict__ out) {
+    __shared__ double sr[kThreads], sm[kThreads];
+    double rate = 0.0, rmin = __longlong_as_double(0x7ff0000000000000LL);
+    for (int b = threadIdx.x; b < nb; b += blockDim.x) {
+        rate = jl_max(rate, part[2 * b]);
+        rmin = jl_min(rmin, part[2 * b + 1]);
+    }
+    sr[threadIdx.x] = rate;
+    sm[threadIdx.x] = rmin;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if ((int)threadIdx.x < s) {
+            sr[threadIdx.x] = jl_max(sr[threadIdx.x], sr[threadIdx.x + s]);
+            sm[threadIdx.x] = jl_min(sm[threadIdx.x], sm[threadIdx.x + s]);
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) { out[0] = sr[0]; out[1] = sm[0]; }
+}
+
+// Fixed-order sums (deterministic) for diagnostics: per-block partials then one block.
+template <typename F>
+__global__ void k_ke_partial(const double* __restrict__ Q, double* __restrict__ part, int64_t cells, int Ns) {
+    __shared__ double s[kThreads];
+    double acc = 0.0;
+    GRID_STRIDE(I, cells) {
+        double r = 0.0;
+        for (int sp = 0; sp < Ns; ++sp) r += Q[I + cells * sp];
+        const double q1 = Q[I + cells * (Ns + 0)], q2 = Q[I + cells * (Ns + 1)], q3 = Q[I + cells * (Ns + 2)];
+        acc += 0.5 * (q1 * q1 + q2 * q2 + q3 * q3) / r;
+    }
+    s[threadIdx.x] = acc;
+    __syncthreads();
+    for (int st = blockDim.x / 2; st > 0; st >>= 1) {
+        if ((int)threadIdx.x < st) s[threadIdx.x] += s[threadIdx.x + st];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) part[blockIdx.x] = s[0];
+}
+
+// quad-weighted sum of tau:grad u and of rho (dissipation_rate, src/diagnostics.jl:354-378)
+template <typename F>
+__global__ void k_diss_partial(const F* __restrict__ prim, const F* __restrict__ g, const F* __restrict__ art,
+                               double* __restrict__ part, Grid3 gr, double mu0) {
+    __shared__ double s1[kThreads], s2[kThreads];
+    const int64_t cells = (int64_t)gr.n[0] * gr.n[1] * gr.n[2];
+    double a1 = 0.0, a2 = 0.0;
+    GRID_STRIDE(I, cells) {
+        const int i = (int)(I % gr.n[0]);
+        const int j = (int)((I / gr.n[0]) % gr.n[1]);
+        const int k = (int)(I / ((int64_t)gr.n[0] * gr.n[1]));
+        const int ijk[3] = {i, j, k};
+        double w = 1.0;
+        for (int d = 0; d < 3; ++d)
+            if (gr.active[d] && !gr.periodic[d] && (ijk[d] == 0 || ijk[d] == gr.n[d] - 1)) w *= 0.5;
+        double gv[9];
+        for (int q = 0; q < 9; ++q) gv[q] = double(g[I + cells * q]);
+        const double mu = mu0 + double(art[I + cells * A_MU]);
+        const double be = double(art[I + cells * A_BETA]);
+        const double divu = gv[0] + gv[4] + gv[8];
+        double acc = 0.0;
+        for (int b = 0; b < 3; ++b)
+            for (int a = 0; a < 3; ++a) {
+                const double tau = mu * (gv[3 * a + b] + gv[3 * b + a]) + (a == b ? (be - 2 * mu / 3) * divu : 0.0);
+                acc += tau * gv[3 * a + b];
+            }
+        a1 += w * acc;
+        a2 += w * double(prim[I + cells * P_RHO]);
+    }
+    s1[threadIdx.x] = a1;
+    s2[threadIdx.x] = a2;
+    __syncthreads();
+    for (int st = blockDim.x / 2; st > 0; st >>= 1) {
+        if ((int)threadIdx.x < st) { s1[threadIdx.x] += s1[threadIdx.x + st]; s2[threadIdx.x] += s2[threadIdx.x + st]; }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) { part[2 * blockIdx.x] = s1[0]; part[2 * blockIdx.x + 1] = s2[0]; }
+}
+
+__global__ void k_sum_final(const double* __restrict__ part, int nb, int width, double* __restrict__ out) {
+    __shared__ double s[kThreads];
+    for (int c = 0; c < width; ++c) {
+        double acc = 0.0;
+        for (int b = threadIdx.x; b < nb; b += blockDim.x) acc += part[(int64_t)width * b + c];
+        s[threadIdx.x] = acc;
+        __syncthreads();
+        for (int st = blockDim.x / 2; st > 0; st >>= 1) {
+            if ((int)threadIdx.x < st) s[threadIdx.x] += s[threadIdx.x + st];
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) out[c] = s[0];
+        __syncthreads();
+    }
+}
+
+// enforce!(::SlipWallBC) (src/boundary.jl:232-243) and a time-constant
+// DirichletBC (src/problem.jl:209-221) on the wall plane of (d, side).
+__global__ void k_bc_plane(double* __restrict__ Q, Grid3 g, int d, int side, int Ns, int kind, BcState st) {
+    const int o1 = d == 0 ? 1 : 0, o2 = d == 2 ? 1 : 2;
+    const int64_t plane = (int64_t)g.n[o1] * g.n[o2];
+    const int64_t cells = (int64_t)g.n[0] * g.n[1] * g.n[2];
+    const int64_t stv[3] = {1, (int64_t)g.n[0], (int64_t)g.n[0] * g.n[1]};
+    const int wall = side == 0 ? 0 : g.n[d] - 1;
+    GRID_STRIDE(t, plane) {
+        const int a = (int)(t % g.n[o1]), b = (int)(t / g.n[o1]);
+        const int64_t I = a * stv[o1] + b * stv[o2] + (int64_t)wall * stv[d];
+        if (kind == CLES_BC_SLIPWALL) {
+            double r = 0.0;
+            for (int sp = 0; sp < Ns; ++sp) r += Q[I + cells * sp];
+            const int mc = Ns + d;
+            const double mn = Q[I + cells * mc];
+            Q[I + cells * (Ns + 3)] -= 0.5 * mn * mn / r;
+            Q[I + cells * mc] = 0;
+        } else {
+            for (int c = 0; c < Ns + 4; ++c) Q[I + cells * c] = st.q[c];
+        }
+    }
+}
+
+template <typename F>
+__global__ void k_convert(const double* __restrict__ a, F* __restrict__ b, int64_t n) {
+    GRID_STRIDE(I, n) b[I] = F(a[I]);
+}
+
+template <typename F>
+__global__ void k_to_double(const F* __restrict__ a, double* __restrict__ b, int64_t n) {
+    GRID_STRIDE(I, n) b[I] = double(a[I]);
+}
+
+}  // namespace
+
+// ------------------------------------------------------------- launchers ----
+#define LAUNCH(kern, n, st, ...)                                      \
+    do {                                                               \
+        kern<<<grid_for(n), kThreads, 0, st>>>(__VA_ARGS__);           \
+        count_launch();                                                \
+        check_launch(#kern);                                           \
+    } while (0)
+
+template <typename F>
+void Pointwise<F>::primitives(const double* Q, F* prim, int64_t cells, int Ns, const PhysConst& pc, cudaStream_t st) {
+    LAUNCH(k_primitives<F>, cells, st, Q, prim, cells, Ns, pc);
+}
+template <typename F>
+void Pointwise<F>::strain(const F* g, F* out, int64_t cells, cudaStream_t st) {
+    LAUNCH(k_strain<F>, cells, st, g, out, cells);
+}
+template <typename F>
+void Pointwise<F>::delta4(const F* f, F* out, const Grid3& g, const double wd[3], cudaStream_t st) {
+    const int64_t cells = (int64_t)g.n[0] * g.n[1] * g.n[2];
+    LAUNCH(k_delta4<F>, cells, st, f, out, g, wd[0], wd[1], wd[2]);
+}
+template <typename F>
+void Pointwise<F>::mu_beta(const F* sensor, const F* prim, const F* g, F* art, int64_t cells, double C_mu,
+                           double C_beta, int gate, cudaStream_t st) {
+    LAUNCH(k_mu_beta<F>, cells, st, sensor, prim, g, art, cells, C_mu, C_beta, gate);
+}
+template <typename F>
+void Pointwise<F>::dilatation(const F* g, F* div, F* sw, int64_t cells, cudaStream_t st) {
+    LAUNCH(k_dilatation<F>, cells, st, g, div, sw, cells);
+}
+template <typename F>
+void Pointwise<F>::beta_dilatation(const F* sensor, const F* prim, const F* sw, F* art, int64_t cells, double C_beta,
+                                   cudaStream_t st) {
+    LAUNCH(k_beta_dilatation<F>, cells, st, sensor, prim, sw, art, cells, C_beta);
+}
+template <typename F>
+void Pointwise<F>::energy(const double* Q, const F* prim, F* out, int64_t cells, int Ns, cudaStream_t st) {
+    LAUNCH(k_energy<F>, cells, st, Q, prim, out, cells, Ns);
+}
+template <typename F>
+void Pointwise<F>::kappa(const F* sensor, const F* prim, F* art, int64_t cells, double C_kappa, cudaStream_t st) {
+    LAUNCH(k_kappa<F>, cells, st, sensor, prim, art, cells, C_kappa);
+}
+template <typename F>
+void Pointwise<F>::dart(const F* sensor, const F* prim, F* art, int64_t cells, double C_D, int sp, cudaStream_t st) {
+    LAUNCH(k_dart<F>, cells, st, sensor, prim, art, cells, C_D, sp);
+}
+template <typename F>
+void Pointwise<F>::fluxes(const double* Q, const F* prim, const F* g, const F* gty, const F* art, F* flux,
+                          int64_t cells, int Ns, const PhysConst& pc, double mu0, double Pr, double Sc,
+                          cudaStream_t st) {
+    LAUNCH(k_fluxes<F>, cells, st, Q, prim, g, gty, art, flux, cells, Ns, pc, mu0, Pr, Sc);
+}
+template <typename F>
+void Pointwise<F>::lsrk(double* Q, double* du, const F* dQ, int64_t n, double A, double B, double dt, cudaStream_t st) {
+    LAUNCH(k_lsrk<F>, n, st, Q, du, dQ, n, A, B, dt);
+}
+template <typename F>
+void Pointwise<F>::rate(const double* Q, const F* prim, const F* art, double* part, double* out, int64_t cells, int Ns,
+                        const double idx[3], const int act[3], double mu0, double Pr, double Sc, cudaStream_t st) {
+    const unsigned nb = grid_for(cells);
+    k_rate_partial<F><<<nb, kThreads, 0, st>>>(Q, prim, art, part, cells, Ns, idx[0], idx[1], idx[2], act[0], act[1],
+                                               act[2], mu0, Pr, Sc);
+    count_launch();
+    check_launch("k_rate_partial");
+    k_rate_final<<<1, kThreads, 0, st>>>(part, (int)nb, out);
+    count_launch();
+    check_launch("k_rate_final");
+}
+template <typename F>
+void Pointwise<F>::kinetic(const double* Q, double* part, double* out, int64_t cells, int Ns, cudaStream_t st) {
+    const unsigned nb = grid_for(cells);
+    k_ke_partial<F><<<nb, kThreads, 0, st>>>(Q, part, cells, Ns);
+    count_launch();
+    check_launch("k_ke_partial");
+    k_sum_final<<<1, kThreads, 0, st>>>(part, (int)nb, 1, out);
+    count_launch();
+    check_launch("k_sum_final");
+}
+template <typename F>
+void Pointwise<F>::dissipation(const F* prim, const F* g, const F* art, double* part, double* out, const Grid3& gr,
+                               double mu0, cudaStream_t st) {
+    const int64_t cells = (int64_t)gr.n[0] * gr.n[1] * gr.n[2];
+    const unsigned nb = grid_for(cells);
+    k_diss_partial<F><<<nb, kThreads, 0, st>>>(prim, g, art, part, gr, mu0);
+    count_launch();
+    check_launch("k_diss_partial");
+    k_sum_final<<<1, kThreads, 0, st>>>(part, (int)nb, 2, out);
+    count_launch();
+    check_launch("k_sum_final");
+}
+template <typename F>
+void Pointwise<F>::convert(const double* a, F* b, int64_t n, cudaStream_t st) {
+    LAUNCH(k_convert<F>, n, st, a, b, n);
+}
+template <typename F>
+void Pointwise<F>::to_double(const F* a, double* b, int64_t n, cudaStream_t st) {
+    LAUNCH(k_to_double<F>, n, st, a, b, n);
+}
+
+void bc_plane(double* Q, const Grid3& g, int d, int side, int Ns, int kind, const BcState& s, cudaStream_t st) {
+    const int o1 = d == 0 ? 1 : 0, o2 = d == 2 ? 1 : 2;
+    const int64_t plane = (int64_t)g.n[o1] * g.n[o2];
+    k_bc_plane<<<grid_for(plane), kThreads, 0, st>>>(Q, g, d, side, Ns, kind, s);
+    count_launch();
+    check_launch("k_bc_plane");
+}
+
+int64_t rate_partials(int64_t cells) { return (int64_t)grid_for(cells); }
+
+template struct Pointwise<double>;
+template struct Pointwise<float>;
+
+}  // namespace cles

@@ -1,0 +1,58 @@
+// Pointwise kernels of the RHS and the integrator.
+#pragma once
+
+#include "cles_internal.h"
+
+namespace cles {
+
+// Slots of the primitive block (one interior field each, component stride = cells).
+// T and the mass fractions are adjacent so their gradients are one batched launch.
+enum { P_RHO = 0, P_U = 1, P_V = 2, P_W = 3, P_P = 4, P_C = 5, P_CP = 6, P_T = 7, P_Y0 = 8 };
+// Slots of the artificial-property block.
+enum { A_MU = 0, A_BETA = 1, A_KAPPA = 2, A_D0 = 3 };
+
+struct PhysConst {
+    double Rk[CLES_MAX_SPECIES];
+    double cvk[CLES_MAX_SPECIES];
+    double cpk[CLES_MAX_SPECIES];
+};
+
+struct Grid3 {
+    int n[3];
+    int active[3];
+    int periodic[3];
+};
+
+struct BcState {
+    double q[CLES_MAX_SPECIES + 4];
+};
+
+template <typename F>
+struct Pointwise {
+    static void primitives(const double* Q, F* prim, int64_t cells, int Ns, const PhysConst& pc, cudaStream_t st);
+    static void strain(const F* g, F* out, int64_t cells, cudaStream_t st);
+    static void delta4(const F* f, F* out, const Grid3& g, const double wd[3], cudaStream_t st);
+    static void mu_beta(const F* sensor, const F* prim, const F* g, F* art, int64_t cells, double C_mu, double C_beta,
+                        int gate, cudaStream_t st);
+    static void dilatation(const F* g, F* div, F* sw, int64_t cells, cudaStream_t st);
+    static void beta_dilatation(const F* sensor, const F* prim, const F* sw, F* art, int64_t cells, double C_beta,
+                                cudaStream_t st);
+    static void energy(const double* Q, const F* prim, F* out, int64_t cells, int Ns, cudaStream_t st);
+    static void kappa(const F* sensor, const F* prim, F* art, int64_t cells, double C_kappa, cudaStream_t st);
+    static void dart(const F* sensor, const F* prim, F* art, int64_t cells, double C_D, int sp, cudaStream_t st);
+    static void fluxes(const double* Q, const F* prim, const F* g, const F* gty, const F* art, F* flux, int64_t cells,
+                       int Ns, const PhysConst& pc, double mu0, double Pr, double Sc, cudaStream_t st);
+    static void lsrk(double* Q, double* du, const F* dQ, int64_t n, double A, double B, double dt, cudaStream_t st);
+    static void rate(const double* Q, const F* prim, const F* art, double* part, double* out, int64_t cells, int Ns,
+                     const double idx[3], const int act[3], double mu0, double Pr, double Sc, cudaStream_t st);
+    static void kinetic(const double* Q, double* part, double* out, int64_t cells, int Ns, cudaStream_t st);
+    static void dissipation(const F* prim, const F* g, const F* art, double* part, double* out, const Grid3& gr,
+                            double mu0, cudaStream_t st);
+    static void convert(const double* a, F* b, int64_t n, cudaStream_t st);
+    static void to_double(const F* a, double* b, int64_t n, cudaStream_t st);
+};
+
+void bc_plane(double* Q, const Grid3& g, int d, int side, int Ns, int kind, const BcState& s, cudaStream_t st);
+int64_t rate_partials(int64_t cells);
+
+}  // namespace cles

@@ -1,0 +1,502 @@
+// Device-resident solver runtime.
+//
+// Orchestrates the kernels of compact.cu and pointwise.cu in the order of the
+// reference's compute_rhs! (src/rhs.jl:624-694), step! (src/timestep.jl:72-99),
+// max_rate (:125-175), filter_state! (:414-426) and run! (:277-405).  All
+// fields live on the device in the interior layout (x fastest, no halos);
+// periodic wraps and closed-edge closures are handled inside the kernels, so
+// the reference's halo exchanges have no device counterpart.
+
+#include "solver.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <limits>
+
+namespace cles {
+
+void DevBuf::alloc(cles_ctx* c, size_t b) {
+    release();
+    ctx = c;
+    if (b == 0) return;
+    if (ctx->budget && ctx->allocated + b > ctx->budget)
+        throw Error(CLES_ENOMEM, "HBM budget exceeded: need " + std::to_string(ctx->allocated + b) + " bytes of " +
+                                     std::to_string(ctx->budget));
+    cudaError_t e = cudaMalloc(&p, b);
+    if (e != cudaSuccess) {
+        p = nullptr;
+        cudaGetLastError();
+        throw Error(CLES_ENOMEM, std::string("cudaMalloc failed: ") + cudaGetErrorString(e));
+    }
+    bytes = b;
+    ctx->allocated += b;
+}
+
+void DevBuf::release() {
+    if (p) {
+        cudaFree(p);
+        if (ctx) ctx->allocated -= bytes;
+    }
+    p = nullptr;
+    bytes = 0;
+}
+
+namespace {
+
+const double RKA[5] = {0.0, -567301805773.0 / 1357537059087.0, -2404267990393.0 / 2016746695238.0,
+                       -3550918686646.0 / 2091501179385.0, -1275806237668.0 / 842570457699.0};
+const double RKB[5] = {1432997174477.0 / 9575080441755.0, 5161836677717.0 / 13612068292357.0,
+                       1720146321549.0 / 2090206949498.0, 3134564353537.0 / 4481467310338.0,
+                       2277821191437.0 / 14882151754819.0};
+const double RKC[5] = {0.0, 1432997174477.0 / 9575080441755.0, 2526269341429.0 / 6820363962896.0,
+                       2006345519317.0 / 3224310063776.0, 2802321613138.0 / 2924317926251.0};
+const double PLANCK_TIME = 5.391247e-44;
+
+inline double jmax(double x, double y) {
+    if (std::isnan(x)) return x;
+    if (std::isnan(y)) return y;
+    return y > x ? y : x;
+}
+inline double jmin(double x, double y) {
+    if (std::isnan(x)) return x;
+    if (std::isnan(y)) return y;
+    return y < x ? y : x;
+}
+
+template <typename F>
+class Solver final : public SolverBase {
+public:
+    Solver(cles_ctx* ctx, const cles_solver_desc& d) : ctx_(ctx) {
+        desc = d;
+        st_ = ctx->stream;
+        for (int k = 0; k < 3; ++k) {
+            const bool p0 = d.bc[k][0] == CLES_BC_PERIODIC, p1 = d.bc[k][1] == CLES_BC_PERIODIC;
+            if (p0 != p1) throw Error(CLES_EINVAL, "dimension " + std::to_string(k + 1) + " mixes periodic and non-periodic conditions");
+            if (d.n_global[k] < 1) throw Error(CLES_EINVAL, "n_global must be >= 1");
+            if (d.n_global[k] == 1 && !p0) throw Error(CLES_EINVAL, "collapsed dimension must use (PeriodicBC(), PeriodicBC())");
+            for (int s = 0; s < 2; ++s)
+                if (d.bc[k][s] < CLES_BC_PERIODIC || d.bc[k][s] > CLES_BC_DIRICHLET) throw Error(CLES_EINVAL, "unknown boundary condition");
+            g_.n[k] = d.n_global[k];
+            g_.active[k] = d.n_global[k] > 1;
+            g_.periodic[k] = g_.active[k] ? p0 : 1;
+            pad_[k] = g_.active[k] ? d.n_halo : 0;
+            h_[k] = !g_.active[k] ? 1.0 : (g_.periodic[k] ? d.L[k] / d.n_global[k] : d.L[k] / (d.n_global[k] - 1));
+        }
+        if (d.n_species < 1 || d.n_species > CLES_MAX_SPECIES) throw Error(CLES_EINVAL, "bad species count");
+        if (d.beta_sensor < 0 || d.beta_sensor > 2) throw Error(CLES_EINVAL, "unknown beta sensor");
+        Ns_ = d.n_species;
+        ncons_ = Ns_ + 4;
+        for (int k = 0; k < Ns_; ++k) {
+            pc_.Rk[k] = d.R[k];
+            pc_.cvk[k] = d.R[k] / (d.gamma[k] - 1);
+            pc_.cpk[k] = pc_.Rk[k] + pc_.cvk[k];
+        }
+        cells_ = (int64_t)g_.n[0] * g_.n[1] * g_.n[2];
+        cfl = d.cfl;
+        const int dt = sizeof(F) == 8 ? CLES_F64 : CLES_F32;
+        for (int k = 0; k < 3; ++k) {
+            if (!g_.active[k]) continue;
+            deriv_[k].reset(new CompactPlan());
+            build_compact_plan(*deriv_[k], d.deriv, g_.n, k, g_.periodic[k] != 0, h_[k], dt);
+            filt_[k].reset(new CompactPlan());
+            build_compact_plan(*filt_[k], d.filt, g_.n, k, g_.periodic[k] != 0, h_[k], dt);
+            if (dt != CLES_F64) {
+                qfilt_[k].reset(new CompactPlan());
+                build_compact_plan(*qfilt_[k], d.filt, g_.n, k, g_.periodic[k] != 0, h_[k], CLES_F64);
+            }
+        }
+        const size_t c = (size_t)cells_;
+        Q_.alloc(ctx, sizeof(double) * c * ncons_);
+        du_.alloc(ctx, sizeof(double) * c * ncons_);
+        dQ_.alloc(ctx, sizeof(F) * c * ncons_);
+        prim_.alloc(ctx, sizeof(F) * c * (P_Y0 + Ns_));
+        g_u_.alloc(ctx, sizeof(F) * c * 9);
+        gty_.alloc(ctx, sizeof(F) * c * 3 * (1 + Ns_));
+        art_.alloc(ctx, sizeof(F) * c * (A_D0 + Ns_));
+        scratch_.alloc(ctx, sizeof(F) * c * 5);
+        flux_.alloc(ctx, sizeof(F) * c * 3 * ncons_);
+        part_.alloc(ctx, sizeof(double) * 2 * (size_t)(rate_partials(cells_) + 1));
+        res_.alloc(ctx, sizeof(double) * 4);
+        CLES_CUDA(cudaMallocHost(&host_res_, sizeof(double) * 4));
+        // du, gradients of collapsed dims and the artificial properties start
+        // at zero, as after allocation in the reference
+        CLES_CUDA(cudaMemsetAsync(Q_.p, 0, Q_.bytes, st_));
+        CLES_CUDA(cudaMemsetAsync(du_.p, 0, du_.bytes, st_));
+        CLES_CUDA(cudaMemsetAsync(dQ_.p, 0, dQ_.bytes, st_));
+        CLES_CUDA(cudaMemsetAsync(prim_.p, 0, prim_.bytes, st_));
+        CLES_CUDA(cudaMemsetAsync(g_u_.p, 0, g_u_.bytes, st_));
+        CLES_CUDA(cudaMemsetAsync(gty_.p, 0, gty_.bytes, st_));
+        CLES_CUDA(cudaMemsetAsync(art_.p, 0, art_.bytes, st_));
+        CLES_CUDA(cudaMemsetAsync(scratch_.p, 0, scratch_.bytes, st_));
+        CLES_CUDA(cudaMemsetAsync(flux_.p, 0, flux_.bytes, st_));
+        if (d.control.retries > 0) save_.alloc(ctx, sizeof(double) * c * ncons_);
+        CLES_CUDA(cudaStreamSynchronize(st_));
+    }
+
+    ~Solver() override {
+        if (host_res_) cudaFreeHost(host_res_);
+    }
+
+    // ------------------------------------------------------------- views --
+    FieldView view(void* p) const { return FieldView{p, cells_, g_.n[0], (int64_t)g_.n[0] * g_.n[1]}; }
+    F* prim(int slot) const { return prim_.as<F>() + (size_t)cells_ * slot; }
+    F* scratch(int k) const { return scratch_.as<F>() + (size_t)cells_ * k; }
+
+    // --------------------------------------------------------- operators --
+    void smooth(F* f) {
+        // smooth! (src/artificial.jl:98-111): one filter pass per active dim, in place
+        for (int k = 0; k < 3; ++k)
+            if (g_.active[k]) launch_compact(*filt_[k], view(f), view(f), 1, OUT_STORE, st_);
+    }
+
+    void apply_bcs() override {
+        for (int k = 0; k < 3; ++k) {
+            if (!g_.active[k]) continue;
+            for (int s = 0; s < 2; ++s) {
+                const int bc = desc.bc[k][s];
+                if (bc == CLES_BC_PERIODIC) continue;
+                BcState bs;
+                for (int c = 0; c < ncons_; ++c) bs.q[c] = desc.bc_state[k][s][c];
+                bc_plane(Q_.as<double>(), g_, k, s, Ns_, bc, bs, st_);
+            }
+        }
+    }
+
+    void compute_artificial() {
+        if (!desc.art_enabled) return;
+        using PW = Pointwise<F>;
+        F* strain = scratch(0);
+        F* sensor = scratch(1);
+        F* sensor_sp = scratch(2);
+        F* tmp_a = scratch(3);
+        F* tmp_b = scratch(4);
+        const double w2[3] = {h_[0] * h_[0], h_[1] * h_[1], h_[2] * h_[2]};
+        const double w1[3] = {h_[0], h_[1], h_[2]};
+        PW::strain(g_u_.as<F>(), strain, cells_, st_);
+        PW::delta4(strain, sensor, g_, w2, st_);
+        smooth(sensor);
+        PW::mu_beta(sensor, prim_.as<F>(), g_u_.as<F>(), art_.as<F>(), cells_, desc.C_mu, desc.C_beta,
+                    desc.beta_sensor == CLES_BETA_GATED_STRAIN, st_);
+        if (desc.beta_sensor == CLES_BETA_DILATATION) {
+            PW::dilatation(g_u_.as<F>(), tmp_a, tmp_b, cells_, st_);
+            PW::delta4(tmp_a, sensor, g_, w2, st_);
+            smooth(sensor);
+            PW::beta_dilatation(sensor, prim_.as<F>(), tmp_b, art_.as<F>(), cells_, desc.C_beta, st_);
+        }
+        PW::energy(Q_.as<double>(), prim_.as<F>(), tmp_a, cells_, Ns_, st_);
+        PW::delta4(tmp_a, sensor, g_, w1, st_);
+        smooth(sensor);
+        PW::kappa(sensor, prim_.as<F>(), art_.as<F>(), cells_, desc.C_kappa, st_);
+        if (Ns_ > 1) {
+            for (int sp = 0; sp < Ns_; ++sp) {
+                PW::delta4(prim(P_Y0 + sp), sensor_sp, g_, w1, st_);
+                smooth(sensor_sp);
+                PW::dart(sensor_sp, prim_.as<F>(), art_.as<F>(), cells_, desc.C_D, sp, st_);
+            }
+        }
+    }
+
+    void compute_rhs(bool primitives_current) override {
+        using PW = Pointwise<F>;
+        if (!primitives_current) PW::primitives(Q_.as<double>(), prim_.as<F>(), cells_, Ns_, pc_, st_);
+        // velocity gradients grad_u[d][j] (src/rhs.jl:596-603), one launch per dim for u, v, w
+        for (int k = 0; k < 3; ++k)
+            if (g_.active[k])
+                launch_compact(*deriv_[k], view(prim(P_U)), view(g_u_.as<F>() + (size_t)cells_ * 3 * k), 3, OUT_STORE, st_);
+        compute_artificial();
+        // temperature and mass-fraction gradients (src/rhs.jl:628-636)
+        for (int k = 0; k < 3; ++k)
+            if (g_.active[k])
+                launch_compact(*deriv_[k], view(prim(P_T)), view(gty_.as<F>() + (size_t)cells_ * (1 + Ns_) * k), 1 + Ns_,
+                               OUT_STORE, st_);
+        PW::fluxes(Q_.as<double>(), prim_.as<F>(), g_u_.as<F>(), gty_.as<F>(), art_.as<F>(), flux_.as<F>(), cells_, Ns_,
+                   pc_, desc.mu0, desc.Pr, desc.Sc, st_);
+        // flux divergence dQ[c] = -sum_d D_d(F_dc) (src/rhs.jl:650-668), accumulated in the store
+        bool first = true;
+        for (int k = 0; k < 3; ++k) {
+            if (!g_.active[k]) continue;
+            launch_compact(*deriv_[k], view(flux_.as<F>() + (size_t)cells_ * ncons_ * k), view(dQ_.as<F>()), ncons_,
+                           first ? OUT_NEGATE : OUT_SUBTRACT, st_);
+            first = false;
+        }
+        if (first) CLES_CUDA(cudaMemsetAsync(dQ_.p, 0, dQ_.bytes, st_));
+    }
+
+    void step(double dt, bool prepared) override {
+        for (int stage = 0; stage < 5; ++stage) {
+            tstage = t + RKC[stage] * dt;
+            const bool first_prepared = prepared && stage == 0;
+            if (!first_prepared) apply_bcs();
+            compute_rhs(first_prepared);
+            Pointwise<F>::lsrk(Q_.as<double>(), du_.as<double>(), dQ_.as<F>(), cells_ * ncons_, RKA[stage], RKB[stage],
+                               dt, st_);
+        }
+        tstage = t + dt;
+        apply_bcs();
+    }
+
+    void max_rate(double* rate, double* rho_min) override {
+        Pointwise<F>::primitives(Q_.as<double>(), prim_.as<F>(), cells_, Ns_, pc_, st_);
+        double idx[3];
+        int act[3];
+        for (int k = 0; k < 3; ++k) { idx[k] = 1.0 / h_[k]; act[k] = g_.active[k]; }
+        Pointwise<F>::rate(Q_.as<double>(), prim_.as<F>(), art_.as<F>(), part_.as<double>(), res_.as<double>(), cells_,
+                           Ns_, idx, act, desc.mu0, desc.Pr, desc.Sc, st_);
+        CLES_CUDA(cudaMemcpyAsync(host_res_, res_.p, 2 * sizeof(double), cudaMemcpyDeviceToHost, st_));
+        CLES_CUDA(cudaStreamSynchronize(st_));
+        *rate = host_res_[0];
+        *rho_min = host_res_[1];
+    }
+
+    void filter_state() override {
+        // filter_state! (src/timestep.jl:414-426): every conserved component
+        // along every active dim in turn, in place (FP64 state in every mode)
+        for (int k = 0; k < 3; ++k) {
+            if (!g_.active[k]) continue;
+            const CompactPlan& p = qfilt_[k] ? *qfilt_[k] : *filt_[k];
+            launch_compact(p, view(Q_.p), view(Q_.p), ncons_, OUT_STORE, st_);
+        }
+    }
+
+    double predicted_dt(double rate) {
+        const cles_step_control& c = desc.control;
+        double r = rate;
+        if (c.predict > 0 && rate_prev > 0) r = jmax(r, r + c.predict * (r - rate_prev));
+        double dt = cfl / r;
+        if (c.max_growth > 0 && dt_prev > 0) dt = jmin(dt, c.max_growth * dt_prev);
+        return dt;
+    }
+
+    int run(double tfinal, int64_t nmax, cles_run_result* res) override {
+        const cles_step_control& ctl = desc.control;
+        const bool have_save = ctl.retries > 0;
+        double save_t = t;
+        int64_t save_step = step_count;
+        if (have_save) {
+            if (!save_.p) save_.alloc(ctx_, sizeof(double) * (size_t)cells_ * ncons_);
+            CLES_CUDA(cudaMemcpyAsync(save_.p, Q_.p, Q_.bytes, cudaMemcpyDeviceToDevice, st_));
+        }
+        int attempts = 0;
+        double dt_seen = 0.0, last_dt = 0.0;
+        int64_t guard_step = -1, done = 0;
+        int failure = CLES_FAIL_NONE;
+        while (t < tfinal && step_count < nmax) {
+            tstage = t;
+            apply_bcs();
+            double rate, rmin;
+            max_rate(&rate, &rmin);
+            double dt = predicted_dt(rate);
+            const int f = check_step(ctl, dt, rmin, dt_seen);
+            if (f != CLES_FAIL_NONE) {
+                if (!have_save || attempts >= ctl.retries) { failure = f; break; }
+                attempts += 1;
+                const int64_t fail_step = step_count;
+                CLES_CUDA(cudaMemcpyAsync(Q_.p, save_.p, Q_.bytes, cudaMemcpyDeviceToDevice, st_));
+                t = save_t;
+                step_count = save_step;
+                cfl *= ctl.cfl_backoff;
+                guard_step = fail_step;
+                dt_prev = 0.0;
+                rate_prev = 0.0;
+                dt_seen = 0.0;
+                continue;
+            }
+            if (have_save && ctl.savepoint_interval > 0 && step_count > guard_step &&
+                step_count % ctl.savepoint_interval == 0) {
+                CLES_CUDA(cudaMemcpyAsync(save_.p, Q_.p, Q_.bytes, cudaMemcpyDeviceToDevice, st_));
+                save_t = t;
+                save_step = step_count;
+            }
+            dt_seen = jmax(dt_seen, dt);
+            dt = jmin(dt, tfinal - t);
+            step(dt, true);
+            t += dt;
+            step_count += 1;
+            dt_prev = dt;
+            rate_prev = rate;
+            last_dt = dt;
+            ++done;
+            if (desc.filter_interval > 0 && step_count % desc.filter_interval == 0) filter_state();
+        }
+        CLES_CUDA(cudaStreamSynchronize(st_));
+        if (res) {
+            res->steps = done;
+            res->t = t;
+            res->last_dt = last_dt;
+            res->cfl = cfl;
+            res->failure = failure;
+            res->retries_used = attempts;
+        }
+        return failure == CLES_FAIL_NONE ? CLES_OK : CLES_EFAILURE;
+    }
+
+    // ---------------------------------------------------------- transfers --
+    void set_state(const double* Q, int layout) override {
+        copy_state_h2d(Q_.as<double>(), Q, g_.n, pad_, ncons_, layout, st_);
+        CLES_CUDA(cudaStreamSynchronize(st_));
+    }
+    void get_state(double* Q, int layout) override {
+        copy_state_d2h(Q, Q_.as<double>(), g_.n, pad_, ncons_, layout, st_);
+        CLES_CUDA(cudaStreamSynchronize(st_));
+    }
+    void get_double(const F* src, int ncomp, double* host, int layout) {
+        if (sizeof(F) == sizeof(double)) {
+            copy_state_d2h(host, reinterpret_cast<const double*>(src), g_.n, pad_, ncomp, layout, st_);
+        } else {
+            DevBuf tmp;
+            tmp.alloc(ctx_, sizeof(double) * (size_t)cells_ * ncomp);
+            Pointwise<F>::to_double(src, tmp.as<double>(), cells_ * ncomp, st_);
+            copy_state_d2h(host, tmp.as<double>(), g_.n, pad_, ncomp, layout, st_);
+            CLES_CUDA(cudaStreamSynchronize(st_));
+        }
+        CLES_CUDA(cudaStreamSynchronize(st_));
+    }
+    void get_rhs(double* dQ, int layout) override { get_double(dQ_.as<F>(), ncons_, dQ, layout); }
+    void get_field(int which, double* host, int layout) override {
+        const F* src = nullptr;
+        switch (which) {
+            case CLES_FIELD_RHO: src = prim(P_RHO); break;
+            case CLES_FIELD_U: src = prim(P_U); break;
+            case CLES_FIELD_V: src = prim(P_V); break;
+            case CLES_FIELD_W: src = prim(P_W); break;
+            case CLES_FIELD_P: src = prim(P_P); break;
+            case CLES_FIELD_T: src = prim(P_T); break;
+            case CLES_FIELD_C: src = prim(P_C); break;
+            case CLES_FIELD_CP: src = prim(P_CP); break;
+            case CLES_FIELD_MU_ART: src = art_.as<F>() + (size_t)cells_ * A_MU; break;
+            case CLES_FIELD_BETA_ART: src = art_.as<F>() + (size_t)cells_ * A_BETA; break;
+            case CLES_FIELD_KAPPA_ART: src = art_.as<F>() + (size_t)cells_ * A_KAPPA; break;
+            case CLES_FIELD_SENSOR: src = scratch(1); break;
+            default:
+                if (which >= CLES_FIELD_Y0 && which < CLES_FIELD_Y0 + Ns_) src = prim(P_Y0 + which - CLES_FIELD_Y0);
+                else if (which >= CLES_FIELD_D_ART0 && which < CLES_FIELD_D_ART0 + Ns_)
+                    src = art_.as<F>() + (size_t)cells_ * (A_D0 + which - CLES_FIELD_D_ART0);
+                else if (which >= CLES_FIELD_GRAD_U0 && which < CLES_FIELD_GRAD_U0 + 9)
+                    src = g_u_.as<F>() + (size_t)cells_ * (which - CLES_FIELD_GRAD_U0);
+        }
+        if (!src) throw Error(CLES_EINVAL, "unknown field");
+        get_double(src, 1, host, layout);
+    }
+
+    double kinetic_energy() override {
+        Pointwise<F>::kinetic(Q_.as<double>(), part_.as<double>(), res_.as<double>(), cells_, Ns_, st_);
+        CLES_CUDA(cudaMemcpyAsync(host_res_, res_.p, sizeof(double), cudaMemcpyDeviceToHost, st_));
+        CLES_CUDA(cudaStreamSynchronize(st_));
+        double cellvol = 1.0, vol = 1.0;
+        for (int k = 0; k < 3; ++k) {
+            cellvol *= g_.active[k] ? h_[k] : 1.0;
+            vol *= g_.active[k] ? desc.L[k] : 1.0;
+        }
+        return host_res_[0] * cellvol / vol;
+    }
+
+    double dissipation_rate() override {
+        // dissipation_rate (src/diagnostics.jl:354-378): refreshes primitives,
+        // gradients and artificial properties from the resident state
+        using PW = Pointwise<F>;
+        PW::primitives(Q_.as<double>(), prim_.as<F>(), cells_, Ns_, pc_, st_);
+        for (int k = 0; k < 3; ++k)
+            if (g_.active[k])
+                launch_compact(*deriv_[k], view(prim(P_U)), view(g_u_.as<F>() + (size_t)cells_ * 3 * k), 3, OUT_STORE, st_);
+        compute_artificial();
+        PW::dissipation(prim_.as<F>(), g_u_.as<F>(), art_.as<F>(), part_.as<double>(), res_.as<double>(), g_, desc.mu0,
+                        st_);
+        CLES_CUDA(cudaMemcpyAsync(host_res_, res_.p, 2 * sizeof(double), cudaMemcpyDeviceToHost, st_));
+        CLES_CUDA(cudaStreamSynchronize(st_));
+        return host_res_[0] / host_res_[1];
+    }
+
+    double* state_device() override { return Q_.as<double>(); }
+
+    cles_solver_info info() const override {
+        cles_solver_info I;
+        std::memset(&I, 0, sizeof(I));
+        for (int k = 0; k < 3; ++k) {
+            I.n_local[k] = g_.n[k];
+            I.active[k] = g_.active[k];
+            I.h[k] = h_[k];
+        }
+        I.n_cons = ncons_;
+        I.n_species = Ns_;
+        I.cells = cells_;
+        I.padded_cells = (int64_t)(g_.n[0] + 2 * pad_[0]) * (g_.n[1] + 2 * pad_[1]) * (g_.n[2] + 2 * pad_[2]);
+        I.device_bytes = ctx_->allocated;
+        return I;
+    }
+
+private:
+    cles_ctx* ctx_;
+    cudaStream_t st_;
+    Grid3 g_{};
+    int pad_[3]{};
+    double h_[3]{};
+    int Ns_ = 1, ncons_ = 5;
+    int64_t cells_ = 0;
+    PhysConst pc_{};
+    std::unique_ptr<CompactPlan> deriv_[3], filt_[3], qfilt_[3];
+    DevBuf Q_, du_, dQ_, prim_, g_u_, gty_, art_, scratch_, flux_, part_, res_, save_;
+    double* host_res_ = nullptr;
+};
+
+}  // namespace
+
+int check_step(const cles_step_control& c, double dt, double rho_min, double dt_seen) {
+    // check_step (src/stepcontrol.jl:184-204)
+    if (!std::isfinite(dt)) return CLES_FAIL_NONFINITE;
+    if (!(rho_min > 0)) return CLES_FAIL_NEGATIVE_DENSITY;
+    if (!(dt > PLANCK_TIME)) return CLES_FAIL_PLANCK;
+    if (!(dt >= c.dt_min)) return CLES_FAIL_DT_MIN;
+    if (c.dt_min_ratio > 0 && dt_seen > 0)
+        if (!(dt >= c.dt_min_ratio * dt_seen)) return CLES_FAIL_DT_COLLAPSE;
+    return CLES_FAIL_NONE;
+}
+
+std::unique_ptr<SolverBase> make_solver(cles_ctx* ctx, const cles_solver_desc& desc) {
+    if (desc.precision == CLES_PREC_MIXED) return std::unique_ptr<SolverBase>(new Solver<float>(ctx, desc));
+    if (desc.precision != CLES_PREC_FP64) throw Error(CLES_EINVAL, "unknown precision mode");
+    return std::unique_ptr<SolverBase>(new Solver<double>(ctx, desc));
+}
+
+namespace {
+void copy3d(double* dst, const double* src, const int n[3], const int pad[3], int ncomp, int layout, bool h2d,
+            cudaStream_t st) {
+    const int64_t cells = (int64_t)n[0] * n[1] * n[2];
+    if (layout == CLES_LAYOUT_INTERIOR) {
+        CLES_CUDA(cudaMemcpyAsync(dst, src, sizeof(double) * cells * ncomp,
+                                  h2d ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToHost, st));
+        return;
+    }
+    if (layout != CLES_LAYOUT_PADDED) throw Error(CLES_EINVAL, "unknown layout");
+    const int F0 = n[0] + 2 * pad[0], F1 = n[1] + 2 * pad[1], F2 = n[2] + 2 * pad[2];
+    const int64_t fcells = (int64_t)F0 * F1 * F2;
+    for (int c = 0; c < ncomp; ++c) {
+        cudaMemcpy3DParms p;
+        std::memset(&p, 0, sizeof(p));
+        if (h2d) {
+            p.srcPtr = make_cudaPitchedPtr(const_cast<double*>(src) + fcells * c, sizeof(double) * F0, F0, F1);
+            p.srcPos = make_cudaPos(sizeof(double) * pad[0], pad[1], pad[2]);
+            p.dstPtr = make_cudaPitchedPtr(dst + cells * c, sizeof(double) * n[0], n[0], n[1]);
+            p.kind = cudaMemcpyHostToDevice;
+        } else {
+            p.srcPtr = make_cudaPitchedPtr(const_cast<double*>(src) + cells * c, sizeof(double) * n[0], n[0], n[1]);
+            p.dstPtr = make_cudaPitchedPtr(dst + fcells * c, sizeof(double) * F0, F0, F1);
+            p.dstPos = make_cudaPos(sizeof(double) * pad[0], pad[1], pad[2]);
+            p.kind = cudaMemcpyDeviceToHost;
+        }
+        p.extent = make_cudaExtent(sizeof(double) * n[0], n[1], n[2]);
+        CLES_CUDA(cudaMemcpy3DAsync(&p, st));
+    }
+}
+}  // namespace
+
+void copy_state_h2d(double* dev, const double* host, const int n[3], const int pad[3], int ncomp, int layout,
+                    cudaStream_t st) {
+    copy3d(dev, host, n, pad, ncomp, layout, true, st);
+}
+void copy_state_d2h(double* host, const double* dev, const int n[3], const int pad[3], int ncomp, int layout,
+                    cudaStream_t st) {
+    copy3d(host, dev, n, pad, ncomp, layout, false, st);
+}
+
+}  // namespace cles

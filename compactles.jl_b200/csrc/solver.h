@@ -1,0 +1,66 @@
+// Device-resident solver runtime (the B200 counterpart of the reference's
+// Solver + compute_rhs! + step! + max_rate + filter_state! + run!).
+#pragma once
+
+#include <memory>
+
+#include "pointwise.h"
+
+struct cles_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    size_t budget = 0;     // 0 = unlimited
+    size_t allocated = 0;
+};
+
+namespace cles {
+
+// Device allocation charged against the context's HBM budget.
+struct DevBuf {
+    cles_ctx* ctx = nullptr;
+    void* p = nullptr;
+    size_t bytes = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+    ~DevBuf() { release(); }
+    void alloc(cles_ctx* c, size_t b);
+    void release();
+    template <typename T> T* as() const { return reinterpret_cast<T*>(p); }
+};
+
+class SolverBase {
+public:
+    virtual ~SolverBase() = default;
+    virtual void apply_bcs() = 0;
+    virtual void max_rate(double* rate, double* rho_min) = 0;
+    virtual void compute_rhs(bool primitives_current) = 0;
+    virtual void step(double dt, bool prepared) = 0;
+    virtual void filter_state() = 0;
+    virtual int run(double tfinal, int64_t nmax, cles_run_result* res) = 0;
+    virtual void set_state(const double* Q, int layout) = 0;
+    virtual void get_state(double* Q, int layout) = 0;
+    virtual void get_rhs(double* dQ, int layout) = 0;
+    virtual void get_field(int which, double* host, int layout) = 0;
+    virtual double kinetic_energy() = 0;
+    virtual double dissipation_rate() = 0;
+    virtual double* state_device() = 0;
+    virtual cles_solver_info info() const = 0;
+
+    cles_solver_desc desc{};
+    double t = 0.0, tstage = 0.0, dt_prev = 0.0, rate_prev = 0.0, cfl = 0.5;
+    int64_t step_count = 0;
+};
+
+std::unique_ptr<SolverBase> make_solver(cles_ctx* ctx, const cles_solver_desc& desc);
+
+// Host layout transfer of a component-slowest state between a host array in
+// `layout` and an interior device array (cudaMemcpy3DAsync per component).
+void copy_state_h2d(double* dev, const double* host, const int n[3], const int pad[3], int ncomp, int layout,
+                    cudaStream_t st);
+void copy_state_d2h(double* host, const double* dev, const int n[3], const int pad[3], int ncomp, int layout,
+                    cudaStream_t st);
+
+int check_step(const cles_step_control& c, double dt, double rho_min, double dt_seen);
+
+}  // namespace cles

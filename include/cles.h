@@ -289,6 +289,21 @@ int  cles_run(cles_solver* s, double tfinal, int64_t nmax, cles_run_result* out)
 int  cles_step_host(cles_solver* s, double* Q_host, int layout, double tfinal,
                     cles_run_result* out);
 
+/* Measurement hook (no counterpart in the reference): while enabled, every
+ * compact-operator launch is bracketed by CUDA events on its stream and its
+ * algorithmic bytes (input read once, output written once, plus the output
+ * read for accumulating stores) are recorded.  Enabling clears the records;
+ * cles_profile_read synchronises and returns one entry per direction
+ * ("compact_x", "compact_y", "compact_z"). */
+typedef struct cles_profile_entry {
+    char    name[32];
+    int64_t launches;
+    double  total_ms;
+    double  bytes;
+} cles_profile_entry;
+int  cles_profile_enable(int on);
+int  cles_profile_read(cles_profile_entry* out, int max_entries, int* n_entries);
+
 /* Volume-averaged kinetic energy ∫½ρ|u|²dV / V and dissipation rate
  * (src/diagnostics.jl:354-378, bench/tgv_energy.jl:175-184) of the resident
  * state. */
