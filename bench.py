@@ -296,9 +296,10 @@ def run_ours(a):
         achieved = tot_b / (tot_ms / 1e3) / 1e9
         peak = float(peaks.get("hbm_gbs", 6650.0))
         traffic = ncu_traffic()
+        per_launch = tot_b / nl
         out["roofline"] = {"bound": "hbm", "kernel": "k_compact (all directions)", "achieved": achieved,
                            "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_source": src,
-                           "traffic": (traffic or {}).get("traffic_per_launch"),
+                           "traffic": (traffic["traffic_ratio"] * per_launch) if traffic else None,
                            "traffic_note": (traffic or {}).get("note"),
                            "algorithmic_bytes_per_launch": tot_b / nl, "avg_launch_ms": tot_ms / nl,
                            "launches": nl, "share_of_step": tot_ms / r["ms"],

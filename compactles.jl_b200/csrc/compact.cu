@@ -37,30 +37,56 @@ struct LineMap {
     int64_t stride;    // element stride along the line
 };
 
-__device__ __forceinline__ LineMap line_map(const CompactParams& P, const FieldView& v, int64_t line) {
+__device__ __forceinline__ LineMap line_map(const CompactParams& P, const FieldView& v, int line) {
+    // lines < 2^31 (checked at plan time), so 32-bit division suffices
     LineMap L;
     if (P.dim == 0) {
-        const int64_t j = line % P.ny, k = line / P.ny;
+        const int j = line % P.ny, k = line / P.ny;
         L.base = j * v.sy + k * v.sz;
         L.stride = 1;
     } else if (P.dim == 1) {
-        const int64_t i = line % P.nx, k = line / P.nx;
+        const int i = line % P.nx, k = line / P.nx;
         L.base = i + k * v.sz;
         L.stride = v.sy;
     } else {
-        const int64_t i = line % P.nx, j = line / P.nx;
+        const int i = line % P.nx, j = line / P.nx;
         L.base = i + j * v.sy;
         L.stride = v.sz;
     }
     return L;
 }
 
+// g in [-n, 2n): periodic wrap without a division; closed lines clamp (the
+// clamped values are never used by a closure row).
 __device__ __forceinline__ int wrap_index(int g, int n, bool periodic) {
-    if (periodic) {
-        g %= n;
-        return g < 0 ? g + n : g;
-    }
+    if (periodic) return g < 0 ? g + n : (g >= n ? g - n : g);
     return g < 0 ? 0 : (g >= n ? n - 1 : g);
+}
+
+// Cooperative copy between the CTA's x lines (contiguous rows in global
+// memory) and the transposed tile: up to 32 threads per row, coalesced.
+template <typename T, bool LOAD>
+__device__ __forceinline__ void tile_rows(const CompactParams& P, const FieldView& v, T* g_field, T* tile, int line0,
+                                          int nl, int n, int TP, int mode) {
+    const int nt = blockDim.x;
+    const int tpr = nt < 32 ? nt : 32;
+    const int rows_per_pass = nt / tpr;
+    const int r = threadIdx.x / tpr, c = threadIdx.x - (threadIdx.x / tpr) * tpr;
+    if (r >= rows_per_pass) return;
+    for (int l = r; l < nl; l += rows_per_pass) {
+        const LineMap Ll = line_map(P, v, line0 + l);
+        T* row = g_field + Ll.base;
+        if (LOAD) {
+            for (int g = c; g < n; g += tpr) tile[g * TP + l] = row[g];
+        } else {
+            for (int g = c; g < n; g += tpr) {
+                const T val = tile[g * TP + l];
+                if (mode == OUT_STORE) row[g] = val;
+                else if (mode == OUT_NEGATE) row[g] = -val;
+                else row[g] = row[g] - val;
+            }
+        }
+    }
 }
 
 template <typename T, int Q, int M, bool XMODE>
@@ -71,8 +97,8 @@ __global__ void __launch_bounds__(512) k_compact(const CompactParams P, const T*
     const int LB = P.LB, S = P.S, n = P.n;
     const int lane = threadIdx.x % LB;
     const int seg = threadIdx.x / LB;
-    const int64_t line0 = (int64_t)blockIdx.x * LB;
-    const int64_t line = line0 + lane;
+    const int line0 = blockIdx.x * LB;
+    const int line = line0 + lane;
     const bool valid = line < P.lines;
     const int comp = blockIdx.y;
     const T* __restrict__ fin = reinterpret_cast<const T*>(in.base) + (int64_t)comp * in.comp_stride;
@@ -89,15 +115,9 @@ __global__ void __launch_bounds__(512) k_compact(const CompactParams P, const T*
     LineMap Lout = line_map(P, out, valid ? line : line0);
 
     // ---- 1. gather --------------------------------------------------------
+    const int nl = (int)((int64_t)LB < P.lines - line0 ? (int64_t)LB : P.lines - line0);
     if (XMODE) {
-        // coalesced row loads into the transposed tile tile[g][lane]
-        const int nl = (int)((int64_t)LB < P.lines - line0 ? (int64_t)LB : P.lines - line0);
-        const int total = nl * n;
-        for (int idx = threadIdx.x; idx < total; idx += blockDim.x) {
-            const int l = idx / n, g = idx - l * n;
-            const LineMap Ll = line_map(P, in, line0 + l);
-            tile[(size_t)g * TP + l] = fin[Ll.base + g];
-        }
+        tile_rows<T, true>(P, in, const_cast<T*>(fin), tile, line0, nl, n, TP, 0);
         __syncthreads();
     }
     constexpr int WN = kMaxSeg + 2 * M;
@@ -106,14 +126,14 @@ __global__ void __launch_bounds__(512) k_compact(const CompactParams P, const T*
     for (int j = 0; j < WN; ++j) {
         if (j < m + 2 * M) {
             const int g = wrap_index(off - M + j, n, periodic);
-            if (XMODE) w[j] = tile[(size_t)g * TP + lane];
+            if (XMODE) w[j] = tile[g * TP + lane];
             else w[j] = valid ? fin[Lin.base + (int64_t)g * Lin.stride] : T(0);
         } else {
             w[j] = T(0);
         }
     }
     auto ld = [&](int g) -> T {
-        if (XMODE) return tile[(size_t)g * TP + lane];
+        if (XMODE) return tile[g * TP + lane];
         return valid ? fin[Lin.base + (int64_t)g * Lin.stride] : T(0);
     };
 
@@ -250,19 +270,9 @@ __global__ void __launch_bounds__(512) k_compact(const CompactParams P, const T*
         __syncthreads();  // every window/closure read of the tile is done
 #pragma unroll
         for (int i = 0; i < kMaxSeg; ++i)
-            if (i < m) tile[(size_t)(off + i) * TP + lane] = y[i];
+            if (i < m) tile[(off + i) * TP + lane] = y[i];
         __syncthreads();
-        const int nl = (int)((int64_t)LB < P.lines - line0 ? (int64_t)LB : P.lines - line0);
-        const int total = nl * n;
-        for (int idx = threadIdx.x; idx < total; idx += blockDim.x) {
-            const int l = idx / n, g = idx - l * n;
-            const LineMap Ll = line_map(P, out, line0 + l);
-            const T v = tile[(size_t)g * TP + l];
-            T* o = fout + Ll.base + g;
-            if (mode == OUT_STORE) *o = v;
-            else if (mode == OUT_NEGATE) *o = -v;
-            else *o = *o - v;
-        }
+        tile_rows<T, false>(P, out, fout, tile, line0, nl, n, TP, mode);
     } else {
         // In place (out == in) is safe: with S > 1 the interface barrier
         // separates every window read of a line from its stores, with S = 1 a

@@ -151,6 +151,7 @@ void build_compact_plan(CompactPlan& plan, const cles_scheme& s, const int n3[3]
     P.nc = nc;
     P.lines = 1;
     for (int k = 0; k < 3; ++k) if (k != dim) P.lines *= n3[k];
+    if (P.lines >= (int64_t)1 << 31) throw Error(CLES_EINVAL, "too many lines for one plan (2^31)");
 
     // RHS coefficients prescaled by 1/h (derivatives) and the high-edge sign
     // (src/operators.jl:87-92).

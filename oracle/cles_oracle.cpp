@@ -1310,6 +1310,14 @@ int orc_get_field(orc_solver* so, int which, double* out) {
     return 0;
 }
 
+// flux[d][c] of the last compute_rhs (padded field), for parity scales.
+int orc_get_flux(orc_solver* so, int d, int c, double* out) {
+    Solver& S = *so->s;
+    if (d < 0 || d > 2 || c < 0 || c >= S.ncons) { set_err("bad flux index"); return CLES_EINVAL; }
+    std::memcpy(out, S.flux[d][c].data(), sizeof(double) * S.fs);
+    return 0;
+}
+
 int orc_check_step(const cles_step_control* c, double dt, double rho_min, double dt_seen) {
     return check_step(*c, dt, rho_min, dt_seen);
 }

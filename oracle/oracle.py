@@ -84,6 +84,7 @@ def lib():
         L.orc_get_clock.argtypes = [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_int64), C.POINTER(C.c_double)]
         L.orc_set_clock.argtypes = [C.c_void_p, C.c_double, C.c_int64, C.c_double]
         L.orc_get_field.argtypes = [C.c_void_p, C.c_int, _DP]
+        L.orc_get_flux.argtypes = [C.c_void_p, C.c_int, C.c_int, _DP]
         L.orc_check_step.argtypes = [C.POINTER(abi.cles_step_control), C.c_double, C.c_double, C.c_double]
         _lib = L
     return _lib
@@ -246,6 +247,26 @@ class Solver:
         rc = lib().orc_get_field(self.ptr, int(which), out)
         if rc:
             raise ValueError(_err())
+        return out
+
+    def flux(self, d, c):
+        """flux[d][c] (0-based) of the last compute_rhs, padded."""
+        out = np.zeros(self.field_shape)
+        if lib().orc_get_flux(self.ptr, int(d), int(c), out):
+            raise ValueError(_err())
+        return out
+
+    def rhs_scales(self, h):
+        """Per conserved component, max over dims and points of |F_dc| / h_d: the size of
+        the directional flux-divergence terms whose sum is the RHS."""
+        sl = interior(self.g, np.zeros(self.field_shape))
+        out = []
+        for c in range(self.n_cons):
+            m = 0.0
+            for d in range(3):
+                if self.desc.n_global[d] > 1:
+                    m = max(m, float(np.abs(interior(self.g, self.flux(d, c))).max()) / h[d])
+            out.append(m)
         return out
 
     def clock(self):

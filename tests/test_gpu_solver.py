@@ -1,11 +1,15 @@
 """GPU parity of the solver path (cles_compute_rhs / cles_step / cles_run
 through the C ABI) against the CPU oracle on identical initial states.
 
-Bounds (the FP64 drop-in's contract): per RHS, the max error of every
-conserved component relative to that component's largest value is at most
-1e-12 (components whose RHS is round-off noise, below 1e-9 of the largest
-component, are held absolutely to 1e-12 of the largest); after 100 steps the
-relative L2 difference of the state is at most 1e-10."""
+Bounds (the FP64 drop-in's contract):
+* per RHS, every conserved component c: max_points |dQ_gpu - dQ_oracle| is at
+  most 1e-12 of that component's RHS scale, max(max|dQ_c|, max_d max|F_dc|/h_d).
+  The second term is the size of the directional flux-divergence terms that
+  are summed into dQ_c; it matters where they cancel (the energy equation of
+  the Taylor-Green box sums terms of size ~250/h into an O(1) result, so an
+  error of a few ulp of the terms is 1e-12 of the result);
+* after 100 steps, the relative L2 difference of the state is at most 1e-10.
+"""
 import numpy as np
 import pytest
 
@@ -17,15 +21,13 @@ from compactles_b200 import abi
 pytestmark = pytest.mark.gpu
 
 
-def rhs_errors(a, b, interior):
+def rhs_errors(a, b, interior, scales=None):
     a = interior(a)
     b = interior(b)
-    top = max(np.abs(b[c]).max() for c in range(b.shape[0]))
     errs = []
     for c in range(b.shape[0]):
-        mc = np.abs(b[c]).max()
-        d = np.abs(a[c] - b[c]).max()
-        errs.append(d / mc if mc > 1e-9 * top else d / top)
+        sc = max(np.abs(b[c]).max(), scales[c] if scales else 0.0)
+        errs.append(np.abs(a[c] - b[c]).max() / sc if sc > 0 else np.abs(a[c] - b[c]).max())
     return errs
 
 
@@ -53,7 +55,8 @@ def _interior(desc):
 def test_tgv_rhs_parity(orc, n):
     pair, Q0, _ = descs(orc, cases.taylor_green, n=n)
     S, O = both(orc, pair, Q0)
-    errs = rhs_errors(S.compute_rhs(), O.compute_rhs(), _interior(pair[0]))
+    dQo = O.compute_rhs()
+    errs = rhs_errors(S.compute_rhs(), dQo, _interior(pair[0]), O.rhs_scales(cl.grid_spacing(pair[0])))
     assert max(errs) < 1e-12, errs
 
 
@@ -86,7 +89,8 @@ def test_rhs_parity_variants(orc, variant):
     S, O = both(orc, (dg, do), Q0)
     S.apply_bcs()
     O.apply_bcs()
-    errs = rhs_errors(S.compute_rhs(), O.compute_rhs(), _interior(dg))
+    dQo = O.compute_rhs()
+    errs = rhs_errors(S.compute_rhs(), dQo, _interior(dg), O.rhs_scales(cl.grid_spacing(dg)))
     assert max(errs) < 1e-12, errs
     # the artificial coefficients themselves
     for which in (abi.CLES_FIELD_MU_ART, abi.CLES_FIELD_BETA_ART, abi.CLES_FIELD_KAPPA_ART):
@@ -206,5 +210,7 @@ def test_mixed_precision_rhs_close(orc):
     dg = pair[0]
     dg.precision = abi.CLES_PREC_MIXED
     S, O = both(orc, (dg, pair[1]), Q0)
-    errs = rhs_errors(S.compute_rhs(), O.compute_rhs(), _interior(dg))
-    assert max(errs) < 1e-4, errs
+    dQo = O.compute_rhs()
+    errs = rhs_errors(S.compute_rhs(), dQo, _interior(dg), O.rhs_scales(cl.grid_spacing(dg)))
+    # FP32 fields and line solves: a few single-precision ulps of the terms
+    assert max(errs) < 2e-6, errs
