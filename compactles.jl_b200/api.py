@@ -91,6 +91,8 @@ def lib():
         L.cles_step_host.argtypes = [vp, vp, C.c_int, C.c_double, C.POINTER(abi.cles_run_result)]
         L.cles_profile_enable.argtypes = [C.c_int]
         L.cles_profile_read.argtypes = [C.POINTER(abi.cles_profile_entry), C.c_int, C.POINTER(C.c_int)]
+        L.cles_max_rate_static.argtypes = [vp, vp, C.c_int64, C.c_int, dp, dp, dp, C.c_double, C.c_double,
+                                           C.c_double, vp, vp]
         L.cles_kinetic_energy.argtypes = [vp, dp]
         L.cles_dissipation_rate.argtypes = [vp, dp]
         _lib = L

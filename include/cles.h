@@ -289,6 +289,28 @@ int  cles_run(cles_solver* s, double tfinal, int64_t nmax, cles_run_result* out)
 int  cles_step_host(cles_solver* s, double* Q_host, int layout, double tfinal,
                     cles_run_result* out);
 
+/* Allocation-free CFL rate reduction (no counterpart in the reference).
+ * For callers that cannot call cudaMalloc -- code inside a host framework
+ * that owns every device allocation, a plugin barred from allocating after
+ * start-up, or a process held to a fixed HBM budget.  Computes what
+ * cles_max_rate computes (the rate max of src/timestep.jl:125-175 and the
+ * minimum mixture density) from caller-owned device arrays, keeping its
+ * per-block partials in a library-owned static device array instead of
+ * allocating:
+ *   Q_dev      conserved state, interior layout, component slowest (n_species+4 fields of `cells`)
+ *   art_dev    mu*, beta*, kappa*, D*_1..D*_Ns (3+n_species fields of `cells`)
+ *   inv_h      1/h per dimension, 0 for a collapsed one
+ *   result_dev two doubles written on the device: rate, rho_min
+ * At most CLES_STATIC_MAX_CELLS cells per call (larger grids: CLES_EINVAL).
+ * All calls on a device share the static array, so calls that overlap on the
+ * GPU race; order them on one stream.  The first call on a device resolves the
+ * array's address (cudaGetSymbolAddress) and should come before any stream
+ * capture.  Work is queued on `stream` (NULL = legacy default stream). */
+#define CLES_STATIC_MAX_CELLS 33554432LL
+int  cles_max_rate_static(const double* Q_dev, const double* art_dev, int64_t cells, int n_species,
+                          const double* R, const double* gamma, const double* inv_h, double mu0, double Pr,
+                          double Sc, double* result_dev, void* stream);
+
 /* Measurement hook (no counterpart in the reference): while enabled, every
  * compact-operator launch is bracketed by CUDA events on its stream and its
  * algorithmic bytes (input read once, output written once, plus the output
