@@ -72,8 +72,38 @@ struct CompactParams {
     int64_t lines;
 };
 
+// Warp-per-line form for periodic tridiagonal x lines of n = 32 * XP points:
+// lane s owns the XP contiguous points [s*XP, (s+1)*XP).  Every lane segment
+// is the same Toeplitz block, so the local factorisation, the spikes and the
+// parallel-cyclic-reduction matrices of the 32-segment interface system are
+// line- and lane-independent and travel as kernel parameters.
+constexpr int kMaxXP = 16;
+struct WarpLineParams {
+    int XP;                                   // points per lane: 4, 8 or 16
+    double l[kMaxXP], dinv[kMaxXP], c[kMaxXP];  // segment Thomas factors
+    double v[kMaxXP], w[kMaxXP];              // spikes: couplings to the previous tail / next head
+    double alpha[4][4], gamma[4][4];          // PCR steps at distances 1, 2, 4, 8 (2x2, row-major)
+    double alpha_f[4], binv_f[4];             // pairing at distance 16, then the 2x2 solve
+    float lf[kMaxXP], dinvf[kMaxXP], cf[kMaxXP], vf[kMaxXP], wf[kMaxXP];
+    float alphaf[4][4], gammaf[4][4], alpha_ff[4], binv_ff[4];
+};
+
+// TMA-pipelined form for periodic tridiagonal y/z lines with equal segments
+// (n = S * m, m <= 32, n <= 256): every segment has the same factorisation and
+// spikes, which travel as kernel parameters; the reduced inverse stays in the
+// table (copied to shared memory once per persistent CTA).
+struct TileLineParams {
+    int m;
+    double l[kMaxSeg], dinv[kMaxSeg], c[kMaxSeg], v[kMaxSeg], w[kMaxSeg];
+    float lf[kMaxSeg], dinvf[kMaxSeg], cf[kMaxSeg], vf[kMaxSeg], wf[kMaxSeg];
+};
+
 // Host-side plan: parameters plus the coefficient tables on the device.
 struct CompactPlan {
+    bool has_tl = false;
+    TileLineParams TL;
+    bool has_xw = false;
+    WarpLineParams XW;
     CompactParams P;
     int dtype = CLES_F64;
     double* tab64 = nullptr;
@@ -87,8 +117,27 @@ struct CompactPlan {
 void build_compact_plan(CompactPlan& plan, const cles_scheme& scheme, const int n3[3], int dim,
                         bool periodic, double h, int dtype);
 
-// Output modes of the compact operator.
-enum { OUT_STORE = 0, OUT_NEGATE = 1, OUT_SUBTRACT = 2 };
+// Output modes of the compact operator.  OUT_RK finishes the flux divergence
+// and applies the low-storage RK update in the store (see launch_compact_rk).
+enum { OUT_STORE = 0, OUT_NEGATE = 1, OUT_SUBTRACT = 2, OUT_RK = 3 };
+
+// Low-storage RK epilogue: with dq = out - D(f), v = A du + dt dq; du = v;
+// Q += B v (src/timestep.jl:86-95).  Q and du share the layout of `out`.
+struct RkEpilogue {
+    double* Q;
+    double* du;
+    double A, B, dt;
+};
+
+// TMA-pipelined y/z launch; false when the plan or the views do not qualify.
+bool try_launch_tma(const CompactPlan& plan, const FieldView& in, const FieldView& out, int count, int mode,
+                    cudaStream_t st, const RkEpilogue* rk = nullptr);
+// Flux divergence of the last direction fused with the RK update; false (and
+// nothing launched) when the plan does not take the TMA path.
+bool launch_compact_rk(const CompactPlan& plan, const FieldView& in, const FieldView& out, int count,
+                       const RkEpilogue& rk, cudaStream_t st);
+// Bounded-wait timeouts recorded by device kernels since the last call (cleared).
+int take_device_timeouts(cudaStream_t st);
 
 // Launch the operator over `count` fields of `in` into `out` (may alias).
 void launch_compact(const CompactPlan& plan, const FieldView& in, const FieldView& out, int count, int mode,

@@ -290,6 +290,158 @@ __global__ void __launch_bounds__(512) k_compact(const CompactParams P, const T*
     }
 }
 
+// ---------------------------------------------------------------------------
+// Warp-per-line kernel for periodic tridiagonal x lines of n = 32 * XP points.
+// Lane s of a warp owns the XP contiguous points [s*XP, (s+1)*XP) of one line:
+// vector loads and stores straight from/to global memory (the warp covers the
+// whole contiguous line), stencil halos from the neighbouring lanes by shuffle,
+// the lane's Thomas sweep in registers, and the 32-segment interface system by
+// parallel cyclic reduction across the lanes with precomputed 2x2 matrices.
+template <typename T> struct Vec;
+template <> struct Vec<double> { using type = double2; static constexpr int W = 2; };
+template <> struct Vec<float> { using type = float4; static constexpr int W = 4; };
+
+template <typename T>
+__device__ __forceinline__ T wl(const double* d, const float* f, int i) {
+    if (sizeof(T) == 8) return T(d[i]);
+    return T(f[i]);
+}
+
+template <typename T, int M, int XP>
+__global__ void __launch_bounds__(256) k_compact_xw(const __grid_constant__ CompactParams P, const __grid_constant__ WarpLineParams W, const FieldView in,
+                                                    const FieldView out, const int mode) {
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const int line = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (line >= P.lines) return;  // whole warps leave together; no block barrier below
+    const int comp = blockIdx.y;
+    const int j = line % P.ny, k = line / P.ny;
+    const T* src = reinterpret_cast<const T*>(in.base) + (int64_t)comp * in.comp_stride + j * in.sy + k * in.sz + lane * XP;
+    T* dst = reinterpret_cast<T*>(out.base) + (int64_t)comp * out.comp_stride + j * out.sy + k * out.sz + lane * XP;
+    using V = typename Vec<T>::type;
+    constexpr int VW = Vec<T>::W;
+    T f[XP];
+#pragma unroll
+    for (int q = 0; q < XP / VW; ++q) {
+        const V v = __ldg(reinterpret_cast<const V*>(src) + q);
+        const T* pv = reinterpret_cast<const T*>(&v);
+#pragma unroll
+        for (int e = 0; e < VW; ++e) f[q * VW + e] = pv[e];
+    }
+    const int lm = (lane + 31) & 31, lp = (lane + 1) & 31;
+    T wv[XP + 2 * M];
+#pragma unroll
+    for (int q = 0; q < M; ++q) {
+        wv[q] = __shfl_sync(FULL, f[XP - M + q], lm);
+        wv[M + XP + q] = __shfl_sync(FULL, f[q], lp);
+    }
+#pragma unroll
+    for (int i = 0; i < XP; ++i) wv[M + i] = f[i];
+    // fill (src/operators.jl:155-172 interior rows)
+    T y[XP];
+    const T a0 = T(P.a0);
+#pragma unroll
+    for (int i = 0; i < XP; ++i) {
+        T acc;
+        if (P.symmetric) {
+            acc = a0 * wv[i + M];
+#pragma unroll
+            for (int m = 1; m <= M; ++m) acc += T(P.ci[m - 1]) * (wv[i + M + m] + wv[i + M - m]);
+        } else {
+            acc = T(0);
+#pragma unroll
+            for (int m = 1; m <= M; ++m) acc += T(P.ci[m - 1]) * (wv[i + M + m] - wv[i + M - m]);
+        }
+        y[i] = acc;
+    }
+    // lane-local Thomas sweep (src/tridiag.jl:46-57)
+#pragma unroll
+    for (int i = 1; i < XP; ++i) y[i] -= wl<T>(W.l, W.lf, i) * y[i - 1];
+    y[XP - 1] *= wl<T>(W.dinv, W.dinvf, XP - 1);
+#pragma unroll
+    for (int i = XP - 2; i >= 0; --i) y[i] = (y[i] - wl<T>(W.c, W.cf, i) * y[i + 1]) * wl<T>(W.dinv, W.dinvf, i);
+    // interface values: parallel cyclic reduction over the 32 lanes
+    T h = y[0], t = y[XP - 1];
+#pragma unroll
+    for (int s = 0; s < 4; ++s) {
+        const int d = 1 << s;
+        const T mh = __shfl_sync(FULL, h, (lane - d) & 31), mt = __shfl_sync(FULL, t, (lane - d) & 31);
+        const T ph = __shfl_sync(FULL, h, (lane + d) & 31), pt = __shfl_sync(FULL, t, (lane + d) & 31);
+        const T* al = nullptr;
+        (void)al;
+        const T nh = h + wl<T>(W.alpha[s], W.alphaf[s], 0) * mh + wl<T>(W.alpha[s], W.alphaf[s], 1) * mt +
+                     wl<T>(W.gamma[s], W.gammaf[s], 0) * ph + wl<T>(W.gamma[s], W.gammaf[s], 1) * pt;
+        const T nt = t + wl<T>(W.alpha[s], W.alphaf[s], 2) * mh + wl<T>(W.alpha[s], W.alphaf[s], 3) * mt +
+                     wl<T>(W.gamma[s], W.gammaf[s], 2) * ph + wl<T>(W.gamma[s], W.gammaf[s], 3) * pt;
+        h = nh;
+        t = nt;
+    }
+    {
+        const T oh = __shfl_sync(FULL, h, (lane + 16) & 31), ot = __shfl_sync(FULL, t, (lane + 16) & 31);
+        const T rh = h + wl<T>(W.alpha_f, W.alpha_ff, 0) * oh + wl<T>(W.alpha_f, W.alpha_ff, 1) * ot;
+        const T rt = t + wl<T>(W.alpha_f, W.alpha_ff, 2) * oh + wl<T>(W.alpha_f, W.alpha_ff, 3) * ot;
+        h = wl<T>(W.binv_f, W.binv_ff, 0) * rh + wl<T>(W.binv_f, W.binv_ff, 1) * rt;
+        t = wl<T>(W.binv_f, W.binv_ff, 2) * rh + wl<T>(W.binv_f, W.binv_ff, 3) * rt;
+    }
+    const T tprev = __shfl_sync(FULL, t, lm);
+    const T hnext = __shfl_sync(FULL, h, lp);
+#pragma unroll
+    for (int i = 0; i < XP; ++i) y[i] -= wl<T>(W.v, W.vf, i) * tprev + wl<T>(W.w, W.wf, i) * hnext;
+    // store
+#pragma unroll
+    for (int q = 0; q < XP / VW; ++q) {
+        V v;
+        T* pv = reinterpret_cast<T*>(&v);
+        if (mode == OUT_SUBTRACT) {
+            const V o = *(reinterpret_cast<const V*>(dst) + q);
+            const T* po = reinterpret_cast<const T*>(&o);
+#pragma unroll
+            for (int e = 0; e < VW; ++e) pv[e] = po[e] - y[q * VW + e];
+        } else if (mode == OUT_NEGATE) {
+#pragma unroll
+            for (int e = 0; e < VW; ++e) pv[e] = -y[q * VW + e];
+        } else {
+#pragma unroll
+            for (int e = 0; e < VW; ++e) pv[e] = y[q * VW + e];
+        }
+        reinterpret_cast<V*>(dst)[q] = v;
+    }
+}
+
+template <typename T, int M>
+void launch_xw_m(const CompactPlan& plan, const FieldView& in, const FieldView& out, int count, int mode,
+                 cudaStream_t st) {
+    const int lines_per_cta = 8;
+    dim3 grid((unsigned)((plan.P.lines + lines_per_cta - 1) / lines_per_cta), (unsigned)count);
+    switch (plan.XW.XP) {
+        case 4: k_compact_xw<T, M, 4><<<grid, 32 * lines_per_cta, 0, st>>>(plan.P, plan.XW, in, out, mode); break;
+        case 8: k_compact_xw<T, M, 8><<<grid, 32 * lines_per_cta, 0, st>>>(plan.P, plan.XW, in, out, mode); break;
+        case 16: k_compact_xw<T, M, 16><<<grid, 32 * lines_per_cta, 0, st>>>(plan.P, plan.XW, in, out, mode); break;
+        default: throw Error(CLES_EINVAL, "warp-line kernel: unsupported points per lane");
+    }
+    count_launch();
+    check_launch("k_compact_xw");
+}
+
+template <typename T>
+bool try_launch_xw(const CompactPlan& plan, const FieldView& in, const FieldView& out, int count, int mode,
+                   cudaStream_t st) {
+    if (!plan.has_xw) return false;
+    // vector accesses need 16-byte aligned rows
+    const size_t el = sizeof(T);
+    auto aligned = [&](const FieldView& v) {
+        return ((uintptr_t)v.base % 16 == 0) && ((v.sy * el) % 16 == 0) && ((v.sz * el) % 16 == 0) &&
+               ((v.comp_stride * el) % 16 == 0 || count == 1);
+    };
+    if (!aligned(in) || !aligned(out)) return false;
+    switch (plan.P.M) {
+        case 1: launch_xw_m<T, 1>(plan, in, out, count, mode, st); return true;
+        case 2: launch_xw_m<T, 2>(plan, in, out, count, mode, st); return true;
+        case 4: launch_xw_m<T, 4>(plan, in, out, count, mode, st); return true;
+        default: return false;
+    }
+}
+
 template <typename T, int Q, int M, bool X>
 void launch_t(const CompactParams& P, const T* tab, const FieldView& in, const FieldView& out, int count, int mode,
               cudaStream_t st) {
@@ -346,8 +498,13 @@ void launch_compact(const CompactPlan& plan, const FieldView& in, const FieldVie
         const double pts = (double)plan.P.lines * plan.P.n * count;
         rec = prof_begin(st, plan.P.dim, pts * el * (mode == OUT_SUBTRACT ? 3.0 : 2.0));
     }
-    if (plan.dtype == CLES_F64) dispatch<double>(plan.P, plan.tab64, in, out, count, mode, st);
-    else dispatch<float>(plan.P, plan.tab32, in, out, count, mode, st);
+    if (plan.dtype == CLES_F64) {
+        if (!try_launch_xw<double>(plan, in, out, count, mode, st) && !try_launch_tma(plan, in, out, count, mode, st))
+            dispatch<double>(plan.P, plan.tab64, in, out, count, mode, st);
+    } else {
+        if (!try_launch_xw<float>(plan, in, out, count, mode, st) && !try_launch_tma(plan, in, out, count, mode, st))
+            dispatch<float>(plan.P, plan.tab32, in, out, count, mode, st);
+    }
     if (rec >= 0) prof_end(rec, st);
 }
 

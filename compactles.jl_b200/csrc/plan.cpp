@@ -117,6 +117,85 @@ struct LocalFactor {
     }
 };
 
+void mat2_mul(const double* a, const double* b, double* o) {  // o = a b (2x2 row-major)
+    const double t0 = a[0] * b[0] + a[1] * b[2], t1 = a[0] * b[1] + a[1] * b[3];
+    const double t2 = a[2] * b[0] + a[3] * b[2], t3 = a[2] * b[1] + a[3] * b[3];
+    o[0] = t0; o[1] = t1; o[2] = t2; o[3] = t3;
+}
+void mat2_inv(const double* a, double* o) {
+    const double det = a[0] * a[3] - a[1] * a[2];
+    if (det == 0.0) throw Error(CLES_EINVAL, "singular 2x2 block in the interface reduction");
+    const double t0 = a[3] / det, t1 = -a[1] / det, t2 = -a[2] / det, t3 = a[0] / det;
+    o[0] = t0; o[1] = t1; o[2] = t2; o[3] = t3;
+}
+
+// Warp-per-line parameters (periodic, q = 1, n = 32 * XP).  The interface
+// system of the 32 lane segments is block tridiagonal and cyclic in
+// X_s = (head_s, tail_s):  A X_{s-1} + X_s + C X_{s+1} = (y_s[0], y_s[XP-1]),
+// A = [[0, v_0], [0, v_{XP-1}]], C = [[w_0, 0], [w_{XP-1}, 0]].  Parallel cyclic
+// reduction at distances 1, 2, 4, 8 makes every equation couple only to the
+// lane 16 away, which in a 32-cycle is the same unknown on both sides; the
+// final pairing then leaves a 2x2 system per lane.  Every matrix is the same
+// for all lanes, so they are computed here once.
+void build_warp_line(CompactPlan& plan, const Band& B, const cles_scheme& s, int n, int dim, bool periodic) {
+    plan.has_xw = false;
+    if (dim != 0 || !periodic || s.q != 1 || n % 32 != 0) return;
+    const int XP = n / 32;
+    if (XP != 4 && XP != 8 && XP != 16) return;
+    if (XP < s.M) return;
+    WarpLineParams& W = plan.XW;
+    std::memset(&W, 0, sizeof(W));
+    W.XP = XP;
+    // local factorisation of one lane segment (rows 0..XP-1 of the Toeplitz band)
+    LocalFactor F;
+    F.build(B, 0, XP);
+    for (int i = 0; i < XP; ++i) {
+        W.l[i] = i > 0 ? F.L[(size_t)i - 1] : 0.0;
+        W.dinv[i] = 1.0 / F.U[i];
+        W.c[i] = i < XP - 1 ? F.U[(size_t)XP + i] : 0.0;
+    }
+    std::vector<double> v(XP, 0.0), w(XP, 0.0);
+    v[0] = B.at(0, n - 1);            // row 0 couples to the previous segment's tail
+    w[XP - 1] = B.at(XP - 1, XP);     // row XP-1 couples to the next segment's head
+    F.solve(v.data());
+    F.solve(w.data());
+    for (int i = 0; i < XP; ++i) { W.v[i] = v[i]; W.w[i] = w[i]; }
+    double A[4] = {0.0, v[0], 0.0, v[XP - 1]};
+    double Bm[4] = {1.0, 0.0, 0.0, 1.0};
+    double Cm[4] = {w[0], 0.0, w[XP - 1], 0.0};
+    for (int k = 0; k < 4; ++k) {
+        double Bi[4], al[4], ga[4], t1[4], t2[4];
+        mat2_inv(Bm, Bi);
+        mat2_mul(A, Bi, al);
+        mat2_mul(Cm, Bi, ga);
+        for (int e = 0; e < 4; ++e) { al[e] = -al[e]; ga[e] = -ga[e]; }
+        double nA[4], nC[4], nB[4];
+        mat2_mul(al, A, nA);
+        mat2_mul(ga, Cm, nC);
+        mat2_mul(al, Cm, t1);
+        mat2_mul(ga, A, t2);
+        for (int e = 0; e < 4; ++e) nB[e] = Bm[e] + t1[e] + t2[e];
+        for (int e = 0; e < 4; ++e) { W.alpha[k][e] = al[e]; W.gamma[k][e] = ga[e]; A[e] = nA[e]; Bm[e] = nB[e]; Cm[e] = nC[e]; }
+    }
+    double E[4], Bi[4], af[4], t[4], Bf[4];
+    for (int e = 0; e < 4; ++e) E[e] = A[e] + Cm[e];
+    mat2_inv(Bm, Bi);
+    mat2_mul(E, Bi, af);
+    for (int e = 0; e < 4; ++e) af[e] = -af[e];
+    mat2_mul(af, E, t);
+    for (int e = 0; e < 4; ++e) Bf[e] = Bm[e] + t[e];
+    mat2_inv(Bf, W.binv_f);
+    for (int e = 0; e < 4; ++e) W.alpha_f[e] = af[e];
+    for (int i = 0; i < kMaxXP; ++i) {
+        W.lf[i] = (float)W.l[i]; W.dinvf[i] = (float)W.dinv[i]; W.cf[i] = (float)W.c[i];
+        W.vf[i] = (float)W.v[i]; W.wf[i] = (float)W.w[i];
+    }
+    for (int k = 0; k < 4; ++k)
+        for (int e = 0; e < 4; ++e) { W.alphaf[k][e] = (float)W.alpha[k][e]; W.gammaf[k][e] = (float)W.gamma[k][e]; }
+    for (int e = 0; e < 4; ++e) { W.alpha_ff[e] = (float)W.alpha_f[e]; W.binv_ff[e] = (float)W.binv_f[e]; }
+    plan.has_xw = true;
+}
+
 }  // namespace
 
 CompactPlan::~CompactPlan() {
@@ -313,6 +392,32 @@ void build_compact_plan(CompactPlan& plan, const cles_scheme& s, const int n3[3]
         }
         std::vector<double> G = dense_inverse(R, N);
         std::copy(G.begin(), G.end(), tab.begin() + P.off_G);
+    }
+
+    build_warp_line(plan, B, s, n, dim, periodic);
+    plan.has_tl = false;
+    if (q == 1 && periodic && dim > 0 && P.seg_rem == 0 && n <= 256 && P.LB == 32) {
+        TileLineParams& T = plan.TL;
+        std::memset(&T, 0, sizeof(T));
+        T.m = P.seg_base;
+        for (int i = 0; i < T.m; ++i) {
+            T.l[i] = tab[P.off_f0 + i];
+            T.dinv[i] = tab[P.off_f1 + i];
+            T.c[i] = tab[P.off_f2 + i];
+            T.v[i] = tab[P.off_V + i];
+            T.w[i] = tab[P.off_W + i];
+            T.lf[i] = (float)T.l[i]; T.dinvf[i] = (float)T.dinv[i]; T.cf[i] = (float)T.c[i];
+            T.vf[i] = (float)T.v[i]; T.wf[i] = (float)T.w[i];
+        }
+        // every segment of a periodic line with equal segments is the same block
+        bool same = true;
+        for (int sg = 1; sg < S && same; ++sg)
+            for (int i = 0; i < T.m; ++i) {
+                const size_t o = (size_t)sg * kMaxSeg + i;
+                same = same && tab[P.off_f0 + o] == T.l[i] && tab[P.off_f1 + o] == T.dinv[i] &&
+                       tab[P.off_f2 + o] == T.c[i] && tab[P.off_V + o] == T.v[i] && tab[P.off_W + o] == T.w[i];
+            }
+        plan.has_tl = same;
     }
 
     plan.dtype = dtype;

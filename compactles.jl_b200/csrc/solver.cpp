@@ -197,7 +197,10 @@ public:
         }
     }
 
-    void compute_rhs(bool primitives_current) override {
+    void compute_rhs(bool primitives_current) override { compute_rhs_impl(primitives_current, nullptr); }
+
+    // Returns true when `rk` was applied inside the last divergence launch.
+    bool compute_rhs_impl(bool primitives_current, const RkEpilogue* rk) {
         using PW = Pointwise<F>;
         if (!primitives_current) PW::primitives(Q_.as<double>(), prim_.as<F>(), cells_, Ns_, pc_, st_);
         // velocity gradients grad_u[d][j] (src/rhs.jl:596-603), one launch per dim for u, v, w
@@ -213,14 +216,22 @@ public:
         PW::fluxes(Q_.as<double>(), prim_.as<F>(), g_u_.as<F>(), gty_.as<F>(), art_.as<F>(), flux_.as<F>(), cells_, Ns_,
                    pc_, desc.mu0, desc.Pr, desc.Sc, st_);
         // flux divergence dQ[c] = -sum_d D_d(F_dc) (src/rhs.jl:650-668), accumulated in the store
-        bool first = true;
+        int last = -1;
+        for (int k = 0; k < 3; ++k)
+            if (g_.active[k]) last = k;
+        bool first = true, fused = false;
         for (int k = 0; k < 3; ++k) {
             if (!g_.active[k]) continue;
-            launch_compact(*deriv_[k], view(flux_.as<F>() + (size_t)cells_ * ncons_ * k), view(dQ_.as<F>()), ncons_,
-                           first ? OUT_NEGATE : OUT_SUBTRACT, st_);
+            const FieldView fin = view(flux_.as<F>() + (size_t)cells_ * ncons_ * k);
+            if (k == last && !first && rk && launch_compact_rk(*deriv_[k], fin, view(dQ_.as<F>()), ncons_, *rk, st_)) {
+                fused = true;
+            } else {
+                launch_compact(*deriv_[k], fin, view(dQ_.as<F>()), ncons_, first ? OUT_NEGATE : OUT_SUBTRACT, st_);
+            }
             first = false;
         }
         if (first) CLES_CUDA(cudaMemsetAsync(dQ_.p, 0, dQ_.bytes, st_));
+        return fused;
     }
 
     void step(double dt, bool prepared) override {
@@ -228,9 +239,12 @@ public:
             tstage = t + RKC[stage] * dt;
             const bool first_prepared = prepared && stage == 0;
             if (!first_prepared) apply_bcs();
-            compute_rhs(first_prepared);
-            Pointwise<F>::lsrk(Q_.as<double>(), du_.as<double>(), dQ_.as<F>(), cells_ * ncons_, RKA[stage], RKB[stage],
-                               dt, st_);
+            // the last flux-divergence direction applies the RK update in its
+            // store when its plan takes the TMA path; otherwise a separate pass
+            const RkEpilogue rk{Q_.as<double>(), du_.as<double>(), RKA[stage], RKB[stage], dt};
+            if (!compute_rhs_impl(first_prepared, &rk))
+                Pointwise<F>::lsrk(Q_.as<double>(), du_.as<double>(), dQ_.as<F>(), cells_ * ncons_, RKA[stage],
+                                   RKB[stage], dt, st_);
         }
         tstage = t + dt;
         apply_bcs();
@@ -245,6 +259,8 @@ public:
                            Ns_, idx, act, desc.mu0, desc.Pr, desc.Sc, st_);
         CLES_CUDA(cudaMemcpyAsync(host_res_, res_.p, 2 * sizeof(double), cudaMemcpyDeviceToHost, st_));
         CLES_CUDA(cudaStreamSynchronize(st_));
+        if (take_device_timeouts(st_))
+            throw Error(CLES_ETIMEOUT, "a bounded device wait expired in a compact-operator kernel");
         *rate = host_res_[0];
         *rho_min = host_res_[1];
     }
