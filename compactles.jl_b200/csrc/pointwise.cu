@@ -35,7 +35,8 @@ inline unsigned grid_for(int64_t n) {
 
 // _primitives!(::IdealMixture) (src/physics.jl:604-653) at the interior.
 template <typename F>
-__global__ void k_primitives(const double* __restrict__ Q, F* __restrict__ prim, int64_t cells, int Ns, PhysConst pc) {
+__global__ void k_primitives(const double* __restrict__ Q, F* __restrict__ prim, int64_t cells, int Ns, PhysConst pc,
+                             int esens) {
     GRID_STRIDE(I, cells) {
         double rho = 0.0;
         for (int sp = 0; sp < Ns; ++sp) rho += Q[I + cells * sp];
@@ -66,6 +67,13 @@ __global__ void k_primitives(const double* __restrict__ Q, F* __restrict__ prim,
             out[cells * P_T] = F(T);
             out[cells * P_C] = F(sqrt(gm * Rm * T));
             out[cells * P_CP] = F(cvm + Rm);
+            if (esens) {
+                // internal energy for the kappa* sensor (src/artificial.jl:322-330): rho floored, |m|^2/2rho
+                const double r = jl_max(rho, 1e-300);
+                const double q1 = Q[I + cells * (Ns + 0)], q2 = Q[I + cells * (Ns + 1)], q3 = Q[I + cells * (Ns + 2)];
+                const double ke = 0.5 * (q1 * q1 + q2 * q2 + q3 * q3) / r;
+                out[cells * (P_Y0 + Ns)] = F((Q[I + cells * (Ns + 3)] - ke) / r);
+            }
         } else {
             out[cells * P_RHO] = F(1);
             out[cells * P_U] = F(0);
@@ -76,6 +84,12 @@ __global__ void k_primitives(const double* __restrict__ Q, F* __restrict__ prim,
             out[cells * P_C] = F(1);
             out[cells * P_CP] = F(1);
             for (int sp = 0; sp < Ns; ++sp) out[cells * (P_Y0 + sp)] = F(sp == 0 ? 1.0 : 0.0);
+            if (esens) {
+                // placeholder density 1: the floor is max(1, 1e-300) = 1
+                const double q1 = Q[I + cells * (Ns + 0)], q2 = Q[I + cells * (Ns + 1)], q3 = Q[I + cells * (Ns + 2)];
+                const double ke = 0.5 * (q1 * q1 + q2 * q2 + q3 * q3) / 1.0;
+                out[cells * (P_Y0 + Ns)] = F((Q[I + cells * (Ns + 3)] - ke) / 1.0);
+            }
         }
     }
 }
@@ -131,6 +145,88 @@ __global__ void k_delta4(const F* __restrict__ f, F* __restrict__ out, Grid3 g, 
     }
 }
 
+// delta4_sum! for NF fields at once, tiled: a block covers 32 x 8 (x, y)
+// columns and walks z; each xy-plane (with 2-point halos) is staged in shared
+// memory for the x and y differences, and every thread keeps its column's
+// five z values in registers for the z difference.  Accumulation order per
+// point is the reference's: out = 0; for d in x, y, z: out += w_d |sum_m D4_m f|.
+constexpr int kTX = 32, kTY = 8, kZC = 32;
+__device__ __forceinline__ int edge_index(int i, int n, int periodic) {
+    if (periodic) return i < 0 ? i + n : (i >= n ? i - n : i);
+    return i < 0 ? 0 : (i >= n ? n - 1 : i);
+}
+template <typename F, int NF>
+__global__ void __launch_bounds__(kTX * kTY) k_delta4_tiled(const F* __restrict__ f0, const F* __restrict__ f1,
+                                                           F* __restrict__ o0, F* __restrict__ o1, Grid3 g,
+                                                           Weights3 w0, Weights3 w1) {
+    __shared__ F tile[NF][kTY + 4][kTX + 4];
+    const F* fs[2] = {f0, f1};
+    F* os[2] = {o0, o1};
+    const Weights3 ws[2] = {w0, w1};
+    const int nx = g.n[0], ny = g.n[1], nz = g.n[2];
+    const int64_t sy = nx, sz = (int64_t)nx * ny;
+    const int tx = threadIdx.x % kTX, ty = threadIdx.x / kTX;
+    const int x0 = blockIdx.x * kTX, y0 = blockIdx.y * kTY, z0 = blockIdx.z * kZC;
+    const int x = x0 + tx, y = y0 + ty;
+    const bool inside = x < nx && y < ny;
+    const double D4[5] = {1.0, -4.0, 6.0, -4.0, 1.0};
+    // z window of my column
+    F zw[NF][5];
+    if (g.active[2]) {
+#pragma unroll
+        for (int f = 0; f < NF; ++f)
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+                zw[f][q + 1] = inside ? fs[f][x + y * sy + edge_index(z0 - 2 + q, nz, g.periodic[2]) * sz] : F(0);
+    }
+    const int zend = min(z0 + kZC, nz);
+    for (int z = z0; z < zend; ++z) {
+        // stage plane z with halos
+        for (int idx = threadIdx.x; idx < (kTX + 4) * (kTY + 4); idx += kTX * kTY) {
+            const int hx = idx % (kTX + 4), hy = idx / (kTX + 4);
+            const int gx = g.active[0] ? edge_index(x0 - 2 + hx, nx, g.periodic[0]) : min(x0 - 2 + hx < 0 ? 0 : x0 - 2 + hx, nx - 1);
+            const int gy = g.active[1] ? edge_index(y0 - 2 + hy, ny, g.periodic[1]) : min(y0 - 2 + hy < 0 ? 0 : y0 - 2 + hy, ny - 1);
+#pragma unroll
+            for (int f = 0; f < NF; ++f) tile[f][hy][hx] = fs[f][gx + gy * sy + (int64_t)z * sz];
+        }
+        if (g.active[2]) {
+#pragma unroll
+            for (int f = 0; f < NF; ++f) {
+#pragma unroll
+                for (int q = 0; q < 4; ++q) zw[f][q] = zw[f][q + 1];
+                zw[f][4] = inside ? fs[f][x + y * sy + edge_index(z + 2, nz, g.periodic[2]) * sz] : F(0);
+            }
+        }
+        __syncthreads();
+        if (inside) {
+#pragma unroll
+            for (int f = 0; f < NF; ++f) {
+                double o = 0.0;
+                if (g.active[0]) {
+                    double acc = 0.0;
+#pragma unroll
+                    for (int m = 0; m < 5; ++m) acc += D4[m] * double(tile[f][ty + 2][tx + m]);
+                    o += ws[f].w[0] * fabs(acc);
+                }
+                if (g.active[1]) {
+                    double acc = 0.0;
+#pragma unroll
+                    for (int m = 0; m < 5; ++m) acc += D4[m] * double(tile[f][ty + m][tx + 2]);
+                    o += ws[f].w[1] * fabs(acc);
+                }
+                if (g.active[2]) {
+                    double acc = 0.0;
+#pragma unroll
+                    for (int m = 0; m < 5; ++m) acc += D4[m] * double(zw[f][m]);
+                    o += ws[f].w[2] * fabs(acc);
+                }
+                os[f][x + y * sy + (int64_t)z * sz] = F(o);
+            }
+        }
+        __syncthreads();
+    }
+}
+
 // Ducros switch (src/artificial.jl:134-147)
 __device__ __forceinline__ double compression_switch(const double* gv) {
     const double div = gv[0] + gv[4] + gv[8];
@@ -156,6 +252,28 @@ __global__ void k_mu_beta(const F* __restrict__ sensor, const F* __restrict__ pr
         }
         art[I + cells * A_MU] = F(C_mu * rs);
         art[I + cells * A_BETA] = F(beta);
+    }
+}
+
+// mu*, beta* (optionally gated) and kappa* from the two smoothed sensors in one
+// pass (src/artificial.jl:306-313 and :334-341).
+template <typename F>
+__global__ void k_art_coef(const F* __restrict__ s_strain, const F* __restrict__ s_energy, const F* __restrict__ prim,
+                           const F* __restrict__ g, F* __restrict__ art, int64_t cells, double C_mu, double C_beta,
+                           double C_kappa, int gate) {
+    GRID_STRIDE(I, cells) {
+        const double rho = double(prim[I + cells * P_RHO]);
+        const double rs = rho * jl_max(double(s_strain[I]), 0.0);
+        double beta = C_beta * rs;
+        if (gate) {
+            double gv[9];
+            for (int k = 0; k < 9; ++k) gv[k] = double(g[I + cells * k]);
+            beta *= compression_switch(gv);
+        }
+        art[I + cells * A_MU] = F(C_mu * rs);
+        art[I + cells * A_BETA] = F(beta);
+        const double scale = rho * double(prim[I + cells * P_C]) / jl_max(double(prim[I + cells * P_T]), 2.220446049250313e-16);
+        art[I + cells * A_KAPPA] = F(C_kappa * scale * jl_max(double(s_energy[I]), 0.0));
     }
 }
 
@@ -213,11 +331,16 @@ __global__ void k_dart(const F* __restrict__ sensor, const F* __restrict__ prim,
 
 // _assemble_fluxes! (src/rhs.jl:495-556).  gty[d*(1+Ns) + 0] = dT/dx_d,
 // gty[d*(1+Ns) + 1 + k] = dY_k/dx_d; flux[d*ncons + c].
-template <typename F>
+// SINGLE (one species): the species diffusion flux rho D dY (Y - 1) is zero in
+// exact arithmetic (Y = 1) and below ~1e-30 of the momentum flux in FP64, so it
+// is taken as 0 and dY/dx_d is neither computed nor read (gty holds dT only).
+template <typename F, bool SINGLE>
 __global__ void k_fluxes(const double* __restrict__ Q, const F* __restrict__ prim, const F* __restrict__ g,
                          const F* __restrict__ gty, const F* __restrict__ art, F* __restrict__ flux, int64_t cells,
                          int Ns, PhysConst pc, double mu0, double Pr, double Sc) {
+    if (SINGLE) Ns = 1;
     const int ncons = Ns + 4;
+    const int gstride = SINGLE ? 1 : 1 + Ns;
     GRID_STRIDE(I, cells) {
         double gv[9];
 #pragma unroll
@@ -243,18 +366,23 @@ __global__ void k_fluxes(const double* __restrict__ Q, const F* __restrict__ pri
         for (int d = 0; d < 3; ++d) {
             const double ud = uv[d];
             const double* td = tau[d];
-            const F* gd = gty + cells * (int64_t)(d * (1 + Ns));
+            const F* gd = gty + cells * (int64_t)(d * gstride);
             F* fd = flux + cells * (int64_t)(d * ncons);
-            double Vc = 0.0;
-            for (int sp = 0; sp < Ns; ++sp)
-                Vc += (D0 + double(art[I + cells * (A_D0 + sp)])) * double(gd[I + cells * (1 + sp)]);
             double hdiff = 0.0;
-            for (int sp = 0; sp < Ns; ++sp) {
-                const double Dk = D0 + double(art[I + cells * (A_D0 + sp)]);
-                const double Yk = double(prim[I + cells * (P_Y0 + sp)]);
-                const double Jkd = r * (-Dk * double(gd[I + cells * (1 + sp)]) + Yk * Vc);
-                fd[I + cells * sp] = F(r * Yk * ud + Jkd);
-                hdiff += pc.cpk[sp] * Tp * Jkd;
+            if (SINGLE) {
+                const double Yk = double(prim[I + cells * P_Y0]);
+                fd[I] = F(r * Yk * ud);
+            } else {
+                double Vc = 0.0;
+                for (int sp = 0; sp < Ns; ++sp)
+                    Vc += (D0 + double(art[I + cells * (A_D0 + sp)])) * double(gd[I + cells * (1 + sp)]);
+                for (int sp = 0; sp < Ns; ++sp) {
+                    const double Dk = D0 + double(art[I + cells * (A_D0 + sp)]);
+                    const double Yk = double(prim[I + cells * (P_Y0 + sp)]);
+                    const double Jkd = r * (-Dk * double(gd[I + cells * (1 + sp)]) + Yk * Vc);
+                    fd[I + cells * sp] = F(r * Yk * ud + Jkd);
+                    hdiff += pc.cpk[sp] * Tp * Jkd;
+                }
             }
             fd[I + cells * (Ns + 0)] = F(r * ud * uv[0] + (d == 0 ? p : 0.0) - td[0]);
             fd[I + cells * (Ns + 1)] = F(r * ud * uv[1] + (d == 1 ? p : 0.0) - td[1]);
@@ -464,8 +592,29 @@ __global__ void k_to_double(const F* __restrict__ a, double* __restrict__ b, int
     } while (0)
 
 template <typename F>
-void Pointwise<F>::primitives(const double* Q, F* prim, int64_t cells, int Ns, const PhysConst& pc, cudaStream_t st) {
-    LAUNCH(k_primitives<F>, cells, st, Q, prim, cells, Ns, pc);
+void Pointwise<F>::primitives(const double* Q, F* prim, int64_t cells, int Ns, const PhysConst& pc, cudaStream_t st,
+                              int esens) {
+    LAUNCH(k_primitives<F>, cells, st, Q, prim, cells, Ns, pc, esens);
+}
+template <typename F>
+void Pointwise<F>::delta4_tiled(const F* f0, const F* f1, F* o0, F* o1, const Grid3& g, const double w0[3],
+                                const double w1[3], cudaStream_t st) {
+    dim3 grid((unsigned)((g.n[0] + kTX - 1) / kTX), (unsigned)((g.n[1] + kTY - 1) / kTY),
+              (unsigned)((g.n[2] + kZC - 1) / kZC));
+    Weights3 a{{w0[0], w0[1], w0[2]}}, b{{0.0, 0.0, 0.0}};
+    if (f1) {
+        b = Weights3{{w1[0], w1[1], w1[2]}};
+        k_delta4_tiled<F, 2><<<grid, kTX * kTY, 0, st>>>(f0, f1, o0, o1, g, a, b);
+    } else {
+        k_delta4_tiled<F, 1><<<grid, kTX * kTY, 0, st>>>(f0, f0, o0, o0, g, a, b);
+    }
+    count_launch();
+    check_launch("k_delta4_tiled");
+}
+template <typename F>
+void Pointwise<F>::art_coef(const F* s_strain, const F* s_energy, const F* prim, const F* g, F* art, int64_t cells,
+                            double C_mu, double C_beta, double C_kappa, int gate, cudaStream_t st) {
+    LAUNCH(k_art_coef<F>, cells, st, s_strain, s_energy, prim, g, art, cells, C_mu, C_beta, C_kappa, gate);
 }
 template <typename F>
 void Pointwise<F>::strain(const F* g, F* out, int64_t cells, cudaStream_t st) {
@@ -506,7 +655,8 @@ template <typename F>
 void Pointwise<F>::fluxes(const double* Q, const F* prim, const F* g, const F* gty, const F* art, F* flux,
                           int64_t cells, int Ns, const PhysConst& pc, double mu0, double Pr, double Sc,
                           cudaStream_t st) {
-    LAUNCH(k_fluxes<F>, cells, st, Q, prim, g, gty, art, flux, cells, Ns, pc, mu0, Pr, Sc);
+    if (Ns == 1) LAUNCH((k_fluxes<F, true>), cells, st, Q, prim, g, gty, art, flux, cells, Ns, pc, mu0, Pr, Sc);
+    else LAUNCH((k_fluxes<F, false>), cells, st, Q, prim, g, gty, art, flux, cells, Ns, pc, mu0, Pr, Sc);
 }
 template <typename F>
 void Pointwise<F>::lsrk(double* Q, double* du, const F* dQ, int64_t n, double A, double B, double dt, cudaStream_t st) {

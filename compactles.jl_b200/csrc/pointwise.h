@@ -23,13 +23,24 @@ struct Grid3 {
     int periodic[3];
 };
 
+struct Weights3 {
+    double w[3];
+};
+
 struct BcState {
     double q[CLES_MAX_SPECIES + 4];
 };
 
 template <typename F>
 struct Pointwise {
-    static void primitives(const double* Q, F* prim, int64_t cells, int Ns, const PhysConst& pc, cudaStream_t st);
+    // esens: also write the kappa*-sensor input (internal energy) into slot P_Y0 + Ns
+    static void primitives(const double* Q, F* prim, int64_t cells, int Ns, const PhysConst& pc, cudaStream_t st,
+                           int esens = 0);
+    // delta4_sum! of one (f1 == nullptr) or two fields in one tiled pass
+    static void delta4_tiled(const F* f0, const F* f1, F* o0, F* o1, const Grid3& g, const double w0[3],
+                             const double w1[3], cudaStream_t st);
+    static void art_coef(const F* s_strain, const F* s_energy, const F* prim, const F* g, F* art, int64_t cells,
+                         double C_mu, double C_beta, double C_kappa, int gate, cudaStream_t st);
     static void strain(const F* g, F* out, int64_t cells, cudaStream_t st);
     static void delta4(const F* f, F* out, const Grid3& g, const double wd[3], cudaStream_t st);
     static void mu_beta(const F* sensor, const F* prim, const F* g, F* art, int64_t cells, double C_mu, double C_beta,

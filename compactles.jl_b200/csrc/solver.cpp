@@ -110,7 +110,7 @@ public:
         Q_.alloc(ctx, sizeof(double) * c * ncons_);
         du_.alloc(ctx, sizeof(double) * c * ncons_);
         dQ_.alloc(ctx, sizeof(F) * c * ncons_);
-        prim_.alloc(ctx, sizeof(F) * c * (P_Y0 + Ns_));
+        prim_.alloc(ctx, sizeof(F) * c * (P_Y0 + Ns_ + 1));  // + the kappa*-sensor input
         g_u_.alloc(ctx, sizeof(F) * c * 9);
         gty_.alloc(ctx, sizeof(F) * c * 3 * (1 + Ns_));
         art_.alloc(ctx, sizeof(F) * c * (A_D0 + Ns_));
@@ -144,10 +144,11 @@ public:
     F* scratch(int k) const { return scratch_.as<F>() + (size_t)cells_ * k; }
 
     // --------------------------------------------------------- operators --
-    void smooth(F* f) {
-        // smooth! (src/artificial.jl:98-111): one filter pass per active dim, in place
+    void smooth(F* f, int count) {
+        // smooth! (src/artificial.jl:98-111): one filter pass per active dim, in
+        // place, over `count` adjacent fields
         for (int k = 0; k < 3; ++k)
-            if (g_.active[k]) launch_compact(*filt_[k], view(f), view(f), 1, OUT_STORE, st_);
+            if (g_.active[k]) launch_compact(*filt_[k], view(f), view(f), count, OUT_STORE, st_);
     }
 
     void apply_bcs() override {
@@ -164,35 +165,36 @@ public:
     }
 
     void compute_artificial() {
+        // compute_artificial! (src/artificial.jl:261-359).  The strain and the
+        // internal-energy sensor chains are independent, so their fourth
+        // differences are one tiled pass, their smoothing one batched filter
+        // launch per direction, and mu*, beta*, kappa* one pointwise pass; each
+        // field sees the reference's operations in the reference's order.
         if (!desc.art_enabled) return;
         using PW = Pointwise<F>;
         F* strain = scratch(0);
-        F* sensor = scratch(1);
-        F* sensor_sp = scratch(2);
+        F* sensor = scratch(1);     // smoothed strain sensor
+        F* sensor_e = scratch(2);   // smoothed internal-energy sensor (adjacent: batched smoothing)
         F* tmp_a = scratch(3);
         F* tmp_b = scratch(4);
         const double w2[3] = {h_[0] * h_[0], h_[1] * h_[1], h_[2] * h_[2]};
         const double w1[3] = {h_[0], h_[1], h_[2]};
         PW::strain(g_u_.as<F>(), strain, cells_, st_);
-        PW::delta4(strain, sensor, g_, w2, st_);
-        smooth(sensor);
-        PW::mu_beta(sensor, prim_.as<F>(), g_u_.as<F>(), art_.as<F>(), cells_, desc.C_mu, desc.C_beta,
-                    desc.beta_sensor == CLES_BETA_GATED_STRAIN, st_);
+        PW::delta4_tiled(strain, prim(P_Y0 + Ns_), sensor, sensor_e, g_, w2, w1, st_);
+        smooth(sensor, 2);
+        PW::art_coef(sensor, sensor_e, prim_.as<F>(), g_u_.as<F>(), art_.as<F>(), cells_, desc.C_mu, desc.C_beta,
+                     desc.C_kappa, desc.beta_sensor == CLES_BETA_GATED_STRAIN, st_);
         if (desc.beta_sensor == CLES_BETA_DILATATION) {
             PW::dilatation(g_u_.as<F>(), tmp_a, tmp_b, cells_, st_);
-            PW::delta4(tmp_a, sensor, g_, w2, st_);
-            smooth(sensor);
+            PW::delta4_tiled(tmp_a, nullptr, sensor, nullptr, g_, w2, w2, st_);
+            smooth(sensor, 1);
             PW::beta_dilatation(sensor, prim_.as<F>(), tmp_b, art_.as<F>(), cells_, desc.C_beta, st_);
         }
-        PW::energy(Q_.as<double>(), prim_.as<F>(), tmp_a, cells_, Ns_, st_);
-        PW::delta4(tmp_a, sensor, g_, w1, st_);
-        smooth(sensor);
-        PW::kappa(sensor, prim_.as<F>(), art_.as<F>(), cells_, desc.C_kappa, st_);
         if (Ns_ > 1) {
             for (int sp = 0; sp < Ns_; ++sp) {
-                PW::delta4(prim(P_Y0 + sp), sensor_sp, g_, w1, st_);
-                smooth(sensor_sp);
-                PW::dart(sensor_sp, prim_.as<F>(), art_.as<F>(), cells_, desc.C_D, sp, st_);
+                PW::delta4_tiled(prim(P_Y0 + sp), nullptr, tmp_a, nullptr, g_, w1, w1, st_);
+                smooth(tmp_a, 1);
+                PW::dart(tmp_a, prim_.as<F>(), art_.as<F>(), cells_, desc.C_D, sp, st_);
             }
         }
     }
@@ -202,16 +204,18 @@ public:
     // Returns true when `rk` was applied inside the last divergence launch.
     bool compute_rhs_impl(bool primitives_current, const RkEpilogue* rk) {
         using PW = Pointwise<F>;
-        if (!primitives_current) PW::primitives(Q_.as<double>(), prim_.as<F>(), cells_, Ns_, pc_, st_);
+        if (!primitives_current) PW::primitives(Q_.as<double>(), prim_.as<F>(), cells_, Ns_, pc_, st_, desc.art_enabled);
         // velocity gradients grad_u[d][j] (src/rhs.jl:596-603), one launch per dim for u, v, w
         for (int k = 0; k < 3; ++k)
             if (g_.active[k])
                 launch_compact(*deriv_[k], view(prim(P_U)), view(g_u_.as<F>() + (size_t)cells_ * 3 * k), 3, OUT_STORE, st_);
         compute_artificial();
-        // temperature and mass-fraction gradients (src/rhs.jl:628-636)
+        // temperature and mass-fraction gradients (src/rhs.jl:628-636); with one
+        // species only dT (the species diffusion flux vanishes, see k_fluxes)
+        const int ngty = Ns_ == 1 ? 1 : 1 + Ns_;
         for (int k = 0; k < 3; ++k)
             if (g_.active[k])
-                launch_compact(*deriv_[k], view(prim(P_T)), view(gty_.as<F>() + (size_t)cells_ * (1 + Ns_) * k), 1 + Ns_,
+                launch_compact(*deriv_[k], view(prim(P_T)), view(gty_.as<F>() + (size_t)cells_ * ngty * k), ngty,
                                OUT_STORE, st_);
         PW::fluxes(Q_.as<double>(), prim_.as<F>(), g_u_.as<F>(), gty_.as<F>(), art_.as<F>(), flux_.as<F>(), cells_, Ns_,
                    pc_, desc.mu0, desc.Pr, desc.Sc, st_);
@@ -251,7 +255,7 @@ public:
     }
 
     void max_rate(double* rate, double* rho_min) override {
-        Pointwise<F>::primitives(Q_.as<double>(), prim_.as<F>(), cells_, Ns_, pc_, st_);
+        Pointwise<F>::primitives(Q_.as<double>(), prim_.as<F>(), cells_, Ns_, pc_, st_, desc.art_enabled);
         double idx[3];
         int act[3];
         for (int k = 0; k < 3; ++k) { idx[k] = 1.0 / h_[k]; act[k] = g_.active[k]; }
@@ -383,7 +387,7 @@ public:
             case CLES_FIELD_MU_ART: src = art_.as<F>() + (size_t)cells_ * A_MU; break;
             case CLES_FIELD_BETA_ART: src = art_.as<F>() + (size_t)cells_ * A_BETA; break;
             case CLES_FIELD_KAPPA_ART: src = art_.as<F>() + (size_t)cells_ * A_KAPPA; break;
-            case CLES_FIELD_SENSOR: src = scratch(1); break;
+            case CLES_FIELD_SENSOR: src = scratch(2); break;  // the last sensor built: internal energy
             default:
                 if (which >= CLES_FIELD_Y0 && which < CLES_FIELD_Y0 + Ns_) src = prim(P_Y0 + which - CLES_FIELD_Y0);
                 else if (which >= CLES_FIELD_D_ART0 && which < CLES_FIELD_D_ART0 + Ns_)
@@ -411,7 +415,7 @@ public:
         // dissipation_rate (src/diagnostics.jl:354-378): refreshes primitives,
         // gradients and artificial properties from the resident state
         using PW = Pointwise<F>;
-        PW::primitives(Q_.as<double>(), prim_.as<F>(), cells_, Ns_, pc_, st_);
+        PW::primitives(Q_.as<double>(), prim_.as<F>(), cells_, Ns_, pc_, st_, desc.art_enabled);
         for (int k = 0; k < 3; ++k)
             if (g_.active[k])
                 launch_compact(*deriv_[k], view(prim(P_U)), view(g_u_.as<F>() + (size_t)cells_ * 3 * k), 3, OUT_STORE, st_);
