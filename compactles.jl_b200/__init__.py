@@ -13,4 +13,5 @@ from .problem import (ArtParams, DirichletBC, IdealMixture, IdealSpecies, Numeri
                       taylor_green_problem)
 from .api import (ClesError, Context, DirPlan, Solver, SolverFailure, apply_along, build, check_step,
                   compact_filter, default_context, grid, kernel_launches, lele_d1_10, lele_d1_6, lib,
-                  pade_d1_4, plan_direction, profile_enable, profile_read, setup)
+                  pade_d1_4, plan_direction, profile_enable, profile_read, setup, Server)
+from . import scenarios

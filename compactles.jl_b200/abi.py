@@ -178,3 +178,24 @@ class cles_profile_entry(C.Structure):
         ("total_ms", C.c_double),
         ("bytes", C.c_double),
     ]
+
+
+CLES_REQ_QUEUED = 0
+CLES_REQ_RUNNING = 1
+CLES_REQ_DONE = 2
+CLES_REQ_FAILED = 3
+CLES_REQ_CANCELLED = 4
+REQ_STATES = {0: "queued", 1: "running", 2: "done", 3: "failed", 4: "cancelled"}
+
+
+class cles_request_status(C.Structure):
+    _fields_ = [
+        ("state", C.c_int),
+        ("failure", C.c_int),
+        ("steps", C.c_int64),
+        ("t", C.c_double),
+        ("submit_s", C.c_double),
+        ("admit_s", C.c_double),
+        ("done_s", C.c_double),
+        ("device_bytes", C.c_size_t),
+    ]

@@ -93,6 +93,15 @@ def lib():
         L.cles_profile_read.argtypes = [C.POINTER(abi.cles_profile_entry), C.c_int, C.POINTER(C.c_int)]
         L.cles_max_rate_static.argtypes = [vp, vp, C.c_int64, C.c_int, dp, dp, dp, C.c_double, C.c_double,
                                            C.c_double, vp, vp]
+        L.cles_run_graph.argtypes = [vp, C.c_double, C.c_int64, C.POINTER(abi.cles_run_result)]
+        L.cles_server_create.argtypes = [C.c_int, C.c_size_t, C.c_int, C.POINTER(vp)]
+        L.cles_server_destroy.argtypes = [vp]
+        L.cles_server_submit.argtypes = [vp, C.POINTER(abi.cles_solver_desc), vp, C.c_int, C.c_double, C.c_int64,
+                                         C.POINTER(C.c_int64)]
+        L.cles_server_tick.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(C.c_int)]
+        L.cles_server_status.argtypes = [vp, C.c_int64, C.POINTER(abi.cles_request_status)]
+        L.cles_server_fetch.argtypes = [vp, C.c_int64, vp]
+        L.cles_server_cancel.argtypes = [vp, C.c_int64]
         L.cles_kinetic_energy.argtypes = [vp, dp]
         L.cles_dissipation_rate.argtypes = [vp, dp]
         _lib = L
@@ -339,6 +348,17 @@ class Solver:
         _check(rc)
         return res
 
+    def run_graph(self, tfinal, nmax=2 ** 62, raise_on_failure=True):
+        """run! with every step as one CUDA-graph launch (device-side dt and floors)."""
+        res = abi.cles_run_result()
+        rc = lib().cles_run_graph(self.ptr, float(tfinal), int(nmax), C.byref(res))
+        if rc == abi.CLES_EFAILURE:
+            if raise_on_failure:
+                raise SolverFailure(abi.FAIL_NAMES[res.failure], res)
+            return res
+        _check(rc)
+        return res
+
     def step_host(self, Q, tfinal, layout="padded"):
         """One run! iteration on a host state array, updated in place."""
         res = abi.cles_run_result()
@@ -370,3 +390,58 @@ def setup(prob, num, ctx=None):
     Q = initialize(desc, prob.ic, eos=prob.eos)
     s.set_state(Q)
     return s, Q
+
+
+class Server:
+    """Continuous-batching server of independent solves on one device (cles_server_*)."""
+
+    def __init__(self, device=0, hbm_budget=0, max_active=64):
+        self.ptr = C.c_void_p()
+        _check(lib().cles_server_create(int(device), int(hbm_budget), int(max_active), C.byref(self.ptr)))
+        self._layout = {}
+
+    def __del__(self):
+        try:
+            if self.ptr:
+                lib().cles_server_destroy(self.ptr)
+                self.ptr = None
+        except Exception:
+            pass
+
+    def submit(self, desc, Q0, tfinal, nmax=2 ** 62, layout="padded"):
+        Q0 = np.ascontiguousarray(Q0, dtype=np.float64)
+        lay = abi.CLES_LAYOUT_PADDED if layout == "padded" else abi.CLES_LAYOUT_INTERIOR
+        rid = C.c_int64()
+        _check(lib().cles_server_submit(self.ptr, C.byref(desc), Q0.ctypes.data_as(C.c_void_p), lay, float(tfinal),
+                                        int(nmax), C.byref(rid)))
+        self._layout[rid.value] = Q0.shape
+        return rid.value
+
+    def tick(self):
+        r, q = C.c_int(), C.c_int()
+        _check(lib().cles_server_tick(self.ptr, C.byref(r), C.byref(q)))
+        return r.value, q.value
+
+    def status(self, rid):
+        st = abi.cles_request_status()
+        _check(lib().cles_server_status(self.ptr, int(rid), C.byref(st)))
+        return {"state": abi.REQ_STATES[st.state], "failure": abi.FAIL_NAMES.get(st.failure), "steps": st.steps,
+                "t": st.t, "submit_s": st.submit_s, "admit_s": st.admit_s, "done_s": st.done_s,
+                "device_bytes": st.device_bytes}
+
+    def fetch(self, rid):
+        out = np.zeros(self._layout[rid])
+        _check(lib().cles_server_fetch(self.ptr, int(rid), out.ctypes.data_as(C.c_void_p)))
+        del self._layout[rid]
+        return out
+
+    def cancel(self, rid):
+        _check(lib().cles_server_cancel(self.ptr, int(rid)))
+
+    def drain(self, max_ticks=10 ** 8):
+        """Tick until nothing is running or queued."""
+        for _ in range(max_ticks):
+            r, q = self.tick()
+            if r == 0 and q == 0:
+                return
+        raise ClesError(abi.CLES_ETIMEOUT, "server did not drain")

@@ -476,6 +476,19 @@ int cles_run(cles_solver* s, double tfinal, int64_t nmax, cles_run_result* out) 
     API_END
 }
 
+int cles_run_graph(cles_solver* s, double tfinal, int64_t nmax, cles_run_result* out) {
+    int rc = CLES_OK;
+    API_BEGIN
+    if (!s) throw Error(CLES_EINVAL, "null solver");
+    CLES_CUDA(cudaSetDevice(s->ctx->device));
+    rc = run_graph(*s->s, tfinal, nmax, out);
+    if (rc == CLES_EFAILURE) {
+        set_last_error("SolverFailure: step control rejected the step (see cles_run_result.failure)");
+        return rc;
+    }
+    API_END
+}
+
 int cles_step_host(cles_solver* s, double* Q_host, int layout, double tfinal, cles_run_result* out) {
     int rc = CLES_OK;
     API_BEGIN

@@ -127,6 +127,7 @@ struct RkEpilogue {
     double* Q;
     double* du;
     double A, B, dt;
+    const double* dtp;  // when set, dt is read from device memory (graph mode)
 };
 
 // TMA-pipelined y/z launch; false when the plan or the views do not qualify.

@@ -228,6 +228,7 @@ __global__ void __launch_bounds__(256, 1)
             base += ob + (int64_t)off * st;
             if (mode == OUT_RK) {
                 const int64_t eo = (int64_t)c * out.comp_stride + x + ob + (int64_t)off * st;
+                const double rdt = rk.dtp ? *rk.dtp : rk.dt;
                 double* Qp = rk.Q + eo;
                 double* dp = rk.du + eo;
 #pragma unroll
@@ -243,7 +244,7 @@ __global__ void __launch_bounds__(256, 1)
 #pragma unroll
                     for (int q = 0; q < 8; ++q) {
                         const T dq = o[q] - y[i0 + q];
-                        const double v = rk.A * dv[q] + rk.dt * double(dq);
+                        const double v = rk.A * dv[q] + rdt * double(dq);
                         dp[(int64_t)(i0 + q) * st] = v;
                         Qp[(int64_t)(i0 + q) * st] = qv[q] + rk.B * v;
                     }
@@ -328,7 +329,7 @@ bool launch_tma_m(const CompactPlan& plan, const CUtensorMap& map, const FieldVi
 
 bool try_launch_tma(const CompactPlan& plan, const FieldView& in, const FieldView& out, int count, int mode,
                     cudaStream_t st, const RkEpilogue* rkp) {
-    RkEpilogue rk{nullptr, nullptr, 0.0, 0.0, 0.0};
+    RkEpilogue rk{nullptr, nullptr, 0.0, 0.0, 0.0, nullptr};
     if (rkp) rk = *rkp;
     if (mode == OUT_RK && !rkp) return false;
     if (!plan.has_tl) return false;

@@ -396,7 +396,8 @@ __global__ void k_fluxes(const double* __restrict__ Q, const F* __restrict__ pri
 // Low-storage RK update (src/timestep.jl:86-95): v = A du + dt dQ; du = v; Q += B v.
 template <typename F>
 __global__ void k_lsrk(double* __restrict__ Q, double* __restrict__ du, const F* __restrict__ dQ, int64_t n, double A,
-                       double B, double dt) {
+                       double B, double dt, const double* __restrict__ dtp) {
+    if (dtp) dt = *dtp;
     GRID_STRIDE(I, n) {
         const double v = A * du[I] + dt * double(dQ[I]);
         du[I] = v;
@@ -581,7 +582,49 @@ __global__ void k_to_double(const F* __restrict__ a, double* __restrict__ b, int
     GRID_STRIDE(I, n) b[I] = double(a[I]);
 }
 
+// Device clock of the graph-mode run loop (one thread).  clk layout: see
+// DeviceClock in pointwise.h.  Before the step: dt from the reduced rate
+// (predicted_dt without prediction or growth cap), the check_step floors
+// (src/stepcontrol.jl:184-204), dt_seen, and the tfinal clip
+// (src/timestep.jl:288-352).
+__global__ void k_clock_before(double* __restrict__ clk, const double* __restrict__ rate_rmin, ClockConst c) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    if (clk[DC_FAILURE] != 0.0 || clk[DC_DONE] != 0.0) { clk[DC_DT] = 0.0; return; }
+    const double rate = rate_rmin[0], rmin = rate_rmin[1];
+    double dt = c.cfl / rate;
+    int f = 0;
+    if (!isfinite(dt)) f = CLES_FAIL_NONFINITE;
+    else if (!(rmin > 0)) f = CLES_FAIL_NEGATIVE_DENSITY;
+    else if (!(dt > 5.391247e-44)) f = CLES_FAIL_PLANCK;
+    else if (!(dt >= c.dt_min)) f = CLES_FAIL_DT_MIN;
+    else if (c.dt_min_ratio > 0 && clk[DC_DT_SEEN] > 0 && !(dt >= c.dt_min_ratio * clk[DC_DT_SEEN])) f = CLES_FAIL_DT_COLLAPSE;
+    clk[DC_RATE] = rate;
+    clk[DC_RHO_MIN] = rmin;
+    if (f) { clk[DC_FAILURE] = f; clk[DC_DT] = 0.0; return; }
+    clk[DC_DT_SEEN] = jl_max(clk[DC_DT_SEEN], dt);
+    clk[DC_DT] = jl_min(dt, c.tfinal - clk[DC_T]);
+}
+// After the step: t += dt, step += 1, done when the run! loop condition fails.
+__global__ void k_clock_after(double* __restrict__ clk, ClockConst c) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    if (clk[DC_FAILURE] != 0.0 || clk[DC_DONE] != 0.0) return;
+    clk[DC_T] += clk[DC_DT];
+    clk[DC_STEP] += 1.0;
+    if (!(clk[DC_T] < c.tfinal) || !(clk[DC_STEP] < c.nmax)) clk[DC_DONE] = 1.0;
+}
+
 }  // namespace
+
+void clock_before(double* clk, const double* rate_rmin, const ClockConst& c, cudaStream_t st) {
+    k_clock_before<<<1, 32, 0, st>>>(clk, rate_rmin, c);
+    count_launch();
+    check_launch("k_clock_before");
+}
+void clock_after(double* clk, const ClockConst& c, cudaStream_t st) {
+    k_clock_after<<<1, 32, 0, st>>>(clk, c);
+    count_launch();
+    check_launch("k_clock_after");
+}
 
 // ------------------------------------------------------------- launchers ----
 #define LAUNCH(kern, n, st, ...)                                      \
@@ -659,8 +702,9 @@ void Pointwise<F>::fluxes(const double* Q, const F* prim, const F* g, const F* g
     else LAUNCH((k_fluxes<F, false>), cells, st, Q, prim, g, gty, art, flux, cells, Ns, pc, mu0, Pr, Sc);
 }
 template <typename F>
-void Pointwise<F>::lsrk(double* Q, double* du, const F* dQ, int64_t n, double A, double B, double dt, cudaStream_t st) {
-    LAUNCH(k_lsrk<F>, n, st, Q, du, dQ, n, A, B, dt);
+void Pointwise<F>::lsrk(double* Q, double* du, const F* dQ, int64_t n, double A, double B, double dt, cudaStream_t st,
+                        const double* dtp) {
+    LAUNCH(k_lsrk<F>, n, st, Q, du, dQ, n, A, B, dt, dtp);
 }
 template <typename F>
 void Pointwise<F>::rate(const double* Q, const F* prim, const F* art, double* part, double* out, int64_t cells, int Ns,

@@ -53,7 +53,8 @@ struct Pointwise {
     static void dart(const F* sensor, const F* prim, F* art, int64_t cells, double C_D, int sp, cudaStream_t st);
     static void fluxes(const double* Q, const F* prim, const F* g, const F* gty, const F* art, F* flux, int64_t cells,
                        int Ns, const PhysConst& pc, double mu0, double Pr, double Sc, cudaStream_t st);
-    static void lsrk(double* Q, double* du, const F* dQ, int64_t n, double A, double B, double dt, cudaStream_t st);
+    static void lsrk(double* Q, double* du, const F* dQ, int64_t n, double A, double B, double dt, cudaStream_t st,
+                     const double* dtp = nullptr);
     static void rate(const double* Q, const F* prim, const F* art, double* part, double* out, int64_t cells, int Ns,
                      const double idx[3], const int act[3], double mu0, double Pr, double Sc, cudaStream_t st);
     static void kinetic(const double* Q, double* part, double* out, int64_t cells, int Ns, cudaStream_t st);
@@ -64,6 +65,14 @@ struct Pointwise {
 };
 
 void bc_plane(double* Q, const Grid3& g, int d, int side, int Ns, int kind, const BcState& s, cudaStream_t st);
+
+// Device clock of the graph-mode run loop: slots of a double[16] buffer.
+enum { DC_T = 0, DC_DT = 1, DC_RATE = 2, DC_RHO_MIN = 3, DC_FAILURE = 4, DC_STEP = 5, DC_DT_SEEN = 6, DC_DONE = 7 };
+struct ClockConst {
+    double cfl, tfinal, nmax, dt_min, dt_min_ratio;
+};
+void clock_before(double* clk, const double* rate_rmin, const ClockConst& c, cudaStream_t st);
+void clock_after(double* clk, const ClockConst& c, cudaStream_t st);
 int64_t rate_partials(int64_t cells);
 
 }  // namespace cles

@@ -135,7 +135,10 @@ public:
     }
 
     ~Solver() override {
+        graph_free();
         if (host_res_) cudaFreeHost(host_res_);
+        if (host_clk_) cudaFreeHost(host_clk_);
+        if (cap_st_) cudaStreamDestroy(cap_st_);
     }
 
     // ------------------------------------------------------------- views --
@@ -428,6 +431,102 @@ public:
     }
 
     double* state_device() override { return Q_.as<double>(); }
+    cudaStream_t stream() const override { return st_; }
+
+    // ------------------------------------------------------------ graph mode --
+    // Captures on a private non-blocking stream (the legacy default stream,
+    // which a context may use, cannot be captured); the graph is launched on
+    // the context's stream.
+    void capture_step(bool with_filter, cudaGraphExec_t* exec) {
+        cudaGraph_t g = nullptr;
+        if (!cap_st_) CLES_CUDA(cudaStreamCreateWithFlags(&cap_st_, cudaStreamNonBlocking));
+        const cudaStream_t user = st_;
+        st_ = cap_st_;
+        const cudaError_t eb = cudaStreamBeginCapture(st_, cudaStreamCaptureModeRelaxed);
+        if (eb != cudaSuccess) {
+            st_ = user;
+            throw Error(CLES_ECUDA, std::string("cudaStreamBeginCapture: ") + cudaGetErrorString(eb));
+        }
+        try {
+            double* clk = clk_.as<double>();
+            apply_bcs();
+            Pointwise<F>::primitives(Q_.as<double>(), prim_.as<F>(), cells_, Ns_, pc_, st_, desc.art_enabled);
+            double idx[3];
+            int act[3];
+            for (int k = 0; k < 3; ++k) { idx[k] = 1.0 / h_[k]; act[k] = g_.active[k]; }
+            Pointwise<F>::rate(Q_.as<double>(), prim_.as<F>(), art_.as<F>(), part_.as<double>(), res_.as<double>(),
+                               cells_, Ns_, idx, act, desc.mu0, desc.Pr, desc.Sc, st_);
+            clock_before(clk, res_.as<double>(), cc_, st_);
+            for (int stage = 0; stage < 5; ++stage) {
+                if (stage > 0) apply_bcs();
+                const RkEpilogue rk{Q_.as<double>(), du_.as<double>(), RKA[stage], RKB[stage], 0.0, clk + DC_DT};
+                if (!compute_rhs_impl(stage == 0, &rk))
+                    Pointwise<F>::lsrk(Q_.as<double>(), du_.as<double>(), dQ_.as<F>(), cells_ * ncons_, RKA[stage],
+                                       RKB[stage], 0.0, st_, clk + DC_DT);
+            }
+            apply_bcs();
+            clock_after(clk, cc_, st_);
+            if (with_filter) filter_state();
+            CLES_CUDA(cudaMemcpyAsync(host_clk_, clk_.p, 8 * sizeof(double), cudaMemcpyDeviceToHost, st_));
+        } catch (...) {
+            cudaStreamEndCapture(st_, &g);
+            st_ = user;
+            if (g) cudaGraphDestroy(g);
+            cudaGetLastError();
+            throw;
+        }
+        const cudaError_t ee = cudaStreamEndCapture(st_, &g);
+        st_ = user;
+        if (ee != cudaSuccess) {
+            if (g) cudaGraphDestroy(g);
+            throw Error(CLES_ECUDA, std::string("cudaStreamEndCapture: ") + cudaGetErrorString(ee));
+        }
+        const cudaError_t e = cudaGraphInstantiate(exec, g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) throw Error(CLES_ECUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
+    }
+
+    void graph_begin(double tfinal, int64_t nmax) override {
+        const cles_step_control& c = desc.control;
+        if (c.predict > 0 || c.max_growth > 0)
+            throw Error(CLES_EINVAL, "graph mode supports neither rate prediction nor growth capping");
+        cc_ = ClockConst{cfl, tfinal, (double)nmax, c.dt_min, c.dt_min_ratio};
+        if (!clk_.p) clk_.alloc(ctx_, 16 * sizeof(double));
+        if (!host_clk_) CLES_CUDA(cudaMallocHost(&host_clk_, 16 * sizeof(double)));
+        double h[16] = {0};
+        h[DC_T] = t;
+        h[DC_STEP] = (double)step_count;
+        h[DC_DONE] = (t < tfinal && step_count < nmax) ? 0.0 : 1.0;
+        std::memcpy(host_clk_, h, sizeof(h));
+        CLES_CUDA(cudaMemcpyAsync(clk_.p, host_clk_, sizeof(h), cudaMemcpyHostToDevice, st_));
+        CLES_CUDA(cudaStreamSynchronize(st_));
+        graph_free();
+        capture_step(true, &gexec_filter_);
+        if (desc.filter_interval != 1) capture_step(false, &gexec_plain_);
+        CLES_CUDA(cudaStreamSynchronize(st_));
+    }
+
+    void graph_launch() override {
+        const int64_t next = (int64_t)host_clk_[DC_STEP] + 1;
+        const bool filt = desc.filter_interval > 0 && next % desc.filter_interval == 0;
+        CLES_CUDA(cudaGraphLaunch(filt || !gexec_plain_ ? gexec_filter_ : gexec_plain_, st_));
+    }
+
+    const double* graph_clock() const override { return host_clk_; }
+
+    void graph_end() override {
+        CLES_CUDA(cudaStreamSynchronize(st_));
+        t = host_clk_[DC_T];
+        step_count = (int64_t)host_clk_[DC_STEP];
+        dt_prev = host_clk_[DC_DT];
+        rate_prev = host_clk_[DC_RATE];
+    }
+
+    void graph_free() {
+        if (gexec_filter_) cudaGraphExecDestroy(gexec_filter_);
+        if (gexec_plain_) cudaGraphExecDestroy(gexec_plain_);
+        gexec_filter_ = gexec_plain_ = nullptr;
+    }
 
     cles_solver_info info() const override {
         cles_solver_info I;
@@ -455,8 +554,12 @@ private:
     int64_t cells_ = 0;
     PhysConst pc_{};
     std::unique_ptr<CompactPlan> deriv_[3], filt_[3], qfilt_[3];
-    DevBuf Q_, du_, dQ_, prim_, g_u_, gty_, art_, scratch_, flux_, part_, res_, save_;
+    DevBuf Q_, du_, dQ_, prim_, g_u_, gty_, art_, scratch_, flux_, part_, res_, save_, clk_;
     double* host_res_ = nullptr;
+    double* host_clk_ = nullptr;
+    ClockConst cc_{};
+    cudaGraphExec_t gexec_filter_ = nullptr, gexec_plain_ = nullptr;
+    cudaStream_t cap_st_ = nullptr;
 };
 
 }  // namespace
@@ -470,6 +573,40 @@ int check_step(const cles_step_control& c, double dt, double rho_min, double dt_
     if (c.dt_min_ratio > 0 && dt_seen > 0)
         if (!(dt >= c.dt_min_ratio * dt_seen)) return CLES_FAIL_DT_COLLAPSE;
     return CLES_FAIL_NONE;
+}
+
+size_t solver_bytes_estimate(const cles_solver_desc& d) {
+    int64_t cells = 1;
+    for (int k = 0; k < 3; ++k) cells *= d.n_global[k] < 1 ? 1 : d.n_global[k];
+    const int Ns = d.n_species, nc = Ns + 4;
+    const size_t F = d.precision == CLES_PREC_MIXED ? sizeof(float) : sizeof(double);
+    const size_t per_cell = 2 * nc * sizeof(double)                     // Q, du
+                            + F * (nc + (P_Y0 + Ns + 1) + 9 + 3 * (1 + Ns) + (A_D0 + Ns) + 5 + 3 * nc) +
+                            (d.control.retries > 0 ? nc * sizeof(double) : 0);
+    return (size_t)cells * per_cell + ((size_t)4 << 20);  // + plan tables and reduction scratch
+}
+
+int run_graph(SolverBase& s, double tfinal, int64_t nmax, cles_run_result* res) {
+    const double t0 = s.t;
+    const int64_t s0 = s.step_count;
+    s.graph_begin(tfinal, nmax);
+    const double* clk = s.graph_clock();
+    while (clk[DC_DONE] == 0.0 && clk[DC_FAILURE] == 0.0) {
+        s.graph_launch();
+        CLES_CUDA(cudaStreamSynchronize(s.stream()));
+    }
+    s.graph_end();
+    const int failure = (int)clk[DC_FAILURE];
+    if (res) {
+        res->steps = s.step_count - s0;
+        res->t = s.t;
+        res->last_dt = clk[DC_DT];
+        res->cfl = s.cfl;
+        res->failure = failure;
+        res->retries_used = 0;
+    }
+    (void)t0;
+    return failure == CLES_FAIL_NONE ? CLES_OK : CLES_EFAILURE;
 }
 
 std::unique_ptr<SolverBase> make_solver(cles_ctx* ctx, const cles_solver_desc& desc) {

@@ -47,12 +47,29 @@ public:
     virtual double* state_device() = 0;
     virtual cles_solver_info info() const = 0;
 
+    // Graph mode: one run! iteration per CUDA-graph launch, with the timestep,
+    // the step-control floors and the clock kept on the device (no host read
+    // inside a step).  graph_begin captures the graphs; graph_launch enqueues one
+    // step and an asynchronous read of the clock into pinned memory, which
+    // graph_clock returns once the stream has been synchronised; graph_end
+    // copies the clock back into t / step.  No rate prediction, growth cap or
+    // rollback in this mode.
+    virtual void graph_begin(double tfinal, int64_t nmax) = 0;
+    virtual void graph_launch() = 0;
+    virtual const double* graph_clock() const = 0;
+    virtual void graph_end() = 0;
+    virtual cudaStream_t stream() const = 0;
+
     cles_solver_desc desc{};
     double t = 0.0, tstage = 0.0, dt_prev = 0.0, rate_prev = 0.0, cfl = 0.5;
     int64_t step_count = 0;
 };
 
 std::unique_ptr<SolverBase> make_solver(cles_ctx* ctx, const cles_solver_desc& desc);
+// Device bytes a solver of `desc` allocates (fields and plan tables), for admission control.
+size_t solver_bytes_estimate(const cles_solver_desc& desc);
+// run! in graph mode on one solver (same contract as SolverBase::run without retries).
+int run_graph(SolverBase& s, double tfinal, int64_t nmax, cles_run_result* res);
 
 // Host layout transfer of a component-slowest state between a host array in
 // `layout` and an interior device array (cudaMemcpy3DAsync per component).

@@ -326,6 +326,50 @@ typedef struct cles_profile_entry {
 int  cles_profile_enable(int on);
 int  cles_profile_read(cles_profile_entry* out, int max_entries, int* n_entries);
 
+/* run! in graph mode (no counterpart in the reference): every step is one
+ * CUDA-graph launch with the timestep, the check_step floors and the clock on
+ * the device, so no host round trip happens inside a step.  Same results as
+ * cles_run for the same state (bitwise in FP64); rate prediction, growth
+ * capping and rollback retries are not available in this mode (CLES_EINVAL). */
+int  cles_run_graph(cles_solver* s, double tfinal, int64_t nmax, cles_run_result* out);
+
+/* ---- serving: continuous batching of independent solves -----------------
+ * No counterpart in the reference (one problem per process there).  A server
+ * owns one device.  Requests (a solver descriptor, an initial state and an
+ * end time) are queued; every cles_server_tick admits queued requests in
+ * arrival order while the active count and the HBM budget allow, advances
+ * every running request by one run! step (one graph launch each, on its own
+ * stream, so the steps of different requests overlap on the device), and
+ * retires finished or failed ones, freeing their memory for the queue.  Each
+ * request's arithmetic is independent of the others, so its result is the
+ * same alone and in any mix.  Requests with rollback retries are stepped on
+ * the host instead of by graph. */
+typedef struct cles_server cles_server;
+#define CLES_REQ_QUEUED    0
+#define CLES_REQ_RUNNING   1
+#define CLES_REQ_DONE      2
+#define CLES_REQ_FAILED    3
+#define CLES_REQ_CANCELLED 4
+typedef struct cles_request_status {
+    int     state;          /* CLES_REQ_* */
+    int     failure;        /* CLES_FAIL_* when failed */
+    int64_t steps;
+    double  t;
+    double  submit_s;       /* seconds since server creation */
+    double  admit_s;        /* -1 while queued */
+    double  done_s;         /* -1 until finished */
+    size_t  device_bytes;   /* admission estimate */
+} cles_request_status;
+int  cles_server_create(int device, size_t hbm_budget_bytes, int max_active, cles_server** out);
+void cles_server_destroy(cles_server* s);
+int  cles_server_submit(cles_server* s, const cles_solver_desc* desc, const double* Q0_host, int layout,
+                        double tfinal, int64_t nmax, int64_t* id);
+int  cles_server_tick(cles_server* s, int* n_running, int* n_queued);
+int  cles_server_status(cles_server* s, int64_t id, cles_request_status* out);
+/* Final state of a finished request (same layout as submitted); releases it. */
+int  cles_server_fetch(cles_server* s, int64_t id, double* Q_host);
+int  cles_server_cancel(cles_server* s, int64_t id);
+
 /* Volume-averaged kinetic energy ∫½ρ|u|²dV / V and dissipation rate
  * (src/diagnostics.jl:354-378, bench/tgv_energy.jl:175-184) of the resident
  * state. */
