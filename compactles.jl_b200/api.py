@@ -337,6 +337,14 @@ class Solver:
     def set_clock(self, t, step, cfl):
         _check(lib().cles_set_clock(self.ptr, float(t), int(step), float(cfl)))
 
+    @property
+    def t(self):
+        return self.clock()[0]
+
+    @property
+    def steps(self):
+        return self.clock()[1]
+
     def run(self, tfinal, nmax=2 ** 62, raise_on_failure=True):
         """run!(solver, Q; tfinal, nmax) without callbacks (src/timestep.jl:277-405)."""
         res = abi.cles_run_result()

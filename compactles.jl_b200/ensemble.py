@@ -1,0 +1,114 @@
+"""Ensemble workload: many independent 2-D He/CO2 shock-interface solves on one GPU.
+
+64 cases from one seed (default 7): grid (nx, ny, 1) with nx and ny drawn
+log-uniform in [128, 1024] x [64, 256] and rounded to even, shock Mach number
+uniform in [1.2, 2.5], an 8-mode interface perturbation of its own seed, slip
+walls in x, periodic y, run to t_end = 0.5 Lx / c_He
+(compactles.jl_b200/scenarios.shock_interface_2d).  The whole ensemble is
+submitted at once to a cles_server and advanced by continuous batching, each
+request one CUDA-graph launch per step on its own stream; this is done in
+mixed precision and again in FP64 on the same GPU.
+
+Reported: aggregate cell-steps/s (sum over cases of cells x steps, over the
+wall time of the batch), solves/s, and per case the relative L2 difference of
+the mixed-precision end state from the FP64 end state (max over conserved
+components).
+
+  python compactles.jl_b200/ensemble.py [--cases 64] [--seed 7]
+"""
+import argparse
+import importlib.util
+import json
+import math
+import pathlib
+import sys
+import time
+
+import numpy as np
+
+HERE = pathlib.Path(__file__).resolve().parent
+
+
+def _package():
+    if "compactles_b200" in sys.modules:
+        return sys.modules["compactles_b200"]
+    spec = importlib.util.spec_from_file_location("compactles_b200", HERE / "__init__.py",
+                                                  submodule_search_locations=[str(HERE)])
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules["compactles_b200"] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def draw_cases(n, seed, nx_range=(128, 1024), ny_range=(64, 256)):
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n):
+        nx = 2 * int(round(math.exp(rng.uniform(*np.log(nx_range))) / 2))
+        ny = 2 * int(round(math.exp(rng.uniform(*np.log(ny_range))) / 2))
+        out.append((nx, ny, float(rng.uniform(1.2, 2.5)), int(rng.integers(1 << 31))))
+    return out
+
+
+def serve(cl, reqs, max_active, budget):
+    srv = cl.Server(hbm_budget=budget, max_active=max_active)
+    t0 = time.perf_counter()
+    ids = [srv.submit(desc, Q0, tf) for desc, Q0, tf in reqs]
+    srv.drain()
+    wall = time.perf_counter() - t0
+    states, steps = [], []
+    for rid in ids:
+        st = srv.status(rid)
+        if st["state"] != "done":
+            raise RuntimeError(f"request ended {st['state']} ({st['failure']})")
+        steps.append(st["steps"])
+        states.append(srv.fetch(rid))
+    return wall, steps, states
+
+
+def rel_l2(a, b, desc):
+    sl = (slice(None),) + _package().problem.interior_slices(desc)
+    a, b = a[sl], b[sl]
+    return max(float(np.linalg.norm(a[c] - b[c]) / max(np.linalg.norm(b[c]), 1e-300)) for c in range(a.shape[0]))
+
+
+def main(argv=None):
+    p = argparse.ArgumentParser()
+    p.add_argument("--cases", type=int, default=64)
+    p.add_argument("--seed", type=int, default=7)
+    p.add_argument("--max-active", type=int, default=64)
+    p.add_argument("--budget-gb", type=float, default=100.0)
+    p.add_argument("--precisions", default="mixed,fp64")
+    a = p.parse_args(argv)
+    cl = _package()
+    sch = (cl.lele_d1_6(), cl.compact_filter(0.45))
+    cases = draw_cases(a.cases, a.seed)
+    # warm the library outside the measurement
+    for prec in ("fp64", "mixed"):
+        wd = cl.scenarios.shock_interface_2d(sch, 64, 32, 1.5, 1, precision=prec)
+        s = cl.Solver(wd[0])
+        s.set_state(wd[1])
+        s.run_graph(wd[2], 5)
+        del s
+    res, states = {}, {}
+    for prec in a.precisions.split(","):
+        reqs = [cl.scenarios.shock_interface_2d(sch, nx, ny, M, sd, precision=prec) for nx, ny, M, sd in cases]
+        wall, steps, st = serve(cl, reqs, a.max_active, int(a.budget_gb * (1 << 30)))
+        cs = sum(nx * ny * k for (nx, ny, _, _), k in zip(cases, steps))
+        res[prec] = {"wall_s": wall, "cell_steps": cs, "cell_steps_per_s": cs / wall,
+                     "solves_per_s": len(cases) / wall, "steps_total": int(sum(steps))}
+        states[prec] = (reqs, st)
+    out = {"workload": f"{a.cases} 2-D He/CO2 shock-interface cases, seed {a.seed}, "
+                       "nx 128-1024, ny 64-256, t_end 0.5 Lx/c_He, served concurrently",
+           "results": res}
+    if "mixed" in states and "fp64" in states:
+        errs = [rel_l2(m, f, r[0]) for r, m, f in zip(states["fp64"][0], states["mixed"][1], states["fp64"][1])]
+        out["mixed_vs_fp64_rel_l2"] = {"max": max(errs), "median": float(np.median(errs)),
+                                       "per_case": [float(e) for e in errs]}
+        out["mixed_speedup"] = res["mixed"]["cell_steps_per_s"] / res["fp64"]["cell_steps_per_s"]
+    print(json.dumps(out), flush=True)
+    return out
+
+
+if __name__ == "__main__":
+    main()

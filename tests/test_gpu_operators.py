@@ -115,3 +115,23 @@ def test_spectral_accuracy_on_gpu():
 def test_plan_errors_match_plan_direction():
     with pytest.raises(cl.ClesError, match="too small"):
         cl.plan_direction(cl.grid((8, 12, 12), (1, 1, 1)), cl.compact_filter(0.45), 1, 0.1)
+
+
+@pytest.mark.parametrize("scheme", ["c6", "filt", "c10"])
+@pytest.mark.parametrize("periodic", [True, False])
+@pytest.mark.parametrize("ng,dim", [((1024, 64, 1), 1), ((768, 48, 1), 1), ((8192, 1, 1), 1), ((300, 256, 1), 2),
+                                    ((2000, 3, 1), 1), ((9, 9, 1024), 3)])
+def test_apply_along_long_lines(orc, scheme, periodic, ng, dim):
+    """Line lengths of the 2-D ensemble and the 1-D tubes (up to 8192 cells),
+    with the other dimensions collapsed or short."""
+    per = tuple(1 if (k != dim - 1 or periodic or ng[k] == 1) else 0 for k in range(3))
+    g = orc.grid(ng, per)
+    f = _field(orc, g, seed=ng[dim - 1] + dim)
+    h = 1.3 / ng[dim - 1]
+    ref = orc.interior(g, orc.Plan(g, _schemes(orc, scheme), dim, h).apply(f))
+    plan = cl.plan_direction(cl.grid(ng, per), _schemes(cl, scheme), dim, h)
+    out = np.zeros_like(f)
+    cl.apply_along(out, plan, f)
+    got = orc.interior(g, out)
+    err = np.abs(got - ref).max() / np.abs(ref).max()
+    assert err < 1e-12, err
