@@ -69,6 +69,12 @@ struct CompactParams {
     int64_t off_f0, off_f1, off_f2, off_f3, off_f4;  // q=1: l, dinv, c ; q=2: L1, L2, U1, U2, Uinv0
     int64_t off_V, off_W;                              // V[s][t][i], W[s][t][i]
     int64_t off_G;                                     // reduced inverse, (2qS) x (2qS) row-major
+    // Closed tridiagonal lines: the interface system is solved by parallel
+    // cyclic reduction with precomputed 2x2 blocks instead of the dense inverse.
+    // Level l (distance 2^l), segment s: alpha[4], gamma[4] at off_pcr + (l*S + s)*8,
+    // then the final 2x2 inverse of segment s at off_pcr + (pcr_levels*S + s)*8.
+    int pcr, pcr_levels;
+    int64_t off_pcr;
     int64_t lines;
 };
 
@@ -99,9 +105,23 @@ struct TileLineParams {
 };
 
 // Host-side plan: parameters plus the coefficient tables on the device.
+// General tile form (closed lines, or the pentadiagonal C10): with equal
+// segments only three segment classes exist -- the first (closure rows, no
+// left spike), the interior ones (all alike) and the last -- so their
+// factorisations and spikes travel as kernel parameters with static indices.
+// f: q = 1 -> l, dinv, c; q = 2 -> L1, L2, U1, U2, 1/U0 (same as the table).
+struct TileGenParams {
+    double f[3][5][kMaxSeg];
+    double v[3][2][kMaxSeg], w[3][2][kMaxSeg];
+    float ff[3][5][kMaxSeg];
+    float vf[3][2][kMaxSeg], wf[3][2][kMaxSeg];
+};
+
 struct CompactPlan {
     bool has_tl = false;
     TileLineParams TL;
+    bool has_tg = false;   // y/z lines fit the general tile kernel (closures, q = 2)
+    TileGenParams TG;
     bool has_xw = false;
     WarpLineParams XW;
     CompactParams P;
@@ -133,6 +153,10 @@ struct RkEpilogue {
 // TMA-pipelined y/z launch; false when the plan or the views do not qualify.
 bool try_launch_tma(const CompactPlan& plan, const FieldView& in, const FieldView& out, int count, int mode,
                     cudaStream_t st, const RkEpilogue* rk = nullptr);
+// x lines of a plan with the general tile form: persistent kernel, cp.async
+// staging into a transposed shared-memory tile; false if the plan does not fit.
+bool try_launch_xt(const CompactPlan& plan, const FieldView& in, const FieldView& out, int count, int mode,
+                   cudaStream_t st);
 // Flux divergence of the last direction fused with the RK update; false (and
 // nothing launched) when the plan does not take the TMA path.
 bool launch_compact_rk(const CompactPlan& plan, const FieldView& in, const FieldView& out, int count,

@@ -69,6 +69,24 @@ template <typename T, bool LOAD>
 __device__ __forceinline__ void tile_rows(const CompactParams& P, const FieldView& v, T* g_field, T* tile, int line0,
                                           int nl, int n, int TP, int mode) {
     const int nt = blockDim.x;
+    if (nl * 32 <= nt) {
+        // few rows (long lines, few per CTA): the whole block strides each row
+        for (int l = 0; l < nl; ++l) {
+            const LineMap Ll = line_map(P, v, line0 + l);
+            T* row = g_field + Ll.base;
+            for (int g = threadIdx.x; g < n; g += nt) {
+                if (LOAD) {
+                    tile[g * TP + l] = row[g];
+                } else {
+                    const T val = tile[g * TP + l];
+                    if (mode == OUT_STORE) row[g] = val;
+                    else if (mode == OUT_NEGATE) row[g] = -val;
+                    else row[g] = row[g] - val;
+                }
+            }
+        }
+        return;
+    }
     const int tpr = nt < 32 ? nt : 32;
     const int rows_per_pass = nt / tpr;
     const int r = threadIdx.x / tpr, c = threadIdx.x - (threadIdx.x / tpr) * tpr;
@@ -89,9 +107,9 @@ __device__ __forceinline__ void tile_rows(const CompactParams& P, const FieldVie
     }
 }
 
-template <typename T, int Q, int M, bool XMODE>
-__global__ void __launch_bounds__(512) k_compact(const CompactParams P, const T* __restrict__ tab, const FieldView in,
-                                                  const FieldView out, const int mode) {
+template <typename T, int Q, int M, bool XMODE, int MS>
+__global__ void __launch_bounds__(512) k_compact(const __grid_constant__ CompactParams P, const T* __restrict__ tab,
+                                                  const FieldView in, const FieldView out, const int mode) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T* smem = reinterpret_cast<T*>(smem_raw);
     const int LB = P.LB, S = P.S, n = P.n;
@@ -120,7 +138,7 @@ __global__ void __launch_bounds__(512) k_compact(const CompactParams P, const T*
         tile_rows<T, true>(P, in, const_cast<T*>(fin), tile, line0, nl, n, TP, 0);
         __syncthreads();
     }
-    constexpr int WN = kMaxSeg + 2 * M;
+    constexpr int WN = MS + 2 * M;
     T w[WN];
 #pragma unroll
     for (int j = 0; j < WN; ++j) {
@@ -138,13 +156,13 @@ __global__ void __launch_bounds__(512) k_compact(const CompactParams P, const T*
     };
 
     // ---- 2. fill -----------------------------------------------------------
-    T y[kMaxSeg];
+    T y[MS];
     const T a0 = T(P.a0);
     T ci[M];
 #pragma unroll
     for (int k = 0; k < M; ++k) ci[k] = T(P.ci[k]);
 #pragma unroll
-    for (int i = 0; i < kMaxSeg; ++i) {
+    for (int i = 0; i < MS; ++i) {
         if (i < m) {
             T acc;
             if (P.symmetric) {
@@ -173,7 +191,7 @@ __global__ void __launch_bounds__(512) k_compact(const CompactParams P, const T*
     }
     if (P.hi_closed && seg == S - 1) {
 #pragma unroll
-        for (int i = 0; i < kMaxSeg; ++i) {
+        for (int i = 0; i < MS; ++i) {
             if (i < m && i >= m - P.nc) {
                 const int jr = m - 1 - i;
                 T acc = T(0);
@@ -189,39 +207,87 @@ __global__ void __launch_bounds__(512) k_compact(const CompactParams P, const T*
     const T* f2 = tab + P.off_f2 + (int64_t)seg * kMaxSeg;
     if (Q == 1) {
 #pragma unroll
-        for (int i = 1; i < kMaxSeg; ++i)
+        for (int i = 1; i < MS; ++i)
             if (i < m) y[i] -= ldg(f0 + i) * y[i - 1];
 #pragma unroll
-        for (int i = 0; i < kMaxSeg; ++i)
+        for (int i = 0; i < MS; ++i)
             if (i == m - 1) y[i] *= ldg(f1 + i);
 #pragma unroll
-        for (int i = kMaxSeg - 2; i >= 0; --i)
+        for (int i = MS - 2; i >= 0; --i)
             if (i < m - 1) y[i] = (y[i] - ldg(f2 + i) * y[i + 1]) * ldg(f1 + i);
     } else {
         const T* f3 = tab + P.off_f3 + (int64_t)seg * kMaxSeg;
         const T* f4 = tab + P.off_f4 + (int64_t)seg * kMaxSeg;
 #pragma unroll
-        for (int k = 0; k < kMaxSeg - 1; ++k) {
+        for (int k = 0; k < MS - 1; ++k) {
             if (k < m - 1) y[k + 1] -= ldg(f0 + k) * y[k];
-            if (k + 2 < kMaxSeg && k < m - 2) y[k + 2] -= ldg(f1 + k) * y[k];
+            if (k + 2 < MS && k < m - 2) y[k + 2] -= ldg(f1 + k) * y[k];
         }
 #pragma unroll
-        for (int i = kMaxSeg - 1; i >= 0; --i) {
+        for (int i = MS - 1; i >= 0; --i) {
             if (i < m) {
                 T acc = y[i];
-                if (i + 1 < kMaxSeg && i + 1 < m) acc -= ldg(f2 + i) * y[i + 1];
-                if (i + 2 < kMaxSeg && i + 2 < m) acc -= ldg(f3 + i) * y[i + 2];
+                if (i + 1 < MS && i + 1 < m) acc -= ldg(f2 + i) * y[i + 1];
+                if (i + 2 < MS && i + 2 < m) acc -= ldg(f3 + i) * y[i + 2];
                 y[i] = acc * ldg(f4 + i);
             }
         }
     }
 
     // ---- 4. interface solve -----------------------------------------------
-    if (P.hasred) {
+    if (Q == 1 && P.pcr) {
+        // closed tridiagonal line: block cyclic reduction of the interface
+        // system in X_s = (head_s, tail_s) with precomputed 2x2 blocks,
+        // double-buffered in shared memory (4 S values per line)
+        T tail = T(0);
+#pragma unroll
+        for (int i = 0; i < MS; ++i)
+            if (i == m - 1) tail = y[i];
+        T* cur = red + (size_t)lane * 4 * S;
+        T* nxt = cur + 2 * S;
+        cur[2 * seg] = y[0];
+        cur[2 * seg + 1] = tail;
+        __syncthreads();
+        const T* pc = tab + P.off_pcr + (int64_t)seg * 8;
+        for (int l = 0; l < P.pcr_levels; ++l) {
+            const int k = 1 << l;
+            const T* c = pc + (int64_t)l * S * 8;
+            T r0 = cur[2 * seg], r1 = cur[2 * seg + 1];
+            if (seg - k >= 0) {
+                const T p0 = cur[2 * (seg - k)], p1 = cur[2 * (seg - k) + 1];
+                r0 += ldg(c + 0) * p0 + ldg(c + 1) * p1;
+                r1 += ldg(c + 2) * p0 + ldg(c + 3) * p1;
+            }
+            if (seg + k < S) {
+                const T p0 = cur[2 * (seg + k)], p1 = cur[2 * (seg + k) + 1];
+                r0 += ldg(c + 4) * p0 + ldg(c + 5) * p1;
+                r1 += ldg(c + 6) * p0 + ldg(c + 7) * p1;
+            }
+            nxt[2 * seg] = r0;
+            nxt[2 * seg + 1] = r1;
+            __syncthreads();
+            T* t = cur; cur = nxt; nxt = t;
+        }
+        {
+            // nxt was last read before the final barrier: it takes the solution
+            const T* bi = pc + (int64_t)P.pcr_levels * S * 8;
+            const T r0 = cur[2 * seg], r1 = cur[2 * seg + 1];
+            nxt[2 * seg] = ldg(bi + 0) * r0 + ldg(bi + 1) * r1;
+            nxt[2 * seg + 1] = ldg(bi + 2) * r0 + ldg(bi + 3) * r1;
+        }
+        __syncthreads();
+        const T zp = seg > 0 ? nxt[2 * (seg - 1) + 1] : T(0);      // tail of the previous segment
+        const T zn = seg < S - 1 ? nxt[2 * (seg + 1)] : T(0);      // head of the next segment
+        const T* V = tab + P.off_V + (int64_t)seg * kMaxSeg;
+        const T* W = tab + P.off_W + (int64_t)seg * kMaxSeg;
+#pragma unroll
+        for (int i = 0; i < MS; ++i)
+            if (i < m) y[i] -= ldg(V + i) * zp + ldg(W + i) * zn;
+    } else if (P.hasred) {
         const int RP = N + 1;  // pitch of the per-line interface vector
         T* rl = red + (size_t)lane * RP;
 #pragma unroll
-        for (int i = 0; i < kMaxSeg; ++i) {
+        for (int i = 0; i < MS; ++i) {
             if (i < Q) rl[2 * Q * seg + i] = y[i];
             if (i < m && i >= m - Q) rl[2 * Q * seg + Q + (i - (m - Q))] = y[i];
         }
@@ -255,7 +321,7 @@ __global__ void __launch_bounds__(512) k_compact(const CompactParams P, const T*
         const T* V = tab + P.off_V + (int64_t)seg * Q * kMaxSeg;
         const T* W = tab + P.off_W + (int64_t)seg * Q * kMaxSeg;
 #pragma unroll
-        for (int i = 0; i < kMaxSeg; ++i) {
+        for (int i = 0; i < MS; ++i) {
             if (i < m) {
                 T acc = T(0);
 #pragma unroll
@@ -269,7 +335,7 @@ __global__ void __launch_bounds__(512) k_compact(const CompactParams P, const T*
     if (XMODE) {
         __syncthreads();  // every window/closure read of the tile is done
 #pragma unroll
-        for (int i = 0; i < kMaxSeg; ++i)
+        for (int i = 0; i < MS; ++i)
             if (i < m) tile[(off + i) * TP + lane] = y[i];
         __syncthreads();
         tile_rows<T, false>(P, out, fout, tile, line0, nl, n, TP, mode);
@@ -279,7 +345,7 @@ __global__ void __launch_bounds__(512) k_compact(const CompactParams P, const T*
         // line belongs to one thread, and different CTAs own disjoint lines.
         if (!valid) return;
 #pragma unroll
-        for (int i = 0; i < kMaxSeg; ++i) {
+        for (int i = 0; i < MS; ++i) {
             if (i < m) {
                 T* o = fout + Lout.base + (int64_t)(off + i) * Lout.stride;
                 if (mode == OUT_STORE) *o = y[i];
@@ -442,14 +508,15 @@ bool try_launch_xw(const CompactPlan& plan, const FieldView& in, const FieldView
     }
 }
 
-template <typename T, int Q, int M, bool X>
+template <typename T, int Q, int M, bool X, int MS>
 void launch_t(const CompactParams& P, const T* tab, const FieldView& in, const FieldView& out, int count, int mode,
               cudaStream_t st) {
     const int N = 2 * Q * P.S;
     size_t smem = 0;
     if (X) smem += sizeof(T) * (size_t)P.n * (P.LB + 1);
-    if (P.hasred) smem += sizeof(T) * (size_t)P.LB * (N + 1);
-    auto kern = k_compact<T, Q, M, X>;
+    if (P.pcr) smem += sizeof(T) * (size_t)P.LB * 4 * P.S;
+    else if (P.hasred) smem += sizeof(T) * (size_t)P.LB * (N + 1);
+    auto kern = k_compact<T, Q, M, X, MS>;
     static thread_local int configured = 0;
     if (smem > 48 * 1024 && configured < (int)smem) {
         CLES_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -465,11 +532,26 @@ void launch_t(const CompactParams& P, const T* tab, const FieldView& in, const F
 template <typename T, int Q, bool X>
 void dispatch_m(const CompactParams& P, const T* tab, const FieldView& in, const FieldView& out, int count, int mode,
                 cudaStream_t st) {
+    // shorter register tiles for the short segments of few-line closed plans
+    const int mmax = P.seg_base + (P.seg_rem ? 1 : 0);
+    if constexpr (Q == 1) {
+      if (mmax <= 16 && P.M != 3) {
+        const bool eight = mmax <= 8;
+        switch (P.M) {
+            case 1: eight ? launch_t<T, Q, 1, X, 8>(P, tab, in, out, count, mode, st)
+                          : launch_t<T, Q, 1, X, 16>(P, tab, in, out, count, mode, st); return;
+            case 2: eight ? launch_t<T, Q, 2, X, 8>(P, tab, in, out, count, mode, st)
+                          : launch_t<T, Q, 2, X, 16>(P, tab, in, out, count, mode, st); return;
+            default: eight ? launch_t<T, Q, 4, X, 8>(P, tab, in, out, count, mode, st)
+                           : launch_t<T, Q, 4, X, 16>(P, tab, in, out, count, mode, st); return;
+        }
+      }
+    }
     switch (P.M) {
-        case 1: launch_t<T, Q, 1, X>(P, tab, in, out, count, mode, st); break;
-        case 2: launch_t<T, Q, 2, X>(P, tab, in, out, count, mode, st); break;
-        case 3: launch_t<T, Q, 3, X>(P, tab, in, out, count, mode, st); break;
-        case 4: launch_t<T, Q, 4, X>(P, tab, in, out, count, mode, st); break;
+        case 1: launch_t<T, Q, 1, X, kMaxSeg>(P, tab, in, out, count, mode, st); break;
+        case 2: launch_t<T, Q, 2, X, kMaxSeg>(P, tab, in, out, count, mode, st); break;
+        case 3: launch_t<T, Q, 3, X, kMaxSeg>(P, tab, in, out, count, mode, st); break;
+        case 4: launch_t<T, Q, 4, X, kMaxSeg>(P, tab, in, out, count, mode, st); break;
         default: throw Error(CLES_EINVAL, "unsupported stencil half-width");
     }
 }
@@ -499,10 +581,12 @@ void launch_compact(const CompactPlan& plan, const FieldView& in, const FieldVie
         rec = prof_begin(st, plan.P.dim, pts * el * (mode == OUT_SUBTRACT ? 3.0 : 2.0));
     }
     if (plan.dtype == CLES_F64) {
-        if (!try_launch_xw<double>(plan, in, out, count, mode, st) && !try_launch_tma(plan, in, out, count, mode, st))
+        if (!try_launch_xw<double>(plan, in, out, count, mode, st) && !try_launch_xt(plan, in, out, count, mode, st) &&
+            !try_launch_tma(plan, in, out, count, mode, st))
             dispatch<double>(plan.P, plan.tab64, in, out, count, mode, st);
     } else {
-        if (!try_launch_xw<float>(plan, in, out, count, mode, st) && !try_launch_tma(plan, in, out, count, mode, st))
+        if (!try_launch_xw<float>(plan, in, out, count, mode, st) && !try_launch_xt(plan, in, out, count, mode, st) &&
+            !try_launch_tma(plan, in, out, count, mode, st))
             dispatch<float>(plan.P, plan.tab32, in, out, count, mode, st);
     }
     if (rec >= 0) prof_end(rec, st);

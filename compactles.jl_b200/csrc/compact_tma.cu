@@ -1,4 +1,6 @@
-// TMA-pipelined compact operator for periodic tridiagonal y/z lines.
+// TMA-pipelined compact operators for y/z lines: periodic tridiagonal lines
+// with identical segments (k_compact_tma), and closed or pentadiagonal lines
+// with per-segment tables (k_compact_tg).
 //
 // y and z lines are strided in memory (x is contiguous), so a group of 32
 // consecutive-x lines is a 2-D box {32 x, n along the line} of the field: one
@@ -270,6 +272,454 @@ __global__ void __launch_bounds__(256, 1)
     }
 }
 
+template <typename T>
+__device__ __forceinline__ T tgv(const double* d, const float* f, int i) {
+    if (sizeof(T) == 8) return T(d[i]);
+    return T(f[i]);
+}
+
+// Local solve of one segment of class CLS (0 first, 1 interior, 2 last).
+template <typename T, int Q, int MS, int CLS>
+__device__ __forceinline__ void tg_solve(const TileGenParams& G, T (&y)[MS]) {
+    if (Q == 1) {
+#pragma unroll
+        for (int i = 1; i < MS; ++i) y[i] -= tgv<T>(G.f[CLS][0], G.ff[CLS][0], i) * y[i - 1];
+        y[MS - 1] *= tgv<T>(G.f[CLS][1], G.ff[CLS][1], MS - 1);
+#pragma unroll
+        for (int i = MS - 2; i >= 0; --i)
+            y[i] = (y[i] - tgv<T>(G.f[CLS][2], G.ff[CLS][2], i) * y[i + 1]) * tgv<T>(G.f[CLS][1], G.ff[CLS][1], i);
+    } else {
+#pragma unroll
+        for (int k = 0; k < MS - 1; ++k) {
+            y[k + 1] -= tgv<T>(G.f[CLS][0], G.ff[CLS][0], k) * y[k];
+            if (k + 2 < MS) y[k + 2] -= tgv<T>(G.f[CLS][1], G.ff[CLS][1], k) * y[k];
+        }
+#pragma unroll
+        for (int i = MS - 1; i >= 0; --i) {
+            T acc = y[i];
+            if (i + 1 < MS) acc -= tgv<T>(G.f[CLS][2], G.ff[CLS][2], i) * y[i + 1];
+            if (i + 2 < MS) acc -= tgv<T>(G.f[CLS][3], G.ff[CLS][3], i) * y[i + 2];
+            y[i] = acc * tgv<T>(G.f[CLS][4], G.ff[CLS][4], i);
+        }
+    }
+}
+
+template <typename T, int Q, int MS, int CLS>
+__device__ __forceinline__ void tg_correct(const TileGenParams& G, T (&y)[MS], const T (&zp)[Q], const T (&zn)[Q]) {
+#pragma unroll
+    for (int i = 0; i < MS; ++i) {
+        T acc = T(0);
+#pragma unroll
+        for (int t = 0; t < Q; ++t)
+            acc += tgv<T>(G.v[CLS][t], G.vf[CLS][t], i) * zp[t] + tgv<T>(G.w[CLS][t], G.wf[CLS][t], i) * zn[t];
+        y[i] -= acc;
+    }
+}
+
+// General tile kernel: the same pipeline for y/z lines whose segments are not
+// all alike -- closed lines (closure rows in the first and last segment, spikes
+// that stop at the ends) and the pentadiagonal C10 scheme (q = 2, two head and
+// two tail values per segment).  Segment coefficients come from the plan's
+// three segment classes (first, interior, last) as kernel parameters, the
+// closure stencils read the whole line from the tile, and the reduced inverse
+// (2qS)^2 sits in shared memory.
+template <typename T, int Q, int M, int MS>
+__global__ void __launch_bounds__(256, 1)
+    k_compact_tg(const __grid_constant__ CUtensorMap map, const __grid_constant__ CompactParams P,
+                 const __grid_constant__ TileGenParams GP, const T* __restrict__ tab, const FieldView out,
+                 const int mode, const int count, const int NS, const RkEpilogue rk) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    const int n = P.n, S = P.S;
+    constexpr int m = MS;  // points per segment (all segments equal at launch)
+    const int N = 2 * Q * S;
+    const size_t tile_elems = (size_t)n * kLanes;
+    T* tiles = reinterpret_cast<T*>(smem_raw);
+    uint64_t* bars = reinterpret_cast<uint64_t*>(smem_raw + sizeof(T) * tile_elems * NS);
+    T* red = reinterpret_cast<T*>(bars + 8);
+    const int RP = N + 1;
+    T* Gs = red + (size_t)kLanes * RP;
+
+    const int tid = threadIdx.x;
+    const int lane = tid & 31;
+    const int seg = tid >> 5;
+    const int off = seg * m;
+    const bool periodic = P.periodic != 0;
+    const int gx = (P.nx + kLanes - 1) / kLanes;
+    const int other = P.dim == 1 ? P.nz : P.ny;
+    const int groups = gx * other;
+    const int work = groups * count;
+
+    if (tid == 0) {
+        for (int s = 0; s < NS; ++s) mbar_init(&bars[s], 1);
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    }
+    for (int i = tid; i < N * N; i += blockDim.x) Gs[i] = tab[P.off_G + i];
+    __syncthreads();
+
+    const unsigned tile_bytes = (unsigned)(sizeof(T) * tile_elems);
+    auto issue = [&](int w, int s) {
+        const int c = w / groups, g = w - (w / groups) * groups;
+        const int x0 = (g % gx) * kLanes, o = g / gx;
+        mbar_expect_tx(&bars[s], tile_bytes);
+        if (P.dim == 1) tma_load_4d(tiles + tile_elems * s, &map, &bars[s], x0, 0, o, c);
+        else tma_load_4d(tiles + tile_elems * s, &map, &bars[s], x0, o, 0, c);
+    };
+    if (tid == 0)
+        for (int s = 0; s < NS; ++s) {
+            const int w = blockIdx.x + s * gridDim.x;
+            if (w < work) issue(w, s);
+        }
+
+    const T a0 = T(P.a0);
+    T ci[M];
+#pragma unroll
+    for (int k = 0; k < M; ++k) ci[k] = T(P.ci[k]);
+    const int cls = seg == 0 ? 0 : (seg == S - 1 ? 2 : 1);   // warp-uniform
+    const bool has_prev = periodic || seg > 0;
+    const bool has_next = periodic || seg < S - 1;
+    const int prev = seg == 0 ? S - 1 : seg - 1;
+    const int next = seg == S - 1 ? 0 : seg + 1;
+
+    int it = 0;
+    for (int w = blockIdx.x; w < work; w += gridDim.x, ++it) {
+        const int stage = it % NS;
+        const unsigned parity = (unsigned)((it / NS) & 1);
+        const bool ok = mbar_wait_bounded(&bars[stage], parity);
+        if (__syncthreads_or(!ok)) {
+            if (tid == 0) atomicAdd(&g_wait_timeouts, 1);
+            return;
+        }
+        const T* tile = tiles + tile_elems * stage;
+        // ---- fill: interior stencil, closure rows at closed edges ----
+        T y[MS];
+        {
+            T wv[MS + 2 * M];
+#pragma unroll
+            for (int j = 0; j < MS + 2 * M; ++j) {
+                int g = off - M + j;
+                if (periodic) g = g < 0 ? g + n : (g >= n ? g - n : g);
+                else g = g < 0 ? 0 : (g >= n ? n - 1 : g);  // clamped values are never used
+                wv[j] = tile[g * kLanes + lane];
+            }
+#pragma unroll
+            for (int i = 0; i < MS; ++i) {
+                T acc;
+                if (P.symmetric) {
+                    acc = a0 * wv[i + M];
+#pragma unroll
+                    for (int k = 1; k <= M; ++k) acc += ci[k - 1] * (wv[i + M + k] + wv[i + M - k]);
+                } else {
+                    acc = T(0);
+#pragma unroll
+                    for (int k = 1; k <= M; ++k) acc += ci[k - 1] * (wv[i + M + k] - wv[i + M - k]);
+                }
+                y[i] = acc;
+            }
+        }
+        if (!periodic) {
+            if (seg == 0) {
+#pragma unroll
+                for (int i = 0; i < kMaxClo; ++i) {
+                    if (i < P.nc) {
+                        T acc = T(0);
+#pragma unroll
+                        for (int k = 0; k < kMaxCloLen; ++k)
+                            if (k < P.clo_len[i]) acc += T(P.clo[i][k]) * tile[k * kLanes + lane];
+                        y[i] = acc;
+                    }
+                }
+            }
+            if (seg == S - 1) {
+#pragma unroll
+                for (int i = MS - kMaxClo; i < MS; ++i) {
+                    if (i >= m - P.nc) {
+                        T acc = T(0);
+#pragma unroll
+                        for (int k = 0; k < kMaxCloLen; ++k)
+                            if (k < P.clo_len[m - 1 - i]) acc += T(P.chi[m - 1 - i][k]) * tile[(n - 1 - k) * kLanes + lane];
+                        y[i] = acc;
+                    }
+                }
+            }
+        }
+        __syncthreads();  // the tile is consumed: refill it with a later group
+        if (tid == 0) {
+            const int w2 = w + NS * gridDim.x;
+            if (w2 < work) issue(w2, stage);
+        }
+        // ---- local solve with this segment's factorisation ----
+        if (cls == 0) tg_solve<T, Q, MS, 0>(GP, y);
+        else if (cls == 1) tg_solve<T, Q, MS, 1>(GP, y);
+        else tg_solve<T, Q, MS, 2>(GP, y);
+        // ---- interface values: heads and tails, then the reduced inverse ----
+        T* rl = red + (size_t)lane * RP;
+#pragma unroll
+        for (int t = 0; t < Q; ++t) {
+            rl[2 * Q * seg + t] = y[t];
+            rl[2 * Q * seg + Q + t] = y[MS - Q + t];
+        }
+        __syncthreads();
+        T zp[Q], zn[Q];
+#pragma unroll
+        for (int t = 0; t < Q; ++t) {
+            zp[t] = T(0);
+            zn[t] = T(0);
+            if (has_prev) {
+                const T* g = Gs + (size_t)(2 * Q * prev + Q + t) * N;
+                T acc = T(0);
+                for (int j = 0; j < N; ++j) acc += g[j] * rl[j];
+                zp[t] = acc;
+            }
+            if (has_next) {
+                const T* g = Gs + (size_t)(2 * Q * next + t) * N;
+                T acc = T(0);
+                for (int j = 0; j < N; ++j) acc += g[j] * rl[j];
+                zn[t] = acc;
+            }
+        }
+        if (cls == 0) tg_correct<T, Q, MS, 0>(GP, y, zp, zn);
+        else if (cls == 1) tg_correct<T, Q, MS, 1>(GP, y, zp, zn);
+        else tg_correct<T, Q, MS, 2>(GP, y, zp, zn);
+        // ---- store ----
+        const int c = w / groups, g = w - (w / groups) * groups;
+        const int x = (g % gx) * kLanes + lane, o = g / gx;
+        if (x < P.nx) {
+            T* base = reinterpret_cast<T*>(out.base) + (int64_t)c * out.comp_stride + x;
+            int64_t st, ob;
+            if (P.dim == 1) { st = out.sy; ob = (int64_t)o * out.sz; }
+            else { st = out.sz; ob = (int64_t)o * out.sy; }
+            base += ob + (int64_t)off * st;
+            if (mode == OUT_RK) {
+                const int64_t eo = (int64_t)c * out.comp_stride + x + ob + (int64_t)off * st;
+                const double rdt = rk.dtp ? *rk.dtp : rk.dt;
+                double* Qp = rk.Q + eo;
+                double* dp = rk.du + eo;
+#pragma unroll
+                for (int i0 = 0; i0 < MS; i0 += 8) {
+                    T o8[8];
+                    double dv[8], qv[8];
+#pragma unroll
+                    for (int q = 0; q < 8; ++q) {
+                        o8[q] = base[(int64_t)(i0 + q) * st];
+                        dv[q] = dp[(int64_t)(i0 + q) * st];
+                        qv[q] = Qp[(int64_t)(i0 + q) * st];
+                    }
+#pragma unroll
+                    for (int q = 0; q < 8; ++q) {
+                        const T dq = o8[q] - y[i0 + q];
+                        const double v = rk.A * dv[q] + rdt * double(dq);
+                        dp[(int64_t)(i0 + q) * st] = v;
+                        Qp[(int64_t)(i0 + q) * st] = qv[q] + rk.B * v;
+                    }
+                }
+            } else if (mode == OUT_SUBTRACT) {
+#pragma unroll
+                for (int i0 = 0; i0 < MS; i0 += 8) {
+                    T o8[8];
+#pragma unroll
+                    for (int q = 0; q < 8; ++q) o8[q] = base[(int64_t)(i0 + q) * st];
+#pragma unroll
+                    for (int q = 0; q < 8; ++q) base[(int64_t)(i0 + q) * st] = o8[q] - y[i0 + q];
+                }
+            } else {
+#pragma unroll
+                for (int i = 0; i < MS; ++i) base[(int64_t)i * st] = mode == OUT_NEGATE ? -y[i] : y[i];
+            }
+        }
+    }
+}
+
+// x lines in the general tile form.  x is the contiguous direction, so a
+// group of 32 lines is 32 rows of the field: every warp copies whole rows with
+// coalesced 4/8-byte cp.async into a transposed shared-memory tile
+// tile[g * 33 + lane] (pitch 33: the column reads of the segment threads and
+// the row writes of the copies are both free of bank conflicts).  NS tiles are
+// in flight; the compute is that of k_compact_tg (three segment classes,
+// closures, reduced inverse in shared memory); results go back through a
+// second transposed tile so that the stores are coalesced rows again.
+__device__ __forceinline__ void cp_async_el(void* dst, const void* src, int bytes) {
+    if (bytes == 8)
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_addr(dst)), "l"(src) : "memory");
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(smem_addr(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
+template <typename T, int Q, int M, int MS, int NS>
+__global__ void __launch_bounds__(256, 1)
+    k_compact_xt(const __grid_constant__ CompactParams P, const __grid_constant__ TileGenParams GP,
+                 const T* __restrict__ tab, const FieldView in, const FieldView out, const int mode, const int count) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    constexpr int TP = kLanes + 1;
+    const int n = P.n, S = P.S;
+    constexpr int m = MS;
+    const int N = 2 * Q * S;
+    const size_t tile_elems = (size_t)n * TP;
+    T* tin = reinterpret_cast<T*>(smem_raw);
+    T* tout = tin + tile_elems * NS;
+    T* red = tout + tile_elems;
+    const int RP = N + 1;
+    T* Gs = red + (size_t)kLanes * RP;
+
+    const int tid = threadIdx.x;
+    const int lane = tid & 31;
+    const int seg = tid >> 5;           // also the warp index
+    const int nwarps = blockDim.x >> 5;
+    const int off = seg * m;
+    const bool periodic = P.periodic != 0;
+    const int64_t lines = P.lines;
+    const int groups = (int)((lines + kLanes - 1) / kLanes);
+    const int work = groups * count;
+    const int cls = seg == 0 ? 0 : (seg == S - 1 ? 2 : 1);
+    const bool has_prev = periodic || seg > 0;
+    const bool has_next = periodic || seg < S - 1;
+    const int prev = seg == 0 ? S - 1 : seg - 1;
+    const int next = seg == S - 1 ? 0 : seg + 1;
+
+    for (int i = tid; i < N * N; i += blockDim.x) Gs[i] = tab[P.off_G + i];
+
+    auto row_of = [&](const FieldView& v, int line) -> int64_t {
+        const int j = line % P.ny, k = line / P.ny;
+        return (int64_t)j * v.sy + (int64_t)k * v.sz;
+    };
+    // warp w copies rows w, w + nwarps, ...; lane strides the row
+    auto issue = [&](int w, int s) {
+        if (w < work) {
+            const int c = w / groups, g0 = (w - c * groups) * kLanes;
+            const T* base = reinterpret_cast<const T*>(in.base) + (int64_t)c * in.comp_stride;
+            T* dst = tin + tile_elems * s;
+            for (int l = seg; l < kLanes; l += nwarps) {
+                const int line = g0 + l;
+                if (line >= lines) break;
+                const T* row = base + row_of(in, line);
+                for (int g = lane; g < n; g += kLanes) cp_async_el(dst + (size_t)g * TP + l, row + g, (int)sizeof(T));
+            }
+        }
+        cp_async_commit();   // an empty group keeps the count in step
+    };
+#pragma unroll
+    for (int s = 0; s < NS; ++s) issue(blockIdx.x + s * gridDim.x, s);
+
+    const T a0 = T(P.a0);
+    T ci[M];
+#pragma unroll
+    for (int k = 0; k < M; ++k) ci[k] = T(P.ci[k]);
+
+    int it = 0;
+    for (int w = blockIdx.x; w < work; w += gridDim.x, ++it) {
+        const int stage = it % NS;
+        cp_async_wait<NS - 1>();
+        __syncthreads();   // this group's rows are in the tile for every thread
+        const T* tile = tin + tile_elems * stage;
+        T y[MS];
+        {
+            T wv[MS + 2 * M];
+#pragma unroll
+            for (int j = 0; j < MS + 2 * M; ++j) {
+                int g = off - M + j;
+                if (periodic) g = g < 0 ? g + n : (g >= n ? g - n : g);
+                else g = g < 0 ? 0 : (g >= n ? n - 1 : g);
+                wv[j] = tile[g * TP + lane];
+            }
+#pragma unroll
+            for (int i = 0; i < MS; ++i) {
+                T acc;
+                if (P.symmetric) {
+                    acc = a0 * wv[i + M];
+#pragma unroll
+                    for (int k = 1; k <= M; ++k) acc += ci[k - 1] * (wv[i + M + k] + wv[i + M - k]);
+                } else {
+                    acc = T(0);
+#pragma unroll
+                    for (int k = 1; k <= M; ++k) acc += ci[k - 1] * (wv[i + M + k] - wv[i + M - k]);
+                }
+                y[i] = acc;
+            }
+        }
+        if (!periodic) {
+            if (seg == 0) {
+#pragma unroll
+                for (int i = 0; i < kMaxClo; ++i) {
+                    if (i < P.nc) {
+                        T acc = T(0);
+#pragma unroll
+                        for (int k = 0; k < kMaxCloLen; ++k)
+                            if (k < P.clo_len[i]) acc += T(P.clo[i][k]) * tile[k * TP + lane];
+                        y[i] = acc;
+                    }
+                }
+            }
+            if (seg == S - 1) {
+#pragma unroll
+                for (int i = MS - kMaxClo; i < MS; ++i) {
+                    if (i >= m - P.nc) {
+                        T acc = T(0);
+#pragma unroll
+                        for (int k = 0; k < kMaxCloLen; ++k)
+                            if (k < P.clo_len[m - 1 - i]) acc += T(P.chi[m - 1 - i][k]) * tile[(n - 1 - k) * TP + lane];
+                        y[i] = acc;
+                    }
+                }
+            }
+        }
+        __syncthreads();                  // the tile is consumed: refill it
+        issue(w + NS * gridDim.x, stage);
+        if (cls == 0) tg_solve<T, Q, MS, 0>(GP, y);
+        else if (cls == 1) tg_solve<T, Q, MS, 1>(GP, y);
+        else tg_solve<T, Q, MS, 2>(GP, y);
+        T* rl = red + (size_t)lane * RP;
+#pragma unroll
+        for (int t = 0; t < Q; ++t) {
+            rl[2 * Q * seg + t] = y[t];
+            rl[2 * Q * seg + Q + t] = y[MS - Q + t];
+        }
+        __syncthreads();   // interface values visible; also the previous group's stores from tout are done
+        T zp[Q], zn[Q];
+#pragma unroll
+        for (int t = 0; t < Q; ++t) {
+            zp[t] = T(0);
+            zn[t] = T(0);
+            if (has_prev) {
+                const T* g = Gs + (size_t)(2 * Q * prev + Q + t) * N;
+                T acc = T(0);
+                for (int j = 0; j < N; ++j) acc += g[j] * rl[j];
+                zp[t] = acc;
+            }
+            if (has_next) {
+                const T* g = Gs + (size_t)(2 * Q * next + t) * N;
+                T acc = T(0);
+                for (int j = 0; j < N; ++j) acc += g[j] * rl[j];
+                zn[t] = acc;
+            }
+        }
+        if (cls == 0) tg_correct<T, Q, MS, 0>(GP, y, zp, zn);
+        else if (cls == 1) tg_correct<T, Q, MS, 1>(GP, y, zp, zn);
+        else tg_correct<T, Q, MS, 2>(GP, y, zp, zn);
+#pragma unroll
+        for (int i = 0; i < MS; ++i) tout[(size_t)(off + i) * TP + lane] = y[i];
+        __syncthreads();   // the output tile is complete
+        {
+            const int c = w / groups, g0 = (w - c * groups) * kLanes;
+            T* base = reinterpret_cast<T*>(out.base) + (int64_t)c * out.comp_stride;
+            for (int l = seg; l < kLanes; l += nwarps) {
+                const int line = g0 + l;
+                if (line >= lines) break;
+                T* row = base + row_of(out, line);
+                for (int g = lane; g < n; g += kLanes) {
+                    const T v = tout[(size_t)g * TP + l];
+                    if (mode == OUT_STORE) row[g] = v;
+                    else if (mode == OUT_NEGATE) row[g] = -v;
+                    else row[g] = row[g] - v;
+                }
+            }
+        }
+        // tout and red are rewritten only after the next group's barriers
+    }
+    cp_async_wait<0>();
+}
+
 // --------------------------------------------------------------- host side --
 PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
     static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
@@ -325,17 +775,130 @@ bool launch_tma_m(const CompactPlan& plan, const CUtensorMap& map, const FieldVi
     }
 }
 
+template <typename T, int Q, int M, int MS>
+void launch_tg_ms(const CompactPlan& plan, const CUtensorMap& map, const FieldView& out, int count, int mode,
+                  cudaStream_t st, const T* tab, const RkEpilogue& rk) {
+    const CompactParams& P = plan.P;
+    const int NS = sizeof(T) == 8 ? 3 : 4;
+    const int N = 2 * Q * P.S;
+    const size_t smem = sizeof(T) * (size_t)P.n * kLanes * NS + 8 * sizeof(uint64_t) +
+                        sizeof(T) * ((size_t)kLanes * (N + 1) + (size_t)N * N);
+    auto kern = k_compact_tg<T, Q, M, MS>;
+    static int configured = 0;
+    if (configured < (int)smem) {
+        CLES_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        configured = (int)smem;
+    }
+    if (!g_num_sms) {
+        int dev = 0;
+        CLES_CUDA(cudaGetDevice(&dev));
+        CLES_CUDA(cudaDeviceGetAttribute(&g_num_sms, cudaDevAttrMultiProcessorCount, dev));
+    }
+    const int gx = (P.nx + kLanes - 1) / kLanes;
+    const int work = gx * (P.dim == 1 ? P.nz : P.ny) * count;
+    const int grid = work < g_num_sms ? work : g_num_sms;
+    kern<<<grid, kLanes * P.S, smem, st>>>(map, P, plan.TG, tab, out, mode, count, NS, rk);
+    count_launch();
+    check_launch("k_compact_tg");
+}
+
+template <typename T>
+bool launch_tg(const CompactPlan& plan, const CUtensorMap& map, const FieldView& out, int count, int mode,
+               cudaStream_t st, const T* tab, const RkEpilogue& rk) {
+    const CompactParams& P = plan.P;
+    const bool m32 = P.seg_base == 32;
+    if (P.q == 1) {
+        switch (P.M) {
+            case 1: m32 ? launch_tg_ms<T, 1, 1, 32>(plan, map, out, count, mode, st, tab, rk)
+                        : launch_tg_ms<T, 1, 1, 16>(plan, map, out, count, mode, st, tab, rk); return true;
+            case 2: m32 ? launch_tg_ms<T, 1, 2, 32>(plan, map, out, count, mode, st, tab, rk)
+                        : launch_tg_ms<T, 1, 2, 16>(plan, map, out, count, mode, st, tab, rk); return true;
+            case 4: m32 ? launch_tg_ms<T, 1, 4, 32>(plan, map, out, count, mode, st, tab, rk)
+                        : launch_tg_ms<T, 1, 4, 16>(plan, map, out, count, mode, st, tab, rk); return true;
+            default: return false;
+        }
+    }
+    if (P.q == 2 && P.M == 3) {
+        m32 ? launch_tg_ms<T, 2, 3, 32>(plan, map, out, count, mode, st, tab, rk)
+            : launch_tg_ms<T, 2, 3, 16>(plan, map, out, count, mode, st, tab, rk);
+        return true;
+    }
+    return false;
+}
+
+template <typename T, int Q, int M, int MS>
+void launch_xt_ms(const CompactPlan& plan, const FieldView& in, const FieldView& out, int count, int mode,
+                  cudaStream_t st, const T* tab) {
+    const CompactParams& P = plan.P;
+    constexpr int NS = sizeof(T) == 8 ? 2 : 3;
+    const int N = 2 * Q * P.S;
+    const size_t smem = sizeof(T) * ((size_t)P.n * (kLanes + 1) * (NS + 1) + (size_t)kLanes * (N + 1) + (size_t)N * N);
+    auto kern = k_compact_xt<T, Q, M, MS, NS>;
+    static int configured = 0;
+    if (configured < (int)smem) {
+        CLES_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        configured = (int)smem;
+    }
+    if (!g_num_sms) {
+        int dev = 0;
+        CLES_CUDA(cudaGetDevice(&dev));
+        CLES_CUDA(cudaDeviceGetAttribute(&g_num_sms, cudaDevAttrMultiProcessorCount, dev));
+    }
+    const int64_t groups = (P.lines + kLanes - 1) / kLanes;
+    const int64_t work = groups * count;
+    const int grid = work < g_num_sms ? (int)work : g_num_sms;
+    kern<<<grid, kLanes * P.S, smem, st>>>(P, plan.TG, tab, in, out, mode, count);
+    count_launch();
+    check_launch("k_compact_xt");
+}
+
+template <typename T>
+bool launch_xt(const CompactPlan& plan, const FieldView& in, const FieldView& out, int count, int mode,
+               cudaStream_t st, const T* tab) {
+    const CompactParams& P = plan.P;
+    const bool m32 = P.seg_base == 32;
+    if (P.q == 1) {
+        switch (P.M) {
+            case 1: m32 ? launch_xt_ms<T, 1, 1, 32>(plan, in, out, count, mode, st, tab)
+                        : launch_xt_ms<T, 1, 1, 16>(plan, in, out, count, mode, st, tab); return true;
+            case 2: m32 ? launch_xt_ms<T, 1, 2, 32>(plan, in, out, count, mode, st, tab)
+                        : launch_xt_ms<T, 1, 2, 16>(plan, in, out, count, mode, st, tab); return true;
+            case 4: m32 ? launch_xt_ms<T, 1, 4, 32>(plan, in, out, count, mode, st, tab)
+                        : launch_xt_ms<T, 1, 4, 16>(plan, in, out, count, mode, st, tab); return true;
+            default: return false;
+        }
+    }
+    if (P.q == 2 && P.M == 3) {
+        m32 ? launch_xt_ms<T, 2, 3, 32>(plan, in, out, count, mode, st, tab)
+            : launch_xt_ms<T, 2, 3, 16>(plan, in, out, count, mode, st, tab);
+        return true;
+    }
+    return false;
+}
+
 }  // namespace
+
+bool try_launch_xt(const CompactPlan& plan, const FieldView& in, const FieldView& out, int count, int mode,
+                   cudaStream_t st) {
+    if (!plan.has_tg || plan.P.dim != 0 || mode == OUT_RK) return false;
+    const CompactParams& P = plan.P;
+    if (P.n > 256 || P.S * kLanes > 256) return false;
+    const size_t el = plan.dtype == CLES_F64 ? 8 : 4;
+    // cp.async of one element needs element-aligned addresses only
+    if ((uintptr_t)in.base % el || (uintptr_t)out.base % el) return false;
+    if (plan.dtype == CLES_F64) return launch_xt<double>(plan, in, out, count, mode, st, plan.tab64);
+    return launch_xt<float>(plan, in, out, count, mode, st, plan.tab32);
+}
 
 bool try_launch_tma(const CompactPlan& plan, const FieldView& in, const FieldView& out, int count, int mode,
                     cudaStream_t st, const RkEpilogue* rkp) {
     RkEpilogue rk{nullptr, nullptr, 0.0, 0.0, 0.0, nullptr};
     if (rkp) rk = *rkp;
     if (mode == OUT_RK && !rkp) return false;
-    if (!plan.has_tl) return false;
+    if (!plan.has_tl && !plan.has_tg) return false;
     const CompactParams& P = plan.P;
-    if (P.dim == 0 || P.q != 1 || !P.periodic || P.n > 256 || P.S * kLanes > 256) return false;
-    if (P.M < 1 || P.M > 4 || P.M == 3) return false;
+    if (P.dim == 0 || P.n > 256 || P.S * kLanes > 256) return false;
+    if (plan.has_tl && (P.q != 1 || !P.periodic || P.M < 1 || P.M > 4 || P.M == 3)) return false;
     PFN_cuTensorMapEncodeTiled_v12000 enc = encode_fn();
     if (!enc) return false;
     const size_t el = plan.dtype == CLES_F64 ? 8 : 4;
@@ -351,6 +914,10 @@ bool try_launch_tma(const CompactPlan& plan, const FieldView& in, const FieldVie
                      in.base, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
                      CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) return false;
+    if (!plan.has_tl) {
+        if (plan.dtype == CLES_F64) return launch_tg<double>(plan, map, out, count, mode, st, plan.tab64, rk);
+        return launch_tg<float>(plan, map, out, count, mode, st, plan.tab32, rk);
+    }
     const int M = P.M;
     if (plan.TL.m != 32 && plan.TL.m != 16) return false;
     if (plan.dtype == CLES_F64) {

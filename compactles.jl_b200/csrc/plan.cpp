@@ -12,7 +12,11 @@
 // segment is corrected with its spike vectors.  With S = 1 and a periodic line
 // this is exactly the reference's single-rank self-coupled solve; with S > 1
 // it is the reference's P-rank distributed solve with ranks mapped to threads.
+// Closed tridiagonal lines replace the dense inverse by block cyclic reduction
+// of the same reduced system (coefficients precomputed here), which keeps
+// long single lines (1-D tubes of thousands of cells) at O(log S) depth.
 
+#include <array>
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -283,15 +287,25 @@ void build_compact_plan(CompactPlan& plan, const cles_scheme& s, const int n3[3]
     }
 
     // Segmentation: S segments of at most kMaxSeg points, local_range split.
-    int S = (n + kMaxSeg - 1) / kMaxSeg;
+    // Closed tridiagonal lines solve their interface system by cyclic reduction
+    // (depth log2 S), so plans with few lines cut them into shorter segments
+    // for more threads per line.
+    P.pcr = (!periodic && q == 1) ? 1 : 0;
+    int seg_target = kMaxSeg;
+    if (P.pcr) {
+        if (P.lines <= 16) seg_target = 8;
+        else if (P.lines <= 1024) seg_target = 16;
+        while (seg_target < kMaxSeg && (n + seg_target - 1) / seg_target > 512) seg_target *= 2;
+    }
+    int S = (n + seg_target - 1) / seg_target;
     if (S < 1) S = 1;
-    const int base = n / S, rem = n % S;
+    const int base = n / S;
     if (base < std::max(2 * q + 1, q + 1)) S = 1;  // tiny lines: one segment
     P.S = S;
     P.seg_base = n / S;
     P.seg_rem = n % S;
     if (P.seg_base + (P.seg_rem ? 1 : 0) > kMaxSeg) throw Error(CLES_EINVAL, "segment longer than the register tile");
-    (void)base; (void)rem;
+    if (S == 1) P.pcr = 0;
     int LB = 32;
     while (LB > 1 && LB * S > 512) LB /= 2;
     if (dim == 0) {
@@ -301,11 +315,9 @@ void build_compact_plan(CompactPlan& plan, const cles_scheme& s, const int n3[3]
         if ((size_t)n * (LB + 1) * el > 200 * 1024) throw Error(CLES_EINVAL, "x line too long for the shared-memory tile");
     }
     if (LB * S > 512) throw Error(CLES_EINVAL, "line too long for one CTA");
-    if (P.lines < LB) {
-        int l = 1;
-        while (l < P.lines) l *= 2;
-        LB = std::max(1, std::min(LB, l));
-    }
+    const int LB_full = LB;
+    // few lines: fewer per CTA so that more SMs take part
+    while (LB > 1 && (P.lines + LB - 1) / LB < 148) LB /= 2;
     P.LB = LB;
     P.hasred = (periodic || S > 1) ? 1 : 0;
 
@@ -319,7 +331,13 @@ void build_compact_plan(CompactPlan& plan, const cles_scheme& s, const int n3[3]
     P.off_V = 5 * arr;
     P.off_W = P.off_V + (int64_t)S * q * kMaxSeg;
     P.off_G = P.off_W + (int64_t)S * q * kMaxSeg;
-    const int64_t total = P.off_G + (P.hasred ? (int64_t)N * N : 0);
+    const int L = [&] { int l = 0; while ((1 << l) < S) ++l; return l; }();
+    P.pcr_levels = P.pcr ? L : 0;
+    // the dense inverse is kept for every plan with a small reduced system
+    // (the tile kernel reads it from shared memory), and for all periodic ones
+    const bool with_g = P.hasred && (!P.pcr || N <= 64);
+    P.off_pcr = P.off_G + (with_g ? (int64_t)N * N : 0);
+    const int64_t total = P.off_pcr + (P.pcr ? (int64_t)(L + 1) * S * 8 : 0);
     std::vector<double> tab((size_t)total, 0.0);
 
     std::vector<LocalFactor> fac(S);
@@ -371,7 +389,57 @@ void build_compact_plan(CompactPlan& plan, const cles_scheme& s, const int n3[3]
             }
         }
     }
-    if (P.hasred) {
+    if (P.pcr) {
+        // Interface system of a closed tridiagonal line in X_s = (head_s, tail_s):
+        //   X_s + A_s X_{s-1} + C_s X_{s+1} = (y_s[0], y_s[m-1]),
+        //   A_s = [[0, v_s[0]], [0, v_s[m-1]]], C_s = [[w_s[0], 0], [w_s[m-1], 0]],
+        // A_0 = C_{S-1} = 0.  Cyclic reduction level l (distance k = 2^l), all
+        // segments at once from the previous level's blocks:
+        //   alpha = -A_s B_{s-k}^-1, gamma = -C_s B_{s+k}^-1 (zero past the ends),
+        //   B_s += alpha C_{s-k} + gamma A_{s+k}, A_s = alpha A_{s-k}, C_s = gamma C_{s+k},
+        // and on the device R_s += alpha R_{s-k} + gamma R_{s+k}.  After
+        // ceil(log2 S) levels no coupling is left and X_s = B_s^-1 R_s.
+        std::vector<std::array<double, 4>> A(S), Bm(S), C(S);
+        for (int sg = 0; sg < S; ++sg) {
+            const int m = seg_len(sg);
+            A[sg] = {0.0, Vs[sg][0], 0.0, Vs[sg][(size_t)m - 1]};
+            C[sg] = {Ws[sg][0], 0.0, Ws[sg][(size_t)m - 1], 0.0};
+            Bm[sg] = {1.0, 0.0, 0.0, 1.0};
+        }
+        for (int l = 0; l < L; ++l) {
+            const int k = 1 << l;
+            std::vector<std::array<double, 4>> nA(S), nB(S), nC(S);
+            for (int sg = 0; sg < S; ++sg) {
+                double al[4] = {0, 0, 0, 0}, ga[4] = {0, 0, 0, 0}, t[4], bi[4];
+                nB[sg] = Bm[sg];
+                nA[sg] = {0, 0, 0, 0};
+                nC[sg] = {0, 0, 0, 0};
+                if (sg - k >= 0) {
+                    mat2_inv(Bm[sg - k].data(), bi);
+                    mat2_mul(A[sg].data(), bi, al);
+                    for (double& e : al) e = -e;
+                    mat2_mul(al, C[sg - k].data(), t);
+                    for (int e = 0; e < 4; ++e) nB[sg][e] += t[e];
+                    mat2_mul(al, A[sg - k].data(), nA[sg].data());
+                }
+                if (sg + k < S) {
+                    mat2_inv(Bm[sg + k].data(), bi);
+                    mat2_mul(C[sg].data(), bi, ga);
+                    for (double& e : ga) e = -e;
+                    mat2_mul(ga, A[sg + k].data(), t);
+                    for (int e = 0; e < 4; ++e) nB[sg][e] += t[e];
+                    mat2_mul(ga, C[sg + k].data(), nC[sg].data());
+                }
+                double* dst = &tab[P.off_pcr + ((size_t)l * S + sg) * 8];
+                for (int e = 0; e < 4; ++e) { dst[e] = al[e]; dst[4 + e] = ga[e]; }
+            }
+            A.swap(nA);
+            Bm.swap(nB);
+            C.swap(nC);
+        }
+        for (int sg = 0; sg < S; ++sg) mat2_inv(Bm[sg].data(), &tab[P.off_pcr + ((size_t)L * S + sg) * 8]);
+    }
+    if (with_g) {
         // Reduced system in z = (head_0, tail_0, head_1, tail_1, ...), 2q per segment.
         std::vector<double> R((size_t)N * N, 0.0);
         for (int sg = 0; sg < S; ++sg) {
@@ -396,7 +464,7 @@ void build_compact_plan(CompactPlan& plan, const cles_scheme& s, const int n3[3]
 
     build_warp_line(plan, B, s, n, dim, periodic);
     plan.has_tl = false;
-    if (q == 1 && periodic && dim > 0 && P.seg_rem == 0 && n <= 256 && P.LB == 32) {
+    if (q == 1 && periodic && dim > 0 && P.seg_rem == 0 && n <= 256 && LB_full == 32) {
         TileLineParams& T = plan.TL;
         std::memset(&T, 0, sizeof(T));
         T.m = P.seg_base;
@@ -418,6 +486,49 @@ void build_compact_plan(CompactPlan& plan, const cles_scheme& s, const int n3[3]
                        tab[P.off_f2 + o] == T.c[i] && tab[P.off_V + o] == T.v[i] && tab[P.off_W + o] == T.w[i];
             }
         plan.has_tl = same;
+    }
+    // general tile kernels (closed or periodic lines, q = 1 or the C10
+    // pentadiagonal; y/z lines by TMA tiles, x lines by cp.async transposed
+    // tiles): equal segments of 16 or 32 points, at most 8 per line
+    plan.has_tg = false;
+    if (with_g && P.seg_rem == 0 && (P.seg_base == 16 || P.seg_base == 32) && S * 32 <= 256 && n <= 256 &&
+        ((q == 1 && (M == 1 || M == 2 || M == 4)) || (q == 2 && M == 3))) {
+        TileGenParams& G = plan.TG;
+        std::memset(&G, 0, sizeof(G));
+        const int nf = q == 1 ? 3 : 5;
+        const int64_t offs[5] = {P.off_f0, P.off_f1, P.off_f2, P.off_f3, P.off_f4};
+        const int src[3] = {0, S > 2 ? 1 : 0, S - 1};
+        bool alike = true;   // interior segments must all be equal to segment 1
+        for (int sg = 2; sg < S - 1 && alike; ++sg)
+            for (int i = 0; i < P.seg_base; ++i) {
+                for (int a = 0; a < nf; ++a)
+                    alike = alike && tab[offs[a] + (size_t)sg * kMaxSeg + i] == tab[offs[a] + (size_t)kMaxSeg + i];
+                for (int t = 0; t < q; ++t) {
+                    alike = alike && tab[P.off_V + ((size_t)sg * q + t) * kMaxSeg + i] ==
+                                         tab[P.off_V + ((size_t)q + t) * kMaxSeg + i];
+                    alike = alike && tab[P.off_W + ((size_t)sg * q + t) * kMaxSeg + i] ==
+                                         tab[P.off_W + ((size_t)q + t) * kMaxSeg + i];
+                }
+            }
+        for (int cls = 0; cls < 3; ++cls) {
+            const int sg = src[cls];
+            for (int i = 0; i < kMaxSeg; ++i) {
+                for (int a = 0; a < nf; ++a) G.f[cls][a][i] = tab[offs[a] + (size_t)sg * kMaxSeg + i];
+                for (int t = 0; t < q; ++t) {
+                    G.v[cls][t][i] = tab[P.off_V + ((size_t)sg * q + t) * kMaxSeg + i];
+                    G.w[cls][t][i] = tab[P.off_W + ((size_t)sg * q + t) * kMaxSeg + i];
+                }
+            }
+        }
+        for (int cls = 0; cls < 3; ++cls)
+            for (int i = 0; i < kMaxSeg; ++i) {
+                for (int a = 0; a < 5; ++a) G.ff[cls][a][i] = (float)G.f[cls][a][i];
+                for (int t = 0; t < 2; ++t) {
+                    G.vf[cls][t][i] = (float)G.v[cls][t][i];
+                    G.wf[cls][t][i] = (float)G.w[cls][t][i];
+                }
+            }
+        plan.has_tg = alike;
     }
 
     plan.dtype = dtype;

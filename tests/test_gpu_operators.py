@@ -135,3 +135,29 @@ def test_apply_along_long_lines(orc, scheme, periodic, ng, dim):
     got = orc.interior(g, out)
     err = np.abs(got - ref).max() / np.abs(ref).max()
     assert err < 1e-12, err
+
+
+@pytest.mark.parametrize("scheme", SCHEMES)
+@pytest.mark.parametrize("periodic", [True, False])
+@pytest.mark.parametrize("dim", [1, 2, 3])
+@pytest.mark.parametrize("n", [64, 128, 192, 256])
+@pytest.mark.parametrize("dtype", ["f64", "f32"])
+def test_apply_along_tile_kernels(orc, scheme, periodic, dim, n, dtype):
+    """Lines with enough lines per plan for the 32-point segments of the tile
+    kernels: TMA tiles for y/z, cp.async transposed tiles for x (closed lines,
+    C10, and the periodic tridiagonal ones)."""
+    ng = tuple(n if k == dim - 1 else 36 for k in range(3))
+    per = tuple(1 if (k != dim - 1 or periodic) else 0 for k in range(3))
+    g = orc.grid(ng, per)
+    f = _field(orc, g, seed=n + 7 * dim)
+    h = 0.9 / n
+    ref = orc.interior(g, orc.Plan(g, _schemes(orc, scheme), dim, h).apply(f))
+    plan = cl.plan_direction(cl.grid(ng, per), _schemes(cl, scheme), dim, h, dtype=dtype)
+    fin = f if dtype == "f64" else f.astype(np.float32)
+    out = np.zeros_like(fin)
+    cl.apply_along(out, plan, fin)
+    got = orc.interior(g, out).astype(np.float64)
+    err = np.abs(got - ref).max() / np.abs(ref).max()
+    # FP32: single-precision inputs and solves; the seeded noise makes the
+    # derivative large compared with the field, hence 5e-6 of the maximum
+    assert err < (1e-12 if dtype == "f64" else 5e-6), err
