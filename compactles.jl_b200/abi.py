@@ -104,6 +104,20 @@ class cles_step_control(C.Structure):
     ]
 
 
+CLES_EOS_IDEAL = 0
+CLES_EOS_NASA9 = 1
+CLES_MAX_NASA9_INTERVALS = 4
+
+
+class cles_nasa9_interval(C.Structure):
+    _fields_ = [
+        ("Tmin", C.c_double),
+        ("Tmax", C.c_double),
+        ("a", C.c_double * 7),
+        ("b1", C.c_double),
+    ]
+
+
 class cles_solver_desc(C.Structure):
     _fields_ = [
         ("n_global", C.c_int * 3),
@@ -130,6 +144,10 @@ class cles_solver_desc(C.Structure):
         ("control", cles_step_control),
         ("n_halo", C.c_int),
         ("precision", C.c_int),
+        ("eos", C.c_int),
+        ("T_guess", C.c_double),
+        ("n_intervals", C.c_int * CLES_MAX_SPECIES),
+        ("nasa9", (cles_nasa9_interval * CLES_MAX_NASA9_INTERVALS) * CLES_MAX_SPECIES),
     ]
 
 

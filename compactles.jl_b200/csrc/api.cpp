@@ -385,6 +385,8 @@ void cles_solver_desc_default(cles_solver_desc* d) {
     cles_step_control_default(&d->control);
     d->n_halo = 4;
     d->precision = CLES_PREC_FP64;
+    d->eos = CLES_EOS_IDEAL;
+    d->T_guess = 300.0;
 }
 
 int cles_solver_create(cles_ctx* ctx, const cles_solver_desc* desc, cles_solver** out) {

@@ -25,6 +25,59 @@ __device__ __forceinline__ double jl_min(double x, double y) {
     return y < x ? y : x;
 }
 
+// Julia's clamp(x, lo, hi): a NaN argument passes through.
+__device__ __forceinline__ double jl_clamp(double x, double lo, double hi) {
+    return x > hi ? hi : (x < lo ? lo : x);
+}
+
+// ---- NASA-9 species thermodynamics (src/physics.jl:298-310, 431-455) ----
+__device__ __forceinline__ int n9_interval(const PhysConst& pc, int k, double T) {
+    const int n = pc.nint[k];
+    for (int i = 0; i < n - 1; ++i)
+        if (T <= pc.Tmax[k][i]) return i;
+    return n - 1;
+}
+__device__ __forceinline__ double n9_cp_R(const double* a, double T) {
+    const double T2 = T * T;
+    return a[0] / T2 + a[1] / T + a[2] + a[3] * T + a[4] * T2 + a[5] * (T2 * T) + a[6] * (T2 * T2);
+}
+__device__ __forceinline__ double n9_h_R(const double* a, double b1, double T) {
+    const double T2 = T * T;
+    return -a[0] / T + a[1] * log(T) + a[2] * T + a[3] * T2 / 2 + a[4] * (T2 * T) / 3 + a[5] * (T2 * T2) / 4 +
+           a[6] * (T2 * T2 * T) / 5 + b1;
+}
+__device__ __forceinline__ double n9_cp(const PhysConst& pc, int k, double T) {
+    return pc.Rk[k] * n9_cp_R(pc.a[k][n9_interval(pc, k, T)], T);
+}
+__device__ __forceinline__ double n9_h(const PhysConst& pc, int k, double T) {
+    const int i = n9_interval(pc, k, T);
+    return pc.Rk[k] * n9_h_R(pc.a[k][i], pc.b1[k][i], T);
+}
+// mixture_temperature (src/physics.jl:466-498): bounded Newton on
+// sum_k Y_k e_k(T) = e, always in FP64.
+__device__ double n9_temperature(const PhysConst& pc, int Ns, double e, const double* Y) {
+    double e0 = 0.0, cv0 = 0.0;
+    for (int k = 0; k < Ns; ++k) {
+        e0 += Y[k] * pc.e_ref[k];
+        cv0 += Y[k] * pc.cv_ref[k];
+    }
+    double T = cv0 > 0 ? jl_clamp(pc.T_guess + (e - e0) / cv0, 1e-3, 1e9) : pc.T_guess;
+    for (int it = 0; it < 30; ++it) {
+        double f = -e, cvm = 0.0;
+        for (int k = 0; k < Ns; ++k) {
+            const int i = n9_interval(pc, k, T);
+            const double* a = pc.a[k][i];
+            f += Y[k] * (pc.Rk[k] * n9_h_R(a, pc.b1[k][i], T) - pc.Rk[k] * T);
+            cvm += Y[k] * (pc.Rk[k] * n9_cp_R(a, T) - pc.Rk[k]);
+        }
+        if (!(cvm > 0)) break;
+        const double d = f / cvm;
+        T = jl_max(T - d, 0.25 * T);
+        if (fabs(d) <= 1e-14 * T) break;
+    }
+    return T;
+}
+
 inline unsigned grid_for(int64_t n) {
     int64_t b = (n + kThreads - 1) / kThreads;
     if (b > 148 * 64) b = 148 * 64;
@@ -33,15 +86,48 @@ inline unsigned grid_for(int64_t n) {
 
 #define GRID_STRIDE(idx, n) for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < (n); idx += (int64_t)gridDim.x * blockDim.x)
 
-// _primitives!(::IdealMixture) (src/physics.jl:604-653) at the interior.
-template <typename F>
+// _primitives!(::IdealMixture) (src/physics.jl:604-653) at the interior, and
+// _primitives!(::Nasa9Mixture) (src/physics.jl:501-570) when N9 (a separate
+// instantiation, so the ideal-gas kernel keeps its small register footprint).
+template <typename F, bool N9>
 __global__ void k_primitives(const double* __restrict__ Q, F* __restrict__ prim, int64_t cells, int Ns, PhysConst pc,
                              int esens) {
     GRID_STRIDE(I, cells) {
         double rho = 0.0;
         for (int sp = 0; sp < Ns; ++sp) rho += Q[I + cells * sp];
         F* out = prim + I;
-        if (rho > 0) {
+        if (N9 && rho > 0) {
+            const double ri = 1 / rho;
+            double Y[CLES_MAX_SPECIES];
+            double Rm = 0.0;
+            for (int sp = 0; sp < Ns; ++sp) {
+                Y[sp] = Q[I + cells * sp] * ri;
+                out[cells * (P_Y0 + sp)] = F(Y[sp]);
+                Rm += Y[sp] * pc.Rk[sp];
+            }
+            const double u = Q[I + cells * (Ns + 0)] * ri;
+            const double v = Q[I + cells * (Ns + 1)] * ri;
+            const double w = Q[I + cells * (Ns + 2)] * ri;
+            const double e = Q[I + cells * (Ns + 3)] * ri - 0.5 * (u * u + v * v + w * w);
+            const double T = n9_temperature(pc, Ns, e, Y);
+            double cpm = 0.0;
+            for (int sp = 0; sp < Ns; ++sp) cpm += Y[sp] * n9_cp(pc, sp, T);
+            const double cvm = cpm - Rm;
+            out[cells * P_RHO] = F(rho);
+            out[cells * P_U] = F(u);
+            out[cells * P_V] = F(v);
+            out[cells * P_W] = F(w);
+            out[cells * P_P] = F(rho * Rm * T);
+            out[cells * P_T] = F(T);
+            out[cells * P_C] = F(sqrt(jl_max((cpm / cvm) * Rm * T, 0.0)));
+            out[cells * P_CP] = F(cpm);
+            if (esens) {
+                const double r = jl_max(rho, 1e-300);
+                const double q1 = Q[I + cells * (Ns + 0)], q2 = Q[I + cells * (Ns + 1)], q3 = Q[I + cells * (Ns + 2)];
+                const double ke = 0.5 * (q1 * q1 + q2 * q2 + q3 * q3) / r;
+                out[cells * (P_Y0 + Ns)] = F((Q[I + cells * (Ns + 3)] - ke) / r);
+            }
+        } else if (rho > 0) {
             const double ri = 1 / rho;
             double Rm = 0.0, cvm = 0.0;
             for (int sp = 0; sp < Ns; ++sp) {
@@ -334,7 +420,7 @@ __global__ void k_dart(const F* __restrict__ sensor, const F* __restrict__ prim,
 // SINGLE (one species): the species diffusion flux rho D dY (Y - 1) is zero in
 // exact arithmetic (Y = 1) and below ~1e-30 of the momentum flux in FP64, so it
 // is taken as 0 and dY/dx_d is neither computed nor read (gty holds dT only).
-template <typename F, bool SINGLE>
+template <typename F, bool SINGLE, bool N9>
 __global__ void k_fluxes(const double* __restrict__ Q, const F* __restrict__ prim, const F* __restrict__ g,
                          const F* __restrict__ gty, const F* __restrict__ art, F* __restrict__ flux, int64_t cells,
                          int Ns, PhysConst pc, double mu0, double Pr, double Sc) {
@@ -381,7 +467,7 @@ __global__ void k_fluxes(const double* __restrict__ Q, const F* __restrict__ pri
                     const double Yk = double(prim[I + cells * (P_Y0 + sp)]);
                     const double Jkd = r * (-Dk * double(gd[I + cells * (1 + sp)]) + Yk * Vc);
                     fd[I + cells * sp] = F(r * Yk * ud + Jkd);
-                    hdiff += pc.cpk[sp] * Tp * Jkd;
+                    hdiff += (N9 ? n9_h(pc, sp, Tp) : pc.cpk[sp] * Tp) * Jkd;
                 }
             }
             fd[I + cells * (Ns + 0)] = F(r * ud * uv[0] + (d == 0 ? p : 0.0) - td[0]);
@@ -637,7 +723,8 @@ void clock_after(double* clk, const ClockConst& c, cudaStream_t st) {
 template <typename F>
 void Pointwise<F>::primitives(const double* Q, F* prim, int64_t cells, int Ns, const PhysConst& pc, cudaStream_t st,
                               int esens) {
-    LAUNCH(k_primitives<F>, cells, st, Q, prim, cells, Ns, pc, esens);
+    if (pc.eos == CLES_EOS_NASA9) LAUNCH((k_primitives<F, true>), cells, st, Q, prim, cells, Ns, pc, esens);
+    else LAUNCH((k_primitives<F, false>), cells, st, Q, prim, cells, Ns, pc, esens);
 }
 template <typename F>
 void Pointwise<F>::delta4_tiled(const F* f0, const F* f1, F* o0, F* o1, const Grid3& g, const double w0[3],
@@ -698,8 +785,10 @@ template <typename F>
 void Pointwise<F>::fluxes(const double* Q, const F* prim, const F* g, const F* gty, const F* art, F* flux,
                           int64_t cells, int Ns, const PhysConst& pc, double mu0, double Pr, double Sc,
                           cudaStream_t st) {
-    if (Ns == 1) LAUNCH((k_fluxes<F, true>), cells, st, Q, prim, g, gty, art, flux, cells, Ns, pc, mu0, Pr, Sc);
-    else LAUNCH((k_fluxes<F, false>), cells, st, Q, prim, g, gty, art, flux, cells, Ns, pc, mu0, Pr, Sc);
+    if (Ns == 1) LAUNCH((k_fluxes<F, true, false>), cells, st, Q, prim, g, gty, art, flux, cells, Ns, pc, mu0, Pr, Sc);
+    else if (pc.eos == CLES_EOS_NASA9)
+        LAUNCH((k_fluxes<F, false, true>), cells, st, Q, prim, g, gty, art, flux, cells, Ns, pc, mu0, Pr, Sc);
+    else LAUNCH((k_fluxes<F, false, false>), cells, st, Q, prim, g, gty, art, flux, cells, Ns, pc, mu0, Pr, Sc);
 }
 template <typename F>
 void Pointwise<F>::lsrk(double* Q, double* du, const F* dQ, int64_t n, double A, double B, double dt, cudaStream_t st,

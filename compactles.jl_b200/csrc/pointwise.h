@@ -15,7 +15,24 @@ struct PhysConst {
     double Rk[CLES_MAX_SPECIES];
     double cvk[CLES_MAX_SPECIES];
     double cpk[CLES_MAX_SPECIES];
+    // Nasa9Mixture (eos == CLES_EOS_NASA9): piecewise cp/R polynomials, and the
+    // species energy and cv at T_guess that seed the Newton solve
+    int eos;
+    double T_guess;
+    double e_ref[CLES_MAX_SPECIES], cv_ref[CLES_MAX_SPECIES];
+    int nint[CLES_MAX_SPECIES];
+    double Tmax[CLES_MAX_SPECIES][CLES_MAX_NASA9_INTERVALS];
+    double a[CLES_MAX_SPECIES][CLES_MAX_NASA9_INTERVALS][7];
+    double b1[CLES_MAX_SPECIES][CLES_MAX_NASA9_INTERVALS];
 };
+
+// Host evaluation of the NASA-9 species functions (the same expressions as
+// the device), used for the Newton seed constants and by validation.
+double nasa9_cp_over_R(const cles_nasa9_interval& iv, double T);
+double nasa9_h_over_R(const cles_nasa9_interval& iv, double T);
+// Fill the NASA-9 part of a PhysConst from a descriptor; throws on a bad table
+// (the checks of Nasa9Species, src/physics.jl:322-345).
+void nasa9_setup(PhysConst& pc, const cles_solver_desc& d);
 
 struct Grid3 {
     int n[3];

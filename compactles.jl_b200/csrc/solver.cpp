@@ -87,11 +87,13 @@ public:
         if (d.beta_sensor < 0 || d.beta_sensor > 2) throw Error(CLES_EINVAL, "unknown beta sensor");
         Ns_ = d.n_species;
         ncons_ = Ns_ + 4;
+        if (d.eos != CLES_EOS_IDEAL && d.eos != CLES_EOS_NASA9) throw Error(CLES_EINVAL, "unknown equation of state");
         for (int k = 0; k < Ns_; ++k) {
             pc_.Rk[k] = d.R[k];
-            pc_.cvk[k] = d.R[k] / (d.gamma[k] - 1);
+            pc_.cvk[k] = d.eos == CLES_EOS_IDEAL ? d.R[k] / (d.gamma[k] - 1) : 0.0;
             pc_.cpk[k] = pc_.Rk[k] + pc_.cvk[k];
         }
+        nasa9_setup(pc_, d);
         cells_ = (int64_t)g_.n[0] * g_.n[1] * g_.n[2];
         cfl = d.cfl;
         const int dt = sizeof(F) == 8 ? CLES_F64 : CLES_F32;
@@ -563,6 +565,61 @@ private:
 };
 
 }  // namespace
+
+double nasa9_cp_over_R(const cles_nasa9_interval& iv, double T) {
+    const double* a = iv.a;
+    const double T2 = T * T;
+    return a[0] / T2 + a[1] / T + a[2] + a[3] * T + a[4] * T2 + a[5] * (T2 * T) + a[6] * (T2 * T2);
+}
+
+double nasa9_h_over_R(const cles_nasa9_interval& iv, double T) {
+    const double* a = iv.a;
+    const double T2 = T * T;
+    return -a[0] / T + a[1] * std::log(T) + a[2] * T + a[3] * T2 / 2 + a[4] * (T2 * T) / 3 + a[5] * (T2 * T2) / 4 +
+           a[6] * (T2 * T2 * T) / 5 + iv.b1;
+}
+
+void nasa9_setup(PhysConst& pc, const cles_solver_desc& d) {
+    pc.eos = d.eos;
+    pc.T_guess = d.T_guess;
+    if (d.eos != CLES_EOS_NASA9) return;
+    if (!(d.T_guess > 0)) throw Error(CLES_EINVAL, "Nasa9Mixture T_guess must be positive");
+    for (int k = 0; k < d.n_species; ++k) {
+        const int n = d.n_intervals[k];
+        if (n < 1 || n > CLES_MAX_NASA9_INTERVALS) throw Error(CLES_EINVAL, "NASA-9 species needs 1..4 intervals");
+        if (!(d.R[k] > 0)) throw Error(CLES_EINVAL, "NASA-9 species has non-positive R");
+        const cles_nasa9_interval* iv = d.nasa9[k];
+        for (int i = 0; i < n; ++i)
+            if (!(iv[i].Tmin > 0 && iv[i].Tmin < iv[i].Tmax)) throw Error(CLES_EINVAL, "invalid NASA-9 interval");
+        // contiguity and continuity of cp and h at the joins
+        // (_validate_nasa9_intervals, src/physics.jl:322-345; relative tolerance 2e-3)
+        for (int i = 0; i + 1 < n; ++i) {
+            const cles_nasa9_interval &lo = iv[i], &hi = iv[i + 1];
+            const double sT = std::max({std::fabs(lo.Tmax), std::fabs(hi.Tmin), 1.0});
+            if (!(std::fabs(lo.Tmax - hi.Tmin) <= 1e-10 * sT)) throw Error(CLES_EINVAL, "non-contiguous NASA-9 intervals");
+            const double Tj = (lo.Tmax + hi.Tmin) / 2;
+            const double cl = nasa9_cp_over_R(lo, Tj), ch = nasa9_cp_over_R(hi, Tj);
+            if (!(std::fabs(cl - ch) <= 2e-3 * std::max({std::fabs(cl), std::fabs(ch), 1.0})))
+                throw Error(CLES_EINVAL, "discontinuous NASA-9 cp at an interval join");
+            const double hl = nasa9_h_over_R(lo, Tj), hh = nasa9_h_over_R(hi, Tj);
+            if (!(std::fabs(hl - hh) <= 2e-3 * std::max({std::fabs(hl), std::fabs(hh), Tj})))
+                throw Error(CLES_EINVAL, "discontinuous NASA-9 h at an interval join");
+        }
+        pc.nint[k] = n;
+        for (int i = 0; i < n; ++i) {
+            pc.Tmax[k][i] = iv[i].Tmax;
+            for (int j = 0; j < 7; ++j) pc.a[k][i][j] = iv[i].a[j];
+            pc.b1[k][i] = iv[i].b1;
+        }
+        // species energy and cv at T_guess: the state-independent part of the
+        // Newton seed (src/physics.jl:475-482)
+        int ig = n - 1;
+        for (int i = 0; i < n - 1; ++i)
+            if (d.T_guess <= iv[i].Tmax) { ig = i; break; }
+        pc.e_ref[k] = d.R[k] * nasa9_h_over_R(iv[ig], d.T_guess) - d.R[k] * d.T_guess;
+        pc.cv_ref[k] = d.R[k] * nasa9_cp_over_R(iv[ig], d.T_guess) - d.R[k];
+    }
+}
 
 int check_step(const cles_step_control& c, double dt, double rho_min, double dt_seen) {
     // check_step (src/stepcontrol.jl:184-204)

@@ -16,6 +16,7 @@ from typing import Callable, Optional, Sequence, Tuple
 import numpy as np
 
 from . import abi
+from .nasa9 import Nasa9Interval, Nasa9Mixture, Nasa9Species, fill_descriptor
 
 
 # ------------------------------------------------------------------- EOS ----
@@ -130,11 +131,26 @@ class Prim:
 
 
 def conserved_from_prim(eos, pr):
-    """conserved_from_prim(::NavierStokes1T, ::IdealMixture, pr) (src/problem.jl:76-90),
-    vectorised over array-valued Prim fields; returns a list of n_cons arrays."""
+    """conserved_from_prim(::NavierStokes1T, ::IdealMixture, pr) (src/problem.jl:76-90)
+    and (::Nasa9Mixture) (src/problem.jl:105-120), vectorised over
+    array-valued Prim fields; returns a list of n_cons arrays."""
     N = len(pr.Y)
     if N != eos.nspecies:
         raise ValueError(f"Prim carries {N} mass fractions; EOS has {eos.nspecies} species")
+    if isinstance(eos, Nasa9Mixture):
+        Rm = 0.0
+        for k in range(N):
+            Rm = Rm + pr.Y[k] * eos.Rk[k]
+        rho = pr.p / (Rm * pr.T_ion) if pr.rho is None else pr.rho
+        T = pr.p / (rho * Rm) if pr.T_ion is None else pr.T_ion
+        e = 0.0
+        for k in range(N):
+            e = e + pr.Y[k] * eos.species_energy(k, T)
+        u = pr.u
+        ke = 0.5 * (u[0] ** 2 + u[1] ** 2 + u[2] ** 2)
+        out = [rho * pr.Y[k] for k in range(N)]
+        out += [rho * u[0], rho * u[1], rho * u[2], rho * (e + ke)]
+        return out
     Rk, cvk = eos.Rk, eos.cvk
     Rm = 0.0
     cvm = 0.0
@@ -213,9 +229,14 @@ def solver_desc(n_global, L_domain, bcs, deriv, filt, eos=None, transport=None, 
     if eos.nspecies > abi.CLES_MAX_SPECIES:
         raise ValueError("too many species")
     d.n_species = eos.nspecies
-    for k, s in enumerate(eos.sp):
-        d.R[k] = s.R
-        d.gamma[k] = s.gamma
+    if isinstance(eos, Nasa9Mixture):
+        fill_descriptor(d, eos)
+    else:
+        d.eos = abi.CLES_EOS_IDEAL
+        d.T_guess = 300.0
+        for k, s in enumerate(eos.sp):
+            d.R[k] = s.R
+            d.gamma[k] = s.gamma
     d.mu0, d.Pr, d.Sc = transport.mu0, transport.Pr, transport.Sc
     d.art_enabled = int(art.enabled)
     d.C_mu, d.C_beta, d.C_kappa, d.C_D = art.C_mu, art.C_beta, art.C_kappa, art.C_D
@@ -269,12 +290,23 @@ def interior_slices(desc):
     return tuple(sl)
 
 
+def eos_from_desc(desc):
+    """The equation of state a descriptor carries."""
+    if desc.eos == abi.CLES_EOS_NASA9:
+        sp = []
+        for k in range(desc.n_species):
+            ivs = [Nasa9Interval(t.Tmin, t.Tmax, tuple(t.a[j] for j in range(7)), t.b1)
+                   for t in list(desc.nasa9[k])[:desc.n_intervals[k]]]
+            sp.append(Nasa9Species(f"species_{k}", desc.R[k], ivs))
+        return Nasa9Mixture(sp, T_guess=desc.T_guess)
+    return IdealMixture([IdealSpecies(f"species_{k}", desc.R[k], desc.gamma[k]) for k in range(desc.n_species)])
+
+
 def initialize(desc, ic, eos=None, layout=abi.CLES_LAYOUT_PADDED, Q=None):
     """initialize!(solver, Q, ic) (src/problem.jl:146-163): evaluate ic at the
     interior nodes and write the conserved state; halos are left as they are
     (zero for a fresh array)."""
-    eos = eos or IdealMixture([IdealSpecies(f"species_{k}", desc.R[k], desc.gamma[k])
-                               for k in range(desc.n_species)])
+    eos = eos or eos_from_desc(desc)
     if Q is None:
         Q = np.zeros(state_shape(desc, layout))
     x, y, z = coords(desc)

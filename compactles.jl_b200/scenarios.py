@@ -21,13 +21,20 @@ builders serve the CUDA library and the CPU oracle.
   on the CPU oracle and on the device at the same step, because the upper
   modes are only 8-16 cells long.
 * taylor_green_box: the README Taylor-Green vortex on an n^3 periodic box.
+* he_co2_shock_tube: examples/shock_tube.jl -- a 4 m closed tube of a NASA-9
+  He/CO2 mixture at 300 K, 10 atm He driver against 1 atm He, diaphragm at
+  2 m, sinusoidally perturbed He/CO2 contact at 3 m (amplitude 10% of the
+  0.2 m span, one wavelength), diffuse widths 3 h_x, slip walls in x,
+  periodic y, artificial properties on, cfl 0.5 with four rollback retries,
+  run to 2.5 ms.  The NASA-9 mixture is passed in (read_nasa9 on a CEA
+  thermo.inp, He then CO2).
 """
 import math
 
 import numpy as np
 
-from .problem import (ArtParams, IdealMixture, IdealSpecies, PER3, Prim, SlipWallBC, Transport, initialize,
-                      single_species, solver_desc, tanh_blend, taylor_green_problem)
+from .problem import (ArtParams, IdealMixture, IdealSpecies, PER3, Prim, SlipWallBC, StepControl, Transport,
+                      initialize, single_species, solver_desc, tanh_blend, taylor_green_problem)
 
 R_UNIVERSAL = 8.31446261815324  # J/(mol K), src/nasa9_data.jl:19
 
@@ -101,3 +108,22 @@ def taylor_green_box(schemes, n, tfinal=1.0, precision="fp64"):
     tp = 2 * math.pi
     desc = solver_desc((n, n, n), (tp, tp, tp), prob.bcs, deriv, filt, precision=precision)
     return desc, initialize(desc, prob.ic), tfinal
+
+
+def he_co2_shock_tube(schemes, eos, nx=768, ny=48, tfinal=2.5e-3, precision="fp64", retries=4):
+    deriv, filt = schemes
+    Lx, Lyz = 4.0, 0.2
+    atm = 101325.0
+    p_driver, p_driven, T0 = 10 * atm, 1 * atm, 300.0
+    hx = Lx / (nx - 1)
+    delta = 3 * hx
+    desc = solver_desc((nx, ny, 1), (Lx, Lyz, Lyz), ((SlipWallBC(), SlipWallBC()), PER3[1], PER3[2]), deriv, filt,
+                       eos=eos, transport=Transport(mu0=0.0), art=ArtParams(enabled=True), cfl=0.5,
+                       control=StepControl(retries=retries), filter_interval=1, precision=precision)
+
+    def ic(x, y, z):
+        xi = 3.0 + 0.1 * Lyz * np.cos(2 * math.pi * y / Lyz)
+        th = tanh_blend(x, xi, delta)
+        p = p_driven + (p_driver - p_driven) * (1 - tanh_blend(x, 2.0, delta))
+        return Prim(Y=(1 - th, th), p=p + 0 * y, T_ion=T0 + 0 * x + 0 * y)
+    return desc, initialize(desc, ic, eos=eos), tfinal

@@ -175,6 +175,20 @@ void cles_step_control_default(cles_step_control* out);
 
 /* The Solver's scalar configuration (src/rhs.jl:122-135, src/problem.jl:243-306).
  * Cartesian metric, no stretching, no folds, no sources. */
+/* Equation of state of the mixture. */
+#define CLES_EOS_IDEAL 0   /* IdealMixture: R[k], gamma[k] (src/physics.jl:87-120) */
+#define CLES_EOS_NASA9 1   /* Nasa9Mixture: R[k] and the NASA-9 intervals (src/physics.jl:402-427) */
+#define CLES_MAX_NASA9_INTERVALS 4
+
+/* One NASA-9 interval (Nasa9Interval, src/physics.jl:291-296):
+ *   cp/R = a1 T^-2 + a2 T^-1 + a3 + a4 T + a5 T^2 + a6 T^3 + a7 T^4
+ *   h/R  = -a1 T^-1 + a2 ln T + a3 T + a4 T^2/2 + a5 T^3/3 + a6 T^4/4 + a7 T^5/5 + b1 */
+typedef struct cles_nasa9_interval {
+    double Tmin, Tmax;
+    double a[7];
+    double b1;
+} cles_nasa9_interval;
+
 typedef struct cles_solver_desc {
     int    n_global[3];
     double L[3];                 /* domain extents */
@@ -196,6 +210,13 @@ typedef struct cles_solver_desc {
     cles_step_control control;
     int    n_halo;               /* halo width of padded host arrays (layout only) */
     int    precision;            /* CLES_PREC_FP64 / CLES_PREC_MIXED */
+    /* CLES_EOS_NASA9: temperature from internal energy by the bounded FP64
+     * Newton of mixture_temperature (src/physics.jl:466-498) in every
+     * precision mode; gamma[] is unused. */
+    int    eos;                  /* CLES_EOS_IDEAL (default) or CLES_EOS_NASA9 */
+    double T_guess;              /* Newton seed reference temperature (default 300 K) */
+    int    n_intervals[CLES_MAX_SPECIES];
+    cles_nasa9_interval nasa9[CLES_MAX_SPECIES][CLES_MAX_NASA9_INTERVALS];
 } cles_solver_desc;
 
 /* Defaults of Problem()/Numerics() for a grid: single_species(1.4, R=1),

@@ -656,8 +656,103 @@ struct Solver {
     double* vel(int j) { return j == 0 ? u.data() : j == 1 ? v.data() : w.data(); }
 };
 
+// ---- Nasa9Mixture (src/physics.jl:255-310, 402-570) ----
+// cp/R and h/R of one interval; x^2, x^3, x^4 written as products.
+double n9_cp_R(const cles_nasa9_interval& iv, double T) {
+    const double* a = iv.a;
+    const double T2 = T * T;
+    return a[0] / T2 + a[1] / T + a[2] + a[3] * T + a[4] * T2 + a[5] * (T2 * T) + a[6] * (T2 * T2);
+}
+double n9_h_R(const cles_nasa9_interval& iv, double T) {
+    const double* a = iv.a;
+    const double T2 = T * T;
+    return -a[0] / T + a[1] * std::log(T) + a[2] * T + a[3] * T2 / 2 + a[4] * (T2 * T) / 3 + a[5] * (T2 * T2) / 4 +
+           a[6] * (T2 * T2 * T) / 5 + iv.b1;
+}
+// _nasa9_interval: the first interval whose Tmax >= T, else the last
+const cles_nasa9_interval& n9_interval(const cles_solver_desc& d, int k, double T) {
+    const int n = d.n_intervals[k];
+    for (int i = 0; i < n - 1; ++i)
+        if (T <= d.nasa9[k][i].Tmax) return d.nasa9[k][i];
+    return d.nasa9[k][n - 1];
+}
+double n9_species_cp(const cles_solver_desc& d, int k, double T) { return d.R[k] * n9_cp_R(n9_interval(d, k, T), T); }
+double n9_species_h(const cles_solver_desc& d, int k, double T) { return d.R[k] * n9_h_R(n9_interval(d, k, T), T); }
+double n9_species_e(const cles_solver_desc& d, int k, double T) { return n9_species_h(d, k, T) - d.R[k] * T; }
+
+// mixture_temperature (src/physics.jl:466-498)
+double n9_temperature(const cles_solver_desc& d, double e, const double* Y) {
+    const int n = d.n_species;
+    double e0 = 0.0, cv0 = 0.0;
+    for (int k = 0; k < n; ++k) {
+        e0 += Y[k] * n9_species_e(d, k, d.T_guess);
+        cv0 += Y[k] * (n9_species_cp(d, k, d.T_guess) - d.R[k]);
+    }
+    double T = d.T_guess;
+    if (cv0 > 0) {
+        const double x = d.T_guess + (e - e0) / cv0;
+        T = x > 1e9 ? 1e9 : (x < 1e-3 ? 1e-3 : x);   // Julia clamp: NaN passes through
+    }
+    for (int it = 0; it < 30; ++it) {
+        double f = -e, cvm = 0.0;
+        for (int k = 0; k < n; ++k) {
+            f += Y[k] * n9_species_e(d, k, T);
+            cvm += Y[k] * (n9_species_cp(d, k, T) - d.R[k]);
+        }
+        if (!(cvm > 0)) break;
+        const double dl = f / cvm;
+        T = jl_max(T - dl, 0.25 * T);
+        if (std::fabs(dl) <= 1e-14 * T) break;
+    }
+    return T;
+}
+
+// species_enthalpy of either equation of state
+inline double species_h(const Solver& S, int k, double T) {
+    return S.desc.eos == CLES_EOS_NASA9 ? n9_species_h(S.desc, k, T) : S.cpk[k] * T;
+}
+
+// _primitives!(::Nasa9Mixture) (src/physics.jl:501-570)
+void primitives_nasa9(Solver& S) {
+    const size_t fs = S.fs;
+    const int Ns = S.Ns;
+    const double* Q = S.Q.data();
+#pragma omp parallel for schedule(static) if ((long)fs >= kThreadMinWork)
+    for (size_t idx = 0; idx < fs; ++idx) {
+        double rho = 0.0;
+        for (int sp = 0; sp < Ns; ++sp) rho += Q[idx + fs * sp];
+        if (rho > 0) {
+            const double ri = 1 / rho;
+            double Y[CLES_MAX_SPECIES];
+            double Rm = 0.0;
+            for (int sp = 0; sp < Ns; ++sp) {
+                Y[sp] = Q[idx + fs * sp] * ri;
+                S.Y[sp][idx] = Y[sp];
+                Rm += Y[sp] * S.Rk[sp];
+            }
+            const double uu = Q[idx + fs * S.i_mom[0]] * ri;
+            const double vv = Q[idx + fs * S.i_mom[1]] * ri;
+            const double ww = Q[idx + fs * S.i_mom[2]] * ri;
+            const double e = Q[idx + fs * S.i_energy] * ri - 0.5 * (uu * uu + vv * vv + ww * ww);
+            const double Ti = n9_temperature(S.desc, e, Y);
+            double cpm = 0.0;
+            for (int sp = 0; sp < Ns; ++sp) cpm += Y[sp] * n9_species_cp(S.desc, sp, Ti);
+            const double cvm = cpm - Rm;
+            S.rho[idx] = rho; S.u[idx] = uu; S.v[idx] = vv; S.w[idx] = ww;
+            S.p[idx] = rho * Rm * Ti; S.T[idx] = Ti;
+            S.c[idx] = std::sqrt(jl_max((cpm / cvm) * Rm * Ti, 0.0));
+            S.cp[idx] = cpm;
+        } else {
+            S.rho[idx] = 1; S.u[idx] = 0; S.v[idx] = 0; S.w[idx] = 0;
+            S.p[idx] = 1; S.T[idx] = 1; S.c[idx] = 1; S.cp[idx] = 1;
+            for (int sp = 0; sp < Ns; ++sp) S.Y[sp][idx] = sp == 0 ? 1.0 : 0.0;
+        }
+    }
+}
+
 // _primitives!(::IdealMixture) over the full padded arrays (src/physics.jl:604-653).
 void primitives(Solver& S) {
+    if (S.desc.eos == CLES_EOS_NASA9) { primitives_nasa9(S); return; }
     const size_t fs = S.fs;
     const int Ns = S.Ns;
     const double* Q = S.Q.data();
@@ -871,7 +966,7 @@ void assemble_fluxes(Solver& S) {
                 const double Dk = D0 + S.D_art[sp][I];
                 const double Jkd = r * (-Dk * S.grad_Y[d][sp][I] + S.Y[sp][I] * Vc);
                 S.flux[d][sp][I] = r * S.Y[sp][I] * ud + Jkd;
-                hdiff += S.cpk[sp] * Tp * Jkd;
+                hdiff += species_h(S, sp, Tp) * Jkd;
             }
             S.flux[d][m1][I] = r * ud * uv[0] + (d == 0 ? pp : 0.0) - td[0];
             S.flux[d][m2][I] = r * ud * uv[1] + (d == 1 ? pp : 0.0) - td[1];
@@ -1177,10 +1272,15 @@ Solver* solver_create(const cles_solver_desc& A) {
     S->D = make_decomp(A.n_global, per, A.n_halo);
     S->Ns = A.n_species; S->ncons = A.n_species + 4;
     S->i_mom[0] = S->Ns; S->i_mom[1] = S->Ns + 1; S->i_mom[2] = S->Ns + 2; S->i_energy = S->Ns + 3;
+    if (A.eos != CLES_EOS_IDEAL && A.eos != CLES_EOS_NASA9) { set_err("unknown equation of state"); return nullptr; }
     for (int k = 0; k < S->Ns; ++k) {
         S->Rk[k] = A.R[k];
-        S->cvk[k] = A.R[k] / (A.gamma[k] - 1);
+        S->cvk[k] = A.eos == CLES_EOS_IDEAL ? A.R[k] / (A.gamma[k] - 1) : 0.0;
         S->cpk[k] = S->Rk[k] + S->cvk[k];
+        if (A.eos == CLES_EOS_NASA9 && (A.n_intervals[k] < 1 || A.n_intervals[k] > CLES_MAX_NASA9_INTERVALS)) {
+            set_err("NASA-9 species needs 1..4 intervals");
+            return nullptr;
+        }
     }
     for (int d = 0; d < 3; ++d) {
         if (!S->D.active[d]) S->h[d] = 1.0;
@@ -1317,6 +1417,12 @@ int orc_get_flux(orc_solver* so, int d, int c, double* out) {
     std::memcpy(out, S.flux[d][c].data(), sizeof(double) * S.fs);
     return 0;
 }
+
+// NASA-9 species functions and the Newton inversion, for the thermodynamic tests
+double orc_nasa9_cp(const cles_solver_desc* d, int k, double T) { return n9_species_cp(*d, k, T); }
+double orc_nasa9_h(const cles_solver_desc* d, int k, double T) { return n9_species_h(*d, k, T); }
+double orc_nasa9_e(const cles_solver_desc* d, int k, double T) { return n9_species_e(*d, k, T); }
+double orc_nasa9_temperature(const cles_solver_desc* d, double e, const double* Y) { return n9_temperature(*d, e, Y); }
 
 int orc_check_step(const cles_step_control* c, double dt, double rho_min, double dt_seen) {
     return check_step(*c, dt, rho_min, dt_seen);

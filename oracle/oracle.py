@@ -77,6 +77,11 @@ def lib():
         L.orc_step.argtypes = [C.c_void_p, C.c_double, C.c_int]
         L.orc_filter_state.argtypes = [C.c_void_p]
         L.orc_run.argtypes = [C.c_void_p, C.c_double, C.c_int64, C.POINTER(abi.cles_run_result)]
+        for nm in ("orc_nasa9_cp", "orc_nasa9_h", "orc_nasa9_e"):
+            getattr(L, nm).restype = C.c_double
+            getattr(L, nm).argtypes = [C.POINTER(abi.cles_solver_desc), C.c_int, C.c_double]
+        L.orc_nasa9_temperature.restype = C.c_double
+        L.orc_nasa9_temperature.argtypes = [C.POINTER(abi.cles_solver_desc), C.c_double, _DP]
         L.orc_kinetic_energy.restype = C.c_double
         L.orc_kinetic_energy.argtypes = [C.c_void_p]
         L.orc_dissipation_rate.restype = C.c_double
@@ -290,3 +295,23 @@ def check_step(control, dt, rho_min, dt_seen):
 
 def default_threads():
     return os.cpu_count() or 1
+
+
+def nasa9_cp(desc, k, T):
+    """species_cp of a NASA-9 descriptor (src/physics.jl:437-441)."""
+    return lib().orc_nasa9_cp(C.byref(desc), int(k), float(T))
+
+
+def nasa9_h(desc, k, T):
+    """species_enthalpy (src/physics.jl:443-447)."""
+    return lib().orc_nasa9_h(C.byref(desc), int(k), float(T))
+
+
+def nasa9_e(desc, k, T):
+    """species_energy (src/physics.jl:449-451)."""
+    return lib().orc_nasa9_e(C.byref(desc), int(k), float(T))
+
+
+def nasa9_temperature(desc, e, Y):
+    """mixture_temperature (src/physics.jl:466-498)."""
+    return lib().orc_nasa9_temperature(C.byref(desc), float(e), np.ascontiguousarray(Y, dtype=np.float64))
