@@ -66,6 +66,8 @@ def lib():
         L.cles_apply_along.argtypes = [vp, vp, vp]
         L.cles_apply_along_batch.argtypes = [vp, vp, vp, C.c_int, C.c_int64]
         L.cles_apply_along_host.argtypes = [vp, vp, vp]
+        L.cles_checkpoint_save.argtypes = [vp, C.c_char_p]
+        L.cles_checkpoint_load.argtypes = [vp, C.c_char_p]
         L.cles_step_control_default.argtypes = [C.POINTER(abi.cles_step_control)]
         L.cles_step_control_default.restype = None
         L.cles_solver_desc_default.argtypes = [C.POINTER(abi.cles_solver_desc)]
@@ -336,6 +338,15 @@ class Solver:
 
     def set_clock(self, t, step, cfl):
         _check(lib().cles_set_clock(self.ptr, float(t), int(step), float(cfl)))
+
+    def save_checkpoint(self, prefix):
+        """save_checkpoint(solver, Q, prefix) (src/io.jl:8-41): writes prefix.r0000.ckpt."""
+        _check(lib().cles_checkpoint_save(self.ptr, str(prefix).encode()))
+        return str(prefix)
+
+    def load_checkpoint(self, prefix):
+        """load_checkpoint!(solver, Q, prefix) (src/io.jl:43-72)."""
+        _check(lib().cles_checkpoint_load(self.ptr, str(prefix).encode()))
 
     @property
     def t(self):

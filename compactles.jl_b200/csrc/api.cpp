@@ -4,6 +4,7 @@
 #include <atomic>
 #include <cstdio>
 #include <cstring>
+#include <vector>
 #include <string>
 
 #include "solver.h"
@@ -453,6 +454,78 @@ int cles_set_clock(cles_solver* s, double t, int64_t step, double cfl) {
     s->s->t = t;
     s->s->step_count = step;
     s->s->cfl = cfl;
+    API_END
+}
+
+// ------------------------------------------------------------ checkpoints --
+namespace {
+constexpr uint64_t kCkptMagic = 0x434c4553434b5054ull;   // "CLES CKPT" (src/io.jl:6)
+
+std::string ckpt_name(const char* prefix) { return std::string(prefix) + ".r0000.ckpt"; }
+
+struct FileCloser {
+    FILE* f;
+    ~FileCloser() { if (f) std::fclose(f); }
+};
+}  // namespace
+
+int cles_checkpoint_save(cles_solver* s, const char* prefix) {
+    API_BEGIN
+    if (!s || !prefix) throw Error(CLES_EINVAL, "null argument");
+    CLES_CUDA(cudaSetDevice(s->ctx->device));
+    const cles_solver_info I = s->s->info();
+    const size_t n = (size_t)I.cells * I.n_cons;
+    std::vector<double> buf(n);
+    s->s->get_state(buf.data(), CLES_LAYOUT_INTERIOR);
+    const std::string path = ckpt_name(prefix);
+    FileCloser fc{std::fopen(path.c_str(), "wb")};
+    if (!fc.f) throw Error(CLES_EINVAL, "cannot open " + path + " for writing");
+    int64_t hdr[10];
+    hdr[0] = I.n_cons;
+    for (int d = 0; d < 3; ++d) {
+        hdr[1 + d] = s->s->desc.n_global[d];
+        hdr[4 + d] = s->s->desc.n_global[d];   // one rank owns the whole grid
+        hdr[7 + d] = 0;                         // its coordinates in the process grid
+    }
+    const double t = s->s->t;
+    const int64_t step = s->s->step_count;
+    bool ok = std::fwrite(&kCkptMagic, sizeof(kCkptMagic), 1, fc.f) == 1 &&
+              std::fwrite(hdr, sizeof(int64_t), 10, fc.f) == 10 && std::fwrite(&t, sizeof(t), 1, fc.f) == 1 &&
+              std::fwrite(&step, sizeof(step), 1, fc.f) == 1 && std::fwrite(buf.data(), sizeof(double), n, fc.f) == n;
+    if (!ok) throw Error(CLES_EINVAL, "short write to " + path);
+    API_END
+}
+
+int cles_checkpoint_load(cles_solver* s, const char* prefix) {
+    API_BEGIN
+    if (!s || !prefix) throw Error(CLES_EINVAL, "null argument");
+    CLES_CUDA(cudaSetDevice(s->ctx->device));
+    const cles_solver_info I = s->s->info();
+    const std::string path = ckpt_name(prefix);
+    FileCloser fc{std::fopen(path.c_str(), "rb")};
+    if (!fc.f) throw Error(CLES_EINVAL, "cannot open " + path);
+    uint64_t magic = 0;
+    int64_t hdr[10];
+    if (std::fread(&magic, sizeof(magic), 1, fc.f) != 1 || magic != kCkptMagic)
+        throw Error(CLES_EINVAL, "not a CompactLES checkpoint");
+    if (std::fread(hdr, sizeof(int64_t), 10, fc.f) != 10) throw Error(CLES_EINVAL, "truncated checkpoint header");
+    if (hdr[0] != I.n_cons) throw Error(CLES_EINVAL, "conserved layout mismatch");
+    for (int d = 0; d < 3; ++d)
+        if (hdr[1 + d] != s->s->desc.n_global[d]) throw Error(CLES_EINVAL, "global grid mismatch");
+    for (int d = 0; d < 3; ++d)
+        if (hdr[4 + d] != s->s->desc.n_global[d]) throw Error(CLES_EINVAL, "decomposition mismatch");
+    for (int d = 0; d < 3; ++d)
+        if (hdr[7 + d] != 0) throw Error(CLES_EINVAL, "rank layout mismatch");
+    double t = 0.0;
+    int64_t step = 0;
+    const size_t n = (size_t)I.cells * I.n_cons;
+    std::vector<double> buf(n);
+    if (std::fread(&t, sizeof(t), 1, fc.f) != 1 || std::fread(&step, sizeof(step), 1, fc.f) != 1 ||
+        std::fread(buf.data(), sizeof(double), n, fc.f) != n)
+        throw Error(CLES_EINVAL, "truncated checkpoint");
+    s->s->set_state(buf.data(), CLES_LAYOUT_INTERIOR);
+    s->s->t = t;
+    s->s->step_count = step;
     API_END
 }
 

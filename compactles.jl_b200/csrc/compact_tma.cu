@@ -738,6 +738,15 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
 
 int g_num_sms = 0;
 
+int num_sms() {
+    if (!g_num_sms) {
+        int dev = 0;
+        CLES_CUDA(cudaGetDevice(&dev));
+        CLES_CUDA(cudaDeviceGetAttribute(&g_num_sms, cudaDevAttrMultiProcessorCount, dev));
+    }
+    return g_num_sms;
+}
+
 template <typename T, int M, int MS>
 void launch_tma_ms(const CompactPlan& plan, const CUtensorMap& map, const FieldView& out, int count, int mode,
                   cudaStream_t st, const T* G, const RkEpilogue& rk) {
@@ -883,6 +892,10 @@ bool try_launch_xt(const CompactPlan& plan, const FieldView& in, const FieldView
     if (!plan.has_tg || plan.P.dim != 0 || mode == OUT_RK) return false;
     const CompactParams& P = plan.P;
     if (P.n > 256 || P.S * kLanes > 256) return false;
+    // a persistent CTA holds ~200 KB of shared memory: worth it only when the
+    // launch has work for every SM (small grids, often run concurrently on
+    // other streams, keep the light generic kernel)
+    if (((P.lines + kLanes - 1) / kLanes) * count < num_sms()) return false;
     const size_t el = plan.dtype == CLES_F64 ? 8 : 4;
     // cp.async of one element needs element-aligned addresses only
     if ((uintptr_t)in.base % el || (uintptr_t)out.base % el) return false;
@@ -898,6 +911,10 @@ bool try_launch_tma(const CompactPlan& plan, const FieldView& in, const FieldVie
     if (!plan.has_tl && !plan.has_tg) return false;
     const CompactParams& P = plan.P;
     if (P.dim == 0 || P.n > 256 || P.S * kLanes > 256) return false;
+    if (!plan.has_tl) {
+        const int64_t gx = (P.nx + kLanes - 1) / kLanes;
+        if (gx * (P.dim == 1 ? P.nz : P.ny) * count < num_sms()) return false;   // see try_launch_xt
+    }
     if (plan.has_tl && (P.q != 1 || !P.periodic || P.M < 1 || P.M > 4 || P.M == 3)) return false;
     PFN_cuTensorMapEncodeTiled_v12000 enc = encode_fn();
     if (!enc) return false;

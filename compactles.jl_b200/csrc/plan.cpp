@@ -12,9 +12,10 @@
 // segment is corrected with its spike vectors.  With S = 1 and a periodic line
 // this is exactly the reference's single-rank self-coupled solve; with S > 1
 // it is the reference's P-rank distributed solve with ranks mapped to threads.
-// Closed tridiagonal lines replace the dense inverse by block cyclic reduction
-// of the same reduced system (coefficients precomputed here), which keeps
-// long single lines (1-D tubes of thousands of cells) at O(log S) depth.
+// Closed tridiagonal lines with more than 32 segments replace the dense
+// inverse by block cyclic reduction of the same reduced system (coefficients
+// precomputed here), which keeps long single lines (1-D tubes of thousands of
+// cells) at O(log S) depth.
 
 #include <array>
 #include <algorithm>
@@ -287,14 +288,12 @@ void build_compact_plan(CompactPlan& plan, const cles_scheme& s, const int n3[3]
     }
 
     // Segmentation: S segments of at most kMaxSeg points, local_range split.
-    // Closed tridiagonal lines solve their interface system by cyclic reduction
-    // (depth log2 S), so plans with few lines cut them into shorter segments
-    // for more threads per line.
+    // Plans of a handful of lines (1-D and very thin 2-D problems) are pure
+    // latency: they take segments of 8-16 points, more threads per line.
     P.pcr = (!periodic && q == 1) ? 1 : 0;
     int seg_target = kMaxSeg;
-    if (P.pcr) {
-        if (P.lines <= 16) seg_target = 8;
-        else if (P.lines <= 1024) seg_target = 16;
+    if (P.pcr && P.lines <= 16) {
+        seg_target = 8;
         while (seg_target < kMaxSeg && (n + seg_target - 1) / seg_target > 512) seg_target *= 2;
     }
     int S = (n + seg_target - 1) / seg_target;
@@ -305,7 +304,9 @@ void build_compact_plan(CompactPlan& plan, const cles_scheme& s, const int n3[3]
     P.seg_base = n / S;
     P.seg_rem = n % S;
     if (P.seg_base + (P.seg_rem ? 1 : 0) > kMaxSeg) throw Error(CLES_EINVAL, "segment longer than the register tile");
-    if (S == 1) P.pcr = 0;
+    // cyclic reduction only where the dense inverse would be large (2S > 64);
+    // below that one dot product per interface value is cheaper than log2(S) barriers
+    if (S == 1 || 2 * S <= 64) P.pcr = 0;
     int LB = 32;
     while (LB > 1 && LB * S > 512) LB /= 2;
     if (dim == 0) {
@@ -316,8 +317,11 @@ void build_compact_plan(CompactPlan& plan, const cles_scheme& s, const int n3[3]
     }
     if (LB * S > 512) throw Error(CLES_EINVAL, "line too long for one CTA");
     const int LB_full = LB;
-    // few lines: fewer per CTA so that more SMs take part
-    while (LB > 1 && (P.lines + LB - 1) / LB < 148) LB /= 2;
+    if (P.lines < LB) {
+        int l = 1;
+        while (l < P.lines) l *= 2;
+        LB = std::max(1, std::min(LB, l));
+    }
     P.LB = LB;
     P.hasred = (periodic || S > 1) ? 1 : 0;
 

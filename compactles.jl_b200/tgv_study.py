@@ -5,7 +5,8 @@ Two cases:
 * ``readme64``: the case behind the README's quoted dissipation peak
   (docs/figures/readme_header.jl:24-95): Re 1600 (mu0 = 1/1600), c0 = 10,
   p = c0^2/gamma + (cos 2x + cos 2y)(cos 2z + 2)/16, 64^3, artificial
-  properties off, cfl 0.6, filter every step, run to t = 12 with nmax 10000;
+  properties off, cfl 0.6, filter every step, run to t = 12 with nmax 10000
+  (scaled by n/64 on finer grids);
   kinetic energy every 10 steps, the centred difference of it, a 5-point mean,
   and its maximum.  The README quotes eps = 0.01265 at t = 9.13
   (README.md:13-16).
@@ -106,7 +107,7 @@ def run_case(cl, case, n, precision, tfinal=None):
     if case == "readme64":
         tfinal = 12.0 if tfinal is None else tfinal
         times, energy = [0.0], [s.kinetic_energy()]
-        nmax = 10_000
+        nmax = 10_000 * max(1, n // 64)   # the README run's cap at 64^3, scaled with the step count
         while s.t < tfinal and s.steps < nmax:
             s.run(tfinal, min(nmax, s.steps + 10))
             if s.steps % 10 == 0:

@@ -284,6 +284,20 @@ int  cles_get_field(cles_solver* s, int which, double* host, int layout);
 int  cles_get_clock(const cles_solver* s, double* t, int64_t* step, double* cfl);
 int  cles_set_clock(cles_solver* s, double t, int64_t step, double cfl);
 
+/* Checkpoint / restart in the reference's raw binary format.
+ * cles_checkpoint_save replaces save_checkpoint(solver, Q, prefix)
+ * (src/io.jl:8-41): it writes `prefix.r0000.ckpt` (one rank: n_local =
+ * n_global, coords = 0), little-endian: UInt64 magic 0x434c4553434b5054,
+ * Int64 n_cons, Int64 n_global[3], Int64 n_local[3], Int64 coords[3],
+ * Float64 t, Int64 step, then the interior of Q as Float64 in Julia order
+ * (x fastest, conserved component slowest), straight from the device state.
+ * cles_checkpoint_load replaces load_checkpoint!(solver, Q, prefix)
+ * (src/io.jl:43-72): it checks the magic, the conserved layout, the global
+ * grid, the decomposition and the rank layout (CLES_EINVAL with the
+ * reference's message on a mismatch) and restores the state, t and step. */
+int  cles_checkpoint_save(cles_solver* s, const char* prefix);
+int  cles_checkpoint_load(cles_solver* s, const char* prefix);
+
 /* check_step(control, dt, rho_min, dt_seen, step, t, cfl)
  * (src/stepcontrol.jl:184-204); *reason = CLES_FAIL_* (CLES_FAIL_NONE = accepted). */
 int  cles_check_step(const cles_step_control* control, double dt, double rho_min,

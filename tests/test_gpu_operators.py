@@ -146,7 +146,8 @@ def test_apply_along_tile_kernels(orc, scheme, periodic, dim, n, dtype):
     """Lines with enough lines per plan for the 32-point segments of the tile
     kernels: TMA tiles for y/z, cp.async transposed tiles for x (closed lines,
     C10, and the periodic tridiagonal ones)."""
-    ng = tuple(n if k == dim - 1 else 36 for k in range(3))
+    # 96 x 96 lines: at least one group of 32 lines per SM, as the tile kernels require
+    ng = tuple(n if k == dim - 1 else 96 for k in range(3))
     per = tuple(1 if (k != dim - 1 or periodic) else 0 for k in range(3))
     g = orc.grid(ng, per)
     f = _field(orc, g, seed=n + 7 * dim)
