@@ -118,6 +118,29 @@ class cles_nasa9_interval(C.Structure):
     ]
 
 
+CLES_BC_NOSLIP_WALL = 3
+CLES_BC_EXTRAPOLATION = 4
+CLES_BC_NSCBC_OUTFLOW = 5
+CLES_BC_NSCBC_INFLOW = 6
+
+
+class cles_bc_params(C.Structure):
+    _fields_ = [
+        ("Twall", C.c_double),
+        ("pinf", C.c_double),
+        ("sigma", C.c_double),
+        ("Lref", C.c_double),
+        ("beta_t", C.c_double),
+        ("u", C.c_double * 3),
+        ("T_ion", C.c_double),
+        ("Y", C.c_double * CLES_MAX_SPECIES),
+        ("eta_u", C.c_double),
+        ("eta_T", C.c_double),
+        ("eta_t", C.c_double),
+        ("eta_Y", C.c_double),
+    ]
+
+
 class cles_solver_desc(C.Structure):
     _fields_ = [
         ("n_global", C.c_int * 3),
@@ -125,6 +148,11 @@ class cles_solver_desc(C.Structure):
         ("origin", C.c_double * 3),
         ("bc", (C.c_int * 2) * 3),
         ("bc_state", ((C.c_double * (CLES_MAX_SPECIES + 4)) * 2) * 3),
+        ("bc_params", (cles_bc_params * 2) * 3),
+        ("bc_switchable", (C.c_int * 2) * 3),
+        ("bc_after", (C.c_int * 2) * 3),
+        ("bc_after_params", (cles_bc_params * 2) * 3),
+        ("bc_after_state", ((C.c_double * (CLES_MAX_SPECIES + 4)) * 2) * 3),
         ("n_species", C.c_int),
         ("R", C.c_double * CLES_MAX_SPECIES),
         ("gamma", C.c_double * CLES_MAX_SPECIES),

@@ -66,6 +66,8 @@ def lib():
         L.cles_apply_along.argtypes = [vp, vp, vp]
         L.cles_apply_along_batch.argtypes = [vp, vp, vp, C.c_int, C.c_int64]
         L.cles_apply_along_host.argtypes = [vp, vp, vp]
+        L.cles_solver_switch_bc.argtypes = [vp, C.c_int, C.c_int]
+        L.cles_solver_bc_switched.argtypes = [vp, C.c_int, C.c_int, C.POINTER(C.c_int)]
         L.cles_checkpoint_save.argtypes = [vp, C.c_char_p]
         L.cles_checkpoint_load.argtypes = [vp, C.c_char_p]
         L.cles_step_control_default.argtypes = [C.POINTER(abi.cles_step_control)]
@@ -338,6 +340,16 @@ class Solver:
 
     def set_clock(self, t, step, cfl):
         _check(lib().cles_set_clock(self.ptr, float(t), int(step), float(cfl)))
+
+    def switch_bc(self, dim, side):
+        """switch!(bc) for the SwitchableBC on face (dim 1..3, side 1 low / 2 high)
+        (src/boundary.jl:150-160); idempotent."""
+        _check(lib().cles_solver_switch_bc(self.ptr, int(dim) - 1, int(side) - 1))
+
+    def switched(self, dim, side):
+        out = C.c_int()
+        _check(lib().cles_solver_bc_switched(self.ptr, int(dim) - 1, int(side) - 1, C.byref(out)))
+        return bool(out.value)
 
     def save_checkpoint(self, prefix):
         """save_checkpoint(solver, Q, prefix) (src/io.jl:8-41): writes prefix.r0000.ckpt."""

@@ -457,6 +457,15 @@ int cles_set_clock(cles_solver* s, double t, int64_t step, double cfl) {
     API_END
 }
 
+int cles_solver_switch_bc(cles_solver* s, int dim, int side) { SOLVER_CALL(s->s->switch_bc(dim, side)) }
+
+int cles_solver_bc_switched(const cles_solver* s, int dim, int side, int* switched) {
+    API_BEGIN
+    if (!s || !switched) throw Error(CLES_EINVAL, "null argument");
+    *switched = s->s->bc_switched(dim, side) ? 1 : 0;
+    API_END
+}
+
 // ------------------------------------------------------------ checkpoints --
 namespace {
 constexpr uint64_t kCkptMagic = 0x434c4553434b5054ull;   // "CLES CKPT" (src/io.jl:6)

@@ -652,8 +652,118 @@ __global__ void k_bc_plane(double* __restrict__ Q, Grid3 g, int d, int side, int
             const double mn = Q[I + cells * mc];
             Q[I + cells * (Ns + 3)] -= 0.5 * mn * mn / r;
             Q[I + cells * mc] = 0;
+        } else if (kind == CLES_BC_NOSLIP_WALL) {
+            // enforce!(::NoSlipWallBC) (src/boundary.jl:245-265)
+            double r = 0.0;
+            for (int sp = 0; sp < Ns; ++sp) r += Q[I + cells * sp];
+            const double m1 = Q[I + cells * Ns], m2 = Q[I + cells * (Ns + 1)], m3 = Q[I + cells * (Ns + 2)];
+            const double ke = 0.5 * (m1 * m1 + m2 * m2 + m3 * m3) / r;
+            Q[I + cells * (Ns + 3)] -= ke;
+            Q[I + cells * Ns] = 0;
+            Q[I + cells * (Ns + 1)] = 0;
+            Q[I + cells * (Ns + 2)] = 0;
+            if (st.iso) {
+                // wall_internal_energy (src/boundary.jl:194-211)
+                double re = 0.0;
+                for (int sp = 0; sp < Ns; ++sp) re += Q[I + cells * sp] * st.ew[sp];
+                Q[I + cells * (Ns + 3)] = st.ew_times_T ? re * st.Twall : re;
+            }
+        } else if (kind == CLES_BC_EXTRAPOLATION) {
+            // enforce!(::ExtrapolationBC) (src/boundary.jl:267-278): copy the adjacent interior plane
+            const int64_t J = I + (side == 0 ? stv[d] : -stv[d]);
+            for (int c = 0; c < Ns + 4; ++c) Q[I + cells * c] = Q[J + cells * c];
         } else {
             for (int c = 0; c < Ns + 4; ++c) Q[I + cells * c] = st.q[c];
+        }
+    }
+}
+
+// correct_rhs!(::NSCBCOutflowBC) (src/nscbc.jl:59-157) and
+// correct_rhs!(::NSCBCInflowBC) with constant targets (src/nscbc.jl:220-307):
+// LODI wave-amplitude corrections of dQ on one boundary plane.
+template <typename F, bool N9>
+__global__ void k_nscbc(F* __restrict__ dQ, const F* __restrict__ prim, const F* __restrict__ g,
+                        const F* __restrict__ gty, int ngty, const F* __restrict__ dpd, const F* __restrict__ dpt0,
+                        const F* __restrict__ dpt1, const F* __restrict__ drd, Grid3 gr, int d, int side, int Ns,
+                        PhysConst pc, NscbcParams bp) {
+    const int o1 = d == 0 ? 1 : 0, o2 = d == 2 ? 1 : 2;
+    const int64_t plane = (int64_t)gr.n[o1] * gr.n[o2];
+    const int64_t cells = (int64_t)gr.n[0] * gr.n[1] * gr.n[2];
+    const int64_t stv[3] = {1, (int64_t)gr.n[0], (int64_t)gr.n[0] * gr.n[1]};
+    const int wall = side == 0 ? 0 : gr.n[d] - 1;
+    const int t1 = d == 0 ? 1 : 0, t2 = d == 2 ? 1 : 2;   // transverse dims
+    GRID_STRIDE(q, plane) {
+        const int a = (int)(q % gr.n[o1]), b = (int)(q / gr.n[o1]);
+        const int64_t I = a * stv[o1] + b * stv[o2] + (int64_t)wall * stv[d];
+        auto P = [&](int slot) { return double(prim[I + cells * slot]); };
+        auto G = [&](int dd, int j) { return double(g[I + cells * (3 * dd + j)]); };
+        const double rho = P(P_RHO), c = P(P_C), p = P(P_P), Tp = P(P_T), cpm = P(P_CP);
+        const double uv[3] = {P(P_U), P(P_V), P(P_W)};
+        const double un = uv[d];
+        const double Ma = fabs(un) / c;
+        if (!(Ma < 1)) continue;   // supersonic: no correction
+        const double dpn = double(dpd[I]);
+        const double dun = G(d, d);
+        const double Rm = p / (rho * Tp);
+        const double phi = cpm / Rm - 1;   // eos_phi, either mixture (src/physics.jl:142-145, 457-460)
+        const double ke = 0.5 * (uv[0] * uv[0] + uv[1] * uv[1] + uv[2] * uv[2]);
+        const int m0 = Ns, ie = Ns + 3;
+        if (bp.kind == CLES_BC_NSCBC_OUTFLOW) {
+            const double sgn = side == 1 ? -1.0 : 1.0;
+            const double Lcomp = side == 1 ? (un - c) * (dpn - rho * c * dun) : (un + c) * (dpn + rho * c * dun);
+            double tin = 0.0;
+            if (bp.act[t1]) {
+                const double ut = uv[t1];
+                tin += ut * double(dpt0[I]) + rho * c * c * G(t1, t1) + sgn * rho * c * ut * G(t1, d);
+            }
+            if (bp.act[t2]) {
+                const double ut = uv[t2];
+                tin += ut * double(dpt1[I]) + rho * c * c * G(t2, t2) + sgn * rho * c * ut * G(t2, d);
+            }
+            const double bt = bp.beta_t < 0 ? Ma : bp.beta_t;
+            const double K = bp.sigma * (1 - Ma * Ma) * c / bp.Lref;
+            const double dL = K * (p - bp.pinf) - bt * tin - Lcomp;
+            const double d1 = dL / (2 * c * c);
+            const double d2 = dL / 2;
+            const double d3 = sgn * dL / (2 * rho * c);
+            for (int k = 0; k < Ns; ++k) dQ[I + cells * k] = F(double(dQ[I + cells * k]) - P(P_Y0 + k) * d1);
+            for (int aa = 0; aa < 3; ++aa)
+                dQ[I + cells * (m0 + aa)] =
+                    F(double(dQ[I + cells * (m0 + aa)]) - (uv[aa] * d1 + (aa == d ? rho * d3 : 0.0)));
+            dQ[I + cells * ie] = F(double(dQ[I + cells * ie]) - (ke * d1 + phi * d2 + rho * un * d3));
+        } else {
+            const bool low = side == 0;
+            const double drn = double(drd[I]);
+            const double K = c / bp.Lref;
+            const double L1c = (un - c) * (dpn - rho * c * dun);
+            const double L5c = (un + c) * (dpn + rho * c * dun);
+            const double L2c = un * (c * c * drn - dpn);
+            const double rel = bp.eta_u * rho * c * c * (1 - Ma * Ma) / bp.Lref * (un - bp.u[d]);
+            const double dL1 = low ? 0.0 : (-rel - L1c);
+            const double dL5 = low ? (rel - L5c) : 0.0;
+            const double dL2 = bp.eta_T * rho * (c * c * c) * (bp.T - Tp) / (bp.Lref * Tp) - L2c;
+            const double d1 = dL2 / (c * c) + (dL5 + dL1) / (2 * c * c);
+            const double d2 = (dL5 + dL1) / 2;
+            const double d3 = (dL5 - dL1) / (2 * rho * c);
+            const double d4 = bp.eta_t * K * (uv[t1] - bp.u[t1]) - un * G(d, t1);
+            const double d5 = bp.eta_t * K * (uv[t2] - bp.u[t2]) - un * G(d, t2);
+            const double cvm = cpm - Rm;
+            double sphiY = 0.0;
+            for (int k = 0; k < Ns; ++k) {
+                const double Yk = P(P_Y0 + k);
+                const double gY = ngty > 1 ? double(gty[I + cells * (d * ngty + 1 + k)]) : 0.0;
+                const double dLs = bp.eta_Y * K * (Yk - bp.Y[k]) - un * gY;
+                dQ[I + cells * k] = F(double(dQ[I + cells * k]) - (Yk * d1 + rho * dLs));
+                // eos_dphi_dY (src/physics.jl:147-152, 462-470)
+                const double cvk = N9 ? n9_cp(pc, k, Tp) - pc.Rk[k] : pc.cvk[k];
+                sphiY += (cvk * Rm - pc.Rk[k] * cvm) / (Rm * Rm) * dLs;
+            }
+            for (int aa = 0; aa < 3; ++aa) {
+                const double extra = aa == d ? rho * d3 : (aa == t1 ? rho * d4 : rho * d5);
+                dQ[I + cells * (m0 + aa)] = F(double(dQ[I + cells * (m0 + aa)]) - (uv[aa] * d1 + extra));
+            }
+            dQ[I + cells * ie] = F(double(dQ[I + cells * ie]) -
+                                   (ke * d1 + phi * d2 + p * sphiY + rho * (un * d3 + uv[t1] * d4 + uv[t2] * d5)));
         }
     }
 }
@@ -844,6 +954,22 @@ void bc_plane(double* Q, const Grid3& g, int d, int side, int Ns, int kind, cons
     k_bc_plane<<<grid_for(plane), kThreads, 0, st>>>(Q, g, d, side, Ns, kind, s);
     count_launch();
     check_launch("k_bc_plane");
+}
+
+template <typename F>
+void Pointwise<F>::nscbc(F* dQ, const F* prim, const F* g, const F* gty, int ngty, const F* dpd, const F* dpt0,
+                         const F* dpt1, const F* drd, const Grid3& gr, int d, int side, int Ns, const PhysConst& pc,
+                         const NscbcParams& bp, cudaStream_t st) {
+    const int o1 = d == 0 ? 1 : 0, o2 = d == 2 ? 1 : 2;
+    const int64_t plane = (int64_t)gr.n[o1] * gr.n[o2];
+    if (pc.eos == CLES_EOS_NASA9)
+        k_nscbc<F, true><<<grid_for(plane), kThreads, 0, st>>>(dQ, prim, g, gty, ngty, dpd, dpt0, dpt1, drd, gr, d, side,
+                                                               Ns, pc, bp);
+    else
+        k_nscbc<F, false><<<grid_for(plane), kThreads, 0, st>>>(dQ, prim, g, gty, ngty, dpd, dpt0, dpt1, drd, gr, d,
+                                                                side, Ns, pc, bp);
+    count_launch();
+    check_launch("k_nscbc");
 }
 
 int64_t rate_partials(int64_t cells) { return (int64_t)grid_for(cells); }

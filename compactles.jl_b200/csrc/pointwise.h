@@ -33,6 +33,8 @@ double nasa9_h_over_R(const cles_nasa9_interval& iv, double T);
 // Fill the NASA-9 part of a PhysConst from a descriptor; throws on a bad table
 // (the checks of Nasa9Species, src/physics.jl:322-345).
 void nasa9_setup(PhysConst& pc, const cles_solver_desc& d);
+// e_k(T) of a NASA-9 descriptor on the host (species_energy)
+double nasa9_species_energy(const cles_solver_desc& d, int k, double T);
 
 struct Grid3 {
     int n[3];
@@ -44,8 +46,24 @@ struct Weights3 {
     double w[3];
 };
 
+// State of one enforced face condition: the Dirichlet state, or the wall
+// energy of an isothermal no-slip wall, rho e = (sum_k Q_k ew_k) * Twall for an
+// ideal mixture (ew_k = cv_k) or sum_k Q_k e_k(Twall) for NASA-9 (ew_k = e_k(Twall)).
 struct BcState {
     double q[CLES_MAX_SPECIES + 4];
+    double ew[CLES_MAX_SPECIES];
+    double Twall;
+    int iso;          // isothermal no-slip wall
+    int ew_times_T;   // ideal-mixture form of the wall energy
+};
+
+// One characteristic (NSCBC) face, parameters resolved on the host.
+struct NscbcParams {
+    int kind;         // CLES_BC_NSCBC_OUTFLOW or CLES_BC_NSCBC_INFLOW
+    int act[3];       // active dimensions
+    double Lref;      // > 0
+    double pinf, sigma, beta_t;
+    double u[3], T, Y[CLES_MAX_SPECIES], eta_u, eta_T, eta_t, eta_Y;
 };
 
 template <typename F>
@@ -79,6 +97,13 @@ struct Pointwise {
                             double mu0, cudaStream_t st);
     static void convert(const double* a, F* b, int64_t n, cudaStream_t st);
     static void to_double(const F* a, double* b, int64_t n, cudaStream_t st);
+    // correct_rhs! of an NSCBC face (src/nscbc.jl:59-307) on the plane of
+    // (d, side): dpd = dp/dx_d, dpt0/dpt1 = dp along the two transverse dims
+    // (outflow, unread when inactive), drd = drho/dx_d (inflow); gty holds
+    // [dT, dY_k] per dimension (ngty fields each).
+    static void nscbc(F* dQ, const F* prim, const F* g, const F* gty, int ngty, const F* dpd, const F* dpt0,
+                      const F* dpt1, const F* drd, const Grid3& gr, int d, int side, int Ns, const PhysConst& pc,
+                      const NscbcParams& bp, cudaStream_t st);
 };
 
 void bc_plane(double* Q, const Grid3& g, int d, int side, int Ns, int kind, const BcState& s, cudaStream_t st);

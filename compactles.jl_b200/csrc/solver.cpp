@@ -75,8 +75,17 @@ public:
             if (p0 != p1) throw Error(CLES_EINVAL, "dimension " + std::to_string(k + 1) + " mixes periodic and non-periodic conditions");
             if (d.n_global[k] < 1) throw Error(CLES_EINVAL, "n_global must be >= 1");
             if (d.n_global[k] == 1 && !p0) throw Error(CLES_EINVAL, "collapsed dimension must use (PeriodicBC(), PeriodicBC())");
-            for (int s = 0; s < 2; ++s)
-                if (d.bc[k][s] < CLES_BC_PERIODIC || d.bc[k][s] > CLES_BC_DIRICHLET) throw Error(CLES_EINVAL, "unknown boundary condition");
+            for (int s = 0; s < 2; ++s) {
+                if (d.bc[k][s] < CLES_BC_PERIODIC || d.bc[k][s] > CLES_BC_NSCBC_INFLOW)
+                    throw Error(CLES_EINVAL, "unknown boundary condition");
+                if (d.bc_switchable[k][s]) {
+                    // SwitchableBC(before, after) (src/boundary.jl:137-148)
+                    if (d.bc_after[k][s] < CLES_BC_PERIODIC || d.bc_after[k][s] > CLES_BC_NSCBC_INFLOW)
+                        throw Error(CLES_EINVAL, "unknown boundary condition");
+                    if ((d.bc_after[k][s] == CLES_BC_PERIODIC) != (d.bc[k][s] == CLES_BC_PERIODIC))
+                        throw Error(CLES_EINVAL, "SwitchableBC: both conditions must agree on periodicity");
+                }
+            }
             g_.n[k] = d.n_global[k];
             g_.active[k] = d.n_global[k] > 1;
             g_.periodic[k] = g_.active[k] ? p0 : 1;
@@ -156,15 +165,96 @@ public:
             if (g_.active[k]) launch_compact(*filt_[k], view(f), view(f), count, OUT_STORE, st_);
     }
 
+    // The condition face (k, s) acts as now: a switchable face forwards to its
+    // `after` condition once switched (src/boundary.jl:170-183).
+    int face_kind(int k, int s) const {
+        return desc.bc_switchable[k][s] && switched_[k][s] ? desc.bc_after[k][s] : desc.bc[k][s];
+    }
+    const cles_bc_params& face_params(int k, int s) const {
+        return desc.bc_switchable[k][s] && switched_[k][s] ? desc.bc_after_params[k][s] : desc.bc_params[k][s];
+    }
+    const double* face_state(int k, int s) const {
+        return desc.bc_switchable[k][s] && switched_[k][s] ? desc.bc_after_state[k][s] : desc.bc_state[k][s];
+    }
+    bool any_nscbc() const {
+        for (int k = 0; k < 3; ++k)
+            for (int s = 0; s < 2; ++s)
+                if (g_.active[k] && (face_kind(k, s) == CLES_BC_NSCBC_OUTFLOW || face_kind(k, s) == CLES_BC_NSCBC_INFLOW))
+                    return true;
+        return false;
+    }
+    void switch_bc(int k, int s) override {
+        if (k < 0 || k > 2 || s < 0 || s > 1 || !desc.bc_switchable[k][s])
+            throw Error(CLES_EINVAL, "face is not a SwitchableBC");
+        switched_[k][s] = true;
+    }
+    bool bc_switched(int k, int s) const override {
+        if (k < 0 || k > 2 || s < 0 || s > 1) throw Error(CLES_EINVAL, "no such face");
+        return switched_[k][s];
+    }
+
     void apply_bcs() override {
+        // apply_bcs! (src/boundary.jl:280-286): active dims, low then high face
         for (int k = 0; k < 3; ++k) {
             if (!g_.active[k]) continue;
             for (int s = 0; s < 2; ++s) {
-                const int bc = desc.bc[k][s];
-                if (bc == CLES_BC_PERIODIC) continue;
+                const int bc = face_kind(k, s);
+                if (bc == CLES_BC_PERIODIC || bc == CLES_BC_NSCBC_OUTFLOW || bc == CLES_BC_NSCBC_INFLOW) continue;
                 BcState bs;
-                for (int c = 0; c < ncons_; ++c) bs.q[c] = desc.bc_state[k][s][c];
+                std::memset(&bs, 0, sizeof(bs));
+                const double* q = face_state(k, s);
+                for (int c = 0; c < ncons_; ++c) bs.q[c] = q[c];
+                if (bc == CLES_BC_NOSLIP_WALL) {
+                    const double Tw = face_params(k, s).Twall;
+                    bs.iso = std::isnan(Tw) ? 0 : 1;
+                    bs.Twall = Tw;
+                    bs.ew_times_T = desc.eos == CLES_EOS_IDEAL ? 1 : 0;
+                    if (bs.iso)
+                        for (int sp = 0; sp < Ns_; ++sp)
+                            bs.ew[sp] = desc.eos == CLES_EOS_IDEAL ? pc_.cvk[sp] : nasa9_species_energy(desc, sp, Tw);
+                }
                 bc_plane(Q_.as<double>(), g_, k, s, Ns_, bc, bs, st_);
+            }
+        }
+    }
+
+    // correct_rhs! of the characteristic faces (src/rhs.jl:688-691), after the
+    // flux divergence and before any RK update
+    void correct_rhs_nscbc() {
+        for (int k = 0; k < 3; ++k) {
+            if (!g_.active[k]) continue;
+            for (int s = 0; s < 2; ++s) {
+                const int bc = face_kind(k, s);
+                if (bc != CLES_BC_NSCBC_OUTFLOW && bc != CLES_BC_NSCBC_INFLOW) continue;
+                const cles_bc_params& bp = face_params(k, s);
+                NscbcParams np;
+                std::memset(&np, 0, sizeof(np));
+                np.kind = bc;
+                for (int j = 0; j < 3; ++j) np.act[j] = g_.active[j];
+                np.Lref = bp.Lref > 0 ? bp.Lref : desc.L[k];
+                np.pinf = bp.pinf; np.sigma = bp.sigma; np.beta_t = bp.beta_t;
+                for (int j = 0; j < 3; ++j) np.u[j] = bp.u[j];
+                np.T = bp.T_ion;
+                for (int sp = 0; sp < Ns_; ++sp) np.Y[sp] = bp.Y[sp];
+                np.eta_u = bp.eta_u; np.eta_T = bp.eta_T; np.eta_t = bp.eta_t; np.eta_Y = bp.eta_Y;
+                // one-sided derivatives from the closure rows (full-field applications);
+                // scratch 0, 3, 4 are free once the fluxes are assembled (2 holds the
+                // last sensor, which get_field exposes)
+                F* dpd = scratch(0);
+                F* dt0 = scratch(3);
+                F* dt1 = scratch(4);
+                launch_compact(*deriv_[k], view(prim(P_P)), view(dpd), 1, OUT_STORE, st_);
+                const int t1 = k == 0 ? 1 : 0, t2 = k == 2 ? 1 : 2;
+                F* drd = nullptr;
+                if (bc == CLES_BC_NSCBC_OUTFLOW) {
+                    if (g_.active[t1]) launch_compact(*deriv_[t1], view(prim(P_P)), view(dt0), 1, OUT_STORE, st_);
+                    if (g_.active[t2]) launch_compact(*deriv_[t2], view(prim(P_P)), view(dt1), 1, OUT_STORE, st_);
+                } else {
+                    drd = dt0;
+                    launch_compact(*deriv_[k], view(prim(P_RHO)), view(drd), 1, OUT_STORE, st_);
+                }
+                Pointwise<F>::nscbc(dQ_.as<F>(), prim_.as<F>(), g_u_.as<F>(), gty_.as<F>(), Ns_ == 1 ? 1 : 1 + Ns_, dpd,
+                                    dt0, dt1, drd, g_, k, s, Ns_, pc_, np, st_);
             }
         }
     }
@@ -209,6 +299,8 @@ public:
     // Returns true when `rk` was applied inside the last divergence launch.
     bool compute_rhs_impl(bool primitives_current, const RkEpilogue* rk) {
         using PW = Pointwise<F>;
+        const bool nscbc = any_nscbc();
+        if (nscbc) rk = nullptr;   // the boundary correction comes between the divergence and the update
         if (!primitives_current) PW::primitives(Q_.as<double>(), prim_.as<F>(), cells_, Ns_, pc_, st_, desc.art_enabled);
         // velocity gradients grad_u[d][j] (src/rhs.jl:596-603), one launch per dim for u, v, w
         for (int k = 0; k < 3; ++k)
@@ -240,6 +332,7 @@ public:
             first = false;
         }
         if (first) CLES_CUDA(cudaMemsetAsync(dQ_.p, 0, dQ_.bytes, st_));
+        if (nscbc) correct_rhs_nscbc();
         return fused;
     }
 
@@ -562,6 +655,7 @@ private:
     ClockConst cc_{};
     cudaGraphExec_t gexec_filter_ = nullptr, gexec_plain_ = nullptr;
     cudaStream_t cap_st_ = nullptr;
+    bool switched_[3][2] = {{false, false}, {false, false}, {false, false}};
 };
 
 }  // namespace
@@ -577,6 +671,14 @@ double nasa9_h_over_R(const cles_nasa9_interval& iv, double T) {
     const double T2 = T * T;
     return -a[0] / T + a[1] * std::log(T) + a[2] * T + a[3] * T2 / 2 + a[4] * (T2 * T) / 3 + a[5] * (T2 * T2) / 4 +
            a[6] * (T2 * T2 * T) / 5 + iv.b1;
+}
+
+double nasa9_species_energy(const cles_solver_desc& d, int k, double T) {
+    const int n = d.n_intervals[k];
+    int i = n - 1;
+    for (int j = 0; j < n - 1; ++j)
+        if (T <= d.nasa9[k][j].Tmax) { i = j; break; }
+    return d.R[k] * nasa9_h_over_R(d.nasa9[k][i], T) - d.R[k] * T;
 }
 
 void nasa9_setup(PhysConst& pc, const cles_solver_desc& d) {

@@ -59,6 +59,9 @@ public:
     virtual const double* graph_clock() const = 0;
     virtual void graph_end() = 0;
     virtual cudaStream_t stream() const = 0;
+    // switch!(::SwitchableBC) on face (dim, side)
+    virtual void switch_bc(int dim, int side) = 0;
+    virtual bool bc_switched(int dim, int side) const = 0;
 
     cles_solver_desc desc{};
     double t = 0.0, tstage = 0.0, dt_prev = 0.0, rate_prev = 0.0, cfl = 0.5;

@@ -111,7 +111,82 @@ class DirichletBC(BoundaryCondition):
         self.state = state
 
 
+class NoSlipWallBC(BoundaryCondition):
+    """NoSlipWallBC(; Twall=NaN) (src/boundary.jl:33-44): zero velocity on the
+    wall plane; a finite Twall also sets the wall's internal energy."""
+    code = abi.CLES_BC_NOSLIP_WALL
+
+    def __init__(self, Twall=float("nan")):
+        self.Twall = float(Twall)
+
+
+class ExtrapolationBC(BoundaryCondition):
+    """ExtrapolationBC() (src/boundary.jl:46-54): copy the adjacent interior plane."""
+    code = abi.CLES_BC_EXTRAPOLATION
+
+
+class NSCBCOutflowBC(BoundaryCondition):
+    """NSCBCOutflowBC(; pinf, sigma=0.25, Lref=0.0, beta_t=-1.0) (src/nscbc.jl:33-57)."""
+    code = abi.CLES_BC_NSCBC_OUTFLOW
+
+    def __init__(self, pinf, sigma=0.25, Lref=0.0, beta_t=-1.0):
+        self.pinf, self.sigma, self.Lref, self.beta_t = float(pinf), float(sigma), float(Lref), float(beta_t)
+
+
+class NSCBCInflowBC(BoundaryCondition):
+    """NSCBCInflowBC(; u, T_ion, Y=[1.0], eta_u=eta_T=eta_t=eta_Y=0.28, Lref=0.0)
+    (src/nscbc.jl:178-218), constant targets."""
+    code = abi.CLES_BC_NSCBC_INFLOW
+
+    def __init__(self, u, T_ion, Y=(1.0,), eta_u=0.28, eta_T=0.28, eta_t=0.28, eta_Y=0.28, Lref=0.0):
+        self.u = tuple(float(v) for v in u)
+        self.T_ion = float(T_ion)
+        self.Y = tuple(float(v) for v in Y)
+        self.eta_u, self.eta_T, self.eta_t, self.eta_Y = float(eta_u), float(eta_T), float(eta_t), float(eta_Y)
+        self.Lref = float(Lref)
+
+
+class SwitchableBC(BoundaryCondition):
+    """SwitchableBC(before, after) (src/boundary.jl:120-160): the face acts as
+    `before` until Solver.switch_bc(dim, side), then as `after`."""
+
+    def __init__(self, before, after):
+        if (before.code == abi.CLES_BC_PERIODIC) != (after.code == abi.CLES_BC_PERIODIC):
+            raise ValueError("SwitchableBC: both conditions must agree on periodicity")
+        if isinstance(before, SwitchableBC) or isinstance(after, SwitchableBC):
+            raise ValueError("SwitchableBC cannot wrap another SwitchableBC")
+        self.before, self.after = before, after
+        self.code = before.code
+
+
 PER3 = tuple((PeriodicBC(), PeriodicBC()) for _ in range(3))
+
+
+def _fill_face(bc, eos, ncons, params, state):
+    """Write one face condition's parameters and Dirichlet state; returns its code."""
+    p = params
+    p.Twall = float("nan")
+    p.sigma, p.beta_t = 0.25, -1.0
+    p.eta_u = p.eta_T = p.eta_t = p.eta_Y = 0.28
+    if bc.code == abi.CLES_BC_DIRICHLET:
+        q = conserved_from_prim(eos, bc.state)
+        for c in range(ncons):
+            state[c] = float(np.asarray(q[c]))
+    elif bc.code == abi.CLES_BC_NOSLIP_WALL:
+        p.Twall = bc.Twall
+    elif bc.code == abi.CLES_BC_NSCBC_OUTFLOW:
+        p.pinf, p.sigma, p.Lref, p.beta_t = bc.pinf, bc.sigma, bc.Lref, bc.beta_t
+    elif bc.code == abi.CLES_BC_NSCBC_INFLOW:
+        if len(bc.Y) != eos.nspecies:
+            raise ValueError(f"NSCBCInflowBC: target composition has {len(bc.Y)} entries; "
+                             f"the EOS has {eos.nspecies} species")
+        for j in range(3):
+            p.u[j] = bc.u[j]
+        p.T_ion = bc.T_ion
+        for k, y in enumerate(bc.Y):
+            p.Y[k] = y
+        p.eta_u, p.eta_T, p.eta_t, p.eta_Y, p.Lref = bc.eta_u, bc.eta_T, bc.eta_t, bc.eta_Y, bc.Lref
+    return bc.code
 
 
 # ------------------------------------------------------------------- Prim ----
@@ -221,11 +296,12 @@ def solver_desc(n_global, L_domain, bcs, deriv, filt, eos=None, transport=None, 
         if n_global[k] == 1 and lo.code != abi.CLES_BC_PERIODIC:
             raise ValueError(f"collapsed dimension {k + 1} must use (PeriodicBC(), PeriodicBC())")
         for s, bc in enumerate((lo, hi)):
-            d.bc[k][s] = bc.code
-            if bc.code == abi.CLES_BC_DIRICHLET:
-                q = conserved_from_prim(eos, bc.state)
-                for c in range(ncons):
-                    d.bc_state[k][s][c] = float(np.asarray(q[c]))
+            if isinstance(bc, SwitchableBC):
+                d.bc[k][s] = _fill_face(bc.before, eos, ncons, d.bc_params[k][s], d.bc_state[k][s])
+                d.bc_switchable[k][s] = 1
+                d.bc_after[k][s] = _fill_face(bc.after, eos, ncons, d.bc_after_params[k][s], d.bc_after_state[k][s])
+            else:
+                d.bc[k][s] = _fill_face(bc, eos, ncons, d.bc_params[k][s], d.bc_state[k][s])
     if eos.nspecies > abi.CLES_MAX_SPECIES:
         raise ValueError("too many species")
     d.n_species = eos.nspecies

@@ -64,6 +64,19 @@ extern "C" {
 #define CLES_BC_PERIODIC   0   /* PeriodicBC */
 #define CLES_BC_SLIPWALL   1   /* SlipWallBC, enforce! at src/boundary.jl:232-243 */
 #define CLES_BC_DIRICHLET  2   /* DirichletBC with a state constant in time (src/problem.jl:192-207) */
+#define CLES_BC_NOSLIP_WALL     3   /* NoSlipWallBC(Twall), enforce! at src/boundary.jl:245-265 */
+#define CLES_BC_EXTRAPOLATION   4   /* ExtrapolationBC, enforce! at src/boundary.jl:267-278 */
+#define CLES_BC_NSCBC_OUTFLOW   5   /* NSCBCOutflowBC, correct_rhs! at src/nscbc.jl:59-157 */
+#define CLES_BC_NSCBC_INFLOW    6   /* NSCBCInflowBC (constant targets), correct_rhs! at src/nscbc.jl:220-307 */
+
+/* Parameters of one face condition (unused fields are ignored). */
+typedef struct cles_bc_params {
+    double Twall;                       /* NoSlipWallBC: NaN = adiabatic, finite = isothermal */
+    double pinf, sigma, Lref, beta_t;   /* NSCBCOutflowBC (sigma 0.25, Lref <= 0 -> domain length, beta_t < 0 -> local Mach) */
+    double u[3], T_ion;                 /* NSCBCInflowBC targets */
+    double Y[CLES_MAX_SPECIES];         /* NSCBCInflowBC target composition (n_species entries) */
+    double eta_u, eta_T, eta_t, eta_Y;  /* NSCBCInflowBC relaxation (0.28 each); Lref above */
+} cles_bc_params;
 
 /* beta sensors (src/artificial.jl:50-57) */
 #define CLES_BETA_STRAIN        0
@@ -196,6 +209,15 @@ typedef struct cles_solver_desc {
     int    bc[3][2];             /* CLES_BC_* per (dim, side) */
     /* conserved state imposed on a CLES_BC_DIRICHLET face (constant in time) */
     double bc_state[3][2][CLES_MAX_SPECIES + 4];
+    cles_bc_params bc_params[3][2];
+    /* SwitchableBC(before, after) (src/boundary.jl:120-177): a face with
+     * bc_switchable set behaves as bc/bc_params/bc_state until
+     * cles_solver_switch_bc, then as bc_after/bc_after_params/bc_after_state.
+     * Both conditions must agree on periodicity. */
+    int    bc_switchable[3][2];
+    int    bc_after[3][2];
+    cles_bc_params bc_after_params[3][2];
+    double bc_after_state[3][2][CLES_MAX_SPECIES + 4];
     int    n_species;            /* IdealMixture species count */
     double R[CLES_MAX_SPECIES];  /* specific gas constants */
     double gamma[CLES_MAX_SPECIES];
@@ -295,6 +317,12 @@ int  cles_set_clock(cles_solver* s, double t, int64_t step, double cfl);
  * (src/io.jl:43-72): it checks the magic, the conserved layout, the global
  * grid, the decomposition and the rank layout (CLES_EINVAL with the
  * reference's message on a mismatch) and restores the state, t and step. */
+/* switch!(bc::SwitchableBC) (src/boundary.jl:150-160) on face (dim 0..2, side
+ * 0 low / 1 high): from now on the face acts as its `after` condition
+ * (idempotent; CLES_EINVAL if the face is not switchable). */
+int  cles_solver_switch_bc(cles_solver* s, int dim, int side);
+int  cles_solver_bc_switched(const cles_solver* s, int dim, int side, int* switched);
+
 int  cles_checkpoint_save(cles_solver* s, const char* prefix);
 int  cles_checkpoint_load(cles_solver* s, const char* prefix);
 

@@ -651,6 +651,18 @@ struct Solver {
     std::vector<double> flux[3][CLES_MAX_SPECIES + 4];
     double t = 0.0, tstage = 0.0, dt_prev = 0.0, rate_prev = 0.0, cfl = 0.5;
     int64_t step = 0;
+    bool switched[3][2] = {{false, false}, {false, false}, {false, false}};   // SwitchableBC state
+
+    // the condition a face acts as now (src/boundary.jl:170-183)
+    int face_kind(int d, int s) const {
+        return desc.bc_switchable[d][s] && switched[d][s] ? desc.bc_after[d][s] : desc.bc[d][s];
+    }
+    const cles_bc_params& face_params(int d, int s) const {
+        return desc.bc_switchable[d][s] && switched[d][s] ? desc.bc_after_params[d][s] : desc.bc_params[d][s];
+    }
+    const double* face_state(int d, int s) const {
+        return desc.bc_switchable[d][s] && switched[d][s] ? desc.bc_after_state[d][s] : desc.bc_state[d][s];
+    }
 
     double* comp(std::vector<double>& A, int cidx) { return A.data() + fs * cidx; }
     double* vel(int j) { return j == 0 ? u.data() : j == 1 ? v.data() : w.data(); }
@@ -976,6 +988,117 @@ void assemble_fluxes(Solver& S) {
     });
 }
 
+// Visit the interior points of the wall plane of (d, side).
+template <class Fn>
+void for_wallplane(const Decomp& D, int d, int side, Fn&& fn) {
+    const int wall = side == 0 ? 0 : D.nl[d] - 1;
+    int lo[3], hi[3];
+    for (int k = 0; k < 3; ++k) { lo[k] = 0; hi[k] = D.nl[k]; }
+    lo[d] = wall; hi[d] = wall + 1;
+    for (int k = lo[2]; k < hi[2]; ++k)
+        for (int j = lo[1]; j < hi[1]; ++j)
+            for (int i = lo[0]; i < hi[0]; ++i) fn(D.at(i + D.nhd[0], j + D.nhd[1], k + D.nhd[2]));
+}
+
+// eos_phi / eos_dphi_dY (src/physics.jl:142-152, 457-470); cv_k at T
+double eos_phi(double rho, double p, double T, double cp) {
+    const double Rm = p / (rho * T);
+    return cp / Rm - 1;
+}
+double eos_dphi_dY(const Solver& S, int k, double rho, double p, double T, double cp) {
+    const double Rm = p / (rho * T);
+    const double cvm = cp - Rm;
+    const double cvk = S.desc.eos == CLES_EOS_NASA9 ? n9_species_cp(S.desc, k, T) - S.Rk[k] : S.cvk[k];
+    return (cvk * Rm - S.Rk[k] * cvm) / (Rm * Rm);
+}
+
+// correct_rhs!(::NSCBCOutflowBC) (src/nscbc.jl:59-157), Cartesian (inv_h = 1)
+void nscbc_outflow(Solver& S, int d, int side) {
+    const cles_bc_params& bc = S.face_params(d, side);
+    deriv_along(S, S.tmp_a.data(), S.p.data(), d);
+    const int t1 = d == 0 ? 1 : 0, t2 = d == 2 ? 1 : 2;
+    const bool act1 = S.D.active[t1], act2 = S.D.active[t2];
+    if (act1) deriv_along(S, S.tmp_b.data(), S.p.data(), t1);
+    if (act2) deriv_along(S, S.sensor_sp.data(), S.p.data(), t2);
+    const double Lref = bc.Lref > 0 ? bc.Lref : S.desc.L[d];
+    const size_t fs = S.fs;
+    const double sgn = side == 1 ? -1.0 : 1.0;
+    for_wallplane(S.D, d, side, [&](size_t I) {
+        const double rho = S.rho[I], c = S.c[I], p = S.p[I];
+        const double uv[3] = {S.u[I], S.v[I], S.w[I]};
+        const double un = uv[d];
+        const double Ma = std::fabs(un) / c;
+        if (!(Ma < 1)) return;
+        const double dpn = 1.0 * S.tmp_a[I];
+        const double dun = S.grad_u[d][d][I];
+        const double Lcomp = side == 1 ? (un - c) * (dpn - rho * c * dun) : (un + c) * (dpn + rho * c * dun);
+        double tin = 0.0;
+        if (act1) {
+            const double ut = uv[t1];
+            tin += ut * 1.0 * S.tmp_b[I] + rho * c * c * S.grad_u[t1][t1][I] + sgn * rho * c * ut * S.grad_u[t1][d][I];
+        }
+        if (act2) {
+            const double ut = uv[t2];
+            tin += ut * 1.0 * S.sensor_sp[I] + rho * c * c * S.grad_u[t2][t2][I] + sgn * rho * c * ut * S.grad_u[t2][d][I];
+        }
+        const double bt = bc.beta_t < 0 ? Ma : bc.beta_t;
+        const double K = bc.sigma * (1 - Ma * Ma) * c / Lref;
+        const double dL = K * (p - bc.pinf) - bt * tin - Lcomp;
+        const double d1 = dL / (2 * c * c), d2 = dL / 2, d3 = sgn * dL / (2 * rho * c);
+        const double phi = eos_phi(rho, p, S.T[I], S.cp[I]);
+        const double ke = 0.5 * (uv[0] * uv[0] + uv[1] * uv[1] + uv[2] * uv[2]);
+        for (int k = 0; k < S.Ns; ++k) S.dQ[I + fs * k] -= S.Y[k][I] * d1;
+        for (int a = 0; a < 3; ++a) S.dQ[I + fs * S.i_mom[a]] -= uv[a] * d1 + (a == d ? rho * d3 : 0.0);
+        S.dQ[I + fs * S.i_energy] -= ke * d1 + phi * d2 + rho * un * d3;
+    });
+}
+
+// correct_rhs!(::NSCBCInflowBC) with constant targets (src/nscbc.jl:220-307)
+void nscbc_inflow(Solver& S, int d, int side) {
+    const cles_bc_params& bc = S.face_params(d, side);
+    deriv_along(S, S.tmp_a.data(), S.p.data(), d);
+    deriv_along(S, S.tmp_b.data(), S.rho.data(), d);
+    const double Lref = bc.Lref > 0 ? bc.Lref : S.desc.L[d];
+    const int t1 = d == 0 ? 1 : 0, t2 = d == 2 ? 1 : 2;
+    const size_t fs = S.fs;
+    const bool low = side == 0;
+    for_wallplane(S.D, d, side, [&](size_t I) {
+        const double rho = S.rho[I], c = S.c[I], p = S.p[I], Tp = S.T[I];
+        const double uv[3] = {S.u[I], S.v[I], S.w[I]};
+        const double un = uv[d];
+        const double Ma = std::fabs(un) / c;
+        if (!(Ma < 1)) return;
+        const double dpn = 1.0 * S.tmp_a[I], drn = 1.0 * S.tmp_b[I], dun = S.grad_u[d][d][I];
+        const double K = c / Lref;
+        const double L1c = (un - c) * (dpn - rho * c * dun);
+        const double L5c = (un + c) * (dpn + rho * c * dun);
+        const double L2c = un * (c * c * drn - dpn);
+        const double rel = bc.eta_u * rho * c * c * (1 - Ma * Ma) / Lref * (un - bc.u[d]);
+        const double dL1 = low ? 0.0 : (-rel - L1c);
+        const double dL5 = low ? (rel - L5c) : 0.0;
+        const double dL2 = bc.eta_T * rho * (c * c * c) * (bc.T_ion - Tp) / (Lref * Tp) - L2c;
+        const double d1 = dL2 / (c * c) + (dL5 + dL1) / (2 * c * c);
+        const double d2 = (dL5 + dL1) / 2;
+        const double d3 = (dL5 - dL1) / (2 * rho * c);
+        const double d4 = bc.eta_t * K * (uv[t1] - bc.u[t1]) - un * S.grad_u[d][t1][I];
+        const double d5 = bc.eta_t * K * (uv[t2] - bc.u[t2]) - un * S.grad_u[d][t2][I];
+        const double cpm = S.cp[I];
+        const double phi = eos_phi(rho, p, Tp, cpm);
+        const double ke = 0.5 * (uv[0] * uv[0] + uv[1] * uv[1] + uv[2] * uv[2]);
+        double sphiY = 0.0;
+        for (int k = 0; k < S.Ns; ++k) {
+            const double dLs = bc.eta_Y * K * (S.Y[k][I] - bc.Y[k]) - un * S.grad_Y[d][k][I];
+            S.dQ[I + fs * k] -= S.Y[k][I] * d1 + rho * dLs;
+            sphiY += eos_dphi_dY(S, k, rho, p, Tp, cpm) * dLs;
+        }
+        for (int a = 0; a < 3; ++a) {
+            const double extra = a == d ? rho * d3 : (a == t1 ? rho * d4 : rho * d5);
+            S.dQ[I + fs * S.i_mom[a]] -= uv[a] * d1 + extra;
+        }
+        S.dQ[I + fs * S.i_energy] -= ke * d1 + phi * d2 + p * sphiY + rho * (un * d3 + uv[t1] * d4 + uv[t2] * d5);
+    });
+}
+
 // compute_rhs! (src/rhs.jl:624-694), unitgeom branch.
 void compute_rhs(Solver& S, bool primitives_current) {
     const Decomp& D = S.D;
@@ -998,6 +1121,13 @@ void compute_rhs(Solver& S, bool primitives_current) {
             for_interior(D, [&](size_t I, int, int, int) { dq[I] -= S.tmp_a[I]; });
         }
     }
+    for (int d = 0; d < 3; ++d)
+        for (int side = 0; side < 2; ++side) {
+            if (!D.active[d]) continue;
+            const int bc = S.face_kind(d, side);
+            if (bc == CLES_BC_NSCBC_OUTFLOW) nscbc_outflow(S, d, side);
+            else if (bc == CLES_BC_NSCBC_INFLOW) nscbc_inflow(S, d, side);
+        }
 }
 
 // enforce! for SlipWallBC (src/boundary.jl:232-243) and a time-constant
@@ -1008,8 +1138,14 @@ void apply_bcs(Solver& S) {
     for (int d = 0; d < 3; ++d)
         for (int side = 0; side < 2; ++side) {
             if (!D.active[d]) continue;
-            const int bc = S.desc.bc[d][side];
-            if (bc == CLES_BC_PERIODIC) continue;
+            const int bc = S.face_kind(d, side);
+            if (bc == CLES_BC_PERIODIC || bc == CLES_BC_NSCBC_OUTFLOW || bc == CLES_BC_NSCBC_INFLOW) continue;
+            const double* bstate = S.face_state(d, side);
+            const double Twall = S.face_params(d, side).Twall;
+            int shift[3] = {0, 0, 0};
+            shift[d] = side == 0 ? 1 : -1;
+            const long sh = (long)D.at(D.nhd[0] + shift[0], D.nhd[1] + shift[1], D.nhd[2] + shift[2]) -
+                            (long)D.at(D.nhd[0], D.nhd[1], D.nhd[2]);
             const int wall = side == 0 ? 0 : D.nl[d] - 1;
             int lo[3], hi[3];
             for (int k = 0; k < 3; ++k) { lo[k] = 0; hi[k] = D.nl[k]; }
@@ -1026,7 +1162,31 @@ void apply_bcs(Solver& S) {
                             S.Q[I + fs * S.i_energy] -= 0.5 * mn * mn / r;
                             S.Q[I + fs * mc] = 0;
                         } else if (bc == CLES_BC_DIRICHLET) {
-                            for (int cc = 0; cc < S.ncons; ++cc) S.Q[I + fs * cc] = S.desc.bc_state[d][side][cc];
+                            for (int cc = 0; cc < S.ncons; ++cc) S.Q[I + fs * cc] = bstate[cc];
+                        } else if (bc == CLES_BC_NOSLIP_WALL) {
+                            // enforce!(::NoSlipWallBC) (src/boundary.jl:245-265)
+                            double r = 0.0;
+                            for (int sp = 0; sp < S.Ns; ++sp) r += S.Q[I + fs * sp];
+                            const double q1 = S.Q[I + fs * S.i_mom[0]], q2 = S.Q[I + fs * S.i_mom[1]],
+                                         q3 = S.Q[I + fs * S.i_mom[2]];
+                            const double ke = 0.5 * (q1 * q1 + q2 * q2 + q3 * q3) / r;
+                            S.Q[I + fs * S.i_energy] -= ke;
+                            for (int a = 0; a < 3; ++a) S.Q[I + fs * S.i_mom[a]] = 0;
+                            if (!std::isnan(Twall)) {
+                                // wall_internal_energy (src/boundary.jl:194-211)
+                                double re = 0.0;
+                                if (S.desc.eos == CLES_EOS_NASA9) {
+                                    for (int sp = 0; sp < S.Ns; ++sp)
+                                        re += S.Q[I + fs * sp] * n9_species_e(S.desc, sp, Twall);
+                                } else {
+                                    for (int sp = 0; sp < S.Ns; ++sp) re += S.Q[I + fs * sp] * S.cvk[sp];
+                                    re *= Twall;
+                                }
+                                S.Q[I + fs * S.i_energy] = re;
+                            }
+                        } else if (bc == CLES_BC_EXTRAPOLATION) {
+                            // enforce!(::ExtrapolationBC) (src/boundary.jl:267-278)
+                            for (int cc = 0; cc < S.ncons; ++cc) S.Q[I + fs * cc] = S.Q[(size_t)((long)I + sh) + fs * cc];
                         }
                     }
         }
@@ -1263,6 +1423,13 @@ Solver* solver_create(const cles_solver_desc& A) {
         if (p0 != p1) { set_err("dimension " + std::to_string(d + 1) + " mixes periodic and non-periodic conditions"); return nullptr; }
         if (A.n_global[d] < 1) { set_err("n_global must be >= 1"); return nullptr; }
         if (A.n_global[d] == 1 && !p0) { set_err("collapsed dimension must use (PeriodicBC(), PeriodicBC())"); return nullptr; }
+        for (int s = 0; s < 2; ++s) {
+            if (A.bc[d][s] < CLES_BC_PERIODIC || A.bc[d][s] > CLES_BC_NSCBC_INFLOW) { set_err("unknown boundary condition"); return nullptr; }
+            if (A.bc_switchable[d][s] && ((A.bc_after[d][s] == CLES_BC_PERIODIC) != (A.bc[d][s] == CLES_BC_PERIODIC))) {
+                set_err("SwitchableBC: both conditions must agree on periodicity");
+                return nullptr;
+            }
+        }
     }
     if (A.n_species < 1 || A.n_species > CLES_MAX_SPECIES) { set_err("bad species count"); return nullptr; }
     auto S = std::make_unique<Solver>();
@@ -1423,6 +1590,15 @@ double orc_nasa9_cp(const cles_solver_desc* d, int k, double T) { return n9_spec
 double orc_nasa9_h(const cles_solver_desc* d, int k, double T) { return n9_species_h(*d, k, T); }
 double orc_nasa9_e(const cles_solver_desc* d, int k, double T) { return n9_species_e(*d, k, T); }
 double orc_nasa9_temperature(const cles_solver_desc* d, double e, const double* Y) { return n9_temperature(*d, e, Y); }
+
+int orc_switch_bc(orc_solver* s, int d, int side) {
+    if (d < 0 || d > 2 || side < 0 || side > 1 || !s->s->desc.bc_switchable[d][side]) {
+        set_err("face is not a SwitchableBC");
+        return CLES_EINVAL;
+    }
+    s->s->switched[d][side] = true;
+    return 0;
+}
 
 int orc_check_step(const cles_step_control* c, double dt, double rho_min, double dt_seen) {
     return check_step(*c, dt, rho_min, dt_seen);

@@ -82,6 +82,7 @@ def lib():
             getattr(L, nm).argtypes = [C.POINTER(abi.cles_solver_desc), C.c_int, C.c_double]
         L.orc_nasa9_temperature.restype = C.c_double
         L.orc_nasa9_temperature.argtypes = [C.POINTER(abi.cles_solver_desc), C.c_double, _DP]
+        L.orc_switch_bc.argtypes = [C.c_void_p, C.c_int, C.c_int]
         L.orc_kinetic_energy.restype = C.c_double
         L.orc_kinetic_energy.argtypes = [C.c_void_p]
         L.orc_dissipation_rate.restype = C.c_double
@@ -246,6 +247,11 @@ class Solver:
         res = abi.cles_run_result()
         rc = lib().orc_run(self.ptr, float(tfinal), int(nmax), C.byref(res))
         return rc, res
+
+    def switch_bc(self, dim, side):
+        """switch!(::SwitchableBC) on face (dim 1..3, side 1 low / 2 high)."""
+        if lib().orc_switch_bc(self.ptr, int(dim) - 1, int(side) - 1):
+            raise ValueError(_err())
 
     def field(self, which):
         out = np.zeros(self.field_shape)
