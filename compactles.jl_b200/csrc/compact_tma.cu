@@ -92,7 +92,7 @@ __device__ __forceinline__ T tl(const double* d, const float* f, int i) {
 }
 
 template <typename T, int M, int MS>
-__global__ void __launch_bounds__(256, 1)
+__global__ void __launch_bounds__(MS == 16 ? 512 : 256, 1)
     k_compact_tma(const __grid_constant__ CUtensorMap map, const __grid_constant__ CompactParams P,
                   const __grid_constant__ TileLineParams TL,
                   const T* __restrict__ Gg, const FieldView out, const int mode, const int count, const int NS,
@@ -910,7 +910,9 @@ bool try_launch_tma(const CompactPlan& plan, const FieldView& in, const FieldVie
     if (mode == OUT_RK && !rkp) return false;
     if (!plan.has_tl && !plan.has_tg) return false;
     const CompactParams& P = plan.P;
-    if (P.dim == 0 || P.n > 256 || P.S * kLanes > 256) return false;
+    // 16-point segments run 16 warps per line group (512 threads), 32-point ones 8
+    const int max_threads = plan.has_tl && plan.TL.m == 16 ? 512 : 256;
+    if (P.dim == 0 || P.n > 256 || P.S * kLanes > max_threads) return false;
     if (!plan.has_tl) {
         const int64_t gx = (P.nx + kLanes - 1) / kLanes;
         if (gx * (P.dim == 1 ? P.nz : P.ny) * count < num_sms()) return false;   // see try_launch_xt

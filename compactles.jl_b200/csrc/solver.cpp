@@ -316,12 +316,18 @@ public:
                                OUT_STORE, st_);
         PW::fluxes(Q_.as<double>(), prim_.as<F>(), g_u_.as<F>(), gty_.as<F>(), art_.as<F>(), flux_.as<F>(), cells_, Ns_,
                    pc_, desc.mu0, desc.Pr, desc.Sc, st_);
-        // flux divergence dQ[c] = -sum_d D_d(F_dc) (src/rhs.jl:650-668), accumulated in the store
+        // flux divergence dQ[c] = -sum_d D_d(F_dc) (src/rhs.jl:650-668), accumulated in the store.
+        // With all three dims active the order is y, x, z: the first direction only
+        // stores (no read of dQ), the x kernel reads dQ with vector loads, and z,
+        // last, carries the RK update.  The sum differs from x, y, z by rounding.
+        int order[3] = {0, 1, 2};
+        if (g_.active[0] && g_.active[1] && g_.active[2]) { order[0] = 1; order[1] = 0; }
         int last = -1;
         for (int k = 0; k < 3; ++k)
             if (g_.active[k]) last = k;
         bool first = true, fused = false;
-        for (int k = 0; k < 3; ++k) {
+        for (int o = 0; o < 3; ++o) {
+            const int k = order[o];
             if (!g_.active[k]) continue;
             const FieldView fin = view(flux_.as<F>() + (size_t)cells_ * ncons_ * k);
             if (k == last && !first && rk && launch_compact_rk(*deriv_[k], fin, view(dQ_.as<F>()), ncons_, *rk, st_)) {
