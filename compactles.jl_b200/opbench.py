@@ -8,6 +8,7 @@ a_m ~ N(0, 1), phi_m ~ U[0, 2pi), seed 20261203 + field index.
 
   python compactles.jl_b200/opbench.py [--n 256] [--fields 5] [--reps 5]
   python compactles.jl_b200/opbench.py --ncu-case      # 3 + 3 launches for an ncu capture
+  python compactles.jl_b200/opbench.py --ncu-case closed   # the same on closed lines
 
 Algorithmic bytes per launch: every field read once and written once,
 2 * sizeof(T) * n^3 per field.  FP32 cases also report their error against
@@ -68,7 +69,7 @@ def run(args):
     results = []
     cases = [(p, dt) for p in (True, False) for dt in ("f64", "f32")]
     if args.ncu_case:
-        cases = [(True, "f64")]
+        cases = [(args.ncu_case != "closed", "f64")]
         schemes = {"c6": schemes["c6"]}
     if getattr(args, "cases", None):
         cases = args.cases
@@ -137,6 +138,7 @@ if __name__ == "__main__":
     p.add_argument("--n", type=int, default=256)
     p.add_argument("--fields", type=int, default=5)
     p.add_argument("--reps", type=int, default=5)
-    p.add_argument("--ncu-case", action="store_true")
+    p.add_argument("--ncu-case", nargs="?", const="periodic", default=None, choices=["periodic", "closed"],
+                   help="3 + 3 C6 FP64 launches (one warm, one captured per direction) for an ncu capture")
     p.add_argument("--keep", action="store_true", help=argparse.SUPPRESS)
     run(p.parse_args())
