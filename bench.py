@@ -246,9 +246,13 @@ def time_e2e(cl, torch, desc, Q0, steps, dist):
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1)
     info = S.info()
-    bytes_state = info.cells * info.n_cons * 8
+    # host to device: each component's whole padded block (contiguous copy,
+    # interior gathered on the device); device to host: the interior, plus the
+    # 16-byte rate read of the step
+    h2d = int(Qh.nbytes)
+    d2h = info.cells * info.n_cons * 8 + 16
     del S
-    return ms, bytes_state
+    return ms, (h2d, d2h)
 
 
 def cpu_sample(n, steps):
@@ -321,7 +325,7 @@ def run_ours(a):
         ms, sb = time_e2e(cl, torch, desc, Q0, k, dist)
         mm = dist.max(ms)
         out["e2e"] = {"value": aggregate(r["cells"], k, dist.world, mm), "unit": UNIT,
-                      "h2d_bytes_per_step": sb, "d2h_bytes_per_step": sb + 16,
+                      "h2d_bytes_per_step": sb[0], "d2h_bytes_per_step": sb[1],
                       "how": "cles_step_host: pinned padded host state in, one run! step, state out"}
     if dist.rank == 0 and dist.world == 1 and not a.no_cpu:
         v, th, secs = cpu_sample(a.cpu_n, a.cpu_steps)

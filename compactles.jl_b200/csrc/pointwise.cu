@@ -768,6 +768,17 @@ __global__ void k_nscbc(F* __restrict__ dQ, const F* __restrict__ prim, const F*
     }
 }
 
+__global__ void k_gather_interior(const double* __restrict__ padded, double* __restrict__ interior, int n0, int n1,
+                                  int n2, int p0, int p1, int p2) {
+    const int64_t cells = (int64_t)n0 * n1 * n2;
+    const int64_t F0 = n0 + 2 * p0, F1 = n1 + 2 * p1;
+    GRID_STRIDE(I, cells) {
+        const int64_t i = I % n0, r = I / n0;
+        const int64_t j = r % n1, k = r / n1;
+        interior[I] = padded[(i + p0) + F0 * ((j + p1) + F1 * (k + p2))];
+    }
+}
+
 template <typename F>
 __global__ void k_convert(const double* __restrict__ a, F* __restrict__ b, int64_t n) {
     GRID_STRIDE(I, n) b[I] = F(a[I]);
@@ -970,6 +981,13 @@ void Pointwise<F>::nscbc(F* dQ, const F* prim, const F* g, const F* gty, int ngt
                                                                 side, Ns, pc, bp);
     count_launch();
     check_launch("k_nscbc");
+}
+
+void gather_interior(const double* padded, double* interior, const int n[3], const int pad[3], cudaStream_t st) {
+    const int64_t cells = (int64_t)n[0] * n[1] * n[2];
+    k_gather_interior<<<grid_for(cells), kThreads, 0, st>>>(padded, interior, n[0], n[1], n[2], pad[0], pad[1], pad[2]);
+    count_launch();
+    check_launch("k_gather_interior");
 }
 
 int64_t rate_partials(int64_t cells) { return (int64_t)grid_for(cells); }

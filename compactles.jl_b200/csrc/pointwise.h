@@ -107,6 +107,8 @@ struct Pointwise {
 };
 
 void bc_plane(double* Q, const Grid3& g, int d, int side, int Ns, int kind, const BcState& s, cudaStream_t st);
+// Interior of one padded field (extents n + 2 pad, x fastest) into the interior layout.
+void gather_interior(const double* padded, double* interior, const int n[3], const int pad[3], cudaStream_t st);
 
 // Device clock of the graph-mode run loop: slots of a double[16] buffer.
 enum { DC_T = 0, DC_DT = 1, DC_RATE = 2, DC_RHO_MIN = 3, DC_FAILURE = 4, DC_STEP = 5, DC_DT_SEEN = 6, DC_DONE = 7 };

@@ -457,7 +457,20 @@ public:
 
     // ---------------------------------------------------------- transfers --
     void set_state(const double* Q, int layout) override {
-        copy_state_h2d(Q_.as<double>(), Q, g_.n, pad_, ncons_, layout, st_);
+        const int64_t fcells = (int64_t)(g_.n[0] + 2 * pad_[0]) * (g_.n[1] + 2 * pad_[1]) * (g_.n[2] + 2 * pad_[2]);
+        if (layout == CLES_LAYOUT_PADDED && fcells != cells_ && (size_t)fcells * sizeof(double) <= flux_.bytes) {
+            // A pitched host-to-device copy of the interior moves 2 KB rows at
+            // about half the link rate; each component's whole padded block goes
+            // over contiguously instead, into the flux buffer (dead between RHS
+            // evaluations), and a kernel gathers the interior.
+            double* stage = flux_.as<double>();
+            for (int c = 0; c < ncons_; ++c) {
+                CLES_CUDA(cudaMemcpyAsync(stage, Q + fcells * c, sizeof(double) * fcells, cudaMemcpyHostToDevice, st_));
+                gather_interior(stage, Q_.as<double>() + cells_ * c, g_.n, pad_, st_);
+            }
+        } else {
+            copy_state_h2d(Q_.as<double>(), Q, g_.n, pad_, ncons_, layout, st_);
+        }
         CLES_CUDA(cudaStreamSynchronize(st_));
     }
     void get_state(double* Q, int layout) override {
