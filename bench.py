@@ -257,9 +257,9 @@ def time_e2e(cl, torch, desc, Q0, steps, dist):
 
 def cpu_sample(n, steps):
     """The oracle on the host cores: `steps` run! steps of the n^3 box after one warm-up step."""
+    cl = _package()          # first: the oracle shares the package's descriptor structs
     sys.path.insert(0, str(ROOT / "oracle"))
     import oracle as orc
-    cl = _package()
     threads = orc.set_threads(os.cpu_count() or 1)
     prob = cl.taylor_green_problem()
     tp = 2 * math.pi
@@ -344,9 +344,9 @@ def run_reference(a):
     if dist.rank != 0:
         dist.close()
         return
+    cl = _package()          # first: the oracle shares the package's descriptor structs
     sys.path.insert(0, str(ROOT / "oracle"))
     import oracle as orc
-    cl = _package()
     threads = orc.set_threads(os.cpu_count() or 1)
     prob = cl.taylor_green_problem()
     tp = 2 * math.pi
