@@ -85,6 +85,10 @@ __device__ __forceinline__ void tma_load_4d(void* dst, const CUtensorMap* map, u
         : "memory");
 }
 
+__device__ __forceinline__ void prefetch_l2(const void* p) {
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(reinterpret_cast<uint64_t>(p)));
+}
+
 template <typename T>
 __device__ __forceinline__ T tl(const double* d, const float* f, int i) {
     if (sizeof(T) == 8) return T(d[i]);
@@ -148,6 +152,30 @@ __global__ void __launch_bounds__(MS == 16 ? 512 : 256, 1)
     for (int w = blockIdx.x; w < work; w += gridDim.x, ++it) {
         const int stage = it % NS;
         const unsigned parity = (unsigned)((it / NS) & 1);
+        if (mode == OUT_RK || mode == OUT_SUBTRACT) {
+            // the store phase reads the output (and du, Q for the RK update):
+            // pull those rows into L2 now, while the tile is still arriving.
+            // Lane l takes row off + l of its segment, both 128-byte halves.
+            const int c = w / groups, g = w - (w / groups) * groups;
+            const int x0 = (g % gx) * kLanes, o = g / gx;
+            if (lane < MS) {
+                const int64_t st = P.dim == 1 ? out.sy : out.sz;
+                const int64_t ob = P.dim == 1 ? (int64_t)o * out.sz : (int64_t)o * out.sy;
+                const int64_t e = (int64_t)c * out.comp_stride + x0 + ob + (int64_t)(off + lane) * st;
+                const bool second = x0 + 16 < P.nx;
+                const T* ob_ = reinterpret_cast<const T*>(out.base) + e;
+                prefetch_l2(ob_);
+                if (sizeof(T) == 8 && second) prefetch_l2(ob_ + 16);
+                if (mode == OUT_RK) {
+                    prefetch_l2(rk.du + e);
+                    prefetch_l2(rk.Q + e);
+                    if (second) {
+                        prefetch_l2(rk.du + e + 16);
+                        prefetch_l2(rk.Q + e + 16);
+                    }
+                }
+            }
+        }
         // bounded wait, decided block-wide so no thread is left at a barrier
         const bool ok = mbar_wait_bounded(&bars[stage], parity);
         if (__syncthreads_or(!ok)) {
