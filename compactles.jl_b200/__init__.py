@@ -6,9 +6,10 @@ run!) over the C ABI of libcles.so (include/cles.h).  The CUDA library is
 required: every compute call goes through it and raises if it is missing.
 """
 from . import abi
-from .problem import (ArtParams, DirichletBC, ExtrapolationBC, IdealMixture, IdealSpecies, NoSlipWallBC,
-                      NSCBCInflowBC, NSCBCOutflowBC, Numerics, PER3, PeriodicBC, Prim, Problem, SlipWallBC,
-                      StepControl, SwitchableBC, Transport,
+from .problem import (ArtParams, AxisBC, CartesianMetric, CylindricalMetric, DirichletBC, ExtrapolationBC,
+                      IdealMixture, IdealSpecies, NoSlipWallBC, NSCBCInflowBC, NSCBCOutflowBC, Numerics, OriginBC,
+                      PER3, PeriodicBC, PoleBC, Prim, Problem, SlipWallBC, SphericalMetric, StepControl, Stretch,
+                      SwitchableBC, Transport, sine_cluster,
                       conserved_from_prim, coords, grid_spacing, initialize, interior_slices,
                       problem_desc, single_species, solver_desc, state_shape, tanh_blend,
                       taylor_green_problem)

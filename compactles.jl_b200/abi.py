@@ -122,6 +122,13 @@ CLES_BC_NOSLIP_WALL = 3
 CLES_BC_EXTRAPOLATION = 4
 CLES_BC_NSCBC_OUTFLOW = 5
 CLES_BC_NSCBC_INFLOW = 6
+CLES_BC_AXIS = 7
+CLES_BC_ORIGIN = 8
+CLES_BC_POLE = 9
+
+CLES_METRIC_CARTESIAN = 0
+CLES_METRIC_CYLINDRICAL = 1
+CLES_METRIC_SPHERICAL = 2
 
 
 class cles_bc_params(C.Structure):
@@ -176,6 +183,9 @@ class cles_solver_desc(C.Structure):
         ("T_guess", C.c_double),
         ("n_intervals", C.c_int * CLES_MAX_SPECIES),
         ("nasa9", (cles_nasa9_interval * CLES_MAX_NASA9_INTERVALS) * CLES_MAX_SPECIES),
+        ("metric", C.c_int),
+        ("stretch_x", C.POINTER(C.c_double) * 3),
+        ("stretch_dxdxi", C.POINTER(C.c_double) * 3),
     ]
 
 

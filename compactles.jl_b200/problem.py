@@ -10,6 +10,7 @@ Initial-condition callables are evaluated vectorised: ic(x, y, z) receives
 broadcastable numpy coordinate arrays and returns a Prim whose fields may be
 arrays.
 """
+import ctypes as C
 from dataclasses import dataclass, field
 from typing import Callable, Optional, Sequence, Tuple
 
@@ -146,11 +147,34 @@ class NSCBCInflowBC(BoundaryCondition):
         self.Lref = float(Lref)
 
 
+class AxisBC(BoundaryCondition):
+    """AxisBC() (src/boundary.jl:53-63): regularized cylindrical axis at the low
+    r face; half-offset r grid, parity mirror rows, antipodal pairing when
+    theta is resolved."""
+    code = abi.CLES_BC_AXIS
+
+
+class OriginBC(BoundaryCondition):
+    """OriginBC() (src/boundary.jl:65-73): regularized spherical origin at the low r face."""
+    code = abi.CLES_BC_ORIGIN
+
+
+class PoleBC(BoundaryCondition):
+    """PoleBC() (src/boundary.jl:75-82): regularized spherical poles, at both theta faces."""
+    code = abi.CLES_BC_POLE
+
+
+_FOLD_CODES = (abi.CLES_BC_AXIS, abi.CLES_BC_ORIGIN, abi.CLES_BC_POLE)
+
+
 class SwitchableBC(BoundaryCondition):
     """SwitchableBC(before, after) (src/boundary.jl:120-160): the face acts as
     `before` until Solver.switch_bc(dim, side), then as `after`."""
 
     def __init__(self, before, after):
+        if before.code in _FOLD_CODES or after.code in _FOLD_CODES:
+            raise ValueError("SwitchableBC cannot wrap a fold condition (AxisBC, OriginBC, PoleBC); "
+                             "setup detects those by type")
         if (before.code == abi.CLES_BC_PERIODIC) != (after.code == abi.CLES_BC_PERIODIC):
             raise ValueError("SwitchableBC: both conditions must agree on periodicity")
         if isinstance(before, SwitchableBC) or isinstance(after, SwitchableBC):
@@ -160,6 +184,46 @@ class SwitchableBC(BoundaryCondition):
 
 
 PER3 = tuple((PeriodicBC(), PeriodicBC()) for _ in range(3))
+
+
+# ----------------------------------------------------------------- metrics --
+class Metric:
+    code = None
+
+
+class CartesianMetric(Metric):
+    """CartesianMetric() (src/metric.jl:24-29)."""
+    code = abi.CLES_METRIC_CARTESIAN
+
+
+class CylindricalMetric(Metric):
+    """CylindricalMetric() (src/metric.jl:31-37): (r, theta, z), physical velocity components."""
+    code = abi.CLES_METRIC_CYLINDRICAL
+
+
+class SphericalMetric(Metric):
+    """SphericalMetric() (src/metric.jl:39-45): (r, theta, phi), theta the polar angle."""
+    code = abi.CLES_METRIC_SPHERICAL
+
+
+@dataclass
+class Stretch:
+    """Stretch(x, dxdxi) (src/metric.jl:47-63): monotone map of the uniform
+    computational coordinate xi in [0, 1]; both callables take numpy arrays."""
+    x: Callable
+    dxdxi: Callable
+
+
+def sine_cluster(lo, hi, xic, a):
+    """sine_cluster(lo, hi, xic, a) (src/metric.jl:65-78): spacing smallest at
+    xi = xic, ratio (1+a)/(1-a)."""
+    if not (0 <= a < 1):
+        raise ValueError("sine_cluster: need 0 ≤ a < 1")
+    lo, hi, xic, a = float(lo), float(hi), float(xic), float(a)
+    L = hi - lo
+    two_pi = 2 * np.pi
+    return Stretch(lambda xi: lo + L * (xi - (a / two_pi) * (np.sin(two_pi * (xi - xic)) + np.sin(two_pi * xic))),
+                   lambda xi: L * (1 - a * np.cos(two_pi * (xi - xic))))
 
 
 def _fill_face(bc, eos, ncons, params, state):
@@ -255,6 +319,7 @@ class Problem:
     name: str = "problem"
     eos: IdealMixture = field(default_factory=single_species)
     transport: Transport = field(default_factory=Transport)
+    metric: Metric = field(default_factory=CartesianMetric)
 
 
 @dataclass
@@ -268,6 +333,7 @@ class Numerics:
     filter_interval: int = 1
     n_halo: int = 4
     precision: str = "fp64"              # "fp64" (drop-in) or "mixed"
+    stretch: tuple = (None, None, None)  # Stretch or None per dimension
 
 
 _BETA = {"strain": abi.CLES_BETA_STRAIN, "gated_strain": abi.CLES_BETA_GATED_STRAIN,
@@ -276,8 +342,11 @@ _BETA = {"strain": abi.CLES_BETA_STRAIN, "gated_strain": abi.CLES_BETA_GATED_STR
 
 def solver_desc(n_global, L_domain, bcs, deriv, filt, eos=None, transport=None, art=None,
                 origin=(0.0, 0.0, 0.0), cfl=0.5, filter_interval=1, control=None,
-                n_halo=4, precision="fp64"):
-    """The flat descriptor for Solver(; n_global, L_domain, bcs, ...) (src/rhs.jl:122-135)."""
+                n_halo=4, precision="fp64", metric=None, stretch=(None, None, None)):
+    """The flat descriptor for Solver(; n_global, L_domain, bcs, ...) (src/rhs.jl:122-135).
+
+    A Stretch on dimension d is sampled at the nodes xi_i = i / (n - 1)
+    (src/metric.jl:99-106); the samples live as long as the descriptor."""
     eos = eos or single_species()
     transport = transport or Transport()
     art = art or ArtParams()
@@ -324,16 +393,52 @@ def solver_desc(n_global, L_domain, bcs, deriv, filt, eos=None, transport=None, 
     d.control = control.to_c()
     d.n_halo = int(n_halo)
     d.precision = abi.CLES_PREC_MIXED if precision == "mixed" else abi.CLES_PREC_FP64
+    d.metric = (metric or CartesianMetric()).code
+    keep = []
+    for k in range(3):
+        st = stretch[k]
+        if st is None:
+            continue
+        n = int(n_global[k])
+        if n < 2:
+            raise ValueError(f"dimension {k + 1}: a stretched dimension must be resolved")
+        xi = np.arange(n, dtype=np.float64) * (1.0 / (n - 1))
+        xs = np.ascontiguousarray(np.broadcast_to(np.asarray(st.x(xi), dtype=np.float64), (n,)))
+        ms = np.ascontiguousarray(np.broadcast_to(np.asarray(st.dxdxi(xi), dtype=np.float64), (n,)))
+        keep += [xs, ms]
+        d.stretch_x[k] = xs.ctypes.data_as(C.POINTER(C.c_double))
+        d.stretch_dxdxi[k] = ms.ctypes.data_as(C.POINTER(C.c_double))
+    d._stretch_keep = keep
     return d
 
 
+def _folds(desc):
+    """(fold at the low end, fold at the high end) per dimension (src/rhs.jl:149-197)."""
+    lo0 = desc.bc[0][0] in (abi.CLES_BC_AXIS, abi.CLES_BC_ORIGIN)
+    poles = desc.bc[1][0] == abi.CLES_BC_POLE and desc.bc[1][1] == abi.CLES_BC_POLE
+    return (lo0, poles, False), (False, poles, False)
+
+
+def stretched(desc, k):
+    return bool(desc.stretch_x[k])
+
+
 def grid_spacing(desc):
-    """h per dimension (src/rhs.jl:198-204): L/N periodic, L/(N-1) closed, 1 collapsed."""
+    """h per dimension (src/rhs.jl:191-204): 1 collapsed, 1/(N-1) stretched,
+    L/N with folds at both ends, L/(N-1/2) with a fold at the low end, L/N
+    periodic, L/(N-1) closed."""
+    flo, fhi = _folds(desc)
     h = []
     for k in range(3):
         n = desc.n_global[k]
         if n == 1:
             h.append(1.0)
+        elif stretched(desc, k):
+            h.append(1.0 / (n - 1))
+        elif flo[k] and fhi[k]:
+            h.append(desc.L[k] / n)
+        elif flo[k]:
+            h.append(desc.L[k] / (n - 0.5))
         elif desc.bc[k][0] == abi.CLES_BC_PERIODIC:
             h.append(desc.L[k] / n)
         else:
@@ -342,9 +447,19 @@ def grid_spacing(desc):
 
 
 def coords(desc):
-    """Interior node coordinates per dimension (global_xcoord, src/rhs.jl:331-335)."""
+    """Interior node coordinates per dimension (global_xcoord, src/rhs.jl:331-335):
+    origin + half-cell fold shift + i h, or the stretch map at the nodes."""
     h = grid_spacing(desc)
-    return tuple(desc.origin[k] + np.arange(desc.n_global[k]) * h[k] for k in range(3))
+    flo, _ = _folds(desc)
+    out = []
+    for k in range(3):
+        n = desc.n_global[k]
+        if stretched(desc, k):
+            out.append(np.array(desc.stretch_x[k][:n], dtype=np.float64))
+            continue
+        shift = h[k] / 2 if flo[k] else 0.0
+        out.append((desc.origin[k] + shift) + np.arange(n) * h[k])
+    return tuple(out)
 
 
 def state_shape(desc, layout=abi.CLES_LAYOUT_PADDED):
@@ -407,7 +522,8 @@ def problem_desc(prob, num, deriv, filt):
     return solver_desc(num.n_global, L, prob.bcs, deriv, filt, eos=prob.eos,
                        transport=prob.transport, art=num.art, origin=origin, cfl=num.cfl,
                        filter_interval=num.filter_interval, control=num.control,
-                       n_halo=num.n_halo, precision=num.precision)
+                       n_halo=num.n_halo, precision=num.precision, metric=prob.metric,
+                       stretch=num.stretch)
 
 
 # ------------------------------------------------------------- test cases ----

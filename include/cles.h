@@ -68,6 +68,16 @@ extern "C" {
 #define CLES_BC_EXTRAPOLATION   4   /* ExtrapolationBC, enforce! at src/boundary.jl:267-278 */
 #define CLES_BC_NSCBC_OUTFLOW   5   /* NSCBCOutflowBC, correct_rhs! at src/nscbc.jl:59-157 */
 #define CLES_BC_NSCBC_INFLOW    6   /* NSCBCInflowBC (constant targets), correct_rhs! at src/nscbc.jl:220-307 */
+/* Coordinate-singularity folds (src/boundary.jl:53-82, src/folds.jl): no state
+ * enforcement; a half-offset grid, mirror rows and the antipodal pairing. */
+#define CLES_BC_AXIS            7   /* AxisBC: low r face of a CylindricalMetric grid */
+#define CLES_BC_ORIGIN          8   /* OriginBC: low r face of a SphericalMetric grid */
+#define CLES_BC_POLE            9   /* PoleBC: both theta faces of a SphericalMetric grid */
+
+/* Orthogonal metrics (src/metric.jl:20-45) */
+#define CLES_METRIC_CARTESIAN    0   /* (x, y, z) */
+#define CLES_METRIC_CYLINDRICAL  1   /* (r, theta, z), scale factors (1, r, 1) */
+#define CLES_METRIC_SPHERICAL    2   /* (r, theta, phi), theta polar, scale factors (1, r, r sin theta) */
 
 /* Parameters of one face condition (unused fields are ignored). */
 typedef struct cles_bc_params {
@@ -187,7 +197,7 @@ typedef struct cles_step_control {
 void cles_step_control_default(cles_step_control* out);
 
 /* The Solver's scalar configuration (src/rhs.jl:122-135, src/problem.jl:243-306).
- * Cartesian metric, no stretching, no folds, no sources. */
+ * Orthogonal metric, optional stretching and coordinate folds; no sources. */
 /* Equation of state of the mixture. */
 #define CLES_EOS_IDEAL 0   /* IdealMixture: R[k], gamma[k] (src/physics.jl:87-120) */
 #define CLES_EOS_NASA9 1   /* Nasa9Mixture: R[k] and the NASA-9 intervals (src/physics.jl:402-427) */
@@ -239,6 +249,18 @@ typedef struct cles_solver_desc {
     double T_guess;              /* Newton seed reference temperature (default 300 K) */
     int    n_intervals[CLES_MAX_SPECIES];
     cles_nasa9_interval nasa9[CLES_MAX_SPECIES][CLES_MAX_NASA9_INTERVALS];
+    /* Geometry (src/rhs.jl:122-311, src/metric.jl).  metric = CLES_METRIC_*.
+     * A Stretch (src/metric.jl:47-68) on dimension d is given by its mapping
+     * sampled at the n_global[d] nodes xi_i = i / (n_global[d] - 1), i = 0..n-1:
+     * stretch_x[d][i] = x(xi_i) and stretch_dxdxi[d][i] = dx/dxi(xi_i) (host
+     * arrays, read at create time only; NULL = uniform).  A stretched dimension
+     * must be non-periodic and not folded; its origin is ignored.  Fold faces
+     * (CLES_BC_AXIS / _ORIGIN / _POLE) select the half-offset grids and the
+     * parity plans of the reference; their validation is the reference's
+     * (src/rhs.jl:143-189). */
+    int    metric;
+    const double* stretch_x[3];
+    const double* stretch_dxdxi[3];
 } cles_solver_desc;
 
 /* Defaults of Problem()/Numerics() for a grid: single_species(1.4, R=1),

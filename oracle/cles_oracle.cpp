@@ -344,6 +344,7 @@ struct BandFactor {
 struct RankPart {
     int n = 0, off = 0;
     bool lo_closed = false, hi_closed = false;
+    int fold_lo = 0, fold_hi = 0;   // parity fold sign of the solution at a folded edge (0 = none)
     TriFactor tf;             // q == 1 path
     BandFactor bf;            // q >= 2 path
     std::vector<double> V, W; // n x q each (column-major: V[i + n*t])
@@ -372,6 +373,7 @@ struct Plan {
     int lines = 0;
     cles_scheme scheme;
     bool lo_closed = false, hi_closed = false;
+    int lo_fold = 0, hi_fold = 0;   // sigma_g of a folded edge (0 = none)
     double a0 = 0.0;
     std::vector<double> ci;
     std::vector<std::vector<double>> clo, chi;
@@ -391,8 +393,12 @@ void build_tri_part(const cles_scheme& s, RankPart& rp) {
             const int r = n - 1 - j;
             a[r] = s.clo_lhs[j][2]; b[r] = s.clo_lhs[j][1]; c[r] = s.clo_lhs[j][0];
         }
-    const double aL = rp.lo_closed ? 0.0 : al;
-    const double cR = rp.hi_closed ? 0.0 : al;
+    // parity fold on a half-offset grid (src/operators.jl:61-70): the coupling
+    // to the ghost unknown g_0 = sigma_g g_1 moves onto the diagonal
+    if (rp.fold_lo) b[0] += (double)rp.fold_lo * al;
+    if (rp.fold_hi) b[n - 1] += (double)rp.fold_hi * al;
+    const double aL = (rp.lo_closed || rp.fold_lo) ? 0.0 : al;
+    const double cR = (rp.hi_closed || rp.fold_hi) ? 0.0 : al;
     rp.tf.build(a, b, c);
     rp.V.assign(n, 0.0); rp.W.assign(n, 0.0);
     if (aL != 0.0) { rp.V[0] = aL; rp.tf.solve(rp.V.data(), 1); }
@@ -408,6 +414,22 @@ bool build_band_part(const cles_scheme& s, RankPart& rp) {
         Ab[q + (size_t)W * i] = 1.0;
         for (int t = 1; t <= q; ++t) { Ab[(q + t) + (size_t)W * i] = s.lhs[t - 1]; Ab[(q - t) + (size_t)W * i] = s.lhs[t - 1]; }
     }
+    // parity folds (src/operators_banded.jl:58-77): row i's coupling to ghost
+    // column i-m maps onto interior column m-i+1 (1-based) with sign sigma_g
+    if (rp.fold_lo)
+        for (int i = 1; i <= q; ++i)
+            for (int m = 1; m <= q; ++m) {
+                if (i - m >= 1) continue;
+                const int jcol = m - i + 1;
+                Ab[(q + (jcol - i)) + (size_t)W * (i - 1)] += (double)rp.fold_lo * s.lhs[m - 1];
+            }
+    if (rp.fold_hi)
+        for (int i = n - q + 1; i <= n; ++i)
+            for (int m = 1; m <= q; ++m) {
+                if (i + m <= n) continue;
+                const int jcol = 2 * n + 1 - (i + m);
+                Ab[(q + (jcol - i)) + (size_t)W * (i - 1)] += (double)rp.fold_hi * s.lhs[m - 1];
+            }
     if (rp.lo_closed)
         for (int j = 0; j < nc; ++j)
             for (int t = -q; t <= q; ++t) {
@@ -421,9 +443,9 @@ bool build_band_part(const cles_scheme& s, RankPart& rp) {
         }
     // Coupling blocks AL[r,t] = lhs[q+r-t] (t >= r), CR[r,t] = lhs[t+q-r] (t <= r), 1-based.
     std::vector<double> AL((size_t)q * q, 0.0), CR((size_t)q * q, 0.0);
-    if (!rp.lo_closed)
+    if (!(rp.lo_closed || rp.fold_lo))
         for (int r = 1; r <= q; ++r) for (int t = r; t <= q; ++t) AL[(r - 1) + (size_t)q * (t - 1)] = s.lhs[q + r - t - 1];
-    if (!rp.hi_closed)
+    if (!(rp.hi_closed || rp.fold_hi))
         for (int r = 1; r <= q; ++r) for (int t = 1; t <= r; ++t) CR[(r - 1) + (size_t)q * (t - 1)] = s.lhs[t + q - r - 1];
     rp.bf.build(Ab, n, q);
     rp.V.assign((size_t)n * q, 0.0); rp.W.assign((size_t)n * q, 0.0);
@@ -476,7 +498,7 @@ void build_reduced(DistSolver& ls) {
     ls.red.factor(R, N);
 }
 
-Plan* plan_create(const Decomp& D, const cles_scheme& s, int dim0, double h, int P) {
+Plan* plan_create(const Decomp& D, const cles_scheme& s, int dim0, double h, int P, int lo_fold = 0, int hi_fold = 0) {
     const int n = D.nl[dim0];
     const int nc = s.nc, M = s.M, q = s.q;
     if (!D.active[dim0]) { set_err("dimension is collapsed"); return nullptr; }
@@ -491,8 +513,10 @@ Plan* plan_create(const Decomp& D, const cles_scheme& s, int dim0, double h, int
     if (M > D.nh) { set_err("stencil half-width exceeds halo width"); return nullptr; }
     auto* p = new Plan();
     p->D = D; p->dim = dim0; p->n = n; p->scheme = s;
-    p->lo_closed = D.closed(dim0);
-    p->hi_closed = D.closed(dim0);
+    p->lo_fold = D.closed(dim0) ? lo_fold : 0;
+    p->hi_fold = D.closed(dim0) ? hi_fold : 0;
+    p->lo_closed = D.closed(dim0) && !p->lo_fold;
+    p->hi_closed = D.closed(dim0) && !p->hi_fold;
     p->lines = 1;
     for (int k = 0; k < 3; ++k) if (k != dim0) p->lines *= D.nl[k];
     const double hinv = 1.0 / h;
@@ -514,6 +538,8 @@ Plan* plan_create(const Decomp& D, const cles_scheme& s, int dim0, double h, int
         local_range(n, P, r, &rp.n, &rp.off);
         rp.lo_closed = p->lo_closed && r == 0;
         rp.hi_closed = p->hi_closed && r == P - 1;
+        rp.fold_lo = r == 0 ? p->lo_fold : 0;
+        rp.fold_hi = r == P - 1 ? p->hi_fold : 0;
         if (!ls.banded) build_tri_part(s, rp);
         else if (!build_band_part(s, rp)) { delete p; return nullptr; }
     }
@@ -634,6 +660,24 @@ void apply_along(const Plan& p, double* out, const double* f) {
 // -------------------------------------------------------------- the solver ---
 struct Savepoint { std::vector<double> Q; double t; int64_t step; };
 
+// Pairing of a folded dimension (PairSpec, src/folds.jl:50-60), one rank:
+// every partner block is local.  pdim / revdim are 0-based, -1 = none.
+struct PairSpec {
+    int pdim = -1, revdim = -1;
+};
+
+// FoldSpec (src/folds.jl:62-75): folded ends, pairing, antipodal signs and
+// the parity plans (index 0: sigma_g = +1, index 1: sigma_g = -1).
+struct FoldSpec {
+    int dim = 0;
+    bool lo = false, hi = false;
+    bool paired = false;
+    PairSpec pair;
+    int sigvel[3] = {1, 1, 1};
+    std::vector<int> sigflux;
+    std::unique_ptr<Plan> dp[2], fp[2];
+};
+
 struct Solver {
     cles_solver_desc desc;
     Decomp D;
@@ -649,6 +693,13 @@ struct Solver {
     std::vector<std::vector<double>> grad_Y[3];
     std::vector<double> mu_art, beta_art, kappa_art, strain, sensor, sensor_sp, tmp_a, tmp_b;
     std::vector<double> flux[3][CLES_MAX_SPECIES + 4];
+    // geometry (src/rhs.jl:53-55, src/metric.jl:109-140)
+    int metric = CLES_METRIC_CARTESIAN;
+    bool stretched[3] = {false, false, false};
+    std::vector<double> st_x[3], st_m[3];   // stretch samples at the interior nodes
+    double orig[3] = {0, 0, 0}, coord_shift[3] = {0, 0, 0};
+    std::unique_ptr<FoldSpec> folds[3];
+    std::vector<double> inv_J, area[3], inv_h[3], inv_r, cot_over_r, pairbuf, pairout;
     double t = 0.0, tstage = 0.0, dt_prev = 0.0, rate_prev = 0.0, cfl = 0.5;
     int64_t step = 0;
     bool switched[3][2] = {{false, false}, {false, false}, {false, false}};   // SwitchableBC state
@@ -816,18 +867,289 @@ void for_interior(const Decomp& D, F&& fn) {
             for (int i = 0; i < D.nl[0]; ++i) fn(D.at(i + o1, j + o2, k + o3), i, j, k);
 }
 
-void deriv_along(Solver& S, double* out, const double* f, int d) { apply_along(*S.dplan[d], out, f); }
-void filt_along(Solver& S, double* out, const double* f, int d) { apply_along(*S.fplan[d], out, f); }
+// ------------------------------------------------------------------ folds ---
+// fold_fill! (src/folds.jl:83-124): mirror the halos beyond a folded end of
+// dimension d with sign sig (half-offset mirror: ghost layer q <-> interior
+// layer q), over the full padded extent of the other dimensions.
+void fold_fill(const Decomp& D, double* f, int d, bool lo, bool hi, int sig) {
+    const int pad = D.nhd[d], n = D.nl[d];
+    const double sgn = (double)sig;
+    const int o1 = d == 0 ? 1 : 0, o2 = d == 2 ? 1 : 2;
+    for (int b = 0; b < D.full[o2]; ++b)
+        for (int a = 0; a < D.full[o1]; ++a)
+            for (int q = 1; q <= pad; ++q) {
+                int g[3], c[3];
+                g[o1] = c[o1] = a;
+                g[o2] = c[o2] = b;
+                if (lo) {
+                    g[d] = pad - q;
+                    c[d] = pad + q - 1;
+                    f[D.at(g[0], g[1], g[2])] = sgn * f[D.at(c[0], c[1], c[2])];
+                }
+                if (hi) {
+                    g[d] = pad + n + q - 1;
+                    c[d] = pad + n - q;
+                    f[D.at(g[0], g[1], g[2])] = sgn * f[D.at(c[0], c[1], c[2])];
+                }
+            }
+}
 
-// compute_primitives_and_gradients! (src/rhs.jl:591-606), Cartesian: the
-// 1/h_d rescale multiplies by exactly 1 and is omitted.
+// _pair_index (src/folds.jl:128-155), one rank: shift pdim by half its
+// extent, reverse revdim.  c holds 0-based padded coordinates.
+void pair_index(const Decomp& D, const PairSpec& pr, int c[3]) {
+    if (pr.pdim >= 0) {
+        const int pd = pr.pdim, half = D.nl[pd] / 2, Hp = D.nhd[pd];
+        int v = c[pd] - Hp + 1;
+        v = v <= half ? v + half : v - half;
+        c[pd] = v - 1 + Hp;
+    }
+    if (pr.revdim >= 0) {
+        const int rd = pr.revdim, Hr = D.nhd[rd];
+        const int v = D.nl[rd] + 1 - (c[rd] - Hr + 1);
+        c[rd] = v - 1 + Hr;
+    }
+}
+
+inline int pair_dim(const PairSpec& pr) { return pr.pdim >= 0 ? pr.pdim : pr.revdim; }
+
+// pair_forward! (src/folds.jl:162-215), on-rank butterfly: the lower half of
+// the pairing dimension receives e, the partner slots o.
+void pair_forward(Solver& S, double* w, const double* f, const FoldSpec& fold, int sig) {
+    const Decomp& D = S.D;
+    const double sf = (double)sig;
+    const int sd = pair_dim(fold.pair), half = D.nl[sd] / 2;
+    for (int k = 0; k < D.nl[2]; ++k)
+        for (int j = 0; j < D.nl[1]; ++j)
+            for (int i = 0; i < D.nl[0]; ++i) {
+                int c[3] = {i + D.nhd[0], j + D.nhd[1], k + D.nhd[2]};
+                const int v = (sd == 0 ? i : sd == 1 ? j : k) + 1;
+                if (v > half) continue;
+                const size_t I = D.at(c[0], c[1], c[2]);
+                pair_index(D, fold.pair, c);
+                const size_t Mx = D.at(c[0], c[1], c[2]);
+                const double a = f[I], b = sf * f[Mx];
+                w[I] = 0.5 * (a + b);
+                w[Mx] = 0.5 * (a - b);
+            }
+}
+
+// pair_backward! (src/folds.jl:217-262), on-rank inverse butterfly.
+void pair_backward(Solver& S, double* out, const FoldSpec& fold, int sig) {
+    const Decomp& D = S.D;
+    const double sf = (double)sig;
+    const int sd = pair_dim(fold.pair), half = D.nl[sd] / 2;
+    for (int k = 0; k < D.nl[2]; ++k)
+        for (int j = 0; j < D.nl[1]; ++j)
+            for (int i = 0; i < D.nl[0]; ++i) {
+                int c[3] = {i + D.nhd[0], j + D.nhd[1], k + D.nhd[2]};
+                const int v = (sd == 0 ? i : sd == 1 ? j : k) + 1;
+                if (v > half) continue;
+                const size_t I = D.at(c[0], c[1], c[2]);
+                pair_index(D, fold.pair, c);
+                const size_t Mx = D.at(c[0], c[1], c[2]);
+                const double Re = out[I], Ro = out[Mx];
+                out[I] = Re + Ro;
+                out[Mx] = sf * (Re - Ro);
+            }
+}
+
+// _fold_plan / fold_apply! (src/folds.jl:271-322)
+Plan& fold_plan(const FoldSpec& fold, int sig, bool isfilter) {
+    const int sg = isfilter ? sig : -sig;
+    return isfilter ? *fold.fp[sg > 0 ? 0 : 1] : *fold.dp[sg > 0 ? 0 : 1];
+}
+void fold_apply(Solver& S, double* out, double* f, const FoldSpec& fold, int sig, bool isfilter) {
+    const Decomp& D = S.D;
+    const int d = fold.dim;
+    if (!fold.paired) {
+        fold_fill(D, f, d, fold.lo, fold.hi, sig);
+        apply_along(fold_plan(fold, sig, isfilter), out, f);
+        return;
+    }
+    double* w = S.pairbuf.data();
+    pair_forward(S, w, f, fold, sig);
+    // exchange_dim_batch!([w], decomp, d): a folded dimension is closed, one rank
+    fold_fill(D, w, d, fold.lo, fold.hi, sig);
+    apply_along(fold_plan(fold, sig, isfilter), out, w);
+    fold_fill(D, w, d, fold.lo, fold.hi, -1);
+    apply_along(fold_plan(fold, -1, isfilter), S.pairout.data(), w);
+    const int sd = pair_dim(fold.pair), half = D.nl[sd] / 2;
+    for (int k = 0; k < D.nl[2]; ++k)
+        for (int j = 0; j < D.nl[1]; ++j)
+            for (int i = 0; i < D.nl[0]; ++i) {
+                const int v = (sd == 0 ? i : sd == 1 ? j : k) + 1;
+                if (v > half) {
+                    const size_t I = D.at(i + D.nhd[0], j + D.nhd[1], k + D.nhd[2]);
+                    out[I] = S.pairout[I];
+                }
+            }
+    pair_backward(S, out, fold, sig);
+}
+
+// deriv_along! / filt_along! (src/rhs.jl:452-475): sig is the field's
+// antipodal sign for the fold on d (ignored without one).
+void deriv_along(Solver& S, double* out, double* f, int d, int sig = 1) {
+    if (!S.folds[d]) apply_along(*S.dplan[d], out, f);
+    else fold_apply(S, out, f, *S.folds[d], sig, false);
+}
+void filt_along(Solver& S, double* out, double* f, int d, int sig = 1) {
+    if (!S.folds[d]) apply_along(*S.fplan[d], out, f);
+    else fold_apply(S, out, f, *S.folds[d], sig, true);
+}
+
+// _scale_grad! (src/rhs.jl:477-483), over the full array
+void scale_grad(Solver& S, std::vector<double>& g, int d) {
+    const double* ih = S.inv_h[d].data();
+    const size_t n = g.size();
+#pragma omp parallel for schedule(static) if ((long)n >= kThreadMinWork)
+    for (size_t I = 0; I < n; ++I) g[I] *= ih[I];
+}
+
+// vel_parity / cons_parity (src/rhs.jl:486-491, src/equations.jl:56-60)
+int vel_parity(const Solver& S, int d, int j) { return S.folds[d] ? S.folds[d]->sigvel[j] : 1; }
+int conserved_parity(const Solver& S, const int* sigvel, int c) {
+    if (c < S.Ns) return 1;
+    if (c == S.i_energy) return 1;
+    return sigvel[c - S.Ns];
+}
+int cons_parity(const Solver& S, int d, int c) { return S.folds[d] ? conserved_parity(S, S.folds[d]->sigvel, c) : 1; }
+
+// ---------------------------------------------------------------- metrics ---
+// metric_correct_gradients! (src/metric.jl:177-221): curvature terms added to
+// the 1/h-scaled coordinate derivatives.
+void metric_correct_gradients(Solver& S) {
+    if (S.metric == CLES_METRIC_CARTESIAN) return;
+    auto& g = S.grad_u;
+    for_interior(S.D, [&](size_t I, int, int, int) {
+        const double ir = S.inv_r[I];
+        if (S.metric == CLES_METRIC_CYLINDRICAL) {
+            g[1][0][I] -= S.v[I] * ir;
+            g[1][1][I] += S.u[I] * ir;
+        } else {
+            const double ctr = S.cot_over_r[I];
+            const double ur = S.u[I], ut = S.v[I], up = S.w[I];
+            g[1][0][I] -= ut * ir;
+            g[1][1][I] += ur * ir;
+            g[2][0][I] -= up * ir;
+            g[2][1][I] -= up * ctr;
+            g[2][2][I] += ur * ir + ut * ctr;
+        }
+    });
+}
+
+// _Pi (src/metric.jl:225-233): momentum flux tensor component (a, b), 0-based
+double metric_Pi(const Solver& S, size_t I, int a, int b) {
+    const auto& g = S.grad_u;
+    const double mu = S.desc.mu0 + S.mu_art[I];
+    const double be = S.beta_art[I];
+    const double divu = g[0][0][I] + g[1][1][I] + g[2][2][I];
+    const double tau = mu * (g[a][b][I] + g[b][a][I]) + (a == b ? (be - 2 * mu / 3) * divu : 0.0);
+    const double uv[3] = {S.u[I], S.v[I], S.w[I]};
+    return S.rho[I] * uv[a] * uv[b] + (a == b ? S.p[I] : 0.0) - tau;
+}
+
+// add_metric_sources! (src/metric.jl:235-269)
+void add_metric_sources(Solver& S) {
+    if (S.metric == CLES_METRIC_CARTESIAN) return;
+    double* d1 = S.comp(S.dQ, S.i_mom[0]);
+    double* d2 = S.comp(S.dQ, S.i_mom[1]);
+    double* d3 = S.comp(S.dQ, S.i_mom[2]);
+    for_interior(S.D, [&](size_t I, int, int, int) {
+        const double ir = S.inv_r[I];
+        if (S.metric == CLES_METRIC_CYLINDRICAL) {
+            d1[I] += ir * metric_Pi(S, I, 1, 1);
+            d2[I] -= ir * metric_Pi(S, I, 1, 0);
+        } else {
+            const double ctr = S.cot_over_r[I];
+            const double Ptt = metric_Pi(S, I, 1, 1);
+            const double Ppp = metric_Pi(S, I, 2, 2);
+            d1[I] += ir * (Ptt + Ppp);
+            d2[I] += -ir * metric_Pi(S, I, 1, 0) + ctr * Ppp;
+            d3[I] += -ir * metric_Pi(S, I, 2, 0) - ctr * metric_Pi(S, I, 2, 1);
+        }
+    });
+}
+
+// curvature_rate (src/timestep.jl:185-200)
+double curvature_rate(const Solver& S, size_t I, const double* uv) {
+    if (S.metric == CLES_METRIC_CYLINDRICAL) return S.D.active[1] ? 0.0 : std::fabs(uv[1]) * S.inv_r[I];
+    if (S.metric == CLES_METRIC_SPHERICAL) {
+        double a = 0.0;
+        if (!S.D.active[1]) a += std::fabs(uv[1]) * S.inv_r[I];
+        if (!S.D.active[2]) a += std::fabs(uv[2]) * (S.inv_r[I] + std::fabs(S.cot_over_r[I]));
+        return a;
+    }
+    return 0.0;
+}
+
+// _phys_and_jac (src/metric.jl:99-106): physical coordinate and mapping
+// Jacobian of full-array index i0 (0-based) along d; halo layers beyond a
+// stretched edge clamp to the edge node (their geometry is never read).
+void phys_and_jac(const Solver& S, int d, int i0, double* x, double* m) {
+    const double xi = S.orig[d] + S.coord_shift[d] + (double)(i0 - S.D.nhd[d]) * S.h[d];
+    if (!S.stretched[d]) { *x = xi; *m = 1.0; return; }
+    const int n = S.D.nl[d];
+    const int i = std::min(std::max(i0 - S.D.nhd[d], 0), n - 1);
+    *x = S.st_x[d][i];
+    *m = S.st_m[d][i];
+}
+
+// gcl_cotr! (src/metric.jl:154-170): cot(theta)/r redefined as
+// inv_J * D_theta(A_theta) with the theta-momentum flux's fold sign.
+void gcl_cotr(Solver& S) {
+    const int sig = S.folds[1] ? S.folds[1]->sigflux[S.i_mom[1]] : 1;
+    deriv_along(S, S.tmp_a.data(), S.area[1].data(), 1, sig);
+    for_interior(S.D, [&](size_t I, int, int, int) { S.cot_over_r[I] = S.inv_J[I] * S.tmp_a[I]; });
+}
+
+// init_geometry! (src/metric.jl:109-150) over the full padded extent
+void init_geometry(Solver& S) {
+    const Decomp& D = S.D;
+    const double tiny = 1e-300;
+    for (int k = 0; k < D.full[2]; ++k)
+        for (int j = 0; j < D.full[1]; ++j)
+            for (int i = 0; i < D.full[0]; ++i) {
+                double x1, m1, x2, m2, x3, m3;
+                phys_and_jac(S, 0, i, &x1, &m1);
+                phys_and_jac(S, 1, j, &x2, &m2);
+                phys_and_jac(S, 2, k, &x3, &m3);
+                double h1 = 1.0, h2 = 1.0, h3 = 1.0;
+                if (S.metric == CLES_METRIC_CYLINDRICAL) h2 = x1;
+                else if (S.metric == CLES_METRIC_SPHERICAL) { h2 = x1; h3 = x1 * std::sin(x2); }
+                h1 *= m1; h2 *= m2; h3 *= m3;
+                h1 = jl_max(h1, tiny); h2 = jl_max(h2, tiny); h3 = jl_max(h3, tiny);
+                const double J = h1 * h2 * h3;
+                const size_t I = D.at(i, j, k);
+                S.inv_J[I] = 1 / J;
+                S.area[0][I] = J / h1;
+                S.area[1][I] = J / h2;
+                S.area[2][I] = J / h3;
+                S.inv_h[0][I] = 1 / h1;
+                S.inv_h[1][I] = 1 / h2;
+                S.inv_h[2][I] = 1 / h3;
+                if (S.metric == CLES_METRIC_CYLINDRICAL) {
+                    S.inv_r[I] = 1 / jl_max(x1, tiny);
+                } else if (S.metric == CLES_METRIC_SPHERICAL) {
+                    S.inv_r[I] = 1 / jl_max(x1, tiny);
+                    S.cot_over_r[I] = std::cos(x2) / jl_max(x1 * std::sin(x2), tiny);
+                }
+            }
+    if (S.metric == CLES_METRIC_SPHERICAL && D.active[1]) gcl_cotr(S);
+}
+
+// compute_primitives_and_gradients! (src/rhs.jl:591-606)
 void primitives_and_gradients(Solver& S, bool primitives_current) {
     if (!primitives_current) { exchange_state(S); primitives(S); }
     for (int jj = 0; jj < 3; ++jj)
         for (int d = 0; d < 3; ++d) {
-            if (S.D.active[d]) deriv_along(S, S.grad_u[d][jj].data(), S.vel(jj), d);
-            else std::fill(S.grad_u[d][jj].begin(), S.grad_u[d][jj].end(), 0.0);
+            if (S.D.active[d]) {
+                deriv_along(S, S.grad_u[d][jj].data(), S.vel(jj), d, vel_parity(S, d, jj));
+                scale_grad(S, S.grad_u[d][jj], d);
+            } else {
+                std::fill(S.grad_u[d][jj].begin(), S.grad_u[d][jj].end(), 0.0);
+            }
         }
+    metric_correct_gradients(S);
 }
 
 // delta4_sum! (src/artificial.jl:67-94)
@@ -860,7 +1182,7 @@ void smooth(Solver& S, double* f) {
     for (int d = 0; d < 3; ++d) {
         if (!S.D.active[d]) continue;
         wrap_dim(S.D, f, d);
-        filt_along(S, S.tmp_a.data(), f, d);
+        filt_along(S, S.tmp_a.data(), f, d, 1);
         copy_interior(S.D, f, S.tmp_a.data());
     }
 }
@@ -1106,21 +1428,40 @@ void compute_rhs(Solver& S, bool primitives_current) {
     compute_artificial(S);
     for (int d = 0; d < 3; ++d) {
         if (!D.active[d]) continue;
-        deriv_along(S, S.grad_T[d].data(), S.T.data(), d);
-        for (int sp = 0; sp < S.Ns; ++sp) deriv_along(S, S.grad_Y[d][sp].data(), S.Y[sp].data(), d);
+        deriv_along(S, S.grad_T[d].data(), S.T.data(), d, 1);
+        scale_grad(S, S.grad_T[d], d);
+        for (int sp = 0; sp < S.Ns; ++sp) {
+            deriv_along(S, S.grad_Y[d][sp].data(), S.Y[sp].data(), d, 1);
+            scale_grad(S, S.grad_Y[d][sp], d);
+        }
     }
     assemble_fluxes(S);
     for (int d = 0; d < 3; ++d)
         for (int cc = 0; cc < S.ncons; ++cc) wrap_dim(D, S.flux[d][cc].data(), d);
+    // unit geometry (Cartesian, unstretched): A_d = inv_J = 1 and the general
+    // path's products are skipped (src/rhs.jl:643-649)
+    bool unitgeom = S.metric == CLES_METRIC_CARTESIAN;
+    for (int d = 0; d < 3; ++d) unitgeom = unitgeom && !S.stretched[d];
     for (int cc = 0; cc < S.ncons; ++cc) {
         double* dq = S.comp(S.dQ, cc);
         for_interior(D, [&](size_t I, int, int, int) { dq[I] = 0; });
         for (int d = 0; d < 3; ++d) {
             if (!D.active[d]) continue;
-            deriv_along(S, S.tmp_a.data(), S.flux[d][cc].data(), d);
-            for_interior(D, [&](size_t I, int, int, int) { dq[I] -= S.tmp_a[I]; });
+            const int sig = S.folds[d] ? S.folds[d]->sigflux[cc] : 1;
+            if (unitgeom) {
+                deriv_along(S, S.tmp_a.data(), S.flux[d][cc].data(), d, sig);
+                for_interior(D, [&](size_t I, int, int, int) { dq[I] -= S.tmp_a[I]; });
+            } else {
+                // tmp_b = A_d F_d over the full array, then dQ -= inv_J D_d(tmp_b)
+                const double* Ad = S.area[d].data();
+                const double* Fd = S.flux[d][cc].data();
+                for (size_t I = 0; I < S.fs; ++I) S.tmp_b[I] = Ad[I] * Fd[I];
+                deriv_along(S, S.tmp_a.data(), S.tmp_b.data(), d, sig);
+                for_interior(D, [&](size_t I, int, int, int) { dq[I] -= S.inv_J[I] * S.tmp_a[I]; });
+            }
         }
     }
+    add_metric_sources(S);
     for (int d = 0; d < 3; ++d)
         for (int side = 0; side < 2; ++side) {
             if (!D.active[d]) continue;
@@ -1140,6 +1481,7 @@ void apply_bcs(Solver& S) {
             if (!D.active[d]) continue;
             const int bc = S.face_kind(d, side);
             if (bc == CLES_BC_PERIODIC || bc == CLES_BC_NSCBC_OUTFLOW || bc == CLES_BC_NSCBC_INFLOW) continue;
+            if (bc == CLES_BC_AXIS || bc == CLES_BC_ORIGIN || bc == CLES_BC_POLE) continue;   // src/boundary.jl:173-175
             const double* bstate = S.face_state(d, side);
             const double Twall = S.face_params(d, side).Twall;
             int shift[3] = {0, 0, 0};
@@ -1223,7 +1565,7 @@ void step(Solver& S, double dt, bool prepared) {
     apply_bcs(S);
 }
 
-// max_rate (src/timestep.jl:125-175), Cartesian (inv_h = 1).
+// max_rate (src/timestep.jl:125-175)
 void max_rate(Solver& S, double* rate_out, double* rho_min_out) {
     exchange_state(S);
     primitives(S);
@@ -1247,11 +1589,11 @@ void max_rate(Solver& S, double* rate_out, double* rho_min_out) {
                 double acc = 0.0, dsum = 0.0;
                 for (int d = 0; d < 3; ++d) {
                     if (!D.active[d]) continue;
-                    const double idx = 1.0 / S.h[d];
+                    const double idx = S.inv_h[d][I] / S.h[d];   // inverse physical spacing
                     acc += (std::fabs(uv[d]) + cc) * idx;
                     dsum += idx * idx;
                 }
-                acc += 0.0;  // curvature_rate, Cartesian
+                acc += curvature_rate(S, I, uv);
                 double Dmax = mu0 / (Sc * r);
                 for (int sp = 0; sp < S.Ns; ++sp) Dmax = jl_max(Dmax, mu0 / (Sc * r) + S.D_art[sp][I]);
                 const double nu = (mu0 + S.mu_art[I] + S.beta_art[I]) * ri +
@@ -1269,7 +1611,7 @@ void filter_state(Solver& S) {
         if (!S.D.active[d]) continue;
         for (int cc = 0; cc < S.ncons; ++cc) wrap_dim(S.D, S.comp(S.Q, cc), d);
         for (int cc = 0; cc < S.ncons; ++cc) {
-            filt_along(S, S.tmp_a.data(), S.comp(S.Q, cc), d);
+            filt_along(S, S.tmp_a.data(), S.comp(S.Q, cc), d, cons_parity(S, d, cc));
             copy_interior(S.D, S.comp(S.Q, cc), S.tmp_a.data());
         }
     }
@@ -1417,6 +1759,15 @@ double kinetic_energy(Solver& S) {
     return ke * cellvol / vol;
 }
 
+inline bool is_fold_bc(int bc) { return bc == CLES_BC_AXIS || bc == CLES_BC_ORIGIN || bc == CLES_BC_POLE; }
+
+// unit_scalefactor (src/metric.jl:91-93)
+bool unit_scalefactor(int metric, int d) {
+    if (metric == CLES_METRIC_CYLINDRICAL) return d != 1;
+    if (metric == CLES_METRIC_SPHERICAL) return d == 0;
+    return true;
+}
+
 Solver* solver_create(const cles_solver_desc& A) {
     for (int d = 0; d < 3; ++d) {
         const bool p0 = A.bc[d][0] == CLES_BC_PERIODIC, p1 = A.bc[d][1] == CLES_BC_PERIODIC;
@@ -1424,18 +1775,85 @@ Solver* solver_create(const cles_solver_desc& A) {
         if (A.n_global[d] < 1) { set_err("n_global must be >= 1"); return nullptr; }
         if (A.n_global[d] == 1 && !p0) { set_err("collapsed dimension must use (PeriodicBC(), PeriodicBC())"); return nullptr; }
         for (int s = 0; s < 2; ++s) {
-            if (A.bc[d][s] < CLES_BC_PERIODIC || A.bc[d][s] > CLES_BC_NSCBC_INFLOW) { set_err("unknown boundary condition"); return nullptr; }
+            if (A.bc[d][s] < CLES_BC_PERIODIC || A.bc[d][s] > CLES_BC_POLE) { set_err("unknown boundary condition"); return nullptr; }
             if (A.bc_switchable[d][s] && ((A.bc_after[d][s] == CLES_BC_PERIODIC) != (A.bc[d][s] == CLES_BC_PERIODIC))) {
                 set_err("SwitchableBC: both conditions must agree on periodicity");
+                return nullptr;
+            }
+            if (A.bc_switchable[d][s] && (is_fold_bc(A.bc[d][s]) || is_fold_bc(A.bc_after[d][s]))) {
+                set_err("SwitchableBC cannot wrap a fold condition (AxisBC, OriginBC, PoleBC); setup detects those by type");
                 return nullptr;
             }
         }
     }
     if (A.n_species < 1 || A.n_species > CLES_MAX_SPECIES) { set_err("bad species count"); return nullptr; }
-    auto S = std::make_unique<Solver>();
-    S->desc = A;
+    if (A.metric < CLES_METRIC_CARTESIAN || A.metric > CLES_METRIC_SPHERICAL) { set_err("unknown metric"); return nullptr; }
+    bool stretched[3];
+    for (int d = 0; d < 3; ++d) {
+        stretched[d] = A.stretch_x[d] != nullptr;
+        if (stretched[d] != (A.stretch_dxdxi[d] != nullptr)) { set_err("a Stretch needs both x and dx/dxi samples"); return nullptr; }
+    }
+    // NSCBC faces: the characteristic analysis covers faces whose normal scale
+    // factor is one (src/nscbc.jl:309-323); this restatement, like the device
+    // path, takes them on a uniform Cartesian grid only
+    for (int d = 0; d < 3; ++d)
+        for (int s = 0; s < 2; ++s)
+            for (int which = 0; which < 2; ++which) {
+                const int bc = which == 0 ? A.bc[d][s] : (A.bc_switchable[d][s] ? A.bc_after[d][s] : -1);
+                if (bc != CLES_BC_NSCBC_OUTFLOW && bc != CLES_BC_NSCBC_INFLOW) continue;
+                if (!unit_scalefactor(A.metric, d)) {
+                    set_err("characteristic boundary conditions need a face whose normal metric scale factor is one");
+                    return nullptr;
+                }
+                if (A.metric != CLES_METRIC_CARTESIAN || stretched[0] || stretched[1] || stretched[2]) {
+                    set_err("characteristic boundary conditions are built for uniform Cartesian grids only");
+                    return nullptr;
+                }
+            }
+    // coordinate-singularity folds (src/rhs.jl:149-190)
+    const bool axis = A.bc[0][0] == CLES_BC_AXIS;
+    const bool orig1 = A.bc[0][0] == CLES_BC_ORIGIN;
+    const bool pole_l = A.bc[1][0] == CLES_BC_POLE, pole_h = A.bc[1][1] == CLES_BC_POLE;
+    if (pole_l != pole_h) { set_err("PoleBC must be applied at both ends of θ"); return nullptr; }
+    const bool poles = pole_l;
+    const double PI = 3.14159265358979323846;
+    if (axis) {
+        if (A.metric != CLES_METRIC_CYLINDRICAL) { set_err("AxisBC requires CylindricalMetric"); return nullptr; }
+        if (stretched[0]) { set_err("folded dimensions cannot be stretched"); return nullptr; }
+        if (!(std::fabs(A.origin[0]) < 1e-14)) { set_err("AxisBC requires origin[1] = 0"); return nullptr; }
+        if (!(A.n_global[1] == 1 || A.n_global[1] % 2 == 0)) { set_err("resolved-θ AxisBC requires an even θ point count over 2π"); return nullptr; }
+    }
+    if (orig1) {
+        if (A.metric != CLES_METRIC_SPHERICAL) { set_err("OriginBC requires SphericalMetric"); return nullptr; }
+        if (stretched[0]) { set_err("folded dimensions cannot be stretched"); return nullptr; }
+        if (!(std::fabs(A.origin[0]) < 1e-14)) { set_err("OriginBC requires origin[1] = 0"); return nullptr; }
+        if (!(A.n_global[2] == 1 || A.n_global[2] % 2 == 0)) { set_err("resolved-φ OriginBC requires an even φ point count over 2π"); return nullptr; }
+        const double tsum = 2 * A.origin[1] + A.L[1];
+        if (!(A.n_global[1] == 1 || std::fabs(tsum - PI) <= 1e-10)) { set_err("OriginBC requires a θ range symmetric about π/2"); return nullptr; }
+    }
+    if (poles) {
+        if (A.metric != CLES_METRIC_SPHERICAL) { set_err("PoleBC requires SphericalMetric"); return nullptr; }
+        if (stretched[1]) { set_err("folded dimensions cannot be stretched"); return nullptr; }
+        if (!(std::fabs(A.origin[1]) < 1e-14 && std::fabs(A.L[1] - PI) <= 1e-10)) { set_err("PoleBC requires the θ domain (0, π)"); return nullptr; }
+        if (!(A.n_global[2] == 1 || A.n_global[2] % 2 == 0)) { set_err("resolved-φ PoleBC requires an even φ point count over 2π"); return nullptr; }
+    }
     int per[3];
     for (int d = 0; d < 3; ++d) per[d] = A.n_global[d] > 1 ? (A.bc[d][0] == CLES_BC_PERIODIC) : 1;
+    if (axis || orig1) per[0] = 0;
+    if (poles) per[1] = 0;
+    for (int d = 0; d < 3; ++d)
+        if (stretched[d] && per[d]) { set_err("dimension " + std::to_string(d + 1) + ": stretched dimensions must be non-periodic"); return nullptr; }
+    auto S = std::make_unique<Solver>();
+    S->desc = A;
+    S->metric = A.metric;
+    for (int d = 0; d < 3; ++d) {
+        S->desc.stretch_x[d] = S->desc.stretch_dxdxi[d] = nullptr;
+        S->stretched[d] = stretched[d];
+        if (stretched[d]) {
+            S->st_x[d].assign(A.stretch_x[d], A.stretch_x[d] + A.n_global[d]);
+            S->st_m[d].assign(A.stretch_dxdxi[d], A.stretch_dxdxi[d] + A.n_global[d]);
+        }
+    }
     S->D = make_decomp(A.n_global, per, A.n_halo);
     S->Ns = A.n_species; S->ncons = A.n_species + 4;
     S->i_mom[0] = S->Ns; S->i_mom[1] = S->Ns + 1; S->i_mom[2] = S->Ns + 2; S->i_energy = S->Ns + 3;
@@ -1449,12 +1867,61 @@ Solver* solver_create(const cles_solver_desc& A) {
             return nullptr;
         }
     }
+    // grid spacing: computational xi in [0, 1] for stretched dims, half-offset
+    // grids on folded dims (src/rhs.jl:191-205)
+    const bool fold_lo_dim[3] = {axis || orig1, poles, false};
+    const bool fold_hi_dim[3] = {false, poles, false};
     for (int d = 0; d < 3; ++d) {
+        const int n = A.n_global[d];
         if (!S->D.active[d]) S->h[d] = 1.0;
-        else S->h[d] = S->D.periodic[d] ? A.L[d] / A.n_global[d] : A.L[d] / (A.n_global[d] - 1);
+        else if (stretched[d]) S->h[d] = 1.0 / (n - 1);
+        else if (fold_lo_dim[d] && fold_hi_dim[d]) S->h[d] = A.L[d] / n;
+        else if (fold_lo_dim[d]) S->h[d] = A.L[d] / (n - 0.5);
+        else S->h[d] = S->D.periodic[d] ? A.L[d] / n : A.L[d] / (n - 1);
+        S->coord_shift[d] = fold_lo_dim[d] ? S->h[d] / 2 : 0.0;
+        S->orig[d] = stretched[d] ? 0.0 : A.origin[d];
+    }
+    // fold specs (src/rhs.jl:216-280)
+    auto foldspec = [&](int d, bool lo, bool hi, int pdim, int revdim, const int sv[3], int area_parity) -> bool {
+        auto F = std::make_unique<FoldSpec>();
+        F->dim = d; F->lo = lo; F->hi = hi;
+        for (int j = 0; j < 3; ++j) F->sigvel[j] = sv[j];
+        for (int cc = 0; cc < S->ncons; ++cc)
+            F->sigflux.push_back(conserved_parity(*S, sv, cc) * sv[d] * area_parity);
+        const bool shift_needed = pdim >= 0 && S->D.active[pdim];
+        const bool rev_needed = revdim >= 0 && S->D.active[revdim];
+        F->paired = shift_needed || rev_needed;
+        F->pair.pdim = shift_needed ? pdim : -1;
+        F->pair.revdim = rev_needed ? revdim : -1;
+        if (shift_needed && S->D.nl[pdim] % 2 != 0) {
+            set_err("pairing dim " + std::to_string(pdim + 1) + " local extent must be even");
+            return false;
+        }
+        for (int t = 0; t < 2; ++t) {
+            const int sg = t == 0 ? 1 : -1;
+            Plan* dp = plan_create(S->D, A.deriv, d, S->h[d], 1, lo ? sg : 0, hi ? sg : 0);
+            if (!dp) return false;
+            F->dp[t].reset(dp);
+            Plan* fp = plan_create(S->D, A.filt, d, S->h[d], 1, lo ? sg : 0, hi ? sg : 0);
+            if (!fp) return false;
+            F->fp[t].reset(fp);
+        }
+        S->folds[d] = std::move(F);
+        return true;
+    };
+    if (axis) {
+        const int sv[3] = {-1, -1, 1};
+        if (!foldspec(0, true, false, 1, -1, sv, -1)) return nullptr;   // A_1 = r is odd
+    } else if (orig1) {
+        const int sv[3] = {-1, 1, -1};
+        if (!foldspec(0, true, false, 2, 1, sv, 1)) return nullptr;    // A_1 = r^2 sin(theta) is even
+    }
+    if (poles) {
+        const int sv[3] = {1, -1, -1};
+        if (!foldspec(1, true, true, 2, -1, sv, -1)) return nullptr;    // A_2 = r sin(theta) is odd in theta
     }
     for (int d = 0; d < 3; ++d) {
-        if (!S->D.active[d]) continue;
+        if (!S->D.active[d] || S->folds[d]) continue;
         Plan* dp = plan_create(S->D, A.deriv, d, S->h[d], 1);
         if (!dp) return nullptr;
         S->dplan[d].reset(dp);
@@ -1473,10 +1940,15 @@ Solver* solver_create(const cles_solver_desc& A) {
         S->grad_T[d] = F();
         for (int sp = 0; sp < S->Ns; ++sp) S->grad_Y[d].push_back(F());
         for (int cc = 0; cc < S->ncons; ++cc) S->flux[d][cc] = F();
+        S->area[d] = F();
+        S->inv_h[d] = F();
     }
     S->mu_art = F(); S->beta_art = F(); S->kappa_art = F(); S->strain = F();
     S->sensor = F(); S->sensor_sp = F(); S->tmp_a = F(); S->tmp_b = F();
+    S->inv_J = F(); S->inv_r = F(); S->cot_over_r = F();
+    if (S->folds[0] || S->folds[1] || S->folds[2]) { S->pairbuf = F(); S->pairout = F(); }
     S->cfl = A.cfl;
+    init_geometry(*S);
     return S.release();
 }
 
@@ -1597,6 +2069,46 @@ int orc_switch_bc(orc_solver* s, int d, int side) {
         return CLES_EINVAL;
     }
     s->s->switched[d][side] = true;
+    return 0;
+}
+
+// Geometry arrays (padded): 0 inv_J, 1..3 A_d, 4..6 1/h_d, 7 1/r, 8 cot(theta)/r.
+int orc_get_geometry(orc_solver* so, int which, double* out) {
+    Solver& S = *so->s;
+    const std::vector<double>* src = nullptr;
+    if (which == 0) src = &S.inv_J;
+    else if (which >= 1 && which <= 3) src = &S.area[which - 1];
+    else if (which >= 4 && which <= 6) src = &S.inv_h[which - 4];
+    else if (which == 7) src = &S.inv_r;
+    else if (which == 8) src = &S.cot_over_r;
+    if (!src) { set_err("unknown geometry array"); return CLES_EINVAL; }
+    std::memcpy(out, src->data(), sizeof(double) * src->size());
+    return 0;
+}
+// Grid spacing and coordinate shift per dimension.
+int orc_grid_spacing(orc_solver* so, double* h, double* shift, double* orig) {
+    Solver& S = *so->s;
+    for (int d = 0; d < 3; ++d) { h[d] = S.h[d]; shift[d] = S.coord_shift[d]; orig[d] = S.orig[d]; }
+    return 0;
+}
+// deriv_along!(out, f, solver, d, sig) followed by _scale_grad! on padded
+// fields (f must hold current halos on periodic dims).
+int orc_solver_deriv(orc_solver* so, double* f, double* out, int d, int sig, int scale) {
+    Solver& S = *so->s;
+    if (d < 0 || d > 2 || !S.D.active[d]) { set_err("dimension is collapsed"); return CLES_EINVAL; }
+    exchange_halos(S.D, f);
+    deriv_along(S, out, f, d, sig);
+    if (scale) {
+        const double* ih = S.inv_h[d].data();
+        for (size_t I = 0; I < S.fs; ++I) out[I] *= ih[I];
+    }
+    return 0;
+}
+int orc_solver_filter(orc_solver* so, double* f, double* out, int d, int sig) {
+    Solver& S = *so->s;
+    if (d < 0 || d > 2 || !S.D.active[d]) { set_err("dimension is collapsed"); return CLES_EINVAL; }
+    exchange_halos(S.D, f);
+    filt_along(S, out, f, d, sig);
     return 0;
 }
 

@@ -92,6 +92,10 @@ def lib():
         L.orc_get_field.argtypes = [C.c_void_p, C.c_int, _DP]
         L.orc_get_flux.argtypes = [C.c_void_p, C.c_int, C.c_int, _DP]
         L.orc_check_step.argtypes = [C.POINTER(abi.cles_step_control), C.c_double, C.c_double, C.c_double]
+        L.orc_get_geometry.argtypes = [C.c_void_p, C.c_int, _DP]
+        L.orc_grid_spacing.argtypes = [C.c_void_p, _DP, _DP, _DP]
+        L.orc_solver_deriv.argtypes = [C.c_void_p, _DP, _DP, C.c_int, C.c_int, C.c_int]
+        L.orc_solver_filter.argtypes = [C.c_void_p, _DP, _DP, C.c_int, C.c_int]
         _lib = L
     return _lib
 
@@ -290,6 +294,38 @@ class Solver:
 
     def kinetic_energy(self):
         return lib().orc_kinetic_energy(self.ptr)
+
+    GEOMETRY = {"inv_J": 0, "A1": 1, "A2": 2, "A3": 3, "inv_h1": 4, "inv_h2": 5, "inv_h3": 6,
+                "inv_r": 7, "cot_over_r": 8}
+
+    def geometry(self, name):
+        """A geometry array of init_geometry! (src/metric.jl:109-150), padded."""
+        out = np.zeros(self.field_shape)
+        if lib().orc_get_geometry(self.ptr, self.GEOMETRY[name], out):
+            raise ValueError(_err())
+        return out
+
+    def spacing(self):
+        """(h, coord_shift, origin) per dimension (src/rhs.jl:191-205, :286)."""
+        h, sh, o = np.zeros(3), np.zeros(3), np.zeros(3)
+        lib().orc_grid_spacing(self.ptr, h, sh, o)
+        return h, sh, o
+
+    def deriv(self, f, d, sig=1, scale=True):
+        """deriv_along!(out, f, solver, d, sig) (+ _scale_grad!) on a padded field, d 1-based."""
+        f = np.array(f, dtype=np.float64, order="C")
+        out = np.zeros_like(f)
+        if lib().orc_solver_deriv(self.ptr, f, out, int(d) - 1, int(sig), int(bool(scale))):
+            raise ValueError(_err())
+        return out
+
+    def filt(self, f, d, sig=1):
+        """filt_along!(out, f, solver, d, sig) on a padded field, d 1-based."""
+        f = np.array(f, dtype=np.float64, order="C")
+        out = np.zeros_like(f)
+        if lib().orc_solver_filter(self.ptr, f, out, int(d) - 1, int(sig)):
+            raise ValueError(_err())
+        return out
 
     def dissipation_rate(self):
         return lib().orc_dissipation_rate(self.ptr)
