@@ -133,9 +133,11 @@ struct CompactPlan {
 };
 
 // Builds the plan of `scheme` along `dim` (0-based) of a grid with interior
-// extents n3[3]; periodic says whether the line wraps.
+// extents n3[3]; periodic says whether the line wraps.  lo_fold / hi_fold set
+// a coordinate-singularity fold at that end of a closed line: the antipodal
+// parity (+1 / -1) of the field the plan is applied to, 0 for a closure.
 void build_compact_plan(CompactPlan& plan, const cles_scheme& scheme, const int n3[3], int dim,
-                        bool periodic, double h, int dtype);
+                        bool periodic, double h, int dtype, int lo_fold = 0, int hi_fold = 0);
 
 // Output modes of the compact operator.  OUT_RK finishes the flux divergence
 // and applies the low-storage RK update in the store (see launch_compact_rk).

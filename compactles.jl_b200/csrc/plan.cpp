@@ -209,7 +209,7 @@ CompactPlan::~CompactPlan() {
 }
 
 void build_compact_plan(CompactPlan& plan, const cles_scheme& s, const int n3[3], int dim, bool periodic,
-                        double h, int dtype) {
+                        double h, int dtype, int lo_fold, int hi_fold) {
     const int n = n3[dim];
     const int q = s.q, M = s.M, nc = s.nc;
     if (q < 1 || q > CLES_MAX_Q) throw Error(CLES_EINVAL, "scheme LHS half-bandwidth q must be 1 or 2");
@@ -220,7 +220,8 @@ void build_compact_plan(CompactPlan& plan, const cles_scheme& s, const int n3[3]
         throw Error(CLES_EINVAL, "local extent " + std::to_string(n) + " along dim " + std::to_string(dim + 1) +
                                      " too small for scheme '" + std::string(s.name) + "' (need >= " +
                                      std::to_string(nmin) + ")");
-    if (!periodic && M > nc)
+    if (periodic) lo_fold = hi_fold = 0;
+    if (!periodic && M > nc && (!lo_fold || !hi_fold))
         throw Error(CLES_EINVAL, "closed lines need the RHS half-width M <= closure rows nc (halos are never read)");
     for (int j = 0; j < nc; ++j)
         if (s.clo_len[j] < 0 || s.clo_len[j] > CLES_MAX_CLO_LEN || s.clo_len[j] > n)
@@ -232,7 +233,15 @@ void build_compact_plan(CompactPlan& plan, const cles_scheme& s, const int n3[3]
     P.q = q; P.M = M; P.symmetric = s.symmetric; P.periodic = periodic ? 1 : 0;
     P.lo_closed = periodic ? 0 : 1;
     P.hi_closed = periodic ? 0 : 1;
-    P.nc = nc;
+    // A folded end carries rows of the interior stencil whose reads beyond the
+    // edge are the half-offset mirror f[-1-g] = sigma f[g] (the fold_fill! halo,
+    // src/folds.jl:83-124), written as closure rows over the interior; both
+    // ends then hold the same number of rows.
+    const int ncr = (lo_fold || hi_fold) ? std::max(nc, M) : nc;
+    if (ncr > CLES_MAX_NC || ((lo_fold || hi_fold) && ncr + M > CLES_MAX_CLO_LEN))
+        throw Error(CLES_EINVAL, "folded rows exceed the closure-row tables");
+    if (n < 2 * ncr + 1) throw Error(CLES_EINVAL, "line too short for the folded rows");
+    P.nc = ncr;
     P.lines = 1;
     for (int k = 0; k < 3; ++k) if (k != dim) P.lines *= n3[k];
     if (P.lines >= (int64_t)1 << 31) throw Error(CLES_EINVAL, "too many lines for one plan (2^31)");
@@ -244,11 +253,43 @@ void build_compact_plan(CompactPlan& plan, const cles_scheme& s, const int n3[3]
     const double scale = s.symmetric ? 1.0 : hinv;
     P.a0 = s.a0;
     for (int m = 0; m < M; ++m) P.ci[m] = s.coeffs[m] * scale;
-    for (int j = 0; j < nc; ++j) {
-        P.clo_len[j] = s.clo_len[j];
-        for (int t = 0; t < s.clo_len[j]; ++t) {
-            P.clo[j][t] = s.clo_rhs[j][t] * scale;
-            P.chi[j][t] = s.clo_rhs[j][t] * (scale * sgn);
+    // row r's interior stencil over a line with mirrored ends, as weights per index
+    auto folded_row = [&](int r, double* w, int len) {
+        std::fill(w, w + len, 0.0);
+        auto add = [&](int g, double c) {
+            double sg = 1.0;
+            if (g < 0) { g = -1 - g; sg = (double)lo_fold; }
+            else if (g >= n) { g = 2 * n - 1 - g; sg = (double)hi_fold; }
+            w[g] += sg * c;
+        };
+        if (s.symmetric) add(r, P.a0);
+        for (int m = 1; m <= M; ++m) {
+            add(r + m, P.ci[m - 1]);
+            add(r - m, s.symmetric ? P.ci[m - 1] : -P.ci[m - 1]);
+        }
+    };
+    std::vector<double> wrow((size_t)n, 0.0);
+    for (int j = 0; j < ncr; ++j) {
+        // low end: row j, stencil on f[0 .. len-1]
+        if (lo_fold) {
+            const int len = j + M + 1;
+            folded_row(j, wrow.data(), n);
+            P.clo_len[j] = len;
+            for (int t = 0; t < len; ++t) P.clo[j][t] = wrow[t];
+        } else {
+            for (int t = 0; t < s.clo_len[j]; ++t) P.clo[j][t] = s.clo_rhs[j][t] * scale;
+            P.clo_len[j] = s.clo_len[j];
+        }
+        // high end: row n-1-j, stencil on f[n-1-t]; the table length is shared
+        // with the low end (unused weights are zero), so it covers the longer
+        if (hi_fold) {
+            const int len = j + M + 1;
+            folded_row(n - 1 - j, wrow.data(), n);
+            for (int t = 0; t < len; ++t) P.chi[j][t] = wrow[n - 1 - t];
+            P.clo_len[j] = std::max(P.clo_len[j], len);
+        } else {
+            for (int t = 0; t < s.clo_len[j]; ++t) P.chi[j][t] = s.clo_rhs[j][t] * (scale * sgn);
+            P.clo_len[j] = std::max(P.clo_len[j], s.clo_len[j]);
         }
     }
 
@@ -265,7 +306,27 @@ void build_compact_plan(CompactPlan& plan, const cles_scheme& s, const int n3[3]
         }
     }
     if (!periodic) {
-        for (int j = 0; j < nc; ++j) {
+        // parity folds (src/operators.jl:61-70, src/operators_banded.jl:58-77):
+        // the coupling of row i to a ghost column maps onto its mirror column
+        // with the solution's sign sigma_g (the field's parity for a filter,
+        // its opposite for a derivative)
+        const int sg_lo = s.symmetric ? lo_fold : -lo_fold;
+        const int sg_hi = s.symmetric ? hi_fold : -hi_fold;
+        if (lo_fold)
+            for (int i = 1; i <= q; ++i)
+                for (int m = 1; m <= q; ++m) {
+                    if (i - m >= 1) continue;
+                    const int jcol = m - i + 1;
+                    B.a[(size_t)(i - 1) * W + q + (jcol - i)] += (double)sg_lo * s.lhs[m - 1];
+                }
+        if (hi_fold)
+            for (int i = n - q + 1; i <= n; ++i)
+                for (int m = 1; m <= q; ++m) {
+                    if (i + m <= n) continue;
+                    const int jcol = 2 * n + 1 - (i + m);
+                    B.a[(size_t)(i - 1) * W + q + (jcol - i)] += (double)sg_hi * s.lhs[m - 1];
+                }
+        for (int j = 0; j < nc && !lo_fold; ++j)
             for (int t = -q; t <= q; ++t) {
                 double v = s.clo_lhs[j][q + t];
                 if (j + t < 0) {
@@ -274,6 +335,7 @@ void build_compact_plan(CompactPlan& plan, const cles_scheme& s, const int n3[3]
                 }
                 B.a[(size_t)j * W + q + t] = v;
             }
+        for (int j = 0; j < nc && !hi_fold; ++j) {
             const int r = n - 1 - j;
             for (int t = -q; t <= q; ++t) {
                 double v = s.clo_lhs[j][q - t];

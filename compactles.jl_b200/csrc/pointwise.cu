@@ -420,14 +420,25 @@ __global__ void k_dart(const F* __restrict__ sensor, const F* __restrict__ prim,
 // SINGLE (one species): the species diffusion flux rho D dY (Y - 1) is zero in
 // exact arithmetic (Y = 1) and below ~1e-30 of the momentum flux in FP64, so it
 // is taken as 0 and dY/dx_d is neither computed nor read (gty holds dT only).
-template <typename F, bool SINGLE, bool N9>
+template <typename F, bool SINGLE, bool N9, bool GEO>
 __global__ void k_fluxes(const double* __restrict__ Q, const F* __restrict__ prim, const F* __restrict__ g,
                          const F* __restrict__ gty, const F* __restrict__ art, F* __restrict__ flux, int64_t cells,
-                         int Ns, PhysConst pc, double mu0, double Pr, double Sc) {
+                         int Ns, PhysConst pc, double mu0, double Pr, double Sc, Geom G) {
     if (SINGLE) Ns = 1;
     const int ncons = Ns + 4;
     const int gstride = SINGLE ? 1 : 1 + Ns;
     GRID_STRIDE(I, cells) {
+        // curvilinear / stretched grids store A_d F_d (src/rhs.jl:670-675)
+        double area[3] = {1.0, 1.0, 1.0};
+        if (GEO) {
+            int i, j, k;
+            cell_ijk(I, G.n, i, j, k);
+            const GeoPoint gp = geo_point(G, i, j, k, I);
+            area[0] = gp.A[0];
+            area[1] = gp.A[1];
+            area[2] = gp.A[2];
+        }
+#define CLES_AF(v) (GEO ? __dmul_rn(ad, (v)) : (v))
         double gv[9];
 #pragma unroll
         for (int k = 0; k < 9; ++k) gv[k] = double(g[I + cells * k]);
@@ -451,13 +462,15 @@ __global__ void k_fluxes(const double* __restrict__ Q, const F* __restrict__ pri
 #pragma unroll
         for (int d = 0; d < 3; ++d) {
             const double ud = uv[d];
+            const double ad = area[d];
             const double* td = tau[d];
             const F* gd = gty + cells * (int64_t)(d * gstride);
             F* fd = flux + cells * (int64_t)(d * ncons);
             double hdiff = 0.0;
             if (SINGLE) {
                 const double Yk = double(prim[I + cells * P_Y0]);
-                fd[I] = F(r * Yk * ud);
+                const double f0 = r * Yk * ud;
+                fd[I] = F(CLES_AF(f0));
             } else {
                 double Vc = 0.0;
                 for (int sp = 0; sp < Ns; ++sp)
@@ -466,17 +479,22 @@ __global__ void k_fluxes(const double* __restrict__ Q, const F* __restrict__ pri
                     const double Dk = D0 + double(art[I + cells * (A_D0 + sp)]);
                     const double Yk = double(prim[I + cells * (P_Y0 + sp)]);
                     const double Jkd = r * (-Dk * double(gd[I + cells * (1 + sp)]) + Yk * Vc);
-                    fd[I + cells * sp] = F(r * Yk * ud + Jkd);
+                    const double fk = r * Yk * ud + Jkd;
+                    fd[I + cells * sp] = F(CLES_AF(fk));
                     hdiff += (N9 ? n9_h(pc, sp, Tp) : pc.cpk[sp] * Tp) * Jkd;
                 }
             }
-            fd[I + cells * (Ns + 0)] = F(r * ud * uv[0] + (d == 0 ? p : 0.0) - td[0]);
-            fd[I + cells * (Ns + 1)] = F(r * ud * uv[1] + (d == 1 ? p : 0.0) - td[1]);
-            fd[I + cells * (Ns + 2)] = F(r * ud * uv[2] + (d == 2 ? p : 0.0) - td[2]);
-            fd[I + cells * (Ns + 3)] =
-                F((E + p) * ud - (uv[0] * td[0] + uv[1] * td[1] + uv[2] * td[2]) - ka * double(gd[I]) + hdiff);
+            const double m0 = r * ud * uv[0] + (d == 0 ? p : 0.0) - td[0];
+            const double m1 = r * ud * uv[1] + (d == 1 ? p : 0.0) - td[1];
+            const double m2 = r * ud * uv[2] + (d == 2 ? p : 0.0) - td[2];
+            const double en = (E + p) * ud - (uv[0] * td[0] + uv[1] * td[1] + uv[2] * td[2]) - ka * double(gd[I]) + hdiff;
+            fd[I + cells * (Ns + 0)] = F(CLES_AF(m0));
+            fd[I + cells * (Ns + 1)] = F(CLES_AF(m1));
+            fd[I + cells * (Ns + 2)] = F(CLES_AF(m2));
+            fd[I + cells * (Ns + 3)] = F(CLES_AF(en));
         }
     }
+#undef CLES_AF
 }
 
 // Low-storage RK update (src/timestep.jl:86-95): v = A du + dt dQ; du = v; Q += B v.
@@ -906,10 +924,24 @@ template <typename F>
 void Pointwise<F>::fluxes(const double* Q, const F* prim, const F* g, const F* gty, const F* art, F* flux,
                           int64_t cells, int Ns, const PhysConst& pc, double mu0, double Pr, double Sc,
                           cudaStream_t st) {
-    if (Ns == 1) LAUNCH((k_fluxes<F, true, false>), cells, st, Q, prim, g, gty, art, flux, cells, Ns, pc, mu0, Pr, Sc);
+    const Geom G{};
+    if (Ns == 1)
+        LAUNCH((k_fluxes<F, true, false, false>), cells, st, Q, prim, g, gty, art, flux, cells, Ns, pc, mu0, Pr, Sc, G);
     else if (pc.eos == CLES_EOS_NASA9)
-        LAUNCH((k_fluxes<F, false, true>), cells, st, Q, prim, g, gty, art, flux, cells, Ns, pc, mu0, Pr, Sc);
-    else LAUNCH((k_fluxes<F, false, false>), cells, st, Q, prim, g, gty, art, flux, cells, Ns, pc, mu0, Pr, Sc);
+        LAUNCH((k_fluxes<F, false, true, false>), cells, st, Q, prim, g, gty, art, flux, cells, Ns, pc, mu0, Pr, Sc, G);
+    else
+        LAUNCH((k_fluxes<F, false, false, false>), cells, st, Q, prim, g, gty, art, flux, cells, Ns, pc, mu0, Pr, Sc, G);
+}
+template <typename F>
+void Pointwise<F>::fluxes_geo(const double* Q, const F* prim, const F* g, const F* gty, const F* art, F* flux,
+                              int64_t cells, int Ns, const PhysConst& pc, double mu0, double Pr, double Sc,
+                              const Geom& G, cudaStream_t st) {
+    if (Ns == 1)
+        LAUNCH((k_fluxes<F, true, false, true>), cells, st, Q, prim, g, gty, art, flux, cells, Ns, pc, mu0, Pr, Sc, G);
+    else if (pc.eos == CLES_EOS_NASA9)
+        LAUNCH((k_fluxes<F, false, true, true>), cells, st, Q, prim, g, gty, art, flux, cells, Ns, pc, mu0, Pr, Sc, G);
+    else
+        LAUNCH((k_fluxes<F, false, false, true>), cells, st, Q, prim, g, gty, art, flux, cells, Ns, pc, mu0, Pr, Sc, G);
 }
 template <typename F>
 void Pointwise<F>::lsrk(double* Q, double* du, const F* dQ, int64_t n, double A, double B, double dt, cudaStream_t st,
@@ -925,6 +957,11 @@ void Pointwise<F>::rate(const double* Q, const F* prim, const F* art, double* pa
     count_launch();
     check_launch("k_rate_partial");
     k_rate_final<<<1, kThreads, 0, st>>>(part, (int)nb, out);
+    count_launch();
+    check_launch("k_rate_final");
+}
+void rate_final(const double* part, int nb, double* out, cudaStream_t st) {
+    k_rate_final<<<1, kThreads, 0, st>>>(part, nb, out);
     count_launch();
     check_launch("k_rate_final");
 }

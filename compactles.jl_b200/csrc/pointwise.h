@@ -66,6 +66,27 @@ struct NscbcParams {
     double u[3], T, Y[CLES_MAX_SPECIES], eta_u, eta_T, eta_t, eta_Y;
 };
 
+// Orthogonal-metric geometry (src/metric.jl:109-150) as per-dimension node
+// tables; the per-point factors J, A_d, 1/h_d, 1/r are recomputed where they
+// are used instead of being streamed from HBM.
+struct Geom {
+    int metric;          // CLES_METRIC_*
+    int n[3];
+    const double* x[3];  // physical node coordinate per dimension (n[d] values)
+    const double* m[3];  // mapping Jacobian dx/dxi per dimension (1 when unstretched)
+    const double* sn;    // sin(theta) at the theta nodes (spherical)
+    const double* cs;    // cos(theta) at the theta nodes (spherical)
+    const double* cotr;  // cot(theta)/r per cell after the GCL correction, or null (analytic)
+};
+
+// On-rank antipodal pairing of a folded dimension (src/folds.jl:128-155):
+// shift pdim by half its extent, reverse revdim (-1 = none); sd is the
+// dimension whose lower half holds the canonical slots.
+struct PairParams {
+    int n[3];
+    int pdim, revdim, sd;
+};
+
 template <typename F>
 struct Pointwise {
     // esens: also write the kappa*-sensor input (internal energy) into slot P_Y0 + Ns
@@ -104,7 +125,85 @@ struct Pointwise {
     static void nscbc(F* dQ, const F* prim, const F* g, const F* gty, int ngty, const F* dpd, const F* dpt0,
                       const F* dpt1, const F* drd, const Grid3& gr, int d, int side, int Ns, const PhysConst& pc,
                       const NscbcParams& bp, cudaStream_t st);
+    // fluxes with each direction's flux multiplied by its area factor A_d
+    // (the A_d F_d product of src/rhs.jl:670-675), for curvilinear / stretched grids
+    static void fluxes_geo(const double* Q, const F* prim, const F* g, const F* gty, const F* art, F* flux,
+                           int64_t cells, int Ns, const PhysConst& pc, double mu0, double Pr, double Sc,
+                           const Geom& G, cudaStream_t st);
 };
+
+// Curvilinear / stretched-grid passes (geometry.cu).
+template <typename F>
+struct MetricOps {
+    // velocity gradients: 1/h_d scaling of the coordinate derivatives (zero on
+    // collapsed dims) plus the curvature terms (src/rhs.jl:596-604, src/metric.jl:177-221)
+    static void metric_grad(F* g, const F* prim, const Geom& G, const Grid3& gr, cudaStream_t st);
+    // 1/h_d scaling of `count` gradient fields per active dim ([d][count] layout)
+    static void scale_grad(F* f, int count, const Geom& G, const Grid3& gr, cudaStream_t st);
+    // dQ_c = -sum_d inv_J D_d(A_d F_dc) from the per-direction derivatives in
+    // fd ([d][ncons] layout), then the momentum sources (src/rhs.jl:650-687)
+    static void metric_div(F* dQ, const F* fd, int ncons, int Ns, const F* prim, const F* g, const F* art,
+                           double mu0, const Geom& G, const Grid3& gr, cudaStream_t st);
+    // max_rate with the inverse physical spacing 1/(h_d h) and the curvature rate
+    static void rate_geo(const double* Q, const F* prim, const F* art, double* part, double* out, int Ns,
+                         const double h[3], double mu0, double Pr, double Sc, const Geom& G, const Grid3& gr,
+                         cudaStream_t st);
+};
+
+// Folded-dimension butterflies (src/folds.jl:162-262) on interior fields of
+// element type T: w <- (e, o) combination of f; out <- (Re + Ro, sig (Re - Ro)).
+template <typename T>
+void pair_forward(const T* f, T* w, const PairParams& pp, int sig, cudaStream_t st);
+template <typename T>
+void pair_backward(T* out, const T* pairout, const PairParams& pp, int sig, cudaStream_t st);
+
+#ifdef __CUDACC__
+// init_geometry! (src/metric.jl:109-140) at interior cell (i, j, k): the same
+// products and quotients in the same order, with no contraction.
+struct GeoPoint {
+    double inv_J, A[3], inv_h[3], inv_r, cotr;
+};
+__device__ __forceinline__ double geo_max(double x, double y) {
+    if (x != x) return x;
+    return y > x ? y : x;
+}
+__device__ __forceinline__ GeoPoint geo_point(const Geom& G, int i, int j, int k, int64_t I) {
+    const double tiny = 1e-300;
+    const double x1 = G.x[0][i];
+    double h1 = 1.0, h2 = 1.0, h3 = 1.0;
+    if (G.metric != CLES_METRIC_CARTESIAN) h2 = x1;
+    if (G.metric == CLES_METRIC_SPHERICAL) h3 = __dmul_rn(x1, G.sn[j]);
+    h1 = geo_max(__dmul_rn(h1, G.m[0][i]), tiny);
+    h2 = geo_max(__dmul_rn(h2, G.m[1][j]), tiny);
+    h3 = geo_max(__dmul_rn(h3, G.m[2][k]), tiny);
+    const double J = __dmul_rn(__dmul_rn(h1, h2), h3);
+    GeoPoint p;
+    p.inv_J = 1.0 / J;
+    p.A[0] = J / h1;
+    p.A[1] = J / h2;
+    p.A[2] = J / h3;
+    p.inv_h[0] = 1.0 / h1;
+    p.inv_h[1] = 1.0 / h2;
+    p.inv_h[2] = 1.0 / h3;
+    p.inv_r = 1.0 / geo_max(x1, tiny);
+    p.cotr = 0.0;
+    if (G.metric == CLES_METRIC_SPHERICAL)
+        p.cotr = G.cotr ? G.cotr[I] : G.cs[j] / geo_max(__dmul_rn(x1, G.sn[j]), tiny);
+    return p;
+}
+__device__ __forceinline__ void cell_ijk(int64_t I, const int n[3], int& i, int& j, int& k) {
+    i = (int)(I % n[0]);
+    const int64_t r = I / n[0];
+    j = (int)(r % n[1]);
+    k = (int)(r / n[1]);
+}
+#endif
+
+// A_d over the interior (double), and cot(theta)/r = inv_J * dA (GCL, src/metric.jl:154-170)
+void geo_area(double* out, int d, const Geom& G, cudaStream_t st);
+void geo_gcl(double* cotr, const double* dA, const Geom& G, cudaStream_t st);
+// k_rate_final of pointwise.cu: reduce nb (rate, rho_min) partials
+void rate_final(const double* part, int nb, double* out, cudaStream_t st);
 
 void bc_plane(double* Q, const Grid3& g, int d, int side, int Ns, int kind, const BcState& s, cudaStream_t st);
 // Interior of one padded field (extents n + 2 pad, x fastest) into the interior layout.

@@ -76,12 +76,15 @@ public:
             if (d.n_global[k] < 1) throw Error(CLES_EINVAL, "n_global must be >= 1");
             if (d.n_global[k] == 1 && !p0) throw Error(CLES_EINVAL, "collapsed dimension must use (PeriodicBC(), PeriodicBC())");
             for (int s = 0; s < 2; ++s) {
-                if (d.bc[k][s] < CLES_BC_PERIODIC || d.bc[k][s] > CLES_BC_NSCBC_INFLOW)
+                if (d.bc[k][s] < CLES_BC_PERIODIC || d.bc[k][s] > CLES_BC_POLE)
                     throw Error(CLES_EINVAL, "unknown boundary condition");
                 if (d.bc_switchable[k][s]) {
-                    // SwitchableBC(before, after) (src/boundary.jl:137-148)
-                    if (d.bc_after[k][s] < CLES_BC_PERIODIC || d.bc_after[k][s] > CLES_BC_NSCBC_INFLOW)
+                    // SwitchableBC(before, after) (src/boundary.jl:113-148)
+                    if (d.bc_after[k][s] < CLES_BC_PERIODIC || d.bc_after[k][s] > CLES_BC_POLE)
                         throw Error(CLES_EINVAL, "unknown boundary condition");
+                    if (is_fold_bc(d.bc[k][s]) || is_fold_bc(d.bc_after[k][s]))
+                        throw Error(CLES_EINVAL, "SwitchableBC cannot wrap a fold condition (AxisBC, OriginBC, PoleBC); "
+                                                 "setup detects those by type");
                     if ((d.bc_after[k][s] == CLES_BC_PERIODIC) != (d.bc[k][s] == CLES_BC_PERIODIC))
                         throw Error(CLES_EINVAL, "SwitchableBC: both conditions must agree on periodicity");
                 }
@@ -105,16 +108,26 @@ public:
         nasa9_setup(pc_, d);
         cells_ = (int64_t)g_.n[0] * g_.n[1] * g_.n[2];
         cfl = d.cfl;
+        setup_geometry(d);
         const int dt = sizeof(F) == 8 ? CLES_F64 : CLES_F32;
         for (int k = 0; k < 3; ++k) {
             if (!g_.active[k]) continue;
-            deriv_[k].reset(new CompactPlan());
-            build_compact_plan(*deriv_[k], d.deriv, g_.n, k, g_.periodic[k] != 0, h_[k], dt);
-            filt_[k].reset(new CompactPlan());
-            build_compact_plan(*filt_[k], d.filt, g_.n, k, g_.periodic[k] != 0, h_[k], dt);
-            if (dt != CLES_F64) {
-                qfilt_[k].reset(new CompactPlan());
-                build_compact_plan(*qfilt_[k], d.filt, g_.n, k, g_.periodic[k] != 0, h_[k], CLES_F64);
+            // a folded dim carries one plan per field parity (src/rhs.jl:256-261)
+            const int nt = fold_[k].on ? 2 : 1;
+            for (int t = 0; t < nt; ++t) {
+                const int sg = t == 0 ? 1 : -1;
+                const int lo = fold_[k].on && fold_[k].lo ? sg : 0, hi = fold_[k].on && fold_[k].hi ? sg : 0;
+                deriv_[k][t].reset(new CompactPlan());
+                build_compact_plan(*deriv_[k][t], d.deriv, g_.n, k, g_.periodic[k] != 0, h_[k], dt, lo, hi);
+                filt_[k][t].reset(new CompactPlan());
+                build_compact_plan(*filt_[k][t], d.filt, g_.n, k, g_.periodic[k] != 0, h_[k], dt, lo, hi);
+                if (dt != CLES_F64) {
+                    qfilt_[k][t].reset(new CompactPlan());
+                    build_compact_plan(*qfilt_[k][t], d.filt, g_.n, k, g_.periodic[k] != 0, h_[k], CLES_F64, lo, hi);
+                }
+                dset_[k][t] = deriv_[k][t].get();
+                fset_[k][t] = filt_[k][t].get();
+                qset_[k][t] = qfilt_[k][t] ? qfilt_[k][t].get() : filt_[k][t].get();
             }
         }
         const size_t c = (size_t)cells_;
@@ -142,7 +155,235 @@ public:
         CLES_CUDA(cudaMemsetAsync(scratch_.p, 0, scratch_.bytes, st_));
         CLES_CUDA(cudaMemsetAsync(flux_.p, 0, flux_.bytes, st_));
         if (d.control.retries > 0) save_.alloc(ctx, sizeof(double) * c * ncons_);
+        if (geo_) build_geometry_tables(d);
         CLES_CUDA(cudaStreamSynchronize(st_));
+    }
+
+    // ----------------------------------------------------------- geometry --
+    static bool is_fold_bc(int bc) { return bc == CLES_BC_AXIS || bc == CLES_BC_ORIGIN || bc == CLES_BC_POLE; }
+    static bool unit_scalefactor(int metric, int k) {
+        // unit_scalefactor (src/metric.jl:91-93)
+        if (metric == CLES_METRIC_CYLINDRICAL) return k != 1;
+        if (metric == CLES_METRIC_SPHERICAL) return k == 0;
+        return true;
+    }
+
+    // The geometry part of Solver(...) (src/rhs.jl:143-311): validation of the
+    // metric, stretching and folds, grid spacing with half-offset folded
+    // dims, the fold specs with their velocity and flux parities.
+    void setup_geometry(const cles_solver_desc& d) {
+        if (d.metric < CLES_METRIC_CARTESIAN || d.metric > CLES_METRIC_SPHERICAL)
+            throw Error(CLES_EINVAL, "unknown metric");
+        bool str[3];
+        for (int k = 0; k < 3; ++k) {
+            str[k] = d.stretch_x[k] != nullptr;
+            if (str[k] != (d.stretch_dxdxi[k] != nullptr))
+                throw Error(CLES_EINVAL, "a Stretch needs both x and dx/dxi samples");
+            stretched_[k] = str[k];
+        }
+        geo_ = d.metric != CLES_METRIC_CARTESIAN || str[0] || str[1] || str[2];
+        for (int k = 0; k < 3; ++k)
+            for (int s = 0; s < 2; ++s)
+                for (int w = 0; w < 2; ++w) {
+                    const int bc = w == 0 ? d.bc[k][s] : (d.bc_switchable[k][s] ? d.bc_after[k][s] : -1);
+                    if (bc != CLES_BC_NSCBC_OUTFLOW && bc != CLES_BC_NSCBC_INFLOW) continue;
+                    if (!unit_scalefactor(d.metric, k))
+                        throw Error(CLES_EINVAL, "characteristic boundary conditions need a face whose normal metric "
+                                                 "scale factor is one");
+                    if (geo_)
+                        throw Error(CLES_EINVAL, "characteristic boundary conditions are built for uniform Cartesian "
+                                                 "grids only");
+                }
+        const bool axis = d.bc[0][0] == CLES_BC_AXIS, orig1 = d.bc[0][0] == CLES_BC_ORIGIN;
+        const bool pole_l = d.bc[1][0] == CLES_BC_POLE, pole_h = d.bc[1][1] == CLES_BC_POLE;
+        if (pole_l != pole_h) throw Error(CLES_EINVAL, "PoleBC must be applied at both ends of θ");
+        const bool poles = pole_l;
+        const double PI = 3.14159265358979323846;
+        if (axis) {
+            if (d.metric != CLES_METRIC_CYLINDRICAL) throw Error(CLES_EINVAL, "AxisBC requires CylindricalMetric");
+            if (str[0]) throw Error(CLES_EINVAL, "folded dimensions cannot be stretched");
+            if (!(std::fabs(d.origin[0]) < 1e-14)) throw Error(CLES_EINVAL, "AxisBC requires origin[1] = 0");
+            if (!(d.n_global[1] == 1 || d.n_global[1] % 2 == 0))
+                throw Error(CLES_EINVAL, "resolved-θ AxisBC requires an even θ point count over 2π");
+        }
+        if (orig1) {
+            if (d.metric != CLES_METRIC_SPHERICAL) throw Error(CLES_EINVAL, "OriginBC requires SphericalMetric");
+            if (str[0]) throw Error(CLES_EINVAL, "folded dimensions cannot be stretched");
+            if (!(std::fabs(d.origin[0]) < 1e-14)) throw Error(CLES_EINVAL, "OriginBC requires origin[1] = 0");
+            if (!(d.n_global[2] == 1 || d.n_global[2] % 2 == 0))
+                throw Error(CLES_EINVAL, "resolved-φ OriginBC requires an even φ point count over 2π");
+            if (!(d.n_global[1] == 1 || std::fabs(2 * d.origin[1] + d.L[1] - PI) <= 1e-10))
+                throw Error(CLES_EINVAL, "OriginBC requires a θ range symmetric about π/2");
+            if (d.n_global[2] == 1 && d.n_global[1] > 1 && d.n_global[1] % 2 != 0)
+                throw Error(CLES_EINVAL, "OriginBC pairs θ with π - θ: the θ point count must be even");
+        }
+        if (poles) {
+            if (d.metric != CLES_METRIC_SPHERICAL) throw Error(CLES_EINVAL, "PoleBC requires SphericalMetric");
+            if (str[1]) throw Error(CLES_EINVAL, "folded dimensions cannot be stretched");
+            if (!(std::fabs(d.origin[1]) < 1e-14 && std::fabs(d.L[1] - PI) <= 1e-10))
+                throw Error(CLES_EINVAL, "PoleBC requires the θ domain (0, π)");
+            if (!(d.n_global[2] == 1 || d.n_global[2] % 2 == 0))
+                throw Error(CLES_EINVAL, "resolved-φ PoleBC requires an even φ point count over 2π");
+        }
+        if (axis || orig1) g_.periodic[0] = 0;
+        if (poles) g_.periodic[1] = 0;
+        for (int k = 0; k < 3; ++k)
+            if (str[k] && g_.periodic[k])
+                throw Error(CLES_EINVAL, "dimension " + std::to_string(k + 1) + ": stretched dimensions must be non-periodic");
+        if (d.metric != CLES_METRIC_CARTESIAN &&
+            ((g_.active[0] && g_.periodic[0]) || (d.metric == CLES_METRIC_SPHERICAL && g_.active[1] && g_.periodic[1])))
+            throw Error(CLES_EINVAL, "a periodic radial (or spherical polar) dimension is not supported");
+        // grid spacing (src/rhs.jl:191-205)
+        const bool flo[3] = {axis || orig1, poles, false}, fhi[3] = {false, poles, false};
+        for (int k = 0; k < 3; ++k) {
+            const int n = d.n_global[k];
+            if (!g_.active[k]) h_[k] = 1.0;
+            else if (str[k]) h_[k] = 1.0 / (n - 1);
+            else if (flo[k] && fhi[k]) h_[k] = d.L[k] / n;
+            else if (flo[k]) h_[k] = d.L[k] / (n - 0.5);
+            else h_[k] = g_.periodic[k] ? d.L[k] / n : d.L[k] / (n - 1);
+            shift_[k] = flo[k] ? h_[k] / 2 : 0.0;
+            orig_[k] = str[k] ? 0.0 : d.origin[k];
+        }
+        // fold specs (src/rhs.jl:216-280, src/equations.jl:56-67)
+        auto foldspec = [&](int k, bool lo, bool hi, int pdim, int revdim, const int sv[3], int area_parity) {
+            Fold& f = fold_[k];
+            f.on = true; f.lo = lo; f.hi = hi;
+            for (int j = 0; j < 3; ++j) f.sigvel[j] = sv[j];
+            for (int c = 0; c < ncons_; ++c) {
+                const int cp = (c < Ns_ || c == Ns_ + 3) ? 1 : sv[c - Ns_];
+                f.sigflux[c] = cp * sv[k] * area_parity;
+                f.sigcons[c] = cp;
+            }
+            const bool shift = pdim >= 0 && g_.active[pdim], rev = revdim >= 0 && g_.active[revdim];
+            f.paired = shift || rev;
+            for (int j = 0; j < 3; ++j) f.pp.n[j] = g_.n[j];
+            f.pp.pdim = shift ? pdim : -1;
+            f.pp.revdim = rev ? revdim : -1;
+            f.pp.sd = shift ? pdim : revdim;
+            if (shift && g_.n[pdim] % 2 != 0)
+                throw Error(CLES_EINVAL, "pairing dim " + std::to_string(pdim + 1) + " local extent must be even");
+        };
+        if (axis) {
+            const int sv[3] = {-1, -1, 1};
+            foldspec(0, true, false, 1, -1, sv, -1);   // A_1 = r is odd
+        } else if (orig1) {
+            const int sv[3] = {-1, 1, -1};
+            foldspec(0, true, false, 2, 1, sv, 1);     // A_1 = r^2 sin(theta) is even
+        }
+        if (poles) {
+            const int sv[3] = {1, -1, -1};
+            foldspec(1, true, true, 2, -1, sv, -1);    // A_2 = r sin(theta) is odd in theta
+        }
+        for (int k = 0; k < 3; ++k)
+            if (fold_[k].on) folded_ = true;
+    }
+
+    // Node tables of Geom (x, dx/dxi per dimension, sin/cos of theta) and the
+    // GCL-corrected cot(theta)/r of a resolved spherical theta.
+    void build_geometry_tables(const cles_solver_desc& d) {
+        std::vector<double> tab;
+        size_t off[8];
+        for (int k = 0; k < 3; ++k) {
+            const int n = g_.n[k];
+            off[k] = tab.size();
+            for (int i = 0; i < n; ++i)
+                tab.push_back(stretched_[k] ? d.stretch_x[k][i] : orig_[k] + shift_[k] + (double)i * h_[k]);
+            off[3 + k] = tab.size();
+            for (int i = 0; i < n; ++i) tab.push_back(stretched_[k] ? d.stretch_dxdxi[k][i] : 1.0);
+        }
+        off[6] = tab.size();
+        for (int j = 0; j < g_.n[1]; ++j) tab.push_back(std::sin(tab[off[1] + j]));
+        off[7] = tab.size();
+        for (int j = 0; j < g_.n[1]; ++j) tab.push_back(std::cos(tab[off[1] + j]));
+        geo_tab_.alloc(ctx_, sizeof(double) * tab.size());
+        CLES_CUDA(cudaMemcpy(geo_tab_.p, tab.data(), sizeof(double) * tab.size(), cudaMemcpyHostToDevice));
+        const double* b = geo_tab_.as<double>();
+        G_.metric = d.metric;
+        for (int k = 0; k < 3; ++k) {
+            G_.n[k] = g_.n[k];
+            G_.x[k] = b + off[k];
+            G_.m[k] = b + off[3 + k];
+        }
+        G_.sn = b + off[6];
+        G_.cs = b + off[7];
+        G_.cotr = nullptr;
+        if (folded_) {
+            pairbuf_.alloc(ctx_, sizeof(double) * (size_t)cells_);
+            pairout_.alloc(ctx_, sizeof(double) * (size_t)cells_);
+        }
+        if (d.metric == CLES_METRIC_SPHERICAL && g_.active[1]) {
+            // gcl_cotr! (src/metric.jl:154-170) in FP64 in every precision mode:
+            // D_theta(A_theta) with the theta-momentum flux's fold sign
+            DevBuf a2, da;
+            a2.alloc(ctx_, sizeof(double) * (size_t)cells_);
+            da.alloc(ctx_, sizeof(double) * (size_t)cells_);
+            cotr_.alloc(ctx_, sizeof(double) * (size_t)cells_);
+            geo_area(a2.as<double>(), 1, G_, st_);
+            const int sig = fold_[1].on ? fold_[1].sigflux[Ns_ + 1] : 1;
+            std::unique_ptr<CompactPlan> tmp[2];
+            const CompactPlan* ps[2] = {dset_[1][0], dset_[1][1]};
+            if (sizeof(F) != 8) {
+                const int nt = fold_[1].on ? 2 : 1;
+                for (int t = 0; t < nt; ++t) {
+                    const int sg = t == 0 ? 1 : -1;
+                    tmp[t].reset(new CompactPlan());
+                    build_compact_plan(*tmp[t], d.deriv, g_.n, 1, g_.periodic[1] != 0, h_[1], CLES_F64,
+                                       fold_[1].on && fold_[1].lo ? sg : 0, fold_[1].on && fold_[1].hi ? sg : 0);
+                    ps[t] = tmp[t].get();
+                }
+            }
+            const int sgs[1] = {sig};
+            along_set(ps, 1, a2.p, da.p, 1, OUT_STORE, sgs);
+            geo_gcl(cotr_.as<double>(), da.as<double>(), G_, st_);
+            CLES_CUDA(cudaStreamSynchronize(st_));
+            G_.cotr = cotr_.as<double>();
+        }
+    }
+
+    // deriv_along! / filt_along! routing (src/rhs.jl:452-475, src/folds.jl:
+    // 276-322) over `count` adjacent fields with antipodal parities sig[c]
+    // (nullptr = all +1).  ps[0] is the plan of parity +1 (the only one off a
+    // fold), ps[1] that of parity -1.  Off a fold or on a self-paired fold the
+    // parity is inside the plan's mirror rows (one launch per run of equal
+    // parity); a paired fold runs the even/odd butterfly per field.
+    void along_set(const CompactPlan* const* ps, int k, const void* in, void* out, int count, int mode,
+                   const int* sig) {
+        const size_t esz = ps[0]->dtype == CLES_F64 ? sizeof(double) : sizeof(float);
+        auto at = [&](const void* base, int c) {
+            return reinterpret_cast<void*>(const_cast<char*>(static_cast<const char*>(base)) + esz * (size_t)cells_ * c);
+        };
+        const Fold& f = fold_[k];
+        if (!f.on) {
+            launch_compact(*ps[0], view(const_cast<void*>(in)), view(out), count, mode, st_);
+            return;
+        }
+        auto sg = [&](int c) { return sig ? sig[c] : 1; };
+        if (!f.paired) {
+            for (int c0 = 0; c0 < count;) {
+                int c1 = c0 + 1;
+                while (c1 < count && sg(c1) == sg(c0)) ++c1;
+                launch_compact(*ps[sg(c0) > 0 ? 0 : 1], view(at(in, c0)), view(at(out, c0)), c1 - c0, mode, st_);
+                c0 = c1;
+            }
+            return;
+        }
+        if (mode != OUT_STORE) throw Error(CLES_EINVAL, "a paired fold stores its result");
+        for (int c = 0; c < count; ++c) {
+            const int s = sg(c);
+            if (esz == sizeof(double))
+                pair_forward<double>(static_cast<const double*>(at(in, c)), pairbuf_.as<double>(), f.pp, s, st_);
+            else
+                pair_forward<float>(static_cast<const float*>(at(in, c)), pairbuf_.as<float>(), f.pp, s, st_);
+            // the even combination folds with the field's parity and the odd
+            // one always as odd, as fold_apply! does (src/folds.jl:296-306)
+            launch_compact(*ps[s > 0 ? 0 : 1], view(pairbuf_.p), view(at(out, c)), 1, OUT_STORE, st_);
+            launch_compact(*ps[1], view(pairbuf_.p), view(pairout_.p), 1, OUT_STORE, st_);
+            if (esz == sizeof(double))
+                pair_backward<double>(static_cast<double*>(at(out, c)), pairout_.as<double>(), f.pp, s, st_);
+            else
+                pair_backward<float>(static_cast<float*>(at(out, c)), pairout_.as<float>(), f.pp, s, st_);
+        }
     }
 
     ~Solver() override {
@@ -162,7 +403,7 @@ public:
         // smooth! (src/artificial.jl:98-111): one filter pass per active dim, in
         // place, over `count` adjacent fields
         for (int k = 0; k < 3; ++k)
-            if (g_.active[k]) launch_compact(*filt_[k], view(f), view(f), count, OUT_STORE, st_);
+            if (g_.active[k]) along_set(fset_[k], k, f, f, count, OUT_STORE, nullptr);
     }
 
     // The condition face (k, s) acts as now: a switchable face forwards to its
@@ -200,6 +441,7 @@ public:
             for (int s = 0; s < 2; ++s) {
                 const int bc = face_kind(k, s);
                 if (bc == CLES_BC_PERIODIC || bc == CLES_BC_NSCBC_OUTFLOW || bc == CLES_BC_NSCBC_INFLOW) continue;
+                if (is_fold_bc(bc)) continue;   // enforce! is a no-op on folds (src/boundary.jl:173-175)
                 BcState bs;
                 std::memset(&bs, 0, sizeof(bs));
                 const double* q = face_state(k, s);
@@ -243,15 +485,15 @@ public:
                 F* dpd = scratch(0);
                 F* dt0 = scratch(3);
                 F* dt1 = scratch(4);
-                launch_compact(*deriv_[k], view(prim(P_P)), view(dpd), 1, OUT_STORE, st_);
+                launch_compact(*dset_[k][0], view(prim(P_P)), view(dpd), 1, OUT_STORE, st_);
                 const int t1 = k == 0 ? 1 : 0, t2 = k == 2 ? 1 : 2;
                 F* drd = nullptr;
                 if (bc == CLES_BC_NSCBC_OUTFLOW) {
-                    if (g_.active[t1]) launch_compact(*deriv_[t1], view(prim(P_P)), view(dt0), 1, OUT_STORE, st_);
-                    if (g_.active[t2]) launch_compact(*deriv_[t2], view(prim(P_P)), view(dt1), 1, OUT_STORE, st_);
+                    if (g_.active[t1]) launch_compact(*dset_[t1][0], view(prim(P_P)), view(dt0), 1, OUT_STORE, st_);
+                    if (g_.active[t2]) launch_compact(*dset_[t2][0], view(prim(P_P)), view(dt1), 1, OUT_STORE, st_);
                 } else {
                     drd = dt0;
-                    launch_compact(*deriv_[k], view(prim(P_RHO)), view(drd), 1, OUT_STORE, st_);
+                    launch_compact(*dset_[k][0], view(prim(P_RHO)), view(drd), 1, OUT_STORE, st_);
                 }
                 Pointwise<F>::nscbc(dQ_.as<F>(), prim_.as<F>(), g_u_.as<F>(), gty_.as<F>(), Ns_ == 1 ? 1 : 1 + Ns_, dpd,
                                     dt0, dt1, drd, g_, k, s, Ns_, pc_, np, st_);
@@ -302,18 +544,29 @@ public:
         const bool nscbc = any_nscbc();
         if (nscbc) rk = nullptr;   // the boundary correction comes between the divergence and the update
         if (!primitives_current) PW::primitives(Q_.as<double>(), prim_.as<F>(), cells_, Ns_, pc_, st_, desc.art_enabled);
-        // velocity gradients grad_u[d][j] (src/rhs.jl:596-603), one launch per dim for u, v, w
-        for (int k = 0; k < 3; ++k)
-            if (g_.active[k])
-                launch_compact(*deriv_[k], view(prim(P_U)), view(g_u_.as<F>() + (size_t)cells_ * 3 * k), 3, OUT_STORE, st_);
+        velocity_gradients();
         compute_artificial();
         // temperature and mass-fraction gradients (src/rhs.jl:628-636); with one
         // species only dT (the species diffusion flux vanishes, see k_fluxes)
         const int ngty = Ns_ == 1 ? 1 : 1 + Ns_;
         for (int k = 0; k < 3; ++k)
             if (g_.active[k])
-                launch_compact(*deriv_[k], view(prim(P_T)), view(gty_.as<F>() + (size_t)cells_ * ngty * k), ngty,
-                               OUT_STORE, st_);
+                along_set(dset_[k], k, prim(P_T), gty_.as<F>() + (size_t)cells_ * ngty * k, ngty, OUT_STORE, nullptr);
+        if (geo_) {
+            MetricOps<F>::scale_grad(gty_.as<F>(), ngty, G_, g_, st_);
+            PW::fluxes_geo(Q_.as<double>(), prim_.as<F>(), g_u_.as<F>(), gty_.as<F>(), art_.as<F>(), flux_.as<F>(),
+                           cells_, Ns_, pc_, desc.mu0, desc.Pr, desc.Sc, G_, st_);
+            // general path (src/rhs.jl:669-687): D_d(A_d F_d) in place over the
+            // flux block, then dQ = -sum_d inv_J D_d(A_d F_d) + metric sources
+            for (int k = 0; k < 3; ++k) {
+                if (!g_.active[k]) continue;
+                F* fk = flux_.as<F>() + (size_t)cells_ * ncons_ * k;
+                along_set(dset_[k], k, fk, fk, ncons_, OUT_STORE, fold_[k].on ? fold_[k].sigflux : nullptr);
+            }
+            MetricOps<F>::metric_div(dQ_.as<F>(), flux_.as<F>(), ncons_, Ns_, prim_.as<F>(), g_u_.as<F>(), art_.as<F>(),
+                                     desc.mu0, G_, g_, st_);
+            return false;
+        }
         PW::fluxes(Q_.as<double>(), prim_.as<F>(), g_u_.as<F>(), gty_.as<F>(), art_.as<F>(), flux_.as<F>(), cells_, Ns_,
                    pc_, desc.mu0, desc.Pr, desc.Sc, st_);
         // flux divergence dQ[c] = -sum_d D_d(F_dc) (src/rhs.jl:650-668), accumulated in the store.
@@ -330,10 +583,10 @@ public:
             const int k = order[o];
             if (!g_.active[k]) continue;
             const FieldView fin = view(flux_.as<F>() + (size_t)cells_ * ncons_ * k);
-            if (k == last && !first && rk && launch_compact_rk(*deriv_[k], fin, view(dQ_.as<F>()), ncons_, *rk, st_)) {
+            if (k == last && !first && rk && launch_compact_rk(*dset_[k][0], fin, view(dQ_.as<F>()), ncons_, *rk, st_)) {
                 fused = true;
             } else {
-                launch_compact(*deriv_[k], fin, view(dQ_.as<F>()), ncons_, first ? OUT_NEGATE : OUT_SUBTRACT, st_);
+                launch_compact(*dset_[k][0], fin, view(dQ_.as<F>()), ncons_, first ? OUT_NEGATE : OUT_SUBTRACT, st_);
             }
             first = false;
         }
@@ -358,13 +611,34 @@ public:
         apply_bcs();
     }
 
-    void max_rate(double* rate, double* rho_min) override {
-        Pointwise<F>::primitives(Q_.as<double>(), prim_.as<F>(), cells_, Ns_, pc_, st_, desc.art_enabled);
+    // velocity gradients grad_u[d][j] (src/rhs.jl:596-604): one launch per dim
+    // for u, v, w (per parity on a fold), then on curvilinear / stretched grids
+    // the 1/h_d scaling and the curvature terms
+    void velocity_gradients() {
+        for (int k = 0; k < 3; ++k)
+            if (g_.active[k])
+                along_set(dset_[k], k, prim(P_U), g_u_.as<F>() + (size_t)cells_ * 3 * k, 3, OUT_STORE,
+                          fold_[k].on ? fold_[k].sigvel : nullptr);
+        if (geo_) MetricOps<F>::metric_grad(g_u_.as<F>(), prim_.as<F>(), G_, g_, st_);
+    }
+
+    // the rate reduction of max_rate on the refreshed primitives
+    void rate_pass() {
+        if (geo_) {
+            MetricOps<F>::rate_geo(Q_.as<double>(), prim_.as<F>(), art_.as<F>(), part_.as<double>(), res_.as<double>(),
+                                   Ns_, h_, desc.mu0, desc.Pr, desc.Sc, G_, g_, st_);
+            return;
+        }
         double idx[3];
         int act[3];
         for (int k = 0; k < 3; ++k) { idx[k] = 1.0 / h_[k]; act[k] = g_.active[k]; }
         Pointwise<F>::rate(Q_.as<double>(), prim_.as<F>(), art_.as<F>(), part_.as<double>(), res_.as<double>(), cells_,
                            Ns_, idx, act, desc.mu0, desc.Pr, desc.Sc, st_);
+    }
+
+    void max_rate(double* rate, double* rho_min) override {
+        Pointwise<F>::primitives(Q_.as<double>(), prim_.as<F>(), cells_, Ns_, pc_, st_, desc.art_enabled);
+        rate_pass();
         CLES_CUDA(cudaMemcpyAsync(host_res_, res_.p, 2 * sizeof(double), cudaMemcpyDeviceToHost, st_));
         CLES_CUDA(cudaStreamSynchronize(st_));
         if (take_device_timeouts(st_))
@@ -378,8 +652,7 @@ public:
         // along every active dim in turn, in place (FP64 state in every mode)
         for (int k = 0; k < 3; ++k) {
             if (!g_.active[k]) continue;
-            const CompactPlan& p = qfilt_[k] ? *qfilt_[k] : *filt_[k];
-            launch_compact(p, view(Q_.p), view(Q_.p), ncons_, OUT_STORE, st_);
+            along_set(qset_[k], k, Q_.p, Q_.p, ncons_, OUT_STORE, fold_[k].on ? fold_[k].sigcons : nullptr);
         }
     }
 
@@ -517,6 +790,7 @@ public:
     }
 
     double kinetic_energy() override {
+        if (geo_) throw Error(CLES_EINVAL, "the kinetic-energy diagnostic is built for uniform Cartesian grids only");
         Pointwise<F>::kinetic(Q_.as<double>(), part_.as<double>(), res_.as<double>(), cells_, Ns_, st_);
         CLES_CUDA(cudaMemcpyAsync(host_res_, res_.p, sizeof(double), cudaMemcpyDeviceToHost, st_));
         CLES_CUDA(cudaStreamSynchronize(st_));
@@ -531,11 +805,10 @@ public:
     double dissipation_rate() override {
         // dissipation_rate (src/diagnostics.jl:354-378): refreshes primitives,
         // gradients and artificial properties from the resident state
+        if (geo_) throw Error(CLES_EINVAL, "the dissipation diagnostic is built for uniform Cartesian grids only");
         using PW = Pointwise<F>;
         PW::primitives(Q_.as<double>(), prim_.as<F>(), cells_, Ns_, pc_, st_, desc.art_enabled);
-        for (int k = 0; k < 3; ++k)
-            if (g_.active[k])
-                launch_compact(*deriv_[k], view(prim(P_U)), view(g_u_.as<F>() + (size_t)cells_ * 3 * k), 3, OUT_STORE, st_);
+        velocity_gradients();
         compute_artificial();
         PW::dissipation(prim_.as<F>(), g_u_.as<F>(), art_.as<F>(), part_.as<double>(), res_.as<double>(), g_, desc.mu0,
                         st_);
@@ -565,11 +838,7 @@ public:
             double* clk = clk_.as<double>();
             apply_bcs();
             Pointwise<F>::primitives(Q_.as<double>(), prim_.as<F>(), cells_, Ns_, pc_, st_, desc.art_enabled);
-            double idx[3];
-            int act[3];
-            for (int k = 0; k < 3; ++k) { idx[k] = 1.0 / h_[k]; act[k] = g_.active[k]; }
-            Pointwise<F>::rate(Q_.as<double>(), prim_.as<F>(), art_.as<F>(), part_.as<double>(), res_.as<double>(),
-                               cells_, Ns_, idx, act, desc.mu0, desc.Pr, desc.Sc, st_);
+            rate_pass();
             clock_before(clk, res_.as<double>(), cc_, st_);
             for (int stage = 0; stage < 5; ++stage) {
                 if (stage > 0) apply_bcs();
@@ -667,7 +936,24 @@ private:
     int Ns_ = 1, ncons_ = 5;
     int64_t cells_ = 0;
     PhysConst pc_{};
-    std::unique_ptr<CompactPlan> deriv_[3], filt_[3], qfilt_[3];
+    std::unique_ptr<CompactPlan> deriv_[3][2], filt_[3][2], qfilt_[3][2];
+    const CompactPlan* dset_[3][2] = {};
+    const CompactPlan* fset_[3][2] = {};
+    const CompactPlan* qset_[3][2] = {};
+    // geometry: curvilinear metric or stretching, node tables, folds
+    struct Fold {
+        bool on = false, lo = false, hi = false, paired = false;
+        PairParams pp{};
+        int sigvel[3] = {1, 1, 1};
+        int sigflux[CLES_MAX_SPECIES + 4] = {};
+        int sigcons[CLES_MAX_SPECIES + 4] = {};
+    };
+    bool geo_ = false, folded_ = false;
+    bool stretched_[3] = {false, false, false};
+    double shift_[3]{}, orig_[3]{};
+    Fold fold_[3];
+    Geom G_{};
+    DevBuf geo_tab_, cotr_, pairbuf_, pairout_;
     DevBuf Q_, du_, dQ_, prim_, g_u_, gty_, art_, scratch_, flux_, part_, res_, save_, clk_;
     double* host_res_ = nullptr;
     double* host_clk_ = nullptr;

@@ -1830,6 +1830,12 @@ Solver* solver_create(const cles_solver_desc& A) {
         if (!(A.n_global[2] == 1 || A.n_global[2] % 2 == 0)) { set_err("resolved-φ OriginBC requires an even φ point count over 2π"); return nullptr; }
         const double tsum = 2 * A.origin[1] + A.L[1];
         if (!(A.n_global[1] == 1 || std::fabs(tsum - PI) <= 1e-10)) { set_err("OriginBC requires a θ range symmetric about π/2"); return nullptr; }
+        // with phi collapsed the pairing is the theta reversal alone; an odd
+        // theta count would leave the middle line without a partner
+        if (A.n_global[2] == 1 && A.n_global[1] > 1 && A.n_global[1] % 2 != 0) {
+            set_err("OriginBC pairs θ with π - θ: the θ point count must be even");
+            return nullptr;
+        }
     }
     if (poles) {
         if (A.metric != CLES_METRIC_SPHERICAL) { set_err("PoleBC requires SphericalMetric"); return nullptr; }
@@ -1843,6 +1849,13 @@ Solver* solver_create(const cles_solver_desc& A) {
     if (poles) per[1] = 0;
     for (int d = 0; d < 3; ++d)
         if (stretched[d] && per[d]) { set_err("dimension " + std::to_string(d + 1) + ": stretched dimensions must be non-periodic"); return nullptr; }
+    // the area factors vary along r (and along theta on a sphere): a periodic
+    // wrap of those dimensions would pair unlike halos; not supported
+    if (A.metric != CLES_METRIC_CARTESIAN &&
+        ((A.n_global[0] > 1 && per[0]) || (A.metric == CLES_METRIC_SPHERICAL && A.n_global[1] > 1 && per[1]))) {
+        set_err("a periodic radial (or spherical polar) dimension is not supported");
+        return nullptr;
+    }
     auto S = std::make_unique<Solver>();
     S->desc = A;
     S->metric = A.metric;
