@@ -206,38 +206,45 @@ __device__ __forceinline__ int64_t pair_partner(const PairParams& pp, int c[3]) 
     return c[0] + (int64_t)pp.n[0] * (c[1] + (int64_t)pp.n[1] * c[2]);
 }
 
-// pair_forward! on-rank branch (src/folds.jl:169-190): for each canonical slot
-// x (lower half of sd) and its partner Mx: w[x] = (f[x] + s f[Mx]) / 2,
-// w[Mx] = (f[x] - s f[Mx]) / 2.
+// Full-grid index of half-grid cell J (the sd extent halved) and of its partner.
+__device__ __forceinline__ void pair_cell(const PairParams& pp, int64_t J, int64_t& I, int64_t& Mx) {
+    int nh[3] = {pp.n[0], pp.n[1], pp.n[2]};
+    nh[pp.sd] /= 2;
+    int c[3];
+    cell_ijk(J, nh, c[0], c[1], c[2]);
+    I = c[0] + (int64_t)pp.n[0] * (c[1] + (int64_t)pp.n[1] * c[2]);
+    Mx = pair_partner(pp, c);
+}
+
+// pair_forward! on-rank branch (src/folds.jl:169-190) over `count` fields
+// (stride fs): for each canonical slot x (lower half of sd) and its partner
+// Mx: w[x] = (f[x] + s f[Mx]) / 2, w[Mx] = (f[x] - s f[Mx]) / 2.
 template <typename T>
-__global__ void k_pair_forward(const T* __restrict__ f, T* __restrict__ w, PairParams pp, double sg, int64_t cells) {
-    const int half = pp.n[pp.sd] / 2;
-    GRID_STRIDE(I, cells) {
-        int c[3];
-        cell_ijk(I, pp.n, c[0], c[1], c[2]);
-        if (c[pp.sd] >= half) continue;
-        const int64_t Mx = pair_partner(pp, c);
-        const double a = double(f[I]), b = sg * double(f[Mx]);
-        w[I] = T(0.5 * (a + b));
-        w[Mx] = T(0.5 * (a - b));
+__global__ void k_pair_forward(const T* __restrict__ f, T* __restrict__ w, PairParams pp, double sg, int64_t half,
+                               int64_t fs) {
+    const T* fc = f + fs * blockIdx.y;
+    T* wc = w + fs * blockIdx.y;
+    GRID_STRIDE(J, half) {
+        int64_t I, Mx;
+        pair_cell(pp, J, I, Mx);
+        const double a = double(fc[I]), b = sg * double(fc[Mx]);
+        wc[I] = T(0.5 * (a + b));
+        wc[Mx] = T(0.5 * (a - b));
     }
 }
 
-// fold_apply! selection plus pair_backward! on-rank branch (src/folds.jl:
-// 296-320, 224-243): the partner slots take the odd-combination result, then
-// out[x] = Re + Ro, out[Mx] = s (Re - Ro).
+// pair_backward! on-rank branch (src/folds.jl:224-243) in place: out holds
+// the even result on the canonical half and the odd result on the partner
+// half; out[x] = Re + Ro, out[Mx] = s (Re - Ro).
 template <typename T>
-__global__ void k_pair_backward(T* __restrict__ out, const T* __restrict__ pairout, PairParams pp, double sg,
-                                int64_t cells) {
-    const int half = pp.n[pp.sd] / 2;
-    GRID_STRIDE(I, cells) {
-        int c[3];
-        cell_ijk(I, pp.n, c[0], c[1], c[2]);
-        if (c[pp.sd] >= half) continue;
-        const int64_t Mx = pair_partner(pp, c);
-        const double Re = double(out[I]), Ro = double(pairout[Mx]);
-        out[I] = T(Re + Ro);
-        out[Mx] = T(sg * (Re - Ro));
+__global__ void k_pair_backward(T* out, PairParams pp, double sg, int64_t half, int64_t fs) {
+    T* oc = out + fs * blockIdx.y;
+    GRID_STRIDE(J, half) {
+        int64_t I, Mx;
+        pair_cell(pp, J, I, Mx);
+        const double Re = double(oc[I]), Ro = double(oc[Mx]);
+        oc[I] = T(Re + Ro);
+        oc[Mx] = T(sg * (Re - Ro));
     }
 }
 
@@ -298,16 +305,18 @@ void MetricOps<F>::rate_geo(const double* Q, const F* prim, const F* art, double
 }
 
 template <typename T>
-void pair_forward(const T* f, T* w, const PairParams& pp, int sig, cudaStream_t st) {
-    const int64_t cells = (int64_t)pp.n[0] * pp.n[1] * pp.n[2];
-    k_pair_forward<T><<<grid_for(cells), kThreads, 0, st>>>(f, w, pp, (double)sig, cells);
+void pair_forward(const T* f, T* w, int count, int64_t fs, const PairParams& pp, int sig, cudaStream_t st) {
+    const int64_t half = (int64_t)pp.n[0] * pp.n[1] * pp.n[2] / 2;
+    const dim3 grid(grid_for(half), (unsigned)count);
+    k_pair_forward<T><<<grid, kThreads, 0, st>>>(f, w, pp, (double)sig, half, fs);
     count_launch();
     check_launch("k_pair_forward");
 }
 template <typename T>
-void pair_backward(T* out, const T* pairout, const PairParams& pp, int sig, cudaStream_t st) {
-    const int64_t cells = (int64_t)pp.n[0] * pp.n[1] * pp.n[2];
-    k_pair_backward<T><<<grid_for(cells), kThreads, 0, st>>>(out, pairout, pp, (double)sig, cells);
+void pair_backward(T* out, int count, int64_t fs, const PairParams& pp, int sig, cudaStream_t st) {
+    const int64_t half = (int64_t)pp.n[0] * pp.n[1] * pp.n[2] / 2;
+    const dim3 grid(grid_for(half), (unsigned)count);
+    k_pair_backward<T><<<grid, kThreads, 0, st>>>(out, pp, (double)sig, half, fs);
     count_launch();
     check_launch("k_pair_backward");
 }
@@ -327,9 +336,9 @@ void geo_gcl(double* cotr, const double* dA, const Geom& G, cudaStream_t st) {
 
 template struct MetricOps<double>;
 template struct MetricOps<float>;
-template void pair_forward<double>(const double*, double*, const PairParams&, int, cudaStream_t);
-template void pair_forward<float>(const float*, float*, const PairParams&, int, cudaStream_t);
-template void pair_backward<double>(double*, const double*, const PairParams&, int, cudaStream_t);
-template void pair_backward<float>(float*, const float*, const PairParams&, int, cudaStream_t);
+template void pair_forward<double>(const double*, double*, int, int64_t, const PairParams&, int, cudaStream_t);
+template void pair_forward<float>(const float*, float*, int, int64_t, const PairParams&, int, cudaStream_t);
+template void pair_backward<double>(double*, int, int64_t, const PairParams&, int, cudaStream_t);
+template void pair_backward<float>(float*, int, int64_t, const PairParams&, int, cudaStream_t);
 
 }  // namespace cles

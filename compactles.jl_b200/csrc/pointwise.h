@@ -150,12 +150,14 @@ struct MetricOps {
                          cudaStream_t st);
 };
 
-// Folded-dimension butterflies (src/folds.jl:162-262) on interior fields of
-// element type T: w <- (e, o) combination of f; out <- (Re + Ro, sig (Re - Ro)).
+// Folded-dimension butterflies (src/folds.jl:162-262) on `count` interior
+// fields of element type T spaced fs apart: w <- (e, o) combination of f;
+// out (even result on the canonical half, odd result on the partner half)
+// <- (Re + Ro, sig (Re - Ro)) in place.
 template <typename T>
-void pair_forward(const T* f, T* w, const PairParams& pp, int sig, cudaStream_t st);
+void pair_forward(const T* f, T* w, int count, int64_t fs, const PairParams& pp, int sig, cudaStream_t st);
 template <typename T>
-void pair_backward(T* out, const T* pairout, const PairParams& pp, int sig, cudaStream_t st);
+void pair_backward(T* out, int count, int64_t fs, const PairParams& pp, int sig, cudaStream_t st);
 
 #ifdef __CUDACC__
 // init_geometry! (src/metric.jl:109-140) at interior cell (i, j, k): the same

@@ -128,6 +128,23 @@ public:
                 dset_[k][t] = deriv_[k][t].get();
                 fset_[k][t] = filt_[k][t].get();
                 qset_[k][t] = qfilt_[k][t] ? qfilt_[k][t].get() : filt_[k][t].get();
+                if (fold_[k].paired) {
+                    // the same plan over the lines of one half of the pairing
+                    // dimension: each parity then runs over its own half only
+                    int nh[3] = {g_.n[0], g_.n[1], g_.n[2]};
+                    nh[fold_[k].pp.sd] /= 2;
+                    hderiv_[k][t].reset(new CompactPlan());
+                    build_compact_plan(*hderiv_[k][t], d.deriv, nh, k, false, h_[k], dt, lo, hi);
+                    hfilt_[k][t].reset(new CompactPlan());
+                    build_compact_plan(*hfilt_[k][t], d.filt, nh, k, false, h_[k], dt, lo, hi);
+                    if (dt != CLES_F64) {
+                        hqfilt_[k][t].reset(new CompactPlan());
+                        build_compact_plan(*hqfilt_[k][t], d.filt, nh, k, false, h_[k], CLES_F64, lo, hi);
+                    }
+                    hdset_[k][t] = hderiv_[k][t].get();
+                    hfset_[k][t] = hfilt_[k][t].get();
+                    hqset_[k][t] = hqfilt_[k][t] ? hqfilt_[k][t].get() : hfilt_[k][t].get();
+                }
             }
         }
         const size_t c = (size_t)cells_;
@@ -308,10 +325,7 @@ public:
         G_.sn = b + off[6];
         G_.cs = b + off[7];
         G_.cotr = nullptr;
-        if (folded_) {
-            pairbuf_.alloc(ctx_, sizeof(double) * (size_t)cells_);
-            pairout_.alloc(ctx_, sizeof(double) * (size_t)cells_);
-        }
+        if (folded_) pairbuf_.alloc(ctx_, sizeof(double) * (size_t)cells_ * std::max(ncons_, 3 + Ns_));
         if (d.metric == CLES_METRIC_SPHERICAL && g_.active[1]) {
             // gcl_cotr! (src/metric.jl:154-170) in FP64 in every precision mode:
             // D_theta(A_theta) with the theta-momentum flux's fold sign
@@ -321,20 +335,28 @@ public:
             cotr_.alloc(ctx_, sizeof(double) * (size_t)cells_);
             geo_area(a2.as<double>(), 1, G_, st_);
             const int sig = fold_[1].on ? fold_[1].sigflux[Ns_ + 1] : 1;
-            std::unique_ptr<CompactPlan> tmp[2];
+            std::unique_ptr<CompactPlan> tmp[2], htmp[2];
             const CompactPlan* ps[2] = {dset_[1][0], dset_[1][1]};
+            const CompactPlan* hs[2] = {hdset_[1][0], hdset_[1][1]};
             if (sizeof(F) != 8) {
                 const int nt = fold_[1].on ? 2 : 1;
                 for (int t = 0; t < nt; ++t) {
                     const int sg = t == 0 ? 1 : -1;
+                    const int lo = fold_[1].on && fold_[1].lo ? sg : 0, hi = fold_[1].on && fold_[1].hi ? sg : 0;
                     tmp[t].reset(new CompactPlan());
-                    build_compact_plan(*tmp[t], d.deriv, g_.n, 1, g_.periodic[1] != 0, h_[1], CLES_F64,
-                                       fold_[1].on && fold_[1].lo ? sg : 0, fold_[1].on && fold_[1].hi ? sg : 0);
+                    build_compact_plan(*tmp[t], d.deriv, g_.n, 1, g_.periodic[1] != 0, h_[1], CLES_F64, lo, hi);
                     ps[t] = tmp[t].get();
+                    if (fold_[1].paired) {
+                        int nh[3] = {g_.n[0], g_.n[1], g_.n[2]};
+                        nh[fold_[1].pp.sd] /= 2;
+                        htmp[t].reset(new CompactPlan());
+                        build_compact_plan(*htmp[t], d.deriv, nh, 1, false, h_[1], CLES_F64, lo, hi);
+                        hs[t] = htmp[t].get();
+                    }
                 }
             }
             const int sgs[1] = {sig};
-            along_set(ps, 1, a2.p, da.p, 1, OUT_STORE, sgs);
+            along_set(ps, 1, a2.p, da.p, 1, OUT_STORE, sgs, hs);
             geo_gcl(cotr_.as<double>(), da.as<double>(), G_, st_);
             CLES_CUDA(cudaStreamSynchronize(st_));
             G_.cotr = cotr_.as<double>();
@@ -346,9 +368,20 @@ public:
     // (nullptr = all +1).  ps[0] is the plan of parity +1 (the only one off a
     // fold), ps[1] that of parity -1.  Off a fold or on a self-paired fold the
     // parity is inside the plan's mirror rows (one launch per run of equal
-    // parity); a paired fold runs the even/odd butterfly per field.
+    // parity).  A paired fold runs the even/odd butterfly: the even
+    // combination with the field's parity over the canonical half of the
+    // pairing dimension and the odd one with parity -1 over the partner half
+    // (hs: the same plans over half the lines), then the inverse butterfly in
+    // place.  The reference applies both parities to every line and keeps
+    // one half of each result; the halves kept are the same.
+    const CompactPlan* const* half_of(const CompactPlan* const* ps, int k) const {
+        if (ps == dset_[k]) return hdset_[k];
+        if (ps == fset_[k]) return hfset_[k];
+        if (ps == qset_[k]) return hqset_[k];
+        return nullptr;
+    }
     void along_set(const CompactPlan* const* ps, int k, const void* in, void* out, int count, int mode,
-                   const int* sig) {
+                   const int* sig, const CompactPlan* const* hs = nullptr) {
         const size_t esz = ps[0]->dtype == CLES_F64 ? sizeof(double) : sizeof(float);
         auto at = [&](const void* base, int c) {
             return reinterpret_cast<void*>(const_cast<char*>(static_cast<const char*>(base)) + esz * (size_t)cells_ * c);
@@ -369,28 +402,42 @@ public:
             return;
         }
         if (mode != OUT_STORE) throw Error(CLES_EINVAL, "a paired fold stores its result");
-        for (int c = 0; c < count; ++c) {
-            const int s = sg(c);
+        if (!hs) hs = half_of(ps, k);
+        if (!hs || !hs[0] || !hs[1]) throw Error(CLES_EINVAL, "internal: no half-grid plans for a paired fold");
+        const int64_t sd_stride = f.pp.sd == 0 ? 1 : f.pp.sd == 1 ? (int64_t)g_.n[0] : (int64_t)g_.n[0] * g_.n[1];
+        const int64_t upper = sd_stride * (g_.n[f.pp.sd] / 2);
+        auto half_view = [&](void* base, bool up) {
+            FieldView v = view(base);
+            v.base = static_cast<char*>(base) + (up ? esz * (size_t)upper : 0);
+            return v;
+        };
+        void* w = pairbuf_.p;
+        for (int c0 = 0; c0 < count;) {
+            int c1 = c0 + 1;
+            while (c1 < count && sg(c1) == sg(c0)) ++c1;
+            const int s = sg(c0), run = c1 - c0;
             if (esz == sizeof(double))
-                pair_forward<double>(static_cast<const double*>(at(in, c)), pairbuf_.as<double>(), f.pp, s, st_);
+                pair_forward<double>(static_cast<const double*>(at(in, c0)), static_cast<double*>(at(w, c0)), run,
+                                     cells_, f.pp, s, st_);
             else
-                pair_forward<float>(static_cast<const float*>(at(in, c)), pairbuf_.as<float>(), f.pp, s, st_);
-            // the even combination folds with the field's parity and the odd
-            // one always as odd, as fold_apply! does (src/folds.jl:296-306)
-            launch_compact(*ps[s > 0 ? 0 : 1], view(pairbuf_.p), view(at(out, c)), 1, OUT_STORE, st_);
-            launch_compact(*ps[1], view(pairbuf_.p), view(pairout_.p), 1, OUT_STORE, st_);
-            if (esz == sizeof(double))
-                pair_backward<double>(static_cast<double*>(at(out, c)), pairout_.as<double>(), f.pp, s, st_);
-            else
-                pair_backward<float>(static_cast<float*>(at(out, c)), pairout_.as<float>(), f.pp, s, st_);
+                pair_forward<float>(static_cast<const float*>(at(in, c0)), static_cast<float*>(at(w, c0)), run, cells_,
+                                    f.pp, s, st_);
+            // even combination, folded with the field's parity (src/folds.jl:296-299)
+            launch_compact(*hs[s > 0 ? 0 : 1], half_view(at(w, c0), false), half_view(at(out, c0), false), run,
+                           OUT_STORE, st_);
+            c0 = c1;
         }
-    }
-
-    ~Solver() override {
-        graph_free();
-        if (host_res_) cudaFreeHost(host_res_);
-        if (host_clk_) cudaFreeHost(host_clk_);
-        if (cap_st_) cudaStreamDestroy(cap_st_);
+        // odd combination, always folded as odd (src/folds.jl:300-301)
+        launch_compact(*hs[1], half_view(w, true), half_view(out, true), count, OUT_STORE, st_);
+        for (int c0 = 0; c0 < count;) {
+            int c1 = c0 + 1;
+            while (c1 < count && sg(c1) == sg(c0)) ++c1;
+            if (esz == sizeof(double))
+                pair_backward<double>(static_cast<double*>(at(out, c0)), c1 - c0, cells_, f.pp, sg(c0), st_);
+            else
+                pair_backward<float>(static_cast<float*>(at(out, c0)), c1 - c0, cells_, f.pp, sg(c0), st_);
+            c0 = c1;
+        }
     }
 
     // ------------------------------------------------------------- views --
@@ -953,7 +1000,11 @@ private:
     double shift_[3]{}, orig_[3]{};
     Fold fold_[3];
     Geom G_{};
-    DevBuf geo_tab_, cotr_, pairbuf_, pairout_;
+    std::unique_ptr<CompactPlan> hderiv_[3][2], hfilt_[3][2], hqfilt_[3][2];
+    const CompactPlan* hdset_[3][2] = {};
+    const CompactPlan* hfset_[3][2] = {};
+    const CompactPlan* hqset_[3][2] = {};
+    DevBuf geo_tab_, cotr_, pairbuf_;
     DevBuf Q_, du_, dQ_, prim_, g_u_, gty_, art_, scratch_, flux_, part_, res_, save_, clk_;
     double* host_res_ = nullptr;
     double* host_clk_ = nullptr;
