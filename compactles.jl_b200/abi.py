@@ -126,6 +126,10 @@ CLES_BC_AXIS = 7
 CLES_BC_ORIGIN = 8
 CLES_BC_POLE = 9
 
+# cles_face_fn: (user, dim, side, t, npts, x1, x2, x3, out)
+FACE_FN = C.CFUNCTYPE(None, C.c_void_p, C.c_int, C.c_int, C.c_double, C.c_int64, C.POINTER(C.c_double),
+                      C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double))
+
 CLES_METRIC_CARTESIAN = 0
 CLES_METRIC_CYLINDRICAL = 1
 CLES_METRIC_SPHERICAL = 2

@@ -15,7 +15,7 @@ import subprocess
 import numpy as np
 
 from . import abi
-from .problem import grid_spacing, state_shape
+from .problem import face_callbacks, grid_spacing, state_shape
 
 _HERE = pathlib.Path(__file__).resolve().parent
 LIB_PATH = _HERE / "libcles.so"
@@ -67,6 +67,7 @@ def lib():
         L.cles_apply_along_batch.argtypes = [vp, vp, vp, C.c_int, C.c_int64]
         L.cles_apply_along_host.argtypes = [vp, vp, vp]
         L.cles_solver_switch_bc.argtypes = [vp, C.c_int, C.c_int]
+        L.cles_solver_set_face_fn.argtypes = [vp, C.c_int, C.c_int, C.c_int, abi.FACE_FN, vp]
         L.cles_solver_bc_switched.argtypes = [vp, C.c_int, C.c_int, C.POINTER(C.c_int)]
         L.cles_checkpoint_save.argtypes = [vp, C.c_char_p]
         L.cles_checkpoint_load.argtypes = [vp, C.c_char_p]
@@ -269,6 +270,10 @@ class Solver:
         _check(lib().cles_solver_create(self.ctx.ptr, C.byref(desc), C.byref(self.ptr)))
         self.n_cons = desc.n_species + 4
         self.h = grid_spacing(desc)
+        # DirichletBC(fun) / NSCBCInflowBC(target=fun) faces, called back at the stage times
+        self._face_cbs, self.face_errors = face_callbacks(desc)
+        for k, s, which, cb in self._face_cbs:
+            _check(lib().cles_solver_set_face_fn(self.ptr, k, s, which, cb, None))
 
     def __del__(self):
         try:

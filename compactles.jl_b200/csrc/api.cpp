@@ -459,6 +459,10 @@ int cles_set_clock(cles_solver* s, double t, int64_t step, double cfl) {
 
 int cles_solver_switch_bc(cles_solver* s, int dim, int side) { SOLVER_CALL(s->s->switch_bc(dim, side)) }
 
+int cles_solver_set_face_fn(cles_solver* s, int dim, int side, int which, cles_face_fn fn, void* user) {
+    SOLVER_CALL(s->s->set_face_fn(dim, side, which, fn, user))
+}
+
 int cles_solver_bc_switched(const cles_solver* s, int dim, int side, int* switched) {
     API_BEGIN
     if (!s || !switched) throw Error(CLES_EINVAL, "null argument");

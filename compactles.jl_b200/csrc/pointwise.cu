@@ -654,7 +654,8 @@ __global__ void k_sum_final(const double* __restrict__ part, int nb, int width, 
 
 // enforce!(::SlipWallBC) (src/boundary.jl:232-243) and a time-constant
 // DirichletBC (src/problem.jl:209-221) on the wall plane of (d, side).
-__global__ void k_bc_plane(double* __restrict__ Q, Grid3 g, int d, int side, int Ns, int kind, BcState st) {
+__global__ void k_bc_plane(double* __restrict__ Q, Grid3 g, int d, int side, int Ns, int kind, BcState st,
+                           const double* __restrict__ qface) {
     const int o1 = d == 0 ? 1 : 0, o2 = d == 2 ? 1 : 2;
     const int64_t plane = (int64_t)g.n[o1] * g.n[o2];
     const int64_t cells = (int64_t)g.n[0] * g.n[1] * g.n[2];
@@ -690,6 +691,9 @@ __global__ void k_bc_plane(double* __restrict__ Q, Grid3 g, int d, int side, int
             // enforce!(::ExtrapolationBC) (src/boundary.jl:267-278): copy the adjacent interior plane
             const int64_t J = I + (side == 0 ? stv[d] : -stv[d]);
             for (int c = 0; c < Ns + 4; ++c) Q[I + cells * c] = Q[J + cells * c];
+        } else if (qface) {
+            // DirichletBC(fun): the stage-time state per node ([c][plane])
+            for (int c = 0; c < Ns + 4; ++c) Q[I + cells * c] = qface[c * plane + t];
         } else {
             for (int c = 0; c < Ns + 4; ++c) Q[I + cells * c] = st.q[c];
         }
@@ -697,13 +701,15 @@ __global__ void k_bc_plane(double* __restrict__ Q, Grid3 g, int d, int side, int
 }
 
 // correct_rhs!(::NSCBCOutflowBC) (src/nscbc.jl:59-157) and
-// correct_rhs!(::NSCBCInflowBC) with constant targets (src/nscbc.jl:220-307):
-// LODI wave-amplitude corrections of dQ on one boundary plane.
+// correct_rhs!(::NSCBCInflowBC) (src/nscbc.jl:220-307): LODI wave-amplitude
+// corrections of dQ on one boundary plane.  Inflow targets are the constants
+// of bp, or per node from tgt ([velocity 0..2, T, Y_k][plane], the stage-time
+// target function's values) when tgt is set.
 template <typename F, bool N9>
 __global__ void k_nscbc(F* __restrict__ dQ, const F* __restrict__ prim, const F* __restrict__ g,
                         const F* __restrict__ gty, int ngty, const F* __restrict__ dpd, const F* __restrict__ dpt0,
                         const F* __restrict__ dpt1, const F* __restrict__ drd, Grid3 gr, int d, int side, int Ns,
-                        PhysConst pc, NscbcParams bp) {
+                        PhysConst pc, NscbcParams bp, const double* __restrict__ tgt) {
     const int o1 = d == 0 ? 1 : 0, o2 = d == 2 ? 1 : 2;
     const int64_t plane = (int64_t)gr.n[o1] * gr.n[o2];
     const int64_t cells = (int64_t)gr.n[0] * gr.n[1] * gr.n[2];
@@ -756,21 +762,27 @@ __global__ void k_nscbc(F* __restrict__ dQ, const F* __restrict__ prim, const F*
             const double L1c = (un - c) * (dpn - rho * c * dun);
             const double L5c = (un + c) * (dpn + rho * c * dun);
             const double L2c = un * (c * c * drn - dpn);
-            const double rel = bp.eta_u * rho * c * c * (1 - Ma * Ma) / bp.Lref * (un - bp.u[d]);
+            double uT[3] = {bp.u[0], bp.u[1], bp.u[2]}, TT = bp.T;
+            if (tgt) {
+                for (int aa = 0; aa < 3; ++aa) uT[aa] = tgt[aa * plane + q];
+                TT = tgt[3 * plane + q];
+            }
+            auto YT = [&](int k) { return tgt ? tgt[(4 + k) * plane + q] : bp.Y[k]; };
+            const double rel = bp.eta_u * rho * c * c * (1 - Ma * Ma) / bp.Lref * (un - uT[d]);
             const double dL1 = low ? 0.0 : (-rel - L1c);
             const double dL5 = low ? (rel - L5c) : 0.0;
-            const double dL2 = bp.eta_T * rho * (c * c * c) * (bp.T - Tp) / (bp.Lref * Tp) - L2c;
+            const double dL2 = bp.eta_T * rho * (c * c * c) * (TT - Tp) / (bp.Lref * Tp) - L2c;
             const double d1 = dL2 / (c * c) + (dL5 + dL1) / (2 * c * c);
             const double d2 = (dL5 + dL1) / 2;
             const double d3 = (dL5 - dL1) / (2 * rho * c);
-            const double d4 = bp.eta_t * K * (uv[t1] - bp.u[t1]) - un * G(d, t1);
-            const double d5 = bp.eta_t * K * (uv[t2] - bp.u[t2]) - un * G(d, t2);
+            const double d4 = bp.eta_t * K * (uv[t1] - uT[t1]) - un * G(d, t1);
+            const double d5 = bp.eta_t * K * (uv[t2] - uT[t2]) - un * G(d, t2);
             const double cvm = cpm - Rm;
             double sphiY = 0.0;
             for (int k = 0; k < Ns; ++k) {
                 const double Yk = P(P_Y0 + k);
                 const double gY = ngty > 1 ? double(gty[I + cells * (d * ngty + 1 + k)]) : 0.0;
-                const double dLs = bp.eta_Y * K * (Yk - bp.Y[k]) - un * gY;
+                const double dLs = bp.eta_Y * K * (Yk - YT(k)) - un * gY;
                 dQ[I + cells * k] = F(double(dQ[I + cells * k]) - (Yk * d1 + rho * dLs));
                 // eos_dphi_dY (src/physics.jl:147-152, 462-470)
                 const double cvk = N9 ? n9_cp(pc, k, Tp) - pc.Rk[k] : pc.cvk[k];
@@ -996,10 +1008,11 @@ void Pointwise<F>::to_double(const F* a, double* b, int64_t n, cudaStream_t st) 
     LAUNCH(k_to_double<F>, n, st, a, b, n);
 }
 
-void bc_plane(double* Q, const Grid3& g, int d, int side, int Ns, int kind, const BcState& s, cudaStream_t st) {
+void bc_plane(double* Q, const Grid3& g, int d, int side, int Ns, int kind, const BcState& s, cudaStream_t st,
+              const double* qface) {
     const int o1 = d == 0 ? 1 : 0, o2 = d == 2 ? 1 : 2;
     const int64_t plane = (int64_t)g.n[o1] * g.n[o2];
-    k_bc_plane<<<grid_for(plane), kThreads, 0, st>>>(Q, g, d, side, Ns, kind, s);
+    k_bc_plane<<<grid_for(plane), kThreads, 0, st>>>(Q, g, d, side, Ns, kind, s, qface);
     count_launch();
     check_launch("k_bc_plane");
 }
@@ -1007,15 +1020,15 @@ void bc_plane(double* Q, const Grid3& g, int d, int side, int Ns, int kind, cons
 template <typename F>
 void Pointwise<F>::nscbc(F* dQ, const F* prim, const F* g, const F* gty, int ngty, const F* dpd, const F* dpt0,
                          const F* dpt1, const F* drd, const Grid3& gr, int d, int side, int Ns, const PhysConst& pc,
-                         const NscbcParams& bp, cudaStream_t st) {
+                         const NscbcParams& bp, cudaStream_t st, const double* tgt) {
     const int o1 = d == 0 ? 1 : 0, o2 = d == 2 ? 1 : 2;
     const int64_t plane = (int64_t)gr.n[o1] * gr.n[o2];
     if (pc.eos == CLES_EOS_NASA9)
         k_nscbc<F, true><<<grid_for(plane), kThreads, 0, st>>>(dQ, prim, g, gty, ngty, dpd, dpt0, dpt1, drd, gr, d, side,
-                                                               Ns, pc, bp);
+                                                               Ns, pc, bp, tgt);
     else
         k_nscbc<F, false><<<grid_for(plane), kThreads, 0, st>>>(dQ, prim, g, gty, ngty, dpd, dpt0, dpt1, drd, gr, d,
-                                                                side, Ns, pc, bp);
+                                                                side, Ns, pc, bp, tgt);
     count_launch();
     check_launch("k_nscbc");
 }

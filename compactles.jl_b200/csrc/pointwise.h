@@ -124,7 +124,7 @@ struct Pointwise {
     // [dT, dY_k] per dimension (ngty fields each).
     static void nscbc(F* dQ, const F* prim, const F* g, const F* gty, int ngty, const F* dpd, const F* dpt0,
                       const F* dpt1, const F* drd, const Grid3& gr, int d, int side, int Ns, const PhysConst& pc,
-                      const NscbcParams& bp, cudaStream_t st);
+                      const NscbcParams& bp, cudaStream_t st, const double* tgt = nullptr);
     // fluxes with each direction's flux multiplied by its area factor A_d
     // (the A_d F_d product of src/rhs.jl:670-675), for curvilinear / stretched grids
     static void fluxes_geo(const double* Q, const F* prim, const F* g, const F* gty, const F* art, F* flux,
@@ -207,7 +207,9 @@ void geo_gcl(double* cotr, const double* dA, const Geom& G, cudaStream_t st);
 // k_rate_final of pointwise.cu: reduce nb (rate, rho_min) partials
 void rate_final(const double* part, int nb, double* out, cudaStream_t st);
 
-void bc_plane(double* Q, const Grid3& g, int d, int side, int Ns, int kind, const BcState& s, cudaStream_t st);
+// qface: per-node conserved state ([c][plane]) of a DirichletBC(fun) face, else null
+void bc_plane(double* Q, const Grid3& g, int d, int side, int Ns, int kind, const BcState& s, cudaStream_t st,
+              const double* qface = nullptr);
 // Interior of one padded field (extents n + 2 pad, x fastest) into the interior layout.
 void gather_interior(const double* padded, double* interior, const int n[3], const int pad[3], cudaStream_t st);
 

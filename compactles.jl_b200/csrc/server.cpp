@@ -23,6 +23,7 @@ namespace {
 struct Request {
     int64_t id = 0;
     cles_solver_desc desc{};
+    std::vector<double> stretch[3][2];   // owned copies of the descriptor's Stretch samples
     std::vector<double> Q0;
     int layout = CLES_LAYOUT_PADDED;
     double tfinal = 0.0;
@@ -121,6 +122,15 @@ int cles_server_submit(cles_server* s, const cles_solver_desc* desc, const doubl
     auto r = std::make_unique<Request>();
     r->id = s->next_id++;
     r->desc = *desc;
+    // the solver is created at admission, after the caller's arrays may be gone
+    for (int k = 0; k < 3; ++k)
+        if (desc->stretch_x[k] && desc->stretch_dxdxi[k]) {
+            const int n = desc->n_global[k];
+            r->stretch[k][0].assign(desc->stretch_x[k], desc->stretch_x[k] + n);
+            r->stretch[k][1].assign(desc->stretch_dxdxi[k], desc->stretch_dxdxi[k] + n);
+            r->desc.stretch_x[k] = r->stretch[k][0].data();
+            r->desc.stretch_dxdxi[k] = r->stretch[k][1].data();
+        }
     r->layout = layout;
     r->tfinal = tfinal;
     r->nmax = nmax;

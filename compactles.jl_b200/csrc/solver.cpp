@@ -173,6 +173,8 @@ public:
         CLES_CUDA(cudaMemsetAsync(flux_.p, 0, flux_.bytes, st_));
         if (d.control.retries > 0) save_.alloc(ctx, sizeof(double) * c * ncons_);
         if (geo_) build_geometry_tables(d);
+        // the Stretch samples are read at create time only (kept in stretch_x_)
+        for (int k = 0; k < 3; ++k) desc.stretch_x[k] = desc.stretch_dxdxi[k] = nullptr;
         CLES_CUDA(cudaStreamSynchronize(st_));
     }
 
@@ -197,6 +199,7 @@ public:
             if (str[k] != (d.stretch_dxdxi[k] != nullptr))
                 throw Error(CLES_EINVAL, "a Stretch needs both x and dx/dxi samples");
             stretched_[k] = str[k];
+            if (str[k]) stretch_x_[k].assign(d.stretch_x[k], d.stretch_x[k] + d.n_global[k]);
         }
         geo_ = d.metric != CLES_METRIC_CARTESIAN || str[0] || str[1] || str[2];
         for (int k = 0; k < 3; ++k)
@@ -464,6 +467,62 @@ public:
     const double* face_state(int k, int s) const {
         return desc.bc_switchable[k][s] && switched_[k][s] ? desc.bc_after_state[k][s] : desc.bc_state[k][s];
     }
+    // a DirichletBC(fun) / NSCBCInflowBC(target = fun) face function and the
+    // face's node coordinates
+    struct FaceFn {
+        cles_face_fn fn = nullptr;
+        void* user = nullptr;
+        std::vector<double> x[3];
+    };
+    // the face function of the condition face (k, s) acts as now, if any
+    const FaceFn& face_fn(int k, int s) const {
+        return face_fn_[k][s][desc.bc_switchable[k][s] && switched_[k][s] ? 1 : 0];
+    }
+    void set_face_fn(int k, int s, int which, cles_face_fn fn, void* user) override {
+        if (k < 0 || k > 2 || s < 0 || s > 1 || which < 0 || which > 1) throw Error(CLES_EINVAL, "no such face");
+        if (which == 1 && !desc.bc_switchable[k][s]) throw Error(CLES_EINVAL, "face is not a SwitchableBC");
+        const int bc = which == 0 ? desc.bc[k][s] : desc.bc_after[k][s];
+        if (fn && bc != CLES_BC_DIRICHLET && bc != CLES_BC_NSCBC_INFLOW)
+            throw Error(CLES_EINVAL, "only DirichletBC and NSCBCInflowBC faces take a function");
+        FaceFn& f = face_fn_[k][s][which];
+        f.fn = fn;
+        f.user = user;
+        if (fn && f.x[0].empty()) {
+            // node coordinates of the face in plane order (xcoord, src/rhs.jl:320-335)
+            const int o1 = k == 0 ? 1 : 0, o2 = k == 2 ? 1 : 2;
+            const int64_t np = (int64_t)g_.n[o1] * g_.n[o2];
+            for (int e = 0; e < 3; ++e) f.x[e].resize((size_t)np);
+            for (int64_t t = 0; t < np; ++t) {
+                int c[3];
+                c[o1] = (int)(t % g_.n[o1]);
+                c[o2] = (int)(t / g_.n[o1]);
+                c[k] = s == 0 ? 0 : g_.n[k] - 1;
+                for (int e = 0; e < 3; ++e) f.x[e][(size_t)t] = node_coord(e, c[e]);
+            }
+        }
+    }
+    // physical coordinate of interior node i along e (global_xcoord, src/rhs.jl:331-335)
+    double node_coord(int e, int i) const {
+        return stretched_[e] ? stretch_x_[e][(size_t)i] : orig_[e] + shift_[e] + (double)i * h_[e];
+    }
+    // Evaluate a face function at the stage time into the device face buffer;
+    // returns the device pointer ([values][plane]).
+    const double* eval_face_fn(int k, int s, int nvals) {
+        const FaceFn& f = face_fn(k, s);
+        const int64_t np = (int64_t)f.x[0].size();
+        face_host_.assign((size_t)(np * nvals), std::numeric_limits<double>::quiet_NaN());
+        f.fn(f.user, k, s, tstage, np, f.x[0].data(), f.x[1].data(), f.x[2].data(), face_host_.data());
+        const size_t bytes = sizeof(double) * face_host_.size();
+        if (face_dev_.bytes < bytes) {
+            CLES_CUDA(cudaStreamSynchronize(st_));
+            face_dev_.release();
+            face_dev_.alloc(ctx_, bytes);
+        }
+        // pageable source: the call returns once the data is staged, so the
+        // host buffer may be refilled by the next evaluation
+        CLES_CUDA(cudaMemcpyAsync(face_dev_.p, face_host_.data(), bytes, cudaMemcpyHostToDevice, st_));
+        return face_dev_.as<double>();
+    }
     bool any_nscbc() const {
         for (int k = 0; k < 3; ++k)
             for (int s = 0; s < 2; ++s)
@@ -502,7 +561,9 @@ public:
                         for (int sp = 0; sp < Ns_; ++sp)
                             bs.ew[sp] = desc.eos == CLES_EOS_IDEAL ? pc_.cvk[sp] : nasa9_species_energy(desc, sp, Tw);
                 }
-                bc_plane(Q_.as<double>(), g_, k, s, Ns_, bc, bs, st_);
+                const double* qface = nullptr;
+                if (bc == CLES_BC_DIRICHLET && face_fn(k, s).fn) qface = eval_face_fn(k, s, ncons_);
+                bc_plane(Q_.as<double>(), g_, k, s, Ns_, bc, bs, st_, qface);
             }
         }
     }
@@ -542,8 +603,10 @@ public:
                     drd = dt0;
                     launch_compact(*dset_[k][0], view(prim(P_RHO)), view(drd), 1, OUT_STORE, st_);
                 }
+                const double* tgt = nullptr;
+                if (bc == CLES_BC_NSCBC_INFLOW && face_fn(k, s).fn) tgt = eval_face_fn(k, s, 4 + Ns_);
                 Pointwise<F>::nscbc(dQ_.as<F>(), prim_.as<F>(), g_u_.as<F>(), gty_.as<F>(), Ns_ == 1 ? 1 : 1 + Ns_, dpd,
-                                    dt0, dt1, drd, g_, k, s, Ns_, pc_, np, st_);
+                                    dt0, dt1, drd, g_, k, s, Ns_, pc_, np, st_, tgt);
             }
         }
     }
@@ -917,6 +980,11 @@ public:
     }
 
     void graph_begin(double tfinal, int64_t nmax) override {
+        for (int k = 0; k < 3; ++k)
+            for (int s = 0; s < 2; ++s)
+                for (int w = 0; w < 2; ++w)
+                    if (face_fn_[k][s][w].fn)
+                        throw Error(CLES_EINVAL, "graph mode cannot call a boundary face function at the stage times");
         const cles_step_control& c = desc.control;
         if (c.predict > 0 || c.max_growth > 0)
             throw Error(CLES_EINVAL, "graph mode supports neither rate prediction nor growth capping");
@@ -995,6 +1063,10 @@ private:
         int sigflux[CLES_MAX_SPECIES + 4] = {};
         int sigcons[CLES_MAX_SPECIES + 4] = {};
     };
+    FaceFn face_fn_[3][2][2];
+    std::vector<double> face_host_;
+    DevBuf face_dev_;
+    std::vector<double> stretch_x_[3];
     bool geo_ = false, folded_ = false;
     bool stretched_[3] = {false, false, false};
     double shift_[3]{}, orig_[3]{};

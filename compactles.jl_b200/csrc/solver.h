@@ -61,6 +61,7 @@ public:
     virtual cudaStream_t stream() const = 0;
     // switch!(::SwitchableBC) on face (dim, side)
     virtual void switch_bc(int dim, int side) = 0;
+    virtual void set_face_fn(int dim, int side, int which, cles_face_fn fn, void* user) = 0;
     virtual bool bc_switched(int dim, int side) const = 0;
 
     cles_solver_desc desc{};

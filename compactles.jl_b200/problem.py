@@ -104,12 +104,15 @@ class SlipWallBC(BoundaryCondition):
 
 
 class DirichletBC(BoundaryCondition):
-    """DirichletBC with a state constant in time: `state` is a Prim (scalar
-    fields) imposed on every node of the face after each stage."""
+    """DirichletBC(fun) (src/problem.jl:174-207): the full state imposed on the
+    face after each stage.  `state` is either a Prim with scalar fields
+    (constant) or a function fun(x, y, z, t) -> Prim evaluated at the stage
+    time on the face's node coordinates (numpy arrays)."""
     code = abi.CLES_BC_DIRICHLET
 
     def __init__(self, state):
-        self.state = state
+        self.fun = state if callable(state) else None
+        self.state = None if callable(state) else state
 
 
 class NoSlipWallBC(BoundaryCondition):
@@ -139,7 +142,10 @@ class NSCBCInflowBC(BoundaryCondition):
     (src/nscbc.jl:178-218), constant targets."""
     code = abi.CLES_BC_NSCBC_INFLOW
 
-    def __init__(self, u, T_ion, Y=(1.0,), eta_u=0.28, eta_T=0.28, eta_t=0.28, eta_Y=0.28, Lref=0.0):
+    def __init__(self, u, T_ion, Y=(1.0,), eta_u=0.28, eta_T=0.28, eta_t=0.28, eta_Y=0.28, Lref=0.0, target=None):
+        # target: optional fun(x, y, z, t) -> Prim overriding the constants per
+        # node at the stage time; its Prim must carry T_ion and the full Y
+        self.target = target
         self.u = tuple(float(v) for v in u)
         self.T_ion = float(T_ion)
         self.Y = tuple(float(v) for v in Y)
@@ -233,9 +239,10 @@ def _fill_face(bc, eos, ncons, params, state):
     p.sigma, p.beta_t = 0.25, -1.0
     p.eta_u = p.eta_T = p.eta_t = p.eta_Y = 0.28
     if bc.code == abi.CLES_BC_DIRICHLET:
-        q = conserved_from_prim(eos, bc.state)
-        for c in range(ncons):
-            state[c] = float(np.asarray(q[c]))
+        if bc.state is not None:
+            q = conserved_from_prim(eos, bc.state)
+            for c in range(ncons):
+                state[c] = float(np.asarray(q[c]))
     elif bc.code == abi.CLES_BC_NOSLIP_WALL:
         p.Twall = bc.Twall
     elif bc.code == abi.CLES_BC_NSCBC_OUTFLOW:
@@ -355,6 +362,7 @@ def solver_desc(n_global, L_domain, bcs, deriv, filt, eos=None, transport=None, 
         raise ValueError(f"art.beta_sensor must be :strain, :gated_strain or :dilatation, got :{art.beta_sensor}")
     d = abi.cles_solver_desc()
     ncons = eos.nspecies + 4
+    face_fns = []
     for k in range(3):
         d.n_global[k] = int(n_global[k])
         d.L[k] = float(L_domain[k])
@@ -369,8 +377,14 @@ def solver_desc(n_global, L_domain, bcs, deriv, filt, eos=None, transport=None, 
                 d.bc[k][s] = _fill_face(bc.before, eos, ncons, d.bc_params[k][s], d.bc_state[k][s])
                 d.bc_switchable[k][s] = 1
                 d.bc_after[k][s] = _fill_face(bc.after, eos, ncons, d.bc_after_params[k][s], d.bc_after_state[k][s])
+                faces = ((0, bc.before), (1, bc.after))
             else:
                 d.bc[k][s] = _fill_face(bc, eos, ncons, d.bc_params[k][s], d.bc_state[k][s])
+                faces = ((0, bc),)
+            for which, b in faces:
+                fn = getattr(b, "fun", None) if b.code == abi.CLES_BC_DIRICHLET else getattr(b, "target", None)
+                if fn is not None:
+                    face_fns.append((k, s, which, b.code, fn))
     if eos.nspecies > abi.CLES_MAX_SPECIES:
         raise ValueError("too many species")
     d.n_species = eos.nspecies
@@ -409,7 +423,42 @@ def solver_desc(n_global, L_domain, bcs, deriv, filt, eos=None, transport=None, 
         d.stretch_x[k] = xs.ctypes.data_as(C.POINTER(C.c_double))
         d.stretch_dxdxi[k] = ms.ctypes.data_as(C.POINTER(C.c_double))
     d._stretch_keep = keep
+    d._face_fns = face_fns
+    d._eos = eos
     return d
+
+
+def face_callbacks(desc):
+    """ctypes callbacks (cles_face_fn) for the function-valued faces of a
+    descriptor built by solver_desc: [(dim, side, which, callback)].  A
+    Dirichlet face writes conserved_from_prim of fun(x, y, z, t); an NSCBC
+    inflow face writes the target velocity, temperature and composition.
+    An exception inside a function fills its face with NaN and is kept in
+    `errors` (the run then fails as non-finite)."""
+    out, errors = [], []
+    eos = getattr(desc, "_eos", None) or eos_from_desc(desc)
+    for k, s, which, code, fn in getattr(desc, "_face_fns", []):
+        def cb(user, dim, side, t, npts, x1, x2, x3, o, fn=fn, code=code):
+            n = int(npts)
+            X = [np.ctypeslib.as_array(x, shape=(n,)) for x in (x1, x2, x3)]
+            dst = np.ctypeslib.as_array(o, shape=((eos.nspecies + 4), n))
+            try:
+                pr = fn(X[0], X[1], X[2], float(t))
+                if code == abi.CLES_BC_DIRICHLET:
+                    vals = conserved_from_prim(eos, pr)
+                else:
+                    if pr.T_ion is None:
+                        raise ValueError("NSCBCInflowBC target must specify T_ion")
+                    if len(pr.Y) != eos.nspecies:
+                        raise ValueError("NSCBCInflowBC target must carry the full composition")
+                    vals = list(pr.u) + [pr.T_ion] + list(pr.Y)
+                for c, v in enumerate(vals):
+                    dst[c, :] = np.broadcast_to(np.asarray(v, dtype=np.float64), (n,))
+            except Exception as e:   # noqa: BLE001 - reported through `errors`
+                errors.append(e)
+                dst[...] = np.nan
+        out.append((k, s, which, abi.FACE_FN(cb)))
+    return out, errors
 
 
 def _folds(desc):

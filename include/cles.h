@@ -343,6 +343,23 @@ int  cles_set_clock(cles_solver* s, double t, int64_t step, double cfl);
  * 0 low / 1 high): from now on the face acts as its `after` condition
  * (idempotent; CLES_EINVAL if the face is not switchable). */
 int  cles_solver_switch_bc(cles_solver* s, int dim, int side);
+
+/* Face conditions given as functions of position and time: DirichletBC(fun)
+ * (src/problem.jl:180-207) and NSCBCInflowBC(target = fun) (src/nscbc.jl:
+ * 178-307).  The library calls fn on the host at the RK stage time at which
+ * the reference evaluates them (each apply_bcs! for a Dirichlet face, each
+ * correct_rhs! for an inflow face), for the npts nodes of face (dim 0..2,
+ * side 0 low / 1 high) in plane order (the lower-numbered transverse
+ * dimension fastest), with their physical coordinates x1, x2, x3.  fn fills
+ *   a CLES_BC_DIRICHLET face:     out[c * npts + p] = conserved component c;
+ *   a CLES_BC_NSCBC_INFLOW face:  out[a * npts + p], a = 0..2 target velocity,
+ *                                 3 target temperature, 4 + k target Y_k.
+ * which = 0 sets the face's condition, 1 the `after` condition of a
+ * SwitchableBC; fn = NULL returns to the descriptor's constants.  A solver
+ * with a face function does not run in graph mode (CLES_EINVAL). */
+typedef void (*cles_face_fn)(void* user, int dim, int side, double t, int64_t npts, const double* x1,
+                             const double* x2, const double* x3, double* out);
+int  cles_solver_set_face_fn(cles_solver* s, int dim, int side, int which, cles_face_fn fn, void* user);
 int  cles_solver_bc_switched(const cles_solver* s, int dim, int side, int* switched);
 
 int  cles_checkpoint_save(cles_solver* s, const char* prefix);

@@ -703,6 +703,9 @@ struct Solver {
     double t = 0.0, tstage = 0.0, dt_prev = 0.0, rate_prev = 0.0, cfl = 0.5;
     int64_t step = 0;
     bool switched[3][2] = {{false, false}, {false, false}, {false, false}};   // SwitchableBC state
+    // DirichletBC(fun) / NSCBCInflowBC(target = fun): [dim][side][before/after]
+    cles_face_fn ffn[3][2][2] = {};
+    void* fuser[3][2][2] = {};
 
     // the condition a face acts as now (src/boundary.jl:170-183)
     int face_kind(int d, int s) const {
@@ -715,6 +718,11 @@ struct Solver {
         return desc.bc_switchable[d][s] && switched[d][s] ? desc.bc_after_state[d][s] : desc.bc_state[d][s];
     }
 
+    cles_face_fn face_fn(int d, int s, void** user) const {
+        const int w = desc.bc_switchable[d][s] && switched[d][s] ? 1 : 0;
+        *user = fuser[d][s][w];
+        return ffn[d][s][w];
+    }
     double* comp(std::vector<double>& A, int cidx) { return A.data() + fs * cidx; }
     double* vel(int j) { return j == 0 ? u.data() : j == 1 ? v.data() : w.data(); }
 };
@@ -1310,6 +1318,33 @@ void assemble_fluxes(Solver& S) {
     });
 }
 
+// Physical coordinate of interior node i along e (global_xcoord, src/rhs.jl:331-335).
+double node_coord(const Solver& S, int e, int i) {
+    if (S.stretched[e]) return S.st_x[e][(size_t)i];
+    return S.orig[e] + S.coord_shift[e] + (double)i * S.h[e];
+}
+
+// A face function evaluated at the stage time for the nodes of face (d, side)
+// in wall-plane order: nvals values per node, [value][node].
+std::vector<double> eval_face(const Solver& S, int d, int side, int nvals) {
+    void* user = nullptr;
+    const cles_face_fn fn = S.face_fn(d, side, &user);
+    const int o1 = d == 0 ? 1 : 0, o2 = d == 2 ? 1 : 2;
+    const int64_t np = (int64_t)S.D.nl[o1] * S.D.nl[o2];
+    std::vector<double> x[3];
+    for (int e = 0; e < 3; ++e) x[e].resize((size_t)np);
+    for (int64_t t = 0; t < np; ++t) {
+        int c[3];
+        c[o1] = (int)(t % S.D.nl[o1]);
+        c[o2] = (int)(t / S.D.nl[o1]);
+        c[d] = side == 0 ? 0 : S.D.nl[d] - 1;
+        for (int e = 0; e < 3; ++e) x[e][(size_t)t] = node_coord(S, e, c[e]);
+    }
+    std::vector<double> out((size_t)(np * nvals), std::numeric_limits<double>::quiet_NaN());
+    fn(user, d, side, S.tstage, np, x[0].data(), x[1].data(), x[2].data(), out.data());
+    return out;
+}
+
 // Visit the interior points of the wall plane of (d, side).
 template <class Fn>
 void for_wallplane(const Decomp& D, int d, int side, Fn&& fn) {
@@ -1375,9 +1410,17 @@ void nscbc_outflow(Solver& S, int d, int side) {
     });
 }
 
-// correct_rhs!(::NSCBCInflowBC) with constant targets (src/nscbc.jl:220-307)
+// correct_rhs!(::NSCBCInflowBC) (src/nscbc.jl:220-307): constant targets, or
+// the stage-time values of the target function per node
 void nscbc_inflow(Solver& S, int d, int side) {
     const cles_bc_params& bc = S.face_params(d, side);
+    void* fu = nullptr;
+    std::vector<double> tv;
+    int64_t tnp = 0, tp = 0;
+    if (S.face_fn(d, side, &fu)) {
+        tv = eval_face(S, d, side, 4 + S.Ns);
+        tnp = (int64_t)(tv.size() / (4 + S.Ns));
+    }
     deriv_along(S, S.tmp_a.data(), S.p.data(), d);
     deriv_along(S, S.tmp_b.data(), S.rho.data(), d);
     const double Lref = bc.Lref > 0 ? bc.Lref : S.desc.L[d];
@@ -1385,6 +1428,14 @@ void nscbc_inflow(Solver& S, int d, int side) {
     const size_t fs = S.fs;
     const bool low = side == 0;
     for_wallplane(S.D, d, side, [&](size_t I) {
+        const int64_t q = tp++;
+        double uT[3] = {bc.u[0], bc.u[1], bc.u[2]}, TT = bc.T_ion, YT[CLES_MAX_SPECIES];
+        for (int k = 0; k < S.Ns; ++k) YT[k] = bc.Y[k];
+        if (tnp) {
+            for (int a = 0; a < 3; ++a) uT[a] = tv[(size_t)(a * tnp + q)];
+            TT = tv[(size_t)(3 * tnp + q)];
+            for (int k = 0; k < S.Ns; ++k) YT[k] = tv[(size_t)((4 + k) * tnp + q)];
+        }
         const double rho = S.rho[I], c = S.c[I], p = S.p[I], Tp = S.T[I];
         const double uv[3] = {S.u[I], S.v[I], S.w[I]};
         const double un = uv[d];
@@ -1395,21 +1446,21 @@ void nscbc_inflow(Solver& S, int d, int side) {
         const double L1c = (un - c) * (dpn - rho * c * dun);
         const double L5c = (un + c) * (dpn + rho * c * dun);
         const double L2c = un * (c * c * drn - dpn);
-        const double rel = bc.eta_u * rho * c * c * (1 - Ma * Ma) / Lref * (un - bc.u[d]);
+        const double rel = bc.eta_u * rho * c * c * (1 - Ma * Ma) / Lref * (un - uT[d]);
         const double dL1 = low ? 0.0 : (-rel - L1c);
         const double dL5 = low ? (rel - L5c) : 0.0;
-        const double dL2 = bc.eta_T * rho * (c * c * c) * (bc.T_ion - Tp) / (Lref * Tp) - L2c;
+        const double dL2 = bc.eta_T * rho * (c * c * c) * (TT - Tp) / (Lref * Tp) - L2c;
         const double d1 = dL2 / (c * c) + (dL5 + dL1) / (2 * c * c);
         const double d2 = (dL5 + dL1) / 2;
         const double d3 = (dL5 - dL1) / (2 * rho * c);
-        const double d4 = bc.eta_t * K * (uv[t1] - bc.u[t1]) - un * S.grad_u[d][t1][I];
-        const double d5 = bc.eta_t * K * (uv[t2] - bc.u[t2]) - un * S.grad_u[d][t2][I];
+        const double d4 = bc.eta_t * K * (uv[t1] - uT[t1]) - un * S.grad_u[d][t1][I];
+        const double d5 = bc.eta_t * K * (uv[t2] - uT[t2]) - un * S.grad_u[d][t2][I];
         const double cpm = S.cp[I];
         const double phi = eos_phi(rho, p, Tp, cpm);
         const double ke = 0.5 * (uv[0] * uv[0] + uv[1] * uv[1] + uv[2] * uv[2]);
         double sphiY = 0.0;
         for (int k = 0; k < S.Ns; ++k) {
-            const double dLs = bc.eta_Y * K * (S.Y[k][I] - bc.Y[k]) - un * S.grad_Y[d][k][I];
+            const double dLs = bc.eta_Y * K * (S.Y[k][I] - YT[k]) - un * S.grad_Y[d][k][I];
             S.dQ[I + fs * k] -= S.Y[k][I] * d1 + rho * dLs;
             sphiY += eos_dphi_dY(S, k, rho, p, Tp, cpm) * dLs;
         }
@@ -1471,8 +1522,8 @@ void compute_rhs(Solver& S, bool primitives_current) {
         }
 }
 
-// enforce! for SlipWallBC (src/boundary.jl:232-243) and a time-constant
-// DirichletBC (src/problem.jl:209-221).
+// enforce! for SlipWallBC (src/boundary.jl:232-243) and DirichletBC, with a
+// constant state or the stage-time state of its function (src/problem.jl:194-207).
 void apply_bcs(Solver& S) {
     const Decomp& D = S.D;
     const size_t fs = S.fs;
@@ -1484,6 +1535,13 @@ void apply_bcs(Solver& S) {
             if (bc == CLES_BC_AXIS || bc == CLES_BC_ORIGIN || bc == CLES_BC_POLE) continue;   // src/boundary.jl:173-175
             const double* bstate = S.face_state(d, side);
             const double Twall = S.face_params(d, side).Twall;
+            void* fu = nullptr;
+            std::vector<double> fvals;
+            int64_t fp = 0, fnp = 0;
+            if (bc == CLES_BC_DIRICHLET && S.face_fn(d, side, &fu)) {
+                fvals = eval_face(S, d, side, S.ncons);
+                fnp = (int64_t)(fvals.size() / S.ncons);
+            }
             int shift[3] = {0, 0, 0};
             shift[d] = side == 0 ? 1 : -1;
             const long sh = (long)D.at(D.nhd[0] + shift[0], D.nhd[1] + shift[1], D.nhd[2] + shift[2]) -
@@ -1504,7 +1562,12 @@ void apply_bcs(Solver& S) {
                             S.Q[I + fs * S.i_energy] -= 0.5 * mn * mn / r;
                             S.Q[I + fs * mc] = 0;
                         } else if (bc == CLES_BC_DIRICHLET) {
-                            for (int cc = 0; cc < S.ncons; ++cc) S.Q[I + fs * cc] = bstate[cc];
+                            if (fnp) {
+                                for (int cc = 0; cc < S.ncons; ++cc) S.Q[I + fs * cc] = fvals[(size_t)(cc * fnp + fp)];
+                                ++fp;
+                            } else {
+                                for (int cc = 0; cc < S.ncons; ++cc) S.Q[I + fs * cc] = bstate[cc];
+                            }
                         } else if (bc == CLES_BC_NOSLIP_WALL) {
                             // enforce!(::NoSlipWallBC) (src/boundary.jl:245-265)
                             double r = 0.0;
@@ -2122,6 +2185,20 @@ int orc_solver_filter(orc_solver* so, double* f, double* out, int d, int sig) {
     if (d < 0 || d > 2 || !S.D.active[d]) { set_err("dimension is collapsed"); return CLES_EINVAL; }
     exchange_halos(S.D, f);
     filt_along(S, out, f, d, sig);
+    return 0;
+}
+
+int orc_solver_set_face_fn(orc_solver* so, int d, int side, int which, cles_face_fn fn, void* user) {
+    Solver& S = *so->s;
+    if (d < 0 || d > 2 || side < 0 || side > 1 || which < 0 || which > 1) { set_err("no such face"); return CLES_EINVAL; }
+    if (which == 1 && !S.desc.bc_switchable[d][side]) { set_err("face is not a SwitchableBC"); return CLES_EINVAL; }
+    const int bc = which == 0 ? S.desc.bc[d][side] : S.desc.bc_after[d][side];
+    if (fn && bc != CLES_BC_DIRICHLET && bc != CLES_BC_NSCBC_INFLOW) {
+        set_err("only DirichletBC and NSCBCInflowBC faces take a function");
+        return CLES_EINVAL;
+    }
+    S.ffn[d][side][which] = fn;
+    S.fuser[d][side][which] = user;
     return 0;
 }
 

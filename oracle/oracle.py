@@ -96,6 +96,7 @@ def lib():
         L.orc_grid_spacing.argtypes = [C.c_void_p, _DP, _DP, _DP]
         L.orc_solver_deriv.argtypes = [C.c_void_p, _DP, _DP, C.c_int, C.c_int, C.c_int]
         L.orc_solver_filter.argtypes = [C.c_void_p, _DP, _DP, C.c_int, C.c_int]
+        L.orc_solver_set_face_fn.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, abi.FACE_FN, C.c_void_p]
         _lib = L
     return _lib
 
@@ -205,6 +206,14 @@ class Solver:
         self.n_cons = desc.n_species + 4
         self.field_shape = padded_shape(self.g)
         self.state_shape = (self.n_cons,) + self.field_shape
+        # function-valued faces, through the package's callback builder when present
+        self._face_cbs, self.face_errors = [], []
+        if getattr(desc, "_face_fns", None):
+            import sys
+            self._face_cbs, self.face_errors = sys.modules["compactles_b200"].problem.face_callbacks(desc)
+        for k, s, which, cb in self._face_cbs:
+            if lib().orc_solver_set_face_fn(self.ptr, k, s, which, cb, None):
+                raise ValueError(_err())
 
     def __del__(self):
         try:
