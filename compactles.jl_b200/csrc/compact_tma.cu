@@ -332,6 +332,40 @@ __device__ __forceinline__ void tg_solve(const TileGenParams& G, T (&y)[MS]) {
     }
 }
 
+// The interface values one segment needs: the previous segment's tails and
+// the next segment's heads, rows of the reduced inverse times the gathered
+// heads and tails.  The 4Q dot products run in one pass over the gathered
+// values with two partial sums each, so their FMA chains overlap instead of
+// running one after the other.  N = 2qS is even.
+template <typename T, int Q>
+__device__ __forceinline__ void tg_interface(const T* Gs, const T* rl, int N, int prev, int next, bool has_prev,
+                                             bool has_next, T (&zp)[Q], T (&zn)[Q]) {
+    const T* gp[Q];
+    const T* gn[Q];
+    T ap[Q][2], an[Q][2];
+#pragma unroll
+    for (int t = 0; t < Q; ++t) {
+        gp[t] = Gs + (size_t)(2 * Q * prev + Q + t) * N;
+        gn[t] = Gs + (size_t)(2 * Q * next + t) * N;
+        ap[t][0] = ap[t][1] = an[t][0] = an[t][1] = T(0);
+    }
+    for (int j = 0; j < N; j += 2) {
+        const T r0 = rl[j], r1 = rl[j + 1];
+#pragma unroll
+        for (int t = 0; t < Q; ++t) {
+            ap[t][0] += gp[t][j] * r0;
+            ap[t][1] += gp[t][j + 1] * r1;
+            an[t][0] += gn[t][j] * r0;
+            an[t][1] += gn[t][j + 1] * r1;
+        }
+    }
+#pragma unroll
+    for (int t = 0; t < Q; ++t) {
+        zp[t] = has_prev ? ap[t][0] + ap[t][1] : T(0);
+        zn[t] = has_next ? an[t][0] + an[t][1] : T(0);
+    }
+}
+
 template <typename T, int Q, int MS, int CLS>
 __device__ __forceinline__ void tg_correct(const TileGenParams& G, T (&y)[MS], const T (&zp)[Q], const T (&zn)[Q]) {
 #pragma unroll
@@ -488,23 +522,7 @@ __global__ void __launch_bounds__(256, 1)
         }
         __syncthreads();
         T zp[Q], zn[Q];
-#pragma unroll
-        for (int t = 0; t < Q; ++t) {
-            zp[t] = T(0);
-            zn[t] = T(0);
-            if (has_prev) {
-                const T* g = Gs + (size_t)(2 * Q * prev + Q + t) * N;
-                T acc = T(0);
-                for (int j = 0; j < N; ++j) acc += g[j] * rl[j];
-                zp[t] = acc;
-            }
-            if (has_next) {
-                const T* g = Gs + (size_t)(2 * Q * next + t) * N;
-                T acc = T(0);
-                for (int j = 0; j < N; ++j) acc += g[j] * rl[j];
-                zn[t] = acc;
-            }
-        }
+        tg_interface<T, Q>(Gs, rl, N, prev, next, has_prev, has_next, zp, zn);
         if (cls == 0) tg_correct<T, Q, MS, 0>(GP, y, zp, zn);
         else if (cls == 1) tg_correct<T, Q, MS, 1>(GP, y, zp, zn);
         else tg_correct<T, Q, MS, 2>(GP, y, zp, zn);
@@ -705,23 +723,7 @@ __global__ void __launch_bounds__(256, 1)
         }
         __syncthreads();   // interface values visible; also the previous group's stores from tout are done
         T zp[Q], zn[Q];
-#pragma unroll
-        for (int t = 0; t < Q; ++t) {
-            zp[t] = T(0);
-            zn[t] = T(0);
-            if (has_prev) {
-                const T* g = Gs + (size_t)(2 * Q * prev + Q + t) * N;
-                T acc = T(0);
-                for (int j = 0; j < N; ++j) acc += g[j] * rl[j];
-                zp[t] = acc;
-            }
-            if (has_next) {
-                const T* g = Gs + (size_t)(2 * Q * next + t) * N;
-                T acc = T(0);
-                for (int j = 0; j < N; ++j) acc += g[j] * rl[j];
-                zn[t] = acc;
-            }
-        }
+        tg_interface<T, Q>(Gs, rl, N, prev, next, has_prev, has_next, zp, zn);
         if (cls == 0) tg_correct<T, Q, MS, 0>(GP, y, zp, zn);
         else if (cls == 1) tg_correct<T, Q, MS, 1>(GP, y, zp, zn);
         else tg_correct<T, Q, MS, 2>(GP, y, zp, zn);

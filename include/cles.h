@@ -63,7 +63,7 @@ extern "C" {
 /* boundary conditions (src/boundary.jl) */
 #define CLES_BC_PERIODIC   0   /* PeriodicBC */
 #define CLES_BC_SLIPWALL   1   /* SlipWallBC, enforce! at src/boundary.jl:232-243 */
-#define CLES_BC_DIRICHLET  2   /* DirichletBC with a state constant in time (src/problem.jl:192-207) */
+#define CLES_BC_DIRICHLET  2   /* DirichletBC: bc_state, or a function of (x, t) via cles_solver_set_face_fn (src/problem.jl:174-207) */
 #define CLES_BC_NOSLIP_WALL     3   /* NoSlipWallBC(Twall), enforce! at src/boundary.jl:245-265 */
 #define CLES_BC_EXTRAPOLATION   4   /* ExtrapolationBC, enforce! at src/boundary.jl:267-278 */
 #define CLES_BC_NSCBC_OUTFLOW   5   /* NSCBCOutflowBC, correct_rhs! at src/nscbc.jl:59-157 */
@@ -217,7 +217,7 @@ typedef struct cles_solver_desc {
     double L[3];                 /* domain extents */
     double origin[3];            /* low corner */
     int    bc[3][2];             /* CLES_BC_* per (dim, side) */
-    /* conserved state imposed on a CLES_BC_DIRICHLET face (constant in time) */
+    /* conserved state imposed on a CLES_BC_DIRICHLET face without a face function */
     double bc_state[3][2][CLES_MAX_SPECIES + 4];
     cles_bc_params bc_params[3][2];
     /* SwitchableBC(before, after) (src/boundary.jl:120-177): a face with
