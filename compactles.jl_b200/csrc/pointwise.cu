@@ -709,7 +709,7 @@ template <typename F, bool N9>
 __global__ void k_nscbc(F* __restrict__ dQ, const F* __restrict__ prim, const F* __restrict__ g,
                         const F* __restrict__ gty, int ngty, const F* __restrict__ dpd, const F* __restrict__ dpt0,
                         const F* __restrict__ dpt1, const F* __restrict__ drd, Grid3 gr, int d, int side, int Ns,
-                        PhysConst pc, NscbcParams bp, const double* __restrict__ tgt) {
+                        PhysConst pc, NscbcParams bp, const double* __restrict__ tgt, Geom Gm, int geo) {
     const int o1 = d == 0 ? 1 : 0, o2 = d == 2 ? 1 : 2;
     const int64_t plane = (int64_t)gr.n[o1] * gr.n[o2];
     const int64_t cells = (int64_t)gr.n[0] * gr.n[1] * gr.n[2];
@@ -726,7 +726,18 @@ __global__ void k_nscbc(F* __restrict__ dQ, const F* __restrict__ prim, const F*
         const double un = uv[d];
         const double Ma = fabs(un) / c;
         if (!(Ma < 1)) continue;   // supersonic: no correction
-        const double dpn = double(dpd[I]);
+        // physical derivatives: 1/h of the normal and transverse dims
+        // (1 on a uniform Cartesian grid; src/nscbc.jl:108, :125-130, :257)
+        double ihd = 1.0, iht1 = 1.0, iht2 = 1.0;
+        if (geo) {
+            int ci, cj, ck;
+            cell_ijk(I, gr.n, ci, cj, ck);
+            const GeoPoint gp = geo_point(Gm, ci, cj, ck, I);
+            ihd = gp.inv_h[d];
+            iht1 = gp.inv_h[t1];
+            iht2 = gp.inv_h[t2];
+        }
+        const double dpn = geo ? ihd * double(dpd[I]) : double(dpd[I]);
         const double dun = G(d, d);
         const double Rm = p / (rho * Tp);
         const double phi = cpm / Rm - 1;   // eos_phi, either mixture (src/physics.jl:142-145, 457-460)
@@ -738,11 +749,11 @@ __global__ void k_nscbc(F* __restrict__ dQ, const F* __restrict__ prim, const F*
             double tin = 0.0;
             if (bp.act[t1]) {
                 const double ut = uv[t1];
-                tin += ut * double(dpt0[I]) + rho * c * c * G(t1, t1) + sgn * rho * c * ut * G(t1, d);
+                tin += ut * iht1 * double(dpt0[I]) + rho * c * c * G(t1, t1) + sgn * rho * c * ut * G(t1, d);
             }
             if (bp.act[t2]) {
                 const double ut = uv[t2];
-                tin += ut * double(dpt1[I]) + rho * c * c * G(t2, t2) + sgn * rho * c * ut * G(t2, d);
+                tin += ut * iht2 * double(dpt1[I]) + rho * c * c * G(t2, t2) + sgn * rho * c * ut * G(t2, d);
             }
             const double bt = bp.beta_t < 0 ? Ma : bp.beta_t;
             const double K = bp.sigma * (1 - Ma * Ma) * c / bp.Lref;
@@ -757,7 +768,7 @@ __global__ void k_nscbc(F* __restrict__ dQ, const F* __restrict__ prim, const F*
             dQ[I + cells * ie] = F(double(dQ[I + cells * ie]) - (ke * d1 + phi * d2 + rho * un * d3));
         } else {
             const bool low = side == 0;
-            const double drn = double(drd[I]);
+            const double drn = geo ? ihd * double(drd[I]) : double(drd[I]);
             const double K = c / bp.Lref;
             const double L1c = (un - c) * (dpn - rho * c * dun);
             const double L5c = (un + c) * (dpn + rho * c * dun);
@@ -1020,15 +1031,17 @@ void bc_plane(double* Q, const Grid3& g, int d, int side, int Ns, int kind, cons
 template <typename F>
 void Pointwise<F>::nscbc(F* dQ, const F* prim, const F* g, const F* gty, int ngty, const F* dpd, const F* dpt0,
                          const F* dpt1, const F* drd, const Grid3& gr, int d, int side, int Ns, const PhysConst& pc,
-                         const NscbcParams& bp, cudaStream_t st, const double* tgt) {
+                         const NscbcParams& bp, cudaStream_t st, const double* tgt, const Geom* G) {
+    const Geom G0 = G ? *G : Geom{};
+    const int geo = G ? 1 : 0;
     const int o1 = d == 0 ? 1 : 0, o2 = d == 2 ? 1 : 2;
     const int64_t plane = (int64_t)gr.n[o1] * gr.n[o2];
     if (pc.eos == CLES_EOS_NASA9)
         k_nscbc<F, true><<<grid_for(plane), kThreads, 0, st>>>(dQ, prim, g, gty, ngty, dpd, dpt0, dpt1, drd, gr, d, side,
-                                                               Ns, pc, bp, tgt);
+                                                               Ns, pc, bp, tgt, G0, geo);
     else
         k_nscbc<F, false><<<grid_for(plane), kThreads, 0, st>>>(dQ, prim, g, gty, ngty, dpd, dpt0, dpt1, drd, gr, d,
-                                                                side, Ns, pc, bp, tgt);
+                                                                side, Ns, pc, bp, tgt, G0, geo);
     count_launch();
     check_launch("k_nscbc");
 }

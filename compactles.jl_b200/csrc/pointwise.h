@@ -124,7 +124,8 @@ struct Pointwise {
     // [dT, dY_k] per dimension (ngty fields each).
     static void nscbc(F* dQ, const F* prim, const F* g, const F* gty, int ngty, const F* dpd, const F* dpt0,
                       const F* dpt1, const F* drd, const Grid3& gr, int d, int side, int Ns, const PhysConst& pc,
-                      const NscbcParams& bp, cudaStream_t st, const double* tgt = nullptr);
+                      const NscbcParams& bp, cudaStream_t st, const double* tgt = nullptr,
+                      const Geom* G = nullptr);
     // fluxes with each direction's flux multiplied by its area factor A_d
     // (the A_d F_d product of src/rhs.jl:670-675), for curvilinear / stretched grids
     static void fluxes_geo(const double* Q, const F* prim, const F* g, const F* gty, const F* art, F* flux,

@@ -210,9 +210,6 @@ public:
                     if (!unit_scalefactor(d.metric, k))
                         throw Error(CLES_EINVAL, "characteristic boundary conditions need a face whose normal metric "
                                                  "scale factor is one");
-                    if (geo_)
-                        throw Error(CLES_EINVAL, "characteristic boundary conditions are built for uniform Cartesian "
-                                                 "grids only");
                 }
         const bool axis = d.bc[0][0] == CLES_BC_AXIS, orig1 = d.bc[0][0] == CLES_BC_ORIGIN;
         const bool pole_l = d.bc[1][0] == CLES_BC_POLE, pole_h = d.bc[1][1] == CLES_BC_POLE;
@@ -593,20 +590,20 @@ public:
                 F* dpd = scratch(0);
                 F* dt0 = scratch(3);
                 F* dt1 = scratch(4);
-                launch_compact(*dset_[k][0], view(prim(P_P)), view(dpd), 1, OUT_STORE, st_);
+                along_set(dset_[k], k, prim(P_P), dpd, 1, OUT_STORE, nullptr);
                 const int t1 = k == 0 ? 1 : 0, t2 = k == 2 ? 1 : 2;
                 F* drd = nullptr;
                 if (bc == CLES_BC_NSCBC_OUTFLOW) {
-                    if (g_.active[t1]) launch_compact(*dset_[t1][0], view(prim(P_P)), view(dt0), 1, OUT_STORE, st_);
-                    if (g_.active[t2]) launch_compact(*dset_[t2][0], view(prim(P_P)), view(dt1), 1, OUT_STORE, st_);
+                    if (g_.active[t1]) along_set(dset_[t1], t1, prim(P_P), dt0, 1, OUT_STORE, nullptr);
+                    if (g_.active[t2]) along_set(dset_[t2], t2, prim(P_P), dt1, 1, OUT_STORE, nullptr);
                 } else {
                     drd = dt0;
-                    launch_compact(*dset_[k][0], view(prim(P_RHO)), view(drd), 1, OUT_STORE, st_);
+                    along_set(dset_[k], k, prim(P_RHO), drd, 1, OUT_STORE, nullptr);
                 }
                 const double* tgt = nullptr;
                 if (bc == CLES_BC_NSCBC_INFLOW && face_fn(k, s).fn) tgt = eval_face_fn(k, s, 4 + Ns_);
                 Pointwise<F>::nscbc(dQ_.as<F>(), prim_.as<F>(), g_u_.as<F>(), gty_.as<F>(), Ns_ == 1 ? 1 : 1 + Ns_, dpd,
-                                    dt0, dt1, drd, g_, k, s, Ns_, pc_, np, st_, tgt);
+                                    dt0, dt1, drd, g_, k, s, Ns_, pc_, np, st_, tgt, geo_ ? &G_ : nullptr);
             }
         }
     }
@@ -675,6 +672,7 @@ public:
             }
             MetricOps<F>::metric_div(dQ_.as<F>(), flux_.as<F>(), ncons_, Ns_, prim_.as<F>(), g_u_.as<F>(), art_.as<F>(),
                                      desc.mu0, G_, g_, st_);
+            if (nscbc) correct_rhs_nscbc();
             return false;
         }
         PW::fluxes(Q_.as<double>(), prim_.as<F>(), g_u_.as<F>(), gty_.as<F>(), art_.as<F>(), flux_.as<F>(), cells_, Ns_,

@@ -1386,17 +1386,17 @@ void nscbc_outflow(Solver& S, int d, int side) {
         const double un = uv[d];
         const double Ma = std::fabs(un) / c;
         if (!(Ma < 1)) return;
-        const double dpn = 1.0 * S.tmp_a[I];
+        const double dpn = S.inv_h[d][I] * S.tmp_a[I];
         const double dun = S.grad_u[d][d][I];
         const double Lcomp = side == 1 ? (un - c) * (dpn - rho * c * dun) : (un + c) * (dpn + rho * c * dun);
         double tin = 0.0;
         if (act1) {
             const double ut = uv[t1];
-            tin += ut * 1.0 * S.tmp_b[I] + rho * c * c * S.grad_u[t1][t1][I] + sgn * rho * c * ut * S.grad_u[t1][d][I];
+            tin += ut * S.inv_h[t1][I] * S.tmp_b[I] + rho * c * c * S.grad_u[t1][t1][I] + sgn * rho * c * ut * S.grad_u[t1][d][I];
         }
         if (act2) {
             const double ut = uv[t2];
-            tin += ut * 1.0 * S.sensor_sp[I] + rho * c * c * S.grad_u[t2][t2][I] + sgn * rho * c * ut * S.grad_u[t2][d][I];
+            tin += ut * S.inv_h[t2][I] * S.sensor_sp[I] + rho * c * c * S.grad_u[t2][t2][I] + sgn * rho * c * ut * S.grad_u[t2][d][I];
         }
         const double bt = bc.beta_t < 0 ? Ma : bc.beta_t;
         const double K = bc.sigma * (1 - Ma * Ma) * c / Lref;
@@ -1441,7 +1441,7 @@ void nscbc_inflow(Solver& S, int d, int side) {
         const double un = uv[d];
         const double Ma = std::fabs(un) / c;
         if (!(Ma < 1)) return;
-        const double dpn = 1.0 * S.tmp_a[I], drn = 1.0 * S.tmp_b[I], dun = S.grad_u[d][d][I];
+        const double dpn = S.inv_h[d][I] * S.tmp_a[I], drn = S.inv_h[d][I] * S.tmp_b[I], dun = S.grad_u[d][d][I];
         const double K = c / Lref;
         const double L1c = (un - c) * (dpn - rho * c * dun);
         const double L5c = (un + c) * (dpn + rho * c * dun);
@@ -1866,10 +1866,6 @@ Solver* solver_create(const cles_solver_desc& A) {
                 if (bc != CLES_BC_NSCBC_OUTFLOW && bc != CLES_BC_NSCBC_INFLOW) continue;
                 if (!unit_scalefactor(A.metric, d)) {
                     set_err("characteristic boundary conditions need a face whose normal metric scale factor is one");
-                    return nullptr;
-                }
-                if (A.metric != CLES_METRIC_CARTESIAN || stretched[0] || stretched[1] || stretched[2]) {
-                    set_err("characteristic boundary conditions are built for uniform Cartesian grids only");
                     return nullptr;
                 }
             }

@@ -225,7 +225,13 @@ def test_geometry_setup_errors():
                        cl.lele_d1_6(), cl.compact_filter(0.45))
     with pytest.raises(cl.ClesError, match="AxisBC requires CylindricalMetric"):
         cl.Solver(d)
-    d = cl.solver_desc((16, 8, 8), (1.0, 1.0, 1.0), ((cl.NSCBCOutflowBC(pinf=1.0), cl.SlipWallBC()), PER, PER),
-                       cl.lele_d1_6(), cl.compact_filter(0.45), stretch=(cl.sine_cluster(0, 1, 0.5, 0.2), None, None))
-    with pytest.raises(cl.ClesError, match="uniform Cartesian"):
+    # a characteristic face needs a unit normal scale factor: not a theta face (src/nscbc.jl:309-323)
+    d = cl.solver_desc((16, 16, 8), (1.0, 1.0, 1.0), (PER, (cl.NSCBCOutflowBC(pinf=1.0), cl.SlipWallBC()), PER),
+                       cl.lele_d1_6(), cl.compact_filter(0.45), metric=cl.CylindricalMetric(), origin=(0.5, 0.0, 0.0))
+    with pytest.raises(cl.ClesError, match="periodic radial|scale factor"):
+        cl.Solver(d)
+    d = cl.solver_desc((16, 16, 8), (1.0, 1.0, 1.0), ((cl.SlipWallBC(), cl.SlipWallBC()),
+                                                      (cl.NSCBCOutflowBC(pinf=1.0), cl.SlipWallBC()), PER),
+                       cl.lele_d1_6(), cl.compact_filter(0.45), metric=cl.CylindricalMetric(), origin=(0.5, 0.0, 0.0))
+    with pytest.raises(cl.ClesError, match="scale factor is one"):
         cl.Solver(d)
