@@ -600,7 +600,7 @@ __global__ void k_ke_partial(const double* __restrict__ Q, double* __restrict__ 
 // quad-weighted sum of tau:grad u and of rho (dissipation_rate, src/diagnostics.jl:354-378)
 template <typename F>
 __global__ void k_diss_partial(const F* __restrict__ prim, const F* __restrict__ g, const F* __restrict__ art,
-                               double* __restrict__ part, Grid3 gr, double mu0) {
+                               double* __restrict__ part, Grid3 gr, double mu0, Geom Gm, int geo, unsigned foldmask) {
     __shared__ double s1[kThreads], s2[kThreads];
     const int64_t cells = (int64_t)gr.n[0] * gr.n[1] * gr.n[2];
     double a1 = 0.0, a2 = 0.0;
@@ -609,9 +609,16 @@ __global__ void k_diss_partial(const F* __restrict__ prim, const F* __restrict__
         const int j = (int)((I / gr.n[0]) % gr.n[1]);
         const int k = (int)(I / ((int64_t)gr.n[0] * gr.n[1]));
         const int ijk[3] = {i, j, k};
+        // quad_weight (src/diagnostics.jl:41-49): 1/2 on a node-centred closed
+        // edge, 1 on a folded (half-offset) one
         double w = 1.0;
-        for (int d = 0; d < 3; ++d)
-            if (gr.active[d] && !gr.periodic[d] && (ijk[d] == 0 || ijk[d] == gr.n[d] - 1)) w *= 0.5;
+        for (int d = 0; d < 3; ++d) {
+            if (!gr.active[d] || gr.periodic[d]) continue;
+            if (ijk[d] == 0 && !((foldmask >> (2 * d)) & 1u)) w *= 0.5;
+            else if (ijk[d] == gr.n[d] - 1 && !((foldmask >> (2 * d + 1)) & 1u)) w *= 0.5;
+        }
+        // the metric Jacobian J = 1/inv_J (src/diagnostics.jl:73-75)
+        const double ij = geo ? geo_point(Gm, i, j, k, I).inv_J : 1.0;
         double gv[9];
         for (int q = 0; q < 9; ++q) gv[q] = double(g[I + cells * q]);
         const double mu = mu0 + double(art[I + cells * A_MU]);
@@ -623,8 +630,8 @@ __global__ void k_diss_partial(const F* __restrict__ prim, const F* __restrict__
                 const double tau = mu * (gv[3 * a + b] + gv[3 * b + a]) + (a == b ? (be - 2 * mu / 3) * divu : 0.0);
                 acc += tau * gv[3 * a + b];
             }
-        a1 += w * acc;
-        a2 += w * double(prim[I + cells * P_RHO]);
+        a1 += w * acc / ij;
+        a2 += w * double(prim[I + cells * P_RHO]) / ij;
     }
     s1[threadIdx.x] = a1;
     s2[threadIdx.x] = a2;
@@ -1000,10 +1007,10 @@ void Pointwise<F>::kinetic(const double* Q, double* part, double* out, int64_t c
 }
 template <typename F>
 void Pointwise<F>::dissipation(const F* prim, const F* g, const F* art, double* part, double* out, const Grid3& gr,
-                               double mu0, cudaStream_t st) {
+                               double mu0, cudaStream_t st, const Geom* G, unsigned foldmask) {
     const int64_t cells = (int64_t)gr.n[0] * gr.n[1] * gr.n[2];
     const unsigned nb = grid_for(cells);
-    k_diss_partial<F><<<nb, kThreads, 0, st>>>(prim, g, art, part, gr, mu0);
+    k_diss_partial<F><<<nb, kThreads, 0, st>>>(prim, g, art, part, gr, mu0, G ? *G : Geom{}, G ? 1 : 0, foldmask);
     count_launch();
     check_launch("k_diss_partial");
     k_sum_final<<<1, kThreads, 0, st>>>(part, (int)nb, 2, out);

@@ -114,8 +114,10 @@ struct Pointwise {
     static void rate(const double* Q, const F* prim, const F* art, double* part, double* out, int64_t cells, int Ns,
                      const double idx[3], const int act[3], double mu0, double Pr, double Sc, cudaStream_t st);
     static void kinetic(const double* Q, double* part, double* out, int64_t cells, int Ns, cudaStream_t st);
+    // G: geometry of a curvilinear / stretched grid (null = unit Jacobian);
+    // foldmask bit 2d + side marks a folded edge (quadrature weight 1)
     static void dissipation(const F* prim, const F* g, const F* art, double* part, double* out, const Grid3& gr,
-                            double mu0, cudaStream_t st);
+                            double mu0, cudaStream_t st, const Geom* G = nullptr, unsigned foldmask = 0u);
     static void convert(const double* a, F* b, int64_t n, cudaStream_t st);
     static void to_double(const F* a, double* b, int64_t n, cudaStream_t st);
     // correct_rhs! of an NSCBC face (src/nscbc.jl:59-307) on the plane of

@@ -913,13 +913,17 @@ public:
     double dissipation_rate() override {
         // dissipation_rate (src/diagnostics.jl:354-378): refreshes primitives,
         // gradients and artificial properties from the resident state
-        if (geo_) throw Error(CLES_EINVAL, "the dissipation diagnostic is built for uniform Cartesian grids only");
         using PW = Pointwise<F>;
         PW::primitives(Q_.as<double>(), prim_.as<F>(), cells_, Ns_, pc_, st_, desc.art_enabled);
         velocity_gradients();
         compute_artificial();
+        unsigned foldmask = 0u;
+        for (int k = 0; k < 3; ++k) {
+            if (fold_[k].on && fold_[k].lo) foldmask |= 1u << (2 * k);
+            if (fold_[k].on && fold_[k].hi) foldmask |= 1u << (2 * k + 1);
+        }
         PW::dissipation(prim_.as<F>(), g_u_.as<F>(), art_.as<F>(), part_.as<double>(), res_.as<double>(), g_, desc.mu0,
-                        st_);
+                        st_, geo_ ? &G_ : nullptr, foldmask);
         CLES_CUDA(cudaMemcpyAsync(host_res_, res_.p, 2 * sizeof(double), cudaMemcpyDeviceToHost, st_));
         CLES_CUDA(cudaStreamSynchronize(st_));
         return host_res_[0] / host_res_[1];

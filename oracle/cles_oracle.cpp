@@ -1755,9 +1755,12 @@ int run(Solver& S, double tfinal, int64_t nmax, cles_run_result* res) {
 
 // quad_weight / volume_integral (src/diagnostics.jl:41-80), no folds.
 double quad_weight(const Solver& S, int d, int i) {
+    // 1 in the interior and on a folded (half-offset) edge, 1/2 on a
+    // node-centred closed edge (src/diagnostics.jl:41-49)
     const Decomp& D = S.D;
     if (!(D.active[d] && !D.periodic[d])) return 1.0;
-    if (i == 0 || i == D.ng[d] - 1) return 0.5;
+    if (i == 0) return (S.folds[d] && S.folds[d]->lo) ? 1.0 : 0.5;
+    if (i == D.ng[d] - 1) return (S.folds[d] && S.folds[d]->hi) ? 1.0 : 0.5;
     return 1.0;
 }
 double volume_integral(Solver& S, const double* f) {
@@ -1771,7 +1774,7 @@ double volume_integral(Solver& S, const double* f) {
             const double wj = wk * quad_weight(S, 1, j);
             for (int i = 0; i < D.nl[0]; ++i) {
                 const size_t I = D.at(i + D.nhd[0], j + D.nhd[1], k + D.nhd[2]);
-                acc += wj * quad_weight(S, 0, i) * f[I] / 1.0;
+                acc += wj * quad_weight(S, 0, i) * f[I] / S.inv_J[I];   // J = 1/inv_J
             }
         }
     }

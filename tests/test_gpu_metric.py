@@ -235,3 +235,12 @@ def test_geometry_setup_errors():
                        cl.lele_d1_6(), cl.compact_filter(0.45), metric=cl.CylindricalMetric(), origin=(0.5, 0.0, 0.0))
     with pytest.raises(cl.ClesError, match="scale factor is one"):
         cl.Solver(d)
+
+
+@pytest.mark.parametrize("case", ["stretched", "annulus", "axis_axisym", "axis_resolved", "sphere"])
+def test_dissipation_rate_matches_oracle(orc, case):
+    # dissipation_rate (src/diagnostics.jl:354-378): J-weighted volume
+    # integrals, unit quadrature weight on a folded edge
+    S, O, d = _pair(orc, case, art=True)
+    ds, do = S.dissipation_rate(), O.dissipation_rate()
+    assert abs(ds - do) <= 1e-11 * abs(do)
