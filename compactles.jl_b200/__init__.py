@@ -6,7 +6,8 @@ run!) over the C ABI of libcles.so (include/cles.h).  The CUDA library is
 required: every compute call goes through it and raises if it is missing.
 """
 from . import abi
-from .problem import (ArtParams, AxisBC, CartesianMetric, CylindricalMetric, DirichletBC, ExtrapolationBC,
+from .problem import (ArtParams, AxisBC, CartesianMetric, ConstantBodyForce, CylindricalMetric, DirichletBC,
+                      ExtrapolationBC,
                       IdealMixture, IdealSpecies, NoSlipWallBC, NSCBCInflowBC, NSCBCOutflowBC, Numerics, OriginBC,
                       PER3, PeriodicBC, PoleBC, Prim, Problem, SlipWallBC, SphericalMetric, StepControl, Stretch,
                       SwitchableBC, Transport, sine_cluster,

@@ -18,6 +18,7 @@ CLES_MAX_M = 4
 CLES_MAX_NC = 4
 CLES_MAX_CLO_LEN = 8
 CLES_MAX_SPECIES = 8
+CLES_MAX_BODY_FORCES = 4
 
 CLES_F64 = 0
 CLES_F32 = 1
@@ -190,6 +191,8 @@ class cles_solver_desc(C.Structure):
         ("metric", C.c_int),
         ("stretch_x", C.POINTER(C.c_double) * 3),
         ("stretch_dxdxi", C.POINTER(C.c_double) * 3),
+        ("n_body_forces", C.c_int),
+        ("body_force", (C.c_double * 3) * CLES_MAX_BODY_FORCES),
     ]
 
 

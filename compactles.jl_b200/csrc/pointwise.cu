@@ -497,6 +497,30 @@ __global__ void k_fluxes(const double* __restrict__ Q, const F* __restrict__ pri
 #undef CLES_AF
 }
 
+// add_source!(::ConstantBodyForce) (src/sources.jl:42-65) for every body force
+// in order; products rounded separately as in the reference.
+template <typename F>
+__global__ void k_body_forces(F* __restrict__ dQ, const double* __restrict__ Q, int64_t cells, int Ns, BodyForces bf) {
+    GRID_STRIDE(I, cells) {
+        double rho = 0.0;
+        for (int sp = 0; sp < Ns; ++sp) rho += Q[I + cells * sp];
+        const double q1 = Q[I + cells * Ns], q2 = Q[I + cells * (Ns + 1)], q3 = Q[I + cells * (Ns + 2)];
+        double m[3] = {double(dQ[I + cells * Ns]), double(dQ[I + cells * (Ns + 1)]), double(dQ[I + cells * (Ns + 2)])};
+        double e = double(dQ[I + cells * (Ns + 3)]);
+        for (int f = 0; f < bf.n; ++f) {
+            for (int a = 0; a < 3; ++a) m[a] = m[a] + __dmul_rn(rho, bf.g[f][a]);
+            e = e + ((__dmul_rn(q1, bf.g[f][0]) + __dmul_rn(q2, bf.g[f][1])) + __dmul_rn(q3, bf.g[f][2]));
+            if (sizeof(F) == 4) {
+                // the stored RHS is FP32: round between sources as the stores do
+                for (int a = 0; a < 3; ++a) m[a] = double(F(m[a]));
+                e = double(F(e));
+            }
+        }
+        for (int a = 0; a < 3; ++a) dQ[I + cells * (Ns + a)] = F(m[a]);
+        dQ[I + cells * (Ns + 3)] = F(e);
+    }
+}
+
 // Low-storage RK update (src/timestep.jl:86-95): v = A du + dt dQ; du = v; Q += B v.
 template <typename F>
 __global__ void k_lsrk(double* __restrict__ Q, double* __restrict__ du, const F* __restrict__ dQ, int64_t n, double A,
@@ -972,6 +996,10 @@ void Pointwise<F>::fluxes_geo(const double* Q, const F* prim, const F* g, const 
         LAUNCH((k_fluxes<F, false, true, true>), cells, st, Q, prim, g, gty, art, flux, cells, Ns, pc, mu0, Pr, Sc, G);
     else
         LAUNCH((k_fluxes<F, false, false, true>), cells, st, Q, prim, g, gty, art, flux, cells, Ns, pc, mu0, Pr, Sc, G);
+}
+template <typename F>
+void Pointwise<F>::body_forces(F* dQ, const double* Q, int64_t cells, int Ns, const BodyForces& bf, cudaStream_t st) {
+    LAUNCH(k_body_forces<F>, cells, st, dQ, Q, cells, Ns, bf);
 }
 template <typename F>
 void Pointwise<F>::lsrk(double* Q, double* du, const F* dQ, int64_t n, double A, double B, double dt, cudaStream_t st,

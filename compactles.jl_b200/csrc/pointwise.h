@@ -87,6 +87,12 @@ struct PairParams {
     int pdim, revdim, sd;
 };
 
+// ConstantBodyForce sources (src/sources.jl:20-82), applied in order.
+struct BodyForces {
+    int n;
+    double g[CLES_MAX_BODY_FORCES][3];
+};
+
 template <typename F>
 struct Pointwise {
     // esens: also write the kappa*-sensor input (internal energy) into slot P_Y0 + Ns
@@ -128,6 +134,9 @@ struct Pointwise {
                       const F* dpt1, const F* drd, const Grid3& gr, int d, int side, int Ns, const PhysConst& pc,
                       const NscbcParams& bp, cudaStream_t st, const double* tgt = nullptr,
                       const Geom* G = nullptr);
+    // add_sources! (src/sources.jl:42-82): dQ += rho g on the momenta and
+    // Q_m . g on the energy, per body force in order
+    static void body_forces(F* dQ, const double* Q, int64_t cells, int Ns, const BodyForces& bf, cudaStream_t st);
     // fluxes with each direction's flux multiplied by its area factor A_d
     // (the A_d F_d product of src/rhs.jl:670-675), for curvilinear / stretched grids
     static void fluxes_geo(const double* Q, const F* prim, const F* g, const F* gty, const F* art, F* flux,

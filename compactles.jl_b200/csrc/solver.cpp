@@ -97,6 +97,8 @@ public:
         }
         if (d.n_species < 1 || d.n_species > CLES_MAX_SPECIES) throw Error(CLES_EINVAL, "bad species count");
         if (d.beta_sensor < 0 || d.beta_sensor > 2) throw Error(CLES_EINVAL, "unknown beta sensor");
+        if (d.n_body_forces < 0 || d.n_body_forces > CLES_MAX_BODY_FORCES)
+            throw Error(CLES_EINVAL, "at most 4 body forces");
         Ns_ = d.n_species;
         ncons_ = Ns_ + 4;
         if (d.eos != CLES_EOS_IDEAL && d.eos != CLES_EOS_NASA9) throw Error(CLES_EINVAL, "unknown equation of state");
@@ -649,7 +651,9 @@ public:
     bool compute_rhs_impl(bool primitives_current, const RkEpilogue* rk) {
         using PW = Pointwise<F>;
         const bool nscbc = any_nscbc();
-        if (nscbc) rk = nullptr;   // the boundary correction comes between the divergence and the update
+        const bool sources = desc.n_body_forces > 0;
+        // the boundary correction and the sources come between the divergence and the update
+        if (nscbc || sources) rk = nullptr;
         if (!primitives_current) PW::primitives(Q_.as<double>(), prim_.as<F>(), cells_, Ns_, pc_, st_, desc.art_enabled);
         velocity_gradients();
         compute_artificial();
@@ -673,6 +677,7 @@ public:
             MetricOps<F>::metric_div(dQ_.as<F>(), flux_.as<F>(), ncons_, Ns_, prim_.as<F>(), g_u_.as<F>(), art_.as<F>(),
                                      desc.mu0, G_, g_, st_);
             if (nscbc) correct_rhs_nscbc();
+            if (sources) add_sources();
             return false;
         }
         PW::fluxes(Q_.as<double>(), prim_.as<F>(), g_u_.as<F>(), gty_.as<F>(), art_.as<F>(), flux_.as<F>(), cells_, Ns_,
@@ -700,6 +705,7 @@ public:
         }
         if (first) CLES_CUDA(cudaMemsetAsync(dQ_.p, 0, dQ_.bytes, st_));
         if (nscbc) correct_rhs_nscbc();
+        if (sources) add_sources();
         return fused;
     }
 
@@ -717,6 +723,15 @@ public:
         }
         tstage = t + dt;
         apply_bcs();
+    }
+
+    // add_sources! (src/rhs.jl:692, src/sources.jl:42-82)
+    void add_sources() {
+        BodyForces bf{};
+        bf.n = desc.n_body_forces;
+        for (int f = 0; f < bf.n; ++f)
+            for (int a = 0; a < 3; ++a) bf.g[f][a] = desc.body_force[f][a];
+        Pointwise<F>::body_forces(dQ_.as<F>(), Q_.as<double>(), cells_, Ns_, bf, st_);
     }
 
     // velocity gradients grad_u[d][j] (src/rhs.jl:596-604): one launch per dim

@@ -213,6 +213,13 @@ class SphericalMetric(Metric):
 
 
 @dataclass
+class ConstantBodyForce:
+    """ConstantBodyForce(acceleration=(0, -9.81, 0)) (src/sources.jl:5-30): adds
+    rho g to the momenta and rho u . g to the total energy."""
+    acceleration: Tuple[float, float, float] = (0.0, -9.81, 0.0)
+
+
+@dataclass
 class Stretch:
     """Stretch(x, dxdxi) (src/metric.jl:47-63): monotone map of the uniform
     computational coordinate xi in [0, 1]; both callables take numpy arrays."""
@@ -327,6 +334,7 @@ class Problem:
     eos: IdealMixture = field(default_factory=single_species)
     transport: Transport = field(default_factory=Transport)
     metric: Metric = field(default_factory=CartesianMetric)
+    sources: tuple = ()
 
 
 @dataclass
@@ -349,7 +357,7 @@ _BETA = {"strain": abi.CLES_BETA_STRAIN, "gated_strain": abi.CLES_BETA_GATED_STR
 
 def solver_desc(n_global, L_domain, bcs, deriv, filt, eos=None, transport=None, art=None,
                 origin=(0.0, 0.0, 0.0), cfl=0.5, filter_interval=1, control=None,
-                n_halo=4, precision="fp64", metric=None, stretch=(None, None, None)):
+                n_halo=4, precision="fp64", metric=None, stretch=(None, None, None), sources=()):
     """The flat descriptor for Solver(; n_global, L_domain, bcs, ...) (src/rhs.jl:122-135).
 
     A Stretch on dimension d is sampled at the nodes xi_i = i / (n - 1)
@@ -408,6 +416,14 @@ def solver_desc(n_global, L_domain, bcs, deriv, filt, eos=None, transport=None, 
     d.n_halo = int(n_halo)
     d.precision = abi.CLES_PREC_MIXED if precision == "mixed" else abi.CLES_PREC_FP64
     d.metric = (metric or CartesianMetric()).code
+    if len(sources) > abi.CLES_MAX_BODY_FORCES:
+        raise ValueError(f"at most {abi.CLES_MAX_BODY_FORCES} sources")
+    for f, src in enumerate(sources):
+        if not isinstance(src, ConstantBodyForce):
+            raise ValueError("sources: ConstantBodyForce only")
+        for a in range(3):
+            d.body_force[f][a] = float(src.acceleration[a])
+    d.n_body_forces = len(sources)
     keep = []
     for k in range(3):
         st = stretch[k]
@@ -572,7 +588,7 @@ def problem_desc(prob, num, deriv, filt):
                        transport=prob.transport, art=num.art, origin=origin, cfl=num.cfl,
                        filter_interval=num.filter_interval, control=num.control,
                        n_halo=num.n_halo, precision=num.precision, metric=prob.metric,
-                       stretch=num.stretch)
+                       stretch=num.stretch, sources=prob.sources)
 
 
 # ------------------------------------------------------------- test cases ----

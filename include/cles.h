@@ -51,6 +51,7 @@ extern "C" {
 #define CLES_MAX_NC       4   /* closure rows per edge */
 #define CLES_MAX_CLO_LEN  8   /* closure RHS stencil length */
 #define CLES_MAX_SPECIES  8
+#define CLES_MAX_BODY_FORCES 4   /* ConstantBodyForce sources per solver */
 
 /* element types */
 #define CLES_F64  0
@@ -261,6 +262,10 @@ typedef struct cles_solver_desc {
     int    metric;
     const double* stretch_x[3];
     const double* stretch_dxdxi[3];
+    /* Problem.sources (src/sources.jl): n_body_forces ConstantBodyForce
+     * accelerations, applied in order after the boundary corrections. */
+    int    n_body_forces;
+    double body_force[CLES_MAX_BODY_FORCES][3];
 } cles_solver_desc;
 
 /* Defaults of Problem()/Numerics() for a grid: single_species(1.4, R=1),

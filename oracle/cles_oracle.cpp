@@ -1520,6 +1520,20 @@ void compute_rhs(Solver& S, bool primitives_current) {
             if (bc == CLES_BC_NSCBC_OUTFLOW) nscbc_outflow(S, d, side);
             else if (bc == CLES_BC_NSCBC_INFLOW) nscbc_inflow(S, d, side);
         }
+    // add_sources! (src/sources.jl:42-82): every ConstantBodyForce in order
+    const size_t fs = S.fs;
+    const int m1 = S.i_mom[0], m2 = S.i_mom[1], m3 = S.i_mom[2], ie = S.i_energy;
+    for (int f = 0; f < S.desc.n_body_forces; ++f) {
+        const double g1 = S.desc.body_force[f][0], g2 = S.desc.body_force[f][1], g3 = S.desc.body_force[f][2];
+        for_interior(D, [&](size_t I, int, int, int) {
+            double rho = 0.0;
+            for (int sp = 0; sp < S.Ns; ++sp) rho += S.Q[I + fs * sp];
+            S.dQ[I + fs * m1] += rho * g1;
+            S.dQ[I + fs * m2] += rho * g2;
+            S.dQ[I + fs * m3] += rho * g3;
+            S.dQ[I + fs * ie] += S.Q[I + fs * m1] * g1 + S.Q[I + fs * m2] * g2 + S.Q[I + fs * m3] * g3;
+        });
+    }
 }
 
 // enforce! for SlipWallBC (src/boundary.jl:232-243) and DirichletBC, with a
@@ -1853,6 +1867,7 @@ Solver* solver_create(const cles_solver_desc& A) {
         }
     }
     if (A.n_species < 1 || A.n_species > CLES_MAX_SPECIES) { set_err("bad species count"); return nullptr; }
+    if (A.n_body_forces < 0 || A.n_body_forces > CLES_MAX_BODY_FORCES) { set_err("at most 4 body forces"); return nullptr; }
     if (A.metric < CLES_METRIC_CARTESIAN || A.metric > CLES_METRIC_SPHERICAL) { set_err("unknown metric"); return nullptr; }
     bool stretched[3];
     for (int d = 0; d < 3; ++d) {

@@ -214,3 +214,37 @@ def test_mixed_precision_rhs_close(orc):
     errs = rhs_errors(S.compute_rhs(), dQo, _interior(dg), O.rhs_scales(cl.grid_spacing(dg)))
     # FP32 fields and line solves: a few single-precision ulps of the terms
     assert max(errs) < 2e-6, errs
+
+
+def test_body_forces_match_oracle(orc):
+    # ConstantBodyForce sources (src/sources.jl:42-82): the reference's known
+    # answer on a uniform state (test/runtests.jl:374-388), then a stratified
+    # box under gravity against the oracle: RHS to 1e-12, 20 steps to 1e-10
+    force = cl.ConstantBodyForce((1.0, 2.0, -3.0))
+    d = cl.solver_desc((12, 12, 12), (2 * np.pi,) * 3, cl.PER3, cl.lele_d1_6(), cl.compact_filter(0.45),
+                       art=cl.ArtParams(enabled=False), sources=(force,))
+    S = cl.Solver(d)
+    S.set_state(cl.initialize(d, lambda x, y, z: cl.Prim(u=(0.5 + 0 * x, 0.25 + 0 * y, -0.1 + 0 * z),
+                                                         p=1.0 + 0 * x, rho=2.0 + 0 * x)))
+    dQ = _interior(d)(S.compute_rhs())
+    assert np.allclose(dQ[1], 2.0, atol=1e-10) and np.allclose(dQ[2], 4.0, atol=1e-10)
+    assert np.allclose(dQ[3], -6.0, atol=1e-10) and np.allclose(dQ[4], 2.6, atol=1e-10)
+    g = (cl.ConstantBodyForce((0.0, -1.0, 0.0)), cl.ConstantBodyForce((0.05, 0.0, 0.0)))
+    PER = (cl.PeriodicBC(), cl.PeriodicBC())
+    bcs = (PER, (cl.SlipWallBC(), cl.SlipWallBC()), PER)
+    ic = lambda x, y, z: cl.Prim(u=(0.1 * np.sin(x), 0.0 * y, 0.05 * np.cos(z)), p=2.0 - 0.3 * y / np.pi + 0 * x,
+                                 rho=1.0 + 0.1 * np.cos(x) + 0 * z)
+    pair = [cl.solver_desc((16, 24, 12), (2 * np.pi, 2 * np.pi, 2 * np.pi), bcs, *sch, art=cl.ArtParams(enabled=True),
+                           sources=g) for sch in ((cl.lele_d1_6(), cl.compact_filter(0.45)),
+                                                  (orc.lele_d1_6(), orc.compact_filter(0.45)))]
+    Q0 = cl.initialize(pair[0], ic)
+    S, O = both(orc, pair, Q0)
+    S.apply_bcs()
+    O.apply_bcs()
+    errs = rhs_errors(S.compute_rhs(), O.compute_rhs(), _interior(pair[0]), O.rhs_scales(cl.grid_spacing(pair[0])))
+    assert max(errs) < 1e-12, errs
+    S.run(1e9, 20)
+    assert O.run(1e9, 20)[0] == 0
+    it = _interior(pair[0])
+    a, b = it(S.get_state()), it(O.get_state())
+    assert np.linalg.norm(a - b) <= 1e-10 * np.linalg.norm(b)
