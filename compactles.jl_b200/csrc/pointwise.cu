@@ -929,7 +929,7 @@ void Pointwise<F>::delta4_tiled(const F* f0, const F* f1, F* o0, F* o1, const Gr
         b = Weights3{{w1[0], w1[1], w1[2]}};
         k_delta4_tiled<F, 2><<<grid, kTX * kTY, 0, st>>>(f0, f1, o0, o1, g, a, b);
     } else {
-        k_delta4_tiled<F, 1><<<grid, kTX * kTY, 0, st>>>(f0, f0, o0, o0, g, a, b);
+        k_delta4_tiled<F, 1><<<grid, kTX * kTY, 0, st>>>(f0, nullptr, o0, nullptr, g, a, b);
     }
     count_launch();
     check_launch("k_delta4_tiled");
