@@ -129,3 +129,35 @@ def test_cancel_queued_and_running():
     assert srv.status(ids[0])["state"] == "cancelled"
     assert srv.status(ids[2])["state"] == "cancelled"
     assert srv.status(ids[1])["state"] == "done"
+
+
+def test_server_curvilinear_request_owns_its_stretch():
+    # The server creates a request's solver at admission: a stretched,
+    # curvilinear request still matches the same solve run alone after the
+    # caller's Stretch samples are gone.
+    import gc
+    PER = (cl.PeriodicBC(), cl.PeriodicBC())
+
+    def make():
+        d = cl.solver_desc((48, 16, 1), (1.0, 2 * np.pi, 1.0), ((cl.SlipWallBC(), cl.SlipWallBC()), PER, PER),
+                           cl.lele_d1_6(), cl.compact_filter(0.45), metric=cl.CylindricalMetric(),
+                           origin=(0.3, 0.0, 0.0), stretch=(cl.sine_cluster(0.3, 1.3, 0.5, 0.3), None, None))
+        Q = cl.initialize(d, lambda r, t, z: cl.Prim(u=(0.0 * r, 0.2 * r + 0 * t, 0.0 * r),
+                                                     p=1.0 + 0.1 * np.exp(-20 * (r - 0.8) ** 2) * np.cos(t),
+                                                     rho=1.0 + 0 * r))
+        return d, Q
+    d, Q = make()
+    S = cl.Solver(d)
+    S.set_state(Q)
+    S.run(1e9, 25)
+    want = S.get_state()
+    srv = cl.Server(max_active=2)
+    blocker_d, blocker_Q = make()
+    rid0 = srv.submit(blocker_d, blocker_Q, 1e9, 25)
+    d2, Q2 = make()
+    rid = srv.submit(d2, Q2, 1e9, 25)
+    del d2._stretch_keep       # the descriptor's own samples go away before admission
+    gc.collect()
+    srv.drain()
+    assert np.array_equal(srv.fetch(rid), want)
+    assert np.array_equal(srv.fetch(rid0), want)
