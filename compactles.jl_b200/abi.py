@@ -92,6 +92,31 @@ class cles_grid(C.Structure):
     ]
 
 
+class cles_split_desc(C.Structure):
+    _fields_ = [
+        ("n_local", C.c_int * 3),
+        ("n_halo", C.c_int),
+        ("dim", C.c_int),
+        ("n_global", C.c_int),
+        ("ranks", C.c_int),
+        ("rank", C.c_int),
+        ("periodic", C.c_int),
+    ]
+
+
+class cles_split_info(C.Structure):
+    _fields_ = [
+        ("halo_elems", C.c_int64),
+        ("iface_elems", C.c_int64),
+        ("field_elems", C.c_int64),
+        ("prev", C.c_int),
+        ("next", C.c_int),
+        ("ranks", C.c_int),
+        ("q", C.c_int),
+        ("M", C.c_int),
+    ]
+
+
 class cles_step_control(C.Structure):
     _fields_ = [
         ("predict", C.c_double),

@@ -66,6 +66,14 @@ def lib():
         L.cles_apply_along.argtypes = [vp, vp, vp]
         L.cles_apply_along_batch.argtypes = [vp, vp, vp, C.c_int, C.c_int64]
         L.cles_apply_along_host.argtypes = [vp, vp, vp]
+        L.cles_split_plan_create.argtypes = [vp, C.POINTER(abi.cles_split_desc), C.POINTER(abi.cles_scheme),
+                                             C.c_double, C.c_int, C.POINTER(vp)]
+        L.cles_split_plan_destroy.argtypes = [vp]
+        L.cles_split_plan_info.argtypes = [vp, C.POINTER(abi.cles_split_info)]
+        L.cles_split_halo_pack.argtypes = [vp, vp, vp, vp, C.c_int, C.c_int64]
+        L.cles_split_halo_unpack.argtypes = [vp, vp, vp, vp, C.c_int, C.c_int64]
+        L.cles_split_apply_begin.argtypes = [vp, vp, vp, vp, C.c_int, C.c_int64]
+        L.cles_split_apply_end.argtypes = [vp, vp, vp, C.c_int, C.c_int64]
         L.cles_solver_switch_bc.argtypes = [vp, C.c_int, C.c_int]
         L.cles_solver_set_face_fn.argtypes = [vp, C.c_int, C.c_int, C.c_int, abi.FACE_FN, vp]
         L.cles_solver_bc_switched.argtypes = [vp, C.c_int, C.c_int, C.POINTER(C.c_int)]

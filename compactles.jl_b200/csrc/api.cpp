@@ -83,6 +83,13 @@ struct cles_plan {
     DevBuf fbuf, obuf;
 };
 
+struct cles_split_plan {
+    cles_ctx* ctx = nullptr;
+    SplitPlan sp;
+    int64_t elem_off = 0, sy = 0, sz = 0, field_elems = 0;
+    DevBuf zbuf;
+};
+
 struct cles_solver {
     cles_ctx* ctx = nullptr;
     std::unique_ptr<SolverBase> s;
@@ -343,6 +350,126 @@ int cles_apply_along_host(cles_plan* plan, const void* f_host, void* out_host) {
     if (rc != CLES_OK) return rc;
     CLES_CUDA(cudaMemcpyAsync(out_host, plan->obuf.p, bytes, cudaMemcpyDeviceToHost, st));
     CLES_CUDA(cudaStreamSynchronize(st));
+    API_END
+}
+
+// ------------------------------------------------------------ split lines ----
+int cles_split_plan_create(cles_ctx* ctx, const cles_split_desc* d, const cles_scheme* scheme, double h, int dtype,
+                           cles_split_plan** out) {
+    API_BEGIN
+    if (!ctx || !d || !scheme || !out) throw Error(CLES_EINVAL, "null argument");
+    if (d->dim < 1 || d->dim > 3) throw Error(CLES_EINVAL, "dim must be 1, 2 or 3");
+    if (dtype != CLES_F64 && dtype != CLES_F32) throw Error(CLES_EINVAL, "dtype must be CLES_F64 or CLES_F32");
+    if (!(h > 0)) throw Error(CLES_EINVAL, "grid spacing must be positive");
+    for (int k = 0; k < 3; ++k)
+        if (d->n_local[k] < 1) throw Error(CLES_EINVAL, "n_local must be >= 1");
+    if (d->n_local[d->dim - 1] <= 1 || d->n_global <= 1) throw Error(CLES_EINVAL, "dimension is collapsed");
+    if (scheme->M > d->n_halo)
+        throw Error(CLES_EINVAL, "stencil half-width " + std::to_string(scheme->M) + " exceeds halo width " +
+                                     std::to_string(d->n_halo));
+    CLES_CUDA(cudaSetDevice(ctx->device));
+    auto* p = new cles_split_plan();
+    try {
+        p->ctx = ctx;
+        build_split_plan(p->sp, *scheme, d->n_local, d->dim - 1, d->periodic != 0, d->n_global, d->ranks, d->rank, h,
+                         dtype);
+        int pad[3];
+        for (int k = 0; k < 3; ++k) pad[k] = d->n_local[k] > 1 ? d->n_halo : 0;
+        const int64_t F0 = d->n_local[0] + 2 * pad[0], F1 = d->n_local[1] + 2 * pad[1],
+                      F2 = d->n_local[2] + 2 * pad[2];
+        p->sy = F0;
+        p->sz = F0 * F1;
+        p->elem_off = pad[0] + pad[1] * F0 + pad[2] * F0 * F1;
+        p->field_elems = F0 * F1 * F2;
+    } catch (...) {
+        delete p;
+        throw;
+    }
+    *out = p;
+    API_END
+}
+
+void cles_split_plan_destroy(cles_split_plan* plan) {
+    if (!plan) return;
+    cudaSetDevice(plan->ctx->device);
+    delete plan;
+}
+
+int cles_split_plan_info(const cles_split_plan* plan, cles_split_info* out) {
+    API_BEGIN
+    if (!plan || !out) throw Error(CLES_EINVAL, "null argument");
+    const SplitPlan& sp = plan->sp;
+    out->halo_elems = (int64_t)sp.M * sp.lines;
+    out->iface_elems = (int64_t)2 * sp.q * sp.lines;
+    out->field_elems = plan->field_elems;
+    out->prev = sp.prev;
+    out->next = sp.next;
+    out->ranks = sp.ranks;
+    out->q = sp.q;
+    out->M = sp.M;
+    API_END
+}
+
+static FieldView split_view(const cles_split_plan* p, const void* f, int64_t stride) {
+    const size_t el = p->sp.dtype == CLES_F64 ? sizeof(double) : sizeof(float);
+    return FieldView{const_cast<char*>(reinterpret_cast<const char*>(f)) + el * p->elem_off, stride, p->sy, p->sz};
+}
+
+static void split_check(const cles_split_plan* p, const void* f, int count, int64_t stride) {
+    if (!p || !f) throw Error(CLES_EINVAL, "null argument");
+    if (count < 1) throw Error(CLES_EINVAL, "count must be >= 1");
+    if (count > 1 && stride < p->field_elems) throw Error(CLES_EINVAL, "field_stride below the padded field size");
+}
+
+int cles_split_halo_pack(cles_split_plan* plan, const void* f_dev, void* send_lo, void* send_hi, int count,
+                         int64_t field_stride) {
+    API_BEGIN
+    split_check(plan, f_dev, count, field_stride);
+    if ((plan->sp.lo_open && !send_lo) || (plan->sp.hi_open && !send_hi))
+        throw Error(CLES_EINVAL, "missing send buffer for an end with a neighbour");
+    CLES_CUDA(cudaSetDevice(plan->ctx->device));
+    split_halo(plan->sp, split_view(plan, f_dev, field_stride), send_lo, send_hi, count, true, plan->ctx->stream);
+    API_END
+}
+
+int cles_split_halo_unpack(cles_split_plan* plan, const void* recv_lo, const void* recv_hi, void* f_dev, int count,
+                           int64_t field_stride) {
+    API_BEGIN
+    split_check(plan, f_dev, count, field_stride);
+    if ((plan->sp.lo_open && !recv_lo) || (plan->sp.hi_open && !recv_hi))
+        throw Error(CLES_EINVAL, "missing receive buffer for an end with a neighbour");
+    CLES_CUDA(cudaSetDevice(plan->ctx->device));
+    split_halo(plan->sp, split_view(plan, f_dev, field_stride), const_cast<void*>(recv_lo),
+               const_cast<void*>(recv_hi), count, false, plan->ctx->stream);
+    API_END
+}
+
+int cles_split_apply_begin(cles_split_plan* plan, const void* f_dev, void* out_dev, void* iface, int count,
+                           int64_t field_stride) {
+    API_BEGIN
+    split_check(plan, f_dev, count, field_stride);
+    if (!out_dev || !iface) throw Error(CLES_EINVAL, "null argument");
+    CLES_CUDA(cudaSetDevice(plan->ctx->device));
+    launch_compact_split(plan->sp.local, split_view(plan, f_dev, field_stride), split_view(plan, out_dev, field_stride),
+                         count, iface, plan->ctx->stream);
+    API_END
+}
+
+int cles_split_apply_end(cles_split_plan* plan, const void* iface_all, void* out_dev, int count,
+                         int64_t field_stride) {
+    API_BEGIN
+    split_check(plan, out_dev, count, field_stride);
+    if (!iface_all) throw Error(CLES_EINVAL, "null argument");
+    CLES_CUDA(cudaSetDevice(plan->ctx->device));
+    const size_t el = plan->sp.dtype == CLES_F64 ? sizeof(double) : sizeof(float);
+    const size_t zb = el * (size_t)count * 2 * plan->sp.q * plan->sp.lines;
+    if (plan->zbuf.bytes < zb) {
+        CLES_CUDA(cudaStreamSynchronize(plan->ctx->stream));   // a smaller buffer may still be in use
+        plan->zbuf.release();
+        plan->zbuf.alloc(plan->ctx, zb);
+    }
+    split_correct(plan->sp, iface_all, plan->zbuf.p, split_view(plan, out_dev, field_stride), count,
+                  plan->ctx->stream);
     API_END
 }
 

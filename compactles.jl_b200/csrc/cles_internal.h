@@ -58,6 +58,10 @@ struct CompactParams {
     int symmetric;
     int periodic;
     int lo_closed, hi_closed;
+    // an open end is a rank interface of a split line: interior rows whose
+    // stencil reads the caller's halo, couplings beyond the end left to the
+    // rank-level spikes
+    int lo_open, hi_open;
     int nc;
     int hasred;
     double a0;
@@ -136,8 +140,23 @@ struct CompactPlan {
 // extents n3[3]; periodic says whether the line wraps.  lo_fold / hi_fold set
 // a coordinate-singularity fold at that end of a closed line: the antipodal
 // parity (+1 / -1) of the field the plan is applied to, 0 for a closure.
+// lo_open / hi_open make that end of a non-periodic line a rank interface.
 void build_compact_plan(CompactPlan& plan, const cles_scheme& scheme, const int n3[3], int dim,
-                        bool periodic, double h, int dtype, int lo_fold = 0, int hi_fold = 0);
+                        bool periodic, double h, int dtype, int lo_fold = 0, int hi_fold = 0,
+                        bool lo_open = false, bool hi_open = false);
+
+// The LHS band of one line (or one rank's piece of a split line), row-major
+// n x (2q+1): interior band, closure rows at closed ends, parity folds, and
+// no couplings beyond a non-periodic end.  Unpivoted banded LU of the whole
+// band; solve() applies its inverse in place.
+struct LineBand {
+    int n = 0, q = 1;
+    std::vector<double> a;
+    std::vector<double> L, U;
+    void factor();
+    void solve(double* x) const;
+};
+LineBand make_line_band(const cles_scheme& s, int n, int lo_fold, int hi_fold, bool lo_open, bool hi_open);
 
 // Output modes of the compact operator.  OUT_RK finishes the flux divergence
 // and applies the low-storage RK update in the store (see launch_compact_rk).
@@ -163,11 +182,47 @@ bool try_launch_xt(const CompactPlan& plan, const FieldView& in, const FieldView
 // nothing launched) when the plan does not take the TMA path.
 bool launch_compact_rk(const CompactPlan& plan, const FieldView& in, const FieldView& out, int count,
                        const RkEpilogue& rk, cudaStream_t st);
+// One rank's piece of a line split across `ranks` ranks along `dim`
+// (src/decomposition.jl:73-78 local_range; src/tridiag.jl:85-170 and
+// src/banded.jl:108-214 with P > 1).  `local` solves the rank's own rows with
+// open (interface) ends.  V / W are this rank's spikes: the response of its
+// local solve to the couplings of its first q rows to the previous rank's
+// last q unknowns and of its last q rows to the next rank's first q.  Gsel
+// holds the 2q rows of the inverse of the (2q ranks)^2 reduced system that
+// give those 2q unknowns from every rank's local heads and tails.
+struct SplitPlan {
+    CompactPlan local;
+    int ranks = 1, rank = 0, dim = 0, q = 1, M = 1, n = 0;
+    int n3[3] = {0, 0, 0};
+    int64_t lines = 0;
+    bool lo_open = false, hi_open = false;
+    int prev = -1, next = -1;   // neighbouring rank coordinates, -1 for none
+    int dtype = CLES_F64;
+    void* tab = nullptr;        // [V q x n][W q x n][Gsel 2q x 2q*ranks], plan dtype
+    ~SplitPlan();
+};
+void build_split_plan(SplitPlan& sp, const cles_scheme& s, const int n3_local[3], int dim, bool periodic,
+                      int n_global, int ranks, int rank, double h, int dtype);
+// Copies the M planes next to each end of the local interior into lo / hi
+// ([count][M][lines]) when pack, or those buffers into the halo planes
+// beyond each open end when !pack.
+void split_halo(const SplitPlan& sp, const FieldView& f, void* lo, void* hi, int count, bool pack, cudaStream_t st);
+// From every rank's heads and tails ([ranks][count][2q][lines]): the 2q
+// neighbouring unknowns per line into zbuf ([count][2q][lines]), then
+// out -= V z_prev + W z_next over the local interior.
+void split_correct(const SplitPlan& sp, const void* gathered, void* zbuf, const FieldView& out, int count,
+                   cudaStream_t st);
+
 // Bounded-wait timeouts recorded by device kernels since the last call (cleared).
 int take_device_timeouts(cudaStream_t st);
 
 // Launch the operator over `count` fields of `in` into `out` (may alias).
 void launch_compact(const CompactPlan& plan, const FieldView& in, const FieldView& out, int count, int mode,
                     cudaStream_t st);
+// Local solve of a split-line plan (generic kernel, OUT_STORE); the first and
+// last q values of every line's local solution also go to iface, laid out
+// [count][2q][lines] in the plan's dtype.
+void launch_compact_split(const CompactPlan& plan, const FieldView& in, const FieldView& out, int count, void* iface,
+                          cudaStream_t st);
 
 }  // namespace cles

@@ -19,7 +19,10 @@
 //   5. correct  — x = y - V z_prev - W z_next, then store (overwrite, negate, or
 //                 subtract-accumulate into the output).
 // Periodic lines wrap by index and closed lines use closure rows, so halos of
-// the caller's arrays are never read.
+// the caller's arrays are never read -- except at the open ends of a split
+// line (one rank's piece), where the stencil reads the halo the caller filled
+// from the neighbouring rank, as the reference's fill does after
+// exchange_halos! (src/operators.jl:113-174).
 
 #include <cstdio>
 
@@ -57,10 +60,11 @@ __device__ __forceinline__ LineMap line_map(const CompactParams& P, const FieldV
 }
 
 // g in [-n, 2n): periodic wrap without a division; closed lines clamp (the
-// clamped values are never used by a closure row).
-__device__ __forceinline__ int wrap_index(int g, int n, bool periodic) {
+// clamped values are never used by a closure row); an open end keeps g, whose
+// element lies in the caller's halo (g >= -M, g < n + M).
+__device__ __forceinline__ int wrap_index(int g, int n, bool periodic, bool lo_open = false, bool hi_open = false) {
     if (periodic) return g < 0 ? g + n : (g >= n ? g - n : g);
-    return g < 0 ? 0 : (g >= n ? n - 1 : g);
+    return g < 0 ? (lo_open ? g : 0) : (g >= n ? (hi_open ? g : n - 1) : g);
 }
 
 // Cooperative copy between the CTA's x lines (contiguous rows in global
@@ -109,7 +113,8 @@ __device__ __forceinline__ void tile_rows(const CompactParams& P, const FieldVie
 
 template <typename T, int Q, int M, bool XMODE, int MS>
 __global__ void __launch_bounds__(512) k_compact(const __grid_constant__ CompactParams P, const T* __restrict__ tab,
-                                                  const FieldView in, const FieldView out, const int mode) {
+                                                  const FieldView in, const FieldView out, const int mode,
+                                                  T* __restrict__ iface) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T* smem = reinterpret_cast<T*>(smem_raw);
     const int LB = P.LB, S = P.S, n = P.n;
@@ -143,8 +148,8 @@ __global__ void __launch_bounds__(512) k_compact(const __grid_constant__ Compact
 #pragma unroll
     for (int j = 0; j < WN; ++j) {
         if (j < m + 2 * M) {
-            const int g = wrap_index(off - M + j, n, periodic);
-            if (XMODE) w[j] = tile[g * TP + lane];
+            const int g = wrap_index(off - M + j, n, periodic, P.lo_open, P.hi_open);
+            if (XMODE && g >= 0 && g < n) w[j] = tile[g * TP + lane];
             else w[j] = valid ? fin[Lin.base + (int64_t)g * Lin.stride] : T(0);
         } else {
             w[j] = T(0);
@@ -332,6 +337,19 @@ __global__ void __launch_bounds__(512) k_compact(const __grid_constant__ Compact
     }
 
     // ---- 5. store ------------------------------------------------------------
+    if (iface && valid) {
+        // local solution's head and tail of a split line: [comp][2q][lines]
+        T* ifc = iface + (int64_t)comp * 2 * Q * P.lines + line;
+        if (seg == 0) {
+#pragma unroll
+            for (int t = 0; t < Q; ++t) ifc[(int64_t)t * P.lines] = y[t];
+        }
+        if (seg == S - 1) {
+#pragma unroll
+            for (int i = 0; i < MS; ++i)
+                if (i < m && i >= m - Q) ifc[(int64_t)(Q + i - (m - Q)) * P.lines] = y[i];
+        }
+    }
     if (XMODE) {
         __syncthreads();  // every window/closure read of the tile is done
 #pragma unroll
@@ -510,7 +528,7 @@ bool try_launch_xw(const CompactPlan& plan, const FieldView& in, const FieldView
 
 template <typename T, int Q, int M, bool X, int MS>
 void launch_t(const CompactParams& P, const T* tab, const FieldView& in, const FieldView& out, int count, int mode,
-              cudaStream_t st) {
+              cudaStream_t st, T* iface) {
     const int N = 2 * Q * P.S;
     size_t smem = 0;
     if (X) smem += sizeof(T) * (size_t)P.n * (P.LB + 1);
@@ -524,48 +542,48 @@ void launch_t(const CompactParams& P, const T* tab, const FieldView& in, const F
     }
     dim3 grid((unsigned)((P.lines + P.LB - 1) / P.LB), (unsigned)count);
     dim3 block((unsigned)(P.LB * P.S));
-    kern<<<grid, block, smem, st>>>(P, tab, in, out, mode);
+    kern<<<grid, block, smem, st>>>(P, tab, in, out, mode, iface);
     count_launch();
     check_launch("k_compact");
 }
 
 template <typename T, int Q, bool X>
 void dispatch_m(const CompactParams& P, const T* tab, const FieldView& in, const FieldView& out, int count, int mode,
-                cudaStream_t st) {
+                cudaStream_t st, T* iface) {
     // shorter register tiles for the short segments of few-line closed plans
     const int mmax = P.seg_base + (P.seg_rem ? 1 : 0);
     if constexpr (Q == 1) {
       if (mmax <= 16 && P.M != 3) {
         const bool eight = mmax <= 8;
         switch (P.M) {
-            case 1: eight ? launch_t<T, Q, 1, X, 8>(P, tab, in, out, count, mode, st)
-                          : launch_t<T, Q, 1, X, 16>(P, tab, in, out, count, mode, st); return;
-            case 2: eight ? launch_t<T, Q, 2, X, 8>(P, tab, in, out, count, mode, st)
-                          : launch_t<T, Q, 2, X, 16>(P, tab, in, out, count, mode, st); return;
-            default: eight ? launch_t<T, Q, 4, X, 8>(P, tab, in, out, count, mode, st)
-                           : launch_t<T, Q, 4, X, 16>(P, tab, in, out, count, mode, st); return;
+            case 1: eight ? launch_t<T, Q, 1, X, 8>(P, tab, in, out, count, mode, st, iface)
+                          : launch_t<T, Q, 1, X, 16>(P, tab, in, out, count, mode, st, iface); return;
+            case 2: eight ? launch_t<T, Q, 2, X, 8>(P, tab, in, out, count, mode, st, iface)
+                          : launch_t<T, Q, 2, X, 16>(P, tab, in, out, count, mode, st, iface); return;
+            default: eight ? launch_t<T, Q, 4, X, 8>(P, tab, in, out, count, mode, st, iface)
+                           : launch_t<T, Q, 4, X, 16>(P, tab, in, out, count, mode, st, iface); return;
         }
       }
     }
     switch (P.M) {
-        case 1: launch_t<T, Q, 1, X, kMaxSeg>(P, tab, in, out, count, mode, st); break;
-        case 2: launch_t<T, Q, 2, X, kMaxSeg>(P, tab, in, out, count, mode, st); break;
-        case 3: launch_t<T, Q, 3, X, kMaxSeg>(P, tab, in, out, count, mode, st); break;
-        case 4: launch_t<T, Q, 4, X, kMaxSeg>(P, tab, in, out, count, mode, st); break;
+        case 1: launch_t<T, Q, 1, X, kMaxSeg>(P, tab, in, out, count, mode, st, iface); break;
+        case 2: launch_t<T, Q, 2, X, kMaxSeg>(P, tab, in, out, count, mode, st, iface); break;
+        case 3: launch_t<T, Q, 3, X, kMaxSeg>(P, tab, in, out, count, mode, st, iface); break;
+        case 4: launch_t<T, Q, 4, X, kMaxSeg>(P, tab, in, out, count, mode, st, iface); break;
         default: throw Error(CLES_EINVAL, "unsupported stencil half-width");
     }
 }
 
 template <typename T>
 void dispatch(const CompactParams& P, const T* tab, const FieldView& in, const FieldView& out, int count, int mode,
-              cudaStream_t st) {
+              cudaStream_t st, T* iface = nullptr) {
     const bool X = P.dim == 0;
     if (P.q == 1) {
-        if (X) dispatch_m<T, 1, true>(P, tab, in, out, count, mode, st);
-        else dispatch_m<T, 1, false>(P, tab, in, out, count, mode, st);
+        if (X) dispatch_m<T, 1, true>(P, tab, in, out, count, mode, st, iface);
+        else dispatch_m<T, 1, false>(P, tab, in, out, count, mode, st, iface);
     } else {
-        if (X) dispatch_m<T, 2, true>(P, tab, in, out, count, mode, st);
-        else dispatch_m<T, 2, false>(P, tab, in, out, count, mode, st);
+        if (X) dispatch_m<T, 2, true>(P, tab, in, out, count, mode, st, iface);
+        else dispatch_m<T, 2, false>(P, tab, in, out, count, mode, st, iface);
     }
 }
 
@@ -590,6 +608,15 @@ void launch_compact(const CompactPlan& plan, const FieldView& in, const FieldVie
             dispatch<float>(plan.P, plan.tab32, in, out, count, mode, st);
     }
     if (rec >= 0) prof_end(rec, st);
+}
+
+void launch_compact_split(const CompactPlan& plan, const FieldView& in, const FieldView& out, int count, void* iface,
+                          cudaStream_t st) {
+    if (count <= 0 || plan.P.lines == 0) return;
+    if (plan.dtype == CLES_F64)
+        dispatch<double>(plan.P, plan.tab64, in, out, count, OUT_STORE, st, static_cast<double*>(iface));
+    else
+        dispatch<float>(plan.P, plan.tab32, in, out, count, OUT_STORE, st, static_cast<float*>(iface));
 }
 
 }  // namespace cles

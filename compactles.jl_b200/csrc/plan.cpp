@@ -208,8 +208,88 @@ CompactPlan::~CompactPlan() {
     if (tab32) cudaFree(tab32);
 }
 
+LineBand make_line_band(const cles_scheme& s, int n, int lo_fold, int hi_fold, bool lo_open, bool hi_open) {
+    const int q = s.q, nc = s.nc, W = 2 * q + 1;
+    LineBand b;
+    b.n = n;
+    b.q = q;
+    b.a.assign((size_t)n * W, 0.0);
+    for (int i = 0; i < n; ++i) {
+        b.a[(size_t)i * W + q] = 1.0;
+        for (int t = 1; t <= q; ++t) {
+            b.a[(size_t)i * W + q + t] = s.lhs[t - 1];
+            b.a[(size_t)i * W + q - t] = s.lhs[t - 1];
+        }
+    }
+    // parity folds (src/operators.jl:61-70, src/operators_banded.jl:58-77):
+    // the coupling of row i to a ghost column maps onto its mirror column
+    // with the solution's sign sigma_g (the field's parity for a filter,
+    // its opposite for a derivative)
+    const int sg_lo = s.symmetric ? lo_fold : -lo_fold;
+    const int sg_hi = s.symmetric ? hi_fold : -hi_fold;
+    if (lo_fold)
+        for (int i = 1; i <= q; ++i)
+            for (int m = 1; m <= q; ++m) {
+                if (i - m >= 1) continue;
+                const int jcol = m - i + 1;
+                b.a[(size_t)(i - 1) * W + q + (jcol - i)] += (double)sg_lo * s.lhs[m - 1];
+            }
+    if (hi_fold)
+        for (int i = n - q + 1; i <= n; ++i)
+            for (int m = 1; m <= q; ++m) {
+                if (i + m <= n) continue;
+                const int jcol = 2 * n + 1 - (i + m);
+                b.a[(size_t)(i - 1) * W + q + (jcol - i)] += (double)sg_hi * s.lhs[m - 1];
+            }
+    // closure rows at closed ends; an open end (rank interface) keeps the
+    // interior rows (src/operators.jl:66-84, src/operators_banded.jl:48-112)
+    for (int j = 0; j < nc && !lo_fold && !lo_open; ++j)
+        for (int t = -q; t <= q; ++t) {
+            double v = s.clo_lhs[j][q + t];
+            if (j + t < 0) {
+                if (q >= 2 && v != 0.0) throw Error(CLES_EINVAL, "closure row references a column before the edge");
+                v = 0.0;  // tridiagonal row 1 ignores its sub-diagonal
+            }
+            b.a[(size_t)j * W + q + t] = v;
+        }
+    for (int j = 0; j < nc && !hi_fold && !hi_open; ++j) {
+        const int r = n - 1 - j;
+        for (int t = -q; t <= q; ++t) {
+            double v = s.clo_lhs[j][q - t];
+            if (r + t >= n) v = 0.0;
+            b.a[(size_t)r * W + q + t] = v;
+        }
+    }
+    // the first/last rows have no couplings beyond the edge (at an open end
+    // they are the rank-level spike columns)
+    for (int i = 0; i < n; ++i)
+        for (int t = -q; t <= q; ++t)
+            if (i + t < 0 || i + t >= n) b.a[(size_t)i * W + q + t] = 0.0;
+    return b;
+}
+
+void LineBand::factor() {
+    Band B;
+    B.n = n; B.q = q; B.periodic = false; B.a = a;
+    LocalFactor F;
+    F.build(B, 0, n);
+    L = std::move(F.L);
+    U = std::move(F.U);
+}
+
+void LineBand::solve(double* x) const {
+    const int m = n;
+    for (int k = 0; k < m - 1; ++k)
+        for (int t = 1; t <= std::min(q, m - 1 - k); ++t) x[k + t] -= L[(size_t)(t - 1) * m + k] * x[k];
+    for (int i = m - 1; i >= 0; --i) {
+        double acc = x[i];
+        for (int t = 1; t <= std::min(q, m - 1 - i); ++t) acc -= U[(size_t)t * m + i] * x[i + t];
+        x[i] = acc / U[i];
+    }
+}
+
 void build_compact_plan(CompactPlan& plan, const cles_scheme& s, const int n3[3], int dim, bool periodic,
-                        double h, int dtype, int lo_fold, int hi_fold) {
+                        double h, int dtype, int lo_fold, int hi_fold, bool lo_open, bool hi_open) {
     const int n = n3[dim];
     const int q = s.q, M = s.M, nc = s.nc;
     if (q < 1 || q > CLES_MAX_Q) throw Error(CLES_EINVAL, "scheme LHS half-bandwidth q must be 1 or 2");
@@ -221,7 +301,11 @@ void build_compact_plan(CompactPlan& plan, const cles_scheme& s, const int n3[3]
                                      " too small for scheme '" + std::string(s.name) + "' (need >= " +
                                      std::to_string(nmin) + ")");
     if (periodic) lo_fold = hi_fold = 0;
-    if (!periodic && M > nc && (!lo_fold || !hi_fold))
+    if (periodic && (lo_open || hi_open)) throw Error(CLES_EINVAL, "a periodic line has no rank interface");
+    if (lo_open && lo_fold) lo_fold = 0;
+    if (hi_open && hi_fold) hi_fold = 0;
+    const bool lo_clo = !periodic && !lo_fold && !lo_open, hi_clo = !periodic && !hi_fold && !hi_open;
+    if (M > nc && (lo_clo || hi_clo))
         throw Error(CLES_EINVAL, "closed lines need the RHS half-width M <= closure rows nc (halos are never read)");
     for (int j = 0; j < nc; ++j)
         if (s.clo_len[j] < 0 || s.clo_len[j] > CLES_MAX_CLO_LEN || s.clo_len[j] > n)
@@ -231,8 +315,10 @@ void build_compact_plan(CompactPlan& plan, const cles_scheme& s, const int n3[3]
     std::memset(&P, 0, sizeof(P));
     P.n = n; P.dim = dim; P.nx = n3[0]; P.ny = n3[1]; P.nz = n3[2];
     P.q = q; P.M = M; P.symmetric = s.symmetric; P.periodic = periodic ? 1 : 0;
-    P.lo_closed = periodic ? 0 : 1;
-    P.hi_closed = periodic ? 0 : 1;
+    P.lo_closed = (periodic || lo_open) ? 0 : 1;
+    P.hi_closed = (periodic || hi_open) ? 0 : 1;
+    P.lo_open = lo_open ? 1 : 0;
+    P.hi_open = hi_open ? 1 : 0;
     // A folded end carries rows of the interior stencil whose reads beyond the
     // edge are the half-offset mirror f[-1-g] = sigma f[g] (the fold_fill! halo,
     // src/folds.jl:83-124), written as closure rows over the interior; both
@@ -296,57 +382,18 @@ void build_compact_plan(CompactPlan& plan, const cles_scheme& s, const int n3[3]
     // Global band with closures (src/operators.jl:66-84, src/operators_banded.jl:48-112).
     Band B;
     B.n = n; B.q = q; B.periodic = periodic;
-    const int W = 2 * q + 1;
-    B.a.assign((size_t)n * W, 0.0);
-    for (int i = 0; i < n; ++i) {
-        B.a[(size_t)i * W + q] = 1.0;
-        for (int t = 1; t <= q; ++t) {
-            B.a[(size_t)i * W + q + t] = s.lhs[t - 1];
-            B.a[(size_t)i * W + q - t] = s.lhs[t - 1];
-        }
-    }
-    if (!periodic) {
-        // parity folds (src/operators.jl:61-70, src/operators_banded.jl:58-77):
-        // the coupling of row i to a ghost column maps onto its mirror column
-        // with the solution's sign sigma_g (the field's parity for a filter,
-        // its opposite for a derivative)
-        const int sg_lo = s.symmetric ? lo_fold : -lo_fold;
-        const int sg_hi = s.symmetric ? hi_fold : -hi_fold;
-        if (lo_fold)
-            for (int i = 1; i <= q; ++i)
-                for (int m = 1; m <= q; ++m) {
-                    if (i - m >= 1) continue;
-                    const int jcol = m - i + 1;
-                    B.a[(size_t)(i - 1) * W + q + (jcol - i)] += (double)sg_lo * s.lhs[m - 1];
-                }
-        if (hi_fold)
-            for (int i = n - q + 1; i <= n; ++i)
-                for (int m = 1; m <= q; ++m) {
-                    if (i + m <= n) continue;
-                    const int jcol = 2 * n + 1 - (i + m);
-                    B.a[(size_t)(i - 1) * W + q + (jcol - i)] += (double)sg_hi * s.lhs[m - 1];
-                }
-        for (int j = 0; j < nc && !lo_fold; ++j)
-            for (int t = -q; t <= q; ++t) {
-                double v = s.clo_lhs[j][q + t];
-                if (j + t < 0) {
-                    if (q >= 2 && v != 0.0) throw Error(CLES_EINVAL, "closure row references a column before the edge");
-                    v = 0.0;  // tridiagonal row 1 ignores its sub-diagonal
-                }
-                B.a[(size_t)j * W + q + t] = v;
-            }
-        for (int j = 0; j < nc && !hi_fold; ++j) {
-            const int r = n - 1 - j;
-            for (int t = -q; t <= q; ++t) {
-                double v = s.clo_lhs[j][q - t];
-                if (r + t >= n) v = 0.0;
-                B.a[(size_t)r * W + q + t] = v;
+    if (periodic) {
+        const int W = 2 * q + 1;
+        B.a.assign((size_t)n * W, 0.0);
+        for (int i = 0; i < n; ++i) {
+            B.a[(size_t)i * W + q] = 1.0;
+            for (int t = 1; t <= q; ++t) {
+                B.a[(size_t)i * W + q + t] = s.lhs[t - 1];
+                B.a[(size_t)i * W + q - t] = s.lhs[t - 1];
             }
         }
-        // the first/last rows have no couplings beyond the edge
-        for (int i = 0; i < n; ++i)
-            for (int t = -q; t <= q; ++t)
-                if (i + t < 0 || i + t >= n) B.a[(size_t)i * W + q + t] = 0.0;
+    } else {
+        B.a = make_line_band(s, n, lo_fold, hi_fold, lo_open, hi_open).a;
     }
 
     // Segmentation: S segments of at most kMaxSeg points, local_range split.
@@ -557,7 +604,7 @@ void build_compact_plan(CompactPlan& plan, const cles_scheme& s, const int n3[3]
     // pentadiagonal; y/z lines by TMA tiles, x lines by cp.async transposed
     // tiles): equal segments of 16 or 32 points, at most 8 per line
     plan.has_tg = false;
-    if (with_g && P.seg_rem == 0 && (P.seg_base == 16 || P.seg_base == 32) && S * 32 <= 256 && n <= 256 &&
+    if (with_g && !lo_open && !hi_open && P.seg_rem == 0 && (P.seg_base == 16 || P.seg_base == 32) && S * 32 <= 256 && n <= 256 &&
         ((q == 1 && (M == 1 || M == 2 || M == 4)) || (q == 2 && M == 3))) {
         TileGenParams& G = plan.TG;
         std::memset(&G, 0, sizeof(G));
@@ -605,6 +652,113 @@ void build_compact_plan(CompactPlan& plan, const cles_scheme& s, const int n3[3]
         std::vector<float> t32(tab.begin(), tab.end());
         CLES_CUDA(cudaMalloc(&plan.tab32, sizeof(float) * total));
         CLES_CUDA(cudaMemcpy(plan.tab32, t32.data(), sizeof(float) * total, cudaMemcpyHostToDevice));
+    }
+}
+
+SplitPlan::~SplitPlan() {
+    if (tab) cudaFree(tab);
+}
+
+void build_split_plan(SplitPlan& sp, const cles_scheme& s, const int n3[3], int dim, bool periodic, int n_global,
+                      int ranks, int rank, double h, int dtype) {
+    if (ranks < 1 || rank < 0 || rank >= ranks) throw Error(CLES_EINVAL, "rank must lie in [0, ranks)");
+    if (dim < 0 || dim > 2) throw Error(CLES_EINVAL, "dim must be 1, 2 or 3");
+    const int q = s.q;
+    if (q < 1 || q > CLES_MAX_Q) throw Error(CLES_EINVAL, "scheme LHS half-bandwidth q must be 1 or 2");
+    // every rank's extent (src/decomposition.jl:73-78)
+    auto range = [&](int r, int* nr, int* off) {
+        const int base = n_global / ranks, rem = n_global % ranks;
+        *nr = base + (r < rem ? 1 : 0);
+        *off = r * base + std::min(r, rem);
+    };
+    int nr = 0, off = 0;
+    range(rank, &nr, &off);
+    if (n3[dim] != nr)
+        throw Error(CLES_EINVAL, "local extent " + std::to_string(n3[dim]) + " along dim " + std::to_string(dim + 1) +
+                                     " is not rank " + std::to_string(rank) + "'s share " + std::to_string(nr) +
+                                     " of " + std::to_string(n_global));
+    // the smallest piece decides, so every rank refuses the same split
+    // (src/operators.jl:50-53, src/operators_banded.jl:37-41)
+    const int nmin = q >= 2 ? std::max({2 * s.nc + 1, 2 * s.M + 1, 2 * q + 1}) : std::max(2 * s.nc + 1, 2 * s.M + 1);
+    if (n_global / ranks < nmin)
+        throw Error(CLES_EINVAL, "local extent " + std::to_string(n_global / ranks) + " along dim " +
+                                     std::to_string(dim + 1) + " too small for scheme '" + std::string(s.name) +
+                                     "' (need >= " + std::to_string(nmin) + ")");
+    sp.ranks = ranks; sp.rank = rank; sp.dim = dim; sp.q = q; sp.M = s.M; sp.n = nr; sp.dtype = dtype;
+    for (int k = 0; k < 3; ++k) sp.n3[k] = n3[k];
+    sp.lo_open = periodic || rank > 0;
+    sp.hi_open = periodic || rank < ranks - 1;
+    sp.prev = sp.lo_open ? (rank - 1 + ranks) % ranks : -1;
+    sp.next = sp.hi_open ? (rank + 1) % ranks : -1;
+    build_compact_plan(sp.local, s, n3, dim, false, h, dtype, 0, 0, sp.lo_open, sp.hi_open);
+    sp.lines = sp.local.P.lines;
+
+    // rank-level spikes of every rank and the reduced system in
+    // z = (head_0, tail_0, head_1, tail_1, ...), 2q per rank
+    const int N = 2 * q * ranks;
+    std::vector<double> R((size_t)N * N, 0.0);
+    std::vector<double> Vme, Wme;
+    for (int rr = 0; rr < ranks; ++rr) {
+        int m = 0, o = 0;
+        range(rr, &m, &o);
+        const bool lo = periodic || rr > 0, hi = periodic || rr < ranks - 1;
+        LineBand b = make_line_band(s, m, 0, 0, lo, hi);
+        b.factor();
+        std::vector<double> V((size_t)q * m, 0.0), W((size_t)q * m, 0.0);
+        for (int t = 0; t < q; ++t) {
+            double* v = &V[(size_t)t * m];
+            double* w = &W[(size_t)t * m];
+            // row r couples to the previous rank's tail unknown t at distance
+            // r + q - t, row i to the next rank's head unknown t at m + t - i
+            if (lo) {
+                for (int r = 0; r < q; ++r) {
+                    const int d = r + q - t;
+                    if (d >= 1 && d <= q) v[r] = s.lhs[d - 1];
+                }
+                b.solve(v);
+            }
+            if (hi) {
+                for (int i = m - q; i < m; ++i) {
+                    const int d = m + t - i;
+                    if (d >= 1 && d <= q) w[i] = s.lhs[d - 1];
+                }
+                b.solve(w);
+            }
+        }
+        const int prev = (rr - 1 + ranks) % ranks, next = (rr + 1) % ranks;
+        for (int r = 0; r < q; ++r) {
+            const int rh = 2 * q * rr + r, rt = 2 * q * rr + q + r;
+            R[(size_t)rh * N + rh] += 1.0;
+            R[(size_t)rt * N + rt] += 1.0;
+            for (int t = 0; t < q; ++t) {
+                const int cprev = 2 * q * prev + q + t, cnext = 2 * q * next + t;
+                R[(size_t)rh * N + cprev] += V[(size_t)t * m + r];
+                R[(size_t)rt * N + cprev] += V[(size_t)t * m + (m - q + r)];
+                R[(size_t)rh * N + cnext] += W[(size_t)t * m + r];
+                R[(size_t)rt * N + cnext] += W[(size_t)t * m + (m - q + r)];
+            }
+        }
+        if (rr == rank) { Vme = std::move(V); Wme = std::move(W); }
+    }
+    const std::vector<double> G = dense_inverse(R, N);
+    const size_t nv = (size_t)q * nr;
+    std::vector<double> tab(2 * nv + (size_t)2 * q * N, 0.0);
+    std::copy(Vme.begin(), Vme.end(), tab.begin());
+    std::copy(Wme.begin(), Wme.end(), tab.begin() + nv);
+    double* Gs = tab.data() + 2 * nv;
+    for (int t = 0; t < q; ++t) {
+        if (sp.lo_open)
+            for (int j = 0; j < N; ++j) Gs[(size_t)t * N + j] = G[(size_t)(2 * q * sp.prev + q + t) * N + j];
+        if (sp.hi_open)
+            for (int j = 0; j < N; ++j) Gs[(size_t)(q + t) * N + j] = G[(size_t)(2 * q * sp.next + t) * N + j];
+    }
+    if (dtype == CLES_F64) {
+        CLES_CUDA(cudaMalloc(&sp.tab, sizeof(double) * tab.size()));
+        CLES_CUDA(cudaMemcpy(sp.tab, tab.data(), sizeof(double) * tab.size(), cudaMemcpyHostToDevice));
+    } else {
+        std::vector<float> t32(tab.begin(), tab.end());
+        CLES_CUDA(cudaMalloc(&sp.tab, sizeof(float) * t32.size()));
+        CLES_CUDA(cudaMemcpy(sp.tab, t32.data(), sizeof(float) * t32.size(), cudaMemcpyHostToDevice));
     }
 }
 

@@ -1,0 +1,177 @@
+// Lines split across ranks: the reference's P > 1 decomposition of a compact
+// operator along one dimension (src/tridiag.jl:136-170, src/banded.jl:177-214,
+// src/halo.jl:143-194), one process per GPU.
+//
+// One application on rank r, with the exchanges done by the caller (NCCL
+// send/recv and all-gather through torch.distributed, or MPI for a Julia
+// host) between the calls:
+//   pack      the M planes at each end of the local interior -> send buffers;
+//   (send the low planes to the previous rank, the high planes to the next)
+//   unpack    received planes -> the padded halo beyond each open end;
+//   local     the generic compact kernel over the rank's rows with open ends
+//             (their stencil reads that halo), storing the local solution y
+//             and each line's first/last q values (launch_compact_split);
+//   (all-gather the heads and tails of every rank)
+//   reduce    per line, the previous rank's last q and the next rank's first q
+//             unknowns from the precomputed rows of the reduced inverse;
+//   correct   out = y - V z_prev - W z_next.
+// The two exchange points are the reference's Sendrecv! halo exchange and its
+// Allgather! of the interface values; nothing here waits on another rank.
+
+#include "cles_internal.h"
+
+namespace cles {
+
+namespace {
+
+constexpr int kThreads = 256;
+
+inline unsigned grid_for(int64_t n) {
+    int64_t b = (n + kThreads - 1) / kThreads;
+    if (b > 148 * 32) b = 148 * 32;
+    return (unsigned)(b < 1 ? 1 : b);
+}
+
+#define GRID_STRIDE(idx, n) \
+    for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < (n); idx += (int64_t)gridDim.x * blockDim.x)
+
+// Element offset of index g along `dim` on line `line` (the compact kernels'
+// line numbering: the other two indices, lower dimension fastest).
+__device__ __forceinline__ int64_t line_elem(int dim, int nx, int ny, int64_t sy, int64_t sz, int g, int line) {
+    if (dim == 0) {
+        const int j = line % ny, k = line / ny;
+        return g + j * sy + k * sz;
+    }
+    if (dim == 1) {
+        const int i = line % nx, k = line / nx;
+        return i + (int64_t)g * sy + k * sz;
+    }
+    const int i = line % nx, j = line / nx;
+    return i + j * sy + (int64_t)g * sz;
+}
+
+// pack: lo[c][p][l] = f[c][p], hi[c][p][l] = f[c][n-M+p];
+// unpack: f[c][-M+p] = lo[c][p][l], f[c][n+p] = hi[c][p][l].
+template <typename T>
+__global__ void k_split_halo(T* __restrict__ f, FieldView v, T* __restrict__ lo, T* __restrict__ hi, int dim, int nx,
+                             int ny, int n, int M, int lines, int count, int lo_on, int hi_on, int pack) {
+    const int64_t total = (int64_t)count * M * lines;
+    GRID_STRIDE(idx, total) {
+        const int line = (int)(idx % lines);
+        const int64_t r = idx / lines;
+        const int p = (int)(r % M);
+        const int64_t comp = r / M;
+        T* fc = f + comp * v.comp_stride;
+        if (pack) {
+            if (lo_on) lo[idx] = fc[line_elem(dim, nx, ny, v.sy, v.sz, p, line)];
+            if (hi_on) hi[idx] = fc[line_elem(dim, nx, ny, v.sy, v.sz, n - M + p, line)];
+        } else {
+            if (lo_on) fc[line_elem(dim, nx, ny, v.sy, v.sz, p - M, line)] = lo[idx];
+            if (hi_on) fc[line_elem(dim, nx, ny, v.sy, v.sz, n + p, line)] = hi[idx];
+        }
+    }
+}
+
+// z[c][r][l] = sum_j Gsel[r][j] * y_all[j] with y_all[2q*rank + k] =
+// gath[rank][c][k][l] (src/tridiag.jl:150-159: gather, then ldiv! of the
+// reduced system; only the 2q unknowns this rank needs are formed).
+template <typename T>
+__global__ void k_split_reduce(const T* __restrict__ gath, const T* __restrict__ Gs, T* __restrict__ z, int lines,
+                               int count, int q, int ranks) {
+    const int m2 = 2 * q, N = m2 * ranks;
+    const int64_t total = (int64_t)count * lines;
+    GRID_STRIDE(idx, total) {
+        const int line = (int)(idx % lines);
+        const int64_t comp = idx / lines;
+        for (int r = 0; r < m2; ++r) {
+            const T* g = Gs + (int64_t)r * N;
+            T acc = T(0);
+            for (int rr = 0; rr < ranks; ++rr)
+                for (int k = 0; k < m2; ++k)
+                    acc += g[m2 * rr + k] * gath[((int64_t)(rr * count + comp) * m2 + k) * lines + line];
+            z[(comp * m2 + r) * lines + line] = acc;
+        }
+    }
+}
+
+// out -= V[:, g] z_prev + W[:, g] z_next (src/tridiag.jl:161-169,
+// src/banded.jl:201-214).
+template <typename T, int Q>
+__global__ void k_split_correct(T* __restrict__ out, FieldView v, const T* __restrict__ V, const T* __restrict__ W,
+                                const T* __restrict__ z, int dim, int nx, int ny, int n, int lines, int64_t cells,
+                                int count) {
+    const int64_t total = (int64_t)count * cells;
+    GRID_STRIDE(idx, total) {
+        const int64_t c = idx % cells;
+        const int64_t comp = idx / cells;
+        const int i = (int)(c % nx);
+        const int64_t jk = c / nx;
+        const int j = (int)(jk % ny), k = (int)(jk / ny);
+        int g, line;
+        if (dim == 0) { g = i; line = j + k * ny; }
+        else if (dim == 1) { g = j; line = i + k * nx; }
+        else { g = k; line = i + j * nx; }
+        const T* zl = z + comp * 2 * Q * lines + line;
+        T acc = T(0);
+#pragma unroll
+        for (int t = 0; t < Q; ++t)
+            acc += V[t * n + g] * zl[(int64_t)t * lines] + W[t * n + g] * zl[(int64_t)(Q + t) * lines];
+        T* o = out + comp * v.comp_stride + i + j * v.sy + k * v.sz;
+        *o = *o - acc;
+    }
+}
+
+template <typename T>
+void halo_t(const SplitPlan& sp, const FieldView& f, void* lo, void* hi, int count, bool pack, cudaStream_t st) {
+    const int64_t total = (int64_t)count * sp.M * sp.lines;
+    k_split_halo<T><<<grid_for(total), kThreads, 0, st>>>(static_cast<T*>(f.base), f, static_cast<T*>(lo),
+                                                          static_cast<T*>(hi), sp.dim, sp.n3[0], sp.n3[1], sp.n,
+                                                          sp.M, (int)sp.lines, count, sp.lo_open ? 1 : 0,
+                                                          sp.hi_open ? 1 : 0, pack ? 1 : 0);
+    count_launch();
+    check_launch("k_split_halo");
+}
+
+template <typename T>
+void correct_t(const SplitPlan& sp, const void* gathered, void* zbuf, const FieldView& out, int count,
+               cudaStream_t st) {
+    const T* tab = static_cast<const T*>(sp.tab);
+    const int64_t nv = (int64_t)sp.q * sp.n;
+    const T* V = tab;
+    const T* W = tab + nv;
+    const T* Gs = tab + 2 * nv;
+    const int64_t nl = (int64_t)count * sp.lines;
+    k_split_reduce<T><<<grid_for(nl), kThreads, 0, st>>>(static_cast<const T*>(gathered), Gs, static_cast<T*>(zbuf),
+                                                         (int)sp.lines, count, sp.q, sp.ranks);
+    count_launch();
+    check_launch("k_split_reduce");
+    const int64_t cells = (int64_t)sp.n3[0] * sp.n3[1] * sp.n3[2];
+    const int64_t total = (int64_t)count * cells;
+    if (sp.q == 1)
+        k_split_correct<T, 1><<<grid_for(total), kThreads, 0, st>>>(static_cast<T*>(out.base), out, V, W,
+                                                                    static_cast<const T*>(zbuf), sp.dim, sp.n3[0],
+                                                                    sp.n3[1], sp.n, (int)sp.lines, cells, count);
+    else
+        k_split_correct<T, 2><<<grid_for(total), kThreads, 0, st>>>(static_cast<T*>(out.base), out, V, W,
+                                                                    static_cast<const T*>(zbuf), sp.dim, sp.n3[0],
+                                                                    sp.n3[1], sp.n, (int)sp.lines, cells, count);
+    count_launch();
+    check_launch("k_split_correct");
+}
+
+}  // namespace
+
+void split_halo(const SplitPlan& sp, const FieldView& f, void* lo, void* hi, int count, bool pack, cudaStream_t st) {
+    if (count <= 0 || sp.lines == 0 || (!sp.lo_open && !sp.hi_open)) return;
+    if (sp.dtype == CLES_F64) halo_t<double>(sp, f, lo, hi, count, pack, st);
+    else halo_t<float>(sp, f, lo, hi, count, pack, st);
+}
+
+void split_correct(const SplitPlan& sp, const void* gathered, void* zbuf, const FieldView& out, int count,
+                   cudaStream_t st) {
+    if (count <= 0 || sp.lines == 0 || (!sp.lo_open && !sp.hi_open)) return;
+    if (sp.dtype == CLES_F64) correct_t<double>(sp, gathered, zbuf, out, count, st);
+    else correct_t<float>(sp, gathered, zbuf, out, count, st);
+}
+
+}  // namespace cles

@@ -182,6 +182,67 @@ int  cles_apply_along_batch(cles_plan* plan, const void* f_dev, void* out_dev,
  * plan-owned device memory).  Float64 padded or interior per the plan. */
 int  cles_apply_along_host(cles_plan* plan, const void* f_host, void* out_host);
 
+/* ---- lines split across ranks -------------------------------------------
+ * The reference's decomposed operator: plan_direction on a Decomp with P > 1
+ * ranks along `dim` (src/operators.jl:44-101, src/tridiag.jl:85-123,
+ * src/banded.jl:108-169) and apply_along! over it (src/operators.jl:199-215,
+ * src/tridiag.jl:136-170, src/banded.jl:177-214), one process per GPU.  The
+ * library does the arithmetic; the caller moves the data between ranks at
+ * the two points the reference calls MPI: the halo Sendrecv!
+ * (src/halo.jl:143-194) and the Allgather! of the interface values
+ * (src/tridiag.jl:148).  One application on rank r:
+ *   cles_split_halo_pack(f -> send_lo, send_hi)
+ *   send send_hi to rank `next` and send_lo to rank `prev`; receive recv_lo
+ *     from `prev` (its send_hi) and recv_hi from `next` (its send_lo)
+ *   cles_split_halo_unpack(recv_lo, recv_hi -> halo of f)
+ *   cles_split_apply_begin(f -> out, iface)
+ *   all-gather iface from every rank along dim, in rank order -> iface_all
+ *   cles_split_apply_end(iface_all -> out)
+ * Plan creation needs no exchange: every rank rebuilds every rank's local
+ * factorisation (the reference all-gathers the spike end values instead).
+ * Fields are padded (n_halo >= the scheme's M on every active dimension);
+ * only the halo planes beyond this rank's open ends are read.  Folds are not
+ * supported on a split dimension. */
+typedef struct cles_split_plan cles_split_plan;
+typedef struct cles_split_desc {
+    int n_local[3];   /* this rank's interior extents (Decomp n_local) */
+    int n_halo;       /* halo width of the padded fields */
+    int dim;          /* split dimension, 1-based */
+    int n_global;     /* global extent along dim */
+    int ranks;        /* ranks along dim */
+    int rank;         /* this rank's coordinate along dim, 0-based */
+    int periodic;     /* the global line wraps */
+} cles_split_desc;
+typedef struct cles_split_info {
+    int64_t halo_elems;   /* elements per field of each of send_lo/send_hi/recv_lo/recv_hi: M x lines */
+    int64_t iface_elems;  /* elements per field of iface: 2q x lines (iface_all holds ranks x count x this) */
+    int64_t field_elems;  /* elements of one padded field */
+    int prev, next;       /* neighbouring rank coordinates along dim, -1 for none */
+    int ranks, q, M;
+} cles_split_info;
+int  cles_split_plan_create(cles_ctx* ctx, const cles_split_desc* desc, const cles_scheme* scheme, double h,
+                            int dtype, cles_split_plan** out);
+void cles_split_plan_destroy(cles_split_plan* plan);
+int  cles_split_plan_info(const cles_split_plan* plan, cles_split_info* out);
+/* Buffers are DEVICE pointers; `count` fields spaced field_stride elements
+ * apart (the padded field size for count = 1); halo and iface buffers hold
+ * `count` consecutive blocks of the per-field sizes in cles_split_info.
+ * Buffers of an end without a neighbour are neither read nor written (pass
+ * NULL). */
+int  cles_split_halo_pack(cles_split_plan* plan, const void* f_dev, void* send_lo, void* send_hi, int count,
+                          int64_t field_stride);
+int  cles_split_halo_unpack(cles_split_plan* plan, const void* recv_lo, const void* recv_hi, void* f_dev, int count,
+                            int64_t field_stride);
+/* Local solve: out = this rank's rows of the line solved with its own
+ * factorisation (the halo of f beyond an open end must be current), iface =
+ * each line's first and last q values of that solution.  out may equal f. */
+int  cles_split_apply_begin(cles_split_plan* plan, const void* f_dev, void* out_dev, void* iface, int count,
+                            int64_t field_stride);
+/* Correction from every rank's iface (iface_all, rank-major): out becomes the
+ * interior of apply_along!(out, plan, f, decomp). */
+int  cles_split_apply_end(cles_split_plan* plan, const void* iface_all, void* out_dev, int count,
+                          int64_t field_stride);
+
 /* ---- solver -------------------------------------------------------------- */
 
 /* StepControl (src/stepcontrol.jl:116-136). */
