@@ -219,7 +219,12 @@ int take_device_timeouts(cudaStream_t st);
 // Launch the operator over `count` fields of `in` into `out` (may alias).
 void launch_compact(const CompactPlan& plan, const FieldView& in, const FieldView& out, int count, int mode,
                     cudaStream_t st);
-// Local solve of a split-line plan (generic kernel, OUT_STORE); the first and
+// y/z lines of a split-line plan in the general tile form, the TMA box
+// widened by the M halo rows at each end; false (nothing launched) when the
+// plan or the views do not qualify.
+bool try_launch_tg_split(const CompactPlan& plan, const FieldView& in, const FieldView& out, int count, void* iface,
+                         cudaStream_t st);
+// Local solve of a split-line plan (tile or generic kernel, OUT_STORE); the first and
 // last q values of every line's local solution also go to iface, laid out
 // [count][2q][lines] in the plan's dtype.
 void launch_compact_split(const CompactPlan& plan, const FieldView& in, const FieldView& out, int count, void* iface,

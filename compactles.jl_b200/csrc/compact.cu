@@ -613,6 +613,7 @@ void launch_compact(const CompactPlan& plan, const FieldView& in, const FieldVie
 void launch_compact_split(const CompactPlan& plan, const FieldView& in, const FieldView& out, int count, void* iface,
                           cudaStream_t st) {
     if (count <= 0 || plan.P.lines == 0) return;
+    if (try_launch_tg_split(plan, in, out, count, iface, st)) return;
     if (plan.dtype == CLES_F64)
         dispatch<double>(plan.P, plan.tab64, in, out, count, OUT_STORE, st, static_cast<double*>(iface));
     else

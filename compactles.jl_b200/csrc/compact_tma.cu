@@ -389,12 +389,15 @@ template <typename T, int Q, int M, int MS>
 __global__ void __launch_bounds__(256, 1)
     k_compact_tg(const __grid_constant__ CUtensorMap map, const __grid_constant__ CompactParams P,
                  const __grid_constant__ TileGenParams GP, const T* __restrict__ tab, const FieldView out,
-                 const int mode, const int count, const int NS, const RkEpilogue rk) {
+                 const int mode, const int count, const int NS, const RkEpilogue rk, const int H,
+                 T* __restrict__ iface) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     const int n = P.n, S = P.S;
     constexpr int m = MS;  // points per segment (all segments equal at launch)
     const int N = 2 * Q * S;
-    const size_t tile_elems = (size_t)n * kLanes;
+    // a split line's tile also holds the H = M halo rows beyond each end
+    // (tile row g + H is line index g, g in [-H, n + H))
+    const size_t tile_elems = (size_t)(n + 2 * H) * kLanes;
     T* tiles = reinterpret_cast<T*>(smem_raw);
     uint64_t* bars = reinterpret_cast<uint64_t*>(smem_raw + sizeof(T) * tile_elems * NS);
     T* red = reinterpret_cast<T*>(bars + 8);
@@ -460,8 +463,9 @@ __global__ void __launch_bounds__(256, 1)
             for (int j = 0; j < MS + 2 * M; ++j) {
                 int g = off - M + j;
                 if (periodic) g = g < 0 ? g + n : (g >= n ? g - n : g);
-                else g = g < 0 ? 0 : (g >= n ? n - 1 : g);  // clamped values are never used
-                wv[j] = tile[g * kLanes + lane];
+                // clamped values are never used; an open end reads its halo row
+                else g = g < 0 ? (P.lo_open ? g : 0) : (g >= n ? (P.hi_open ? g : n - 1) : g);
+                wv[j] = tile[(g + H) * kLanes + lane];
             }
 #pragma unroll
             for (int i = 0; i < MS; ++i) {
@@ -478,29 +482,28 @@ __global__ void __launch_bounds__(256, 1)
                 y[i] = acc;
             }
         }
-        if (!periodic) {
-            if (seg == 0) {
+        if (P.lo_closed && seg == 0) {
 #pragma unroll
-                for (int i = 0; i < kMaxClo; ++i) {
-                    if (i < P.nc) {
-                        T acc = T(0);
+            for (int i = 0; i < kMaxClo; ++i) {
+                if (i < P.nc) {
+                    T acc = T(0);
 #pragma unroll
-                        for (int k = 0; k < kMaxCloLen; ++k)
-                            if (k < P.clo_len[i]) acc += T(P.clo[i][k]) * tile[k * kLanes + lane];
-                        y[i] = acc;
-                    }
+                    for (int k = 0; k < kMaxCloLen; ++k)
+                        if (k < P.clo_len[i]) acc += T(P.clo[i][k]) * tile[(k + H) * kLanes + lane];
+                    y[i] = acc;
                 }
             }
-            if (seg == S - 1) {
+        }
+        if (P.hi_closed && seg == S - 1) {
 #pragma unroll
-                for (int i = MS - kMaxClo; i < MS; ++i) {
-                    if (i >= m - P.nc) {
-                        T acc = T(0);
+            for (int i = MS - kMaxClo; i < MS; ++i) {
+                if (i >= m - P.nc) {
+                    T acc = T(0);
 #pragma unroll
-                        for (int k = 0; k < kMaxCloLen; ++k)
-                            if (k < P.clo_len[m - 1 - i]) acc += T(P.chi[m - 1 - i][k]) * tile[(n - 1 - k) * kLanes + lane];
-                        y[i] = acc;
-                    }
+                    for (int k = 0; k < kMaxCloLen; ++k)
+                        if (k < P.clo_len[m - 1 - i])
+                            acc += T(P.chi[m - 1 - i][k]) * tile[(n - 1 - k + H) * kLanes + lane];
+                    y[i] = acc;
                 }
             }
         }
@@ -529,6 +532,18 @@ __global__ void __launch_bounds__(256, 1)
         // ---- store ----
         const int c = w / groups, g = w - (w / groups) * groups;
         const int x = (g % gx) * kLanes + lane, o = g / gx;
+        if (iface && x < P.nx) {
+            // a split line's local heads and tails: [comp][2q][lines], line = x + o nx
+            T* ifc = iface + (int64_t)c * 2 * Q * P.lines + x + (int64_t)o * P.nx;
+            if (seg == 0) {
+#pragma unroll
+                for (int t = 0; t < Q; ++t) ifc[(int64_t)t * P.lines] = y[t];
+            }
+            if (seg == S - 1) {
+#pragma unroll
+                for (int t = 0; t < Q; ++t) ifc[(int64_t)(Q + t) * P.lines] = y[MS - Q + t];
+            }
+        }
         if (x < P.nx) {
             T* base = reinterpret_cast<T*>(out.base) + (int64_t)c * out.comp_stride + x;
             int64_t st, ob;
@@ -816,11 +831,11 @@ bool launch_tma_m(const CompactPlan& plan, const CUtensorMap& map, const FieldVi
 
 template <typename T, int Q, int M, int MS>
 void launch_tg_ms(const CompactPlan& plan, const CUtensorMap& map, const FieldView& out, int count, int mode,
-                  cudaStream_t st, const T* tab, const RkEpilogue& rk) {
+                  cudaStream_t st, const T* tab, const RkEpilogue& rk, int H, T* iface) {
     const CompactParams& P = plan.P;
     const int NS = sizeof(T) == 8 ? 3 : 4;
     const int N = 2 * Q * P.S;
-    const size_t smem = sizeof(T) * (size_t)P.n * kLanes * NS + 8 * sizeof(uint64_t) +
+    const size_t smem = sizeof(T) * (size_t)(P.n + 2 * H) * kLanes * NS + 8 * sizeof(uint64_t) +
                         sizeof(T) * ((size_t)kLanes * (N + 1) + (size_t)N * N);
     auto kern = k_compact_tg<T, Q, M, MS>;
     static int configured = 0;
@@ -835,31 +850,38 @@ void launch_tg_ms(const CompactPlan& plan, const CUtensorMap& map, const FieldVi
     }
     const int gx = (P.nx + kLanes - 1) / kLanes;
     const int work = gx * (P.dim == 1 ? P.nz : P.ny) * count;
-    const int grid = work < g_num_sms ? work : g_num_sms;
-    kern<<<grid, kLanes * P.S, smem, st>>>(map, P, plan.TG, tab, out, mode, count, NS, rk);
+    // lines of fewer than 8 segments leave an SM with few warps: run as many
+    // persistent CTAs per SM as shared memory and 256 threads per SM-slot allow
+    int per_sm = 256 / (kLanes * P.S);
+    const int by_smem = (int)((227 * 1024) / (smem + 1024));
+    if (per_sm > by_smem) per_sm = by_smem;
+    if (per_sm < 1) per_sm = 1;
+    const int slots = g_num_sms * per_sm;
+    const int grid = work < slots ? work : slots;
+    kern<<<grid, kLanes * P.S, smem, st>>>(map, P, plan.TG, tab, out, mode, count, NS, rk, H, iface);
     count_launch();
     check_launch("k_compact_tg");
 }
 
 template <typename T>
 bool launch_tg(const CompactPlan& plan, const CUtensorMap& map, const FieldView& out, int count, int mode,
-               cudaStream_t st, const T* tab, const RkEpilogue& rk) {
+               cudaStream_t st, const T* tab, const RkEpilogue& rk, int H = 0, T* iface = nullptr) {
     const CompactParams& P = plan.P;
     const bool m32 = P.seg_base == 32;
     if (P.q == 1) {
         switch (P.M) {
-            case 1: m32 ? launch_tg_ms<T, 1, 1, 32>(plan, map, out, count, mode, st, tab, rk)
-                        : launch_tg_ms<T, 1, 1, 16>(plan, map, out, count, mode, st, tab, rk); return true;
-            case 2: m32 ? launch_tg_ms<T, 1, 2, 32>(plan, map, out, count, mode, st, tab, rk)
-                        : launch_tg_ms<T, 1, 2, 16>(plan, map, out, count, mode, st, tab, rk); return true;
-            case 4: m32 ? launch_tg_ms<T, 1, 4, 32>(plan, map, out, count, mode, st, tab, rk)
-                        : launch_tg_ms<T, 1, 4, 16>(plan, map, out, count, mode, st, tab, rk); return true;
+            case 1: m32 ? launch_tg_ms<T, 1, 1, 32>(plan, map, out, count, mode, st, tab, rk, H, iface)
+                        : launch_tg_ms<T, 1, 1, 16>(plan, map, out, count, mode, st, tab, rk, H, iface); return true;
+            case 2: m32 ? launch_tg_ms<T, 1, 2, 32>(plan, map, out, count, mode, st, tab, rk, H, iface)
+                        : launch_tg_ms<T, 1, 2, 16>(plan, map, out, count, mode, st, tab, rk, H, iface); return true;
+            case 4: m32 ? launch_tg_ms<T, 1, 4, 32>(plan, map, out, count, mode, st, tab, rk, H, iface)
+                        : launch_tg_ms<T, 1, 4, 16>(plan, map, out, count, mode, st, tab, rk, H, iface); return true;
             default: return false;
         }
     }
     if (P.q == 2 && P.M == 3) {
-        m32 ? launch_tg_ms<T, 2, 3, 32>(plan, map, out, count, mode, st, tab, rk)
-            : launch_tg_ms<T, 2, 3, 16>(plan, map, out, count, mode, st, tab, rk);
+        m32 ? launch_tg_ms<T, 2, 3, 32>(plan, map, out, count, mode, st, tab, rk, H, iface)
+            : launch_tg_ms<T, 2, 3, 16>(plan, map, out, count, mode, st, tab, rk, H, iface);
         return true;
     }
     return false;
@@ -920,6 +942,7 @@ bool launch_xt(const CompactPlan& plan, const FieldView& in, const FieldView& ou
 bool try_launch_xt(const CompactPlan& plan, const FieldView& in, const FieldView& out, int count, int mode,
                    cudaStream_t st) {
     if (!plan.has_tg || plan.P.dim != 0 || mode == OUT_RK) return false;
+    if (plan.P.lo_open || plan.P.hi_open) return false;   // halo rows are not staged here
     const CompactParams& P = plan.P;
     if (P.n > 256 || P.S * kLanes > 256) return false;
     // a persistent CTA holds ~200 KB of shared memory: worth it only when the
@@ -939,6 +962,7 @@ bool try_launch_tma(const CompactPlan& plan, const FieldView& in, const FieldVie
     if (rkp) rk = *rkp;
     if (mode == OUT_RK && !rkp) return false;
     if (!plan.has_tl && !plan.has_tg) return false;
+    if (plan.P.lo_open || plan.P.hi_open) return false;   // split lines: try_launch_tg_split
     const CompactParams& P = plan.P;
     // 16-point segments run 16 warps per line group (512 threads), 32-point ones 8
     const int max_threads = plan.has_tl && plan.TL.m == 16 ? 512 : 256;
@@ -979,6 +1003,43 @@ bool try_launch_tma(const CompactPlan& plan, const FieldView& in, const FieldVie
     if (M == 1) return launch_tma_m<float, 1>(plan, map, out, count, mode, st, G, rk);
     if (M == 2) return launch_tma_m<float, 2>(plan, map, out, count, mode, st, G, rk);
     return launch_tma_m<float, 4>(plan, map, out, count, mode, st, G, rk);
+}
+
+bool try_launch_tg_split(const CompactPlan& plan, const FieldView& in, const FieldView& out, int count, void* iface,
+                         cudaStream_t st) {
+    if (!plan.has_tg) return false;
+    const CompactParams& P = plan.P;
+    if (P.dim == 0 || P.S * kLanes > 256) return false;
+    // the box covers the line and the M halo rows beyond each end (both ends,
+    // so the tile layout does not depend on which end is open)
+    const int H = (P.lo_open || P.hi_open) ? P.M : 0;
+    const int rows = P.n + 2 * H;
+    if (rows > 256) return false;   // TMA box extent limit
+    const int64_t gx = (P.nx + kLanes - 1) / kLanes;
+    if (gx * (P.dim == 1 ? P.nz : P.ny) * count < num_sms()) return false;
+    PFN_cuTensorMapEncodeTiled_v12000 enc = encode_fn();
+    if (!enc) return false;
+    const size_t el = plan.dtype == CLES_F64 ? 8 : 4;
+    if ((uintptr_t)in.base % 16 || (in.sy * el) % 16 || (in.sz * el) % 16 || (in.comp_stride * el) % 16) return false;
+    const int64_t lstride = P.dim == 1 ? in.sy : in.sz;
+    if (in.comp_stride < (int64_t)(P.nz + (P.dim == 2 ? 2 * H : 0)) * in.sz) return false;
+    // the map starts H planes before the interior along the line: every box
+    // starts at line coordinate 0, x at a multiple of 32
+    void* base = const_cast<char*>(reinterpret_cast<const char*>(in.base)) - (int64_t)H * lstride * (int64_t)el;
+    CUtensorMap map;
+    cuuint64_t dims[4] = {(cuuint64_t)P.nx, (cuuint64_t)(P.ny + (P.dim == 1 ? 2 * H : 0)),
+                          (cuuint64_t)(P.nz + (P.dim == 2 ? 2 * H : 0)), (cuuint64_t)count};
+    cuuint64_t strides[3] = {(cuuint64_t)(in.sy * el), (cuuint64_t)(in.sz * el), (cuuint64_t)(in.comp_stride * el)};
+    cuuint32_t box[4] = {(cuuint32_t)kLanes, (cuuint32_t)(P.dim == 1 ? rows : 1), (cuuint32_t)(P.dim == 2 ? rows : 1), 1};
+    cuuint32_t estr[4] = {1, 1, 1, 1};
+    CUresult r = enc(&map, plan.dtype == CLES_F64 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4,
+                     base, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                     CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return false;
+    const RkEpilogue rk{nullptr, nullptr, 0.0, 0.0, 0.0, nullptr};
+    if (plan.dtype == CLES_F64)
+        return launch_tg<double>(plan, map, out, count, OUT_STORE, st, plan.tab64, rk, H, static_cast<double*>(iface));
+    return launch_tg<float>(plan, map, out, count, OUT_STORE, st, plan.tab32, rk, H, static_cast<float*>(iface));
 }
 
 bool launch_compact_rk(const CompactPlan& plan, const FieldView& in, const FieldView& out, int count,

@@ -604,7 +604,7 @@ void build_compact_plan(CompactPlan& plan, const cles_scheme& s, const int n3[3]
     // pentadiagonal; y/z lines by TMA tiles, x lines by cp.async transposed
     // tiles): equal segments of 16 or 32 points, at most 8 per line
     plan.has_tg = false;
-    if (with_g && !lo_open && !hi_open && P.seg_rem == 0 && (P.seg_base == 16 || P.seg_base == 32) && S * 32 <= 256 && n <= 256 &&
+    if (with_g && P.seg_rem == 0 && (P.seg_base == 16 || P.seg_base == 32) && S * 32 <= 256 && n <= 256 &&
         ((q == 1 && (M == 1 || M == 2 || M == 4)) || (q == 2 && M == 3))) {
         TileGenParams& G = plan.TG;
         std::memset(&G, 0, sizeof(G));

@@ -18,6 +18,8 @@
 // The two exchange points are the reference's Sendrecv! halo exchange and its
 // Allgather! of the interface values; nothing here waits on another rank.
 
+#include <algorithm>
+
 #include "cles_internal.h"
 
 namespace cles {
@@ -95,29 +97,58 @@ __global__ void k_split_reduce(const T* __restrict__ gath, const T* __restrict__
 }
 
 // out -= V[:, g] z_prev + W[:, g] z_next (src/tridiag.jl:161-169,
-// src/banded.jl:201-214).
+// src/banded.jl:201-214).  Rows (j, k, comp) are taken RB at a time per
+// block-stride step, threads along x: coalesced, no 64-bit division per
+// element, and RB loads in flight per thread before the stores.
+constexpr int RB = 4;
+
+template <typename T, int Q>
+__device__ __forceinline__ void correct_coeffs(const T* __restrict__ V, const T* __restrict__ W,
+                                               const T* __restrict__ z, int dim, int nx, int ny, int nz, int n,
+                                               int lines, int row, int i, T* vg, T* wg, const T*& zl) {
+    const int j = row % ny;
+    const int kc = row / ny;
+    const int k = kc % nz, comp = kc / nz;
+    const T* zc = z + (int64_t)comp * 2 * Q * lines;
+    int g, line;
+    if (dim == 0) { g = i; line = j + k * ny; }
+    else if (dim == 1) { g = j; line = i + k * nx; }
+    else { g = k; line = i + j * nx; }
+#pragma unroll
+    for (int t = 0; t < Q; ++t) { vg[t] = V[t * n + g]; wg[t] = W[t * n + g]; }
+    zl = zc + line;
+}
+
 template <typename T, int Q>
 __global__ void k_split_correct(T* __restrict__ out, FieldView v, const T* __restrict__ V, const T* __restrict__ W,
-                                const T* __restrict__ z, int dim, int nx, int ny, int n, int lines, int64_t cells,
+                                const T* __restrict__ z, int dim, int nx, int ny, int nz, int n, int lines,
                                 int count) {
-    const int64_t total = (int64_t)count * cells;
-    GRID_STRIDE(idx, total) {
-        const int64_t c = idx % cells;
-        const int64_t comp = idx / cells;
-        const int i = (int)(c % nx);
-        const int64_t jk = c / nx;
-        const int j = (int)(jk % ny), k = (int)(jk / ny);
-        int g, line;
-        if (dim == 0) { g = i; line = j + k * ny; }
-        else if (dim == 1) { g = j; line = i + k * nx; }
-        else { g = k; line = i + j * nx; }
-        const T* zl = z + comp * 2 * Q * lines + line;
-        T acc = T(0);
+    const int rows = ny * nz * count;
+    for (int r0 = blockIdx.x * RB; r0 < rows; r0 += gridDim.x * RB) {
+        for (int i = threadIdx.x; i < nx; i += blockDim.x) {
+            T o[RB], acc[RB];
+            T* po[RB];
 #pragma unroll
-        for (int t = 0; t < Q; ++t)
-            acc += V[t * n + g] * zl[(int64_t)t * lines] + W[t * n + g] * zl[(int64_t)(Q + t) * lines];
-        T* o = out + comp * v.comp_stride + i + j * v.sy + k * v.sz;
-        *o = *o - acc;
+            for (int b = 0; b < RB; ++b) {
+                const int row = r0 + b;
+                po[b] = nullptr;
+                acc[b] = T(0);
+                if (row < rows) {
+                    const int j = row % ny, kc = row / ny;
+                    const int k = kc % nz, comp = kc / nz;
+                    po[b] = out + (int64_t)comp * v.comp_stride + j * v.sy + k * v.sz + i;
+                    o[b] = *po[b];
+                    T vg[Q], wg[Q];
+                    const T* zl;
+                    correct_coeffs<T, Q>(V, W, z, dim, nx, ny, nz, n, lines, row, i, vg, wg, zl);
+#pragma unroll
+                    for (int t = 0; t < Q; ++t) acc[b] += vg[t] * zl[(int64_t)t * lines] + wg[t] * zl[(int64_t)(Q + t) * lines];
+                }
+            }
+#pragma unroll
+            for (int b = 0; b < RB; ++b)
+                if (po[b]) *po[b] = o[b] - acc[b];
+        }
     }
 }
 
@@ -145,16 +176,17 @@ void correct_t(const SplitPlan& sp, const void* gathered, void* zbuf, const Fiel
                                                          (int)sp.lines, count, sp.q, sp.ranks);
     count_launch();
     check_launch("k_split_reduce");
-    const int64_t cells = (int64_t)sp.n3[0] * sp.n3[1] * sp.n3[2];
-    const int64_t total = (int64_t)count * cells;
+    const int64_t rows = (int64_t)sp.n3[1] * sp.n3[2] * count;
+    if (rows >= ((int64_t)1 << 31)) throw Error(CLES_EINVAL, "too many rows for one correction launch");
+    // a block per x row (threads cover up to 256 x points per step)
+    const int bt = sp.n3[0] >= 256 ? 256 : ((sp.n3[0] + 31) / 32) * 32;
+    const unsigned nb = (unsigned)std::min<int64_t>((rows + RB - 1) / RB, 148 * 64);
     if (sp.q == 1)
-        k_split_correct<T, 1><<<grid_for(total), kThreads, 0, st>>>(static_cast<T*>(out.base), out, V, W,
-                                                                    static_cast<const T*>(zbuf), sp.dim, sp.n3[0],
-                                                                    sp.n3[1], sp.n, (int)sp.lines, cells, count);
+        k_split_correct<T, 1><<<nb, bt, 0, st>>>(static_cast<T*>(out.base), out, V, W, static_cast<const T*>(zbuf),
+                                                 sp.dim, sp.n3[0], sp.n3[1], sp.n3[2], sp.n, (int)sp.lines, count);
     else
-        k_split_correct<T, 2><<<grid_for(total), kThreads, 0, st>>>(static_cast<T*>(out.base), out, V, W,
-                                                                    static_cast<const T*>(zbuf), sp.dim, sp.n3[0],
-                                                                    sp.n3[1], sp.n, (int)sp.lines, cells, count);
+        k_split_correct<T, 2><<<nb, bt, 0, st>>>(static_cast<T*>(out.base), out, V, W, static_cast<const T*>(zbuf),
+                                                 sp.dim, sp.n3[0], sp.n3[1], sp.n3[2], sp.n, (int)sp.lines, count);
     count_launch();
     check_launch("k_split_correct");
 }

@@ -154,6 +154,24 @@ def test_split_long_lines(orc, case):
     assert np.abs(got - ref).max() <= 1e-12 * np.abs(ref).max()
 
 
+@pytest.mark.parametrize("scheme", ["c6", "c10", "filt", "pade"])
+@pytest.mark.parametrize("dim,P", [(2, 2), (3, 4)])
+@pytest.mark.parametrize("periodic", [True, False])
+def test_split_tile_path(orc, scheme, dim, P, periodic):
+    # y/z pieces of equal 32-point segments and enough line groups for the
+    # TMA tile kernel, whose box then also carries the halo rows
+    ng = (64, 256, 80) if dim == 2 else (64, 80, 256)
+    per = tuple(1 if (k != dim - 1 or periodic) else 0 for k in range(3))
+    g = orc.grid(ng, per)
+    f = _field(orc, g, seed=11 + dim)
+    h = 1.0 / 256
+    ref = orc.interior(g, orc.Plan(g, _schemes(orc, scheme), dim, h, P=P).apply(f))
+    got = run_split(f, ng, periodic, dim, P, _schemes(cl, scheme), h)
+    assert np.abs(got - ref).max() <= 1e-12 * np.abs(ref).max()
+    got32 = run_split(f, ng, periodic, dim, P, _schemes(cl, scheme), h, dtype="f32")
+    assert np.abs(got32 - ref).max() <= 2e-6 * np.abs(ref).max()
+
+
 def test_split_batch_of_fields(orc):
     ng, per = (12, 40, 64), (1, 1, 0)
     g = orc.grid(ng, per)
