@@ -611,16 +611,19 @@ __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_gr
 template <typename T, int Q, int M, int MS, int NS>
 __global__ void __launch_bounds__(256, 1)
     k_compact_xt(const __grid_constant__ CompactParams P, const __grid_constant__ TileGenParams GP,
-                 const T* __restrict__ tab, const FieldView in, const FieldView out, const int mode, const int count) {
+                 const T* __restrict__ tab, const FieldView in, const FieldView out, const int mode, const int count,
+                 const int H, T* __restrict__ iface) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     constexpr int TP = kLanes + 1;
     const int n = P.n, S = P.S;
     constexpr int m = MS;
     const int N = 2 * Q * S;
-    const size_t tile_elems = (size_t)n * TP;
+    // input tiles also hold a split line's H = M halo elements beyond each
+    // end (tile row g + H is line index g); the output tile holds the line
+    const size_t tile_elems = (size_t)(n + 2 * H) * TP;
     T* tin = reinterpret_cast<T*>(smem_raw);
     T* tout = tin + tile_elems * NS;
-    T* red = tout + tile_elems;
+    T* red = tout + (size_t)n * TP;
     const int RP = N + 1;
     T* Gs = red + (size_t)kLanes * RP;
 
@@ -654,8 +657,9 @@ __global__ void __launch_bounds__(256, 1)
             for (int l = seg; l < kLanes; l += nwarps) {
                 const int line = g0 + l;
                 if (line >= lines) break;
-                const T* row = base + row_of(in, line);
-                for (int g = lane; g < n; g += kLanes) cp_async_el(dst + (size_t)g * TP + l, row + g, (int)sizeof(T));
+                const T* row = base + row_of(in, line) - H;
+                for (int g = lane; g < n + 2 * H; g += kLanes)
+                    cp_async_el(dst + (size_t)g * TP + l, row + g, (int)sizeof(T));
             }
         }
         cp_async_commit();   // an empty group keeps the count in step
@@ -681,8 +685,8 @@ __global__ void __launch_bounds__(256, 1)
             for (int j = 0; j < MS + 2 * M; ++j) {
                 int g = off - M + j;
                 if (periodic) g = g < 0 ? g + n : (g >= n ? g - n : g);
-                else g = g < 0 ? 0 : (g >= n ? n - 1 : g);
-                wv[j] = tile[g * TP + lane];
+                else g = g < 0 ? (P.lo_open ? g : 0) : (g >= n ? (P.hi_open ? g : n - 1) : g);
+                wv[j] = tile[(g + H) * TP + lane];
             }
 #pragma unroll
             for (int i = 0; i < MS; ++i) {
@@ -699,29 +703,28 @@ __global__ void __launch_bounds__(256, 1)
                 y[i] = acc;
             }
         }
-        if (!periodic) {
-            if (seg == 0) {
+        if (P.lo_closed && seg == 0) {
 #pragma unroll
-                for (int i = 0; i < kMaxClo; ++i) {
-                    if (i < P.nc) {
-                        T acc = T(0);
+            for (int i = 0; i < kMaxClo; ++i) {
+                if (i < P.nc) {
+                    T acc = T(0);
 #pragma unroll
-                        for (int k = 0; k < kMaxCloLen; ++k)
-                            if (k < P.clo_len[i]) acc += T(P.clo[i][k]) * tile[k * TP + lane];
-                        y[i] = acc;
-                    }
+                    for (int k = 0; k < kMaxCloLen; ++k)
+                        if (k < P.clo_len[i]) acc += T(P.clo[i][k]) * tile[(k + H) * TP + lane];
+                    y[i] = acc;
                 }
             }
-            if (seg == S - 1) {
+        }
+        if (P.hi_closed && seg == S - 1) {
 #pragma unroll
-                for (int i = MS - kMaxClo; i < MS; ++i) {
-                    if (i >= m - P.nc) {
-                        T acc = T(0);
+            for (int i = MS - kMaxClo; i < MS; ++i) {
+                if (i >= m - P.nc) {
+                    T acc = T(0);
 #pragma unroll
-                        for (int k = 0; k < kMaxCloLen; ++k)
-                            if (k < P.clo_len[m - 1 - i]) acc += T(P.chi[m - 1 - i][k]) * tile[(n - 1 - k) * TP + lane];
-                        y[i] = acc;
-                    }
+                    for (int k = 0; k < kMaxCloLen; ++k)
+                        if (k < P.clo_len[m - 1 - i])
+                            acc += T(P.chi[m - 1 - i][k]) * tile[(n - 1 - k + H) * TP + lane];
+                    y[i] = acc;
                 }
             }
         }
@@ -742,6 +745,22 @@ __global__ void __launch_bounds__(256, 1)
         if (cls == 0) tg_correct<T, Q, MS, 0>(GP, y, zp, zn);
         else if (cls == 1) tg_correct<T, Q, MS, 1>(GP, y, zp, zn);
         else tg_correct<T, Q, MS, 2>(GP, y, zp, zn);
+        if (iface) {
+            // a split line's local heads and tails: [comp][2q][lines]
+            const int c = w / groups;
+            const int64_t line = (int64_t)(w - c * groups) * kLanes + lane;
+            if (line < lines) {
+                T* ifc = iface + (int64_t)c * 2 * Q * lines + line;
+                if (seg == 0) {
+#pragma unroll
+                    for (int t = 0; t < Q; ++t) ifc[(int64_t)t * lines] = y[t];
+                }
+                if (seg == S - 1) {
+#pragma unroll
+                    for (int t = 0; t < Q; ++t) ifc[(int64_t)(Q + t) * lines] = y[MS - Q + t];
+                }
+            }
+        }
 #pragma unroll
         for (int i = 0; i < MS; ++i) tout[(size_t)(off + i) * TP + lane] = y[i];
         __syncthreads();   // the output tile is complete
@@ -889,11 +908,12 @@ bool launch_tg(const CompactPlan& plan, const CUtensorMap& map, const FieldView&
 
 template <typename T, int Q, int M, int MS>
 void launch_xt_ms(const CompactPlan& plan, const FieldView& in, const FieldView& out, int count, int mode,
-                  cudaStream_t st, const T* tab) {
+                  cudaStream_t st, const T* tab, int H, T* iface) {
     const CompactParams& P = plan.P;
     constexpr int NS = sizeof(T) == 8 ? 2 : 3;
     const int N = 2 * Q * P.S;
-    const size_t smem = sizeof(T) * ((size_t)P.n * (kLanes + 1) * (NS + 1) + (size_t)kLanes * (N + 1) + (size_t)N * N);
+    const size_t smem = sizeof(T) * ((size_t)(P.n + 2 * H) * (kLanes + 1) * NS + (size_t)P.n * (kLanes + 1) +
+                                     (size_t)kLanes * (N + 1) + (size_t)N * N);
     auto kern = k_compact_xt<T, Q, M, MS, NS>;
     static int configured = 0;
     if (configured < (int)smem) {
@@ -907,31 +927,37 @@ void launch_xt_ms(const CompactPlan& plan, const FieldView& in, const FieldView&
     }
     const int64_t groups = (P.lines + kLanes - 1) / kLanes;
     const int64_t work = groups * count;
-    const int grid = work < g_num_sms ? (int)work : g_num_sms;
-    kern<<<grid, kLanes * P.S, smem, st>>>(P, plan.TG, tab, in, out, mode, count);
+    // as k_compact_tg: several persistent CTAs per SM for lines of fewer than 8 segments
+    int per_sm = 256 / (kLanes * P.S);
+    const int by_smem = (int)((227 * 1024) / (smem + 1024));
+    if (per_sm > by_smem) per_sm = by_smem;
+    if (per_sm < 1) per_sm = 1;
+    const int64_t slots = (int64_t)g_num_sms * per_sm;
+    const int grid = (int)(work < slots ? work : slots);
+    kern<<<grid, kLanes * P.S, smem, st>>>(P, plan.TG, tab, in, out, mode, count, H, iface);
     count_launch();
     check_launch("k_compact_xt");
 }
 
 template <typename T>
 bool launch_xt(const CompactPlan& plan, const FieldView& in, const FieldView& out, int count, int mode,
-               cudaStream_t st, const T* tab) {
+               cudaStream_t st, const T* tab, int H = 0, T* iface = nullptr) {
     const CompactParams& P = plan.P;
     const bool m32 = P.seg_base == 32;
     if (P.q == 1) {
         switch (P.M) {
-            case 1: m32 ? launch_xt_ms<T, 1, 1, 32>(plan, in, out, count, mode, st, tab)
-                        : launch_xt_ms<T, 1, 1, 16>(plan, in, out, count, mode, st, tab); return true;
-            case 2: m32 ? launch_xt_ms<T, 1, 2, 32>(plan, in, out, count, mode, st, tab)
-                        : launch_xt_ms<T, 1, 2, 16>(plan, in, out, count, mode, st, tab); return true;
-            case 4: m32 ? launch_xt_ms<T, 1, 4, 32>(plan, in, out, count, mode, st, tab)
-                        : launch_xt_ms<T, 1, 4, 16>(plan, in, out, count, mode, st, tab); return true;
+            case 1: m32 ? launch_xt_ms<T, 1, 1, 32>(plan, in, out, count, mode, st, tab, H, iface)
+                        : launch_xt_ms<T, 1, 1, 16>(plan, in, out, count, mode, st, tab, H, iface); return true;
+            case 2: m32 ? launch_xt_ms<T, 1, 2, 32>(plan, in, out, count, mode, st, tab, H, iface)
+                        : launch_xt_ms<T, 1, 2, 16>(plan, in, out, count, mode, st, tab, H, iface); return true;
+            case 4: m32 ? launch_xt_ms<T, 1, 4, 32>(plan, in, out, count, mode, st, tab, H, iface)
+                        : launch_xt_ms<T, 1, 4, 16>(plan, in, out, count, mode, st, tab, H, iface); return true;
             default: return false;
         }
     }
     if (P.q == 2 && P.M == 3) {
-        m32 ? launch_xt_ms<T, 2, 3, 32>(plan, in, out, count, mode, st, tab)
-            : launch_xt_ms<T, 2, 3, 16>(plan, in, out, count, mode, st, tab);
+        m32 ? launch_xt_ms<T, 2, 3, 32>(plan, in, out, count, mode, st, tab, H, iface)
+            : launch_xt_ms<T, 2, 3, 16>(plan, in, out, count, mode, st, tab, H, iface);
         return true;
     }
     return false;
@@ -1009,7 +1035,18 @@ bool try_launch_tg_split(const CompactPlan& plan, const FieldView& in, const Fie
                          cudaStream_t st) {
     if (!plan.has_tg) return false;
     const CompactParams& P = plan.P;
-    if (P.dim == 0 || P.S * kLanes > 256) return false;
+    if (P.dim == 0) {
+        // x pieces: cp.async rows widened by the M halo elements at each end
+        if (P.n > 256 || P.S * kLanes > 256) return false;
+        if (((P.lines + kLanes - 1) / kLanes) * count < num_sms()) return false;
+        const size_t el = plan.dtype == CLES_F64 ? 8 : 4;
+        if ((uintptr_t)in.base % el || (uintptr_t)out.base % el) return false;
+        const int H = (P.lo_open || P.hi_open) ? P.M : 0;
+        if (plan.dtype == CLES_F64)
+            return launch_xt<double>(plan, in, out, count, OUT_STORE, st, plan.tab64, H, static_cast<double*>(iface));
+        return launch_xt<float>(plan, in, out, count, OUT_STORE, st, plan.tab32, H, static_cast<float*>(iface));
+    }
+    if (P.S * kLanes > 256) return false;
     // the box covers the line and the M halo rows beyond each end (both ends,
     // so the tile layout does not depend on which end is open)
     const int H = (P.lo_open || P.hi_open) ? P.M : 0;

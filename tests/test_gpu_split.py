@@ -155,12 +155,13 @@ def test_split_long_lines(orc, case):
 
 
 @pytest.mark.parametrize("scheme", ["c6", "c10", "filt", "pade"])
-@pytest.mark.parametrize("dim,P", [(2, 2), (3, 4)])
+@pytest.mark.parametrize("dim,P", [(1, 2), (1, 4), (2, 2), (3, 4)])
 @pytest.mark.parametrize("periodic", [True, False])
 def test_split_tile_path(orc, scheme, dim, P, periodic):
-    # y/z pieces of equal 32-point segments and enough line groups for the
-    # TMA tile kernel, whose box then also carries the halo rows
-    ng = (64, 256, 80) if dim == 2 else (64, 80, 256)
+    # pieces of equal 32-point segments and enough line groups for the tile
+    # kernels: y/z through TMA boxes that also carry the halo rows, x through
+    # cp.async rows widened by the halo elements
+    ng = {1: (256, 80, 64), 2: (64, 256, 80), 3: (64, 80, 256)}[dim]
     per = tuple(1 if (k != dim - 1 or periodic) else 0 for k in range(3))
     g = orc.grid(ng, per)
     f = _field(orc, g, seed=11 + dim)
