@@ -401,6 +401,9 @@ void build_compact_plan(CompactPlan& plan, const cles_scheme& s, const int n3[3]
     // latency: they take segments of 8-16 points, more threads per line.
     P.pcr = (!periodic && q == 1) ? 1 : 0;
     int seg_target = kMaxSeg;
+    // a split line's piece of 32 points (or of 16k points, k odd) takes 16-point
+    // segments so that it has equal segments, more than one, for the tile kernels
+    if ((lo_open || hi_open) && n % 16 == 0 && (n == 32 || n % 32 != 0) && n / 16 <= 8) seg_target = 16;
     if (P.pcr && P.lines <= 16) {
         seg_target = 8;
         while (seg_target < kMaxSeg && (n + seg_target - 1) / seg_target > 512) seg_target *= 2;

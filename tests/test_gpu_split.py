@@ -155,12 +155,13 @@ def test_split_long_lines(orc, case):
 
 
 @pytest.mark.parametrize("scheme", ["c6", "c10", "filt", "pade"])
-@pytest.mark.parametrize("dim,P", [(1, 2), (1, 4), (2, 2), (3, 4)])
+@pytest.mark.parametrize("dim,P", [(1, 2), (1, 4), (2, 2), (3, 4), (3, 8)])
 @pytest.mark.parametrize("periodic", [True, False])
 def test_split_tile_path(orc, scheme, dim, P, periodic):
-    # pieces of equal 32-point segments and enough line groups for the tile
-    # kernels: y/z through TMA boxes that also carry the halo rows, x through
-    # cp.async rows widened by the halo elements
+    # pieces of equal 32-point segments (16-point ones for the 32-point pieces
+    # of P = 8) and enough line groups for the tile kernels: y/z through TMA
+    # boxes that also carry the halo rows, x through cp.async rows widened by
+    # the halo elements
     ng = {1: (256, 80, 64), 2: (64, 256, 80), 3: (64, 80, 256)}[dim]
     per = tuple(1 if (k != dim - 1 or periodic) else 0 for k in range(3))
     g = orc.grid(ng, per)
