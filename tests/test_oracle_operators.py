@@ -213,3 +213,38 @@ def test_plan_errors_like_plan_direction(orc):
     with pytest.raises(ValueError, match="too small"):
         orc.Plan(g, orc.compact_filter(0.45), 1, 0.1)
     orc.Plan(g, orc.lele_d1_6(), 1, 0.1)  # 2nc+1 = 5, 2M+1 = 5: fine
+
+
+def _mpi_field(orc, ng, periodic, L, fn):
+    # fillf! on the global grid (nodes at i h, h = L/n periodic, L/(n-1) closed)
+    g = orc.grid(ng, periodic)
+    f = np.zeros(orc.padded_shape(g))
+    xs = []
+    for k in range(3):
+        h = L / ng[k] if periodic[k] else L / (ng[k] - 1)
+        xs.append(np.arange(ng[k]) * h)
+    z, y, x = np.meshgrid(xs[2], xs[1], xs[0], indexing="ij")
+    orc.interior(g, f)[...] = fn(x, y, z)
+    orc.exchange_halos(g, f)
+    return g, f, (x, y, z)
+
+
+@pytest.mark.parametrize("P", [2, 4, 8])
+def test_p_rank_solve_meets_the_reference_mpi_suite(orc, P):
+    # test/mpi_tests.jl:117-192 with its tolerances: sin(3x) cos(2y) on 72
+    # points along the split dimension (16 elsewhere), C6 on x, y, z and C10 on
+    # x, y, periodic; the cubic 1 + 2x + 3x^2 - x^3 between slip walls, C6 and
+    # C10, exact to 1e-9 with x split
+    n = 72
+    fx = lambda x, y, z: np.sin(3 * x) * np.cos(2 * y)
+    for mk, tol, axes in ((orc.lele_d1_6, 1e-4, (1, 2, 3)), (orc.lele_d1_10, 1e-8, (1, 2))):
+        for ax in axes:
+            ng = tuple(n if k == ax - 1 else 16 for k in range(3))
+            g, f, (x, y, z) = _mpi_field(orc, ng, (1, 1, 1), 2 * np.pi, fx)
+            got = orc.interior(g, orc.Plan(g, mk(), ax, 2 * np.pi / n, P=P).apply(f))
+            exact = {1: 3 * np.cos(3 * x) * np.cos(2 * y), 2: -2 * np.sin(3 * x) * np.sin(2 * y), 3: 0 * x}[ax]
+            assert np.abs(got - exact).max() < (1e-10 if ax == 3 else tol), (ax, P)
+    g, f, (x, y, z) = _mpi_field(orc, (n, 12, 12), (0, 1, 1), 1.0, lambda x, y, z: 1 + 2 * x + 3 * x ** 2 - x ** 3)
+    for mk in (orc.lele_d1_6, orc.lele_d1_10):
+        got = orc.interior(g, orc.Plan(g, mk(), 1, 1.0 / (n - 1), P=P).apply(f))
+        assert np.abs(got - (2 + 6 * x - 3 * x ** 2)).max() < 1e-9
