@@ -15,9 +15,11 @@
  * (src/decomposition.jl:129-134): Float64, x fastest, extent n_local[d] +
  * 2*n_halo on every active dimension and 1 on a collapsed one; a conserved
  * state appends the component index as the slowest dimension.  An
- * "interior" field drops the halos (extent n_local[d]).  Halos are never read
- * by this library: periodic lines wrap by index, closed lines use closure
- * rows, exactly the values the reference would read from current halos.
+ * "interior" field drops the halos (extent n_local[d]).  On one rank halos
+ * are never read by this library: periodic lines wrap by index, closed lines
+ * use closure rows, exactly the values the reference would read from current
+ * halos.  The split-line entry points (cles_split_*) read the halo planes
+ * beyond a rank interface, which cles_split_halo_unpack fills.
  *
  * Ownership.  The library allocates and frees its own device memory (plans,
  * solver state, scratch).  Caller buffers (host or device) are never freed or
