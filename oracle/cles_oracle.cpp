@@ -2094,6 +2094,24 @@ orc_solver* orc_solver_create(const cles_solver_desc* d) {
     return new orc_solver{s};
 }
 void orc_solver_destroy(orc_solver* s) { if (s) { delete s->s; delete s; } }
+// The same Solver on a Decomp split `P` ways along `dim` (1-based): the
+// derivative and filter plans along dim emulate P ranks (Decomp dims,
+// src/decomposition.jl:80-122; LineSolver / BandLineSolver with P > 1,
+// src/tridiag.jl:85-170, src/banded.jl:108-214).  Halo exchange needs no
+// emulation: the oracle holds the whole field.  Folded dimensions are refused.
+int orc_solver_split(orc_solver* s, int dim, int P) {
+    Solver& S = *s->s;
+    const int d = dim - 1;
+    if (d < 0 || d > 2 || !S.D.active[d]) { set_err("split dimension must be an active 1, 2 or 3"); return CLES_EINVAL; }
+    if (S.folds[d]) { set_err("folds on a split dimension are not supported"); return CLES_EINVAL; }
+    Plan* dp = plan_create(S.D, S.desc.deriv, d, S.h[d], P);
+    if (!dp) return CLES_EINVAL;
+    Plan* fp = plan_create(S.D, S.desc.filt, d, S.h[d], P);
+    if (!fp) { delete dp; return CLES_EINVAL; }
+    S.dplan[d].reset(dp);
+    S.fplan[d].reset(fp);
+    return 0;
+}
 int64_t orc_field_size(orc_solver* s) { return (int64_t)s->s->fs; }
 int orc_set_state(orc_solver* s, const double* Q) { std::memcpy(s->s->Q.data(), Q, sizeof(double) * s->s->Q.size()); return 0; }
 int orc_get_state(orc_solver* s, double* Q) { std::memcpy(Q, s->s->Q.data(), sizeof(double) * s->s->Q.size()); return 0; }

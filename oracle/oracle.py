@@ -66,6 +66,7 @@ def lib():
         L.orc_exchange_dim.argtypes = [C.POINTER(abi.cles_grid), _DP, C.c_int]
         L.orc_solver_create.restype = C.c_void_p
         L.orc_solver_create.argtypes = [C.POINTER(abi.cles_solver_desc)]
+        L.orc_solver_split.argtypes = [C.c_void_p, C.c_int, C.c_int]
         L.orc_solver_destroy.argtypes = [C.c_void_p]
         L.orc_field_size.restype = C.c_int64
         L.orc_field_size.argtypes = [C.c_void_p]
@@ -260,6 +261,12 @@ class Solver:
         res = abi.cles_run_result()
         rc = lib().orc_run(self.ptr, float(tfinal), int(nmax), C.byref(res))
         return rc, res
+
+    def split(self, dim, P):
+        """Emulate P ranks along dim (1-based) in every compact application along it."""
+        if lib().orc_solver_split(self.ptr, int(dim), int(P)):
+            raise ValueError(_err())
+        return self
 
     def switch_bc(self, dim, side):
         """switch!(::SwitchableBC) on face (dim 1..3, side 1 low / 2 high)."""

@@ -1,0 +1,63 @@
+"""The oracle's solver with a dimension split across emulated ranks
+(orc_solver_split): the reference's MPI-suite check that the artificial
+properties do not depend on the split axis (test/mpi_tests.jl:823-873).
+
+A compressible, vortical field on 72^3 (periodic, [0, 2 pi)^3) is split four
+ways along x, y and z in turn; the whole-domain sum of beta* after one
+compute_rhs! must agree across the three splits to the reference's
+tolerances (strain 1e-10, gated strain 1e-4, dilatation 1e-5, the last two
+set by the switch H(-div u) toggling at points of round-off dilatation), and
+with the undecomposed solve; the three sensors must differ by more than
+0.1 % so the check cannot pass on an ignored beta_sensor.
+
+The spreads come out at the values the reference's comment reports for its
+own runs (2e-6 gated strain, 2e-7 dilatation, round-off for strain): here
+2.5e-6, 1.6e-7 and 1e-15."""
+import numpy as np
+import pytest
+
+import compactles_b200 as cl
+
+N = 72
+TOL = {"strain": 1e-10, "gated_strain": 1e-4, "dilatation": 1e-5}
+
+
+def _ic(x, y, z):
+    return cl.Prim(u=(np.sin(x) * np.cos(y) * np.cos(z), -np.cos(x) * np.sin(y) * np.cos(z), 0.3 * np.sin(2 * z)),
+                   p=1 + 0.2 * np.cos(x) + 0 * y, rho=1 + 0.3 * np.sin(y) + 0 * z)
+
+
+def _beta_total(orc, sensor, split_dim, P=4):
+    d = cl.solver_desc((N, N, N), (2 * np.pi,) * 3, cl.PER3, orc.lele_d1_6(), orc.compact_filter(0.45),
+                       art=cl.ArtParams(enabled=True, beta_sensor=sensor))
+    S = orc.Solver(d)
+    if split_dim:
+        S.split(split_dim, P)
+    S.set_state(cl.initialize(d, _ic))
+    S.compute_rhs()
+    beta = S.field(cl.abi.CLES_FIELD_BETA_ART)[cl.interior_slices(d)]
+    return float(beta.sum())
+
+
+def test_artificial_properties_independent_of_the_split_axis(orc):
+    totals = {}
+    for sensor, tol in TOL.items():
+        sums = [_beta_total(orc, sensor, ax) for ax in (1, 2, 3)]
+        single = _beta_total(orc, sensor, 0)
+        spread = max(sums) - min(sums)
+        assert spread <= tol * max(max(sums), 1e-30), (sensor, sums)
+        assert abs(np.mean(sums) - single) <= tol * max(abs(single), 1e-30), (sensor, sums, single)
+        totals[sensor] = sums[0]
+    for sensor in ("gated_strain", "dilatation"):
+        assert abs(totals["strain"] - totals[sensor]) / totals["strain"] > 1e-3, sensor
+
+
+def test_split_refuses_a_folded_or_collapsed_dimension(orc):
+    d = cl.solver_desc((24, 24, 1), (1.0, 2 * np.pi, 1.0), ((cl.AxisBC(), cl.SlipWallBC()), cl.PER3[1], cl.PER3[2]),
+                       orc.lele_d1_6(), orc.compact_filter(0.45), metric=cl.CylindricalMetric())
+    S = orc.Solver(d)
+    with pytest.raises(ValueError, match="folds"):
+        S.split(1, 2)
+    with pytest.raises(ValueError, match="active"):
+        S.split(3, 2)
+    S.split(2, 2)   # theta (no fold on it) splits
