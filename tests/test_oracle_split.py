@@ -1,6 +1,8 @@
 """The oracle's solver with a dimension split across emulated ranks
-(orc_solver_split): the reference's MPI-suite check that the artificial
-properties do not depend on the split axis (test/mpi_tests.jl:823-873).
+(orc_solver_split), held to the reference's MPI-suite checks: freestream
+preservation and periodic conservation with a dimension split
+(test/mpi_tests.jl:293-366, the fold-free cases), and artificial
+properties that do not depend on the split axis (:823-873).
 
 A compressible, vortical field on 72^3 (periodic, [0, 2 pi)^3) is split four
 ways along x, y and z in turn; the whole-domain sum of beta* after one
@@ -61,3 +63,42 @@ def test_split_refuses_a_folded_or_collapsed_dimension(orc):
     with pytest.raises(ValueError, match="active"):
         S.split(3, 2)
     S.split(2, 2)   # theta (no fold on it) splits
+
+
+@pytest.mark.parametrize("case", ["cartesian_x", "stretched_x", "cylinder_offaxis_theta"])
+@pytest.mark.parametrize("P", [2, 4, 8])
+def test_freestream_preserved_when_split(orc, case, P):
+    # test/mpi_tests.jl:293-334 (the fold-free cases): a uniform state gives
+    # dQ within 1e-8 with the named dimension split
+    PER = (cl.PeriodicBC(), cl.PeriodicBC())
+    WALLS = (cl.SlipWallBC(), cl.SlipWallBC())
+    sch = (orc.lele_d1_6(), orc.compact_filter(0.45))
+    if case == "cartesian_x":
+        d, ax = cl.solver_desc((N, 12, 12), (1.0, 1.0, 1.0), cl.PER3, *sch, art=cl.ArtParams(enabled=False)), 1
+    elif case == "stretched_x":
+        d = cl.solver_desc((N, 12, 12), (1.0, 1.0, 1.0), (WALLS, PER, PER), *sch, art=cl.ArtParams(enabled=False),
+                           stretch=(cl.sine_cluster(0.0, 1.0, 0.5, 0.4), None, None))
+        ax = 1
+    else:
+        d = cl.solver_desc((12, N, 12), (1.0, 2 * np.pi, 0.5), (WALLS, PER, PER), *sch, art=cl.ArtParams(enabled=False),
+                           metric=cl.CylindricalMetric(), origin=(0.2, 0.0, 0.0))
+        ax = 2
+    S = orc.Solver(d).split(ax, P)
+    S.set_state(cl.initialize(d, lambda x, y, z: cl.Prim(u=(0.0 * x, 0.0 * y, 0.0 * z), p=1.0 + 0 * x, rho=1.0 + 0 * x)))
+    S.apply_bcs()
+    dQ = S.compute_rhs()[(slice(None),) + cl.interior_slices(d)]
+    assert np.abs(dQ).max() < 1e-8
+
+
+@pytest.mark.parametrize("P", [2, 4, 8])
+def test_periodic_rhs_conserves_when_split(orc, P):
+    # test/mpi_tests.jl:342-366: the periodic RHS sums to zero over the domain
+    d = cl.solver_desc((N, 16, 16), (2 * np.pi,) * 3, cl.PER3, orc.lele_d1_6(), orc.compact_filter(0.45),
+                       transport=cl.Transport(mu0=1e-3), art=cl.ArtParams(enabled=False))
+    S = orc.Solver(d).split(1, P)
+    S.set_state(cl.initialize(d, lambda x, y, z: cl.Prim(
+        u=(0.1 * np.sin(x) * np.cos(y), -0.1 * np.cos(x) * np.sin(y), 0.05 * np.sin(z)),
+        p=1 + 0.05 * np.cos(x) * np.cos(z), rho=1 + 0.1 * np.sin(y) + 0 * z)))
+    dQ = S.compute_rhs()[(slice(None),) + cl.interior_slices(d)]
+    worst = max(abs(dQ[c].sum()) for c in range(dQ.shape[0]))
+    assert worst < 1e-8 * N * 16 * 16
