@@ -2088,6 +2088,16 @@ void orc_exchange_dim(const cles_grid* g, double* f, int dim) {
     wrap_dim(D, f, dim - 1);
 }
 
+// BandFactor + solve_col! (src/banded.jl:31-80) on one (2q+1) x n band,
+// Ab[(q + t) + (2q+1) i] = A[i, i + t]; b is overwritten with A^-1 b.
+int orc_band_solve(int q, int n, const double* Ab, double* b) {
+    if (q < 1 || n < 1) { set_err("band_solve: q >= 1 and n >= 1"); return CLES_EINVAL; }
+    BandFactor F;
+    F.build(std::vector<double>(Ab, Ab + (size_t)(2 * q + 1) * n), n, q);
+    F.solve(b, 1);
+    return 0;
+}
+
 orc_solver* orc_solver_create(const cles_solver_desc* d) {
     Solver* s = solver_create(*d);
     if (!s) return nullptr;

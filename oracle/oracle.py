@@ -67,6 +67,7 @@ def lib():
         L.orc_solver_create.restype = C.c_void_p
         L.orc_solver_create.argtypes = [C.POINTER(abi.cles_solver_desc)]
         L.orc_solver_split.argtypes = [C.c_void_p, C.c_int, C.c_int]
+        L.orc_band_solve.argtypes = [C.c_int, C.c_int, _DP, _DP]
         L.orc_solver_destroy.argtypes = [C.c_void_p]
         L.orc_field_size.restype = C.c_int64
         L.orc_field_size.argtypes = [C.c_void_p]
@@ -193,6 +194,20 @@ class Plan:
                 self.ptr = None
         except Exception:
             pass
+
+
+def band_solve(A, b, q):
+    """BandFactor(Ab, q) + solve_col! on the dense n x n banded matrix A."""
+    n = A.shape[0]
+    Ab = np.zeros((n, 2 * q + 1))
+    for i in range(n):
+        for t in range(-q, q + 1):
+            if 0 <= i + t < n:
+                Ab[i, q + t] = A[i, i + t]
+    x = np.ascontiguousarray(b, dtype=np.float64).copy()
+    if lib().orc_band_solve(int(q), int(n), np.ascontiguousarray(Ab), x):
+        raise ValueError(_err())
+    return x
 
 
 class Solver:

@@ -248,3 +248,17 @@ def test_p_rank_solve_meets_the_reference_mpi_suite(orc, P):
     for mk in (orc.lele_d1_6, orc.lele_d1_10):
         got = orc.interior(g, orc.Plan(g, mk(), 1, 1.0 / (n - 1), P=P).apply(f))
         assert np.abs(got - (2 + 6 * x - 3 * x ** 2)).max() < 1e-9
+
+
+@pytest.mark.parametrize("q", [1, 2])
+@pytest.mark.parametrize("n", [9, 17])
+def test_banded_lu_matches_dense(orc, q, n):
+    # test/runtests.jl:69-84: a random banded matrix with a dominant diagonal
+    rng = np.random.default_rng(7 + 10 * q + n)
+    A = np.zeros((n, n))
+    for i in range(n):
+        for j in range(max(0, i - q), min(n, i + q + 1)):
+            A[i, j] = (3.0 if i == j else 0.0) + rng.standard_normal()
+    x = rng.standard_normal(n)
+    y = orc.band_solve(A, A @ x, q)
+    assert np.allclose(y, x, atol=1e-9, rtol=1e-9)
