@@ -1,7 +1,9 @@
 """The oracle's solver with a dimension split across emulated ranks
 (orc_solver_split), held to the reference's MPI-suite checks: freestream
-preservation and periodic conservation with a dimension split
-(test/mpi_tests.jl:293-366, the fold-free cases), and artificial
+preservation (Cartesian, stretched, cylinder off-axis and through a
+resolved axis, sphere with origin and poles) and periodic conservation with
+a dimension split (test/mpi_tests.jl:293-366, every case whose split
+dimension carries no fold), and artificial
 properties that do not depend on the split axis (:823-873).
 
 A compressible, vortical field on 72^3 (periodic, [0, 2 pi)^3) is split four
@@ -65,11 +67,12 @@ def test_split_refuses_a_folded_or_collapsed_dimension(orc):
     S.split(2, 2)   # theta (no fold on it) splits
 
 
-@pytest.mark.parametrize("case", ["cartesian_x", "stretched_x", "cylinder_offaxis_theta"])
+@pytest.mark.parametrize("case", ["cartesian_x", "stretched_x", "cylinder_offaxis_theta", "cylinder_axis_theta",
+                                  "sphere_origin_poles_phi"])
 @pytest.mark.parametrize("P", [2, 4, 8])
 def test_freestream_preserved_when_split(orc, case, P):
-    # test/mpi_tests.jl:293-334 (the fold-free cases): a uniform state gives
-    # dQ within 1e-8 with the named dimension split
+    # test/mpi_tests.jl:293-334: a uniform state gives dQ within 1e-8 with the
+    # named dimension split (every case whose split dimension carries no fold)
     PER = (cl.PeriodicBC(), cl.PeriodicBC())
     WALLS = (cl.SlipWallBC(), cl.SlipWallBC())
     sch = (orc.lele_d1_6(), orc.compact_filter(0.45))
@@ -79,10 +82,21 @@ def test_freestream_preserved_when_split(orc, case, P):
         d = cl.solver_desc((N, 12, 12), (1.0, 1.0, 1.0), (WALLS, PER, PER), *sch, art=cl.ArtParams(enabled=False),
                            stretch=(cl.sine_cluster(0.0, 1.0, 0.5, 0.4), None, None))
         ax = 1
-    else:
+    elif case == "cylinder_offaxis_theta":
         d = cl.solver_desc((12, N, 12), (1.0, 2 * np.pi, 0.5), (WALLS, PER, PER), *sch, art=cl.ArtParams(enabled=False),
                            metric=cl.CylindricalMetric(), origin=(0.2, 0.0, 0.0))
         ax = 2
+    elif case == "cylinder_axis_theta":
+        # resolved theta through the axis: the paired fold on r, theta split
+        d = cl.solver_desc((40, N, 1), (1.0, 2 * np.pi, 1.0), ((cl.AxisBC(), cl.SlipWallBC()), PER, PER), *sch,
+                           art=cl.ArtParams(enabled=False), metric=cl.CylindricalMetric())
+        ax = 2
+    else:
+        # origin and poles folded, phi (the origin's pairing dimension) split
+        d = cl.solver_desc((40, 16, N), (1.0, np.pi, 2 * np.pi),
+                           ((cl.OriginBC(), cl.SlipWallBC()), (cl.PoleBC(), cl.PoleBC()), PER), *sch,
+                           art=cl.ArtParams(enabled=False), metric=cl.SphericalMetric())
+        ax = 3
     S = orc.Solver(d).split(ax, P)
     S.set_state(cl.initialize(d, lambda x, y, z: cl.Prim(u=(0.0 * x, 0.0 * y, 0.0 * z), p=1.0 + 0 * x, rho=1.0 + 0 * x)))
     S.apply_bcs()
