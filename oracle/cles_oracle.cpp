@@ -2133,6 +2133,8 @@ int orc_step(orc_solver* s, double dt, int prepared) { step(*s->s, dt, prepared 
 int orc_filter_state(orc_solver* s) { filter_state(*s->s); return 0; }
 int orc_run(orc_solver* s, double tfinal, int64_t nmax, cles_run_result* r) { return run(*s->s, tfinal, nmax, r); }
 double orc_kinetic_energy(orc_solver* s) { return kinetic_energy(*s->s); }
+// volume_integral(solver, f) (src/diagnostics.jl:41-80) of a padded field
+double orc_volume_integral(orc_solver* s, const double* f) { return volume_integral(*s->s, f); }
 double orc_dissipation_rate(orc_solver* s) { return dissipation_rate(*s->s); }
 int orc_get_clock(orc_solver* s, double* t, int64_t* step_, double* cfl) { *t = s->s->t; *step_ = s->s->step; *cfl = s->s->cfl; return 0; }
 int orc_set_clock(orc_solver* s, double t, int64_t step_, double cfl) { s->s->t = t; s->s->step = step_; s->s->cfl = cfl; return 0; }

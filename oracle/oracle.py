@@ -68,6 +68,8 @@ def lib():
         L.orc_solver_create.argtypes = [C.POINTER(abi.cles_solver_desc)]
         L.orc_solver_split.argtypes = [C.c_void_p, C.c_int, C.c_int]
         L.orc_band_solve.argtypes = [C.c_int, C.c_int, _DP, _DP]
+        L.orc_volume_integral.argtypes = [C.c_void_p, _DP]
+        L.orc_volume_integral.restype = C.c_double
         L.orc_solver_destroy.argtypes = [C.c_void_p]
         L.orc_field_size.restype = C.c_int64
         L.orc_field_size.argtypes = [C.c_void_p]
@@ -276,6 +278,13 @@ class Solver:
         res = abi.cles_run_result()
         rc = lib().orc_run(self.ptr, float(tfinal), int(nmax), C.byref(res))
         return rc, res
+
+    def volume_integral(self, f):
+        """volume_integral(solver, f) of a padded field (src/diagnostics.jl:41-80)."""
+        f = np.ascontiguousarray(f, dtype=np.float64)
+        if f.shape != self.field_shape:
+            raise ValueError(f"field shape {f.shape} is not the solver's {self.field_shape}")
+        return float(lib().orc_volume_integral(self.ptr, f))
 
     def split(self, dim, P):
         """Emulate P ranks along dim (1-based) in every compact application along it."""

@@ -2,7 +2,9 @@
 reference's round-trip test (test/runtests.jl:1352-1389, the ideal-mixture
 parts: StiffenedGas is outside this path), and the curvature term of the
 oracle's max_rate (test/runtests.jl:641-665): swirl through a collapsed
-angular dimension must shorten dt in cylindrical and spherical metrics."""
+angular dimension must shorten dt in cylindrical and spherical metrics;
+and the oracle's volume quadrature, which the dissipation-rate diagnostic
+rests on (test/runtests.jl:955-990)."""
 import numpy as np
 import pytest
 
@@ -61,3 +63,25 @@ def test_cartesian_rate_has_no_curvature_term(orc):
 
     # collapsed y and z carry no advective rate either, so the swirl is invisible
     assert rate(2.0) == rate(0.0)
+
+
+def test_volume_quadrature(orc):
+    # test/runtests.jl:955-990: Cartesian exact (half weights on node-centred
+    # walls), the cylindrical axis fold O(h^2) at the outer wall only
+    PER, WALLS = cl.PER3[1], (cl.SlipWallBC(), cl.SlipWallBC())
+    d = cl.solver_desc((24, 16, 12), (2.0, 1.0, 0.5), (WALLS, PER, PER), orc.lele_d1_6(), orc.compact_filter(0.45),
+                       art=cl.ArtParams(enabled=False))
+    S = orc.Solver(d)
+    ones = np.ones(S.field_shape)
+    assert abs(S.volume_integral(ones) - 1.0) < 1e-12
+    lin = np.zeros(S.field_shape)
+    x = cl.coords(d)[0]
+    lin[cl.interior_slices(d)] = x[None, None, :]
+    assert abs(S.volume_integral(lin) - 1.0) < 1e-12
+    dc = cl.solver_desc((64, 1, 12), (1.0, 1.0, 1.0), ((cl.AxisBC(), cl.SlipWallBC()), PER, PER), orc.lele_d1_6(),
+                        orc.compact_filter(0.45), metric=cl.CylindricalMetric(), art=cl.ArtParams(enabled=False))
+    Sc = orc.Solver(dc)
+    v = Sc.volume_integral(np.ones(Sc.field_shape))
+    h = cl.grid_spacing(dc)[0]
+    assert abs(v - 0.5) <= 1e-3 * 0.5
+    assert v - 0.5 < h * h
