@@ -8,9 +8,11 @@
 //   pack      the M planes at each end of the local interior -> send buffers;
 //   (send the low planes to the previous rank, the high planes to the next)
 //   unpack    received planes -> the padded halo beyond each open end;
-//   local     the generic compact kernel over the rank's rows with open ends
-//             (their stencil reads that halo), storing the local solution y
-//             and each line's first/last q values (launch_compact_split);
+//   local     a compact kernel over the rank's rows with open ends (their
+//             stencil reads that halo: the tile kernels stage it beside the
+//             line, the generic kernel reads it from global memory), storing
+//             the local solution y and each line's first/last q values
+//             (launch_compact_split);
 //   (all-gather the heads and tails of every rank)
 //   reduce    per line, the previous rank's last q and the next rank's first q
 //             unknowns from the precomputed rows of the reduced inverse;
