@@ -4,8 +4,10 @@ pattern of src/halo.jl:143-194, including two ranks that wrap around each
 other and a closed end with no neighbour) and all-gathers the interface
 values in rank order (src/tridiag.jl:148); split_apply_along runs its
 phases in the right order around those exchanges, checked end to end with
-a CPU stand-in for the device plan that keeps the C ABI's buffer layout.
-The same calls carry device tensors over NCCL on GPUs."""
+a CPU stand-in for the device plan that keeps the C ABI's buffer layout;
+and the exchange stays inside a sub-communicator (the reference's
+decomp.sub[dim]) on a 2 x 2 grid of four ranks.  The same calls carry
+device tensors over NCCL on GPUs."""
 import importlib.util
 import os
 import pathlib
@@ -223,3 +225,48 @@ def test_split_apply_along_orchestration_over_gloo(world, periodic):
     for rank, off, piece in got:
         piece = np.array(piece)
         assert np.allclose(piece, ref[off:off + piece.shape[0]], rtol=0, atol=1e-13), rank
+
+
+def _subgroup_worker(rank, world, port, q):
+    # four ranks on a 2 x 2 grid: rows {0, 1} and {2, 3} each split a
+    # periodic line two ways; every rank exchanges within its own row only
+    os.environ.update({"MASTER_ADDR": "127.0.0.1", "MASTER_PORT": str(port)})
+    import torch.distributed as dist
+    cl = _package()
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        rows = [dist.new_group([0, 1]), dist.new_group([2, 3])]
+        row = rank // 2
+        g = rows[row]
+        coord = dist.get_rank(g)
+        ex = cl.LineExchange((coord - 1) % 2, (coord + 1) % 2, group=g)
+        n = 4
+        send_lo = torch.arange(n, dtype=torch.float64) + 100 * rank
+        send_hi = torch.arange(n, dtype=torch.float64) + 100 * rank + 50
+        recv_lo = torch.full((n,), -1.0, dtype=torch.float64)
+        recv_hi = torch.full((n,), -1.0, dtype=torch.float64)
+        ex.halo(send_lo, send_hi, recv_lo, recv_hi)
+        allv = torch.zeros(2, 3, dtype=torch.float64)
+        ex.gather(torch.full((3,), float(rank), dtype=torch.float64), allv)
+        q.put((rank, recv_lo.tolist(), recv_hi.tolist(), allv.tolist()))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_line_exchange_within_a_sub_communicator():
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    ps = [ctx.Process(target=_subgroup_worker, args=(r, 4, port, q)) for r in range(4)]
+    for p in ps:
+        p.start()
+    for p in ps:
+        p.join(120)
+        assert p.exitcode == 0
+    got = sorted(q.get(timeout=10) for _ in range(4))
+    for rank, lo, hi, allv in got:
+        partner = rank ^ 1              # the other rank of the same row, both neighbours
+        assert lo == [100 * partner + 50 + i for i in range(4)]
+        assert hi == [100 * partner + i for i in range(4)]
+        row0 = 2 * (rank // 2)
+        assert allv == [[float(row0)] * 3, [float(row0 + 1)] * 3]
