@@ -12,7 +12,7 @@ rate), five RK stages and filter_state!.
 Under torchrun (N > 1) every rank advances its own 256^3 box (replicas,
 weak scaling); the time is the max over ranks.  `--impl reference` times the
 CPU oracle (the FP64 restatement of the reference; the Julia reference cannot
-run on this machine) on the host cores.
+run on this machine) on every host core, on the same 256^3 box.
 """
 import argparse
 import importlib.util
@@ -52,8 +52,8 @@ def parse(argv=None):
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
     p.add_argument("--n", type=int, default=256, help="grid points per dimension")
-    p.add_argument("--cpu-n", type=int, default=128, help="grid of the bounded CPU sample")
-    p.add_argument("--cpu-steps", type=int, default=1)
+    p.add_argument("--cpu-n", type=int, default=128, help="grid of the one-thread CPU sample")
+    p.add_argument("--cpu-steps", type=int, default=3, help="timed steps of the all-core CPU sample")
     p.add_argument("--e2e-steps", type=int, default=5)
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
@@ -184,22 +184,20 @@ def measured_peaks():
 
 
 # DRAM traffic over algorithmic bytes of the C6 compact kernels on 5 FP64
-# fields of 256^3, from one ncu capture (dram__bytes_read.sum +
-# dram__bytes_write.sum; x / y / z 0.963 / 0.958 / 0.959, summarised in
-# profiles/compact_c6_256cube_fp64.md).  Traffic grows in proportion to
-# fields x points, so a launch's traffic is this ratio times its algorithmic
-# bytes.
+# fields of 256^3, from one ncu capture of the operator benchmark
+# (dram__bytes_read.sum + dram__bytes_write.sum; x / y / z 0.963 / 0.958 /
+# 0.959).  Traffic grows in proportion to fields x points, so a launch's
+# traffic is this ratio times its algorithmic bytes.
 NCU_TRAFFIC_RATIO = 0.960
 
 
 def ncu_traffic():
     """Per-launch DRAM bytes of the compact kernel, as a ratio to its algorithmic bytes (one ncu capture)."""
     return {"traffic_ratio": NCU_TRAFFIC_RATIO,
-            "note": "dram__bytes_read.sum + dram__bytes_write.sum over algorithmic bytes, ncu capture of the C6 "
-                    "compact kernels on 5 FP64 fields of 256^3 (x/y/z: 0.963/0.958/0.959, "
-                    "profiles/compact_c6_256cube_fp64.md); the per-launch traffic is this ratio times the "
-                    "average algorithmic bytes of the timed launches (traffic grows in proportion to fields x "
-                    "points)"}
+            "note": "dram__bytes_read.sum + dram__bytes_write.sum over algorithmic bytes, from one ncu capture "
+                    "of the C6 compact kernels on 5 FP64 fields of 256^3 (x/y/z: 0.963/0.958/0.959); the "
+                    "per-launch traffic is this ratio times the average algorithmic bytes of the timed launches "
+                    "(traffic grows in proportion to fields x points)"}
 
 
 # -------------------------------------------------------------- our arm ------
@@ -265,21 +263,28 @@ def time_e2e(cl, torch, desc, Q0, steps, dist):
     return ms, (h2d, d2h)
 
 
-def cpu_sample(n, steps):
-    """The oracle on the host cores: `steps` run! steps of the n^3 box after one warm-up step."""
+def _oracle_tgv(n):
     cl = _package()          # first: the oracle shares the package's descriptor structs
     sys.path.insert(0, str(ROOT / "oracle"))
     import oracle as orc
-    threads = orc.set_threads(os.cpu_count() or 1)
     prob = cl.taylor_green_problem()
     tp = 2 * math.pi
     desc = cl.solver_desc((n, n, n), (tp, tp, tp), prob.bcs, orc.lele_d1_6(), orc.compact_filter(0.45))
     O = orc.Solver(desc)
     O.set_state(cl.initialize(desc, prob.ic))
+    return orc, O
+
+
+def cpu_sample(n, steps, threads=None):
+    """The oracle on the host cores: `steps` run! steps of the n^3 box after one
+    warm-up step, on `threads` OpenMP threads (None: every host core)."""
+    orc, O = _oracle_tgv(n)
+    threads = orc.set_threads(threads or os.cpu_count() or 1)
     O.run(1e9, 1)
     t0 = time.perf_counter()
     O.run(1e9, 1 + steps)
     dt = time.perf_counter() - t0
+    orc.set_threads(os.cpu_count() or 1)
     return n ** 3 * steps / dt, threads, dt
 
 
@@ -338,45 +343,42 @@ def run_ours(a):
                       "h2d_bytes_per_step": sb[0], "d2h_bytes_per_step": sb[1],
                       "how": "cles_step_host: pinned padded host state in, one run! step, state out"}
     if dist.rank == 0 and dist.world == 1 and not a.no_cpu:
-        v, th, secs = cpu_sample(a.cpu_n, a.cpu_steps)
+        v, th, secs = cpu_sample(a.n, a.cpu_steps)
+        v1, _, secs1 = cpu_sample(a.cpu_n, 1, threads=1)
         out["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": th, "kind": "port",
-                               "sample": f"{a.cpu_steps} run! step(s) of the same Taylor-Green case at "
-                                         f"{a.cpu_n}^3 on the CPU oracle (FP64, OpenMP), {secs:.1f} s"}
+                               "sample": f"{a.cpu_steps} run! steps (after 1 untimed) of the same {a.n}^3 "
+                                         f"Taylor-Green case on the CPU oracle (FP64, OpenMP, {th} threads), "
+                                         f"{secs:.1f} s",
+                               "single_thread": {"value": v1, "unit": UNIT, "cores": 1,
+                                                 "sample": f"1 run! step (after 1 untimed) of the same case at "
+                                                           f"{a.cpu_n}^3 on one thread, {secs1:.1f} s"}}
     if dist.rank == 0:
         print(json.dumps(out), flush=True)
     dist.close()
 
 
 def run_reference(a):
-    """The oracle on the host cores: W untimed steps, then K timed run! steps of
-    the bounded a.cpu_n^3 sample of the same case."""
+    """The oracle on the host cores, every core: W untimed steps, then K timed
+    run! steps of the same a.n^3 box the GPU arm times."""
     dist = Dist(backend="gloo")
     if dist.rank != 0:
         dist.close()
         return
-    cl = _package()          # first: the oracle shares the package's descriptor structs
-    sys.path.insert(0, str(ROOT / "oracle"))
-    import oracle as orc
+    orc, O = _oracle_tgv(a.n)
     threads = orc.set_threads(os.cpu_count() or 1)
-    prob = cl.taylor_green_problem()
-    tp = 2 * math.pi
-    n = a.cpu_n
-    desc = cl.solver_desc((n, n, n), (tp, tp, tp), prob.bcs, orc.lele_d1_6(), orc.compact_filter(0.45))
-    O = orc.Solver(desc)
-    O.set_state(cl.initialize(desc, prob.ic))
     O.run(1e9, a.warmup)
     t0 = time.perf_counter()
     O.run(1e9, a.warmup + a.steps)
     secs = time.perf_counter() - t0
-    value = n ** 3 * a.steps / secs
+    value = a.n ** 3 * a.steps / secs
     out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": dist.world, "steps": a.steps,
            "warmup": a.warmup, "ms_per_step": 1e3 * secs / a.steps, "higher_is_better": True,
            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (analytic Taylor-Green)",
            "impl": "reference",
-           "config": {"workload": WORKLOAD, "grid": [a.n] * 3, "form": "fp64 CPU", "sample_grid": [n] * 3},
+           "config": {"workload": WORKLOAD, "grid": [a.n] * 3, "form": "fp64 CPU"},
            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
                             "sample": f"{a.steps} timed run! steps (after {a.warmup} untimed) of the same "
-                                      f"Taylor-Green case at {n}^3 on the FP64 CPU oracle, {secs:.1f} s; the Julia "
+                                      f"{a.n}^3 Taylor-Green case on the FP64 CPU oracle, {secs:.1f} s; the Julia "
                                       f"reference itself cannot run on this machine"},
            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out), flush=True)

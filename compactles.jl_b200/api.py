@@ -60,6 +60,7 @@ def lib():
         L.cles_ctx_create.argtypes = [C.c_int, vp, C.c_size_t, C.POINTER(vp)]
         L.cles_ctx_destroy.argtypes = [vp]
         L.cles_ctx_set_stream.argtypes = [vp, vp]
+        L.cles_selftest_bounded_wait.argtypes = [vp, C.c_int64]
         L.cles_plan_create.argtypes = [vp, C.POINTER(abi.cles_grid), C.POINTER(abi.cles_scheme), C.c_int, C.c_double,
                                        C.c_int, C.c_int, C.POINTER(vp)]
         L.cles_plan_destroy.argtypes = [vp]

@@ -267,6 +267,18 @@ int cles_ctx_set_stream(cles_ctx* ctx, void* stream) {
     API_END
 }
 
+int cles_selftest_bounded_wait(cles_ctx* ctx, int64_t limit_ns) {
+    API_BEGIN
+    if (!ctx) throw Error(CLES_EINVAL, "null context");
+    if (limit_ns < 1000 || limit_ns > 2000000000LL)
+        throw Error(CLES_EINVAL, "limit_ns must lie in [1e3, 2e9]");
+    CLES_CUDA(cudaSetDevice(ctx->device));
+    launch_wait_selftest((uint64_t)limit_ns, ctx->stream);
+    if (take_device_timeouts(ctx->stream))
+        throw Error(CLES_ETIMEOUT, "a bounded device wait expired (self-test)");
+    API_END
+}
+
 // ------------------------------------------------------------------ plans ----
 int cles_plan_create(cles_ctx* ctx, const cles_grid* grid, const cles_scheme* scheme, int dim, double h, int dtype,
                      int layout, cles_plan** out) {

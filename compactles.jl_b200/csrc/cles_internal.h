@@ -215,6 +215,9 @@ void split_correct(const SplitPlan& sp, const void* gathered, void* zbuf, const 
 
 // Bounded-wait timeouts recorded by device kernels since the last call (cleared).
 int take_device_timeouts(cudaStream_t st);
+// One CTA that waits limit_ns on an mbarrier nothing completes (the expiry
+// path of the operators' bounded wait).
+void launch_wait_selftest(uint64_t limit_ns, cudaStream_t st);
 
 // Launch the operator over `count` fields of `in` into `out` (may alias).
 void launch_compact(const CompactPlan& plan, const FieldView& in, const FieldView& out, int count, int mode,

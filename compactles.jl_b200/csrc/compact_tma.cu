@@ -66,13 +66,16 @@ __device__ __forceinline__ uint64_t global_ns() {
     return t;
 }
 
-// Wait for phase `parity` of `bar`, at most ~2 s.
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, unsigned parity) {
+constexpr uint64_t kWaitLimitNs = 2000000000ull;
+
+// Wait for phase `parity` of `bar`, at most limit_ns (2 s in every operator).
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, unsigned parity,
+                                                  uint64_t limit_ns = kWaitLimitNs) {
     if (mbar_try_wait(bar, parity)) return true;
     const uint64_t t0 = global_ns();
     while (true) {
         if (mbar_try_wait(bar, parity)) return true;
-        if (global_ns() - t0 > 2000000000ull) return false;
+        if (global_ns() - t0 > limit_ns) return false;
     }
 }
 
@@ -1092,6 +1095,27 @@ bool launch_compact_rk(const CompactPlan& plan, const FieldView& in, const Field
     const bool ok = try_launch_tma(plan, in, out, count, OUT_RK, st, &rk);
     if (rec >= 0) prof_end(rec, st);
     return ok;
+}
+
+// The expiry path of the bounded wait, run on purpose: one CTA initialises an
+// mbarrier and waits on its first phase, which nothing completes (no copy is
+// issued and no thread arrives, so nothing is in flight when it gives up).
+// It records the expiry in g_wait_timeouts exactly as the operators do.
+__global__ void k_wait_selftest(uint64_t limit_ns) {
+    __shared__ __align__(8) uint64_t bar;
+    if (threadIdx.x == 0) {
+        mbar_init(&bar, 1);
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    }
+    __syncthreads();
+    const bool ok = mbar_wait_bounded(&bar, 0u, limit_ns);
+    if (__syncthreads_or(!ok) && threadIdx.x == 0) atomicAdd(&g_wait_timeouts, 1);
+}
+
+void launch_wait_selftest(uint64_t limit_ns, cudaStream_t st) {
+    k_wait_selftest<<<1, 64, 0, st>>>(limit_ns);
+    check_launch("k_wait_selftest");
+    count_launch(1);
 }
 
 int take_device_timeouts(cudaStream_t st) {

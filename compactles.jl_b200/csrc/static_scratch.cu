@@ -21,11 +21,24 @@
 //     them) race on the array and may return each other's partials.  Order such
 //     calls on one stream or synchronise between them;
 //   * the first call on a device looks up the array's device address with
-//     cudaGetSymbolAddress (once per device, with that device current).  Make
-//     that first call before any stream capture.
-// The per-cell arithmetic is the one of cles_max_rate (the primitives of
-// src/physics.jl:604-653 and the rate of src/timestep.jl:125-175), so both
-// entry points return identical values for the same inputs.
+//     cudaGetSymbolAddress (once per device context, with that device
+//     current).  Make that first call before any stream capture.  The address
+//     is cached together with the context's unique id (cuCtxGetId): after a
+//     cudaDeviceReset the module is loaded into a new context, the ids differ
+//     and the next call looks the address up again instead of using a stale
+//     one (that call is again a set-up call, outside any capture);
+//   * `stream` must belong to the current device (checked with
+//     cudaStreamGetDevice; a stream of another device is CLES_EINVAL).
+// Scope: an ideal mixture (R and gamma per species) on a uniform Cartesian
+// grid, one 1/h per dimension.  The per-cell arithmetic is the one of
+// cles_max_rate for such a solver in FP64 (the primitives of
+// src/physics.jl:604-653 and the rate of src/timestep.jl:125-175), so the
+// two return identical values there.  It has no per-node 1/h (stretched or
+// curvilinear grids), no curvature_rate term (src/timestep.jl:150-161) and
+// no NASA-9 thermodynamics, and it reads FP64 primitives where a mixed-
+// precision solver rounds them to FP32: on those solvers use cles_max_rate.
+
+#include <cuda.h>
 
 #include <mutex>
 
@@ -151,22 +164,53 @@ k_rate_static_final(const double* __restrict__ scratch, int nb, double* __restri
     }
 }
 
-// Device address of g_rate_scratch, looked up once per device.
+// Device address of g_rate_scratch, looked up once per device context.
 constexpr int kMaxDevices = 64;
 std::mutex g_scratch_mu;
 double* g_scratch_ptr[kMaxDevices] = {};
+unsigned long long g_scratch_ctx[kMaxDevices] = {};
+
+using CtxGetCurrentFn = CUresult (*)(CUcontext*);
+using CtxGetIdFn = CUresult (*)(CUcontext, unsigned long long*);
+
+// Unique id of the current device context (cuCtxGetId, through the runtime's
+// driver entry points so the library needs no libcuda link).
+unsigned long long current_context_id() {
+    static CtxGetCurrentFn get_cur = nullptr;
+    static CtxGetIdFn get_id = nullptr;
+    if (!get_cur || !get_id) {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            throw Error(CLES_ECUDA, "cuCtxGetCurrent is unavailable");
+        get_cur = reinterpret_cast<CtxGetCurrentFn>(p);
+        if (cudaGetDriverEntryPoint("cuCtxGetId", &p, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            throw Error(CLES_ECUDA, "cuCtxGetId is unavailable");
+        get_id = reinterpret_cast<CtxGetIdFn>(p);
+    }
+    CUcontext c = nullptr;
+    unsigned long long id = 0;
+    if (get_cur(&c) != CUDA_SUCCESS || !c || get_id(c, &id) != CUDA_SUCCESS)
+        throw Error(CLES_ECUDA, "no current CUDA context");
+    return id;
+}
 
 double* scratch_for_current_device() {
     int dev = 0;
     CLES_CUDA(cudaGetDevice(&dev));
     if (dev < 0 || dev >= kMaxDevices) throw Error(CLES_EINVAL, "device index out of range");
+    CLES_CUDA(cudaSetDevice(dev));   // makes the device's primary context current on this thread
+    const unsigned long long ctx = current_context_id();
     std::lock_guard<std::mutex> lock(g_scratch_mu);
-    if (!g_scratch_ptr[dev]) {
+    if (!g_scratch_ptr[dev] || g_scratch_ctx[dev] != ctx) {
         void* p = nullptr;
         const cudaError_t e = cudaGetSymbolAddress(&p, g_rate_scratch);
         if (e != cudaSuccess || !p)
             throw Error(CLES_ECUDA, std::string("cudaGetSymbolAddress(g_rate_scratch): ") + cudaGetErrorString(e));
         g_scratch_ptr[dev] = static_cast<double*>(p);
+        g_scratch_ctx[dev] = ctx;
     }
     return g_scratch_ptr[dev];
 }
@@ -199,9 +243,18 @@ extern "C" int cles_max_rate_static(const double* Q_dev, const double* art_dev, 
         a.mu0 = mu0;
         a.Pr = Pr;
         a.Sc = Sc;
+        cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+        if (st) {
+            int dev = 0, sdev = 0;
+            CLES_CUDA(cudaGetDevice(&dev));
+            CLES_CUDA(cudaStreamGetDevice(st, &sdev));
+            if (sdev != dev)
+                throw Error(CLES_EINVAL, "cles_max_rate_static: the stream belongs to device " +
+                                             std::to_string(sdev) + ", not the current device " +
+                                             std::to_string(dev));
+        }
         double* scratch = scratch_for_current_device();
         const int nb = (int)((cells + kCellsPerBlock - 1) / kCellsPerBlock);
-        cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
         k_rate_static_partial<<<nb, kStaticThreads, 0, st>>>(Q_dev, art_dev, cells, n_species, a, scratch);
         count_launch();
         check_launch("k_rate_static_partial");

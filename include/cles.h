@@ -161,6 +161,17 @@ const char* cles_last_error(void);
 /* Number of kernels this library has launched so far in this process. */
 int64_t cles_kernel_launches(void);
 
+/* Self-test of the bounded device wait (no counterpart in the reference).
+ * Every mbarrier wait in the compact-operator kernels gives up after 2 s,
+ * records the expiry in a device counter and returns; the next call that
+ * reads the counter (cles_max_rate, and so every run! step) returns
+ * CLES_ETIMEOUT and clears it.  This call runs that expiry path on purpose:
+ * one CTA waits limit_ns (1e3 .. 2e9) on an mbarrier that nothing completes
+ * (no copy is issued, so nothing is in flight when it gives up), then the
+ * counter is read on the context's stream.  Returns CLES_ETIMEOUT when the
+ * path works; the context stays usable. */
+int  cles_selftest_bounded_wait(cles_ctx* ctx, int64_t limit_ns);
+
 /* ---- directional plans ---------------------------------------------------
  * cles_plan_create replaces plan_direction(decomp, scheme, dim, h)
  * (src/operators.jl:44-101, src/operators_banded.jl:29-125): LHS assembly
@@ -462,11 +473,15 @@ int  cles_step_host(cles_solver* s, double* Q_host, int layout, double tfinal,
 /* Allocation-free CFL rate reduction (no counterpart in the reference).
  * For callers that cannot call cudaMalloc -- code inside a host framework
  * that owns every device allocation, a plugin barred from allocating after
- * start-up, or a process held to a fixed HBM budget.  Computes what
- * cles_max_rate computes (the rate max of src/timestep.jl:125-175 and the
- * minimum mixture density) from caller-owned device arrays, keeping its
- * per-block partials in a library-owned static device array instead of
- * allocating:
+ * start-up, or a process held to a fixed HBM budget.  For an ideal mixture on
+ * a uniform Cartesian grid it computes what cles_max_rate computes for an
+ * FP64 solver (the rate max of src/timestep.jl:125-175 and the minimum
+ * mixture density; identical values) from caller-owned device arrays,
+ * keeping its per-block partials in a library-owned static device array
+ * instead of allocating.  It has no per-node 1/h (stretched or curvilinear
+ * grids), no curvature_rate term and no NASA-9 thermodynamics, and it works
+ * on FP64 primitives where a mixed-precision solver rounds them to FP32: for
+ * those solvers call cles_max_rate.  Arguments:
  *   Q_dev      conserved state, interior layout, component slowest (n_species+4 fields of `cells`)
  *   art_dev    mu*, beta*, kappa*, D*_1..D*_Ns (3+n_species fields of `cells`)
  *   inv_h      1/h per dimension, 0 for a collapsed one
@@ -475,7 +490,10 @@ int  cles_step_host(cles_solver* s, double* Q_host, int layout, double tfinal,
  * All calls on a device share the static array, so calls that overlap on the
  * GPU race; order them on one stream.  The first call on a device resolves the
  * array's address (cudaGetSymbolAddress) and should come before any stream
- * capture.  Work is queued on `stream` (NULL = legacy default stream). */
+ * capture; after a cudaDeviceReset the next call resolves it again (the
+ * cached address is keyed by the context's unique id), so that call is a
+ * first call too.  Work is queued on `stream` (NULL = legacy default stream),
+ * which must belong to the current device (CLES_EINVAL otherwise). */
 #define CLES_STATIC_MAX_CELLS 33554432LL
 int  cles_max_rate_static(const double* Q_dev, const double* art_dev, int64_t cells, int n_species,
                           const double* R, const double* gamma, const double* inv_h, double mu0, double Pr,

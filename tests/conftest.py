@@ -35,3 +35,13 @@ def orc():
     import oracle
     oracle.lib()
     return oracle
+
+
+def pytest_terminal_summary(terminalreporter, exitstatus, config):
+    # parity figures that tests recorded beside their asserted bounds, so a
+    # quiet run still shows them
+    parity = sys.modules.get("parity")
+    if parity is not None and parity.LINES:
+        terminalreporter.section("parity figures")
+        for ln in parity.LINES:
+            terminalreporter.write_line(ln)

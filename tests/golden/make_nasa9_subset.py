@@ -6,7 +6,7 @@ The coefficient file itself is not copied; the fixture holds the parsed
 numbers for the species the thermodynamic tests use, with each record's
 specific gas constant R = 1000 R_u / M.  Run from the repository root:
 
-    python tests/golden/make_nasa9_subset.py /root/reference/data/thermo.inp
+    python tests/golden/make_nasa9_subset.py <CompactLES.jl source tree>/data/thermo.inp
 """
 import importlib.util
 import json
@@ -33,4 +33,6 @@ def main(path):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference/data/thermo.inp")
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_nasa9_subset.py <CompactLES.jl source tree>/data/thermo.inp")
+    main(sys.argv[1])
