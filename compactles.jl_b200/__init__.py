@@ -16,7 +16,7 @@ from .problem import (ArtParams, AxisBC, CartesianMetric, ConstantBodyForce, Cyl
                       taylor_green_problem)
 from .api import (ClesError, Context, DirPlan, Solver, SolverFailure, apply_along, build, check_step,
                   compact_filter, default_context, grid, kernel_launches, lele_d1_10, lele_d1_6, lib,
-                  pade_d1_4, plan_direction, profile_enable, profile_read, setup, Server)
+                  pade_d1_4, plan_direction, profile_enable, profile_read, setup, Server, Batch)
 from . import scenarios
 from .split import LineExchange, SplitPlan, exchange_halos, split_apply_along
 from .nasa9 import Nasa9Interval, Nasa9Mixture, Nasa9Species, nasa9_constant_cp, read_nasa9

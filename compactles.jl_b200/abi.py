@@ -276,6 +276,30 @@ CLES_REQ_CANCELLED = 4
 REQ_STATES = {0: "queued", 1: "running", 2: "done", 3: "failed", 4: "cancelled"}
 
 
+class cles_batch_tuning(C.Structure):
+    _fields_ = [
+        ("op", C.c_int),
+        ("dim", C.c_int),
+        ("threads", C.c_int),
+        ("smem", C.c_int64),
+        ("ctas", C.c_int),
+        ("tuned_ms", C.c_double),
+    ]
+
+
+class cles_batch_stats(C.Structure):
+    _fields_ = [
+        ("members", C.c_int),
+        ("active", C.c_int),
+        ("compositions", C.c_int),
+        ("steps", C.c_int64),
+        ("launches_per_step", C.c_int),
+        ("cells_total", C.c_int64),
+        ("n_roles", C.c_int),
+        ("tuning", cles_batch_tuning * 9),
+    ]
+
+
 class cles_request_status(C.Structure):
     _fields_ = [
         ("state", C.c_int),

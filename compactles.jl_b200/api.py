@@ -116,6 +116,17 @@ def lib():
         L.cles_server_status.argtypes = [vp, C.c_int64, C.POINTER(abi.cles_request_status)]
         L.cles_server_fetch.argtypes = [vp, C.c_int64, vp]
         L.cles_server_cancel.argtypes = [vp, C.c_int64]
+        L.cles_batch_create.argtypes = [vp, C.POINTER(abi.cles_solver_desc), C.POINTER(vp)]
+        L.cles_batch_destroy.argtypes = [vp]
+        L.cles_batch_destroy.restype = None
+        L.cles_batch_add.argtypes = [vp, C.POINTER(abi.cles_solver_desc), vp, C.c_int, C.c_double, C.c_int64,
+                                     C.POINTER(C.c_int64)]
+        L.cles_batch_step.argtypes = [vp, C.POINTER(C.c_int)]
+        L.cles_batch_run.argtypes = [vp, C.c_int64, C.POINTER(C.c_int)]
+        L.cles_batch_status.argtypes = [vp, C.c_int64, C.POINTER(abi.cles_request_status)]
+        L.cles_batch_fetch.argtypes = [vp, C.c_int64, vp]
+        L.cles_batch_cancel.argtypes = [vp, C.c_int64]
+        L.cles_batch_stats_get.argtypes = [vp, C.POINTER(abi.cles_batch_stats)]
         L.cles_kinetic_energy.argtypes = [vp, dp]
         L.cles_dissipation_rate.argtypes = [vp, dp]
         _lib = L
@@ -490,3 +501,66 @@ class Server:
             if r == 0 and q == 0:
                 return
         raise ClesError(abi.CLES_ETIMEOUT, "server did not drain")
+
+
+class Batch:
+    """Many solves of one physics class advanced together (cles_batch_*): one
+    arena, one captured CUDA graph per composition, O(stages) launches per step
+    whatever the number of members.  `cls` is a solver descriptor of the class
+    (grid extents, domain and boundary states are per member)."""
+
+    def __init__(self, cls, ctx=None):
+        self.ctx = ctx or default_context()
+        self.ptr = C.c_void_p()
+        _check(lib().cles_batch_create(self.ctx.ptr, C.byref(cls), C.byref(self.ptr)))
+        self._shape = {}
+
+    def __del__(self):
+        try:
+            if self.ptr:
+                lib().cles_batch_destroy(self.ptr)
+                self.ptr = None
+        except Exception:
+            pass
+
+    def add(self, desc, Q0, tfinal, nmax=2 ** 62, layout="padded"):
+        Q0 = np.ascontiguousarray(Q0, dtype=np.float64)
+        lay = abi.CLES_LAYOUT_PADDED if layout == "padded" else abi.CLES_LAYOUT_INTERIOR
+        mid = C.c_int64()
+        _check(lib().cles_batch_add(self.ptr, C.byref(desc), Q0.ctypes.data_as(C.c_void_p), lay, float(tfinal),
+                                    int(nmax), C.byref(mid)))
+        self._shape[mid.value] = Q0.shape
+        return mid.value
+
+    def step(self):
+        n = C.c_int()
+        _check(lib().cles_batch_step(self.ptr, C.byref(n)))
+        return n.value
+
+    def run(self, max_steps=2 ** 62):
+        n = C.c_int()
+        _check(lib().cles_batch_run(self.ptr, int(max_steps), C.byref(n)))
+        return n.value
+
+    def status(self, mid):
+        st = abi.cles_request_status()
+        _check(lib().cles_batch_status(self.ptr, int(mid), C.byref(st)))
+        return {"state": abi.REQ_STATES[st.state], "failure": abi.FAIL_NAMES.get(st.failure), "steps": st.steps,
+                "t": st.t, "admit_s": st.admit_s, "done_s": st.done_s, "device_bytes": st.device_bytes}
+
+    def fetch(self, mid):
+        out = np.zeros(self._shape[mid])
+        _check(lib().cles_batch_fetch(self.ptr, int(mid), out.ctypes.data_as(C.c_void_p)))
+        return out
+
+    def cancel(self, mid):
+        _check(lib().cles_batch_cancel(self.ptr, int(mid)))
+
+    def stats(self):
+        st = abi.cles_batch_stats()
+        _check(lib().cles_batch_stats_get(self.ptr, C.byref(st)))
+        ops = ("deriv", "filter", "filter_state")
+        return {"members": st.members, "active": st.active, "compositions": st.compositions, "steps": st.steps,
+                "launches_per_step": st.launches_per_step, "cells_total": st.cells_total,
+                "tuning": [{"op": ops[t.op], "dim": t.dim, "threads": t.threads, "smem": t.smem, "ctas": t.ctas,
+                            "tuned_ms": t.tuned_ms} for t in st.tuning[:st.n_roles]]}

@@ -2,6 +2,7 @@
 // exception, records its text for cles_last_error() and returns a status.
 
 #include <atomic>
+#include <chrono>
 #include <cstdio>
 #include <cstring>
 #include <vector>
@@ -47,6 +48,7 @@ void prof_end(int rec, cudaStream_t st) { CLES_CUDA(cudaEventRecord(g_prof[rec].
 
 void set_last_error(const std::string& s) { g_last_error = s; }
 void count_launch(int n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+int64_t launch_count() { return g_launches.load(std::memory_order_relaxed); }
 void check_launch(const char* what) {
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) throw Error(CLES_ECUDA, std::string(what) + " launch: " + cudaGetErrorString(e));
@@ -732,3 +734,100 @@ int cles_step_host(cles_solver* s, double* Q_host, int layout, double tfinal, cl
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------- batches ----
+struct cles_batch {
+    cles_ctx* ctx = nullptr;
+    std::unique_ptr<BatchBase> b;
+    std::vector<std::pair<int64_t, int>> layouts;   // member id -> layout it was added with
+    std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
+    double now() const {
+        return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    }
+    int layout_of(int64_t id) const {
+        for (auto& e : layouts)
+            if (e.first == id) return e.second;
+        throw Error(CLES_EINVAL, "no batch member with this id");
+    }
+};
+
+int cles_batch_create(cles_ctx* ctx, const cles_solver_desc* cls, cles_batch** out) {
+    API_BEGIN
+    if (!ctx || !cls || !out) throw Error(CLES_EINVAL, "null argument");
+    CLES_CUDA(cudaSetDevice(ctx->device));
+    auto* b = new cles_batch();
+    try {
+        b->ctx = ctx;
+        b->b = make_batch(ctx, *cls);
+    } catch (...) {
+        delete b;
+        throw;
+    }
+    *out = b;
+    API_END
+}
+
+void cles_batch_destroy(cles_batch* b) {
+    if (!b) return;
+    cudaSetDevice(b->ctx->device);
+    delete b;
+}
+
+int cles_batch_add(cles_batch* b, const cles_solver_desc* desc, const double* Q0, int layout, double tfinal,
+                   int64_t nmax, int64_t* id) {
+    API_BEGIN
+    if (!b || !desc || !Q0 || !id) throw Error(CLES_EINVAL, "null argument");
+    CLES_CUDA(cudaSetDevice(b->ctx->device));
+    *id = b->b->add(*desc, Q0, layout, tfinal, nmax, b->now());
+    b->layouts.emplace_back(*id, layout);
+    API_END
+}
+
+int cles_batch_step(cles_batch* b, int* n_active) {
+    API_BEGIN
+    if (!b) throw Error(CLES_EINVAL, "null batch");
+    CLES_CUDA(cudaSetDevice(b->ctx->device));
+    const int n = b->b->step(b->now());
+    if (n_active) *n_active = n;
+    API_END
+}
+
+int cles_batch_run(cles_batch* b, int64_t max_steps, int* n_active) {
+    API_BEGIN
+    if (!b) throw Error(CLES_EINVAL, "null batch");
+    CLES_CUDA(cudaSetDevice(b->ctx->device));
+    int n = b->b->n_active();
+    for (int64_t s = 0; s < max_steps && n > 0; ++s) n = b->b->step(b->now());
+    if (n == 0) b->b->step(b->now());   // retires the last members (nothing left to step)
+    if (n_active) *n_active = n;
+    API_END
+}
+
+int cles_batch_status(cles_batch* b, int64_t id, cles_request_status* out) {
+    API_BEGIN
+    if (!b || !out) throw Error(CLES_EINVAL, "null argument");
+    b->b->status(id, out);
+    API_END
+}
+
+int cles_batch_fetch(cles_batch* b, int64_t id, double* Q) {
+    API_BEGIN
+    if (!b || !Q) throw Error(CLES_EINVAL, "null argument");
+    CLES_CUDA(cudaSetDevice(b->ctx->device));
+    b->b->fetch(id, Q, b->layout_of(id));
+    API_END
+}
+
+int cles_batch_cancel(cles_batch* b, int64_t id) {
+    API_BEGIN
+    if (!b) throw Error(CLES_EINVAL, "null batch");
+    b->b->remove(id, b->now());
+    API_END
+}
+
+int cles_batch_stats_get(const cles_batch* b, cles_batch_stats* out) {
+    API_BEGIN
+    if (!b || !out) throw Error(CLES_EINVAL, "null argument");
+    b->b->stats(out);
+    API_END
+}

@@ -25,6 +25,7 @@ void set_last_error(const std::string& s);
             throw ::cles::Error(CLES_ECUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
     } while (0)
 void count_launch(int n = 1);
+int64_t launch_count();   // kernels launched by this library so far
 // CUDA-event bracketing of compact launches (cles_profile_enable)
 bool profiling();
 int prof_begin(cudaStream_t st, int family, double bytes);
@@ -141,9 +142,11 @@ struct CompactPlan {
 // a coordinate-singularity fold at that end of a closed line: the antipodal
 // parity (+1 / -1) of the field the plan is applied to, 0 for a closure.
 // lo_open / hi_open make that end of a non-periodic line a rank interface.
+// pow2_segments (batched plans): S is the fewest power-of-two segments of at
+// most kMaxSeg points.
 void build_compact_plan(CompactPlan& plan, const cles_scheme& scheme, const int n3[3], int dim,
                         bool periodic, double h, int dtype, int lo_fold = 0, int hi_fold = 0,
-                        bool lo_open = false, bool hi_open = false);
+                        bool lo_open = false, bool hi_open = false, bool pow2_segments = false);
 
 // The LHS band of one line (or one rank's piece of a split line), row-major
 // n x (2q+1): interior band, closure rows at closed ends, parity folds, and
@@ -212,6 +215,35 @@ void split_halo(const SplitPlan& sp, const FieldView& f, void* lo, void* hi, int
 // out -= V z_prev + W z_next over the local interior.
 void split_correct(const SplitPlan& sp, const void* gathered, void* zbuf, const FieldView& out, int count,
                    cudaStream_t st);
+
+// ---- batched line solves over many grids (batch_compact.cu) ----------------
+// One grid's directional plan in a batched launch.  Its lines are cut into
+// power-of-two segments (build_compact_plan with pow2_segments), and P.LB is
+// the launch's threads / P.S, so every CTA of the launch runs LB x S threads.
+// The grid's fields start at element `off` of the launch's arena blocks.
+struct BatchLinePlan {
+    CompactParams P;
+    const void* tab;      // the plan's coefficient table (launch dtype)
+    int64_t off;          // element offset of the grid's cell (0, 0, 0)
+    int64_t sy, sz;       // strides of the grid's fields
+    const double* clk;    // graph-mode clock of the grid (dt in slot 1)
+};
+// Kernel template of a batched launch (shared by all its plans).
+struct BatchLaunchKind {
+    int dtype;            // CLES_F64 / CLES_F32
+    int q, M, xmode;
+    int threads;          // LB x S of every plan
+    size_t smem;          // dynamic shared memory (max over the plans)
+};
+// Dynamic shared memory one plan needs with LB lines per CTA.
+size_t batch_plan_smem(const CompactParams& P, int LB, int dtype);
+// blocks[b] = (plan, first line); blockIdx.y = field.  in / out / Q / du are
+// arena block starts (fields cells_total elements apart).  mode OUT_RK applies
+// the low-storage RK update with coefficients (A, B) and each grid's dt
+// (clk[1]); skip_idle leaves out every grid whose dt is 0 (done or failed).
+void launch_compact_batch(const BatchLaunchKind& kind, const BatchLinePlan* plans, const int2* blocks, int nblocks,
+                          const void* in, void* out, int64_t cells_total, int count, int mode, double* Q, double* du,
+                          double A, double B, int skip_idle, cudaStream_t st);
 
 // Bounded-wait timeouts recorded by device kernels since the last call (cleared).
 int take_device_timeouts(cudaStream_t st);

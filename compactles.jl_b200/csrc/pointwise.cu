@@ -241,18 +241,18 @@ __device__ __forceinline__ int edge_index(int i, int n, int periodic) {
     if (periodic) return i < 0 ? i + n : (i >= n ? i - n : i);
     return i < 0 ? 0 : (i >= n ? n - 1 : i);
 }
+// One block's tile (x0, y0, z0) of the tiled delta4_sum!.
 template <typename F, int NF>
-__global__ void __launch_bounds__(kTX * kTY) k_delta4_tiled(const F* __restrict__ f0, const F* __restrict__ f1,
-                                                           F* __restrict__ o0, F* __restrict__ o1, Grid3 g,
-                                                           Weights3 w0, Weights3 w1) {
-    __shared__ F tile[NF][kTY + 4][kTX + 4];
+__device__ __forceinline__ void delta4_tile(const F* __restrict__ f0, const F* __restrict__ f1, F* __restrict__ o0,
+                                            F* __restrict__ o1, const Grid3& g, const Weights3& w0,
+                                            const Weights3& w1, const int x0, const int y0, const int z0,
+                                            F (*tile)[kTY + 4][kTX + 4]) {
     const F* fs[2] = {f0, f1};
     F* os[2] = {o0, o1};
     const Weights3 ws[2] = {w0, w1};
     const int nx = g.n[0], ny = g.n[1], nz = g.n[2];
     const int64_t sy = nx, sz = (int64_t)nx * ny;
     const int tx = threadIdx.x % kTX, ty = threadIdx.x / kTX;
-    const int x0 = blockIdx.x * kTX, y0 = blockIdx.y * kTY, z0 = blockIdx.z * kZC;
     const int x = x0 + tx, y = y0 + ty;
     const bool inside = x < nx && y < ny;
     const double D4[5] = {1.0, -4.0, 6.0, -4.0, 1.0};
@@ -311,6 +311,14 @@ __global__ void __launch_bounds__(kTX * kTY) k_delta4_tiled(const F* __restrict_
         }
         __syncthreads();
     }
+}
+
+template <typename F, int NF>
+__global__ void __launch_bounds__(kTX * kTY) k_delta4_tiled(const F* __restrict__ f0, const F* __restrict__ f1,
+                                                           F* __restrict__ o0, F* __restrict__ o1, Grid3 g,
+                                                           Weights3 w0, Weights3 w1) {
+    __shared__ F tile[NF][kTY + 4][kTX + 4];
+    delta4_tile<F, NF>(f0, f1, o0, o1, g, w0, w1, blockIdx.x * kTX, blockIdx.y * kTY, blockIdx.z * kZC, tile);
 }
 
 // Ducros switch (src/artificial.jl:134-147)
@@ -533,15 +541,14 @@ __global__ void k_lsrk(double* __restrict__ Q, double* __restrict__ du, const F*
     }
 }
 
-// max_rate per-block partials (src/timestep.jl:125-175), Cartesian.
+// The max_rate contribution of cell I (src/timestep.jl:125-175), Cartesian;
+// fields are `cells` elements apart.
 template <typename F>
-__global__ void k_rate_partial(const double* __restrict__ Q, const F* __restrict__ prim, const F* __restrict__ art,
-                               double* __restrict__ part, int64_t cells, int Ns, double idx0, double idx1, double idx2,
-                               int a0, int a1, int a2, double mu0, double Pr, double Sc) {
-    double rate = 0.0, rmin = __longlong_as_double(0x7ff0000000000000LL);
-    const double idx[3] = {idx0, idx1, idx2};
-    const int act[3] = {a0, a1, a2};
-    GRID_STRIDE(I, cells) {
+__device__ __forceinline__ void rate_cell(const double* __restrict__ Q, const F* __restrict__ prim,
+                                          const F* __restrict__ art, int64_t I, int64_t cells, int Ns,
+                                          const double idx[3], const int act[3], double mu0, double Pr, double Sc,
+                                          double& rate, double& rmin) {
+    {
         double rq = 0.0;
         for (int sp = 0; sp < Ns; ++sp) rq += Q[I + cells * sp];
         rmin = jl_min(rmin, rq);
@@ -563,7 +570,11 @@ __global__ void k_rate_partial(const double* __restrict__ Q, const F* __restrict
         acc += 2 * nu * dsum;
         rate = jl_max(rate, acc);
     }
-    // block reduction (max / min are exact, so the order does not matter)
+}
+
+// Block max / min of (rate, rmin) into part[2 b], part[2 b + 1] (max / min are
+// exact, so the order does not matter).
+__device__ __forceinline__ void rate_block_reduce(double rate, double rmin, double* __restrict__ part, int b) {
     __shared__ double sr[kThreads], sm[kThreads];
     sr[threadIdx.x] = rate;
     sm[threadIdx.x] = rmin;
@@ -576,9 +587,21 @@ __global__ void k_rate_partial(const double* __restrict__ Q, const F* __restrict
         __syncthreads();
     }
     if (threadIdx.x == 0) {
-        part[2 * blockIdx.x] = sr[0];
-        part[2 * blockIdx.x + 1] = sm[0];
+        part[2 * b] = sr[0];
+        part[2 * b + 1] = sm[0];
     }
+}
+
+// max_rate per-block partials (src/timestep.jl:125-175), Cartesian.
+template <typename F>
+__global__ void k_rate_partial(const double* __restrict__ Q, const F* __restrict__ prim, const F* __restrict__ art,
+                               double* __restrict__ part, int64_t cells, int Ns, double idx0, double idx1, double idx2,
+                               int a0, int a1, int a2, double mu0, double Pr, double Sc) {
+    double rate = 0.0, rmin = __longlong_as_double(0x7ff0000000000000LL);
+    const double idx[3] = {idx0, idx1, idx2};
+    const int act[3] = {a0, a1, a2};
+    GRID_STRIDE(I, cells) rate_cell(Q, prim, art, I, cells, Ns, idx, act, mu0, Pr, Sc, rate, rmin);
+    rate_block_reduce(rate, rmin, part, blockIdx.x);
 }
 
 __global__ void k_rate_final(const double* __restrict__ part, int nb, double* __restrict__ out) {
@@ -685,14 +708,16 @@ __global__ void k_sum_final(const double* __restrict__ part, int nb, int width, 
 
 // enforce!(::SlipWallBC) (src/boundary.jl:232-243) and a time-constant
 // DirichletBC (src/problem.jl:209-221) on the wall plane of (d, side).
-__global__ void k_bc_plane(double* __restrict__ Q, Grid3 g, int d, int side, int Ns, int kind, BcState st,
-                           const double* __restrict__ qface) {
+// The plane of face (d, side) of one grid whose fields are `cells` elements
+// apart, threads t0, t0 + tstep, ... of it.
+__device__ __forceinline__ void bc_plane_body(double* __restrict__ Q, const Grid3& g, const int64_t cells, int d,
+                                              int side, int Ns, int kind, const BcState& st,
+                                              const double* __restrict__ qface, int64_t t0, int64_t tstep) {
     const int o1 = d == 0 ? 1 : 0, o2 = d == 2 ? 1 : 2;
     const int64_t plane = (int64_t)g.n[o1] * g.n[o2];
-    const int64_t cells = (int64_t)g.n[0] * g.n[1] * g.n[2];
     const int64_t stv[3] = {1, (int64_t)g.n[0], (int64_t)g.n[0] * g.n[1]};
     const int wall = side == 0 ? 0 : g.n[d] - 1;
-    GRID_STRIDE(t, plane) {
+    for (int64_t t = t0; t < plane; t += tstep) {
         const int a = (int)(t % g.n[o1]), b = (int)(t / g.n[o1]);
         const int64_t I = a * stv[o1] + b * stv[o2] + (int64_t)wall * stv[d];
         if (kind == CLES_BC_SLIPWALL) {
@@ -729,6 +754,13 @@ __global__ void k_bc_plane(double* __restrict__ Q, Grid3 g, int d, int side, int
             for (int c = 0; c < Ns + 4; ++c) Q[I + cells * c] = st.q[c];
         }
     }
+}
+
+__global__ void k_bc_plane(double* __restrict__ Q, Grid3 g, int d, int side, int Ns, int kind, BcState st,
+                           const double* __restrict__ qface) {
+    const int64_t cells = (int64_t)g.n[0] * g.n[1] * g.n[2];
+    bc_plane_body(Q, g, cells, d, side, Ns, kind, st, qface, blockIdx.x * (int64_t)blockDim.x + threadIdx.x,
+                  (int64_t)gridDim.x * blockDim.x);
 }
 
 // correct_rhs!(::NSCBCOutflowBC) (src/nscbc.jl:59-157) and
@@ -866,10 +898,9 @@ __global__ void k_to_double(const F* __restrict__ a, double* __restrict__ b, int
 // (predicted_dt without prediction or growth cap), the check_step floors
 // (src/stepcontrol.jl:184-204), dt_seen, and the tfinal clip
 // (src/timestep.jl:288-352).
-__global__ void k_clock_before(double* __restrict__ clk, const double* __restrict__ rate_rmin, ClockConst c) {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+__device__ __forceinline__ void clock_before_body(double* __restrict__ clk, const double rate, const double rmin,
+                                                  const ClockConst& c) {
     if (clk[DC_FAILURE] != 0.0 || clk[DC_DONE] != 0.0) { clk[DC_DT] = 0.0; return; }
-    const double rate = rate_rmin[0], rmin = rate_rmin[1];
     double dt = c.cfl / rate;
     int f = 0;
     if (!isfinite(dt)) f = CLES_FAIL_NONFINITE;
@@ -883,13 +914,83 @@ __global__ void k_clock_before(double* __restrict__ clk, const double* __restric
     clk[DC_DT_SEEN] = jl_max(clk[DC_DT_SEEN], dt);
     clk[DC_DT] = jl_min(dt, c.tfinal - clk[DC_T]);
 }
-// After the step: t += dt, step += 1, done when the run! loop condition fails.
-__global__ void k_clock_after(double* __restrict__ clk, ClockConst c) {
+__global__ void k_clock_before(double* __restrict__ clk, const double* __restrict__ rate_rmin, ClockConst c) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    clock_before_body(clk, rate_rmin[0], rate_rmin[1], c);
+}
+// After the step: t += dt, step += 1, done when the run! loop condition fails.
+__device__ __forceinline__ void clock_after_body(double* __restrict__ clk, const ClockConst& c) {
     if (clk[DC_FAILURE] != 0.0 || clk[DC_DONE] != 0.0) return;
     clk[DC_T] += clk[DC_DT];
     clk[DC_STEP] += 1.0;
     if (!(clk[DC_T] < c.tfinal) || !(clk[DC_STEP] < c.nmax)) clk[DC_DONE] = 1.0;
+}
+__global__ void k_clock_after(double* __restrict__ clk, ClockConst c) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    clock_after_body(clk, c);
+}
+
+// ---- batched forms over the grids of a batch --------------------------------
+template <typename F, int NF>
+__global__ void __launch_bounds__(kTX * kTY) k_delta4_batch(const F* __restrict__ f0, const F* __restrict__ f1,
+                                                           F* __restrict__ o0, F* __restrict__ o1, int p0, int p1,
+                                                           const BatchGrid* __restrict__ grids,
+                                                           const BatchTile* __restrict__ tiles) {
+    __shared__ F tile[NF][kTY + 4][kTX + 4];
+    const BatchTile t = tiles[blockIdx.x];
+    const BatchGrid& G = grids[t.grid];
+    Weights3 w0, w1;
+    for (int d = 0; d < 3; ++d) {
+        w0.w[d] = p0 == 2 ? G.h[d] * G.h[d] : G.h[d];
+        w1.w[d] = p1 == 2 ? G.h[d] * G.h[d] : G.h[d];
+    }
+    delta4_tile<F, NF>(f0 + G.off, f1 ? f1 + G.off : nullptr, o0 + G.off, o1 ? o1 + G.off : nullptr, G.g, w0, w1,
+                       t.x0, t.y0, t.z0, tile);
+}
+
+template <typename F>
+__global__ void k_rate_batch_partial(const double* __restrict__ Q, const F* __restrict__ prim,
+                                     const F* __restrict__ art, const BatchGrid* __restrict__ grids,
+                                     const BatchChunk* __restrict__ chunks, double* __restrict__ part, int64_t ct,
+                                     int Ns, double mu0, double Pr, double Sc) {
+    const BatchChunk ch = chunks[blockIdx.x];
+    const BatchGrid& G = grids[ch.grid];
+    double idx[3];
+    int act[3];
+    for (int d = 0; d < 3; ++d) { idx[d] = 1.0 / G.h[d]; act[d] = G.g.active[d]; }
+    double rate = 0.0, rmin = __longlong_as_double(0x7ff0000000000000LL);
+    const int64_t end = min(ch.c0 + (int64_t)kBatchChunk, G.cells);
+    for (int64_t c = ch.c0 + threadIdx.x; c < end; c += blockDim.x)
+        rate_cell(Q, prim, art, G.off + c, ct, Ns, idx, act, mu0, Pr, Sc, rate, rmin);
+    rate_block_reduce(rate, rmin, part, blockIdx.x);
+}
+
+// One block per grid: the grid's max / min over its chunk partials, then its clock_before.
+__global__ void k_rate_batch_final(const double* __restrict__ part, const int* __restrict__ chunk_first,
+                                   const BatchGrid* __restrict__ grids) {
+    const int g = blockIdx.x;
+    double rate = 0.0, rmin = __longlong_as_double(0x7ff0000000000000LL);
+    for (int b = chunk_first[g] + threadIdx.x; b < chunk_first[g + 1]; b += blockDim.x) {
+        rate = jl_max(rate, part[2 * b]);
+        rmin = jl_min(rmin, part[2 * b + 1]);
+    }
+    __shared__ double out[2];
+    // the same tree as k_rate_final, into out[]
+    rate_block_reduce(rate, rmin, out, 0);
+    __syncthreads();
+    if (threadIdx.x == 0) clock_before_body(grids[g].clk, out[0], out[1], grids[g].cc);
+}
+
+__global__ void k_bc_batch(double* __restrict__ Q, const BatchGrid* __restrict__ grids,
+                           const BatchFace* __restrict__ faces, int64_t ct, int Ns) {
+    const BatchFace& f = faces[blockIdx.x];
+    const BatchGrid& G = grids[f.grid];
+    bc_plane_body(Q + G.off, G.g, ct, f.d, f.side, Ns, f.kind, f.st, nullptr, threadIdx.x, blockDim.x);
+}
+
+__global__ void k_clock_after_batch(const BatchGrid* __restrict__ grids, int G) {
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g < G) clock_after_body(grids[g].clk, grids[g].cc);
 }
 
 }  // namespace
@@ -899,6 +1000,42 @@ void clock_before(double* clk, const double* rate_rmin, const ClockConst& c, cud
     count_launch();
     check_launch("k_clock_before");
 }
+template <typename F>
+void BatchOps<F>::delta4(const F* f0, const F* f1, F* o0, F* o1, int p0, int p1, const BatchGrid* grids,
+                         const BatchTile* tiles, int ntiles, int64_t, cudaStream_t st) {
+    if (ntiles <= 0) return;
+    if (f1) k_delta4_batch<F, 2><<<ntiles, kTX * kTY, 0, st>>>(f0, f1, o0, o1, p0, p1, grids, tiles);
+    else k_delta4_batch<F, 1><<<ntiles, kTX * kTY, 0, st>>>(f0, f1, o0, o1, p0, p1, grids, tiles);
+    count_launch();
+    check_launch("k_delta4_batch");
+}
+template <typename F>
+void BatchOps<F>::rate_clock(const double* Q, const F* prim, const F* art, const BatchGrid* grids, int G,
+                             const BatchChunk* chunks, int nchunks, const int* chunk_first, double* part,
+                             int64_t ct, int Ns, double mu0, double Pr, double Sc, cudaStream_t st) {
+    k_rate_batch_partial<F><<<nchunks, kThreads, 0, st>>>(Q, prim, art, grids, chunks, part, ct, Ns, mu0, Pr, Sc);
+    count_launch();
+    check_launch("k_rate_batch_partial");
+    k_rate_batch_final<<<G, kThreads, 0, st>>>(part, chunk_first, grids);
+    count_launch();
+    check_launch("k_rate_batch_final");
+}
+template struct BatchOps<double>;
+template struct BatchOps<float>;
+
+void batch_bc(double* Q, const BatchGrid* grids, const BatchFace* faces, int nfaces, int64_t ct, int Ns,
+              cudaStream_t st) {
+    if (nfaces <= 0) return;
+    k_bc_batch<<<nfaces, kThreads, 0, st>>>(Q, grids, faces, ct, Ns);
+    count_launch();
+    check_launch("k_bc_batch");
+}
+void batch_clock_after(const BatchGrid* grids, int G, cudaStream_t st) {
+    k_clock_after_batch<<<(G + 127) / 128, 128, 0, st>>>(grids, G);
+    count_launch();
+    check_launch("k_clock_after_batch");
+}
+
 void clock_after(double* clk, const ClockConst& c, cudaStream_t st) {
     k_clock_after<<<1, 32, 0, st>>>(clk, c);
     count_launch();

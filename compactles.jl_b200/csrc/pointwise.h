@@ -234,4 +234,41 @@ void clock_before(double* clk, const double* rate_rmin, const ClockConst& c, cud
 void clock_after(double* clk, const ClockConst& c, cudaStream_t st);
 int64_t rate_partials(int64_t cells);
 
+// ---- many grids advanced together (batch.cpp) ------------------------------
+// The fields of every grid of a batch live in shared arena blocks: field f of
+// grid g starts at element f * cells_total + off.  Per-cell kernels run over
+// all cells_total elements at once; the kernels below take tables of grids,
+// tiles, faces and cell chunks.
+struct BatchGrid {
+    Grid3 g;
+    int64_t off;      // element offset of the grid's cell (0, 0, 0) in every block
+    int64_t cells;
+    double h[3];      // grid spacing (1 on a collapsed dimension)
+    double* clk;      // graph-mode clock (DC_* slots) of this grid
+    ClockConst cc;
+};
+struct BatchTile { int grid, x0, y0, z0; };     // one delta4 tile (32 x 8 x 32 cells)
+struct BatchFace { int grid, d, side, kind; BcState st; };
+struct BatchChunk { int grid; int64_t c0; };    // cells [c0, c0 + kBatchChunk) of a grid
+constexpr int kBatchChunk = 2048;
+
+template <typename F>
+struct BatchOps {
+    // delta4_sum! of one (f1 == nullptr) or two fields of every grid; field k
+    // is weighted by h_d^pk per dimension
+    static void delta4(const F* f0, const F* f1, F* o0, F* o1, int p0, int p1, const BatchGrid* grids,
+                       const BatchTile* tiles, int ntiles, int64_t cells_total, cudaStream_t st);
+    // max_rate of every grid (per-chunk partials, then one block per grid
+    // reduces them) followed by the graph-mode clock_before of that grid;
+    // chunk_first[g] .. chunk_first[g + 1] are grid g's chunks
+    static void rate_clock(const double* Q, const F* prim, const F* art, const BatchGrid* grids, int G,
+                           const BatchChunk* chunks, int nchunks, const int* chunk_first, double* part,
+                           int64_t cells_total, int Ns, double mu0, double Pr, double Sc, cudaStream_t st);
+};
+// enforce! on the listed faces (one block per face)
+void batch_bc(double* Q, const BatchGrid* grids, const BatchFace* faces, int nfaces, int64_t cells_total, int Ns,
+              cudaStream_t st);
+// clock_after of every grid
+void batch_clock_after(const BatchGrid* grids, int G, cudaStream_t st);
+
 }  // namespace cles

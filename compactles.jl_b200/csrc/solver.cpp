@@ -42,15 +42,20 @@ void DevBuf::release() {
     bytes = 0;
 }
 
+// LSRK(5,4) coefficients (src/timestep.jl:5-21)
+const double kLsrkA[5] = {0.0, -567301805773.0 / 1357537059087.0, -2404267990393.0 / 2016746695238.0,
+                          -3550918686646.0 / 2091501179385.0, -1275806237668.0 / 842570457699.0};
+const double kLsrkB[5] = {1432997174477.0 / 9575080441755.0, 5161836677717.0 / 13612068292357.0,
+                          1720146321549.0 / 2090206949498.0, 3134564353537.0 / 4481467310338.0,
+                          2277821191437.0 / 14882151754819.0};
+const double kLsrkC[5] = {0.0, 1432997174477.0 / 9575080441755.0, 2526269341429.0 / 6820363962896.0,
+                          2006345519317.0 / 3224310063776.0, 2802321613138.0 / 2924317926251.0};
+
 namespace {
 
-const double RKA[5] = {0.0, -567301805773.0 / 1357537059087.0, -2404267990393.0 / 2016746695238.0,
-                       -3550918686646.0 / 2091501179385.0, -1275806237668.0 / 842570457699.0};
-const double RKB[5] = {1432997174477.0 / 9575080441755.0, 5161836677717.0 / 13612068292357.0,
-                       1720146321549.0 / 2090206949498.0, 3134564353537.0 / 4481467310338.0,
-                       2277821191437.0 / 14882151754819.0};
-const double RKC[5] = {0.0, 1432997174477.0 / 9575080441755.0, 2526269341429.0 / 6820363962896.0,
-                       2006345519317.0 / 3224310063776.0, 2802321613138.0 / 2924317926251.0};
+const double (&RKA)[5] = kLsrkA;
+const double (&RKB)[5] = kLsrkB;
+const double (&RKC)[5] = kLsrkC;
 const double PLANCK_TIME = 5.391247e-44;
 
 inline double jmax(double x, double y) {

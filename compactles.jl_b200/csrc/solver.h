@@ -84,4 +84,24 @@ void copy_state_d2h(double* host, const double* dev, const int n[3], const int p
 
 int check_step(const cles_step_control& c, double dt, double rho_min, double dt_seen);
 
+// Many solves of one physics class advanced together (batch.cpp).
+class BatchBase {
+public:
+    virtual ~BatchBase() = default;
+    virtual int64_t add(const cles_solver_desc& d, const double* Q0, int layout, double tfinal, int64_t nmax,
+                        double now) = 0;
+    virtual int step(double now) = 0;          // returns the members still running
+    virtual int n_active() const = 0;
+    virtual void remove(int64_t id, double now) = 0;
+    virtual void status(int64_t id, cles_request_status* out) const = 0;
+    virtual void fetch(int64_t id, double* Q, int layout) = 0;
+    virtual void stats(cles_batch_stats* s) const = 0;
+};
+std::unique_ptr<BatchBase> make_batch(cles_ctx* ctx, const cles_solver_desc& cls);
+// d fits a batch of class cls (supported and equal in every class field)
+bool batch_compatible(const cles_solver_desc& cls, const cles_solver_desc& d);
+
+// LSRK(5,4) coefficients A, B, C per stage (src/timestep.jl:5-21)
+extern const double kLsrkA[5], kLsrkB[5], kLsrkC[5];
+
 }  // namespace cles

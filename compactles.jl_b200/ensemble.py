@@ -4,17 +4,22 @@
 log-uniform in [128, 1024] x [64, 256] and rounded to even, shock Mach number
 uniform in [1.2, 2.5], an 8-mode interface perturbation of its own seed, slip
 walls in x, periodic y, run to t_end = 0.5 Lx / c_He
-(compactles.jl_b200/scenarios.shock_interface_2d).  The whole ensemble is
-submitted at once to a cles_server and advanced by continuous batching, each
-request one CUDA-graph launch per step on its own stream; this is done in
-mixed precision and again in FP64 on the same GPU.
+(compactles.jl_b200/scenarios.shock_interface_2d).  Two ways to run the
+whole ensemble, each in mixed precision and in FP64 on the same GPU:
+  batch   one cles_batch: every case's fields in one arena, one captured
+          CUDA graph per composition, a fixed number of launches per step
+          for all cases together (line solves from per-grid descriptor
+          tables, autotuned lines per CTA); cases retire as they finish;
+  server  a cles_server: each case its own solver and stream, one CUDA-graph
+          launch per case per step.
 
-Reported: aggregate cell-steps/s (sum over cases of cells x steps, over the
-wall time of the batch), solves/s, and per case the relative L2 difference of
-the mixed-precision end state from the FP64 end state (max over conserved
-components).
+Reported per mode and precision: aggregate cell-steps/s (sum over cases of
+cells x steps, over the wall time of the whole ensemble), solves/s, and per
+case the relative L2 difference of the mixed-precision end state from the
+FP64 end state (max over conserved components); for the batch, its
+compositions, launches per step and the autotuner's choices.
 
-  python compactles.jl_b200/ensemble.py [--cases 64] [--seed 7]
+  python compactles.jl_b200/ensemble.py [--cases 64] [--seed 7] [--modes batch,server]
 """
 import argparse
 import importlib.util
@@ -66,6 +71,22 @@ def serve(cl, reqs, max_active, budget):
     return wall, steps, states
 
 
+def run_batch(cl, reqs):
+    B = cl.Batch(reqs[0][0])
+    t0 = time.perf_counter()
+    ids = [B.add(desc, Q0, tf) for desc, Q0, tf in reqs]
+    B.run()
+    wall = time.perf_counter() - t0
+    states, steps = [], []
+    for mid in ids:
+        st = B.status(mid)
+        if st["state"] != "done":
+            raise RuntimeError(f"member ended {st['state']} ({st['failure']})")
+        steps.append(st["steps"])
+        states.append(B.fetch(mid))
+    return wall, steps, states, B.stats()
+
+
 def rel_l2(a, b, desc):
     sl = (slice(None),) + _package().problem.interior_slices(desc)
     a, b = a[sl], b[sl]
@@ -79,6 +100,7 @@ def main(argv=None):
     p.add_argument("--max-active", type=int, default=64)
     p.add_argument("--budget-gb", type=float, default=100.0)
     p.add_argument("--precisions", default="mixed,fp64")
+    p.add_argument("--modes", default="batch,server")
     a = p.parse_args(argv)
     cl = _package()
     sch = (cl.lele_d1_6(), cl.compact_filter(0.45))
@@ -90,22 +112,42 @@ def main(argv=None):
         s.set_state(wd[1])
         s.run_graph(wd[2], 5)
         del s
+        wb = cl.Batch(wd[0])
+        wb.add(*wd)
+        wb.run(5)
+        del wb
     res, states = {}, {}
-    for prec in a.precisions.split(","):
-        reqs = [cl.scenarios.shock_interface_2d(sch, nx, ny, M, sd, precision=prec) for nx, ny, M, sd in cases]
-        wall, steps, st = serve(cl, reqs, a.max_active, int(a.budget_gb * (1 << 30)))
-        cs = sum(nx * ny * k for (nx, ny, _, _), k in zip(cases, steps))
-        res[prec] = {"wall_s": wall, "cell_steps": cs, "cell_steps_per_s": cs / wall,
-                     "solves_per_s": len(cases) / wall, "steps_total": int(sum(steps))}
-        states[prec] = (reqs, st)
+    for mode in a.modes.split(","):
+        for prec in a.precisions.split(","):
+            reqs = [cl.scenarios.shock_interface_2d(sch, nx, ny, M, sd, precision=prec) for nx, ny, M, sd in cases]
+            extra = {}
+            if mode == "batch":
+                wall, steps, st, bstats = run_batch(cl, reqs)
+                extra = {"compositions": bstats["compositions"], "launches_per_step": bstats["launches_per_step"],
+                         "batch_steps": bstats["steps"], "tuning_last": bstats["tuning"]}
+            else:
+                wall, steps, st = serve(cl, reqs, a.max_active, int(a.budget_gb * (1 << 30)))
+            cs = sum(nx * ny * k for (nx, ny, _, _), k in zip(cases, steps))
+            res[f"{mode}_{prec}"] = {"wall_s": wall, "cell_steps": cs, "cell_steps_per_s": cs / wall,
+                                     "solves_per_s": len(cases) / wall, "steps_total": int(sum(steps)), **extra}
+            states[(mode, prec)] = (reqs, st)
     out = {"workload": f"{a.cases} 2-D He/CO2 shock-interface cases, seed {a.seed}, "
-                       "nx 128-1024, ny 64-256, t_end 0.5 Lx/c_He, served concurrently",
+                       "nx 128-1024, ny 64-256, t_end 0.5 Lx/c_He",
            "results": res}
-    if "mixed" in states and "fp64" in states:
-        errs = [rel_l2(m, f, r[0]) for r, m, f in zip(states["fp64"][0], states["mixed"][1], states["fp64"][1])]
-        out["mixed_vs_fp64_rel_l2"] = {"max": max(errs), "median": float(np.median(errs)),
-                                       "per_case": [float(e) for e in errs]}
-        out["mixed_speedup"] = res["mixed"]["cell_steps_per_s"] / res["fp64"]["cell_steps_per_s"]
+    for mode in a.modes.split(","):
+        if (mode, "mixed") in states and (mode, "fp64") in states:
+            f, m = states[(mode, "fp64")], states[(mode, "mixed")]
+            errs = [rel_l2(x, y, r[0]) for r, x, y in zip(f[0], m[1], f[1])]
+            out[f"{mode}_mixed_vs_fp64_rel_l2"] = {"max": max(errs), "median": float(np.median(errs))}
+            out[f"{mode}_mixed_speedup"] = (res[f"{mode}_mixed"]["cell_steps_per_s"] /
+                                            res[f"{mode}_fp64"]["cell_steps_per_s"])
+    if ("batch", "fp64") in states and ("server", "fp64") in states:
+        b, s_ = states[("batch", "fp64")], states[("server", "fp64")]
+        errs = [rel_l2(x, y, r[0]) for r, x, y in zip(b[0], b[1], s_[1])]
+        out["batch_vs_server_fp64_rel_l2_max"] = max(errs)
+        for prec in a.precisions.split(","):
+            out[f"batch_over_server_{prec}"] = (res[f"batch_{prec}"]["cell_steps_per_s"] /
+                                                res[f"server_{prec}"]["cell_steps_per_s"])
     print(json.dumps(out), flush=True)
     return out
 

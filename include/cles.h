@@ -558,6 +558,66 @@ int  cles_server_status(cles_server* s, int64_t id, cles_request_status* out);
 int  cles_server_fetch(cles_server* s, int64_t id, double* Q_host);
 int  cles_server_cancel(cles_server* s, int64_t id);
 
+/* ---- batches: many solves of one physics class advanced together --------
+ * No counterpart in the reference (one problem per process there).  A batch
+ * holds independent solves ("members") that share everything in the solver
+ * descriptor except the grid extents (n_global, with the same dimensions
+ * active), the domain (L, origin) and the boundary states: species, transport,
+ * artificial-property parameters, schemes, cfl, filter_interval, step-control
+ * floors, precision and the kind of every face.  Supported: ideal mixtures on
+ * uniform Cartesian grids with periodic, slip-wall, no-slip-wall,
+ * extrapolation and constant Dirichlet faces, stepped as run! in graph mode
+ * (no rate prediction, growth cap or rollback).  cles_batch_create takes the
+ * class from `cls` (its grid fields are ignored apart from which dimensions
+ * are active); CLES_EINVAL names the first differing field of a member.
+ *
+ * Every member's fields live in one device arena, so one step of the whole
+ * batch is a fixed number of kernel launches -- per-cell kernels over every
+ * member's cells at once, line solves, stencils, boundary planes and
+ * reductions from per-grid descriptor tables -- captured once as a CUDA
+ * graph per batch composition.  Each member keeps its own dt, clock, end
+ * time and SolverFailure checks.  The composition changes when members are
+ * added, finish, fail or are cancelled; the next step then rebuilds the arena
+ * and tables and re-captures the graph.  A project-written autotuner times
+ * the thread count (lines per CTA, x-tile depth) of every batched line-solve
+ * launch the first time a launch shape is built and keeps the fastest.  A
+ * member's arithmetic does not depend on the other members, so its results
+ * are the same alone and in any mix. */
+typedef struct cles_batch cles_batch;
+typedef struct cles_batch_tuning {
+    int     op;          /* 0 derivative, 1 filter of derived fields, 2 filter_state! of Q */
+    int     dim;         /* 1-based direction */
+    int     threads;     /* chosen threads per CTA */
+    int64_t smem;        /* dynamic shared memory per CTA */
+    int     ctas;        /* CTAs per field */
+    double  tuned_ms;    /* the winner's time per launch (one field) when it was tuned here, else 0 */
+} cles_batch_tuning;
+typedef struct cles_batch_stats {
+    int     members;           /* added so far */
+    int     active;            /* not yet finished, failed or cancelled */
+    int     compositions;      /* arena rebuilds / graph captures */
+    int64_t steps;             /* batch steps (graph launches) */
+    int     launches_per_step; /* kernels in one captured step */
+    int64_t cells_total;       /* arena cells of the current composition (with alignment padding) */
+    int     n_roles;
+    cles_batch_tuning tuning[9];
+} cles_batch_stats;
+int  cles_batch_create(cles_ctx* ctx, const cles_solver_desc* cls, cles_batch** out);
+void cles_batch_destroy(cles_batch* b);
+/* Adds a member with its initial state (host, padded or interior layout);
+ * it joins the batch at the next step. */
+int  cles_batch_add(cles_batch* b, const cles_solver_desc* desc, const double* Q0_host, int layout, double tfinal,
+                    int64_t nmax, int64_t* id);
+/* One run! step of every running member; *n_active = members still running. */
+int  cles_batch_step(cles_batch* b, int* n_active);
+/* Steps until no member is running or max_steps batch steps were taken. */
+int  cles_batch_run(cles_batch* b, int64_t max_steps, int* n_active);
+int  cles_batch_status(cles_batch* b, int64_t id, cles_request_status* out);
+/* A member's current (or final) state, in the layout it was added with. */
+int  cles_batch_fetch(cles_batch* b, int64_t id, double* Q_host);
+int  cles_batch_cancel(cles_batch* b, int64_t id);
+int  cles_batch_stats_get(const cles_batch* b, cles_batch_stats* out);
+
 /* Volume-averaged kinetic energy ∫½ρ|u|²dV / V and dissipation rate
  * (src/diagnostics.jl:354-378, bench/tgv_energy.jl:175-184) of the resident
  * state. */
