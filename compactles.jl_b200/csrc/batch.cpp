@@ -24,10 +24,11 @@
 // Autotuning.  Each batched line-solve launch has one free knob: the threads
 // per CTA, which fixes the lines per CTA (LB = threads / S) for y/z lines and
 // the depth of the transposed shared-memory tile for x lines.  The first time
-// a launch of a given shape is built (direction, operator, element type and
-// the grids' line lengths and counts), every candidate (128, 256, 512 threads
-// that fit the segments and shared memory) is timed with CUDA events on the
-// batch's own fields and the fastest is kept for that shape.
+// a launch of a given shape is built (operator, direction, element type, the
+// largest segment count and the total line count to within a factor of two),
+// every candidate (128, 256, 512 threads that fit the segments and shared
+// memory) is timed with CUDA events on the batch's own fields and the fastest
+// is kept for that shape.
 //
 // Arithmetic per grid does not depend on the composition (segmentation is a
 // function of the line length alone, reductions are max / min), so a member's
@@ -260,9 +261,20 @@ public:
     }
 
     int step(double now) override {
+        launch(now);
+        return collect(now);
+    }
+
+    void launch(double now) override {
         if (dirty_) compose(now);
-        if (order_.empty()) return 0;
+        if (order_.empty()) return;
         CLES_CUDA(cudaGraphLaunch(exec_, st_));
+        launched_ = true;
+    }
+
+    int collect(double now) override {
+        if (!launched_) return n_active_after_step();
+        launched_ = false;
         CLES_CUDA(cudaStreamSynchronize(st_));
         ++steps_;
         for (size_t g = 0; g < order_.size(); ++g) {
@@ -601,15 +613,22 @@ private:
         return true;
     }
 
+    // The launch shape the tuned choice is kept for: operator, direction,
+    // element type, bandwidth, periodicity, the largest segment count and the
+    // total line count to within a factor of two (so compositions that differ
+    // by a few members reuse the choice instead of timing again).
     std::string role_key(int role, int k) const {
-        std::vector<std::pair<int, int64_t>> v;
-        for (Member* m : order_) v.emplace_back(m->n[k], m->cells / m->n[k]);
-        std::sort(v.begin(), v.end());
-        std::string key = std::to_string(role) + "/" + std::to_string(k) + "/" + std::to_string(sizeof(F)) + "/" +
-                          std::to_string(cls_.deriv.q) + std::to_string(cls_.filt.q) + "/" +
-                          std::to_string(periodic_of(k));
-        for (auto& e : v) key += ":" + std::to_string(e.first) + "x" + std::to_string(e.second);
-        return key;
+        int smax = 0;
+        int64_t lines = 0;
+        for (Member* m : order_) {
+            smax = std::max(smax, plan_of(*m, role, k)->P.S);
+            lines += m->cells / m->n[k];
+        }
+        int lg = 0;
+        while ((int64_t)1 << (lg + 1) <= lines) ++lg;
+        return std::to_string(role) + "/" + std::to_string(k) + "/" + std::to_string(sizeof(F)) + "/" +
+               std::to_string(cls_.deriv.q) + std::to_string(cls_.filt.q) + "/" + std::to_string(periodic_of(k)) +
+               "/S" + std::to_string(smax) + "/L" + std::to_string(lg);
     }
     int periodic_of(int k) const { return cls_.bc[k][0] == CLES_BC_PERIODIC ? 1 : 0; }
 
@@ -783,7 +802,7 @@ private:
     std::vector<Member*> order_;
     std::vector<int64_t> cancelled_;
     int64_t next_id_ = 1;
-    bool dirty_ = false;
+    bool dirty_ = false, launched_ = false;
     int64_t ct_ = 0;
     DevBuf Q_, art_, clk_;
     DevBuf du_, dQ_, prim_, g_u_, gty_, scratch_, flux_, part_;

@@ -84,15 +84,26 @@ inline unsigned grid_for(int64_t n) {
     return (unsigned)(b < 1 ? 1 : b);
 }
 
+#define LAUNCH(kern, n, st, ...)                                      \
+    do {                                                               \
+        kern<<<grid_for(n), kThreads, 0, st>>>(__VA_ARGS__);           \
+        count_launch();                                                \
+        check_launch(#kern);                                           \
+    } while (0)
+
 #define GRID_STRIDE(idx, n) for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < (n); idx += (int64_t)gridDim.x * blockDim.x)
 
 // _primitives!(::IdealMixture) (src/physics.jl:604-653) at the interior, and
 // _primitives!(::Nasa9Mixture) (src/physics.jl:501-570) when N9 (a separate
 // instantiation, so the ideal-gas kernel keeps its small register footprint).
-template <typename F, bool N9>
+// PM (batched solves): the species constants are per batch member, mc[24 m ..]
+// = R_k, cv_k, cp_k (8 each) of member m = tmap[cell / 64].
+template <typename F, bool N9, bool PM = false>
 __global__ void k_primitives(const double* __restrict__ Q, F* __restrict__ prim, int64_t cells, int Ns, PhysConst pc,
-                             int esens) {
+                             int esens, const double* __restrict__ mc = nullptr, const int* __restrict__ tmap = nullptr) {
     GRID_STRIDE(I, cells) {
+        const double* mcI = nullptr;
+        if constexpr (PM) mcI = mc + 24 * tmap[I >> 6];
         double rho = 0.0;
         for (int sp = 0; sp < Ns; ++sp) rho += Q[I + cells * sp];
         F* out = prim + I;
@@ -132,8 +143,13 @@ __global__ void k_primitives(const double* __restrict__ Q, F* __restrict__ prim,
             double Rm = 0.0, cvm = 0.0;
             for (int sp = 0; sp < Ns; ++sp) {
                 const double q = Q[I + cells * sp];
-                Rm += q * pc.Rk[sp];
-                cvm += q * pc.cvk[sp];
+                if constexpr (PM) {
+                    Rm += q * mcI[sp];
+                    cvm += q * mcI[8 + sp];
+                } else {
+                    Rm += q * pc.Rk[sp];
+                    cvm += q * pc.cvk[sp];
+                }
                 out[cells * (P_Y0 + sp)] = F(q * ri);
             }
             Rm *= ri;
@@ -428,10 +444,11 @@ __global__ void k_dart(const F* __restrict__ sensor, const F* __restrict__ prim,
 // SINGLE (one species): the species diffusion flux rho D dY (Y - 1) is zero in
 // exact arithmetic (Y = 1) and below ~1e-30 of the momentum flux in FP64, so it
 // is taken as 0 and dY/dx_d is neither computed nor read (gty holds dT only).
-template <typename F, bool SINGLE, bool N9, bool GEO>
+template <typename F, bool SINGLE, bool N9, bool GEO, bool PM = false>
 __global__ void k_fluxes(const double* __restrict__ Q, const F* __restrict__ prim, const F* __restrict__ g,
                          const F* __restrict__ gty, const F* __restrict__ art, F* __restrict__ flux, int64_t cells,
-                         int Ns, PhysConst pc, double mu0, double Pr, double Sc, Geom G) {
+                         int Ns, PhysConst pc, double mu0, double Pr, double Sc, Geom G,
+                         const double* __restrict__ mc = nullptr, const int* __restrict__ tmap = nullptr) {
     if (SINGLE) Ns = 1;
     const int ncons = Ns + 4;
     const int gstride = SINGLE ? 1 : 1 + Ns;
@@ -489,7 +506,8 @@ __global__ void k_fluxes(const double* __restrict__ Q, const F* __restrict__ pri
                     const double Jkd = r * (-Dk * double(gd[I + cells * (1 + sp)]) + Yk * Vc);
                     const double fk = r * Yk * ud + Jkd;
                     fd[I + cells * sp] = F(CLES_AF(fk));
-                    hdiff += (N9 ? n9_h(pc, sp, Tp) : pc.cpk[sp] * Tp) * Jkd;
+                    if constexpr (PM) hdiff += mc[24 * tmap[I >> 6] + 16 + sp] * Tp * Jkd;
+                    else hdiff += (N9 ? n9_h(pc, sp, Tp) : pc.cpk[sp] * Tp) * Jkd;
                 }
             }
             const double m0 = r * ud * uv[0] + (d == 0 ? p : 0.0) - td[0];
@@ -1020,6 +1038,23 @@ void BatchOps<F>::rate_clock(const double* Q, const F* prim, const F* art, const
     count_launch();
     check_launch("k_rate_batch_final");
 }
+template <typename F>
+void BatchOps<F>::primitives(const double* Q, F* prim, int64_t ct, int Ns, const PhysConst& pc, int esens,
+                             const double* mc, const int* tmap, cudaStream_t st) {
+    LAUNCH((k_primitives<F, false, true>), ct, st, Q, prim, ct, Ns, pc, esens, mc, tmap);
+}
+template <typename F>
+void BatchOps<F>::fluxes(const double* Q, const F* prim, const F* g, const F* gty, const F* art, F* flux, int64_t ct,
+                         int Ns, const PhysConst& pc, double mu0, double Pr, double Sc, const double* mc,
+                         const int* tmap, cudaStream_t st) {
+    const Geom G{};
+    if (Ns == 1)
+        LAUNCH((k_fluxes<F, true, false, false>), ct, st, Q, prim, g, gty, art, flux, ct, Ns, pc, mu0, Pr, Sc, G,
+               nullptr, nullptr);
+    else
+        LAUNCH((k_fluxes<F, false, false, false, true>), ct, st, Q, prim, g, gty, art, flux, ct, Ns, pc, mu0, Pr, Sc,
+               G, mc, tmap);
+}
 template struct BatchOps<double>;
 template struct BatchOps<float>;
 
@@ -1043,18 +1078,12 @@ void clock_after(double* clk, const ClockConst& c, cudaStream_t st) {
 }
 
 // ------------------------------------------------------------- launchers ----
-#define LAUNCH(kern, n, st, ...)                                      \
-    do {                                                               \
-        kern<<<grid_for(n), kThreads, 0, st>>>(__VA_ARGS__);           \
-        count_launch();                                                \
-        check_launch(#kern);                                           \
-    } while (0)
 
 template <typename F>
 void Pointwise<F>::primitives(const double* Q, F* prim, int64_t cells, int Ns, const PhysConst& pc, cudaStream_t st,
                               int esens) {
-    if (pc.eos == CLES_EOS_NASA9) LAUNCH((k_primitives<F, true>), cells, st, Q, prim, cells, Ns, pc, esens);
-    else LAUNCH((k_primitives<F, false>), cells, st, Q, prim, cells, Ns, pc, esens);
+    if (pc.eos == CLES_EOS_NASA9) LAUNCH((k_primitives<F, true>), cells, st, Q, prim, cells, Ns, pc, esens, nullptr, nullptr);
+    else LAUNCH((k_primitives<F, false>), cells, st, Q, prim, cells, Ns, pc, esens, nullptr, nullptr);
 }
 template <typename F>
 void Pointwise<F>::delta4_tiled(const F* f0, const F* f1, F* o0, F* o1, const Grid3& g, const double w0[3],
@@ -1117,22 +1146,22 @@ void Pointwise<F>::fluxes(const double* Q, const F* prim, const F* g, const F* g
                           cudaStream_t st) {
     const Geom G{};
     if (Ns == 1)
-        LAUNCH((k_fluxes<F, true, false, false>), cells, st, Q, prim, g, gty, art, flux, cells, Ns, pc, mu0, Pr, Sc, G);
+        LAUNCH((k_fluxes<F, true, false, false>), cells, st, Q, prim, g, gty, art, flux, cells, Ns, pc, mu0, Pr, Sc, G, nullptr, nullptr);
     else if (pc.eos == CLES_EOS_NASA9)
-        LAUNCH((k_fluxes<F, false, true, false>), cells, st, Q, prim, g, gty, art, flux, cells, Ns, pc, mu0, Pr, Sc, G);
+        LAUNCH((k_fluxes<F, false, true, false>), cells, st, Q, prim, g, gty, art, flux, cells, Ns, pc, mu0, Pr, Sc, G, nullptr, nullptr);
     else
-        LAUNCH((k_fluxes<F, false, false, false>), cells, st, Q, prim, g, gty, art, flux, cells, Ns, pc, mu0, Pr, Sc, G);
+        LAUNCH((k_fluxes<F, false, false, false>), cells, st, Q, prim, g, gty, art, flux, cells, Ns, pc, mu0, Pr, Sc, G, nullptr, nullptr);
 }
 template <typename F>
 void Pointwise<F>::fluxes_geo(const double* Q, const F* prim, const F* g, const F* gty, const F* art, F* flux,
                               int64_t cells, int Ns, const PhysConst& pc, double mu0, double Pr, double Sc,
                               const Geom& G, cudaStream_t st) {
     if (Ns == 1)
-        LAUNCH((k_fluxes<F, true, false, true>), cells, st, Q, prim, g, gty, art, flux, cells, Ns, pc, mu0, Pr, Sc, G);
+        LAUNCH((k_fluxes<F, true, false, true>), cells, st, Q, prim, g, gty, art, flux, cells, Ns, pc, mu0, Pr, Sc, G, nullptr, nullptr);
     else if (pc.eos == CLES_EOS_NASA9)
-        LAUNCH((k_fluxes<F, false, true, true>), cells, st, Q, prim, g, gty, art, flux, cells, Ns, pc, mu0, Pr, Sc, G);
+        LAUNCH((k_fluxes<F, false, true, true>), cells, st, Q, prim, g, gty, art, flux, cells, Ns, pc, mu0, Pr, Sc, G, nullptr, nullptr);
     else
-        LAUNCH((k_fluxes<F, false, false, true>), cells, st, Q, prim, g, gty, art, flux, cells, Ns, pc, mu0, Pr, Sc, G);
+        LAUNCH((k_fluxes<F, false, false, true>), cells, st, Q, prim, g, gty, art, flux, cells, Ns, pc, mu0, Pr, Sc, G, nullptr, nullptr);
 }
 template <typename F>
 void Pointwise<F>::body_forces(F* dQ, const double* Q, int64_t cells, int Ns, const BodyForces& bf, cudaStream_t st) {

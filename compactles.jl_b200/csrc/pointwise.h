@@ -254,6 +254,13 @@ constexpr int kBatchChunk = 2048;
 
 template <typename F>
 struct BatchOps {
+    // primitives / fluxes of an ideal mixture whose species constants are per
+    // member: mc[24 m ..] = R_k, cv_k, cp_k (8 each) of member m = tmap[cell / 64]
+    static void primitives(const double* Q, F* prim, int64_t cells_total, int Ns, const PhysConst& pc, int esens,
+                           const double* mc, const int* tmap, cudaStream_t st);
+    static void fluxes(const double* Q, const F* prim, const F* g, const F* gty, const F* art, F* flux,
+                       int64_t cells_total, int Ns, const PhysConst& pc, double mu0, double Pr, double Sc,
+                       const double* mc, const int* tmap, cudaStream_t st);
     // delta4_sum! of one (f1 == nullptr) or two fields of every grid; field k
     // is weighted by h_d^pk per dimension
     static void delta4(const F* f0, const F* f1, F* o0, F* o1, int p0, int p1, const BatchGrid* grids,

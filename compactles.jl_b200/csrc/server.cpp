@@ -1,12 +1,18 @@
 // Continuous-batching server of independent solves on one device (cles_server_*).
 //
-// Each request owns a stream and a device-resident solver.  A tick admits
-// queued requests in arrival order while the active count and the HBM budget
-// allow, enqueues one run! step for every running request (one CUDA-graph
-// launch each, see SolverBase::graph_begin), waits for them together, and
-// retires finished or failed requests, returning their memory to the budget.
-// Requests never share buffers or reductions, so a result does not depend on
-// which other requests were in flight.
+// A tick admits queued requests in arrival order while the active count and
+// the HBM budget allow, enqueues one run! step for every running request,
+// waits for them together, and retires finished or failed requests, returning
+// their memory to the budget.  Two ways to hold a request:
+//   * its own stream and device-resident solver, one CUDA-graph launch per
+//     step (see SolverBase::graph_begin);
+//   * with batching on (cles_server_set_batching), a request the batch path
+//     supports joins a batch of its physics class (batch.cpp): the members'
+//     fields share one arena and one captured step of O(stages) launches
+//     advances them all, each with its own dt and end time.  Requests admitted
+//     while others run join the running batch at its next step.
+// Requests never share reductions or change each other's arithmetic, so a
+// result does not depend on which other requests were in flight.
 
 #include <chrono>
 #include <cstring>
@@ -37,7 +43,17 @@ struct Request {
     bool graph = true;
     cles_ctx ctx{};
     std::unique_ptr<SolverBase> solver;
+    int batch = -1;            // index of the batch slot holding it, or -1
+    int64_t member = 0;        // its id in that batch
     std::vector<double> Qout;
+};
+
+// One batch of a physics class with its own stream.
+struct BatchSlot {
+    cles_ctx ctx{};
+    cles_solver_desc cls{};
+    std::unique_ptr<BatchBase> b;
+    int members = 0;           // requests currently held
 };
 
 size_t state_elems(const cles_solver_desc& d, int layout) {
@@ -60,6 +76,8 @@ struct cles_server {
     std::deque<int64_t> queue;
     std::vector<int64_t> running;
     std::map<int64_t, std::unique_ptr<Request>> reqs;
+    bool batching = false;
+    std::vector<std::unique_ptr<BatchSlot>> batches;
     std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
     double now() const {
         return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
@@ -70,7 +88,37 @@ struct cles_server {
             cudaStreamDestroy(r.ctx.stream);
             r.ctx.stream = nullptr;
         }
+        if (r.batch >= 0) {
+            BatchSlot& b = *batches[r.batch];
+            b.members -= 1;
+            // an emptied batch is replaced by a fresh one, which frees its arena
+            if (b.members == 0) b.b = make_batch(&b.ctx, b.cls);
+            r.batch = -1;
+        }
         used -= r.bytes;
+    }
+    // the batch slot of r's class, created on first use
+    int batch_for(const cles_solver_desc& d) {
+        for (size_t i = 0; i < batches.size(); ++i)
+            if (batch_compatible(batches[i]->cls, d)) return (int)i;
+        auto slot = std::make_unique<BatchSlot>();
+        slot->ctx.device = device;
+        CLES_CUDA(cudaStreamCreateWithFlags(&slot->ctx.stream, cudaStreamNonBlocking));
+        slot->cls = d;
+        try {
+            slot->b = make_batch(&slot->ctx, d);
+        } catch (...) {
+            cudaStreamDestroy(slot->ctx.stream);
+            throw;
+        }
+        batches.push_back(std::move(slot));
+        return (int)batches.size() - 1;
+    }
+    ~cles_server() {
+        for (auto& b : batches) {
+            b->b.reset();
+            if (b->ctx.stream) cudaStreamDestroy(b->ctx.stream);
+        }
     }
 };
 
@@ -153,6 +201,29 @@ int cles_server_tick(cles_server* s, int* n_running, int* n_queued) {
     while (!s->queue.empty() && (int)s->running.size() < s->max_active) {
         Request& r = *s->reqs[s->queue.front()];
         if (s->budget && s->used + r.bytes > s->budget) break;
+        if (s->batching && r.graph && batch_compatible(r.desc, r.desc)) {
+            s->used += r.bytes;
+            try {
+                const int bi = s->batch_for(r.desc);
+                r.member = s->batches[bi]->b->add(r.desc, r.Q0.data(), r.layout, r.tfinal, r.nmax, s->now());
+                r.batch = bi;
+                s->batches[bi]->members += 1;
+            } catch (const Error& e) {
+                s->used -= r.bytes;
+                if (e.code == CLES_ENOMEM) break;
+                r.state = CLES_REQ_FAILED;
+                r.done_s = s->now();
+                s->queue.pop_front();
+                continue;
+            }
+            r.Q0.clear();
+            r.Q0.shrink_to_fit();
+            r.state = CLES_REQ_RUNNING;
+            r.admit_s = s->now();
+            s->queue.pop_front();
+            s->running.push_back(r.id);
+            continue;
+        }
         r.ctx.device = s->device;
         CLES_CUDA(cudaStreamCreateWithFlags(&r.ctx.stream, cudaStreamNonBlocking));
         s->used += r.bytes;
@@ -175,10 +246,14 @@ int cles_server_tick(cles_server* s, int* n_running, int* n_queued) {
         s->queue.pop_front();
         s->running.push_back(r.id);
     }
-    // one step for every running request; host-stepped ones run synchronously
+    // one step for every running request (every batch one captured step);
+    // host-stepped ones run synchronously
+    const double tnow = s->now();
+    for (auto& b : s->batches)
+        if (b->members > 0) b->b->launch(tnow);
     for (int64_t id : s->running) {
         Request& r = *s->reqs[id];
-        if (r.graph) r.solver->graph_launch();
+        if (r.graph && r.batch < 0) r.solver->graph_launch();
     }
     for (int64_t id : s->running) {
         Request& r = *s->reqs[id];
@@ -188,12 +263,38 @@ int cles_server_tick(cles_server* s, int* n_running, int* n_queued) {
             if (rc == CLES_EFAILURE) r.failure = res.failure;
         }
     }
-    for (int64_t id : s->running) CLES_CUDA(cudaStreamSynchronize(s->reqs[id]->ctx.stream));
+    for (auto& b : s->batches)
+        if (b->members > 0) b->b->collect(s->now());
+    for (int64_t id : s->running)
+        if (s->reqs[id]->batch < 0) CLES_CUDA(cudaStreamSynchronize(s->reqs[id]->ctx.stream));
     // retire finished and failed requests
     std::vector<int64_t> still;
     for (int64_t id : s->running) {
         Request& r = *s->reqs[id];
         bool done = false;
+        if (r.batch >= 0) {
+            BatchBase& B = *s->batches[r.batch]->b;
+            cles_request_status bs{};
+            B.status(r.member, &bs);
+            r.t = bs.t;
+            r.steps = bs.steps;
+            r.failure = bs.failure;
+            done = bs.state == CLES_REQ_DONE;
+            if (done) {
+                r.Qout.resize(state_elems(r.desc, r.layout));
+                B.fetch(r.member, r.Qout.data(), r.layout);
+                r.state = CLES_REQ_DONE;
+                r.done_s = s->now();
+                s->release(r);
+            } else if (bs.state == CLES_REQ_FAILED) {
+                r.state = CLES_REQ_FAILED;
+                r.done_s = s->now();
+                s->release(r);
+            } else {
+                still.push_back(id);
+            }
+            continue;
+        }
         if (r.graph) {
             const double* clk = r.solver->graph_clock();
             r.t = clk[DC_T];
@@ -223,6 +324,13 @@ int cles_server_tick(cles_server* s, int* n_running, int* n_queued) {
     s->running.swap(still);
     if (n_running) *n_running = (int)s->running.size();
     if (n_queued) *n_queued = (int)s->queue.size();
+    SAPI_END
+}
+
+int cles_server_set_batching(cles_server* s, int on) {
+    SAPI_BEGIN
+    if (!s) throw Error(CLES_EINVAL, "null server");
+    s->batching = on != 0;
     SAPI_END
 }
 
@@ -265,7 +373,8 @@ int cles_server_cancel(cles_server* s, int64_t id) {
         for (auto q = s->queue.begin(); q != s->queue.end(); ++q)
             if (*q == id) { s->queue.erase(q); break; }
     } else if (r.state == CLES_REQ_RUNNING) {
-        CLES_CUDA(cudaStreamSynchronize(r.ctx.stream));
+        if (r.batch >= 0) s->batches[r.batch]->b->remove(r.member, s->now());
+        else CLES_CUDA(cudaStreamSynchronize(r.ctx.stream));
         s->release(r);
         for (auto q = s->running.begin(); q != s->running.end(); ++q)
             if (*q == id) { s->running.erase(q); break; }

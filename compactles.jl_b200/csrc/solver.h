@@ -90,7 +90,9 @@ public:
     virtual ~BatchBase() = default;
     virtual int64_t add(const cles_solver_desc& d, const double* Q0, int layout, double tfinal, int64_t nmax,
                         double now) = 0;
-    virtual int step(double now) = 0;          // returns the members still running
+    virtual int step(double now) = 0;          // launch + collect; returns the members still running
+    virtual void launch(double now) = 0;       // (re)compose if needed and enqueue one step on the batch's stream
+    virtual int collect(double now) = 0;       // wait for it and update the members' clocks
     virtual int n_active() const = 0;
     virtual void remove(int64_t id, double now) = 0;
     virtual void status(int64_t id, cles_request_status* out) const = 0;

@@ -8,14 +8,20 @@ The stream is processed two ways on the same GPU:
   run! loop (cles_run), in arrival order; its time-to-solution follows from
   the measured service times of the sequential queue;
 * served: requests are submitted to a cles_server when their arrival time
-  comes and advanced by continuous batching (one graph launch per request
-  per tick, steps of different requests overlapping on the device).
+  comes and advanced by continuous batching.  Without --batching each
+  request has its own solver (one graph launch per request per tick, steps of
+  different requests overlapping on the device); with --batching requests of
+  one physics class share a batch (one captured step advances all of them).
 
-The arrival rate offers 1.5x the one-at-a-time capacity.  Reported: solves/s
-and p50/p99 time-to-solution of both, and whether every served result equals
-its one-at-a-time result (bitwise, FP64).
+--load sets the arrival rate as a multiple of the one-at-a-time capacity
+(1.5 by default, the latency case); --load inf submits every request at time
+zero, which measures the server's capacity.  Reported: solves/s and p50/p99
+time-to-solution of both, and whether every served result equals the same
+request run alone: bitwise against the one-at-a-time run without batching;
+with batching bitwise against the request alone in a batch of its own, and
+within 1e-10 relative L2 of the one-at-a-time (one-grid solver) run.
 
-  python compactles.jl_b200/serving.py [--requests 24] [--scale small|full]
+  python compactles.jl_b200/serving.py [--requests 24] [--scale small|full] [--load 1.5|inf] [--batching]
 """
 import argparse
 import importlib.util
@@ -88,8 +94,23 @@ def one_at_a_time(cl, reqs):
     return out, service
 
 
-def served(cl, reqs, arrivals, max_active, budget):
-    srv = cl.Server(hbm_budget=budget, max_active=max_active)
+def alone_in_batch(cl, reqs):
+    out = []
+    for name, desc, Q0, tf in reqs:
+        B = cl.Batch(desc)
+        mid = B.add(desc, Q0, tf)
+        B.run()
+        out.append(B.fetch(mid))
+        del B
+    return out
+
+
+def rel_l2(a, b):
+    return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+
+def served(cl, reqs, arrivals, max_active, budget, batching=False):
+    srv = cl.Server(hbm_budget=budget, max_active=max_active, batching=batching)
     ids = [None] * len(reqs)
     t0 = time.perf_counter()
     nxt = 0
@@ -124,6 +145,8 @@ def main(argv=None):
     p.add_argument("--seed", type=int, default=11)
     p.add_argument("--max-active", type=int, default=64)
     p.add_argument("--budget-gb", type=float, default=60.0)
+    p.add_argument("--load", default="1.5", help="offered load over the one-at-a-time capacity, or inf")
+    p.add_argument("--batching", action="store_true")
     a = p.parse_args(argv)
     cl = _package()
     reqs = make_requests(cl, a.requests, a.seed, a.scale)
@@ -132,9 +155,12 @@ def main(argv=None):
     s = cl.Solver(w[0]); s.set_state(w[1]); s.run(w[2], 5); s.run_graph(w[2], 10); del s
     base, service = one_at_a_time(cl, reqs)
     rng = np.random.default_rng(a.seed + 1)
-    lam = 1.5 * len(reqs) / sum(service)               # offered load 1.5x one-at-a-time capacity
-    arrivals = np.cumsum(rng.exponential(1.0 / lam, size=len(reqs)))
-    arrivals -= arrivals[0]
+    if a.load == "inf":
+        arrivals = np.zeros(len(reqs))
+    else:
+        lam = float(a.load) * len(reqs) / sum(service)     # offered load over one-at-a-time capacity
+        arrivals = np.cumsum(rng.exponential(1.0 / lam, size=len(reqs)))
+        arrivals -= arrivals[0]
     # one at a time on the same arrival stream
     fin, tts_base = [], []
     t = 0.0
@@ -142,18 +168,27 @@ def main(argv=None):
         t = max(t, arrivals[i]) + service[i]
         fin.append(t)
         tts_base.append(t - arrivals[i])
-    res, done = served(cl, reqs, list(arrivals), a.max_active, int(a.budget_gb * (1 << 30)))
+    res, done = served(cl, reqs, list(arrivals), a.max_active, int(a.budget_gb * (1 << 30)), a.batching)
     tts = [done[i] - arrivals[i] for i in range(len(reqs))]
-    same = all(np.array_equal(res[i], base[i]) for i in range(len(reqs)))
+    extra = {}
+    if a.batching:
+        alone = alone_in_batch(cl, reqs)
+        same = all(np.array_equal(res[i], alone[i]) for i in range(len(reqs)))
+        extra["max_rel_l2_vs_one_grid_solver"] = max(rel_l2(res[i], base[i]) for i in range(len(reqs)))
+    else:
+        same = all(np.array_equal(res[i], base[i]) for i in range(len(reqs)))
     out = {
         "workload": f"{len(reqs)} requests ({a.scale}): tubes / 2-D shock-interface / TGV boxes, Poisson seed {a.seed}",
-        "offered_load": "1.5x one-at-a-time capacity",
+        "offered_load": ("every request at time zero (capacity)" if a.load == "inf"
+                         else f"{a.load}x one-at-a-time capacity"),
+        "batching": a.batching,
         "served": {"solves_per_s": len(reqs) / max(done), "p50_s": float(np.percentile(tts, 50)),
                    "p99_s": float(np.percentile(tts, 99))},
         "one_at_a_time": {"solves_per_s": len(reqs) / fin[-1], "p50_s": float(np.percentile(tts_base, 50)),
                           "p99_s": float(np.percentile(tts_base, 99)), "service_s_total": sum(service)},
         "speedup_solves_per_s": (len(reqs) / max(done)) / (len(reqs) / fin[-1]),
         "results_equal_alone": same,
+        **extra,
     }
     print(json.dumps(out), flush=True)
     return out

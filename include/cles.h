@@ -557,6 +557,13 @@ int  cles_server_status(cles_server* s, int64_t id, cles_request_status* out);
 /* Final state of a finished request (same layout as submitted); releases it. */
 int  cles_server_fetch(cles_server* s, int64_t id, double* Q_host);
 int  cles_server_cancel(cles_server* s, int64_t id);
+/* Batching (off by default): while on, an admitted request that the batch
+ * path supports (see cles_batch_create) joins a batch of its physics class
+ * instead of getting its own solver; every tick advances each batch by one
+ * captured step, whatever its member count.  Batched results equal the same
+ * request run alone through a batch, bitwise, and the one-grid solver's to
+ * rounding (different line-solve kernels). */
+int  cles_server_set_batching(cles_server* s, int on);
 
 /* ---- batches: many solves of one physics class advanced together --------
  * No counterpart in the reference (one problem per process there).  A batch
