@@ -47,7 +47,23 @@ namespace cles {
 
 namespace {
 
-constexpr int64_t kAlignCells = 64;
+constexpr int64_t kAlignCells = 64;   // = the cell tile of the per-member constant map (cell / 64)
+
+// Segment length of a batched plan, from its own lines alone (so that a
+// member's arithmetic never depends on the other members): the longest of
+// 32, 16, 8 points whose segments give the plan at least 148 x 512 threads,
+// else 8.  Few long lines (the large x extents of the 2-D cases, 1-D tubes)
+// get many short segments, so that one grid alone still fills the GPU.
+int batch_seg_max(int n, int64_t lines) {
+    int m = 32;
+    while (m > 8) {
+        int S = 1;
+        while ((n + S - 1) / S > m) S *= 2;
+        if (lines * S >= 148 * 512) break;
+        m /= 2;
+    }
+    return m;
+}
 
 __global__ void k_fill_const(double* __restrict__ a, int64_t n, double v) {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
@@ -69,14 +85,13 @@ bool face_supported(int bc) {
 }
 
 // The fields every member of a batch must share (everything but the grid
-// extents, the domain and the boundary states), checked field by field.
+// extents, the domain, the boundary states and the species gas constants and
+// heat-capacity ratios), checked field by field.
 void check_class(const cles_solver_desc& c, const cles_solver_desc& d) {
     auto bad = [](const std::string& what) {
         throw Error(CLES_EINVAL, "batch member differs from the batch's class in " + what);
     };
     if (d.n_species != c.n_species) bad("n_species");
-    for (int k = 0; k < c.n_species; ++k)
-        if (d.R[k] != c.R[k] || d.gamma[k] != c.gamma[k]) bad("species R / gamma");
     if (d.mu0 != c.mu0 || d.Pr != c.Pr || d.Sc != c.Sc) bad("transport");
     if (d.art_enabled != c.art_enabled || d.C_mu != c.C_mu || d.C_beta != c.C_beta || d.C_kappa != c.C_kappa ||
         d.C_D != c.C_D || d.beta_sensor != c.beta_sensor)
@@ -141,6 +156,7 @@ struct Member {
     int state = CLES_REQ_QUEUED;
     int failure = CLES_FAIL_NONE;
     double clk[16] = {0};
+    double mc[24] = {0};           // R_k, cv_k, cp_k of its ideal mixture
     int64_t off = 0;               // arena offset while placed
     double admit_s = -1, done_s = -1;
 };
@@ -212,15 +228,21 @@ public:
         const int dtF = sizeof(F) == 8 ? CLES_F64 : CLES_F32;
         for (int k = 0; k < 3; ++k) {
             if (!m->active[k]) continue;
+            const int sm = batch_seg_max(m->n[k], m->cells / m->n[k]);
             m->deriv[k].reset(new CompactPlan());
-            build_compact_plan(*m->deriv[k], d.deriv, m->n, k, m->periodic[k], m->h[k], dtF, 0, 0, false, false, true);
+            build_compact_plan(*m->deriv[k], d.deriv, m->n, k, m->periodic[k], m->h[k], dtF, 0, 0, false, false, sm);
             m->filt[k].reset(new CompactPlan());
-            build_compact_plan(*m->filt[k], d.filt, m->n, k, m->periodic[k], m->h[k], dtF, 0, 0, false, false, true);
+            build_compact_plan(*m->filt[k], d.filt, m->n, k, m->periodic[k], m->h[k], dtF, 0, 0, false, false, sm);
             if (dtF != CLES_F64) {
                 m->qfilt[k].reset(new CompactPlan());
                 build_compact_plan(*m->qfilt[k], d.filt, m->n, k, m->periodic[k], m->h[k], CLES_F64, 0, 0, false,
-                                   false, true);
+                                   false, sm);
             }
+        }
+        for (int sp = 0; sp < Ns_; ++sp) {
+            m->mc[sp] = d.R[sp];
+            m->mc[8 + sp] = d.R[sp] / (d.gamma[sp] - 1);
+            m->mc[16 + sp] = m->mc[sp] + m->mc[8 + sp];
         }
         // initial state to the interior layout on the host
         m->Qhost.assign((size_t)(m->cells * ncons_), 0.0);
@@ -472,7 +494,7 @@ private:
 
     void release_derived() {
         for (DevBuf* b : {&du_, &dQ_, &prim_, &g_u_, &gty_, &scratch_, &flux_, &part_, &grids_, &tiles_, &faces_,
-                          &chunks_, &chunk_first_})
+                          &chunks_, &chunk_first_, &mc_, &tmap_})
             b->release();
         for (auto& rr : roles_)
             for (auto& r : rr) { r.plans.release(); r.blocks.release(); r.nblocks = 0; }
@@ -512,8 +534,13 @@ private:
         std::vector<BatchFace> faces;
         std::vector<BatchChunk> chunks;
         std::vector<int> first(G + 1, 0);
+        std::vector<double> mc(24 * (size_t)G);
+        std::vector<int> tmap((size_t)(ct_ / kAlignCells), 0);
         for (int g = 0; g < G; ++g) {
             const Member& m = *order_[g];
+            std::memcpy(&mc[24 * (size_t)g], m.mc, sizeof(m.mc));
+            const int64_t t1 = (g + 1 < G ? order_[g + 1]->off : ct_) / kAlignCells;
+            for (int64_t t = m.off / kAlignCells; t < t1; ++t) tmap[(size_t)t] = g;
             BatchGrid& B = grids[g];
             std::memset(&B, 0, sizeof(B));
             for (int k = 0; k < 3; ++k) {
@@ -546,7 +573,7 @@ private:
                         f.st.iso = std::isnan(Tw) ? 0 : 1;
                         f.st.Twall = Tw;
                         f.st.ew_times_T = 1;
-                        for (int sp = 0; sp < Ns_; ++sp) f.st.ew[sp] = pc_.cvk[sp];
+                        for (int sp = 0; sp < Ns_; ++sp) f.st.ew[sp] = m.mc[8 + sp];
                     }
                     faces.push_back(f);
                 }
@@ -560,6 +587,8 @@ private:
         upload(faces_, ctx_, faces, st_);
         upload(chunks_, ctx_, chunks, st_);
         upload(chunk_first_, ctx_, first, st_);
+        upload(mc_, ctx_, mc, st_);
+        upload(tmap_, ctx_, tmap, st_);
         part_.release();
         part_.alloc(ctx_, sizeof(double) * 2 * std::max<size_t>(chunks.size(), 1));
         ntiles_ = (int)tiles.size();
@@ -581,6 +610,7 @@ private:
         std::vector<int2> blocks;
         const int dtype = role == R_QFILT ? CLES_F64 : (sizeof(F) == 8 ? CLES_F64 : CLES_F32);
         size_t smem = 0;
+        int ms = 8;
         for (int g = 0; g < G; ++g) {
             const Member& m = *order_[g];
             const CompactPlan* p = plan_of(m, role, k);
@@ -596,6 +626,8 @@ private:
             bp.sz = (int64_t)m.n[0] * m.n[1];
             bp.clk = clk_.as<double>() + 16 * (size_t)g;
             smem = std::max(smem, batch_plan_smem(p->P, LB, dtype));
+            const int mlen = p->P.seg_base + (p->P.seg_rem ? 1 : 0);
+            ms = std::max(ms, mlen <= 8 ? 8 : (mlen <= 16 ? 16 : 32));
             for (int64_t l = 0; l < p->P.lines; l += LB) blocks.push_back(make_int2(g, (int)l));
         }
         if (smem > 200 * 1024) return false;
@@ -606,6 +638,7 @@ private:
         R.kind.xmode = k == 0 ? 1 : 0;
         R.kind.threads = threads;
         R.kind.smem = smem;
+        R.kind.ms = ms;
         upload(R.plans, ctx_, plans, st_);
         upload(R.blocks, ctx_, blocks, st_);
         R.nblocks = (int)blocks.size();
@@ -683,6 +716,10 @@ private:
         for (int k = 0; k < 3; ++k)
             if (act_[k]) along(R_FILT, k, f, f, count, OUT_STORE);
     }
+    void primitives() {
+        BatchOps<F>::primitives(Q_.as<double>(), prim_.as<F>(), ct_, Ns_, pc_, cls_.art_enabled, mc_.as<double>(),
+                                tmap_.as<int>(), st_);
+    }
     void bcs() {
         batch_bc(Q_.as<double>(), grids_.as<BatchGrid>(), faces_.as<BatchFace>(), nfaces_, ct_, Ns_, st_);
     }
@@ -722,15 +759,15 @@ private:
 
     void rhs_and_update(bool primitives_current, int stage) {
         using PW = Pointwise<F>;
-        if (!primitives_current) PW::primitives(Q_.as<double>(), prim_.as<F>(), ct_, Ns_, pc_, st_, cls_.art_enabled);
+        if (!primitives_current) primitives();
         for (int k = 0; k < 3; ++k)
             if (act_[k]) along(R_DERIV, k, field(prim_, P_U), g_u_.as<F>() + (size_t)ct_ * 3 * k, 3, OUT_STORE);
         artificial();
         const int ngty = Ns_ == 1 ? 1 : 1 + Ns_;
         for (int k = 0; k < 3; ++k)
             if (act_[k]) along(R_DERIV, k, field(prim_, P_T), gty_.as<F>() + (size_t)ct_ * ngty * k, ngty, OUT_STORE);
-        PW::fluxes(Q_.as<double>(), prim_.as<F>(), g_u_.as<F>(), gty_.as<F>(), art_.as<F>(), flux_.as<F>(), ct_, Ns_,
-                   pc_, cls_.mu0, cls_.Pr, cls_.Sc, st_);
+        BatchOps<F>::fluxes(Q_.as<double>(), prim_.as<F>(), g_u_.as<F>(), gty_.as<F>(), art_.as<F>(), flux_.as<F>(),
+                            ct_, Ns_, pc_, cls_.mu0, cls_.Pr, cls_.Sc, mc_.as<double>(), tmap_.as<int>(), st_);
         // dQ = -sum_d D_d(F_d) with the RK update in the last direction's store
         // (y, x, z on 3-D grids, as the solver orders them)
         int order[3] = {0, 1, 2};
@@ -757,7 +794,7 @@ private:
         try {
             using PW = Pointwise<F>;
             bcs();
-            PW::primitives(Q_.as<double>(), prim_.as<F>(), ct_, Ns_, pc_, st_, cls_.art_enabled);
+            primitives();
             BatchOps<F>::rate_clock(Q_.as<double>(), prim_.as<F>(), art_.as<F>(), grids_.as<BatchGrid>(),
                                     (int)order_.size(), chunks_.as<BatchChunk>(), nchunks_, chunk_first_.as<int>(),
                                     part_.as<double>(), ct_, Ns_, cls_.mu0, cls_.Pr, cls_.Sc, st_);
@@ -806,7 +843,7 @@ private:
     int64_t ct_ = 0;
     DevBuf Q_, art_, clk_;
     DevBuf du_, dQ_, prim_, g_u_, gty_, scratch_, flux_, part_;
-    DevBuf grids_, tiles_, faces_, chunks_, chunk_first_;
+    DevBuf grids_, tiles_, faces_, chunks_, chunk_first_, mc_, tmap_;
     int ntiles_ = 0, nfaces_ = 0, nchunks_ = 0;
     Role roles_[3][3];
     double tuned_ms_[3][3] = {};

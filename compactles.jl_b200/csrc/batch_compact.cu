@@ -20,7 +20,7 @@ namespace cles {
 
 namespace {
 
-template <typename T, int Q, int M, bool XMODE>
+template <typename T, int Q, int M, bool XMODE, int MS>
 __global__ void __launch_bounds__(512) k_compact_batch(const BatchLinePlan* __restrict__ plans,
                                                         const int2* __restrict__ blocks, const T* in_base,
                                                         T* out_base, const int64_t ct, const int mode,
@@ -44,15 +44,15 @@ __global__ void __launch_bounds__(512) k_compact_batch(const BatchLinePlan* __re
     const FieldView out{out_base + off, ct, bp->sy, bp->sz};
     const int comp = blockIdx.y;
     const RkStore rk{Qs, dus, A, B, dt, (int64_t)comp * ct + off};
-    compact_lines<T, Q, M, XMODE, kMaxSeg, true>(Ps, static_cast<const T*>(bp->tab), in, out, mode, nullptr, bk.y,
+    compact_lines<T, Q, M, XMODE, MS, true>(Ps, static_cast<const T*>(bp->tab), in, out, mode, nullptr, bk.y,
                                                  comp, &rk, smem_raw);
 }
 
-template <typename T, int Q, int M, bool X>
+template <typename T, int Q, int M, bool X, int MS>
 void launch_k(const BatchLaunchKind& k, const BatchLinePlan* plans, const int2* blocks, int nblocks, const void* in,
               void* out, int64_t ct, int count, int mode, double* Q_, double* du, double A, double B, int skip,
               cudaStream_t st) {
-    auto kern = k_compact_batch<T, Q, M, X>;
+    auto kern = k_compact_batch<T, Q, M, X, MS>;
     static thread_local size_t configured = 0;
     if (k.smem > 48 * 1024 && configured < k.smem) {
         CLES_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)k.smem));
@@ -65,30 +65,36 @@ void launch_k(const BatchLaunchKind& k, const BatchLinePlan* plans, const int2* 
     check_launch("k_compact_batch");
 }
 
-template <typename T, int Q, bool X>
-void launch_m(const BatchLaunchKind& k, const BatchLinePlan* plans, const int2* blocks, int nb, const void* in,
+template <typename T, int Q, int M, bool X>
+void launch_ms(const BatchLaunchKind& k, const BatchLinePlan* plans, const int2* blocks, int nb, const void* in,
+               void* out, int64_t ct, int count, int mode, double* Q_, double* du, double A, double B, int skip,
+               cudaStream_t st) {
+    switch (k.ms) {
+        case 8: launch_k<T, Q, M, X, 8>(k, plans, blocks, nb, in, out, ct, count, mode, Q_, du, A, B, skip, st); break;
+        case 16: launch_k<T, Q, M, X, 16>(k, plans, blocks, nb, in, out, ct, count, mode, Q_, du, A, B, skip, st); break;
+        case 32: launch_k<T, Q, M, X, 32>(k, plans, blocks, nb, in, out, ct, count, mode, Q_, du, A, B, skip, st); break;
+        default: throw Error(CLES_EINVAL, "batched register tile must be 8, 16 or 32 points");
+    }
+}
+
+// The schemes of the library: C4 (q 1, M 1), C6 (1, 2), the C8 filter (1, 4), C10 (2, 3).
+template <typename T, bool X>
+void launch_x(const BatchLaunchKind& k, const BatchLinePlan* plans, const int2* blocks, int nb, const void* in,
               void* out, int64_t ct, int count, int mode, double* Q_, double* du, double A, double B, int skip,
               cudaStream_t st) {
-    switch (k.M) {
-        case 1: launch_k<T, Q, 1, X>(k, plans, blocks, nb, in, out, ct, count, mode, Q_, du, A, B, skip, st); break;
-        case 2: launch_k<T, Q, 2, X>(k, plans, blocks, nb, in, out, ct, count, mode, Q_, du, A, B, skip, st); break;
-        case 3: launch_k<T, Q, 3, X>(k, plans, blocks, nb, in, out, ct, count, mode, Q_, du, A, B, skip, st); break;
-        case 4: launch_k<T, Q, 4, X>(k, plans, blocks, nb, in, out, ct, count, mode, Q_, du, A, B, skip, st); break;
-        default: throw Error(CLES_EINVAL, "unsupported stencil half-width");
-    }
+    if (k.q == 1 && k.M == 1) launch_ms<T, 1, 1, X>(k, plans, blocks, nb, in, out, ct, count, mode, Q_, du, A, B, skip, st);
+    else if (k.q == 1 && k.M == 2) launch_ms<T, 1, 2, X>(k, plans, blocks, nb, in, out, ct, count, mode, Q_, du, A, B, skip, st);
+    else if (k.q == 1 && k.M == 4) launch_ms<T, 1, 4, X>(k, plans, blocks, nb, in, out, ct, count, mode, Q_, du, A, B, skip, st);
+    else if (k.q == 2 && k.M == 3) launch_ms<T, 2, 3, X>(k, plans, blocks, nb, in, out, ct, count, mode, Q_, du, A, B, skip, st);
+    else throw Error(CLES_EINVAL, "batched solves support the C4, C6, C10 and C8-filter stencil shapes only");
 }
 
 template <typename T>
 void launch_t(const BatchLaunchKind& k, const BatchLinePlan* plans, const int2* blocks, int nb, const void* in,
               void* out, int64_t ct, int count, int mode, double* Q_, double* du, double A, double B, int skip,
               cudaStream_t st) {
-    if (k.q == 1) {
-        if (k.xmode) launch_m<T, 1, true>(k, plans, blocks, nb, in, out, ct, count, mode, Q_, du, A, B, skip, st);
-        else launch_m<T, 1, false>(k, plans, blocks, nb, in, out, ct, count, mode, Q_, du, A, B, skip, st);
-    } else {
-        if (k.xmode) launch_m<T, 2, true>(k, plans, blocks, nb, in, out, ct, count, mode, Q_, du, A, B, skip, st);
-        else launch_m<T, 2, false>(k, plans, blocks, nb, in, out, ct, count, mode, Q_, du, A, B, skip, st);
-    }
+    if (k.xmode) launch_x<T, true>(k, plans, blocks, nb, in, out, ct, count, mode, Q_, du, A, B, skip, st);
+    else launch_x<T, false>(k, plans, blocks, nb, in, out, ct, count, mode, Q_, du, A, B, skip, st);
 }
 
 }  // namespace

@@ -142,11 +142,11 @@ struct CompactPlan {
 // a coordinate-singularity fold at that end of a closed line: the antipodal
 // parity (+1 / -1) of the field the plan is applied to, 0 for a closure.
 // lo_open / hi_open make that end of a non-periodic line a rank interface.
-// pow2_segments (batched plans): S is the fewest power-of-two segments of at
-// most kMaxSeg points.
+// pow2_seg_max > 0 (batched plans): S is the fewest power-of-two segments of
+// at most pow2_seg_max (8, 16 or 32) points.
 void build_compact_plan(CompactPlan& plan, const cles_scheme& scheme, const int n3[3], int dim,
                         bool periodic, double h, int dtype, int lo_fold = 0, int hi_fold = 0,
-                        bool lo_open = false, bool hi_open = false, bool pow2_segments = false);
+                        bool lo_open = false, bool hi_open = false, int pow2_seg_max = 0);
 
 // The LHS band of one line (or one rank's piece of a split line), row-major
 // n x (2q+1): interior band, closure rows at closed ends, parity folds, and
@@ -232,6 +232,7 @@ struct BatchLinePlan {
 struct BatchLaunchKind {
     int dtype;            // CLES_F64 / CLES_F32
     int q, M, xmode;
+    int ms;               // register tile: 8, 16 or 32 points (>= every plan's longest segment)
     int threads;          // LB x S of every plan
     size_t smem;          // dynamic shared memory (max over the plans)
 };

@@ -289,7 +289,7 @@ void LineBand::solve(double* x) const {
 }
 
 void build_compact_plan(CompactPlan& plan, const cles_scheme& s, const int n3[3], int dim, bool periodic,
-                        double h, int dtype, int lo_fold, int hi_fold, bool lo_open, bool hi_open, bool pow2_segments) {
+                        double h, int dtype, int lo_fold, int hi_fold, bool lo_open, bool hi_open, int pow2_seg_max) {
     const int n = n3[dim];
     const int q = s.q, M = s.M, nc = s.nc;
     if (q < 1 || q > CLES_MAX_Q) throw Error(CLES_EINVAL, "scheme LHS half-bandwidth q must be 1 or 2");
@@ -412,12 +412,13 @@ void build_compact_plan(CompactPlan& plan, const cles_scheme& s, const int n3[3]
     if (S < 1) S = 1;
     const int base = n / S;
     if (base < std::max(2 * q + 1, q + 1)) S = 1;  // tiny lines: one segment
-    if (pow2_segments) {
-        // batched plans: the fewest power-of-two segments of at most kMaxSeg
-        // points, so that every plan's lines-per-CTA times segments equals the
-        // batched launch's thread count (segments then hold > kMaxSeg / 2 points)
+    if (pow2_seg_max > 0) {
+        // batched plans: the fewest power-of-two segments of at most
+        // pow2_seg_max points, so that every plan's lines-per-CTA times
+        // segments equals the batched launch's thread count
         S = 1;
-        while ((n + S - 1) / S > kMaxSeg) S *= 2;
+        while ((n + S - 1) / S > std::min(pow2_seg_max, kMaxSeg)) S *= 2;
+        if (n / S < std::max(2 * q + 1, q + 1)) throw Error(CLES_EINVAL, "batched segments too short for the scheme");
     }
     P.S = S;
     P.seg_base = n / S;

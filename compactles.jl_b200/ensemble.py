@@ -71,11 +71,17 @@ def serve(cl, reqs, max_active, budget):
     return wall, steps, states
 
 
-def run_batch(cl, reqs):
+def run_batch(cl, reqs, trace=None):
     B = cl.Batch(reqs[0][0])
     t0 = time.perf_counter()
     ids = [B.add(desc, Q0, tf) for desc, Q0, tf in reqs]
-    B.run()
+    n = len(reqs)
+    while n > 0:
+        ts = time.perf_counter()
+        n = B.step()
+        if trace is not None:
+            trace.append((n, time.perf_counter() - ts))
+    B.step()
     wall = time.perf_counter() - t0
     states, steps = [], []
     for mid in ids:
@@ -122,9 +128,16 @@ def main(argv=None):
             reqs = [cl.scenarios.shock_interface_2d(sch, nx, ny, M, sd, precision=prec) for nx, ny, M, sd in cases]
             extra = {}
             if mode == "batch":
-                wall, steps, st, bstats = run_batch(cl, reqs)
+                trace = []
+                wall, steps, st, bstats = run_batch(cl, reqs, trace)
+                # where the time goes: batch steps by the number of members still running
+                bands = {}
+                for lo, hi in ((33, 10 ** 9), (9, 32), (2, 8), (0, 1)):
+                    sel = [dt for n, dt in trace if lo <= n <= hi]
+                    bands[f"{lo}-{hi if hi < 10 ** 9 else 'all'} running"] = {
+                        "steps": len(sel), "s": sum(sel), "ms_per_step": 1e3 * sum(sel) / max(len(sel), 1)}
                 extra = {"compositions": bstats["compositions"], "launches_per_step": bstats["launches_per_step"],
-                         "batch_steps": bstats["steps"], "tuning_last": bstats["tuning"]}
+                         "batch_steps": bstats["steps"], "time_by_members_running": bands}
             else:
                 wall, steps, st = serve(cl, reqs, a.max_active, int(a.budget_gb * (1 << 30)))
             cs = sum(nx * ny * k for (nx, ny, _, _), k in zip(cases, steps))
