@@ -49,21 +49,11 @@ namespace {
 
 constexpr int64_t kAlignCells = 64;   // = the cell tile of the per-member constant map (cell / 64)
 
-// Segment length of a batched plan, from its own lines alone (so that a
-// member's arithmetic never depends on the other members): the longest of
-// 32, 16, 8 points whose segments give the plan at least 148 x 512 threads,
-// else 8.  Few long lines (the large x extents of the 2-D cases, 1-D tubes)
-// get many short segments, so that one grid alone still fills the GPU.
-int batch_seg_max(int n, int64_t lines) {
-    int m = 32;
-    while (m > 8) {
-        int S = 1;
-        while ((n + S - 1) / S > m) S *= 2;
-        if (lines * S >= 148 * 512) break;
-        m /= 2;
-    }
-    return m;
-}
+// Segment length of a batched plan: the fewest power-of-two segments of at
+// most 32 points.  Fixed by the line length alone, so a member's arithmetic
+// never depends on the other members; long segments keep the interface
+// system (whose cost per point grows as n / m^2) small.
+int batch_seg_max(int, int64_t) { return 32; }
 
 __global__ void k_fill_const(double* __restrict__ a, int64_t n, double v) {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)

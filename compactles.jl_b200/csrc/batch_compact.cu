@@ -105,7 +105,7 @@ size_t batch_plan_smem(const CompactParams& P, int LB, int dtype) {
     size_t smem = 0;
     if (P.dim == 0) smem += el * (size_t)P.n * (LB + 1);
     if (P.pcr) smem += el * (size_t)LB * 4 * P.S;
-    else if (P.hasred) smem += el * (size_t)LB * (N + 1);
+    else if (P.hasred) smem += el * ((size_t)LB * (N + 1) + (size_t)N * (N + 1));   // + the staged inverse
     return smem;
 }
 

@@ -106,7 +106,7 @@ __device__ __forceinline__ void tile_rows(const CompactParams& P, const FieldVie
 
 // The line solve of one CTA: lines [line0, line0 + LB) of component `comp`.
 // RK (batched solves): mode OUT_RK applies the RK update of the state in rk
-// instead of a store.
+// instead of a store, and the interface inverse is staged in shared memory.
 template <typename T, int Q, int M, bool XMODE, int MS, bool RK = false>
 __device__ __forceinline__ void compact_lines(const CompactParams& P, const T* __restrict__ tab, const FieldView& in,
                                               const FieldView& out, const int mode, T* __restrict__ iface,
@@ -126,6 +126,18 @@ __device__ __forceinline__ void compact_lines(const CompactParams& P, const T* _
     const int TP = LB + 1;  // tile pitch (x lines)
     T* tile = smem;
     T* red = XMODE ? smem + (size_t)n * TP : smem;
+    // batched launches stage the dense inverse of the interface system in
+    // shared memory (row pitch N + 1, so segments of one warp hit different
+    // banks) instead of reading it from global memory per thread
+    T* Gsm = nullptr;
+    if constexpr (RK) {
+        if (P.hasred && !(Q == 1 && P.pcr)) {
+            const int Nq = 2 * Q * S;
+            Gsm = red + (size_t)LB * (Nq + 1);
+            for (int i = threadIdx.x; i < Nq * Nq; i += blockDim.x)
+                Gsm[(i / Nq) * (Nq + 1) + i % Nq] = tab[P.off_G + i];
+        }
+    }
     const int N = 2 * Q * S;
 
     LineMap Lin = line_map(P, in, valid ? line : line0);
@@ -302,18 +314,28 @@ __device__ __forceinline__ void compact_lines(const CompactParams& P, const T* _
         if (has_prev) {
 #pragma unroll
             for (int t = 0; t < Q; ++t) {
-                const T* g = G + (int64_t)(2 * Q * prev + Q + t) * N;
                 T acc = T(0);
-                for (int j = 0; j < N; ++j) acc += ldg(g + j) * rl[j];
+                if (RK && Gsm) {
+                    const T* g = Gsm + (int64_t)(2 * Q * prev + Q + t) * (N + 1);
+                    for (int j = 0; j < N; ++j) acc += g[j] * rl[j];
+                } else {
+                    const T* g = G + (int64_t)(2 * Q * prev + Q + t) * N;
+                    for (int j = 0; j < N; ++j) acc += ldg(g + j) * rl[j];
+                }
                 zp[t] = acc;
             }
         }
         if (has_next) {
 #pragma unroll
             for (int t = 0; t < Q; ++t) {
-                const T* g = G + (int64_t)(2 * Q * next + t) * N;
                 T acc = T(0);
-                for (int j = 0; j < N; ++j) acc += ldg(g + j) * rl[j];
+                if (RK && Gsm) {
+                    const T* g = Gsm + (int64_t)(2 * Q * next + t) * (N + 1);
+                    for (int j = 0; j < N; ++j) acc += g[j] * rl[j];
+                } else {
+                    const T* g = G + (int64_t)(2 * Q * next + t) * N;
+                    for (int j = 0; j < N; ++j) acc += ldg(g + j) * rl[j];
+                }
                 zn[t] = acc;
             }
         }

@@ -98,8 +98,14 @@ __device__ __forceinline__ T tl(const double* d, const float* f, int i) {
     return T(f[i]);
 }
 
+// FP32 lines of 32-point segments run two persistent CTAs per SM (3 tiles in
+// flight each, at most 128 registers a thread): one CTA of 8 warps cannot
+// keep an SM's issue slots busy on the shorter FP32 tiles.
+template <typename T>
+constexpr int tma_ctas_per_sm(int ms) { return sizeof(T) == 4 && ms == 32 ? 2 : 1; }
+
 template <typename T, int M, int MS>
-__global__ void __launch_bounds__(MS == 16 ? 512 : 256, 1)
+__global__ void __launch_bounds__(MS == 16 ? 512 : 256, tma_ctas_per_sm<T>(MS))
     k_compact_tma(const __grid_constant__ CUtensorMap map, const __grid_constant__ CompactParams P,
                   const __grid_constant__ TileLineParams TL,
                   const T* __restrict__ Gg, const FieldView out, const int mode, const int count, const int NS,
@@ -818,7 +824,8 @@ template <typename T, int M, int MS>
 void launch_tma_ms(const CompactPlan& plan, const CUtensorMap& map, const FieldView& out, int count, int mode,
                   cudaStream_t st, const T* G, const RkEpilogue& rk) {
     const CompactParams& P = plan.P;
-    const int NS = sizeof(T) == 8 ? 3 : 4;
+    constexpr int per_sm = tma_ctas_per_sm<T>(MS);
+    const int NS = sizeof(T) == 8 || per_sm == 2 ? 3 : 4;
     const int N = 2 * P.S;
     const size_t smem = sizeof(T) * (size_t)P.n * kLanes * NS + 8 * sizeof(uint64_t) +
                         sizeof(T) * ((size_t)kLanes * (N + 1) + (size_t)N * N);
@@ -835,7 +842,8 @@ void launch_tma_ms(const CompactPlan& plan, const CUtensorMap& map, const FieldV
     }
     const int gx = (P.nx + kLanes - 1) / kLanes;
     const int work = gx * (P.dim == 1 ? P.nz : P.ny) * count;
-    const int grid = work < g_num_sms ? work : g_num_sms;
+    const int slots = g_num_sms * (2 * (smem + 1024) <= 227 * 1024 ? per_sm : 1);
+    const int grid = work < slots ? work : slots;
     kern<<<grid, kLanes * P.S, smem, st>>>(map, P, plan.TL, G, out, mode, count, NS, rk);
     count_launch();
     check_launch("k_compact_tma");
