@@ -4,8 +4,8 @@
 // A launch carries a table of per-grid plans (BatchLinePlan: the plan's
 // parameters, its coefficient table and where the grid's fields sit in the
 // batch arena) and a table of CTAs, each naming one plan and its first line.
-// Every CTA copies its plan's parameters into shared memory and runs the
-// generic segmented spike solve of compact_body.cuh on LB lines of that grid.
+// Every CTA reads its plan's parameters in place and runs the generic
+// segmented spike solve of compact_body.cuh on LB lines of that grid.
 // All plans of a launch share the kernel template (element type, q, M, x or
 // y/z staging) and the thread count LB x S; S is a power of two per grid, so
 // short lines get many lines per CTA and long lines few.  The RK update of
@@ -20,25 +20,23 @@ namespace cles {
 
 namespace {
 
+// At most 256 threads a CTA, so that a thread may hold the 32-point register
+// tiles of FP64 lines without spilling.
 template <typename T, int Q, int M, bool XMODE, int MS>
-__global__ void __launch_bounds__(512) k_compact_batch(const BatchLinePlan* __restrict__ plans,
+__global__ void __launch_bounds__(kBatchMaxThreads, 1) k_compact_batch(const BatchLinePlan* __restrict__ plans,
                                                         const int2* __restrict__ blocks, const T* in_base,
                                                         T* out_base, const int64_t ct, const int mode,
                                                         double* Qs, double* dus, const double A, const double B,
                                                         const int skip_idle) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    __shared__ __align__(16) CompactParams Ps;
     const int2 bk = blocks[blockIdx.x];
-    const BatchLinePlan* bp = plans + bk.x;
-    {
-        const int* src = reinterpret_cast<const int*>(&bp->P);
-        int* dst = reinterpret_cast<int*>(&Ps);
-        for (int i = threadIdx.x; i < (int)(sizeof(CompactParams) / sizeof(int)); i += blockDim.x) dst[i] = src[i];
-    }
+    // the plan is read in place through a restrict-qualified const pointer:
+    // nothing the kernel stores can alias it, so its fields load once
+    const BatchLinePlan* __restrict__ bp = plans + bk.x;
+    const CompactParams& Ps = bp->P;
     double dt = 0.0;
     if (bp->clk) dt = bp->clk[DC_DT];
     if (skip_idle && dt == 0.0) return;   // the same for every thread of the CTA
-    __syncthreads();
     const int64_t off = bp->off;
     const FieldView in{const_cast<T*>(in_base) + off, ct, bp->sy, bp->sz};
     const FieldView out{out_base + off, ct, bp->sy, bp->sz};

@@ -201,15 +201,20 @@ __device__ __forceinline__ void compact_lines(const CompactParams& P, const T* _
         }
     }
     if (P.hi_closed && seg == S - 1) {
+        // closure row jr sits at i = m - 1 - jr; written as selects over every
+        // element (static indices keep y in registers)
+        T hv[kMaxClo];
 #pragma unroll
-        for (int i = 0; i < MS; ++i) {
-            if (i < m && i >= m - P.nc) {
-                const int jr = m - 1 - i;
-                T acc = T(0);
+        for (int jr = 0; jr < kMaxClo; ++jr) {
+            T acc = T(0);
+            if (jr < P.nc)
                 for (int k = 0; k < P.clo_len[jr]; ++k) acc += T(P.chi[jr][k]) * ld(n - 1 - k);
-                y[i] = acc;
-            }
+            hv[jr] = acc;
         }
+#pragma unroll
+        for (int i = 0; i < MS; ++i)
+#pragma unroll
+            for (int jr = 0; jr < kMaxClo; ++jr) y[i] = (jr < P.nc && i == m - 1 - jr) ? hv[jr] : y[i];
     }
 
     // ---- 3. local solve -----------------------------------------------------
@@ -220,9 +225,14 @@ __device__ __forceinline__ void compact_lines(const CompactParams& P, const T* _
 #pragma unroll
         for (int i = 1; i < MS; ++i)
             if (i < m) y[i] -= ldg(f0 + i) * y[i - 1];
+        {
+            // the last row's pivot, as a select over every element: a branch
+            // taken for one i would be folded into a dynamic index of y and
+            // move y to local memory
+            const T dl = ldg(f1 + (m - 1));
 #pragma unroll
-        for (int i = 0; i < MS; ++i)
-            if (i == m - 1) y[i] *= ldg(f1 + i);
+            for (int i = 0; i < MS; ++i) y[i] = (i == m - 1) ? y[i] * dl : y[i];
+        }
 #pragma unroll
         for (int i = MS - 2; i >= 0; --i)
             if (i < m - 1) y[i] = (y[i] - ldg(f2 + i) * y[i + 1]) * ldg(f1 + i);
@@ -252,8 +262,7 @@ __device__ __forceinline__ void compact_lines(const CompactParams& P, const T* _
         // double-buffered in shared memory (4 S values per line)
         T tail = T(0);
 #pragma unroll
-        for (int i = 0; i < MS; ++i)
-            if (i == m - 1) tail = y[i];
+        for (int i = 0; i < MS; ++i) tail = (i == m - 1) ? y[i] : tail;
         T* cur = red + (size_t)lane * 4 * S;
         T* nxt = cur + 2 * S;
         cur[2 * seg] = y[0];
@@ -298,9 +307,12 @@ __device__ __forceinline__ void compact_lines(const CompactParams& P, const T* _
         const int RP = N + 1;  // pitch of the per-line interface vector
         T* rl = red + (size_t)lane * RP;
 #pragma unroll
-        for (int i = 0; i < MS; ++i) {
-            if (i < Q) rl[2 * Q * seg + i] = y[i];
-            if (i < m && i >= m - Q) rl[2 * Q * seg + Q + (i - (m - Q))] = y[i];
+        for (int t = 0; t < Q; ++t) {
+            rl[2 * Q * seg + t] = y[t];
+            T tv = T(0);
+#pragma unroll
+            for (int i = 0; i < MS; ++i) tv = (i == m - Q + t) ? y[i] : tv;
+            rl[2 * Q * seg + Q + t] = tv;
         }
         __syncthreads();
         T zp[Q], zn[Q];
@@ -362,8 +374,12 @@ __device__ __forceinline__ void compact_lines(const CompactParams& P, const T* _
         }
         if (seg == S - 1) {
 #pragma unroll
-            for (int i = 0; i < MS; ++i)
-                if (i < m && i >= m - Q) ifc[(int64_t)(Q + i - (m - Q)) * P.lines] = y[i];
+            for (int t = 0; t < Q; ++t) {
+                T tv = T(0);
+#pragma unroll
+                for (int i = 0; i < MS; ++i) tv = (i == m - Q + t) ? y[i] : tv;
+                ifc[(int64_t)(Q + t) * P.lines] = tv;
+            }
         }
     }
     if (XMODE) {
