@@ -26,7 +26,7 @@
 // the depth of the transposed shared-memory tile for x lines.  The first time
 // a launch of a given shape is built (operator, direction, element type, the
 // largest segment count and the total line count to within a factor of two),
-// every candidate (64, 128, 256 threads that fit the segments and shared
+// every candidate (128, 256, 512 threads that fit the segments and shared
 // memory) is timed with CUDA events on the batch's own fields and the fastest
 // is kept for that shape.
 //
@@ -669,7 +669,7 @@ private:
                 if (it != cache.end() && role_tables(r, k, it->second, roles_[r][k])) continue;
                 int best = -1;
                 float best_ms = 1e30f;
-                for (int th : {64, 128, 256}) {
+                for (int th : {128, 256, 512}) {
                     Role R;
                     if (!role_tables(r, k, th, R)) continue;
                     const bool f64 = R.kind.dtype == CLES_F64;

@@ -20,10 +20,8 @@ namespace cles {
 
 namespace {
 
-// At most 256 threads a CTA, so that a thread may hold the 32-point register
-// tiles of FP64 lines without spilling.
 template <typename T, int Q, int M, bool XMODE, int MS>
-__global__ void __launch_bounds__(kBatchMaxThreads, 1) k_compact_batch(const BatchLinePlan* __restrict__ plans,
+__global__ void __launch_bounds__(kBatchMaxThreads) k_compact_batch(const BatchLinePlan* __restrict__ plans,
                                                         const int2* __restrict__ blocks, const T* in_base,
                                                         T* out_base, const int64_t ct, const int mode,
                                                         double* Qs, double* dus, const double A, const double B,

@@ -228,7 +228,7 @@ struct BatchLinePlan {
     int64_t sy, sz;       // strides of the grid's fields
     const double* clk;    // graph-mode clock of the grid (dt in slot 1)
 };
-constexpr int kBatchMaxThreads = 256;   // threads per CTA of a batched line-solve launch (at most)
+constexpr int kBatchMaxThreads = 512;   // threads per CTA of a batched line-solve launch (at most)
 // Kernel template of a batched launch (shared by all its plans).
 struct BatchLaunchKind {
     int dtype;            // CLES_F64 / CLES_F32
