@@ -116,7 +116,7 @@ def lib():
         L.cles_server_status.argtypes = [vp, C.c_int64, C.POINTER(abi.cles_request_status)]
         L.cles_server_fetch.argtypes = [vp, C.c_int64, vp]
         L.cles_server_cancel.argtypes = [vp, C.c_int64]
-        L.cles_server_set_batching.argtypes = [vp, C.c_int]
+        L.cles_server_set_batching.argtypes = [vp, C.c_int, C.c_int]
         L.cles_batch_create.argtypes = [vp, C.POINTER(abi.cles_solver_desc), C.POINTER(vp)]
         L.cles_batch_destroy.argtypes = [vp]
         L.cles_batch_destroy.restype = None
@@ -452,12 +452,12 @@ def setup(prob, num, ctx=None):
 class Server:
     """Continuous-batching server of independent solves on one device (cles_server_*)."""
 
-    def __init__(self, device=0, hbm_budget=0, max_active=64, batching=False):
+    def __init__(self, device=0, hbm_budget=0, max_active=64, batching=False, batch_members=0):
         self.ptr = C.c_void_p()
         _check(lib().cles_server_create(int(device), int(hbm_budget), int(max_active), C.byref(self.ptr)))
         self._layout = {}
         if batching:
-            _check(lib().cles_server_set_batching(self.ptr, 1))
+            _check(lib().cles_server_set_batching(self.ptr, 1, int(batch_members)))
 
     def __del__(self):
         try:

@@ -306,13 +306,21 @@ __device__ __forceinline__ void compact_lines(const CompactParams& P, const T* _
     } else if (P.hasred) {
         const int RP = N + 1;  // pitch of the per-line interface vector
         T* rl = red + (size_t)lane * RP;
+        {
+            // heads y[0..Q), tails y[m-Q..m) by a window sliding over y while
+            // i < m (static indices, so y stays in registers)
+            T tl[Q];
 #pragma unroll
-        for (int t = 0; t < Q; ++t) {
-            rl[2 * Q * seg + t] = y[t];
-            T tv = T(0);
+            for (int t = 0; t < Q; ++t) { rl[2 * Q * seg + t] = y[t]; tl[t] = T(0); }
 #pragma unroll
-            for (int i = 0; i < MS; ++i) tv = (i == m - Q + t) ? y[i] : tv;
-            rl[2 * Q * seg + Q + t] = tv;
+            for (int i = 0; i < MS; ++i) {
+                const bool in = i < m;
+#pragma unroll
+                for (int t = 0; t < Q - 1; ++t) tl[t] = in ? tl[t + 1] : tl[t];
+                tl[Q - 1] = in ? y[i] : tl[Q - 1];
+            }
+#pragma unroll
+            for (int t = 0; t < Q; ++t) rl[2 * Q * seg + Q + t] = tl[t];
         }
         __syncthreads();
         T zp[Q], zn[Q];
@@ -373,13 +381,18 @@ __device__ __forceinline__ void compact_lines(const CompactParams& P, const T* _
             for (int t = 0; t < Q; ++t) ifc[(int64_t)t * P.lines] = y[t];
         }
         if (seg == S - 1) {
+            T tl[Q];
 #pragma unroll
-            for (int t = 0; t < Q; ++t) {
-                T tv = T(0);
+            for (int t = 0; t < Q; ++t) tl[t] = T(0);
 #pragma unroll
-                for (int i = 0; i < MS; ++i) tv = (i == m - Q + t) ? y[i] : tv;
-                ifc[(int64_t)(Q + t) * P.lines] = tv;
+            for (int i = 0; i < MS; ++i) {
+                const bool in = i < m;
+#pragma unroll
+                for (int t = 0; t < Q - 1; ++t) tl[t] = in ? tl[t + 1] : tl[t];
+                tl[Q - 1] = in ? y[i] : tl[Q - 1];
             }
+#pragma unroll
+            for (int t = 0; t < Q; ++t) ifc[(int64_t)(Q + t) * P.lines] = tl[t];
         }
     }
     if (XMODE) {

@@ -10,7 +10,9 @@
 //     supports joins a batch of its physics class (batch.cpp): the members'
 //     fields share one arena and one captured step of O(stages) launches
 //     advances them all, each with its own dt and end time.  Requests admitted
-//     while others run join the running batch at its next step.
+//     while others run join the running batch at its next step.  With a
+//     member limit a class spreads over several batches, each on its own
+//     stream, whose steps overlap on the device.
 // Requests never share reductions or change each other's arithmetic, so a
 // result does not depend on which other requests were in flight.
 
@@ -77,6 +79,7 @@ struct cles_server {
     std::vector<int64_t> running;
     std::map<int64_t, std::unique_ptr<Request>> reqs;
     bool batching = false;
+    int batch_limit = 0;   // members per batch (0 = no limit)
     std::vector<std::unique_ptr<BatchSlot>> batches;
     std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
     double now() const {
@@ -100,7 +103,8 @@ struct cles_server {
     // the batch slot of r's class, created on first use
     int batch_for(const cles_solver_desc& d) {
         for (size_t i = 0; i < batches.size(); ++i)
-            if (batch_compatible(batches[i]->cls, d)) return (int)i;
+            if ((batch_limit <= 0 || batches[i]->members < batch_limit) && batch_compatible(batches[i]->cls, d))
+                return (int)i;
         auto slot = std::make_unique<BatchSlot>();
         slot->ctx.device = device;
         CLES_CUDA(cudaStreamCreateWithFlags(&slot->ctx.stream, cudaStreamNonBlocking));
@@ -327,10 +331,12 @@ int cles_server_tick(cles_server* s, int* n_running, int* n_queued) {
     SAPI_END
 }
 
-int cles_server_set_batching(cles_server* s, int on) {
+int cles_server_set_batching(cles_server* s, int on, int max_members) {
     SAPI_BEGIN
     if (!s) throw Error(CLES_EINVAL, "null server");
+    if (max_members < 0) throw Error(CLES_EINVAL, "max_members must be >= 0");
     s->batching = on != 0;
+    s->batch_limit = max_members;
     SAPI_END
 }
 

@@ -11,7 +11,10 @@ whole ensemble, each in mixed precision and in FP64 on the same GPU:
           for all cases together (line solves from per-grid descriptor
           tables, autotuned lines per CTA); cases retire as they finish;
   server  a cles_server: each case its own solver and stream, one CUDA-graph
-          launch per case per step.
+          launch per case per step;
+  batchesK a cles_server with batching: the cases spread over batches of at
+          most K members (default 16), each on its own stream, whose captured
+          steps run concurrently.
 
 Reported per mode and precision: aggregate cell-steps/s (sum over cases of
 cells x steps, over the wall time of the whole ensemble), solves/s, and per
@@ -55,8 +58,8 @@ def draw_cases(n, seed, nx_range=(128, 1024), ny_range=(64, 256)):
     return out
 
 
-def serve(cl, reqs, max_active, budget):
-    srv = cl.Server(hbm_budget=budget, max_active=max_active)
+def serve(cl, reqs, max_active, budget, batching=False, batch_members=0):
+    srv = cl.Server(hbm_budget=budget, max_active=max_active, batching=batching, batch_members=batch_members)
     t0 = time.perf_counter()
     ids = [srv.submit(desc, Q0, tf) for desc, Q0, tf in reqs]
     srv.drain()
@@ -138,6 +141,11 @@ def main(argv=None):
                         "steps": len(sel), "s": sum(sel), "ms_per_step": 1e3 * sum(sel) / max(len(sel), 1)}
                 extra = {"compositions": bstats["compositions"], "launches_per_step": bstats["launches_per_step"],
                          "batch_steps": bstats["steps"], "time_by_members_running": bands}
+            elif mode.startswith("batches"):
+                # a cles_server with batching: the cases spread over batches of at
+                # most k members, each on its own stream, stepped concurrently
+                k = int(mode[len("batches"):] or 16)
+                wall, steps, st = serve(cl, reqs, a.max_active, int(a.budget_gb * (1 << 30)), True, k)
             else:
                 wall, steps, st = serve(cl, reqs, a.max_active, int(a.budget_gb * (1 << 30)))
             cs = sum(nx * ny * k for (nx, ny, _, _), k in zip(cases, steps))

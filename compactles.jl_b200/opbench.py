@@ -9,6 +9,7 @@ a_m ~ N(0, 1), phi_m ~ U[0, 2pi), seed 20261203 + field index.
   python compactles.jl_b200/opbench.py [--n 256] [--fields 5] [--reps 5]
   python compactles.jl_b200/opbench.py --ncu-case      # 3 + 3 launches for an ncu capture
   python compactles.jl_b200/opbench.py --ncu-case closed   # the same on closed lines
+  python compactles.jl_b200/opbench.py --ncu-case periodic --ncu-scheme c10 --ncu-dtype f32
 
 Algorithmic bytes per launch: every field read once and written once,
 2 * sizeof(T) * n^3 per field.  FP32 cases also report their error against
@@ -69,8 +70,8 @@ def run(args):
     results = []
     cases = [(p, dt) for p in (True, False) for dt in ("f64", "f32")]
     if args.ncu_case:
-        cases = [(args.ncu_case != "closed", "f64")]
-        schemes = {"c6": schemes["c6"]}
+        cases = [(args.ncu_case != "closed", args.ncu_dtype)]
+        schemes = {args.ncu_scheme: schemes[args.ncu_scheme]}
     if getattr(args, "cases", None):
         cases = args.cases
     if getattr(args, "schemes", None):
@@ -125,7 +126,7 @@ def run(args):
             # the captured launches: one per direction
             for dim in (1, 2, 3):
                 g = cl.grid((n, n, n), (periodic,) * 3)
-                plan = cl.plan_direction(g, schemes["c6"], dim, h, dtype=dts, layout="interior", ctx=ctx)
+                plan = cl.plan_direction(g, schemes[args.ncu_scheme], dim, h, dtype=dts, layout="interior", ctx=ctx)
                 cl.api._check(cl.lib().cles_apply_along_batch(plan.ptr, C.c_void_p(fin.data_ptr()),
                                                               C.c_void_p(fout.data_ptr()), nf, n ** 3))
             torch.cuda.synchronize()
@@ -139,6 +140,8 @@ if __name__ == "__main__":
     p.add_argument("--fields", type=int, default=5)
     p.add_argument("--reps", type=int, default=5)
     p.add_argument("--ncu-case", nargs="?", const="periodic", default=None, choices=["periodic", "closed"],
-                   help="3 + 3 C6 FP64 launches (one warm, one captured per direction) for an ncu capture")
+                   help="3 + 3 launches (one warm, one captured per direction) for an ncu capture")
+    p.add_argument("--ncu-scheme", choices=["c6", "c10", "filter"], default="c6")
+    p.add_argument("--ncu-dtype", choices=["f64", "f32"], default="f64")
     p.add_argument("--keep", action="store_true", help=argparse.SUPPRESS)
     run(p.parse_args())

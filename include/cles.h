@@ -560,10 +560,12 @@ int  cles_server_cancel(cles_server* s, int64_t id);
 /* Batching (off by default): while on, an admitted request that the batch
  * path supports (see cles_batch_create) joins a batch of its physics class
  * instead of getting its own solver; every tick advances each batch by one
- * captured step, whatever its member count.  Batched results equal the same
+ * captured step, whatever its member count.  max_members > 0 caps the
+ * members of one batch: a class then spreads over several batches, each on
+ * its own stream, stepped concurrently.  Batched results equal the same
  * request run alone through a batch, bitwise, and the one-grid solver's to
  * rounding (different line-solve kernels). */
-int  cles_server_set_batching(cles_server* s, int on);
+int  cles_server_set_batching(cles_server* s, int on, int max_members);
 
 /* ---- batches: many solves of one physics class advanced together --------
  * No counterpart in the reference (one problem per process there).  A batch
