@@ -395,7 +395,7 @@ __device__ __forceinline__ void tg_correct(const TileGenParams& G, T (&y)[MS], c
 // closure stencils read the whole line from the tile, and the reduced inverse
 // (2qS)^2 sits in shared memory.
 template <typename T, int Q, int M, int MS>
-__global__ void __launch_bounds__(256, 1)
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1)
     k_compact_tg(const __grid_constant__ CUtensorMap map, const __grid_constant__ CompactParams P,
                  const __grid_constant__ TileGenParams GP, const T* __restrict__ tab, const FieldView out,
                  const int mode, const int count, const int NS, const RkEpilogue rk, const int H,
@@ -618,7 +618,7 @@ template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 
 template <typename T, int Q, int M, int MS, int NS>
-__global__ void __launch_bounds__(256, 1)
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1)
     k_compact_xt(const __grid_constant__ CompactParams P, const __grid_constant__ TileGenParams GP,
                  const T* __restrict__ tab, const FieldView in, const FieldView out, const int mode, const int count,
                  const int H, T* __restrict__ iface) {
@@ -863,7 +863,7 @@ template <typename T, int Q, int M, int MS>
 void launch_tg_ms(const CompactPlan& plan, const CUtensorMap& map, const FieldView& out, int count, int mode,
                   cudaStream_t st, const T* tab, const RkEpilogue& rk, int H, T* iface) {
     const CompactParams& P = plan.P;
-    const int NS = sizeof(T) == 8 ? 3 : 4;
+    const int NS = 3;
     const int N = 2 * Q * P.S;
     const size_t smem = sizeof(T) * (size_t)(P.n + 2 * H) * kLanes * NS + 8 * sizeof(uint64_t) +
                         sizeof(T) * ((size_t)kLanes * (N + 1) + (size_t)N * N);
@@ -881,8 +881,10 @@ void launch_tg_ms(const CompactPlan& plan, const CUtensorMap& map, const FieldVi
     const int gx = (P.nx + kLanes - 1) / kLanes;
     const int work = gx * (P.dim == 1 ? P.nz : P.ny) * count;
     // lines of fewer than 8 segments leave an SM with few warps: run as many
-    // persistent CTAs per SM as shared memory and 256 threads per SM-slot allow
+    // persistent CTAs per SM as shared memory and 256 threads per SM-slot allow;
+    // FP32 (at most 128 registers a thread) runs at least two
     int per_sm = 256 / (kLanes * P.S);
+    if (sizeof(T) == 4 && per_sm < 2) per_sm = 2;
     const int by_smem = (int)((227 * 1024) / (smem + 1024));
     if (per_sm > by_smem) per_sm = by_smem;
     if (per_sm < 1) per_sm = 1;
@@ -921,7 +923,7 @@ template <typename T, int Q, int M, int MS>
 void launch_xt_ms(const CompactPlan& plan, const FieldView& in, const FieldView& out, int count, int mode,
                   cudaStream_t st, const T* tab, int H, T* iface) {
     const CompactParams& P = plan.P;
-    constexpr int NS = sizeof(T) == 8 ? 2 : 3;
+    constexpr int NS = 2;
     const int N = 2 * Q * P.S;
     const size_t smem = sizeof(T) * ((size_t)(P.n + 2 * H) * (kLanes + 1) * NS + (size_t)P.n * (kLanes + 1) +
                                      (size_t)kLanes * (N + 1) + (size_t)N * N);
@@ -938,8 +940,10 @@ void launch_xt_ms(const CompactPlan& plan, const FieldView& in, const FieldView&
     }
     const int64_t groups = (P.lines + kLanes - 1) / kLanes;
     const int64_t work = groups * count;
-    // as k_compact_tg: several persistent CTAs per SM for lines of fewer than 8 segments
+    // as k_compact_tg: several persistent CTAs per SM for lines of fewer than 8
+    // segments, and at least two for FP32
     int per_sm = 256 / (kLanes * P.S);
+    if (sizeof(T) == 4 && per_sm < 2) per_sm = 2;
     const int by_smem = (int)((227 * 1024) / (smem + 1024));
     if (per_sm > by_smem) per_sm = by_smem;
     if (per_sm < 1) per_sm = 1;
