@@ -128,6 +128,7 @@ def lib():
         L.cles_batch_fetch.argtypes = [vp, C.c_int64, vp]
         L.cles_batch_cancel.argtypes = [vp, C.c_int64]
         L.cles_batch_stats_get.argtypes = [vp, C.POINTER(abi.cles_batch_stats)]
+        L.cles_batch_set_strategy.argtypes = [vp, C.c_int]
         L.cles_kinetic_energy.argtypes = [vp, dp]
         L.cles_dissipation_rate.argtypes = [vp, dp]
         _lib = L
@@ -512,11 +513,19 @@ class Batch:
     whatever the number of members.  `cls` is a solver descriptor of the class
     (grid extents, domain and boundary states are per member)."""
 
-    def __init__(self, cls, ctx=None):
+    STRATEGIES = {"auto": 0, "batched": 1, "per_member": 2}
+
+    def __init__(self, cls, ctx=None, strategy="auto"):
         self.ctx = ctx or default_context()
         self.ptr = C.c_void_p()
         _check(lib().cles_batch_create(self.ctx.ptr, C.byref(cls), C.byref(self.ptr)))
         self._shape = {}
+        if strategy != "auto":
+            self.set_strategy(strategy)
+
+    def set_strategy(self, strategy):
+        """How line solves launch: "batched", "per_member" or "auto" (the autotuner picks per operator)."""
+        _check(lib().cles_batch_set_strategy(self.ptr, self.STRATEGIES[strategy]))
 
     def __del__(self):
         try:

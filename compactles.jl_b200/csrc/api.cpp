@@ -831,3 +831,10 @@ int cles_batch_stats_get(const cles_batch* b, cles_batch_stats* out) {
     b->b->stats(out);
     API_END
 }
+
+int cles_batch_set_strategy(cles_batch* b, int strategy) {
+    API_BEGIN
+    if (!b) throw Error(CLES_EINVAL, "null batch");
+    b->b->set_strategy(strategy);
+    API_END
+}

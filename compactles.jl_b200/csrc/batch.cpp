@@ -139,7 +139,8 @@ struct Member {
     bool periodic[3] = {true, true, true};
     double h[3] = {1, 1, 1};
     int64_t cells = 0;
-    std::unique_ptr<CompactPlan> deriv[3], filt[3], qfilt[3];
+    std::unique_ptr<CompactPlan> deriv[3], filt[3], qfilt[3];      // batched segmentation
+    std::unique_ptr<CompactPlan> sderiv[3], sfilt[3], sqfilt[3];   // the one-grid solver's plans
     std::vector<double> Qhost;     // interior layout: initial state until placed, final state once retired
     bool placed = false;           // its state lives in the arena
     bool retired = false;          // finished, failed or removed; Qhost holds the last state
@@ -157,7 +158,10 @@ struct Role {
     BatchLaunchKind kind{};
     DevBuf plans, blocks;
     int nblocks = 0;
+    bool per_member = false;   // launch each member's one-grid kernel instead of the batched one
 };
+
+constexpr int kAuxStreams = 8;   // streams the per-member launches of one role spread over
 
 enum { R_DERIV = 0, R_FILT = 1, R_QFILT = 2 };
 
@@ -185,6 +189,11 @@ public:
         CLES_CUDA(cudaStreamCreateWithFlags(&cap_st_, cudaStreamNonBlocking));
         CLES_CUDA(cudaEventCreate(&ev0_));
         CLES_CUDA(cudaEventCreate(&ev1_));
+        for (int i = 0; i < kAuxStreams; ++i) {
+            CLES_CUDA(cudaStreamCreateWithFlags(&aux_[i], cudaStreamNonBlocking));
+            CLES_CUDA(cudaEventCreateWithFlags(&aux_ev_[i], cudaEventDisableTiming));
+        }
+        CLES_CUDA(cudaEventCreateWithFlags(&fork_ev_, cudaEventDisableTiming));
     }
     ~Batch() override {
         if (exec_) cudaGraphExecDestroy(exec_);
@@ -192,6 +201,11 @@ public:
         if (cap_st_) cudaStreamDestroy(cap_st_);
         cudaEventDestroy(ev0_);
         cudaEventDestroy(ev1_);
+        for (int i = 0; i < kAuxStreams; ++i) {
+            cudaStreamDestroy(aux_[i]);
+            cudaEventDestroy(aux_ev_[i]);
+        }
+        cudaEventDestroy(fork_ev_);
     }
 
     int64_t add(const cles_solver_desc& d, const double* Q0, int layout, double tfinal, int64_t nmax,
@@ -227,6 +241,14 @@ public:
                 m->qfilt[k].reset(new CompactPlan());
                 build_compact_plan(*m->qfilt[k], d.filt, m->n, k, m->periodic[k], m->h[k], CLES_F64, 0, 0, false,
                                    false, sm);
+            }
+            m->sderiv[k].reset(new CompactPlan());
+            build_compact_plan(*m->sderiv[k], d.deriv, m->n, k, m->periodic[k], m->h[k], dtF);
+            m->sfilt[k].reset(new CompactPlan());
+            build_compact_plan(*m->sfilt[k], d.filt, m->n, k, m->periodic[k], m->h[k], dtF);
+            if (dtF != CLES_F64) {
+                m->sqfilt[k].reset(new CompactPlan());
+                build_compact_plan(*m->sqfilt[k], d.filt, m->n, k, m->periodic[k], m->h[k], CLES_F64);
             }
         }
         for (int sp = 0; sp < Ns_; ++sp) {
@@ -345,6 +367,13 @@ public:
                                 &m.Qhost[(size_t)(c * m.cells + (int64_t)j * m.n[0] + (int64_t)kk * m.n[0] * m.n[1])],
                                 sizeof(double) * m.n[0]);
                 }
+    }
+
+    void set_strategy(int st) override {
+        if (st != CLES_BATCH_AUTO && st != CLES_BATCH_BATCHED && st != CLES_BATCH_PER_MEMBER)
+            throw Error(CLES_EINVAL, "unknown batch strategy");
+        strategy_ = st;
+        dirty_ = true;   // re-tune and re-capture at the next step
     }
 
     void stats(cles_batch_stats* s) const override {
@@ -629,6 +658,7 @@ private:
         R.kind.threads = threads;
         R.kind.smem = smem;
         R.kind.ms = ms;
+        R.per_member = false;
         upload(R.plans, ctx_, plans, st_);
         upload(R.blocks, ctx_, blocks, st_);
         R.nblocks = (int)blocks.size();
@@ -663,10 +693,15 @@ private:
                 tuned_ms_[r][k] = 0.0;
                 if (!act_[k]) continue;
                 if (r == R_QFILT && cls_.filter_interval == 0) continue;
+                if (strategy_ == CLES_BATCH_PER_MEMBER) { set_role(r, k, 0); continue; }
                 const std::string key = role_key(r, k);
                 auto& cache = batch_tuning_cache();
-                auto it = cache.find(key);
-                if (it != cache.end() && role_tables(r, k, it->second, roles_[r][k])) continue;
+                auto it = strategy_ == CLES_BATCH_AUTO ? cache.find(key) : cache.end();
+                if (it != cache.end() && (it->second == 0 || role_tables(r, k, it->second, roles_[r][k]))) {
+                    set_role(r, k, it->second);
+                    continue;
+                }
+                roles_[r][k].per_member = false;
                 int best = -1;
                 float best_ms = 1e30f;
                 for (int th : {128, 256, 512}) {
@@ -689,18 +724,91 @@ private:
                     ms /= reps;
                     if (ms < best_ms) { best_ms = ms; best = th; }
                 }
+                // the other strategy: every member's one-grid kernel, on the auxiliary streams
+                if (strategy_ == CLES_BATCH_AUTO) {
+                    const bool f64 = (r == R_QFILT) || sizeof(F) == 8;
+                    const void* in = f64 && r == R_QFILT ? static_cast<const void*>(Q_.p) : static_cast<const void*>(prim_.p);
+                    void* out = r == R_QFILT ? flux_.p : scratch_.p;
+                    along_members(r, k, in, out, 1, OUT_STORE, 0);
+                    CLES_CUDA(cudaEventRecord(ev0_, st_));
+                    const int reps = 3;
+                    for (int i = 0; i < reps; ++i) along_members(r, k, in, out, 1, OUT_STORE, 0);
+                    CLES_CUDA(cudaEventRecord(ev1_, st_));
+                    CLES_CUDA(cudaEventSynchronize(ev1_));
+                    float ms = 0;
+                    CLES_CUDA(cudaEventElapsedTime(&ms, ev0_, ev1_));
+                    ms /= reps;
+                    if (ms < best_ms) { best_ms = ms; best = 0; }   // 0 threads: per-member launches
+                }
                 if (best < 0) throw Error(CLES_EINVAL, "no batched launch shape fits the lines of this batch");
-                cache[key] = best;
+                if (strategy_ == CLES_BATCH_AUTO) cache[key] = best;
                 tuned_ms_[r][k] = best_ms;
-                role_tables(r, k, best, roles_[r][k]);
+                set_role(r, k, best);
             }
+    }
+    void set_role(int r, int k, int choice) {
+        if (choice == 0) {
+            Role& R = roles_[r][k];
+            R.plans.release();
+            R.blocks.release();
+            R.nblocks = (int)order_.size();   // members, for the statistics
+            R.kind = BatchLaunchKind{};
+            R.per_member = true;
+        } else {
+            roles_[r][k].per_member = false;
+            role_tables(r, k, choice, roles_[r][k]);
+        }
     }
 
     // ------------------------------------------------------------ the step --
+    const CompactPlan* solo_plan_of(const Member& m, int role, int k) const {
+        if (role == R_DERIV) return m.sderiv[k].get();
+        if (role == R_FILT) return m.sfilt[k].get();
+        return m.sqfilt[k] ? m.sqfilt[k].get() : m.sfilt[k].get();
+    }
+
+    // Each member's one-grid kernel (the solver's own choice of tile, warp or
+    // generic kernel) on its views of the arena, spread over the auxiliary
+    // streams between a fork and a join on the batch stream.  OUT_RK tries the
+    // fused update; a member whose kernel cannot fuse it gets a subtracting
+    // store, and its `rk_fused_` entry says so for the separate RK pass.
+    void along_members(int role, int k, const void* in, void* out, int count, int mode, int stage) {
+        const size_t el = (role == R_QFILT || sizeof(F) == 8) ? sizeof(double) : sizeof(float);
+        CLES_CUDA(cudaEventRecord(fork_ev_, st_));
+        const int ns = std::min<int>(kAuxStreams, (int)order_.size());
+        for (int i = 0; i < ns; ++i) CLES_CUDA(cudaStreamWaitEvent(aux_[i], fork_ev_, 0));
+        for (size_t g = 0; g < order_.size(); ++g) {
+            const Member& m = *order_[g];
+            const CompactPlan* p = solo_plan_of(m, role, k);
+            cudaStream_t st = aux_[g % ns];
+            const int64_t sy = m.n[0], sz = (int64_t)m.n[0] * m.n[1];
+            const FieldView vin{const_cast<char*>(static_cast<const char*>(in)) + el * (size_t)m.off, ct_, sy, sz};
+            const FieldView vout{static_cast<char*>(out) + el * (size_t)m.off, ct_, sy, sz};
+            if (mode == OUT_RK) {
+                const RkEpilogue rk{Q_.as<double>() + m.off, du_.as<double>() + m.off, kLsrkA[stage], kLsrkB[stage],
+                                    0.0, clk_.as<double>() + 16 * g + DC_DT};
+                const bool fused = launch_compact_rk(*p, vin, vout, count, rk, st);
+                if (!fused) launch_compact(*p, vin, vout, count, OUT_SUBTRACT, st);
+                rk_fused_[g] = fused ? 1 : 0;
+            } else {
+                launch_compact(*p, vin, vout, count, mode, st);
+            }
+        }
+        for (int i = 0; i < ns; ++i) {
+            CLES_CUDA(cudaEventRecord(aux_ev_[i], aux_[i]));
+            CLES_CUDA(cudaStreamWaitEvent(st_, aux_ev_[i], 0));
+        }
+    }
+
     void along(int role, int k, const void* in, void* out, int count, int mode, int stage = 0, int skip = 0) {
         Role& R = roles_[role][k];
+        if (R.per_member) {
+            along_members(role, k, in, out, count, mode, stage);
+            return;
+        }
         launch_compact_batch(R.kind, R.plans.as<BatchLinePlan>(), R.blocks.as<int2>(), R.nblocks, in, out, ct_, count,
                              mode, Q_.as<double>(), du_.as<double>(), kLsrkA[stage], kLsrkB[stage], skip, st_);
+        if (mode == OUT_RK) std::fill(rk_fused_.begin(), rk_fused_.end(), 1);
     }
     void smooth(F* f, int count) {
         for (int k = 0; k < 3; ++k)
@@ -773,9 +881,23 @@ private:
             const int mode = seen == nact ? OUT_RK : (seen == 1 ? OUT_NEGATE : OUT_SUBTRACT);
             along(R_DERIV, k, fin, dQ_.p, ncons_, mode, stage);
         }
+        // members whose last divergence could not apply the update (per-member
+        // kernels without the fused store): one batched RK pass, each with its dt
+        if (roles_[R_DERIV][last_dim()].per_member)
+            BatchOps<F>::lsrk(Q_.as<double>(), du_.as<double>(), dQ_.as<F>(), ct_, ncons_, tmap_.as<int>(),
+                              grids_.as<BatchGrid>(), need_lsrk_.as<int>(), kLsrkA[stage], kLsrkB[stage], st_);
+    }
+    int last_dim() const {
+        int l = 0;
+        for (int k = 0; k < 3; ++k)
+            if (act_[k]) l = k;
+        return l;
     }
 
     void capture() {
+        rk_fused_.assign(order_.size(), 1);
+        need_lsrk_.release();
+        need_lsrk_.alloc(ctx_, sizeof(int) * order_.size());
         cudaGraph_t g = nullptr;
         const cudaStream_t user = st_;
         st_ = cap_st_;
@@ -813,6 +935,10 @@ private:
             throw Error(CLES_ECUDA, std::string("cudaStreamEndCapture: ") + cudaGetErrorString(ee));
         }
         launches_per_step_ = (int)(launch_count() - l0);
+        // which members the separate RK pass updates (read by the graph when it runs)
+        std::vector<int> need(order_.size());
+        for (size_t i = 0; i < order_.size(); ++i) need[i] = rk_fused_[i] ? 0 : 1;
+        CLES_CUDA(cudaMemcpy(need_lsrk_.p, need.data(), sizeof(int) * need.size(), cudaMemcpyHostToDevice));
         const cudaError_t e = cudaGraphInstantiate(&exec_, g, 0);
         cudaGraphDestroy(g);
         if (e != cudaSuccess) throw Error(CLES_ECUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
@@ -821,6 +947,10 @@ private:
     cles_ctx* ctx_;
     cudaStream_t st_ = nullptr, cap_st_ = nullptr;
     cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
+    cudaStream_t aux_[kAuxStreams] = {};
+    cudaEvent_t aux_ev_[kAuxStreams] = {}, fork_ev_ = nullptr;
+    std::vector<int> rk_fused_;   // per member: its RK update ran inside the last divergence
+    DevBuf need_lsrk_;            // per member: 1 when the separate batched RK pass must update it
     cles_solver_desc cls_;
     int Ns_ = 1, ncons_ = 5;
     bool act_[3] = {false, false, false};
@@ -830,6 +960,7 @@ private:
     std::vector<int64_t> cancelled_;
     int64_t next_id_ = 1;
     bool dirty_ = false, launched_ = false;
+    int strategy_ = CLES_BATCH_AUTO;
     int64_t ct_ = 0;
     DevBuf Q_, art_, clk_;
     DevBuf du_, dQ_, prim_, g_u_, gty_, scratch_, flux_, part_;

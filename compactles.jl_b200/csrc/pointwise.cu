@@ -1006,6 +1006,25 @@ __global__ void k_bc_batch(double* __restrict__ Q, const BatchGrid* __restrict__
     bc_plane_body(Q + G.off, G.g, ct, f.d, f.side, Ns, f.kind, f.st, nullptr, threadIdx.x, blockDim.x);
 }
 
+// The LSRK update of the members flagged in need[] (whose last divergence did
+// not apply it), each with its own dt; fields are ct elements apart.
+template <typename F>
+__global__ void k_lsrk_batch(double* __restrict__ Q, double* __restrict__ du, const F* __restrict__ dQ, int64_t ct,
+                             int ncons, const int* __restrict__ tmap, const BatchGrid* __restrict__ grids,
+                             const int* __restrict__ need, double A, double B) {
+    GRID_STRIDE(I, ct) {
+        const int g = tmap[I >> 6];
+        if (!need[g]) continue;
+        const double dt = grids[g].clk[DC_DT];
+        for (int c = 0; c < ncons; ++c) {
+            const int64_t e = I + ct * c;
+            const double v = A * du[e] + dt * double(dQ[e]);
+            du[e] = v;
+            Q[e] += B * v;
+        }
+    }
+}
+
 __global__ void k_clock_after_batch(const BatchGrid* __restrict__ grids, int G) {
     const int g = blockIdx.x * blockDim.x + threadIdx.x;
     if (g < G) clock_after_body(grids[g].clk, grids[g].cc);
@@ -1054,6 +1073,11 @@ void BatchOps<F>::fluxes(const double* Q, const F* prim, const F* g, const F* gt
     else
         LAUNCH((k_fluxes<F, false, false, false, true>), ct, st, Q, prim, g, gty, art, flux, ct, Ns, pc, mu0, Pr, Sc,
                G, mc, tmap);
+}
+template <typename F>
+void BatchOps<F>::lsrk(double* Q, double* du, const F* dQ, int64_t ct, int ncons, const int* tmap,
+                       const BatchGrid* grids, const int* need, double A, double B, cudaStream_t st) {
+    LAUNCH(k_lsrk_batch<F>, ct, st, Q, du, dQ, ct, ncons, tmap, grids, need, A, B);
 }
 template struct BatchOps<double>;
 template struct BatchOps<float>;

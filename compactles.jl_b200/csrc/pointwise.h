@@ -268,6 +268,10 @@ struct BatchOps {
     // max_rate of every grid (per-chunk partials, then one block per grid
     // reduces them) followed by the graph-mode clock_before of that grid;
     // chunk_first[g] .. chunk_first[g + 1] are grid g's chunks
+    // LSRK update (src/timestep.jl:86-95) of the members with need[m] != 0,
+    // each with the dt of its clock
+    static void lsrk(double* Q, double* du, const F* dQ, int64_t cells_total, int ncons, const int* tmap,
+                     const BatchGrid* grids, const int* need, double A, double B, cudaStream_t st);
     static void rate_clock(const double* Q, const F* prim, const F* art, const BatchGrid* grids, int G,
                            const BatchChunk* chunks, int nchunks, const int* chunk_first, double* part,
                            int64_t cells_total, int Ns, double mu0, double Pr, double Sc, cudaStream_t st);

@@ -98,6 +98,7 @@ public:
     virtual void status(int64_t id, cles_request_status* out) const = 0;
     virtual void fetch(int64_t id, double* Q, int layout) = 0;
     virtual void stats(cles_batch_stats* s) const = 0;
+    virtual void set_strategy(int strategy) = 0;
 };
 std::unique_ptr<BatchBase> make_batch(cles_ctx* ctx, const cles_solver_desc& cls);
 // d fits a batch of class cls (supported and equal in every class field)

@@ -596,9 +596,9 @@ typedef struct cles_batch cles_batch;
 typedef struct cles_batch_tuning {
     int     op;          /* 0 derivative, 1 filter of derived fields, 2 filter_state! of Q */
     int     dim;         /* 1-based direction */
-    int     threads;     /* chosen threads per CTA */
+    int     threads;     /* chosen threads per CTA of the batched kernel; 0 = per-member kernels */
     int64_t smem;        /* dynamic shared memory per CTA */
-    int     ctas;        /* CTAs per field */
+    int     ctas;        /* CTAs per field (per-member kernels: the member count) */
     double  tuned_ms;    /* the winner's time per launch (one field) when it was tuned here, else 0 */
 } cles_batch_tuning;
 typedef struct cles_batch_stats {
@@ -626,6 +626,20 @@ int  cles_batch_status(cles_batch* b, int64_t id, cles_request_status* out);
 int  cles_batch_fetch(cles_batch* b, int64_t id, double* Q_host);
 int  cles_batch_cancel(cles_batch* b, int64_t id);
 int  cles_batch_stats_get(const cles_batch* b, cles_batch_stats* out);
+/* How the line solves of a batch step are launched.  CLES_BATCH_BATCHED: one
+ * batched kernel per operator and direction over every member (a fixed
+ * number of launches per step).  CLES_BATCH_PER_MEMBER: every member's
+ * one-grid kernel (the tile, warp or generic kernel the solver would pick),
+ * spread over eight streams inside the captured step; members whose last
+ * divergence cannot apply the RK update get one batched RK pass.
+ * CLES_BATCH_AUTO (default): the autotuner times both for every operator and
+ * direction and keeps the faster.  Results of the two forms agree to
+ * rounding; with a fixed form a member's results do not depend on the other
+ * members.  Takes effect at the next step. */
+#define CLES_BATCH_AUTO        0
+#define CLES_BATCH_BATCHED     1
+#define CLES_BATCH_PER_MEMBER  2
+int  cles_batch_set_strategy(cles_batch* b, int strategy);
 
 /* Volume-averaged kinetic energy ∫½ρ|u|²dV / V and dissipation rate
  * (src/diagnostics.jl:354-378, bench/tgv_energy.jl:175-184) of the resident

@@ -5,11 +5,14 @@ Checked here, against the one-grid solver and the CPU oracle on the same
 inputs:
 * every member of a batch of uneven 2-D He/CO2 shock-interface grids matches
   the one-grid solver and the oracle to 1e-10 relative L2 after 30 steps
-  (FP64), and its results are bitwise the same alone and in the mix;
+  (FP64), and, with a fixed launch form (batched kernels or per-member
+  kernels), its results are bitwise the same alone and in the mix; the two
+  forms and the autotuner's mix of them agree to 1e-12;
 * members with different end times retire as they finish (the composition
   changes and the step is re-captured), each ending exactly at its end time
   with the state of its solo run;
-* the kernels in one captured step do not grow with the number of members;
+* with the batched form, the kernels in one captured step do not grow with
+  the number of members;
 * 3-D Taylor-Green boxes and 1-D two-species tubes in batches, FP64 and the
   mixed form (FP32 fields, FP64 state; 1e-5 relative L2 against the FP64
   oracle after 20 steps, FP32 rounding of the terms accumulated over the
@@ -38,8 +41,8 @@ def _cases(m, precision="fp64", shapes=SHAPES):
     return [scenarios.shock_interface_2d(sch, nx, ny, M, sd, precision=precision) for nx, ny, M, sd in shapes]
 
 
-def _batch(reqs, steps=None):
-    B = cl.Batch(reqs[0][0])
+def _batch(reqs, steps=None, strategy="auto"):
+    B = cl.Batch(reqs[0][0], strategy=strategy)
     ids = [B.add(d, Q0, tf) for d, Q0, tf in reqs]
     if steps is None:
         assert B.run() == 0
@@ -73,12 +76,30 @@ def test_batch_matches_solo_and_oracle(orc):
         assert rs < 1e-10, rs
 
 
-def test_batch_member_alone_equals_in_mix():
+@pytest.mark.parametrize("strategy", ["batched", "per_member"])
+def test_batch_member_alone_equals_in_mix(strategy):
+    # with a fixed launch form a member's arithmetic does not depend on the others
     reqs = _cases(cl)
-    B, ids = _batch(reqs, steps=12)
+    B, ids = _batch(reqs, steps=12, strategy=strategy)
     for k in (1, 2):
-        A, aid = _batch([reqs[k]], steps=12)
+        A, aid = _batch([reqs[k]], steps=12, strategy=strategy)
         assert np.array_equal(A.fetch(aid[0]), B.fetch(ids[k]))
+
+
+def test_batch_strategies_agree():
+    # the batched kernels, the per-member kernels and the autotuner's mix of
+    # them give the same states to rounding
+    reqs = _cases(cl)
+    out = {}
+    for strategy in ("batched", "per_member", "auto"):
+        B, ids = _batch(reqs, steps=20, strategy=strategy)
+        out[strategy] = [B.fetch(i) for i in ids]
+        if strategy == "auto":
+            assert {t["threads"] for t in B.stats()["tuning"]} <= {0, 128, 256, 512}
+    for k, (d, _, _) in enumerate(reqs):
+        for strategy in ("per_member", "auto"):
+            r = _rel(out[strategy][k], out["batched"][k], d)
+            assert r < 1e-12, (strategy, k, r)
 
 
 def test_batch_members_retire_at_their_end_times():
@@ -98,8 +119,8 @@ def test_batch_members_retire_at_their_end_times():
 
 def test_batch_launches_do_not_grow_with_members():
     reqs = _cases(cl)
-    B2, _ = _batch(reqs[:2], steps=1)
-    B4, _ = _batch(reqs, steps=1)
+    B2, _ = _batch(reqs[:2], steps=1, strategy="batched")
+    B4, _ = _batch(reqs, steps=1, strategy="batched")
     n2, n4 = B2.stats()["launches_per_step"], B4.stats()["launches_per_step"]
     assert n2 == n4 and 0 < n4 < 200
     tun = B4.stats()["tuning"]
