@@ -83,14 +83,15 @@ struct CompactParams {
     int64_t lines;
 };
 
-// Warp-per-line form for periodic tridiagonal x lines of n = 32 * XP points:
+// Warp-per-line form for periodic tridiagonal x lines of n = 32 * XP points
+// (XP = 2, 4, 6, 8, 12, 16: n = 64, 128, 192, 256, 384, 512):
 // lane s owns the XP contiguous points [s*XP, (s+1)*XP).  Every lane segment
 // is the same Toeplitz block, so the local factorisation, the spikes and the
 // parallel-cyclic-reduction matrices of the 32-segment interface system are
 // line- and lane-independent and travel as kernel parameters.
 constexpr int kMaxXP = 16;
 struct WarpLineParams {
-    int XP;                                   // points per lane: 4, 8 or 16
+    int XP;                                   // points per lane: 2, 4, 6, 8, 12 or 16
     double l[kMaxXP], dinv[kMaxXP], c[kMaxXP];  // segment Thomas factors
     double v[kMaxXP], w[kMaxXP];              // spikes: couplings to the previous tail / next head
     double alpha[4][4], gamma[4][4];          // PCR steps at distances 1, 2, 4, 8 (2x2, row-major)

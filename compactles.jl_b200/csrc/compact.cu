@@ -25,6 +25,7 @@
 // exchange_halos! (src/operators.jl:113-174).
 
 #include <cstdio>
+#include <type_traits>
 
 #include "cles_internal.h"
 #include "compact_body.cuh"
@@ -42,15 +43,21 @@ __global__ void __launch_bounds__(512) k_compact(const __grid_constant__ Compact
 }
 
 // ---------------------------------------------------------------------------
-// Warp-per-line kernel for periodic tridiagonal x lines of n = 32 * XP points.
+// Warp-per-line kernel for periodic tridiagonal x lines of n = 32 * XP points
+// (XP = 2, 4, 6, 8, 12, 16).
 // Lane s of a warp owns the XP contiguous points [s*XP, (s+1)*XP) of one line:
 // vector loads and stores straight from/to global memory (the warp covers the
 // whole contiguous line), stencil halos from the neighbouring lanes by shuffle,
 // the lane's Thomas sweep in registers, and the 32-segment interface system by
 // parallel cyclic reduction across the lanes with precomputed 2x2 matrices.
-template <typename T> struct Vec;
-template <> struct Vec<double> { using type = double2; static constexpr int W = 2; };
-template <> struct Vec<float> { using type = float4; static constexpr int W = 4; };
+// Vector type of the lane's loads and stores: double2, or float4 where the
+// lane's XP points are a multiple of 4 (float2 otherwise).
+template <typename T, int XP> struct Vec;
+template <int XP> struct Vec<double, XP> { using type = double2; static constexpr int W = 2; };
+template <int XP> struct Vec<float, XP> {
+    using type = typename std::conditional<XP % 4 == 0, float4, float2>::type;
+    static constexpr int W = XP % 4 == 0 ? 4 : 2;
+};
 
 template <typename T>
 __device__ __forceinline__ T wl(const double* d, const float* f, int i) {
@@ -69,8 +76,8 @@ __global__ void __launch_bounds__(256) k_compact_xw(const __grid_constant__ Comp
     const int j = line % P.ny, k = line / P.ny;
     const T* src = reinterpret_cast<const T*>(in.base) + (int64_t)comp * in.comp_stride + j * in.sy + k * in.sz + lane * XP;
     T* dst = reinterpret_cast<T*>(out.base) + (int64_t)comp * out.comp_stride + j * out.sy + k * out.sz + lane * XP;
-    using V = typename Vec<T>::type;
-    constexpr int VW = Vec<T>::W;
+    using V = typename Vec<T, XP>::type;
+    constexpr int VW = Vec<T, XP>::W;
     T f[XP];
 #pragma unroll
     for (int q = 0; q < XP / VW; ++q) {
@@ -165,8 +172,15 @@ void launch_xw_m(const CompactPlan& plan, const FieldView& in, const FieldView& 
     const int lines_per_cta = 8;
     dim3 grid((unsigned)((plan.P.lines + lines_per_cta - 1) / lines_per_cta), (unsigned)count);
     switch (plan.XW.XP) {
+        case 2:
+            // the stencil halo comes from the neighbouring lanes' XP points: XP >= M
+            if constexpr (M <= 2) k_compact_xw<T, M, 2><<<grid, 32 * lines_per_cta, 0, st>>>(plan.P, plan.XW, in, out, mode);
+            else throw Error(CLES_EINVAL, "warp-line kernel: fewer points per lane than the stencil half-width");
+            break;
         case 4: k_compact_xw<T, M, 4><<<grid, 32 * lines_per_cta, 0, st>>>(plan.P, plan.XW, in, out, mode); break;
+        case 6: k_compact_xw<T, M, 6><<<grid, 32 * lines_per_cta, 0, st>>>(plan.P, plan.XW, in, out, mode); break;
         case 8: k_compact_xw<T, M, 8><<<grid, 32 * lines_per_cta, 0, st>>>(plan.P, plan.XW, in, out, mode); break;
+        case 12: k_compact_xw<T, M, 12><<<grid, 32 * lines_per_cta, 0, st>>>(plan.P, plan.XW, in, out, mode); break;
         case 16: k_compact_xw<T, M, 16><<<grid, 32 * lines_per_cta, 0, st>>>(plan.P, plan.XW, in, out, mode); break;
         default: throw Error(CLES_EINVAL, "warp-line kernel: unsupported points per lane");
     }

@@ -146,7 +146,8 @@ void build_warp_line(CompactPlan& plan, const Band& B, const cles_scheme& s, int
     plan.has_xw = false;
     if (dim != 0 || !periodic || s.q != 1 || n % 32 != 0) return;
     const int XP = n / 32;
-    if (XP != 4 && XP != 8 && XP != 16) return;
+    // an even count of points per lane, for the lane's vector loads
+    if (XP != 2 && XP != 4 && XP != 6 && XP != 8 && XP != 12 && XP != 16) return;
     if (XP < s.M) return;
     WarpLineParams& W = plan.XW;
     std::memset(&W, 0, sizeof(W));
