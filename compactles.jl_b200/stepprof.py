@@ -7,9 +7,11 @@ Cases:
              set is about 3.6 GB), single species, artificial properties on;
   interface  a 2-D He/CO2 shock-interface grid (n x n/2, two species, slip
              walls in x): adds the species sensors and diffusion fluxes;
-  batch      the 64-case ensemble of 2-D shock-interface grids in one batch.
+  batch      the 64-case ensemble of 2-D shock-interface grids in one batch;
+  tube       a 1-D two-species shock tube of n cells (pressure ratio 10,
+             Atwood 0.5): one line, the latency-bound end of the serving mix.
 
-  python compactles.jl_b200/stepprof.py [--case tgv|interface|batch] [--n 192] [--precision fp64|mixed]
+  python compactles.jl_b200/stepprof.py [--case tgv|interface|batch|tube] [--n 192] [--precision fp64|mixed]
 """
 import argparse
 import importlib.util
@@ -32,7 +34,7 @@ def _package():
 
 def main(argv=None):
     p = argparse.ArgumentParser()
-    p.add_argument("--case", choices=["tgv", "interface", "batch"], default="tgv")
+    p.add_argument("--case", choices=["tgv", "interface", "batch", "tube"], default="tgv")
     p.add_argument("--n", type=int, default=192)
     p.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
     a = p.parse_args(argv)
@@ -56,6 +58,8 @@ def main(argv=None):
     else:
         if a.case == "tgv":
             desc, Q0, tf = cl.scenarios.taylor_green_box(sch, a.n, tfinal=1e9, precision=a.precision)
+        elif a.case == "tube":
+            desc, Q0, tf = cl.scenarios.two_species_tube(sch, a.n, 10.0, 0.5, precision=a.precision)
         else:
             desc, Q0, tf = cl.scenarios.shock_interface_2d(sch, a.n, a.n // 2, 2.0, 5, precision=a.precision)
         S = cl.Solver(desc)
