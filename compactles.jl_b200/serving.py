@@ -187,6 +187,10 @@ def main(argv=None):
         "one_at_a_time": {"solves_per_s": len(reqs) / fin[-1], "p50_s": float(np.percentile(tts_base, 50)),
                           "p99_s": float(np.percentile(tts_base, 99)), "service_s_total": sum(service)},
         "speedup_solves_per_s": (len(reqs) / max(done)) / (len(reqs) / fin[-1]),
+        # no schedule finishes before its longest request does alone: the
+        # capacity ratio over one-at-a-time is at most total / longest
+        "longest_request_alone_s": max(service),
+        "speedup_bound_total_over_longest": sum(service) / max(service),
         "results_equal_alone": same,
         **extra,
     }

@@ -7,8 +7,10 @@ warp-per-line x kernel (periodic n = 128/256/512) in its subtract-accumulate
 flux-divergence store, and the TMA tile kernel with the LSRK stage update
 fused into its store at n = 256.  The 64^3 box is the quick-start
 configuration itself: its right-hand side is compared at steps 0, 1, 10 and
-100 (device and oracle fed the oracle's state at that step), and the two
-independent 100-step runs are compared in relative L2.
+100 (device and oracle fed the oracle's state at that step), the two
+independent 100-step runs are compared in relative L2, and the whole run to
+t = 1 (the configuration's end time) is compared in relative L2 and kinetic
+energy.
 
 Bounds: per RHS, 1e-12 of each component's term scale (tests/parity.py says
 why; the plain relative error is recorded beside it); relative L2 of the state
@@ -126,3 +128,21 @@ def test_quickstart_tgv64_mixed(orc):
                   t_rel=dt_rel)
     assert rel < 1e-5, rel
     assert abs(ke_g - ke_o) <= 1e-6 * ke_o
+
+
+def test_quickstart_tgv64_to_t1(orc):
+    """The quick-start configuration as the reference runs it: the 64^3 box to t = 1."""
+    dg, do, Q0 = _descs(orc, 64)
+    S = cl.Solver(dg)
+    S.set_state(Q0)
+    O = orc.Solver(do)
+    O.set_state(Q0)
+    rg = S.run(1.0)
+    rc, ro = O.run(1.0)
+    assert rc == 0 and rg.steps == ro.steps and abs(rg.t - 1.0) < 1e-12 and abs(ro.t - 1.0) < 1e-12
+    it = _interior(dg)
+    rel = _rel_l2(it(S.get_state()), it(O.get_state()))
+    ke_g, ke_o = S.kinetic_energy(), O.kinetic_energy()
+    parity.record(f"TGV 64^3 FP64 to t = 1 ({ro.steps} steps)", state_l2=rel, ke_rel=abs(ke_g - ke_o) / ke_o)
+    assert rel < 1e-10, rel
+    assert abs(ke_g - ke_o) <= 1e-12 * ke_o
