@@ -20,3 +20,4 @@ from .api import (ClesError, Context, DirPlan, Solver, SolverFailure, apply_alon
 from . import scenarios
 from .split import LineExchange, SplitPlan, exchange_halos, split_apply_along
 from .nasa9 import Nasa9Interval, Nasa9Mixture, Nasa9Species, nasa9_constant_cp, read_nasa9
+from .decomp import Decomp, LocalGroup, TorchExchange, assemble, local_range

@@ -12,6 +12,7 @@ CLES_ENUMERIC = 3
 CLES_ETIMEOUT = 4
 CLES_ECUDA = 5
 CLES_EFAILURE = 6
+CLES_EXCHANGE = 7
 
 CLES_MAX_Q = 2
 CLES_MAX_M = 4
@@ -151,6 +152,28 @@ CLES_BC_NSCBC_INFLOW = 6
 CLES_BC_AXIS = 7
 CLES_BC_ORIGIN = 8
 CLES_BC_POLE = 9
+
+# ---- decomposition (cles_decomp / cles_exchange) ----
+CLES_REDUCE_MAX = 0
+CLES_REDUCE_SUM = 1
+
+
+class cles_decomp(C.Structure):
+    _fields_ = [("dims", C.c_int * 3), ("coords", C.c_int * 3), ("rank", C.c_int)]
+
+
+# halo(user, dim, prev, next, send_lo, send_hi, recv_lo, recv_hi, bytes, stream)
+HALO_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
+                      C.c_void_p, C.c_int64, C.c_void_p)
+# gather(user, dim, local, all, bytes, stream)
+GATHER_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p)
+# allreduce(user, op, vals, count)
+ALLREDUCE_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_int, C.POINTER(C.c_double), C.c_int)
+
+
+class cles_exchange(C.Structure):
+    _fields_ = [("user", C.c_void_p), ("halo", HALO_FN), ("gather", GATHER_FN), ("allreduce", ALLREDUCE_FN)]
+
 
 # cles_face_fn: (user, dim, side, t, npts, x1, x2, x3, out)
 FACE_FN = C.CFUNCTYPE(None, C.c_void_p, C.c_int, C.c_int, C.c_double, C.c_int64, C.POINTER(C.c_double),

@@ -85,6 +85,14 @@ def lib():
         L.cles_solver_desc_default.argtypes = [C.POINTER(abi.cles_solver_desc)]
         L.cles_solver_desc_default.restype = None
         L.cles_solver_create.argtypes = [vp, C.POINTER(abi.cles_solver_desc), C.POINTER(vp)]
+        L.cles_solver_create_decomposed.argtypes = [vp, C.POINTER(abi.cles_solver_desc), C.POINTER(abi.cles_decomp),
+                                                    C.POINTER(abi.cles_exchange), C.POINTER(vp)]
+        L.cles_local_group_create.argtypes = [C.POINTER(C.c_int), C.c_double, C.POINTER(vp)]
+        L.cles_local_group_destroy.argtypes = [vp]
+        L.cles_local_group_destroy.restype = None
+        L.cles_local_group_exchange.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(abi.cles_exchange)]
+        L.cles_local_group_abort.argtypes = [vp]
+        L.cles_local_group_abort.restype = None
         L.cles_solver_destroy.argtypes = [vp]
         L.cles_solver_info_get.argtypes = [vp, C.POINTER(abi.cles_solver_info)]
         L.cles_set_state.argtypes = [vp, vp, C.c_int]
@@ -283,15 +291,31 @@ def apply_along(out, plan, f):
 
 # ----------------------------------------------------------------- solver ----
 class Solver:
-    """Device-resident Solver (src/rhs.jl:17-72) built from a cles_solver_desc."""
+    """Device-resident Solver (src/rhs.jl:17-72) built from a cles_solver_desc.
 
-    def __init__(self, desc, ctx=None):
+    With `decomp` (a decomp.Decomp or an abi.cles_decomp) and `exchange` (an
+    object whose `.struct` is an abi.cles_exchange, e.g. decomp.LocalGroup's
+    or decomp.TorchExchange's), the solver is one rank of a decomposed grid:
+    `desc` describes the global problem and states, fields and checkpoints are
+    this rank's block."""
+
+    def __init__(self, desc, ctx=None, decomp=None, exchange=None):
         self.ctx = ctx or default_context()
         self.desc = desc
         self.ptr = C.c_void_p()
-        _check(lib().cles_solver_create(self.ctx.ptr, C.byref(desc), C.byref(self.ptr)))
+        if decomp is None:
+            _check(lib().cles_solver_create(self.ctx.ptr, C.byref(desc), C.byref(self.ptr)))
+        else:
+            if exchange is None:
+                raise ValueError("a decomposed solver needs an exchange")
+            dc = decomp.struct() if hasattr(decomp, "struct") else decomp
+            self._exchange = exchange   # the callbacks must outlive the solver
+            _check(lib().cles_solver_create_decomposed(self.ctx.ptr, C.byref(desc), C.byref(dc),
+                                                       C.byref(exchange.struct), C.byref(self.ptr)))
         self.n_cons = desc.n_species + 4
         self.h = grid_spacing(desc)
+        inf = self.info()
+        self.n_local = tuple(int(v) for v in inf.n_local)
         # DirichletBC(fun) / NSCBCInflowBC(target=fun) faces, called back at the stage times
         self._face_cbs, self.face_errors = face_callbacks(desc)
         for k, s, which, cb in self._face_cbs:
@@ -310,8 +334,17 @@ class Solver:
         _check(lib().cles_solver_info_get(self.ptr, C.byref(i)))
         return i
 
+    def state_shape(self, layout=abi.CLES_LAYOUT_PADDED):
+        """Host state shape (component, z, y, x) of this solver's block."""
+        sh = []
+        for k in (2, 1, 0):
+            n = self.n_local[k]
+            pad = self.desc.n_halo if (self.desc.n_global[k] > 1 and layout == abi.CLES_LAYOUT_PADDED) else 0
+            sh.append(n + 2 * pad)
+        return (self.n_cons,) + tuple(sh)
+
     def _arr(self, layout, ncomp=None):
-        sh = state_shape(self.desc, layout)
+        sh = self.state_shape(layout)
         if ncomp is not None:
             sh = (ncomp,) + sh[1:]
         return np.zeros(sh)
@@ -323,8 +356,8 @@ class Solver:
     def set_state(self, Q, layout="padded"):
         Q = np.ascontiguousarray(Q, dtype=np.float64)
         lay = self._layout(layout)
-        if Q.shape != state_shape(self.desc, lay):
-            raise ValueError(f"state shape {Q.shape} != {state_shape(self.desc, lay)}")
+        if Q.shape != self.state_shape(lay):
+            raise ValueError(f"state shape {Q.shape} != {self.state_shape(lay)}")
         _check(lib().cles_set_state(self.ptr, Q.ctypes.data_as(C.c_void_p), lay))
 
     def get_state(self, layout="padded"):
@@ -379,7 +412,8 @@ class Solver:
         return bool(out.value)
 
     def save_checkpoint(self, prefix):
-        """save_checkpoint(solver, Q, prefix) (src/io.jl:8-41): writes prefix.r0000.ckpt."""
+        """save_checkpoint(solver, Q, prefix) (src/io.jl:8-41): writes prefix.rNNNN.ckpt
+        (NNNN: the decomposition's rank, 0000 on one rank)."""
         _check(lib().cles_checkpoint_save(self.ptr, str(prefix).encode()))
         return str(prefix)
 

@@ -547,6 +547,23 @@ int cles_solver_create(cles_ctx* ctx, const cles_solver_desc* desc, cles_solver*
     API_END
 }
 
+int cles_solver_create_decomposed(cles_ctx* ctx, const cles_solver_desc* desc, const cles_decomp* decomp,
+                                  const cles_exchange* ex, cles_solver** out) {
+    API_BEGIN
+    if (!ctx || !desc || !decomp || !ex || !out) throw Error(CLES_EINVAL, "null argument");
+    CLES_CUDA(cudaSetDevice(ctx->device));
+    auto* s = new cles_solver();
+    s->ctx = ctx;
+    try {
+        s->s = make_solver(ctx, *desc, decomp, ex);
+    } catch (...) {
+        delete s;
+        throw;
+    }
+    *out = s;
+    API_END
+}
+
 void cles_solver_destroy(cles_solver* s) {
     if (!s) return;
     cudaSetDevice(s->ctx->device);
@@ -615,7 +632,16 @@ int cles_solver_bc_switched(const cles_solver* s, int dim, int side, int* switch
 namespace {
 constexpr uint64_t kCkptMagic = 0x434c4553434b5054ull;   // "CLES CKPT" (src/io.jl:6)
 
-std::string ckpt_name(const char* prefix) { return std::string(prefix) + ".r0000.ckpt"; }
+// _ckpt_name (src/io.jl:8-9): prefix.rNNNN.ckpt with the communicator rank
+std::string ckpt_name(const char* prefix, int rank) {
+    char num[16];
+    std::snprintf(num, sizeof(num), "%04d", rank);
+    return std::string(prefix) + ".r" + num + ".ckpt";
+}
+int ckpt_rank(const cles_solver* s) {
+    const cles_decomp* dc = s->s->decomposition();
+    return dc ? dc->rank : 0;
+}
 
 struct FileCloser {
     FILE* f;
@@ -631,15 +657,16 @@ int cles_checkpoint_save(cles_solver* s, const char* prefix) {
     const size_t n = (size_t)I.cells * I.n_cons;
     std::vector<double> buf(n);
     s->s->get_state(buf.data(), CLES_LAYOUT_INTERIOR);
-    const std::string path = ckpt_name(prefix);
+    const std::string path = ckpt_name(prefix, ckpt_rank(s));
     FileCloser fc{std::fopen(path.c_str(), "wb")};
     if (!fc.f) throw Error(CLES_EINVAL, "cannot open " + path + " for writing");
     int64_t hdr[10];
     hdr[0] = I.n_cons;
+    const cles_decomp* dc = s->s->decomposition();
     for (int d = 0; d < 3; ++d) {
         hdr[1 + d] = s->s->desc.n_global[d];
-        hdr[4 + d] = s->s->desc.n_global[d];   // one rank owns the whole grid
-        hdr[7 + d] = 0;                         // its coordinates in the process grid
+        hdr[4 + d] = I.n_local[d];              // this rank's block
+        hdr[7 + d] = dc ? dc->coords[d] : 0;    // its coordinates in the process grid
     }
     const double t = s->s->t;
     const int64_t step = s->s->step_count;
@@ -655,7 +682,7 @@ int cles_checkpoint_load(cles_solver* s, const char* prefix) {
     if (!s || !prefix) throw Error(CLES_EINVAL, "null argument");
     CLES_CUDA(cudaSetDevice(s->ctx->device));
     const cles_solver_info I = s->s->info();
-    const std::string path = ckpt_name(prefix);
+    const std::string path = ckpt_name(prefix, ckpt_rank(s));
     FileCloser fc{std::fopen(path.c_str(), "rb")};
     if (!fc.f) throw Error(CLES_EINVAL, "cannot open " + path);
     uint64_t magic = 0;
@@ -666,10 +693,11 @@ int cles_checkpoint_load(cles_solver* s, const char* prefix) {
     if (hdr[0] != I.n_cons) throw Error(CLES_EINVAL, "conserved layout mismatch");
     for (int d = 0; d < 3; ++d)
         if (hdr[1 + d] != s->s->desc.n_global[d]) throw Error(CLES_EINVAL, "global grid mismatch");
+    const cles_decomp* dc = s->s->decomposition();
     for (int d = 0; d < 3; ++d)
-        if (hdr[4 + d] != s->s->desc.n_global[d]) throw Error(CLES_EINVAL, "decomposition mismatch");
+        if (hdr[4 + d] != I.n_local[d]) throw Error(CLES_EINVAL, "decomposition mismatch");
     for (int d = 0; d < 3; ++d)
-        if (hdr[7 + d] != 0) throw Error(CLES_EINVAL, "rank layout mismatch");
+        if (hdr[7 + d] != (dc ? dc->coords[d] : 0)) throw Error(CLES_EINVAL, "rank layout mismatch");
     double t = 0.0;
     int64_t step = 0;
     const size_t n = (size_t)I.cells * I.n_cons;

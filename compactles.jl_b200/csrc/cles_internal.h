@@ -207,15 +207,36 @@ struct SplitPlan {
 };
 void build_split_plan(SplitPlan& sp, const cles_scheme& s, const int n3_local[3], int dim, bool periodic,
                       int n_global, int ranks, int rank, double h, int dtype);
-// Copies the M planes next to each end of the local interior into lo / hi
+// The M planes at each end of a local interior along `dim` (lines: the
+// product of the other two extents, lower dimension fastest).
+struct HaloSpec {
+    int dim = 0;
+    int n3[3] = {0, 0, 0};
+    int M = 0;
+    int64_t lines = 0;
+    bool lo_open = false, hi_open = false;
+};
+HaloSpec halo_spec(const SplitPlan& sp);
+// Copies the M planes next to each open end of the local interior into lo / hi
 // ([count][M][lines]) when pack, or those buffers into the halo planes
 // beyond each open end when !pack.
+void halo_planes(const HaloSpec& hs, const FieldView& f, void* lo, void* hi, int count, bool pack, int dtype,
+                 cudaStream_t st);
 void split_halo(const SplitPlan& sp, const FieldView& f, void* lo, void* hi, int count, bool pack, cudaStream_t st);
 // From every rank's heads and tails ([ranks][count][2q][lines]): the 2q
 // neighbouring unknowns per line into zbuf ([count][2q][lines]), then
 // out -= V z_prev + W z_next over the local interior.
 void split_correct(const SplitPlan& sp, const void* gathered, void* zbuf, const FieldView& out, int count,
                    cudaStream_t st);
+// The same with the local solution read from `loc` and the corrected value
+// r = loc - V z_prev - W z_next written to `out` by mode: OUT_STORE out = r,
+// OUT_NEGATE out = -r, OUT_SUBTRACT out -= r (loc may alias out except for
+// OUT_SUBTRACT).
+void split_correct(const SplitPlan& sp, const void* gathered, void* zbuf, const FieldView& loc, const FieldView& out,
+                   int count, int mode, cudaStream_t st);
+// dst = src over an n3 interior of `count` fields (views of equal extents,
+// any strides).
+void copy_view(const FieldView& src, const FieldView& dst, const int n3[3], int count, int dtype, cudaStream_t st);
 
 // ---- batched line solves over many grids (batch_compact.cu) ----------------
 // One grid's directional plan in a batched launch.  Its lines are cut into

@@ -337,6 +337,58 @@ __global__ void __launch_bounds__(kTX * kTY) k_delta4_tiled(const F* __restrict_
     delta4_tile<F, NF>(f0, f1, o0, o1, g, w0, w1, blockIdx.x * kTX, blockIdx.y * kTY, blockIdx.z * kZC, tile);
 }
 
+// delta4_sum! of one or two fields on a rank's block of a decomposed grid
+// (src/artificial.jl:67-94 after exchange_halos!): the same sums in the same
+// order as k_delta4, with the neighbours beyond an open end of a split
+// dimension read from the exchanged planes.
+template <typename F, int NF>
+__global__ void k_delta4_halo(const F* __restrict__ f0, const F* __restrict__ f1, F* __restrict__ o0,
+                              F* __restrict__ o1, Grid3 g, Weights3 w0, Weights3 w1, Halo4 h) {
+    const int64_t cells = (int64_t)g.n[0] * g.n[1] * g.n[2];
+    const double D4[5] = {1.0, -4.0, 6.0, -4.0, 1.0};
+    const int64_t st[3] = {1, (int64_t)g.n[0], (int64_t)g.n[0] * g.n[1]};
+    const F* fs[2] = {f0, f1};
+    F* os[2] = {o0, o1};
+    const Weights3 ws[2] = {w0, w1};
+    GRID_STRIDE(I, cells) {
+        const int i = (int)(I % g.n[0]);
+        const int j = (int)((I / g.n[0]) % g.n[1]);
+        const int k = (int)(I / ((int64_t)g.n[0] * g.n[1]));
+        const int ijk[3] = {i, j, k};
+        // line index and line count of each dimension (split_halo's numbering)
+        const int64_t line[3] = {j + (int64_t)k * g.n[1], i + (int64_t)k * g.n[0], i + (int64_t)j * g.n[0]};
+        const int64_t lines[3] = {(int64_t)g.n[1] * g.n[2], (int64_t)g.n[0] * g.n[2], (int64_t)g.n[0] * g.n[1]};
+#pragma unroll
+        for (int f = 0; f < NF; ++f) {
+            double o = 0.0;
+            for (int d = 0; d < 3; ++d) {
+                if (!g.active[d]) continue;
+                const int nd = g.n[d];
+                const int il = ijk[d];
+                double acc = 0.0;
+#pragma unroll
+                for (int m = -2; m <= 2; ++m) {
+                    const int ilm = il + m;
+                    double v;
+                    if (ilm < 0 && h.open_lo[d]) {
+                        v = double(static_cast<const F*>(h.lo[d])[(int64_t)(2 * f + ilm + 2) * lines[d] + line[d]]);
+                    } else if (ilm >= nd && h.open_hi[d]) {
+                        v = double(static_cast<const F*>(h.hi[d])[(int64_t)(2 * f + ilm - nd) * lines[d] + line[d]]);
+                    } else {
+                        int e = ilm;
+                        if (g.periodic[d]) e = e < 0 ? e + nd : (e >= nd ? e - nd : e);
+                        else e = e < 0 ? 0 : (e >= nd ? nd - 1 : e);
+                        v = double(fs[f][I + (int64_t)(e - il) * st[d]]);
+                    }
+                    acc += D4[m + 2] * v;
+                }
+                o += ws[f].w[d] * fabs(acc);
+            }
+            os[f][I] = F(o);
+        }
+    }
+}
+
 // Ducros switch (src/artificial.jl:134-147)
 __device__ __forceinline__ double compression_switch(const double* gv) {
     const double div = gv[0] + gv[4] + gv[8];
@@ -1123,6 +1175,18 @@ void Pointwise<F>::delta4_tiled(const F* f0, const F* f1, F* o0, F* o1, const Gr
     }
     count_launch();
     check_launch("k_delta4_tiled");
+}
+template <typename F>
+void Pointwise<F>::delta4_halo(const F* f0, const F* f1, F* o0, F* o1, const Grid3& g, const double w0[3],
+                               const double w1[3], const Halo4& h, cudaStream_t st) {
+    const int64_t cells = (int64_t)g.n[0] * g.n[1] * g.n[2];
+    Weights3 a{{w0[0], w0[1], w0[2]}}, b{{0.0, 0.0, 0.0}};
+    if (f1) {
+        b = Weights3{{w1[0], w1[1], w1[2]}};
+        LAUNCH((k_delta4_halo<F, 2>), cells, st, f0, f1, o0, o1, g, a, b, h);
+    } else {
+        LAUNCH((k_delta4_halo<F, 1>), cells, st, f0, nullptr, o0, nullptr, g, a, b, h);
+    }
 }
 template <typename F>
 void Pointwise<F>::art_coef(const F* s_strain, const F* s_energy, const F* prim, const F* g, F* art, int64_t cells,

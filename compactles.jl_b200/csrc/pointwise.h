@@ -46,6 +46,17 @@ struct Weights3 {
     double w[3];
 };
 
+// Neighbours of a decomposed grid for delta4_sum!: along a split dimension d
+// the two planes beyond an open end (a rank interface) come from lo[d] /
+// hi[d], laid out [field][plane][line] (plane 0 nearest the low end, line the
+// other two indices with the lower dimension fastest).  Elements of the
+// field's type.
+struct Halo4 {
+    const void* lo[3];
+    const void* hi[3];
+    int open_lo[3], open_hi[3];
+};
+
 // State of one enforced face condition: the Dirichlet state, or the wall
 // energy of an isothermal no-slip wall, rho e = (sum_k Q_k ew_k) * Twall for an
 // ideal mixture (ew_k = cv_k) or sum_k Q_k e_k(Twall) for NASA-9 (ew_k = e_k(Twall)).
@@ -101,6 +112,10 @@ struct Pointwise {
     // delta4_sum! of one (f1 == nullptr) or two fields in one tiled pass
     static void delta4_tiled(const F* f0, const F* f1, F* o0, F* o1, const Grid3& g, const double w0[3],
                              const double w1[3], cudaStream_t st);
+    // the same on a rank's block of a decomposed grid: g.periodic is 0 along
+    // split dimensions, whose open ends read the exchanged planes of h
+    static void delta4_halo(const F* f0, const F* f1, F* o0, F* o1, const Grid3& g, const double w0[3],
+                            const double w1[3], const Halo4& h, cudaStream_t st);
     static void art_coef(const F* s_strain, const F* s_energy, const F* prim, const F* g, F* art, int64_t cells,
                          double C_mu, double C_beta, double C_kappa, int gate, cudaStream_t st);
     static void strain(const F* g, F* out, int64_t cells, cudaStream_t st);

@@ -72,7 +72,9 @@ inline double jmin(double x, double y) {
 template <typename F>
 class Solver final : public SolverBase {
 public:
-    Solver(cles_ctx* ctx, const cles_solver_desc& d) : ctx_(ctx) {
+    Solver(cles_ctx* ctx, const cles_solver_desc& d, const cles_decomp* dc = nullptr,
+           const cles_exchange* ex = nullptr)
+        : ctx_(ctx) {
         desc = d;
         st_ = ctx->stream;
         for (int k = 0; k < 3; ++k) {
@@ -100,6 +102,7 @@ public:
             pad_[k] = g_.active[k] ? d.n_halo : 0;
             h_[k] = !g_.active[k] ? 1.0 : (g_.periodic[k] ? d.L[k] / d.n_global[k] : d.L[k] / (d.n_global[k] - 1));
         }
+        if (dc) decompose(d, *dc, ex);
         if (d.n_species < 1 || d.n_species > CLES_MAX_SPECIES) throw Error(CLES_EINVAL, "bad species count");
         if (d.beta_sensor < 0 || d.beta_sensor > 2) throw Error(CLES_EINVAL, "unknown beta sensor");
         if (d.n_body_forces < 0 || d.n_body_forces > CLES_MAX_BODY_FORCES)
@@ -116,9 +119,14 @@ public:
         cells_ = (int64_t)g_.n[0] * g_.n[1] * g_.n[2];
         cfl = d.cfl;
         setup_geometry(d);
+        if (decomposed_) check_decomposable(d);
         const int dt = sizeof(F) == 8 ? CLES_F64 : CLES_F32;
         for (int k = 0; k < 3; ++k) {
             if (!g_.active[k]) continue;
+            if (split_[k].on) {
+                build_split_plans(d, k, dt);
+                continue;
+            }
             // a folded dim carries one plan per field parity (src/rhs.jl:256-261)
             const int nt = fold_[k].on ? 2 : 1;
             for (int t = 0; t < nt; ++t) {
@@ -179,11 +187,205 @@ public:
         CLES_CUDA(cudaMemsetAsync(scratch_.p, 0, scratch_.bytes, st_));
         CLES_CUDA(cudaMemsetAsync(flux_.p, 0, flux_.bytes, st_));
         if (d.control.retries > 0) save_.alloc(ctx, sizeof(double) * c * ncons_);
+        if (decomposed_) alloc_split_buffers();
         if (geo_) build_geometry_tables(d);
         // the Stretch samples are read at create time only (kept in stretch_x_)
         for (int k = 0; k < 3; ++k) desc.stretch_x[k] = desc.stretch_dxdxi[k] = nullptr;
         CLES_CUDA(cudaStreamSynchronize(st_));
     }
+
+    ~Solver() override {
+        graph_free();
+        if (cap_st_) cudaStreamDestroy(cap_st_);
+        if (host_res_) cudaFreeHost(host_res_);
+        if (host_clk_) cudaFreeHost(host_clk_);
+    }
+
+    // ------------------------------------------------------ decomposition --
+    // Decomp(n_global, periodic; dims) on this rank (src/decomposition.jl:80-122):
+    // the local extents and offsets by local_range, before any plan is built.
+    void decompose(const cles_solver_desc& d, const cles_decomp& dc, const cles_exchange* ex) {
+        if (!ex || !ex->halo || !ex->gather || !ex->allreduce)
+            throw Error(CLES_EINVAL, "a decomposed solver needs halo, gather and allreduce callbacks");
+        ex_ = *ex;
+        dc_ = dc;
+        for (int k = 0; k < 3; ++k) {
+            if (dc.dims[k] < 1) throw Error(CLES_EINVAL, "process grid dims must be >= 1");
+            if (!g_.active[k] && dc.dims[k] != 1)
+                throw Error(CLES_EINVAL, "collapsed dimensions must not be decomposed: dims=(" +
+                                             std::to_string(dc.dims[0]) + ", " + std::to_string(dc.dims[1]) + ", " +
+                                             std::to_string(dc.dims[2]) + ")");
+            if (dc.coords[k] < 0 || dc.coords[k] >= dc.dims[k])
+                throw Error(CLES_EINVAL, "rank coordinates must lie in [0, dims)");
+            const int N = d.n_global[k], P = dc.dims[k], r = dc.coords[k];
+            const int base = N / P, rem = N % P;
+            g_.n[k] = base + (r < rem ? 1 : 0);
+            off_[k] = r * base + std::min(r, rem);
+            if (g_.n[k] < 1) throw Error(CLES_EINVAL, "a rank's local extent is empty");
+            split_[k].on = P > 1;
+            if (split_[k].on) decomposed_ = true;
+        }
+        // a process grid of one rank is the ordinary solver
+    }
+
+    void check_decomposable(const cles_solver_desc& d) {
+        if (geo_)
+            throw Error(CLES_EINVAL, "a decomposed solver needs a uniform Cartesian grid (no metric, stretching or folds)");
+        for (int k = 0; k < 3; ++k) {
+            if (!split_[k].on) continue;
+            for (int s = 0; s < 2; ++s)
+                for (int w = 0; w < 2; ++w) {
+                    const int bc = w == 0 ? d.bc[k][s] : (d.bc_switchable[k][s] ? d.bc_after[k][s] : -1);
+                    if (bc == CLES_BC_NSCBC_OUTFLOW || bc == CLES_BC_NSCBC_INFLOW)
+                        throw Error(CLES_EINVAL, "characteristic (NSCBC) faces on a decomposed dimension are not "
+                                                 "supported");
+                }
+        }
+    }
+
+    // LineSolver / BandLineSolver with P > 1 (src/tridiag.jl:85-170,
+    // src/banded.jl:108-214) for the derivative and the filter along a split
+    // dim; their local plans stand in the plan sets.
+    void build_split_plans(const cles_solver_desc& d, int k, int dt) {
+        Split& S = split_[k];
+        const bool per = g_.periodic[k] != 0;
+        S.deriv.reset(new SplitPlan());
+        build_split_plan(*S.deriv, d.deriv, g_.n, k, per, d.n_global[k], dc_.dims[k], dc_.coords[k], h_[k], dt);
+        S.filt.reset(new SplitPlan());
+        build_split_plan(*S.filt, d.filt, g_.n, k, per, d.n_global[k], dc_.dims[k], dc_.coords[k], h_[k], dt);
+        if (dt != CLES_F64) {
+            S.qfilt.reset(new SplitPlan());
+            build_split_plan(*S.qfilt, d.filt, g_.n, k, per, d.n_global[k], dc_.dims[k], dc_.coords[k], h_[k],
+                             CLES_F64);
+        }
+        dset_[k][0] = &S.deriv->local;
+        fset_[k][0] = &S.filt->local;
+        qset_[k][0] = S.qfilt ? &S.qfilt->local : &S.filt->local;
+        S.lines = S.deriv->lines;
+        S.prev = S.deriv->prev;
+        S.next = S.deriv->next;
+        S.lo_open = S.deriv->lo_open;
+        S.hi_open = S.deriv->hi_open;
+        hpad_ = std::max({hpad_, S.deriv->M, S.filt->M, 2});
+    }
+
+    // Padded copy of the fields of one split application and the exchange
+    // buffers of every split dim (8-byte elements: the FP64 state filter).
+    void alloc_split_buffers() {
+        int64_t padded = 0;
+        for (int k = 0; k < 3; ++k) {
+            Split& S = split_[k];
+            if (!S.on) continue;
+            padded = std::max(padded, cells_ / g_.n[k] * (g_.n[k] + 2 * hpad_));
+            const size_t halo = sizeof(double) * (size_t)ncons_ * hpad_ * (size_t)S.lines;
+            const size_t iface = sizeof(double) * (size_t)ncons_ * 2 * CLES_MAX_Q * (size_t)S.lines;
+            S.send_lo.alloc(ctx_, halo);
+            S.send_hi.alloc(ctx_, halo);
+            S.recv_lo.alloc(ctx_, halo);
+            S.recv_hi.alloc(ctx_, halo);
+            S.iface.alloc(ctx_, iface);
+            S.zbuf.alloc(ctx_, iface);
+            S.iface_all.alloc(ctx_, iface * (size_t)dc_.dims[k]);
+        }
+        padbuf_.alloc(ctx_, sizeof(double) * (size_t)ncons_ * (size_t)padded);
+    }
+
+    // The fields of one application along split dim k, with hpad_ halo planes
+    // beyond each end of the dim (element size esz).
+    FieldView padded_view(int k, size_t esz) const {
+        int np[3] = {g_.n[0], g_.n[1], g_.n[2]};
+        np[k] += 2 * hpad_;
+        const int64_t sy = np[0], sz = (int64_t)np[0] * np[1];
+        const int64_t lead = (int64_t)hpad_ * (k == 0 ? 1 : k == 1 ? sy : sz);
+        return FieldView{static_cast<char*>(padbuf_.p) + esz * (size_t)lead, sz * np[2], sy, sz};
+    }
+
+    void exchange_halo(int k, int64_t bytes) {
+        Split& S = split_[k];
+        if (ex_.halo(ex_.user, k, S.prev, S.next, S.send_lo.p, S.send_hi.p, S.recv_lo.p, S.recv_hi.p, bytes,
+                     reinterpret_cast<void*>(st_)) != 0)
+            throw Error(CLES_EXCHANGE, "halo exchange along dim " + std::to_string(k + 1) + " failed");
+    }
+
+    void allreduce(int op, double* v, int n) {
+        if (ex_.allreduce(ex_.user, op, v, n) != 0) throw Error(CLES_EXCHANGE, "allreduce failed");
+    }
+
+    // apply_along! on split dim k (src/operators.jl:118-131 with P > 1 ranks):
+    // the fields are copied into the padded buffer, the M planes next to each
+    // rank interface are exchanged into its halo, the local solve with open
+    // ends writes `loc` and every line's heads and tails, which are gathered
+    // along the dim; the correction then writes `out` by mode (OUT_STORE,
+    // OUT_NEGATE, or OUT_SUBTRACT with loc distinct from out).
+    void split_apply(const SplitPlan& P, int k, const void* in, void* loc, void* out, int count, int mode) {
+        Split& S = split_[k];
+        const size_t esz = P.dtype == CLES_F64 ? sizeof(double) : sizeof(float);
+        if (count > ncons_) throw Error(CLES_EINVAL, "internal: too many fields for a split application");
+        const FieldView vin = view(const_cast<void*>(in));
+        const FieldView pv = padded_view(k, esz);
+        copy_view(vin, pv, g_.n, count, P.dtype, st_);
+        split_halo(P, vin, S.send_lo.p, S.send_hi.p, count, true, st_);
+        exchange_halo(k, (int64_t)(esz * (size_t)count * P.M * (size_t)P.lines));
+        split_halo(P, pv, S.recv_lo.p, S.recv_hi.p, count, false, st_);
+        launch_compact_split(P.local, pv, view(loc), count, S.iface.p, st_);
+        const int64_t ib = (int64_t)(esz * (size_t)count * 2 * P.q * (size_t)P.lines);
+        if (ex_.gather(ex_.user, k, S.iface.p, S.iface_all.p, ib, reinterpret_cast<void*>(st_)) != 0)
+            throw Error(CLES_EXCHANGE, "interface gather along dim " + std::to_string(k + 1) + " failed");
+        split_correct(P, S.iface_all.p, S.zbuf.p, view(loc), view(out), count, mode, st_);
+    }
+
+    const SplitPlan& split_plan_of(const CompactPlan* const* ps, int k) const {
+        const Split& S = split_[k];
+        if (ps == dset_[k]) return *S.deriv;
+        if (ps == fset_[k]) return *S.filt;
+        if (ps == qset_[k]) return S.qfilt ? *S.qfilt : *S.filt;
+        throw Error(CLES_EINVAL, "internal: no split plan for this operator");
+    }
+
+    // delta4_sum! of one or two fields (src/artificial.jl:67-94); on a
+    // decomposed grid the two planes beyond each rank interface of every split
+    // dim are exchanged first (the reference's exchange_halos! before it).
+    void delta4(const F* f0, const F* f1, F* o0, F* o1, const double w0[3], const double w1[3]) {
+        if (!decomposed_) {
+            Pointwise<F>::delta4_tiled(f0, f1, o0, o1, g_, w0, w1, st_);
+            return;
+        }
+        Halo4 h{};
+        Grid3 gl = g_;
+        const int dt = sizeof(F) == 8 ? CLES_F64 : CLES_F32;
+        for (int k = 0; k < 3; ++k) {
+            Split& S = split_[k];
+            if (!S.on) continue;
+            gl.periodic[k] = 0;
+            HaloSpec hs;
+            hs.dim = k;
+            for (int e = 0; e < 3; ++e) hs.n3[e] = g_.n[e];
+            hs.M = 2;
+            hs.lines = S.lines;
+            hs.lo_open = S.lo_open;
+            hs.hi_open = S.hi_open;
+            const size_t fb = sizeof(F) * 2 * (size_t)S.lines;
+            halo_planes(hs, view(const_cast<F*>(f0)), S.send_lo.p, S.send_hi.p, 1, true, dt, st_);
+            if (f1)
+                halo_planes(hs, view(const_cast<F*>(f1)), static_cast<char*>(S.send_lo.p) + fb,
+                            static_cast<char*>(S.send_hi.p) + fb, 1, true, dt, st_);
+            exchange_halo(k, (int64_t)(fb * (f1 ? 2 : 1)));
+            h.lo[k] = S.recv_lo.p;
+            h.hi[k] = S.recv_hi.p;
+            h.open_lo[k] = S.lo_open ? 1 : 0;
+            h.open_hi[k] = S.hi_open ? 1 : 0;
+        }
+        Pointwise<F>::delta4_halo(f0, f1, o0, o1, gl, w0, w1, h, st_);
+    }
+
+    // at_lo_edge / at_hi_edge (src/decomposition.jl:137-140): the faces of a
+    // split dim belong to the first and the last rank along it
+    bool owns_face(int k, int s) const {
+        if (!split_[k].on) return true;
+        return s == 0 ? dc_.coords[k] == 0 : dc_.coords[k] == dc_.dims[k] - 1;
+    }
+
+    const cles_decomp* decomposition() const override { return decomposed_ ? &dc_ : nullptr; }
 
     // ----------------------------------------------------------- geometry --
     static bool is_fold_bc(int bc) { return bc == CLES_BC_AXIS || bc == CLES_BC_ORIGIN || bc == CLES_BC_POLE; }
@@ -393,6 +595,12 @@ public:
         auto at = [&](const void* base, int c) {
             return reinterpret_cast<void*>(const_cast<char*>(static_cast<const char*>(base)) + esz * (size_t)cells_ * c);
         };
+        if (split_[k].on) {
+            if (mode != OUT_STORE && mode != OUT_NEGATE)
+                throw Error(CLES_EINVAL, "internal: a split application stores or negates");
+            split_apply(split_plan_of(ps, k), k, in, out, out, count, mode);
+            return;
+        }
         const Fold& f = fold_[k];
         if (!f.on) {
             launch_compact(*ps[0], view(const_cast<void*>(in)), view(out), count, mode, st_);
@@ -501,7 +709,7 @@ public:
                 c[o1] = (int)(t % g_.n[o1]);
                 c[o2] = (int)(t / g_.n[o1]);
                 c[k] = s == 0 ? 0 : g_.n[k] - 1;
-                for (int e = 0; e < 3; ++e) f.x[e][(size_t)t] = node_coord(e, c[e]);
+                for (int e = 0; e < 3; ++e) f.x[e][(size_t)t] = node_coord(e, off_[e] + c[e]);
             }
         }
     }
@@ -552,6 +760,7 @@ public:
                 const int bc = face_kind(k, s);
                 if (bc == CLES_BC_PERIODIC || bc == CLES_BC_NSCBC_OUTFLOW || bc == CLES_BC_NSCBC_INFLOW) continue;
                 if (is_fold_bc(bc)) continue;   // enforce! is a no-op on folds (src/boundary.jl:173-175)
+                if (!owns_face(k, s)) continue;
                 BcState bs;
                 std::memset(&bs, 0, sizeof(bs));
                 const double* q = face_state(k, s);
@@ -631,19 +840,19 @@ public:
         const double w2[3] = {h_[0] * h_[0], h_[1] * h_[1], h_[2] * h_[2]};
         const double w1[3] = {h_[0], h_[1], h_[2]};
         PW::strain(g_u_.as<F>(), strain, cells_, st_);
-        PW::delta4_tiled(strain, prim(P_Y0 + Ns_), sensor, sensor_e, g_, w2, w1, st_);
+        delta4(strain, prim(P_Y0 + Ns_), sensor, sensor_e, w2, w1);
         smooth(sensor, 2);
         PW::art_coef(sensor, sensor_e, prim_.as<F>(), g_u_.as<F>(), art_.as<F>(), cells_, desc.C_mu, desc.C_beta,
                      desc.C_kappa, desc.beta_sensor == CLES_BETA_GATED_STRAIN, st_);
         if (desc.beta_sensor == CLES_BETA_DILATATION) {
             PW::dilatation(g_u_.as<F>(), tmp_a, tmp_b, cells_, st_);
-            PW::delta4_tiled(tmp_a, nullptr, sensor, nullptr, g_, w2, w2, st_);
+            delta4(tmp_a, nullptr, sensor, nullptr, w2, w2);
             smooth(sensor, 1);
             PW::beta_dilatation(sensor, prim_.as<F>(), tmp_b, art_.as<F>(), cells_, desc.C_beta, st_);
         }
         if (Ns_ > 1) {
             for (int sp = 0; sp < Ns_; ++sp) {
-                PW::delta4_tiled(prim(P_Y0 + sp), nullptr, tmp_a, nullptr, g_, w1, w1, st_);
+                delta4(prim(P_Y0 + sp), nullptr, tmp_a, nullptr, w1, w1);
                 smooth(tmp_a, 1);
                 PW::dart(tmp_a, prim_.as<F>(), art_.as<F>(), cells_, desc.C_D, sp, st_);
             }
@@ -691,17 +900,34 @@ public:
         // With all three dims active the order is y, x, z: the first direction only
         // stores (no read of dQ), the x kernel reads dQ with vector loads, and z,
         // last, carries the RK update.  The sum differs from x, y, z by rounding.
+        // On a decomposed grid the split dims come first, each corrected
+        // straight into dQ (negated or subtracted) from its local solution
+        // written over its own flux block; the last unsplit dim may carry the
+        // RK update.
         int order[3] = {0, 1, 2};
-        if (g_.active[0] && g_.active[1] && g_.active[2]) { order[0] = 1; order[1] = 0; }
+        if (decomposed_) {
+            int no = 0;
+            for (int k = 0; k < 3; ++k)
+                if (split_[k].on) order[no++] = k;
+            for (int k = 0; k < 3; ++k)
+                if (!split_[k].on) order[no++] = k;
+        } else if (g_.active[0] && g_.active[1] && g_.active[2]) {
+            order[0] = 1;
+            order[1] = 0;
+        }
         int last = -1;
-        for (int k = 0; k < 3; ++k)
-            if (g_.active[k]) last = k;
+        for (int o = 0; o < 3; ++o)
+            if (g_.active[order[o]]) last = order[o];
         bool first = true, fused = false;
         for (int o = 0; o < 3; ++o) {
             const int k = order[o];
             if (!g_.active[k]) continue;
-            const FieldView fin = view(flux_.as<F>() + (size_t)cells_ * ncons_ * k);
-            if (k == last && !first && rk && launch_compact_rk(*dset_[k][0], fin, view(dQ_.as<F>()), ncons_, *rk, st_)) {
+            F* fk = flux_.as<F>() + (size_t)cells_ * ncons_ * k;
+            const FieldView fin = view(fk);
+            if (split_[k].on) {
+                split_apply(*split_[k].deriv, k, fk, fk, dQ_.p, ncons_, first ? OUT_NEGATE : OUT_SUBTRACT);
+            } else if (k == last && !first && rk &&
+                       launch_compact_rk(*dset_[k][0], fin, view(dQ_.as<F>()), ncons_, *rk, st_)) {
                 fused = true;
             } else {
                 launch_compact(*dset_[k][0], fin, view(dQ_.as<F>()), ncons_, first ? OUT_NEGATE : OUT_SUBTRACT, st_);
@@ -773,6 +999,13 @@ public:
             throw Error(CLES_ETIMEOUT, "a bounded device wait expired in a compact-operator kernel");
         *rate = host_res_[0];
         *rho_min = host_res_[1];
+        if (decomposed_) {
+            // one collective: both reduced with max by negating the density (src/timestep.jl:170-173)
+            double v[2] = {*rate, -*rho_min};
+            allreduce(CLES_REDUCE_MAX, v, 2);
+            *rate = v[0];
+            *rho_min = -v[1];
+        }
     }
 
     void filter_state() override {
@@ -927,7 +1160,9 @@ public:
             cellvol *= g_.active[k] ? h_[k] : 1.0;
             vol *= g_.active[k] ? desc.L[k] : 1.0;
         }
-        return host_res_[0] * cellvol / vol;
+        double sum = host_res_[0];
+        if (decomposed_) allreduce(CLES_REDUCE_SUM, &sum, 1);
+        return sum * cellvol / vol;
     }
 
     double dissipation_rate() override {
@@ -946,7 +1181,9 @@ public:
                         st_, geo_ ? &G_ : nullptr, foldmask);
         CLES_CUDA(cudaMemcpyAsync(host_res_, res_.p, 2 * sizeof(double), cudaMemcpyDeviceToHost, st_));
         CLES_CUDA(cudaStreamSynchronize(st_));
-        return host_res_[0] / host_res_[1];
+        double v[2] = {host_res_[0], host_res_[1]};
+        if (decomposed_) allreduce(CLES_REDUCE_SUM, v, 2);
+        return v[0] / v[1];
     }
 
     double* state_device() override { return Q_.as<double>(); }
@@ -1002,6 +1239,7 @@ public:
     }
 
     void graph_begin(double tfinal, int64_t nmax) override {
+        if (decomposed_) throw Error(CLES_EINVAL, "graph mode does not run a decomposed solver (its exchanges are host calls)");
         for (int k = 0; k < 3; ++k)
             for (int s = 0; s < 2; ++s)
                 for (int w = 0; w < 2; ++w)
@@ -1106,6 +1344,22 @@ private:
     cudaGraphExec_t gexec_filter_ = nullptr, gexec_plain_ = nullptr;
     cudaStream_t cap_st_ = nullptr;
     bool switched_[3][2] = {{false, false}, {false, false}, {false, false}};
+    // decomposition: this rank's offsets, the split dims' plans and buffers
+    struct Split {
+        bool on = false;
+        std::unique_ptr<SplitPlan> deriv, filt, qfilt;
+        int64_t lines = 0;
+        int prev = -1, next = -1;
+        bool lo_open = false, hi_open = false;
+        DevBuf send_lo, send_hi, recv_lo, recv_hi, iface, iface_all, zbuf;
+    };
+    bool decomposed_ = false;
+    cles_decomp dc_{};
+    cles_exchange ex_{};
+    int off_[3] = {0, 0, 0};
+    int hpad_ = 0;
+    Split split_[3];
+    DevBuf padbuf_;
 };
 
 }  // namespace
@@ -1218,10 +1472,11 @@ int run_graph(SolverBase& s, double tfinal, int64_t nmax, cles_run_result* res) 
     return failure == CLES_FAIL_NONE ? CLES_OK : CLES_EFAILURE;
 }
 
-std::unique_ptr<SolverBase> make_solver(cles_ctx* ctx, const cles_solver_desc& desc) {
-    if (desc.precision == CLES_PREC_MIXED) return std::unique_ptr<SolverBase>(new Solver<float>(ctx, desc));
+std::unique_ptr<SolverBase> make_solver(cles_ctx* ctx, const cles_solver_desc& desc, const cles_decomp* dc,
+                                        const cles_exchange* ex) {
+    if (desc.precision == CLES_PREC_MIXED) return std::unique_ptr<SolverBase>(new Solver<float>(ctx, desc, dc, ex));
     if (desc.precision != CLES_PREC_FP64) throw Error(CLES_EINVAL, "unknown precision mode");
-    return std::unique_ptr<SolverBase>(new Solver<double>(ctx, desc));
+    return std::unique_ptr<SolverBase>(new Solver<double>(ctx, desc, dc, ex));
 }
 
 namespace {

@@ -63,13 +63,16 @@ public:
     virtual void switch_bc(int dim, int side) = 0;
     virtual void set_face_fn(int dim, int side, int which, cles_face_fn fn, void* user) = 0;
     virtual bool bc_switched(int dim, int side) const = 0;
+    // this rank's place in a decomposition (nullptr on an undecomposed solver)
+    virtual const cles_decomp* decomposition() const { return nullptr; }
 
     cles_solver_desc desc{};
     double t = 0.0, tstage = 0.0, dt_prev = 0.0, rate_prev = 0.0, cfl = 0.5;
     int64_t step_count = 0;
 };
 
-std::unique_ptr<SolverBase> make_solver(cles_ctx* ctx, const cles_solver_desc& desc);
+std::unique_ptr<SolverBase> make_solver(cles_ctx* ctx, const cles_solver_desc& desc,
+                                        const cles_decomp* decomp = nullptr, const cles_exchange* ex = nullptr);
 // Device bytes a solver of `desc` allocates (fields and plan tables), for admission control.
 size_t solver_bytes_estimate(const cles_solver_desc& desc);
 // run! in graph mode on one solver (same contract as SolverBase::run without retries).

@@ -121,14 +121,14 @@ __device__ __forceinline__ void correct_coeffs(const T* __restrict__ V, const T*
     zl = zc + line;
 }
 
-template <typename T, int Q>
-__global__ void k_split_correct(T* __restrict__ out, FieldView v, const T* __restrict__ V, const T* __restrict__ W,
-                                const T* __restrict__ z, int dim, int nx, int ny, int nz, int n, int lines,
-                                int count) {
+template <typename T, int Q, int MODE>
+__global__ void k_split_correct(const T* __restrict__ loc, FieldView lv, T* __restrict__ out, FieldView v,
+                                const T* __restrict__ V, const T* __restrict__ W, const T* __restrict__ z, int dim,
+                                int nx, int ny, int nz, int n, int lines, int count) {
     const int rows = ny * nz * count;
     for (int r0 = blockIdx.x * RB; r0 < rows; r0 += gridDim.x * RB) {
         for (int i = threadIdx.x; i < nx; i += blockDim.x) {
-            T o[RB], acc[RB];
+            T o[RB], acc[RB], prev[RB];
             T* po[RB];
 #pragma unroll
             for (int b = 0; b < RB; ++b) {
@@ -139,7 +139,8 @@ __global__ void k_split_correct(T* __restrict__ out, FieldView v, const T* __res
                     const int j = row % ny, kc = row / ny;
                     const int k = kc % nz, comp = kc / nz;
                     po[b] = out + (int64_t)comp * v.comp_stride + j * v.sy + k * v.sz + i;
-                    o[b] = *po[b];
+                    o[b] = loc[(int64_t)comp * lv.comp_stride + j * lv.sy + k * lv.sz + i];
+                    if (MODE == OUT_SUBTRACT) prev[b] = *po[b];
                     T vg[Q], wg[Q];
                     const T* zl;
                     correct_coeffs<T, Q>(V, W, z, dim, nx, ny, nz, n, lines, row, i, vg, wg, zl);
@@ -148,26 +149,83 @@ __global__ void k_split_correct(T* __restrict__ out, FieldView v, const T* __res
                 }
             }
 #pragma unroll
-            for (int b = 0; b < RB; ++b)
-                if (po[b]) *po[b] = o[b] - acc[b];
+            for (int b = 0; b < RB; ++b) {
+                if (!po[b]) continue;
+                const T r = o[b] - acc[b];
+                if (MODE == OUT_NEGATE) *po[b] = -r;
+                else if (MODE == OUT_SUBTRACT) *po[b] = prev[b] - r;
+                else *po[b] = r;
+            }
         }
     }
 }
 
+// dst = src over the interior of two views of one grid shape (rows of x
+// points, a block per RB rows as in the correction).
 template <typename T>
-void halo_t(const SplitPlan& sp, const FieldView& f, void* lo, void* hi, int count, bool pack, cudaStream_t st) {
-    const int64_t total = (int64_t)count * sp.M * sp.lines;
+__global__ void k_copy_view(const T* __restrict__ src, FieldView sv, T* __restrict__ dst, FieldView dv, int nx,
+                            int ny, int nz, int count) {
+    const int rows = ny * nz * count;
+    for (int r0 = blockIdx.x * RB; r0 < rows; r0 += gridDim.x * RB) {
+        for (int i = threadIdx.x; i < nx; i += blockDim.x) {
+            T val[RB];
+#pragma unroll
+            for (int b = 0; b < RB; ++b) {
+                const int row = r0 + b;
+                if (row < rows) {
+                    const int j = row % ny, kc = row / ny;
+                    const int k = kc % nz, comp = kc / nz;
+                    val[b] = src[(int64_t)comp * sv.comp_stride + j * sv.sy + k * sv.sz + i];
+                }
+            }
+#pragma unroll
+            for (int b = 0; b < RB; ++b) {
+                const int row = r0 + b;
+                if (row < rows) {
+                    const int j = row % ny, kc = row / ny;
+                    const int k = kc % nz, comp = kc / nz;
+                    dst[(int64_t)comp * dv.comp_stride + j * dv.sy + k * dv.sz + i] = val[b];
+                }
+            }
+        }
+    }
+}
+
+inline void row_launch(int nx, int64_t rows, unsigned* nb, int* bt) {
+    // a block per x row (threads cover up to 256 x points per step)
+    *bt = nx >= 256 ? 256 : ((nx + 31) / 32) * 32;
+    *nb = (unsigned)std::min<int64_t>((rows + RB - 1) / RB, 148 * 64);
+}
+
+template <typename T>
+void halo_t(const HaloSpec& hs, const FieldView& f, void* lo, void* hi, int count, bool pack, cudaStream_t st) {
+    const int64_t total = (int64_t)count * hs.M * hs.lines;
     k_split_halo<T><<<grid_for(total), kThreads, 0, st>>>(static_cast<T*>(f.base), f, static_cast<T*>(lo),
-                                                          static_cast<T*>(hi), sp.dim, sp.n3[0], sp.n3[1], sp.n,
-                                                          sp.M, (int)sp.lines, count, sp.lo_open ? 1 : 0,
-                                                          sp.hi_open ? 1 : 0, pack ? 1 : 0);
+                                                          static_cast<T*>(hi), hs.dim, hs.n3[0], hs.n3[1],
+                                                          hs.n3[hs.dim], hs.M, (int)hs.lines, count,
+                                                          hs.lo_open ? 1 : 0, hs.hi_open ? 1 : 0, pack ? 1 : 0);
     count_launch();
     check_launch("k_split_halo");
 }
 
+template <typename T, int Q>
+void correct_mode(int mode, unsigned nb, int bt, cudaStream_t st, const T* loc, const FieldView& lv, T* out,
+                  const FieldView& v, const T* V, const T* W, const T* z, const SplitPlan& sp, int count) {
+    const int nx = sp.n3[0], ny = sp.n3[1], nz = sp.n3[2], lines = (int)sp.lines;
+    if (mode == OUT_NEGATE)
+        k_split_correct<T, Q, OUT_NEGATE><<<nb, bt, 0, st>>>(loc, lv, out, v, V, W, z, sp.dim, nx, ny, nz, sp.n, lines,
+                                                            count);
+    else if (mode == OUT_SUBTRACT)
+        k_split_correct<T, Q, OUT_SUBTRACT><<<nb, bt, 0, st>>>(loc, lv, out, v, V, W, z, sp.dim, nx, ny, nz, sp.n,
+                                                              lines, count);
+    else
+        k_split_correct<T, Q, OUT_STORE><<<nb, bt, 0, st>>>(loc, lv, out, v, V, W, z, sp.dim, nx, ny, nz, sp.n, lines,
+                                                           count);
+}
+
 template <typename T>
-void correct_t(const SplitPlan& sp, const void* gathered, void* zbuf, const FieldView& out, int count,
-               cudaStream_t st) {
+void correct_t(const SplitPlan& sp, const void* gathered, void* zbuf, const FieldView& loc, const FieldView& out,
+               int count, int mode, cudaStream_t st) {
     const T* tab = static_cast<const T*>(sp.tab);
     const int64_t nv = (int64_t)sp.q * sp.n;
     const T* V = tab;
@@ -180,32 +238,75 @@ void correct_t(const SplitPlan& sp, const void* gathered, void* zbuf, const Fiel
     check_launch("k_split_reduce");
     const int64_t rows = (int64_t)sp.n3[1] * sp.n3[2] * count;
     if (rows >= ((int64_t)1 << 31)) throw Error(CLES_EINVAL, "too many rows for one correction launch");
-    // a block per x row (threads cover up to 256 x points per step)
-    const int bt = sp.n3[0] >= 256 ? 256 : ((sp.n3[0] + 31) / 32) * 32;
-    const unsigned nb = (unsigned)std::min<int64_t>((rows + RB - 1) / RB, 148 * 64);
-    if (sp.q == 1)
-        k_split_correct<T, 1><<<nb, bt, 0, st>>>(static_cast<T*>(out.base), out, V, W, static_cast<const T*>(zbuf),
-                                                 sp.dim, sp.n3[0], sp.n3[1], sp.n3[2], sp.n, (int)sp.lines, count);
-    else
-        k_split_correct<T, 2><<<nb, bt, 0, st>>>(static_cast<T*>(out.base), out, V, W, static_cast<const T*>(zbuf),
-                                                 sp.dim, sp.n3[0], sp.n3[1], sp.n3[2], sp.n, (int)sp.lines, count);
+    unsigned nb;
+    int bt;
+    row_launch(sp.n3[0], rows, &nb, &bt);
+    const T* lp = static_cast<const T*>(loc.base);
+    T* op = static_cast<T*>(out.base);
+    const T* z = static_cast<const T*>(zbuf);
+    if (sp.q == 1) correct_mode<T, 1>(mode, nb, bt, st, lp, loc, op, out, V, W, z, sp, count);
+    else correct_mode<T, 2>(mode, nb, bt, st, lp, loc, op, out, V, W, z, sp, count);
     count_launch();
     check_launch("k_split_correct");
 }
 
 }  // namespace
 
+HaloSpec halo_spec(const SplitPlan& sp) {
+    HaloSpec h;
+    h.dim = sp.dim;
+    for (int k = 0; k < 3; ++k) h.n3[k] = sp.n3[k];
+    h.M = sp.M;
+    h.lines = sp.lines;
+    h.lo_open = sp.lo_open;
+    h.hi_open = sp.hi_open;
+    return h;
+}
+
+void halo_planes(const HaloSpec& hs, const FieldView& f, void* lo, void* hi, int count, bool pack, int dtype,
+                 cudaStream_t st) {
+    if (count <= 0 || hs.lines == 0 || (!hs.lo_open && !hs.hi_open)) return;
+    if (dtype == CLES_F64) halo_t<double>(hs, f, lo, hi, count, pack, st);
+    else halo_t<float>(hs, f, lo, hi, count, pack, st);
+}
+
 void split_halo(const SplitPlan& sp, const FieldView& f, void* lo, void* hi, int count, bool pack, cudaStream_t st) {
-    if (count <= 0 || sp.lines == 0 || (!sp.lo_open && !sp.hi_open)) return;
-    if (sp.dtype == CLES_F64) halo_t<double>(sp, f, lo, hi, count, pack, st);
-    else halo_t<float>(sp, f, lo, hi, count, pack, st);
+    halo_planes(halo_spec(sp), f, lo, hi, count, pack, sp.dtype, st);
+}
+
+void split_correct(const SplitPlan& sp, const void* gathered, void* zbuf, const FieldView& loc, const FieldView& out,
+                   int count, int mode, cudaStream_t st) {
+    if (count <= 0 || sp.lines == 0) return;
+    if (!sp.lo_open && !sp.hi_open) {
+        // one closed piece: the local solution is the answer
+        if (mode == OUT_STORE && loc.base == out.base) return;
+        throw Error(CLES_EINVAL, "internal: a closed piece has no correction to apply");
+    }
+    if (sp.dtype == CLES_F64) correct_t<double>(sp, gathered, zbuf, loc, out, count, mode, st);
+    else correct_t<float>(sp, gathered, zbuf, loc, out, count, mode, st);
 }
 
 void split_correct(const SplitPlan& sp, const void* gathered, void* zbuf, const FieldView& out, int count,
                    cudaStream_t st) {
     if (count <= 0 || sp.lines == 0 || (!sp.lo_open && !sp.hi_open)) return;
-    if (sp.dtype == CLES_F64) correct_t<double>(sp, gathered, zbuf, out, count, st);
-    else correct_t<float>(sp, gathered, zbuf, out, count, st);
+    split_correct(sp, gathered, zbuf, out, out, count, OUT_STORE, st);
+}
+
+void copy_view(const FieldView& src, const FieldView& dst, const int n3[3], int count, int dtype, cudaStream_t st) {
+    const int64_t rows = (int64_t)n3[1] * n3[2] * count;
+    if (rows == 0 || n3[0] == 0) return;
+    if (rows >= ((int64_t)1 << 31)) throw Error(CLES_EINVAL, "too many rows for one copy launch");
+    unsigned nb;
+    int bt;
+    row_launch(n3[0], rows, &nb, &bt);
+    if (dtype == CLES_F64)
+        k_copy_view<double><<<nb, bt, 0, st>>>(static_cast<const double*>(src.base), src,
+                                               static_cast<double*>(dst.base), dst, n3[0], n3[1], n3[2], count);
+    else
+        k_copy_view<float><<<nb, bt, 0, st>>>(static_cast<const float*>(src.base), src, static_cast<float*>(dst.base),
+                                              dst, n3[0], n3[1], n3[2], count);
+    count_launch();
+    check_launch("k_copy_view");
 }
 
 }  // namespace cles

@@ -46,6 +46,7 @@ extern "C" {
 #define CLES_ETIMEOUT  4   /* a bounded device wait expired */
 #define CLES_ECUDA     5   /* a CUDA runtime call failed */
 #define CLES_EFAILURE  6   /* run! raised SolverFailure (src/stepcontrol.jl:145-152) */
+#define CLES_EXCHANGE  7   /* a decomposed solver's exchange callback failed */
 
 /* ---- fixed maxima of the descriptors ----------------------------------- */
 #define CLES_MAX_Q        2   /* LHS half-bandwidth (1 tridiagonal, 2 pentadiagonal) */
@@ -362,6 +363,79 @@ typedef struct cles_solver_info {
 int  cles_solver_create(cles_ctx* ctx, const cles_solver_desc* desc, cles_solver** out);
 void cles_solver_destroy(cles_solver* s);
 int  cles_solver_info_get(const cles_solver* s, cles_solver_info* out);
+
+/* ---- one rank of a decomposed grid (Decomp, src/decomposition.jl:80-140) --
+ * The process grid splits each active dimension d into dims[d] pieces by
+ * local_range (src/decomposition.jl:73-78); this rank owns the block at
+ * `coords`.  `rank` is its number in the communicator (checkpoint file
+ * names, src/io.jl:8).  Collapsed dimensions are not split. */
+typedef struct cles_decomp {
+    int dims[3];
+    int coords[3];
+    int rank;
+} cles_decomp;
+
+enum { CLES_REDUCE_MAX = 0, CLES_REDUCE_SUM = 1 };
+
+/* The three points where the reference calls MPI, as host callbacks (one
+ * process per GPU: NCCL through torch.distributed, or MPI.jl from Julia).
+ * Each returns 0 on success; a non-zero return fails the solver call with
+ * CLES_EXCHANGE.  Every rank makes the same calls in the same order.
+ *
+ * halo: Sendrecv! with both neighbours along dimension `dim` (0-based,
+ *   src/halo.jl:143-194): recv_lo <- the previous rank's send_hi, recv_hi <-
+ *   the next rank's send_lo.  prev / next are the neighbours' coordinates
+ *   along dim (-1 at a closed end; equal to this rank's coordinate when it is
+ *   its own periodic neighbour).  `bytes` per buffer.
+ * gather: Allgather! over the ranks along dim in coordinate order
+ *   (src/tridiag.jl:148, src/banded.jl:190): `all` receives dims[dim] blocks
+ *   of `bytes`, block r from the rank at coordinate r.
+ * allreduce: Allreduce! over every rank of `count` host doubles in place
+ *   (CLES_REDUCE_MAX: max_rate, src/timestep.jl:173; CLES_REDUCE_SUM: the
+ *   volume integrals of the diagnostics).
+ *
+ * Buffers of halo and gather are device memory.  On entry the sends are
+ * complete in the order of `stream` (the solver's stream); on return the
+ * receives must be complete in that order (NCCL on `stream`, or a stream
+ * synchronisation around host-driven copies). */
+typedef struct cles_exchange {
+    void* user;
+    int (*halo)(void* user, int dim, int prev, int next, const void* send_lo, const void* send_hi, void* recv_lo,
+                void* recv_hi, int64_t bytes, void* stream);
+    int (*gather)(void* user, int dim, const void* local, void* all, int64_t bytes, void* stream);
+    int (*allreduce)(void* user, int op, double* vals, int count);
+} cles_exchange;
+
+/* Replaces Solver(...) on a Decomp with several ranks: `desc` describes the
+ * GLOBAL problem (n_global, L, faces); the solver holds this rank's block.
+ * Compact applications along a split dimension run the P > 1 line solve
+ * (local solve with open ends, interface gather, reduced solve, correction:
+ * src/tridiag.jl:136-170, src/banded.jl:177-214), delta4_sum! reads the
+ * exchanged planes beyond each rank interface, boundary conditions act only
+ * on the faces this rank owns (at_lo_edge / at_hi_edge), and max_rate
+ * reduces (rate, -rho_min) with max over every rank.  States, fields and
+ * checkpoints are this rank's block (n_local of cles_solver_info).
+ * Supported: uniform Cartesian grids (no metric, stretching or folds), no
+ * characteristic (NSCBC) faces on a split dimension; host-stepped run!
+ * (cles_run_graph refuses a decomposed solver).  `ex` is copied. */
+int  cles_solver_create_decomposed(cles_ctx* ctx, const cles_solver_desc* desc, const cles_decomp* decomp,
+                                   const cles_exchange* ex, cles_solver** out);
+
+/* An in-process exchange among the prod(dims) ranks of one process, one host
+ * thread per rank (several GPUs driven from one process, or several ranks on
+ * one GPU for a decomposition test).  Each call synchronises the caller's
+ * stream, meets the other ranks at a host barrier, copies from their buffers
+ * with cudaMemcpyAsync on the caller's stream, synchronises again and meets
+ * them once more; the device never waits on another rank.  A barrier that
+ * is not met within `timeout_s` seconds (or after cles_local_group_abort)
+ * fails the call. */
+typedef struct cles_local_group cles_local_group;
+int  cles_local_group_create(const int dims[3], double timeout_s, cles_local_group** out);
+void cles_local_group_destroy(cles_local_group* g);
+/* The exchange of the rank at `coords` (valid while the group lives). */
+int  cles_local_group_exchange(cles_local_group* g, const int coords[3], cles_exchange* out);
+/* Fail every pending and future barrier of the group (a rank that stopped). */
+void cles_local_group_abort(cles_local_group* g);
 
 /* Conserved state in and out (host arrays, layout CLES_LAYOUT_PADDED or
  * _INTERIOR, Float64, component slowest).  Output writes the interior only. */

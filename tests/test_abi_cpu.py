@@ -34,18 +34,20 @@ def test_library_loads_and_exports_every_declared_symbol():
 def test_struct_layout_matches_the_c_header(tmp_path):
     src = tmp_path / "sz.c"
     src.write_text('#include <stdio.h>\n#include <stddef.h>\n#include "cles.h"\n'
-                   "int main(void){printf(\"%zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu\\n\","
+                   "int main(void){printf(\"%zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu\\n\","
                    "sizeof(cles_scheme), sizeof(cles_grid), sizeof(cles_step_control), sizeof(cles_solver_desc),"
                    "sizeof(cles_solver_info), sizeof(cles_run_result), offsetof(cles_solver_desc, deriv),"
                    "offsetof(cles_solver_desc, precision), sizeof(cles_split_desc), sizeof(cles_split_info),"
-                   "offsetof(cles_split_info, prev));return 0;}\n")
+                   "offsetof(cles_split_info, prev), sizeof(cles_decomp), offsetof(cles_decomp, rank),"
+                   "sizeof(cles_exchange), offsetof(cles_exchange, allreduce));return 0;}\n")
     exe = tmp_path / "sz"
     subprocess.run(["gcc", "-I", str(HEADER.parent), str(src), "-o", str(exe)], check=True)
     got = list(map(int, subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()))
     want = [C.sizeof(abi.cles_scheme), C.sizeof(abi.cles_grid), C.sizeof(abi.cles_step_control),
             C.sizeof(abi.cles_solver_desc), C.sizeof(abi.cles_solver_info), C.sizeof(abi.cles_run_result),
             abi.cles_solver_desc.deriv.offset, abi.cles_solver_desc.precision.offset, C.sizeof(abi.cles_split_desc),
-            C.sizeof(abi.cles_split_info), abi.cles_split_info.prev.offset]
+            C.sizeof(abi.cles_split_info), abi.cles_split_info.prev.offset, C.sizeof(abi.cles_decomp),
+            abi.cles_decomp.rank.offset, C.sizeof(abi.cles_exchange), abi.cles_exchange.allreduce.offset]
     assert got == want
 
 
