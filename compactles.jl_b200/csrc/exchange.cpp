@@ -1,14 +1,16 @@
 // In-process exchange among the ranks of a decomposed grid (cles_local_group_*).
 //
 // Every rank is one host thread of this process with its own solver and
-// stream (on one GPU or several).  An exchange synchronises the caller's
-// stream, so its sends are complete, publishes the caller's buffers, meets the
-// other ranks at a host barrier, copies what it receives from their buffers
-// with cudaMemcpyAsync on its own stream, synchronises again and meets them a
-// second time, after which every rank may reuse its buffers.  Kernels never
-// wait on another rank: all waiting is on the host, bounded by the group's
-// timeout, after which (or after cles_local_group_abort) every barrier of the
-// group fails and the callers return CLES_EXCHANGE.
+// stream (on one GPU or several).  An exchange records a "sends ready" event
+// on the caller's stream and publishes it with the caller's buffers; after a
+// host barrier each rank's stream waits on its peers' ready events and copies
+// what it receives with cudaMemcpyAsync, then records a "copied" event; after
+// a second barrier each stream waits on the copied events of the peers that
+// read its buffers, so nothing later on it overwrites them too early.  The
+// host never waits for the device here, and no kernel waits on another rank:
+// the ordering is stream-event dependencies.  The barriers are bounded by the
+// group's timeout, after which (or after cles_local_group_abort) every
+// barrier of the group fails and the callers return CLES_EXCHANGE.
 
 #include <cuda_runtime.h>
 
@@ -26,6 +28,7 @@ namespace {
 struct Post {
     const void* a = nullptr;   // halo: send_lo; gather: the local block
     const void* b = nullptr;   // halo: send_hi
+    cudaEvent_t ready = nullptr, copied = nullptr;
     double vals[8] = {0};
     int count = 0;
 };
@@ -34,6 +37,7 @@ struct Endpoint {
     cles_local_group* g = nullptr;
     int rank = 0;
     int coords[3] = {0, 0, 0};
+    cudaEvent_t ready = nullptr, copied = nullptr;   // created on the caller's device at first use
 };
 
 }  // namespace
@@ -49,6 +53,13 @@ struct cles_local_group {
     bool aborted = false;
     std::vector<Post> post;
     std::vector<Endpoint> eps;
+
+    ~cles_local_group() {
+        for (Endpoint& e : eps) {
+            if (e.ready) cudaEventDestroy(e.ready);
+            if (e.copied) cudaEventDestroy(e.copied);
+        }
+    }
 
     int linear(const int c[3]) const { return c[0] + dims[0] * (c[1] + dims[1] * c[2]); }
 
@@ -85,29 +96,63 @@ int fail(cles_local_group* g) {
     return 1;
 }
 
+bool events(Endpoint* e) {
+    if (!e->ready && cudaEventCreateWithFlags(&e->ready, cudaEventDisableTiming) != cudaSuccess) return false;
+    if (!e->copied && cudaEventCreateWithFlags(&e->copied, cudaEventDisableTiming) != cudaSuccess) return false;
+    return true;
+}
+
+// first half: publish `a`, `b` with a ready event recorded on st
+bool publish(Endpoint* e, cudaStream_t st, const void* a, const void* b) {
+    cles_local_group* g = e->g;
+    if (!events(e) || cudaEventRecord(e->ready, st) != cudaSuccess) return false;
+    Post& me = g->post[e->rank];
+    me.a = a;
+    me.b = b;
+    me.ready = e->ready;
+    return true;
+}
+
+// after the copies from `peers`: record and publish the copied event, meet
+// everyone, then order st after the copies of the ranks that read from us
+bool finish(Endpoint* e, cudaStream_t st, const std::vector<int>& readers) {
+    cles_local_group* g = e->g;
+    if (cudaEventRecord(e->copied, st) != cudaSuccess) return false;
+    g->post[e->rank].copied = e->copied;
+    if (!g->barrier()) return false;
+    for (int r : readers)
+        if (r != e->rank && cudaStreamWaitEvent(st, g->post[r].copied, 0) != cudaSuccess) return false;
+    return true;
+}
+
 int lg_halo(void* user, int dim, int prev, int next, const void* send_lo, const void* send_hi, void* recv_lo,
             void* recv_hi, int64_t bytes, void* stream) {
     auto* e = static_cast<Endpoint*>(user);
     cles_local_group* g = e->g;
     const cudaStream_t st = static_cast<cudaStream_t>(stream);
     if (dim < 0 || dim > 2) return fail(g);
-    if (cudaStreamSynchronize(st) != cudaSuccess) return fail(g);
-    g->post[e->rank].a = send_lo;
-    g->post[e->rank].b = send_hi;
+    if (!publish(e, st, send_lo, send_hi)) return fail(g);
     if (!g->barrier()) return 1;
     bool ok = true;
     int c[3] = {e->coords[0], e->coords[1], e->coords[2]};
+    std::vector<int> readers;
     if (prev >= 0) {
         c[dim] = prev;
-        ok = ok && cudaMemcpyAsync(recv_lo, g->post[g->linear(c)].b, (size_t)bytes, cudaMemcpyDefault, st) == cudaSuccess;
+        const Post& p = g->post[g->linear(c)];
+        readers.push_back(g->linear(c));
+        ok = ok && (g->linear(c) == e->rank || cudaStreamWaitEvent(st, p.ready, 0) == cudaSuccess) &&
+             cudaMemcpyAsync(recv_lo, p.b, (size_t)bytes, cudaMemcpyDefault, st) == cudaSuccess;
     }
     if (next >= 0) {
         c[dim] = next;
-        ok = ok && cudaMemcpyAsync(recv_hi, g->post[g->linear(c)].a, (size_t)bytes, cudaMemcpyDefault, st) == cudaSuccess;
+        const Post& p = g->post[g->linear(c)];
+        readers.push_back(g->linear(c));
+        ok = ok && (g->linear(c) == e->rank || cudaStreamWaitEvent(st, p.ready, 0) == cudaSuccess) &&
+             cudaMemcpyAsync(recv_hi, p.a, (size_t)bytes, cudaMemcpyDefault, st) == cudaSuccess;
     }
-    ok = cudaStreamSynchronize(st) == cudaSuccess && ok;
-    if (!ok) return fail(g);
-    return g->barrier() ? 0 : 1;
+    // the neighbours that read our sends are the same two ranks
+    if (!ok || !finish(e, st, readers)) return fail(g);
+    return 0;
 }
 
 int lg_gather(void* user, int dim, const void* local, void* all, int64_t bytes, void* stream) {
@@ -115,19 +160,22 @@ int lg_gather(void* user, int dim, const void* local, void* all, int64_t bytes, 
     cles_local_group* g = e->g;
     const cudaStream_t st = static_cast<cudaStream_t>(stream);
     if (dim < 0 || dim > 2) return fail(g);
-    if (cudaStreamSynchronize(st) != cudaSuccess) return fail(g);
-    g->post[e->rank].a = local;
+    if (!publish(e, st, local, nullptr)) return fail(g);
     if (!g->barrier()) return 1;
     bool ok = true;
     int c[3] = {e->coords[0], e->coords[1], e->coords[2]};
+    std::vector<int> line;
     for (int r = 0; r < g->dims[dim]; ++r) {
         c[dim] = r;
-        ok = ok && cudaMemcpyAsync(static_cast<char*>(all) + (size_t)r * (size_t)bytes, g->post[g->linear(c)].a,
-                                   (size_t)bytes, cudaMemcpyDefault, st) == cudaSuccess;
+        const int src = g->linear(c);
+        line.push_back(src);
+        ok = ok && (src == e->rank || cudaStreamWaitEvent(st, g->post[src].ready, 0) == cudaSuccess) &&
+             cudaMemcpyAsync(static_cast<char*>(all) + (size_t)r * (size_t)bytes, g->post[src].a, (size_t)bytes,
+                             cudaMemcpyDefault, st) == cudaSuccess;
     }
-    ok = cudaStreamSynchronize(st) == cudaSuccess && ok;
-    if (!ok) return fail(g);
-    return g->barrier() ? 0 : 1;
+    // every rank of the line reads our block
+    if (!ok || !finish(e, st, line)) return fail(g);
+    return 0;
 }
 
 // Julia's max (NaN wins), as the reductions of max_rate see it

@@ -423,12 +423,14 @@ int  cles_solver_create_decomposed(cles_ctx* ctx, const cles_solver_desc* desc, 
 
 /* An in-process exchange among the prod(dims) ranks of one process, one host
  * thread per rank (several GPUs driven from one process, or several ranks on
- * one GPU for a decomposition test).  Each call synchronises the caller's
- * stream, meets the other ranks at a host barrier, copies from their buffers
- * with cudaMemcpyAsync on the caller's stream, synchronises again and meets
- * them once more; the device never waits on another rank.  A barrier that
- * is not met within `timeout_s` seconds (or after cles_local_group_abort)
- * fails the call. */
+ * one GPU for a decomposition test).  Each call records a "sends ready" event
+ * on the caller's stream, meets the other ranks at a host barrier, makes its
+ * stream wait on its peers' ready events and copies from their buffers with
+ * cudaMemcpyAsync, records a "copied" event, meets them again and makes its
+ * stream wait on the copied events of the ranks that read its buffers.  The
+ * host does not wait for the device, and no kernel waits on another rank
+ * (stream-event dependencies only).  A barrier that is not met within
+ * `timeout_s` seconds (or after cles_local_group_abort) fails the call. */
 typedef struct cles_local_group cles_local_group;
 int  cles_local_group_create(const int dims[3], double timeout_s, cles_local_group** out);
 void cles_local_group_destroy(cles_local_group* g);

@@ -162,7 +162,7 @@ def test_mixed_against_fp64_oracle(orc):
 
 
 def test_checkpoint_per_rank(tmp_path, orc):
-    dg, do, Q0 = _tgv(orc, 24)
+    dg, do, Q0 = _tgv(orc, 32)
     R = Ranks(dg, (1, 1, 2), Q0)
     R.each(lambda S: S.run(1e9, 3))
     before = R.state()
@@ -173,23 +173,32 @@ def test_checkpoint_per_rank(tmp_path, orc):
     R2.each(lambda S: S.load_checkpoint(prefix))
     np.testing.assert_array_equal(R2.state(), before)
     assert R2.solvers[1].steps == 3
-    # a rank cannot read another rank's block
-    R3 = Ranks(dg, (1, 1, 3), np.zeros_like(Q0))
-    with pytest.raises(cl.ClesError):
+    # a rank of another decomposition cannot read the block
+    R3 = Ranks(dg, (1, 2, 1), np.zeros_like(Q0))
+    with pytest.raises(cl.ClesError, match="decomposition mismatch"):
         R3.solvers[0].load_checkpoint(prefix)
 
 
 def test_refusals(orc):
-    dg, _, Q0 = _tgv(orc, 16)
+    dg, _, Q0 = _tgv(orc, 32)
     grp = cl.LocalGroup((1, 1, 2))
     d = dg
     d.n_global[2] = 1
     with pytest.raises(cl.ClesError, match="collapsed"):
         cl.Solver(d, decomp=cl.Decomp(d.n_global, (1, 1, 2), (0, 0, 0)), exchange=grp.exchange((0, 0, 0)))
-    dg, _, Q0 = _tgv(orc, 16)
+    dg, _, Q0 = _tgv(orc, 32)
     R = Ranks(dg, (1, 1, 2), Q0)
     with pytest.raises(cl.ClesError, match="graph mode"):
         R.solvers[0].run_graph(1.0, 1)
+
+
+def test_a_piece_below_the_scheme_minimum_is_refused(orc):
+    # src/operators.jl:50-53: every rank refuses a split whose smallest piece is too short
+    dg, _, Q0 = _tgv(orc, 16)
+    grp = cl.LocalGroup((1, 1, 2))
+    with pytest.raises(cl.ClesError, match="too small"):
+        cl.Solver(dg, decomp=cl.Decomp(dg.n_global, (1, 1, 2), (0, 0, 1)),
+                  exchange=grp.exchange((0, 0, 1)))
 
 
 def test_nscbc_on_a_split_dim_is_refused():
@@ -202,7 +211,7 @@ def test_nscbc_on_a_split_dim_is_refused():
 
 
 def test_a_stopped_rank_fails_the_exchange_instead_of_waiting(orc):
-    dg, _, Q0 = _tgv(orc, 16)
+    dg, _, Q0 = _tgv(orc, 32)
     R = Ranks(dg, (1, 1, 2), Q0, timeout_s=2.0)
     # rank 1 never joins: rank 0's first exchange gives up after the group's
     # timeout (host barrier), with nothing of rank 0 left waiting on the device
@@ -214,3 +223,22 @@ def test_a_stopped_rank_fails_the_exchange_instead_of_waiting(orc):
     S = cl.Solver(dg)
     S.set_state(Q0)
     S.run(1e9, 1)
+
+
+def test_tgv256_split_z_matches_undecomposed():
+    """At the benchmark's 256^3 (tile kernels on every split piece): 2 z-slabs
+    against the undecomposed solver, itself parity-tested against the oracle
+    at this size."""
+    sch = (cl.lele_d1_6(), cl.compact_filter(0.45))
+    dg, Q0, _ = scenarios.taylor_green_box(sch, 256, tfinal=1e9)
+    S = cl.Solver(dg)
+    S.set_state(Q0)
+    S.run(1e9, 2)
+    ref = S.get_state(layout="interior")
+    del S
+    torch.cuda.empty_cache()
+    R = Ranks(dg, (1, 1, 2), Q0)
+    R.each(lambda S: S.run(1e9, 2))
+    rel = _rel_l2(R.state(), ref)
+    parity.record("TGV 256^3 FP64 decomposed (1, 1, 2) 2 steps vs undecomposed", state_l2=rel)
+    assert rel < 1e-12, rel
