@@ -260,7 +260,7 @@ int cles_ctx_create(int device, void* stream, size_t budget, cles_ctx** out) {
     API_END
 }
 
-void cles_ctx_destroy(cles_ctx* ctx) { delete ctx; }
+void cles_ctx_destroy(cles_ctx* ctx) { ctx_release(ctx); }
 
 int cles_ctx_set_stream(cles_ctx* ctx, void* stream) {
     API_BEGIN
@@ -317,14 +317,17 @@ int cles_plan_create(cles_ctx* ctx, const cles_grid* grid, const cles_scheme* sc
         delete p;
         throw;
     }
+    ctx_retain(ctx);
     *out = p;
     API_END
 }
 
 void cles_plan_destroy(cles_plan* plan) {
     if (!plan) return;
-    cudaSetDevice(plan->ctx->device);
+    cles_ctx* c = plan->ctx;
+    cudaSetDevice(c->device);
     delete plan;
+    ctx_release(c);
 }
 
 static int apply_impl(cles_plan* plan, const void* f, void* out, int count, int64_t stride) {
@@ -399,14 +402,17 @@ int cles_split_plan_create(cles_ctx* ctx, const cles_split_desc* d, const cles_s
         delete p;
         throw;
     }
+    ctx_retain(ctx);
     *out = p;
     API_END
 }
 
 void cles_split_plan_destroy(cles_split_plan* plan) {
     if (!plan) return;
-    cudaSetDevice(plan->ctx->device);
+    cles_ctx* c = plan->ctx;
+    cudaSetDevice(c->device);
     delete plan;
+    ctx_release(c);
 }
 
 int cles_split_plan_info(const cles_split_plan* plan, cles_split_info* out) {
@@ -543,6 +549,7 @@ int cles_solver_create(cles_ctx* ctx, const cles_solver_desc* desc, cles_solver*
         delete s;
         throw;
     }
+    ctx_retain(ctx);
     *out = s;
     API_END
 }
@@ -560,14 +567,17 @@ int cles_solver_create_decomposed(cles_ctx* ctx, const cles_solver_desc* desc, c
         delete s;
         throw;
     }
+    ctx_retain(ctx);
     *out = s;
     API_END
 }
 
 void cles_solver_destroy(cles_solver* s) {
     if (!s) return;
-    cudaSetDevice(s->ctx->device);
+    cles_ctx* c = s->ctx;
+    cudaSetDevice(c->device);
     delete s;
+    ctx_release(c);
 }
 
 #define SOLVER_CALL(body)                                        \
@@ -791,14 +801,17 @@ int cles_batch_create(cles_ctx* ctx, const cles_solver_desc* cls, cles_batch** o
         delete b;
         throw;
     }
+    ctx_retain(ctx);
     *out = b;
     API_END
 }
 
 void cles_batch_destroy(cles_batch* b) {
     if (!b) return;
-    cudaSetDevice(b->ctx->device);
+    cles_ctx* c = b->ctx;
+    cudaSetDevice(c->device);
     delete b;
+    ctx_release(c);
 }
 
 int cles_batch_add(cles_batch* b, const cles_solver_desc* desc, const double* Q0, int layout, double tfinal,

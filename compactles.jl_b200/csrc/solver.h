@@ -2,6 +2,7 @@
 // Solver + compute_rhs! + step! + max_rate + filter_state! + run!).
 #pragma once
 
+#include <atomic>
 #include <memory>
 
 #include "pointwise.h"
@@ -11,7 +12,21 @@ struct cles_ctx {
     cudaStream_t stream = nullptr;
     size_t budget = 0;     // 0 = unlimited
     size_t allocated = 0;
+    // the caller's handle plus one per live plan, solver or batch made with
+    // it: cles_ctx_destroy only drops the caller's, so objects destroyed after
+    // their context (in any order) still find it
+    std::atomic<int> refs{1};
 };
+
+namespace cles {
+inline cles_ctx* ctx_retain(cles_ctx* c) {
+    c->refs.fetch_add(1);
+    return c;
+}
+inline void ctx_release(cles_ctx* c) {
+    if (c && c->refs.fetch_sub(1) == 1) delete c;
+}
+}  // namespace cles
 
 namespace cles {
 
