@@ -91,6 +91,14 @@ inline unsigned grid_for(int64_t n) {
         check_launch(#kern);                                           \
     } while (0)
 
+// opt a kernel in to `bytes` of dynamic shared memory (above the 48 KB
+// default) on the current device; a host call, set before every launch so
+// that every device and thread sees it
+template <typename K>
+void set_smem_attr(K kern, size_t bytes) {
+    CLES_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+}
+
 #define GRID_STRIDE(idx, n) for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < (n); idx += (int64_t)gridDim.x * blockDim.x)
 
 // _primitives!(::IdealMixture) (src/physics.jl:604-653) at the interior, and
@@ -257,12 +265,37 @@ __device__ __forceinline__ int edge_index(int i, int n, int periodic) {
     if (periodic) return i < 0 ? i + n : (i >= n ? i - n : i);
     return i < 0 ? 0 : (i >= n ? n - 1 : i);
 }
-// One block's tile (x0, y0, z0) of the tiled delta4_sum!.
+// One block's tile (x0, y0, z0) of the tiled delta4_sum!.  The halo'd xy
+// planes z0-2 .. z0+kZC+1 stream through a ring of kRing planes in shared
+// memory by cp.async (one commit group per plane, three planes in flight
+// while a plane is computed); the x and y differences read the plane, the z
+// difference the four ring neighbours along the column.
+constexpr int kRing = 8;
+constexpr int kPlane = (kTY + 4) * (kTX + 4);
+template <typename F, int NF>
+constexpr size_t delta4_smem() {
+    return sizeof(F) * (size_t)kRing * NF * kPlane;
+}
+__device__ __forceinline__ unsigned d4_smem_addr(const void* p) {
+    return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+template <typename F>
+__device__ __forceinline__ void d4_cp_async(F* dst, const F* src) {
+    if constexpr (sizeof(F) == 8)
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d4_smem_addr(dst)), "l"(src) : "memory");
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(d4_smem_addr(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void d4_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void d4_wait2() { asm volatile("cp.async.wait_group 2;" ::: "memory"); }
+
 template <typename F, int NF>
 __device__ __forceinline__ void delta4_tile(const F* __restrict__ f0, const F* __restrict__ f1, F* __restrict__ o0,
                                             F* __restrict__ o1, const Grid3& g, const Weights3& w0,
                                             const Weights3& w1, const int x0, const int y0, const int z0,
-                                            F (*tile)[kTY + 4][kTX + 4]) {
+                                            F* __restrict__ ring) {
+    constexpr int NT = kTX * kTY, TW = kTX + 4;
+    static_assert(kPlane <= 2 * NT, "two staging slots per thread");
     const F* fs[2] = {f0, f1};
     F* os[2] = {o0, o1};
     const Weights3 ws[2] = {w0, w1};
@@ -271,70 +304,87 @@ __device__ __forceinline__ void delta4_tile(const F* __restrict__ f0, const F* _
     const int tx = threadIdx.x % kTX, ty = threadIdx.x / kTX;
     const int x = x0 + tx, y = y0 + ty;
     const bool inside = x < nx && y < ny;
+    const bool zact = g.active[2] != 0;
     const double D4[5] = {1.0, -4.0, 6.0, -4.0, 1.0};
-    // z window of my column
-    F zw[NF][5];
-    if (g.active[2]) {
+    // this thread's two staging slots of a halo'd plane: ring offset and
+    // in-plane source offset (periodic wrap or clamping, as delta4_sum!)
+    int soff_s[2];
+    int64_t soff_g[2];
+    bool sv[2];
 #pragma unroll
-        for (int f = 0; f < NF; ++f)
-#pragma unroll
-            for (int q = 0; q < 4; ++q)
-                zw[f][q + 1] = inside ? fs[f][x + y * sy + edge_index(z0 - 2 + q, nz, g.periodic[2]) * sz] : F(0);
+    for (int s = 0; s < 2; ++s) {
+        const int idx = threadIdx.x + NT * s;
+        sv[s] = idx < kPlane;
+        const int hx = idx % TW, hy = idx / TW;
+        const int gx = g.active[0] ? edge_index(x0 - 2 + hx, nx, g.periodic[0]) : min(x0 - 2 + hx < 0 ? 0 : x0 - 2 + hx, nx - 1);
+        const int gy = g.active[1] ? edge_index(y0 - 2 + hy, ny, g.periodic[1]) : min(y0 - 2 + hy < 0 ? 0 : y0 - 2 + hy, ny - 1);
+        soff_s[s] = idx;
+        soff_g[s] = (int64_t)gx + (int64_t)gy * sy;
     }
     const int zend = min(z0 + kZC, nz);
+    // plane r of the block (r = 0 is z0 - 2) into ring slot r % kRing; planes
+    // past the last one any output reads are left out (empty group)
+    const int rlast = zact ? (zend - 1 + 2) - (z0 - 2) : 2;
+    auto issue = [&](int r) {
+        if (r <= rlast) {
+            const int zz = zact ? edge_index(z0 - 2 + r, nz, g.periodic[2]) : 0;
+            F* slot = ring + (size_t)(r % kRing) * NF * kPlane;
+#pragma unroll
+            for (int f = 0; f < NF; ++f)
+#pragma unroll
+                for (int s = 0; s < 2; ++s)
+                    if (sv[s]) d4_cp_async(slot + f * kPlane + soff_s[s], fs[f] + soff_g[s] + (int64_t)zz * sz);
+        }
+        d4_commit();
+    };
+    // planes 0 .. 6: the five the first output needs and two more in flight
+#pragma unroll
+    for (int r = 0; r < 7; ++r) issue(r);
     for (int z = z0; z < zend; ++z) {
-        // stage plane z with halos
-        for (int idx = threadIdx.x; idx < (kTX + 4) * (kTY + 4); idx += kTX * kTY) {
-            const int hx = idx % (kTX + 4), hy = idx / (kTX + 4);
-            const int gx = g.active[0] ? edge_index(x0 - 2 + hx, nx, g.periodic[0]) : min(x0 - 2 + hx < 0 ? 0 : x0 - 2 + hx, nx - 1);
-            const int gy = g.active[1] ? edge_index(y0 - 2 + hy, ny, g.periodic[1]) : min(y0 - 2 + hy < 0 ? 0 : y0 - 2 + hy, ny - 1);
-#pragma unroll
-            for (int f = 0; f < NF; ++f) tile[f][hy][hx] = fs[f][gx + gy * sy + (int64_t)z * sz];
-        }
-        if (g.active[2]) {
-#pragma unroll
-            for (int f = 0; f < NF; ++f) {
-#pragma unroll
-                for (int q = 0; q < 4; ++q) zw[f][q] = zw[f][q + 1];
-                zw[f][4] = inside ? fs[f][x + y * sy + edge_index(z + 2, nz, g.periodic[2]) * sz] : F(0);
-            }
-        }
-        __syncthreads();
+        const int rz = z - z0 + 2;
+        d4_wait2();         // this thread's copies of plane rz + 2 have landed
+        __syncthreads();    // everyone's, and plane rz - 3 is no longer read
+        issue(rz + 5);
         if (inside) {
+            const F* pl = ring + (size_t)(rz % kRing) * NF * kPlane;
 #pragma unroll
             for (int f = 0; f < NF; ++f) {
+                const F* t = pl + f * kPlane;
                 double o = 0.0;
                 if (g.active[0]) {
                     double acc = 0.0;
 #pragma unroll
-                    for (int m = 0; m < 5; ++m) acc += D4[m] * double(tile[f][ty + 2][tx + m]);
+                    for (int m = 0; m < 5; ++m) acc += D4[m] * double(t[(ty + 2) * TW + tx + m]);
                     o += ws[f].w[0] * fabs(acc);
                 }
                 if (g.active[1]) {
                     double acc = 0.0;
 #pragma unroll
-                    for (int m = 0; m < 5; ++m) acc += D4[m] * double(tile[f][ty + m][tx + 2]);
+                    for (int m = 0; m < 5; ++m) acc += D4[m] * double(t[(ty + m) * TW + tx + 2]);
                     o += ws[f].w[1] * fabs(acc);
                 }
-                if (g.active[2]) {
+                if (zact) {
                     double acc = 0.0;
 #pragma unroll
-                    for (int m = 0; m < 5; ++m) acc += D4[m] * double(zw[f][m]);
+                    for (int m = 0; m < 5; ++m)
+                        acc += D4[m] * double(ring[(size_t)((rz - 2 + m) % kRing) * NF * kPlane + f * kPlane +
+                                                   (ty + 2) * TW + tx + 2]);
                     o += ws[f].w[2] * fabs(acc);
                 }
                 os[f][x + y * sy + (int64_t)z * sz] = F(o);
             }
         }
-        __syncthreads();
     }
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
 }
 
 template <typename F, int NF>
 __global__ void __launch_bounds__(kTX * kTY) k_delta4_tiled(const F* __restrict__ f0, const F* __restrict__ f1,
                                                            F* __restrict__ o0, F* __restrict__ o1, Grid3 g,
                                                            Weights3 w0, Weights3 w1) {
-    __shared__ F tile[NF][kTY + 4][kTX + 4];
-    delta4_tile<F, NF>(f0, f1, o0, o1, g, w0, w1, blockIdx.x * kTX, blockIdx.y * kTY, blockIdx.z * kZC, tile);
+    extern __shared__ __align__(16) unsigned char d4_raw[];
+    delta4_tile<F, NF>(f0, f1, o0, o1, g, w0, w1, blockIdx.x * kTX, blockIdx.y * kTY, blockIdx.z * kZC,
+                       reinterpret_cast<F*>(d4_raw));
 }
 
 // delta4_sum! of one or two fields on a rank's block of a decomposed grid
@@ -1006,7 +1056,7 @@ __global__ void __launch_bounds__(kTX * kTY) k_delta4_batch(const F* __restrict_
                                                            F* __restrict__ o0, F* __restrict__ o1, int p0, int p1,
                                                            const BatchGrid* __restrict__ grids,
                                                            const BatchTile* __restrict__ tiles) {
-    __shared__ F tile[NF][kTY + 4][kTX + 4];
+    extern __shared__ __align__(16) unsigned char d4_raw[];
     const BatchTile t = tiles[blockIdx.x];
     const BatchGrid& G = grids[t.grid];
     Weights3 w0, w1;
@@ -1015,7 +1065,7 @@ __global__ void __launch_bounds__(kTX * kTY) k_delta4_batch(const F* __restrict_
         w1.w[d] = p1 == 2 ? G.h[d] * G.h[d] : G.h[d];
     }
     delta4_tile<F, NF>(f0 + G.off, f1 ? f1 + G.off : nullptr, o0 + G.off, o1 ? o1 + G.off : nullptr, G.g, w0, w1,
-                       t.x0, t.y0, t.z0, tile);
+                       t.x0, t.y0, t.z0, reinterpret_cast<F*>(d4_raw));
 }
 
 template <typename F>
@@ -1093,8 +1143,15 @@ template <typename F>
 void BatchOps<F>::delta4(const F* f0, const F* f1, F* o0, F* o1, int p0, int p1, const BatchGrid* grids,
                          const BatchTile* tiles, int ntiles, int64_t, cudaStream_t st) {
     if (ntiles <= 0) return;
-    if (f1) k_delta4_batch<F, 2><<<ntiles, kTX * kTY, 0, st>>>(f0, f1, o0, o1, p0, p1, grids, tiles);
-    else k_delta4_batch<F, 1><<<ntiles, kTX * kTY, 0, st>>>(f0, f1, o0, o1, p0, p1, grids, tiles);
+    if (f1) {
+        constexpr size_t sm = delta4_smem<F, 2>();
+        set_smem_attr(k_delta4_batch<F, 2>, sm);
+        k_delta4_batch<F, 2><<<ntiles, kTX * kTY, sm, st>>>(f0, f1, o0, o1, p0, p1, grids, tiles);
+    } else {
+        constexpr size_t sm = delta4_smem<F, 1>();
+        set_smem_attr(k_delta4_batch<F, 1>, sm);
+        k_delta4_batch<F, 1><<<ntiles, kTX * kTY, sm, st>>>(f0, f1, o0, o1, p0, p1, grids, tiles);
+    }
     count_launch();
     check_launch("k_delta4_batch");
 }
@@ -1169,9 +1226,13 @@ void Pointwise<F>::delta4_tiled(const F* f0, const F* f1, F* o0, F* o1, const Gr
     Weights3 a{{w0[0], w0[1], w0[2]}}, b{{0.0, 0.0, 0.0}};
     if (f1) {
         b = Weights3{{w1[0], w1[1], w1[2]}};
-        k_delta4_tiled<F, 2><<<grid, kTX * kTY, 0, st>>>(f0, f1, o0, o1, g, a, b);
+        constexpr size_t sm = delta4_smem<F, 2>();
+        set_smem_attr(k_delta4_tiled<F, 2>, sm);
+        k_delta4_tiled<F, 2><<<grid, kTX * kTY, sm, st>>>(f0, f1, o0, o1, g, a, b);
     } else {
-        k_delta4_tiled<F, 1><<<grid, kTX * kTY, 0, st>>>(f0, nullptr, o0, nullptr, g, a, b);
+        constexpr size_t sm = delta4_smem<F, 1>();
+        set_smem_attr(k_delta4_tiled<F, 1>, sm);
+        k_delta4_tiled<F, 1><<<grid, kTX * kTY, sm, st>>>(f0, nullptr, o0, nullptr, g, a, b);
     }
     count_launch();
     check_launch("k_delta4_tiled");
