@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <memory>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -123,6 +124,7 @@ struct TileGenParams {
     float vf[3][2][kMaxSeg], wf[3][2][kMaxSeg];
 };
 
+struct SigPlan;
 struct CompactPlan {
     bool has_tl = false;
     TileLineParams TL;
@@ -135,7 +137,33 @@ struct CompactPlan {
     double* tab64 = nullptr;
     float* tab32 = nullptr;
     size_t tab_elems = 0;
+    // few long closed x lines: the line is cut into pieces solved side by side
+    std::unique_ptr<SigPlan> sig;
     ~CompactPlan();
+};
+
+// Few long closed x lines (1-D problems, very thin 2-D grids) split into P
+// pieces inside the GPU: the reference's P > 1 line solve (src/tridiag.jl:
+// 136-170, src/banded.jl:177-214) with the pieces of one line in place of
+// ranks and global memory in place of the exchange.  Pieces of one class
+// share a local plan: the first (closed low end, open high end), the P - 2
+// middle ones (both ends open, equal lengths) and the last.  One launch
+// solves every piece with its halo read from the neighbouring pieces and
+// writes its heads and tails; a second forms the reduced system's unknowns
+// beside each piece from the dense inverse G and corrects:
+// x = y - V z_prev - W z_next.
+constexpr int kSigFields = 12;   // fields per pass (larger counts run in passes)
+struct SigPlan {
+    int P = 0, q = 1;
+    int len[3] = {0, 0, 0};        // piece length of the first, middle and last class
+    int64_t lines = 0;             // lines of the whole plan
+    CompactPlan cls[3];            // local plans of the classes (forced equal S and LB)
+    int dtype = CLES_F64;
+    void* tab = nullptr;           // class c: V [q][len_c], W [q][len_c]; then G (2qP)^2; plan dtype
+    int64_t off_V[3] = {0, 0, 0}, off_W[3] = {0, 0, 0}, off_G = 0;
+    void* loc = nullptr;           // local solutions: kSigFields x lines x n
+    void* iface[3] = {nullptr, nullptr, nullptr};   // heads / tails: kSigFields x 2q x lines of the class
+    ~SigPlan();
 };
 
 // Builds the plan of `scheme` along `dim` (0-based) of a grid with interior
@@ -145,9 +173,12 @@ struct CompactPlan {
 // lo_open / hi_open make that end of a non-periodic line a rank interface.
 // pow2_seg_max > 0 (batched plans): S is the fewest power-of-two segments of
 // at most pow2_seg_max (8, 16 or 32) points.
+// force_S / force_LB > 0 fix the segments per line and the lines per CTA (the
+// classes of a SigPlan, which share one launch).
 void build_compact_plan(CompactPlan& plan, const cles_scheme& scheme, const int n3[3], int dim,
                         bool periodic, double h, int dtype, int lo_fold = 0, int hi_fold = 0,
-                        bool lo_open = false, bool hi_open = false, int pow2_seg_max = 0);
+                        bool lo_open = false, bool hi_open = false, int pow2_seg_max = 0, int force_S = 0,
+                        int force_LB = 0);
 
 // The LHS band of one line (or one rank's piece of a split line), row-major
 // n x (2q+1): interior band, closure rows at closed ends, parity folds, and

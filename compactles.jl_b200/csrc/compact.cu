@@ -24,6 +24,7 @@
 // from the neighbouring rank, as the reference's fill does after
 // exchange_halos! (src/operators.jl:113-174).
 
+#include <algorithm>
 #include <cstdio>
 #include <type_traits>
 
@@ -40,6 +41,125 @@ __global__ void __launch_bounds__(512) k_compact(const __grid_constant__ Compact
                                                   T* __restrict__ iface) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     compact_lines<T, Q, M, XMODE, MS>(P, tab, in, out, mode, iface, blockIdx.x * P.LB, blockIdx.y, nullptr, smem_raw);
+}
+
+// ---------------------------------------------------------------------------
+// Few long closed x lines cut into pieces (SigPlan).  k_compact_pieces: the
+// CTAs of the three piece classes in one launch (blockIdx.x picks the class),
+// each the segmented solve of its pieces with open ends reading the
+// neighbouring pieces' points, local solutions to `loc`, heads and tails to
+// the class's iface block.  k_sig_correct: per (piece, line, field) the 2q
+// unknowns beside the piece from the dense inverse of the piece-interface
+// system, then x = y - V z_prev - W z_next into `out` by mode.
+struct SigLocal {
+    FieldView in[3], loc[3];
+    void* iface[3];
+    int nblk[3];
+};
+
+template <typename T, int Q, int M, int MS>
+__global__ void __launch_bounds__(512) k_compact_pieces(const __grid_constant__ CompactParams P0,
+                                                         const __grid_constant__ CompactParams P1,
+                                                         const __grid_constant__ CompactParams P2,
+                                                         const T* __restrict__ tab0, const T* __restrict__ tab1,
+                                                         const T* __restrict__ tab2, const __grid_constant__ SigLocal L) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    int b = blockIdx.x, c = 0;
+    if (b >= L.nblk[0]) {
+        b -= L.nblk[0];
+        c = 1;
+        if (b >= L.nblk[1]) {
+            b -= L.nblk[1];
+            c = 2;
+        }
+    }
+    const CompactParams& P = c == 0 ? P0 : (c == 1 ? P1 : P2);
+    const T* tab = c == 0 ? tab0 : (c == 1 ? tab1 : tab2);
+    compact_lines<T, Q, M, true, MS>(P, tab, L.in[c], L.loc[c], OUT_STORE, static_cast<T*>(L.iface[c]), b * P.LB,
+                                     blockIdx.y, nullptr, smem_raw);
+}
+
+struct SigCorrect {
+    const void* iface[3];
+    int64_t lines_c[3];
+    const void* tab;
+    int64_t off_V[3], off_W[3], off_G;
+    FieldView loc, out;            // element (g, line) of field c: base + c comp_stride + line offset + g
+    int len[3];
+    int P, ny;                     // pieces; the plan's ny (line l: j = l % ny, k = l / ny)
+};
+
+constexpr int kSigPts = 4;   // points per thread of the correction (pieces of at most 1024 points)
+template <typename T, int Q, int MODE>
+__global__ void __launch_bounds__(256) k_sig_correct(const __grid_constant__ SigCorrect C) {
+    __shared__ T h[2 * Q * 64];
+    __shared__ T grow[2 * Q][2 * Q * 64];
+    __shared__ T z[2 * Q];
+    const int k = blockIdx.x, P = C.P, N = 2 * Q * P;
+    const int64_t l = blockIdx.y;
+    const int comp = blockIdx.z;
+    auto cls = [&](int kk) { return kk == 0 ? 0 : (kk == P - 1 ? 2 : 1); };
+    const int c = cls(k), len = C.len[c];
+    const int off = k == 0 ? 0 : C.len[0] + (k - 1) * C.len[1];
+    const T* tab = static_cast<const T*>(C.tab);
+    const T* V = tab + C.off_V[c];
+    const T* W = tab + C.off_W[c];
+    const int64_t jj = l % C.ny, kz = l / C.ny;
+    const T* lp = static_cast<const T*>(C.loc.base) + (int64_t)comp * C.loc.comp_stride + jj * C.loc.sy +
+                  kz * C.loc.sz + off;
+    T* op = static_cast<T*>(C.out.base) + (int64_t)comp * C.out.comp_stride + jj * C.out.sy + kz * C.out.sz + off;
+    // loads that do not wait for the interface unknowns, issued first
+    T yv[kSigPts], vv[kSigPts][Q], wv[kSigPts][Q], ov[kSigPts];
+#pragma unroll
+    for (int e = 0; e < kSigPts; ++e) {
+        const int i = threadIdx.x + e * blockDim.x;
+        if (i < len) {
+            yv[e] = lp[i];
+#pragma unroll
+            for (int t = 0; t < Q; ++t) {
+                vv[e][t] = V[t * len + i];
+                wv[e][t] = W[t * len + i];
+            }
+            if (MODE == OUT_SUBTRACT) ov[e] = op[i];
+        }
+    }
+    // the 2q rows of the inverse this piece needs: prev tail rows, next head rows
+    for (int j = threadIdx.x; j < 2 * Q * N; j += blockDim.x) {
+        const int rr = j / N, col = j % N, t = rr % Q;
+        const bool nxt = rr >= Q;
+        const bool exists = nxt ? k + 1 < P : k > 0;
+        const int row = nxt ? 2 * Q * (k + 1) + t : 2 * Q * (k - 1) + Q + t;
+        grow[rr][col] = exists ? tab[C.off_G + (int64_t)row * N + col] : T(0);
+    }
+    for (int j = threadIdx.x; j < N; j += blockDim.x) {
+        const int kk = j / (2 * Q), r = j % (2 * Q), cc = cls(kk);
+        const int64_t lc = cc == 1 ? (int64_t)(kk - 1) + (int64_t)(P - 2) * l : l;
+        h[j] = static_cast<const T*>(C.iface[cc])[((int64_t)comp * 2 * Q + r) * C.lines_c[cc] + lc];
+    }
+    __syncthreads();
+    // z[0..q): previous piece's tail, z[q..2q): next piece's head; one warp each
+    const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+    if (warp < 2 * Q) {
+        T acc = T(0);
+        for (int j = lane; j < N; j += 32) acc += grow[warp][j] * h[j];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+        if (lane == 0) z[warp] = acc;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int e = 0; e < kSigPts; ++e) {
+        const int i = threadIdx.x + e * blockDim.x;
+        if (i < len) {
+            T acc = T(0);
+#pragma unroll
+            for (int t = 0; t < Q; ++t) acc += vv[e][t] * z[t] + wv[e][t] * z[Q + t];
+            const T r = yv[e] - acc;
+            if (MODE == OUT_NEGATE) op[i] = -r;
+            else if (MODE == OUT_SUBTRACT) op[i] = ov[e] - r;
+            else op[i] = r;
+        }
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -268,11 +388,113 @@ void dispatch(const CompactParams& P, const T* tab, const FieldView& in, const F
     }
 }
 
+template <typename T, int Q, int M, int MS>
+void launch_pieces(const SigPlan& sp, const SigLocal& L, int count, cudaStream_t st) {
+    size_t smem = 0;
+    for (int c = 0; c < 3; ++c) {
+        const CompactParams& P = sp.cls[c].P;
+        const int N = 2 * Q * P.S;
+        size_t s = sizeof(T) * (size_t)P.n * (P.LB + 1);
+        if (P.hasred) s += sizeof(T) * (size_t)P.LB * (N + 1);
+        smem = std::max(smem, s);
+    }
+    auto kern = k_compact_pieces<T, Q, M, MS>;
+    if (smem > 48 * 1024) CLES_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const CompactParams& P0 = sp.cls[0].P;
+    dim3 grid((unsigned)(L.nblk[0] + L.nblk[1] + L.nblk[2]), (unsigned)count);
+    auto tb = [&](int c) -> const T* {
+        return sizeof(T) == 8 ? reinterpret_cast<const T*>(sp.cls[c].tab64) : reinterpret_cast<const T*>(sp.cls[c].tab32);
+    };
+    kern<<<grid, (unsigned)(P0.LB * P0.S), smem, st>>>(sp.cls[0].P, sp.cls[1].P, sp.cls[2].P, tb(0), tb(1), tb(2), L);
+    count_launch();
+    check_launch("k_compact_pieces");
+}
+
+template <typename T, int Q>
+void launch_sig_correct(const SigCorrect& C, int64_t lines, int count, int mode, cudaStream_t st) {
+    dim3 grid((unsigned)C.P, (unsigned)lines, (unsigned)count);
+    if (mode == OUT_NEGATE) k_sig_correct<T, Q, OUT_NEGATE><<<grid, 256, 0, st>>>(C);
+    else if (mode == OUT_SUBTRACT) k_sig_correct<T, Q, OUT_SUBTRACT><<<grid, 256, 0, st>>>(C);
+    else k_sig_correct<T, Q, OUT_STORE><<<grid, 256, 0, st>>>(C);
+    count_launch();
+    check_launch("k_sig_correct");
+}
+
+template <typename T>
+void launch_sig(const CompactPlan& plan, const FieldView& in, const FieldView& out, int count, int mode,
+                cudaStream_t st) {
+    const SigPlan& sp = *plan.sig;
+    if (mode != OUT_STORE && mode != OUT_NEGATE && mode != OUT_SUBTRACT)
+        throw Error(CLES_EINVAL, "internal: pieced lines store, negate or subtract");
+    const CompactParams& P = plan.P;
+    const int n = P.n, Pp = sp.P, q = sp.q;
+    const int64_t L = sp.lines;
+    // the stride between lines of the plan (one of ny, nz is 1)
+    const int64_t in_ls = P.ny > 1 ? in.sy : in.sz;
+    for (int c0 = 0; c0 < count; c0 += kSigFields) {
+        const int cc = std::min(kSigFields, count - c0);
+        const T* ib = static_cast<const T*>(in.base) + (int64_t)c0 * in.comp_stride;
+        T* ob = static_cast<T*>(out.base) + (int64_t)c0 * out.comp_stride;
+        T* lb = static_cast<T*>(sp.loc);
+        const int64_t lcs = L * n;   // loc: [field][line][n]
+        SigLocal Lc;
+        const int64_t off_c[3] = {0, sp.len[0], sp.len[0] + (int64_t)(Pp - 2) * sp.len[1]};
+        for (int c = 0; c < 3; ++c) {
+            const bool midc = c == 1;
+            Lc.in[c] = FieldView{const_cast<T*>(ib) + off_c[c], in.comp_stride, midc ? (int64_t)sp.len[1] : in_ls,
+                                 midc ? in_ls : 0};
+            Lc.loc[c] = FieldView{lb + off_c[c], lcs, midc ? (int64_t)sp.len[1] : (int64_t)n, midc ? (int64_t)n : 0};
+            Lc.iface[c] = sp.iface[c];
+            const CompactParams& Pc = sp.cls[c].P;
+            Lc.nblk[c] = (int)((Pc.lines + Pc.LB - 1) / Pc.LB);
+        }
+        if (q == 1) {
+            switch (P.M) {
+                case 1: launch_pieces<T, 1, 1, 16>(sp, Lc, cc, st); break;
+                case 2: launch_pieces<T, 1, 2, 16>(sp, Lc, cc, st); break;
+                case 4: launch_pieces<T, 1, 4, 16>(sp, Lc, cc, st); break;
+                default: throw Error(CLES_EINVAL, "pieced lines: unsupported stencil half-width");
+            }
+        } else {
+            if (P.M != 3) throw Error(CLES_EINVAL, "pieced lines: unsupported stencil half-width");
+            launch_pieces<T, 2, 3, kMaxSeg>(sp, Lc, cc, st);
+        }
+        SigCorrect C;
+        for (int c = 0; c < 3; ++c) {
+            C.iface[c] = sp.iface[c];
+            C.lines_c[c] = sp.cls[c].P.lines;
+            C.off_V[c] = sp.off_V[c];
+            C.off_W[c] = sp.off_W[c];
+            C.len[c] = sp.len[c];
+        }
+        C.tab = sp.tab;
+        C.off_G = sp.off_G;
+        C.loc = FieldView{lb, lcs, P.ny > 1 ? (int64_t)n : 0, P.ny > 1 ? 0 : (int64_t)n};
+        C.out = FieldView{ob, out.comp_stride, out.sy, out.sz};
+        C.P = Pp;
+        C.ny = P.ny;
+        if (q == 1) launch_sig_correct<T, 1>(C, L, cc, mode, st);
+        else launch_sig_correct<T, 2>(C, L, cc, mode, st);
+    }
+}
+
 }  // namespace
 
 void launch_compact(const CompactPlan& plan, const FieldView& in, const FieldView& out, int count, int mode,
                     cudaStream_t st) {
     if (count <= 0 || plan.P.lines == 0) return;
+    if (plan.sig) {
+        int rec = -1;
+        if (profiling()) {
+            const double el = plan.dtype == CLES_F64 ? 8.0 : 4.0;
+            rec = prof_begin(st, plan.P.dim, (double)plan.P.lines * plan.P.n * count * el *
+                                                 (mode == OUT_SUBTRACT ? 3.0 : 2.0));
+        }
+        if (plan.dtype == CLES_F64) launch_sig<double>(plan, in, out, count, mode, st);
+        else launch_sig<float>(plan, in, out, count, mode, st);
+        if (rec >= 0) prof_end(rec, st);
+        return;
+    }
     int rec = -1;
     if (profiling()) {
         const double el = plan.dtype == CLES_F64 ? 8.0 : 4.0;

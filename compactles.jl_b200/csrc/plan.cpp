@@ -289,8 +289,115 @@ void LineBand::solve(double* x) const {
     }
 }
 
+// The pieces of a SigPlan: P = ceil(n / 256) (at most 64) pieces, the middle
+// ones of equal length n / P and the remainder shared by the first and last;
+// S segments of at most 16 points in every piece (32 beyond 512-point
+// pieces), two pieces per CTA.  Spikes of each class and the reduced system
+// over all pieces as in build_split_plan (the rank-level spikes of
+// src/tridiag.jl:85-123 and src/banded.jl:108-169), its dense inverse whole.
+static void build_sig_plan(CompactPlan& plan, const cles_scheme& s, const int n3[3], double h, int dtype) {
+    const int n = n3[0], q = s.q;
+    const int P = std::min(64, (n + 255) / 256);
+    if (P < 4) return;
+    // pieces of at most 1024 points (the correction's four points a thread)
+    if ((n / P) + (n % P) > 1024) return;
+    const int mid = n / P, rem = n - P * mid;
+    const int len[3] = {mid + rem / 2, mid, mid + (rem - rem / 2)};
+    const int maxlen = std::max(len[0], len[2]);
+    int S = (maxlen + 15) / 16;
+    if (S > 32) S = (maxlen + kMaxSeg - 1) / kMaxSeg;
+    if (S > 32 || mid / S < std::max(2 * q + 1, q + 1)) return;
+    const int LB = 2;
+    auto sp = std::unique_ptr<SigPlan>(new SigPlan());
+    sp->P = P;
+    sp->q = q;
+    sp->lines = plan.P.lines;
+    sp->dtype = dtype;
+    for (int c = 0; c < 3; ++c) sp->len[c] = len[c];
+    const int L = (int)plan.P.lines;
+    for (int c = 0; c < 3; ++c) {
+        // the middle class enumerates (piece - 1) fastest, then the line
+        int nc3[3] = {len[c], c == 1 ? P - 2 : L, c == 1 ? L : 1};
+        build_compact_plan(sp->cls[c], s, nc3, 0, false, h, dtype, 0, 0, c > 0, c < 2, 0, S, LB);
+        if (sp->cls[c].P.pcr || sp->cls[c].P.S != S || sp->cls[c].P.LB != LB) return;
+    }
+    // spikes per class, reduced system in z = (head_0, tail_0, head_1, ...)
+    std::vector<double> Vc[3], Wc[3];
+    for (int c = 0; c < 3; ++c) {
+        const int m = len[c];
+        const bool lo = c > 0, hi = c < 2;
+        LineBand b = make_line_band(s, m, 0, 0, lo, hi);
+        b.factor();
+        Vc[c].assign((size_t)q * m, 0.0);
+        Wc[c].assign((size_t)q * m, 0.0);
+        for (int t = 0; t < q; ++t) {
+            double* v = &Vc[c][(size_t)t * m];
+            double* w = &Wc[c][(size_t)t * m];
+            if (lo) {
+                for (int r = 0; r < q; ++r) {
+                    const int d = r + q - t;
+                    if (d >= 1 && d <= q) v[r] = s.lhs[d - 1];
+                }
+                b.solve(v);
+            }
+            if (hi) {
+                for (int i = m - q; i < m; ++i) {
+                    const int d = m + t - i;
+                    if (d >= 1 && d <= q) w[i] = s.lhs[d - 1];
+                }
+                b.solve(w);
+            }
+        }
+    }
+    const int N = 2 * q * P;
+    std::vector<double> R((size_t)N * N, 0.0);
+    for (int rr = 0; rr < P; ++rr) {
+        const int c = rr == 0 ? 0 : (rr == P - 1 ? 2 : 1), m = len[c];
+        for (int r = 0; r < q; ++r) {
+            const int rh = 2 * q * rr + r, rt = 2 * q * rr + q + r;
+            R[(size_t)rh * N + rh] += 1.0;
+            R[(size_t)rt * N + rt] += 1.0;
+            for (int t = 0; t < q; ++t) {
+                if (rr > 0) {
+                    const int cprev = 2 * q * (rr - 1) + q + t;
+                    R[(size_t)rh * N + cprev] += Vc[c][(size_t)t * m + r];
+                    R[(size_t)rt * N + cprev] += Vc[c][(size_t)t * m + (m - q + r)];
+                }
+                if (rr < P - 1) {
+                    const int cnext = 2 * q * (rr + 1) + t;
+                    R[(size_t)rh * N + cnext] += Wc[c][(size_t)t * m + r];
+                    R[(size_t)rt * N + cnext] += Wc[c][(size_t)t * m + (m - q + r)];
+                }
+            }
+        }
+    }
+    const std::vector<double> G = dense_inverse(R, N);
+    std::vector<double> tab;
+    for (int c = 0; c < 3; ++c) {
+        sp->off_V[c] = (int64_t)tab.size();
+        tab.insert(tab.end(), Vc[c].begin(), Vc[c].end());
+        sp->off_W[c] = (int64_t)tab.size();
+        tab.insert(tab.end(), Wc[c].begin(), Wc[c].end());
+    }
+    sp->off_G = (int64_t)tab.size();
+    tab.insert(tab.end(), G.begin(), G.end());
+    const size_t el = dtype == CLES_F64 ? sizeof(double) : sizeof(float);
+    CLES_CUDA(cudaMalloc(&sp->tab, el * tab.size()));
+    if (dtype == CLES_F64) {
+        CLES_CUDA(cudaMemcpy(sp->tab, tab.data(), sizeof(double) * tab.size(), cudaMemcpyHostToDevice));
+    } else {
+        std::vector<float> t32(tab.begin(), tab.end());
+        CLES_CUDA(cudaMemcpy(sp->tab, t32.data(), sizeof(float) * t32.size(), cudaMemcpyHostToDevice));
+    }
+    CLES_CUDA(cudaMalloc(&sp->loc, el * (size_t)kSigFields * (size_t)L * (size_t)n));
+    for (int c = 0; c < 3; ++c)
+        CLES_CUDA(cudaMalloc(&sp->iface[c], el * (size_t)kSigFields * 2 * q * (size_t)sp->cls[c].P.lines));
+    plan.sig = std::move(sp);
+}
+
 void build_compact_plan(CompactPlan& plan, const cles_scheme& s, const int n3[3], int dim, bool periodic,
-                        double h, int dtype, int lo_fold, int hi_fold, bool lo_open, bool hi_open, int pow2_seg_max) {
+                        double h, int dtype, int lo_fold, int hi_fold, bool lo_open, bool hi_open, int pow2_seg_max,
+                        int force_S, int force_LB) {
     const int n = n3[dim];
     const int q = s.q, M = s.M, nc = s.nc;
     if (q < 1 || q > CLES_MAX_Q) throw Error(CLES_EINVAL, "scheme LHS half-bandwidth q must be 1 or 2");
@@ -421,6 +528,10 @@ void build_compact_plan(CompactPlan& plan, const cles_scheme& s, const int n3[3]
         while ((n + S - 1) / S > std::min(pow2_seg_max, kMaxSeg)) S *= 2;
         if (n / S < std::max(2 * q + 1, q + 1)) throw Error(CLES_EINVAL, "batched segments too short for the scheme");
     }
+    if (force_S > 0) {
+        S = force_S;
+        if (n / S < std::max(2 * q + 1, q + 1)) throw Error(CLES_EINVAL, "forced segments too short for the scheme");
+    }
     P.S = S;
     P.seg_base = n / S;
     P.seg_rem = n % S;
@@ -436,9 +547,10 @@ void build_compact_plan(CompactPlan& plan, const cles_scheme& s, const int n3[3]
         while (LB > 1 && (size_t)n * (LB + 1) * el > 110 * 1024) LB /= 2;
         if ((size_t)n * (LB + 1) * el > 200 * 1024) throw Error(CLES_EINVAL, "x line too long for the shared-memory tile");
     }
+    if (force_LB > 0) LB = force_LB;
     if (LB * S > 512) throw Error(CLES_EINVAL, "line too long for one CTA");
     const int LB_full = LB;
-    if (P.lines < LB) {
+    if (P.lines < LB && force_LB <= 0) {
         int l = 1;
         while (l < P.lines) l *= 2;
         LB = std::max(1, std::min(LB, l));
@@ -665,6 +777,18 @@ void build_compact_plan(CompactPlan& plan, const cles_scheme& s, const int n3[3]
         CLES_CUDA(cudaMalloc(&plan.tab32, sizeof(float) * total));
         CLES_CUDA(cudaMemcpy(plan.tab32, t32.data(), sizeof(float) * total, cudaMemcpyHostToDevice));
     }
+    // a handful of long closed x lines is latency-bound in one CTA per line:
+    // cut it into pieces solved side by side (SigPlan)
+    if (dim == 0 && !periodic && !lo_fold && !hi_fold && !lo_open && !hi_open && pow2_seg_max == 0 &&
+        force_S == 0 && P.lines <= 16 && n >= 2048 && (n3[1] == 1 || n3[2] == 1))
+        build_sig_plan(plan, s, n3, h, dtype);
+}
+
+SigPlan::~SigPlan() {
+    if (tab) cudaFree(tab);
+    if (loc) cudaFree(loc);
+    for (void* p : iface)
+        if (p) cudaFree(p);
 }
 
 SplitPlan::~SplitPlan() {
