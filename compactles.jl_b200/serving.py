@@ -17,9 +17,14 @@ The stream is processed two ways on the same GPU:
 (1.5 by default, the latency case); --load inf submits every request at time
 zero, which measures the server's capacity.  Reported: solves/s and p50/p99
 time-to-solution of both, and whether every served result equals the same
-request run alone: bitwise against the one-at-a-time run without batching;
-with batching bitwise against the request alone in a batch of its own, and
-within 1e-10 relative L2 of the one-at-a-time (one-grid solver) run.
+request run alone: bitwise against the one-at-a-time run without batching.
+With batching the relative L2 distance to the one-at-a-time (one-grid
+solver) run is reported and held to 1e-10, and bitwise equality with the
+request alone in a batch of its own is reported beside it: a batch's
+autotuner picks each class's launch form (batched kernels or per-member
+kernels) from the batch's composition, and the two forms round differently,
+so a request alone and in the mix agree bitwise only where the choices
+coincide (under a fixed form they always do).
 
   python compactles.jl_b200/serving.py [--requests 24] [--scale small|full] [--load 1.5|inf] [--batching]
 """
@@ -173,8 +178,9 @@ def main(argv=None):
     extra = {}
     if a.batching:
         alone = alone_in_batch(cl, reqs)
-        same = all(np.array_equal(res[i], alone[i]) for i in range(len(reqs)))
+        extra["bitwise_equal_alone_in_batch"] = all(np.array_equal(res[i], alone[i]) for i in range(len(reqs)))
         extra["max_rel_l2_vs_one_grid_solver"] = max(rel_l2(res[i], base[i]) for i in range(len(reqs)))
+        same = extra["max_rel_l2_vs_one_grid_solver"] <= 1e-10
     else:
         same = all(np.array_equal(res[i], base[i]) for i in range(len(reqs)))
     out = {
