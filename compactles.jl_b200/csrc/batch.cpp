@@ -11,7 +11,7 @@
 // reads.  Everything that depends on a grid's shape or spacing takes a table:
 //   * line solves: a launch table of per-grid plans (power-of-two segments)
 //     and a CTA table (launch_compact_batch);
-//   * delta4_sum!: a table of 32 x 8 x 32 tiles;
+//   * delta4_sum!: a table of 32 x 16 x 32 tiles;
 //   * boundary planes: a table of faces;
 //   * max_rate + the graph-mode clock: a table of 2048-cell chunks, then one
 //     block per grid; every grid keeps its own dt, clock and stop condition.
@@ -573,10 +573,11 @@ private:
             B.clk = clk_.as<double>() + 16 * (size_t)g;
             B.cc = ClockConst{cls_.cfl, m.tfinal, (double)m.nmax, cls_.control.dt_min, cls_.control.dt_min_ratio};
             // delta4 tiles
-            const int tx = (m.n[0] + 31) / 32, ty = (m.n[1] + 7) / 8, tz = (m.n[2] + 31) / 32;
+            const int tx = (m.n[0] + kD4X - 1) / kD4X, ty = (m.n[1] + kD4Y - 1) / kD4Y,
+                      tz = (m.n[2] + kD4Z - 1) / kD4Z;
             for (int z = 0; z < tz; ++z)
                 for (int y = 0; y < ty; ++y)
-                    for (int x = 0; x < tx; ++x) tiles.push_back(BatchTile{g, 32 * x, 8 * y, 32 * z});
+                    for (int x = 0; x < tx; ++x) tiles.push_back(BatchTile{g, kD4X * x, kD4Y * y, kD4Z * z});
             // faces (apply_bcs! order: dims, low then high)
             for (int k = 0; k < 3; ++k) {
                 if (!m.active[k]) continue;

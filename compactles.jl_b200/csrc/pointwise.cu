@@ -255,23 +255,25 @@ __global__ void k_delta4(const F* __restrict__ f, F* __restrict__ out, Grid3 g, 
     }
 }
 
-// delta4_sum! for NF fields at once, tiled: a block covers 32 x 8 (x, y)
-// columns and walks z; each xy-plane (with 2-point halos) is staged in shared
-// memory for the x and y differences, and every thread keeps its column's
-// five z values in registers for the z difference.  Accumulation order per
-// point is the reference's: out = 0; for d in x, y, z: out += w_d |sum_m D4_m f|.
-constexpr int kTX = 32, kTY = 8, kZC = 32;
+// delta4_sum! for NF fields at once, tiled: a block of 256 threads covers
+// 32 x 16 (x, y) columns and walks z; each thread owns two neighbouring rows
+// of one x column.  The halo'd xy planes z0-2 .. z0+kZC+1 stream through a
+// ring of kRing planes in shared memory by cp.async (one commit group per
+// plane); at plane z the x and y differences read plane z (the six column
+// values of a thread serve both rows' y differences) and the z difference a
+// register window of the thread's two columns, fed from plane z+2.  Eight
+// shared-memory reads a point and field.  Accumulation order per point is
+// the reference's: out = 0; for d in x, y, z: out += w_d |sum_m D4_m f|.
+constexpr int kTX = kD4X, kTY = kD4Y, kZC = kD4Z;
 __device__ __forceinline__ int edge_index(int i, int n, int periodic) {
     if (periodic) return i < 0 ? i + n : (i >= n ? i - n : i);
     return i < 0 ? 0 : (i >= n ? n - 1 : i);
 }
-// One block's tile (x0, y0, z0) of the tiled delta4_sum!.  The halo'd xy
-// planes z0-2 .. z0+kZC+1 stream through a ring of kRing planes in shared
-// memory by cp.async (one commit group per plane, three planes in flight
-// while a plane is computed); the x and y differences read the plane, the z
-// difference the four ring neighbours along the column.
-constexpr int kRing = 8;
+constexpr int kRing = 6;
+constexpr int kD4Threads = 256;
 constexpr int kPlane = (kTY + 4) * (kTX + 4);
+constexpr int kStage = (kPlane + kD4Threads - 1) / kD4Threads;   // staging slots a thread
+static_assert(kTX * kTY == 2 * kD4Threads, "two rows a thread");
 template <typename F, int NF>
 constexpr size_t delta4_smem() {
     return sizeof(F) * (size_t)kRing * NF * kPlane;
@@ -287,91 +289,119 @@ __device__ __forceinline__ void d4_cp_async(F* dst, const F* src) {
         asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(d4_smem_addr(dst)), "l"(src) : "memory");
 }
 __device__ __forceinline__ void d4_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-__device__ __forceinline__ void d4_wait2() { asm volatile("cp.async.wait_group 2;" ::: "memory"); }
 
 template <typename F, int NF>
 __device__ __forceinline__ void delta4_tile(const F* __restrict__ f0, const F* __restrict__ f1, F* __restrict__ o0,
                                             F* __restrict__ o1, const Grid3& g, const Weights3& w0,
                                             const Weights3& w1, const int x0, const int y0, const int z0,
                                             F* __restrict__ ring) {
-    constexpr int NT = kTX * kTY, TW = kTX + 4;
-    static_assert(kPlane <= 2 * NT, "two staging slots per thread");
+    constexpr int TW = kTX + 4;
     const F* fs[2] = {f0, f1};
     F* os[2] = {o0, o1};
     const Weights3 ws[2] = {w0, w1};
     const int nx = g.n[0], ny = g.n[1], nz = g.n[2];
     const int64_t sy = nx, sz = (int64_t)nx * ny;
     const int tx = threadIdx.x % kTX, ty = threadIdx.x / kTX;
-    const int x = x0 + tx, y = y0 + ty;
-    const bool inside = x < nx && y < ny;
+    const int x = x0 + tx, ya = y0 + 2 * ty;
+    const bool ins[2] = {x < nx && ya < ny, x < nx && ya + 1 < ny};
     const bool zact = g.active[2] != 0;
     const double D4[5] = {1.0, -4.0, 6.0, -4.0, 1.0};
-    // this thread's two staging slots of a halo'd plane: ring offset and
-    // in-plane source offset (periodic wrap or clamping, as delta4_sum!)
-    int soff_s[2];
-    int64_t soff_g[2];
-    bool sv[2];
+    // this thread's staging slots of a halo'd plane: ring offset and in-plane
+    // source offset (periodic wrap or clamping, as delta4_sum!)
+    int64_t soff_g[kStage];
+    bool sv[kStage];
 #pragma unroll
-    for (int s = 0; s < 2; ++s) {
-        const int idx = threadIdx.x + NT * s;
+    for (int s = 0; s < kStage; ++s) {
+        const int idx = threadIdx.x + kD4Threads * s;
         sv[s] = idx < kPlane;
         const int hx = idx % TW, hy = idx / TW;
         const int gx = g.active[0] ? edge_index(x0 - 2 + hx, nx, g.periodic[0]) : min(x0 - 2 + hx < 0 ? 0 : x0 - 2 + hx, nx - 1);
         const int gy = g.active[1] ? edge_index(y0 - 2 + hy, ny, g.periodic[1]) : min(y0 - 2 + hy < 0 ? 0 : y0 - 2 + hy, ny - 1);
-        soff_s[s] = idx;
         soff_g[s] = (int64_t)gx + (int64_t)gy * sy;
     }
     const int zend = min(z0 + kZC, nz);
     // plane r of the block (r = 0 is z0 - 2) into ring slot r % kRing; planes
     // past the last one any output reads are left out (empty group)
     const int rlast = zact ? (zend - 1 + 2) - (z0 - 2) : 2;
+    auto slot = [&](int r) { return ring + (size_t)(r % kRing) * NF * kPlane; };
     auto issue = [&](int r) {
         if (r <= rlast) {
             const int zz = zact ? edge_index(z0 - 2 + r, nz, g.periodic[2]) : 0;
-            F* slot = ring + (size_t)(r % kRing) * NF * kPlane;
+            F* sl = slot(r);
 #pragma unroll
             for (int f = 0; f < NF; ++f)
 #pragma unroll
-                for (int s = 0; s < 2; ++s)
-                    if (sv[s]) d4_cp_async(slot + f * kPlane + soff_s[s], fs[f] + soff_g[s] + (int64_t)zz * sz);
+                for (int s = 0; s < kStage; ++s)
+                    if (sv[s])
+                        d4_cp_async(sl + f * kPlane + threadIdx.x + kD4Threads * s, fs[f] + soff_g[s] + (int64_t)zz * sz);
         }
         d4_commit();
     };
-    // planes 0 .. 6: the five the first output needs and two more in flight
+    // column offset of row t (0, 1) of this thread in a plane
+    const int cofs = (2 * ty + 2) * TW + tx + 2;
+    // planes 0 .. 5; the z window starts with planes 0 .. 3 (z0-2 .. z0+1)
 #pragma unroll
-    for (int r = 0; r < 7; ++r) issue(r);
+    for (int r = 0; r < kRing; ++r) issue(r);
+    F zw[NF][2][5];
+    asm volatile("cp.async.wait_group 2;" ::: "memory");
+    __syncthreads();
+    if (zact) {
+#pragma unroll
+        for (int f = 0; f < NF; ++f)
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+#pragma unroll
+                for (int t = 0; t < 2; ++t) zw[f][t][q + 1] = slot(q)[f * kPlane + cofs + t * TW];
+    }
     for (int z = z0; z < zend; ++z) {
         const int rz = z - z0 + 2;
-        d4_wait2();         // this thread's copies of plane rz + 2 have landed
-        __syncthreads();    // everyone's, and plane rz - 3 is no longer read
-        issue(rz + 5);
-        if (inside) {
-            const F* pl = ring + (size_t)(rz % kRing) * NF * kPlane;
+        // this thread's copies of plane rz + 2 have landed (plane rz + 3 may
+        // still be in flight); after the barrier everyone's have, and plane
+        // rz - 2 is read by no one
+        asm volatile("cp.async.wait_group 1;" ::: "memory");
+        __syncthreads();
+        issue(rz + 4);
+        const F* pl = slot(rz);
+        const F* pc = slot(rz + 2);
 #pragma unroll
-            for (int f = 0; f < NF; ++f) {
-                const F* t = pl + f * kPlane;
+        for (int f = 0; f < NF; ++f) {
+            const F* t0 = pl + f * kPlane;
+            if (zact) {
+#pragma unroll
+                for (int t = 0; t < 2; ++t) {
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) zw[f][t][q] = zw[f][t][q + 1];
+                    zw[f][t][4] = pc[f * kPlane + cofs + t * TW];
+                }
+            }
+            // the column x: tile rows 2ty .. 2ty+5 (both rows' y stencils)
+            F cy[6];
+#pragma unroll
+            for (int k = 0; k < 6; ++k) cy[k] = t0[(2 * ty + k) * TW + tx + 2];
+#pragma unroll
+            for (int t = 0; t < 2; ++t) {
+                if (!ins[t]) continue;
                 double o = 0.0;
                 if (g.active[0]) {
+                    const F* row = t0 + (2 * ty + 2 + t) * TW + tx;
                     double acc = 0.0;
 #pragma unroll
-                    for (int m = 0; m < 5; ++m) acc += D4[m] * double(t[(ty + 2) * TW + tx + m]);
+                    for (int m = 0; m < 5; ++m) acc += D4[m] * double(m == 2 ? cy[2 + t] : row[m]);
                     o += ws[f].w[0] * fabs(acc);
                 }
                 if (g.active[1]) {
                     double acc = 0.0;
 #pragma unroll
-                    for (int m = 0; m < 5; ++m) acc += D4[m] * double(t[(ty + m) * TW + tx + 2]);
+                    for (int m = 0; m < 5; ++m) acc += D4[m] * double(cy[t + m]);
                     o += ws[f].w[1] * fabs(acc);
                 }
                 if (zact) {
                     double acc = 0.0;
 #pragma unroll
-                    for (int m = 0; m < 5; ++m)
-                        acc += D4[m] * double(ring[(size_t)((rz - 2 + m) % kRing) * NF * kPlane + f * kPlane +
-                                                   (ty + 2) * TW + tx + 2]);
+                    for (int m = 0; m < 5; ++m) acc += D4[m] * double(zw[f][t][m]);
                     o += ws[f].w[2] * fabs(acc);
                 }
-                os[f][x + y * sy + (int64_t)z * sz] = F(o);
+                os[f][x + (int64_t)(ya + t) * sy + (int64_t)z * sz] = F(o);
             }
         }
     }
@@ -379,7 +409,7 @@ __device__ __forceinline__ void delta4_tile(const F* __restrict__ f0, const F* _
 }
 
 template <typename F, int NF>
-__global__ void __launch_bounds__(kTX * kTY) k_delta4_tiled(const F* __restrict__ f0, const F* __restrict__ f1,
+__global__ void __launch_bounds__(kD4Threads) k_delta4_tiled(const F* __restrict__ f0, const F* __restrict__ f1,
                                                            F* __restrict__ o0, F* __restrict__ o1, Grid3 g,
                                                            Weights3 w0, Weights3 w1) {
     extern __shared__ __align__(16) unsigned char d4_raw[];
@@ -1052,7 +1082,7 @@ __global__ void k_clock_after(double* __restrict__ clk, ClockConst c) {
 
 // ---- batched forms over the grids of a batch --------------------------------
 template <typename F, int NF>
-__global__ void __launch_bounds__(kTX * kTY) k_delta4_batch(const F* __restrict__ f0, const F* __restrict__ f1,
+__global__ void __launch_bounds__(kD4Threads) k_delta4_batch(const F* __restrict__ f0, const F* __restrict__ f1,
                                                            F* __restrict__ o0, F* __restrict__ o1, int p0, int p1,
                                                            const BatchGrid* __restrict__ grids,
                                                            const BatchTile* __restrict__ tiles) {
@@ -1146,11 +1176,11 @@ void BatchOps<F>::delta4(const F* f0, const F* f1, F* o0, F* o1, int p0, int p1,
     if (f1) {
         constexpr size_t sm = delta4_smem<F, 2>();
         set_smem_attr(k_delta4_batch<F, 2>, sm);
-        k_delta4_batch<F, 2><<<ntiles, kTX * kTY, sm, st>>>(f0, f1, o0, o1, p0, p1, grids, tiles);
+        k_delta4_batch<F, 2><<<ntiles, kD4Threads, sm, st>>>(f0, f1, o0, o1, p0, p1, grids, tiles);
     } else {
         constexpr size_t sm = delta4_smem<F, 1>();
         set_smem_attr(k_delta4_batch<F, 1>, sm);
-        k_delta4_batch<F, 1><<<ntiles, kTX * kTY, sm, st>>>(f0, f1, o0, o1, p0, p1, grids, tiles);
+        k_delta4_batch<F, 1><<<ntiles, kD4Threads, sm, st>>>(f0, f1, o0, o1, p0, p1, grids, tiles);
     }
     count_launch();
     check_launch("k_delta4_batch");
@@ -1228,11 +1258,11 @@ void Pointwise<F>::delta4_tiled(const F* f0, const F* f1, F* o0, F* o1, const Gr
         b = Weights3{{w1[0], w1[1], w1[2]}};
         constexpr size_t sm = delta4_smem<F, 2>();
         set_smem_attr(k_delta4_tiled<F, 2>, sm);
-        k_delta4_tiled<F, 2><<<grid, kTX * kTY, sm, st>>>(f0, f1, o0, o1, g, a, b);
+        k_delta4_tiled<F, 2><<<grid, kD4Threads, sm, st>>>(f0, f1, o0, o1, g, a, b);
     } else {
         constexpr size_t sm = delta4_smem<F, 1>();
         set_smem_attr(k_delta4_tiled<F, 1>, sm);
-        k_delta4_tiled<F, 1><<<grid, kTX * kTY, sm, st>>>(f0, nullptr, o0, nullptr, g, a, b);
+        k_delta4_tiled<F, 1><<<grid, kD4Threads, sm, st>>>(f0, nullptr, o0, nullptr, g, a, b);
     }
     count_launch();
     check_launch("k_delta4_tiled");

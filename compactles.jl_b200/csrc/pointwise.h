@@ -262,7 +262,9 @@ struct BatchGrid {
     double* clk;      // graph-mode clock (DC_* slots) of this grid
     ClockConst cc;
 };
-struct BatchTile { int grid, x0, y0, z0; };     // one delta4 tile (32 x 8 x 32 cells)
+// cells of one delta4_sum! tile (x, y, z)
+constexpr int kD4X = 32, kD4Y = 16, kD4Z = 32;
+struct BatchTile { int grid, x0, y0, z0; };     // one delta4 tile (kD4X x kD4Y x kD4Z cells)
 struct BatchFace { int grid, d, side, kind; BcState st; };
 struct BatchChunk { int grid; int64_t c0; };    // cells [c0, c0 + kBatchChunk) of a grid
 constexpr int kBatchChunk = 2048;
