@@ -289,7 +289,7 @@ void LineBand::solve(double* x) const {
     }
 }
 
-// The pieces of a SigPlan: P = ceil(n / 256) (at most 64) pieces, the middle
+// The pieces of a SigPlan: P = ceil(n / 128) (at most 64) pieces, the middle
 // ones of equal length n / P and the remainder shared by the first and last;
 // S segments of at most 16 points in every piece (32 beyond 512-point
 // pieces), two pieces per CTA.  Spikes of each class and the reduced system
@@ -297,7 +297,7 @@ void LineBand::solve(double* x) const {
 // src/tridiag.jl:85-123 and src/banded.jl:108-169), its dense inverse whole.
 static void build_sig_plan(CompactPlan& plan, const cles_scheme& s, const int n3[3], double h, int dtype) {
     const int n = n3[0], q = s.q;
-    const int P = std::min(64, (n + 255) / 256);
+    const int P = std::min(64, (n + 127) / 128);
     if (P < 4) return;
     // pieces of at most 1024 points (the correction's four points a thread)
     if ((n / P) + (n % P) > 1024) return;
