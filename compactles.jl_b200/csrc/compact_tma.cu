@@ -6,7 +6,8 @@
 // consecutive-x lines is a 2-D box {32 x, n along the line} of the field: one
 // `cp.async.bulk.tensor` copy brings it into shared memory as tile[g][lane],
 // which every thread then reads by column without bank conflicts.  The kernel
-// is persistent (one CTA per SM) and keeps NS tiles in flight: the copy of a
+// is persistent (two CTAs per SM for 32-point segments, one for 16-point
+// ones) and keeps NS tiles in flight: the copy of a
 // later group is issued as soon as the current tile has been read into
 // registers, so HBM is busy while the segments solve.  Compute per group is
 // the segmented spike solve of compact.cu (fill, per-segment Thomas sweep,
@@ -92,20 +93,45 @@ __device__ __forceinline__ void prefetch_l2(const void* p) {
     asm volatile("prefetch.global.L2 [%0];" ::"l"(reinterpret_cast<uint64_t>(p)));
 }
 
+// The MS + 2M stencil inputs of the segment starting at line index `off`,
+// read down one column of a tile whose row g + H holds line index g (PITCH
+// elements a row; `col` already points at this lane's column).  The segment's
+// own MS values sit at fixed offsets from one address; only the M values
+// before and the M after it can fall beyond the line: they wrap on periodic
+// lines, read the halo row at an open end and clamp to the end value
+// otherwise (closure rows replace what a clamped value feeds).
+template <typename T, int M, int MS, int PITCH>
+__device__ __forceinline__ void gather_window(const T* col, int off, int n, int H, bool periodic, bool lo_open,
+                                              bool hi_open, T (&wv)[MS + 2 * M]) {
+    const T* mid = col + (off + H) * PITCH;
+#pragma unroll
+    for (int j = 0; j < MS; ++j) wv[M + j] = mid[j * PITCH];
+#pragma unroll
+    for (int k = 0; k < M; ++k) {
+        int g = off - M + k;
+        if (g < 0) g = periodic ? g + n : (lo_open ? g : 0);
+        wv[k] = col[(g + H) * PITCH];
+        int h = off + MS + k;
+        if (h >= n) h = periodic ? h - n : (hi_open ? h : n - 1);
+        wv[MS + M + k] = col[(h + H) * PITCH];
+    }
+}
+
 template <typename T>
 __device__ __forceinline__ T tl(const double* d, const float* f, int i) {
     if (sizeof(T) == 8) return T(d[i]);
     return T(f[i]);
 }
 
-// FP32 lines of 32-point segments run two persistent CTAs per SM (3 tiles in
-// flight each, at most 128 registers a thread): one CTA of 8 warps cannot
-// keep an SM's issue slots busy on the shorter FP32 tiles.
-template <typename T>
-constexpr int tma_ctas_per_sm(int ms) { return sizeof(T) == 4 && ms == 32 ? 2 : 1; }
-
-template <typename T, int M, int MS>
-__global__ void __launch_bounds__(MS == 16 ? 512 : 256, tma_ctas_per_sm<T>(MS))
+// CPS persistent CTAs share an SM.  Lines of 32-point segments run two (at
+// most 128 registers a thread; as many tiles in flight as half the SM's
+// shared memory holds: 3 in FP32, 1 for a 256-point FP64 line): one CTA of 8
+// warps, whose segments all wait on the same tile, cannot keep an SM's issue
+// slots busy.  The FP64 RK-fused store is the exception: its three extra
+// global streams (dQ, du, Q) want the deeper pipeline of one CTA with three
+// tiles in flight (256^3 Taylor-Green step, z lines: 5.5 TB/s against 5.1).
+template <typename T, int M, int MS, int CPS>
+__global__ void __launch_bounds__(MS == 16 ? 512 : 256, CPS)
     k_compact_tma(const __grid_constant__ CUtensorMap map, const __grid_constant__ CompactParams P,
                   const __grid_constant__ TileLineParams TL,
                   const T* __restrict__ Gg, const FieldView out, const int mode, const int count, const int NS,
@@ -196,16 +222,7 @@ __global__ void __launch_bounds__(MS == 16 ? 512 : 256, tma_ctas_per_sm<T>(MS))
         T y[MS];
         {
             T wv[MS + 2 * M];
-#pragma unroll
-            for (int j = 0; j < MS + 2 * M; ++j) {
-                if (j < m + 2 * M) {
-                    int g = off - M + j;
-                    g = g < 0 ? g + n : (g >= n ? g - n : g);
-                    wv[j] = tile[g * kLanes + lane];
-                } else {
-                    wv[j] = T(0);
-                }
-            }
+            gather_window<T, M, MS, kLanes>(tile + lane, off, n, 0, true, false, false, wv);
 #pragma unroll
             for (int i = 0; i < MS; ++i) {
                 T acc;
@@ -393,9 +410,10 @@ __device__ __forceinline__ void tg_correct(const TileGenParams& G, T (&y)[MS], c
 // two tail values per segment).  Segment coefficients come from the plan's
 // three segment classes (first, interior, last) as kernel parameters, the
 // closure stencils read the whole line from the tile, and the reduced inverse
-// (2qS)^2 sits in shared memory.
+// (2qS)^2 sits in shared memory.  Two CTAs share an SM (at most 128 registers
+// a thread), each with the tiles in flight that half the shared memory holds.
 template <typename T, int Q, int M, int MS>
-__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1)
+__global__ void __launch_bounds__(256, 2)
     k_compact_tg(const __grid_constant__ CUtensorMap map, const __grid_constant__ CompactParams P,
                  const __grid_constant__ TileGenParams GP, const T* __restrict__ tab, const FieldView out,
                  const int mode, const int count, const int NS, const RkEpilogue rk, const int H,
@@ -468,14 +486,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1)
         T y[MS];
         {
             T wv[MS + 2 * M];
-#pragma unroll
-            for (int j = 0; j < MS + 2 * M; ++j) {
-                int g = off - M + j;
-                if (periodic) g = g < 0 ? g + n : (g >= n ? g - n : g);
-                // clamped values are never used; an open end reads its halo row
-                else g = g < 0 ? (P.lo_open ? g : 0) : (g >= n ? (P.hi_open ? g : n - 1) : g);
-                wv[j] = tile[(g + H) * kLanes + lane];
-            }
+            gather_window<T, M, MS, kLanes>(tile + lane, off, n, H, periodic, P.lo_open, P.hi_open, wv);
 #pragma unroll
             for (int i = 0; i < MS; ++i) {
                 T acc;
@@ -603,10 +614,12 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1)
 // group of 32 lines is 32 rows of the field: every warp copies whole rows with
 // coalesced 4/8-byte cp.async into a transposed shared-memory tile
 // tile[g * 33 + lane] (pitch 33: the column reads of the segment threads and
-// the row writes of the copies are both free of bank conflicts).  NS tiles are
-// in flight; the compute is that of k_compact_tg (three segment classes,
-// closures, reduced inverse in shared memory); results go back through a
-// second transposed tile so that the stores are coalesced rows again.
+// the row writes of the copies are both free of bank conflicts).  The compute
+// is that of k_compact_tg (three segment classes, closures, reduced inverse in
+// shared memory); results go back into the same tile, so that the stores are
+// coalesced rows again, and the tile is refilled once they are out.  Two CTAs
+// share an SM (at most 128 registers a thread), each with one FP64 tile or two
+// FP32 tiles: while one CTA waits on its copies the other computes.
 __device__ __forceinline__ void cp_async_el(void* dst, const void* src, int bytes) {
     if (bytes == 8)
         asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_addr(dst)), "l"(src) : "memory");
@@ -618,7 +631,7 @@ template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 
 template <typename T, int Q, int M, int MS, int NS>
-__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1)
+__global__ void __launch_bounds__(256, 2)
     k_compact_xt(const __grid_constant__ CompactParams P, const __grid_constant__ TileGenParams GP,
                  const T* __restrict__ tab, const FieldView in, const FieldView out, const int mode, const int count,
                  const int H, T* __restrict__ iface) {
@@ -631,8 +644,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1)
     // end (tile row g + H is line index g); the output tile holds the line
     const size_t tile_elems = (size_t)(n + 2 * H) * TP;
     T* tin = reinterpret_cast<T*>(smem_raw);
-    T* tout = tin + tile_elems * NS;
-    T* red = tout + (size_t)n * TP;
+    T* red = tin + tile_elems * NS;
     const int RP = N + 1;
     T* Gs = red + (size_t)kLanes * RP;
 
@@ -690,13 +702,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1)
         T y[MS];
         {
             T wv[MS + 2 * M];
-#pragma unroll
-            for (int j = 0; j < MS + 2 * M; ++j) {
-                int g = off - M + j;
-                if (periodic) g = g < 0 ? g + n : (g >= n ? g - n : g);
-                else g = g < 0 ? (P.lo_open ? g : 0) : (g >= n ? (P.hi_open ? g : n - 1) : g);
-                wv[j] = tile[(g + H) * TP + lane];
-            }
+            gather_window<T, M, MS, TP>(tile + lane, off, n, H, periodic, P.lo_open, P.hi_open, wv);
 #pragma unroll
             for (int i = 0; i < MS; ++i) {
                 T acc;
@@ -737,8 +743,6 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1)
                 }
             }
         }
-        __syncthreads();                  // the tile is consumed: refill it
-        issue(w + NS * gridDim.x, stage);
         if (cls == 0) tg_solve<T, Q, MS, 0>(GP, y);
         else if (cls == 1) tg_solve<T, Q, MS, 1>(GP, y);
         else tg_solve<T, Q, MS, 2>(GP, y);
@@ -748,7 +752,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1)
             rl[2 * Q * seg + t] = y[t];
             rl[2 * Q * seg + Q + t] = y[MS - Q + t];
         }
-        __syncthreads();   // interface values visible; also the previous group's stores from tout are done
+        __syncthreads();   // interface values visible; every thread has read the tile
         T zp[Q], zn[Q];
         tg_interface<T, Q>(Gs, rl, N, prev, next, has_prev, has_next, zp, zn);
         if (cls == 0) tg_correct<T, Q, MS, 0>(GP, y, zp, zn);
@@ -770,6 +774,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1)
                 }
             }
         }
+        T* tout = tin + tile_elems * stage + (size_t)H * TP;   // results go back into the input tile
 #pragma unroll
         for (int i = 0; i < MS; ++i) tout[(size_t)(off + i) * TP + lane] = y[i];
         __syncthreads();   // the output tile is complete
@@ -788,7 +793,8 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1)
                 }
             }
         }
-        // tout and red are rewritten only after the next group's barriers
+        __syncthreads();   // the tile is written out: refill it
+        issue(w + NS * gridDim.x, stage);
     }
     cp_async_wait<0>();
 }
@@ -820,16 +826,26 @@ int num_sms() {
     return g_num_sms;
 }
 
-template <typename T, int M, int MS>
+// Tiles in flight (1 to 3) for a CTA that shares its SM with another: half of
+// the 227 KB, less 1 KB the runtime reserves per CTA and the CTA's own
+// interface buffers.  A tile is at most 256 rows of 32 lanes (64 KB in FP64).
+inline int tiles_for_two_ctas(size_t tile_bytes, size_t extra) {
+    const size_t fit = ((227 * 1024) / 2 - 1024 - extra) / tile_bytes;
+    return fit < 1 ? 1 : (fit > 3 ? 3 : (int)fit);
+}
+
+template <typename T, int M, int MS, int CPS>
 void launch_tma_ms(const CompactPlan& plan, const CUtensorMap& map, const FieldView& out, int count, int mode,
                   cudaStream_t st, const T* G, const RkEpilogue& rk) {
     const CompactParams& P = plan.P;
-    constexpr int per_sm = tma_ctas_per_sm<T>(MS);
-    const int NS = sizeof(T) == 8 || per_sm == 2 ? 3 : 4;
+    constexpr int per_sm = CPS;
     const int N = 2 * P.S;
-    const size_t smem = sizeof(T) * (size_t)P.n * kLanes * NS + 8 * sizeof(uint64_t) +
-                        sizeof(T) * ((size_t)kLanes * (N + 1) + (size_t)N * N);
-    auto kern = k_compact_tma<T, M, MS>;
+    const size_t extra = 8 * sizeof(uint64_t) + sizeof(T) * ((size_t)kLanes * (N + 1) + (size_t)N * N);
+    const size_t tile_bytes = sizeof(T) * (size_t)P.n * kLanes;
+    int NS = sizeof(T) == 8 ? 3 : 4;
+    if (per_sm == 2) NS = tiles_for_two_ctas(tile_bytes, extra);
+    const size_t smem = tile_bytes * NS + extra;
+    auto kern = k_compact_tma<T, M, MS, CPS>;
     static int configured = 0;
     if (configured < (int)smem) {
         CLES_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -853,8 +869,16 @@ template <typename T, int M>
 bool launch_tma_m(const CompactPlan& plan, const CUtensorMap& map, const FieldView& out, int count, int mode,
                   cudaStream_t st, const T* G, const RkEpilogue& rk) {
     switch (plan.TL.m) {
-        case 32: launch_tma_ms<T, M, 32>(plan, map, out, count, mode, st, G, rk); return true;
-        case 16: launch_tma_ms<T, M, 16>(plan, map, out, count, mode, st, G, rk); return true;
+        case 32:
+            if constexpr (sizeof(T) == 8) {
+                if (mode == OUT_RK) {
+                    launch_tma_ms<T, M, 32, 1>(plan, map, out, count, mode, st, G, rk);
+                    return true;
+                }
+            }
+            launch_tma_ms<T, M, 32, 2>(plan, map, out, count, mode, st, G, rk);
+            return true;
+        case 16: launch_tma_ms<T, M, 16, 1>(plan, map, out, count, mode, st, G, rk); return true;
         default: return false;
     }
 }
@@ -863,10 +887,11 @@ template <typename T, int Q, int M, int MS>
 void launch_tg_ms(const CompactPlan& plan, const CUtensorMap& map, const FieldView& out, int count, int mode,
                   cudaStream_t st, const T* tab, const RkEpilogue& rk, int H, T* iface) {
     const CompactParams& P = plan.P;
-    const int NS = 3;
     const int N = 2 * Q * P.S;
-    const size_t smem = sizeof(T) * (size_t)(P.n + 2 * H) * kLanes * NS + 8 * sizeof(uint64_t) +
-                        sizeof(T) * ((size_t)kLanes * (N + 1) + (size_t)N * N);
+    const size_t extra = 8 * sizeof(uint64_t) + sizeof(T) * ((size_t)kLanes * (N + 1) + (size_t)N * N);
+    const size_t tile_bytes = sizeof(T) * (size_t)(P.n + 2 * H) * kLanes;
+    const int NS = tiles_for_two_ctas(tile_bytes, extra);
+    const size_t smem = tile_bytes * NS + extra;
     auto kern = k_compact_tg<T, Q, M, MS>;
     static int configured = 0;
     if (configured < (int)smem) {
@@ -880,11 +905,10 @@ void launch_tg_ms(const CompactPlan& plan, const CUtensorMap& map, const FieldVi
     }
     const int gx = (P.nx + kLanes - 1) / kLanes;
     const int work = gx * (P.dim == 1 ? P.nz : P.ny) * count;
-    // lines of fewer than 8 segments leave an SM with few warps: run as many
-    // persistent CTAs per SM as shared memory and 256 threads per SM-slot allow;
-    // FP32 (at most 128 registers a thread) runs at least two
+    // at least two persistent CTAs per SM (the kernel is built for two), more
+    // for lines of fewer than 8 segments, as shared memory allows
     int per_sm = 256 / (kLanes * P.S);
-    if (sizeof(T) == 4 && per_sm < 2) per_sm = 2;
+    if (per_sm < 2) per_sm = 2;
     const int by_smem = (int)((227 * 1024) / (smem + 1024));
     if (per_sm > by_smem) per_sm = by_smem;
     if (per_sm < 1) per_sm = 1;
@@ -923,9 +947,9 @@ template <typename T, int Q, int M, int MS>
 void launch_xt_ms(const CompactPlan& plan, const FieldView& in, const FieldView& out, int count, int mode,
                   cudaStream_t st, const T* tab, int H, T* iface) {
     const CompactParams& P = plan.P;
-    constexpr int NS = 2;
+    constexpr int NS = sizeof(T) == 8 ? 1 : 2;
     const int N = 2 * Q * P.S;
-    const size_t smem = sizeof(T) * ((size_t)(P.n + 2 * H) * (kLanes + 1) * NS + (size_t)P.n * (kLanes + 1) +
+    const size_t smem = sizeof(T) * ((size_t)(P.n + 2 * H) * (kLanes + 1) * NS +
                                      (size_t)kLanes * (N + 1) + (size_t)N * N);
     auto kern = k_compact_xt<T, Q, M, MS, NS>;
     static int configured = 0;
@@ -940,10 +964,10 @@ void launch_xt_ms(const CompactPlan& plan, const FieldView& in, const FieldView&
     }
     const int64_t groups = (P.lines + kLanes - 1) / kLanes;
     const int64_t work = groups * count;
-    // as k_compact_tg: several persistent CTAs per SM for lines of fewer than 8
-    // segments, and at least two for FP32
+    // at least two persistent CTAs per SM (the kernel is built for two), more
+    // for lines of fewer than 8 segments, as shared memory allows
     int per_sm = 256 / (kLanes * P.S);
-    if (sizeof(T) == 4 && per_sm < 2) per_sm = 2;
+    if (per_sm < 2) per_sm = 2;
     const int by_smem = (int)((227 * 1024) / (smem + 1024));
     if (per_sm > by_smem) per_sm = by_smem;
     if (per_sm < 1) per_sm = 1;
