@@ -696,6 +696,19 @@ __global__ void __launch_bounds__(256, 2)
     int it = 0;
     for (int w = blockIdx.x; w < work; w += gridDim.x, ++it) {
         const int stage = it % NS;
+        if (mode == OUT_SUBTRACT) {
+            // the subtract store reads this group's output rows: pull them
+            // into L2 while the group's rows are still arriving (lane l < the
+            // row's 128-byte lines takes line l; its offset stays below n)
+            const int c = w / groups, g0 = (w - c * groups) * kLanes;
+            const T* obase = reinterpret_cast<const T*>(out.base) + (int64_t)c * out.comp_stride;
+            const int per_row = (n * (int)sizeof(T) + 127) / 128;
+            for (int l = seg; l < kLanes; l += nwarps) {
+                const int line = g0 + l;
+                if (line >= lines) break;
+                if (lane < per_row) prefetch_l2(obase + row_of(out, line) + lane * (128 / (int)sizeof(T)));
+            }
+        }
         cp_async_wait<NS - 1>();
         __syncthreads();   // this group's rows are in the tile for every thread
         const T* tile = tin + tile_elems * stage;
@@ -785,11 +798,26 @@ __global__ void __launch_bounds__(256, 2)
                 const int line = g0 + l;
                 if (line >= lines) break;
                 T* row = base + row_of(out, line);
-                for (int g = lane; g < n; g += kLanes) {
-                    const T v = tout[(size_t)g * TP + l];
-                    if (mode == OUT_STORE) row[g] = v;
-                    else if (mode == OUT_NEGATE) row[g] = -v;
-                    else row[g] = row[g] - v;
+                if (mode == OUT_SUBTRACT) {
+                    // read the row's old values four a lane before writing,
+                    // so that their loads are in flight together
+                    constexpr int kPerLane = 4;
+                    for (int g0 = lane; g0 < n; g0 += kPerLane * kLanes) {
+                        T old[kPerLane];
+#pragma unroll
+                        for (int k = 0; k < kPerLane; ++k)
+                            if (g0 + k * kLanes < n) old[k] = row[g0 + k * kLanes];
+#pragma unroll
+                        for (int k = 0; k < kPerLane; ++k) {
+                            const int g = g0 + k * kLanes;
+                            if (g < n) row[g] = old[k] - tout[(size_t)g * TP + l];
+                        }
+                    }
+                } else {
+                    for (int g = lane; g < n; g += kLanes) {
+                        const T v = tout[(size_t)g * TP + l];
+                        row[g] = mode == OUT_NEGATE ? -v : v;
+                    }
                 }
             }
         }
