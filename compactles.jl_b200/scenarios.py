@@ -21,6 +21,10 @@ builders serve the CUDA library and the CPU oracle.
   on the CPU oracle and on the device at the same step, because the upper
   modes are only 8-16 cells long.
 * taylor_green_box: the README Taylor-Green vortex on an n^3 periodic box.
+* slip_wall_box: the same velocity field on [0, pi]^3 closed by slip walls on
+  all six faces (the field's normal velocity vanishes on each of them): every
+  line is closed, so the x pass runs the closed-line x kernel with its
+  subtract store and the z pass the closed-line RK-fused store.
 * he_co2_shock_tube: examples/shock_tube.jl -- a 4 m closed tube of a NASA-9
   He/CO2 mixture at 300 K, 10 atm He driver against 1 atm He, diaphragm at
   2 m, sinusoidally perturbed He/CO2 contact at 3 m (amplitude 10% of the
@@ -108,6 +112,16 @@ def taylor_green_box(schemes, n, tfinal=1.0, precision="fp64"):
     tp = 2 * math.pi
     desc = solver_desc((n, n, n), (tp, tp, tp), prob.bcs, deriv, filt, precision=precision)
     return desc, initialize(desc, prob.ic), tfinal
+
+
+def slip_wall_box(schemes, n, tfinal=1.0, precision="fp64"):
+    deriv, filt = schemes
+    wall = (SlipWallBC(), SlipWallBC())
+    desc = solver_desc((n, n, n), (math.pi,) * 3, (wall, wall, wall), deriv, filt, precision=precision)
+
+    def ic(x, y, z):
+        return Prim(u=(np.sin(x) * np.cos(y), -np.cos(x) * np.sin(y), 0.0 * z), p=71.43 + 0.0 * x, rho=1.0 + 0.0 * x)
+    return desc, initialize(desc, ic), tfinal
 
 
 def he_co2_shock_tube(schemes, eos, nx=768, ny=48, tfinal=2.5e-3, precision="fp64", retries=4):

@@ -85,3 +85,20 @@ def test_volume_quadrature(orc):
     h = cl.grid_spacing(dc)[0]
     assert abs(v - 0.5) <= 1e-3 * 0.5
     assert v - 0.5 < h * h
+
+
+def test_slip_wall_box_has_no_flow_through_its_walls():
+    """The closed-line benchmark box: every face a slip wall, and the field's
+    momentum normal to each face zero on that face."""
+    n = 24
+    desc, Q0, _ = cl.scenarios.slip_wall_box((cl.lele_d1_6(), cl.compact_filter(0.45)), n)
+    assert tuple(desc.n_global) == (n, n, n)
+    Qi = Q0[(slice(None),) + cl.interior_slices(desc)]      # [comp][z][y][x]
+    assert Qi.shape == (5, n, n, n)
+    scale = np.abs(Qi[1:4]).max()
+    assert scale > 0.5
+    for comp, axis in ((1, 3), (2, 2), (3, 1)):             # rho u on x faces, rho v on y, rho w on z
+        for end in (0, n - 1):
+            face = np.take(Qi[comp], end, axis=axis - 1)
+            assert np.abs(face).max() <= 1e-12 * scale
+    assert np.allclose(Qi[0], 1.0)
