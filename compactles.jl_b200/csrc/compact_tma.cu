@@ -5,11 +5,11 @@
 // y and z lines are strided in memory (x is contiguous), so a group of 32
 // consecutive-x lines is a 2-D box {32 x, n along the line} of the field: one
 // `cp.async.bulk.tensor` copy brings it into shared memory as tile[g][lane],
-// which every thread then reads by column without bank conflicts.  The kernel
-// is persistent (two CTAs per SM for 32-point segments, one for 16-point
-// ones) and keeps NS tiles in flight: the copy of a
-// later group is issued as soon as the current tile has been read into
-// registers, so HBM is busy while the segments solve.  Compute per group is
+// which every thread then reads by column without bank conflicts.  The
+// kernels are persistent (two CTAs per SM for 32-point segments, one for
+// 16-point ones and for the FP64 RK-fused store of k_compact_tma) and keep NS
+// tiles in flight: the copy of a later group is issued as soon as the current
+// tile has been read into registers, so HBM is busy while the segments solve.  Compute per group is
 // the segmented spike solve of compact.cu (fill, per-segment Thomas sweep,
 // interface values from the reduced inverse, correction) with the segment
 // coefficients as kernel parameters; results go straight from registers to
